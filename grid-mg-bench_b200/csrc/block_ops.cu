@@ -1,0 +1,566 @@
+// block_ops.cu -- block projection, promotion and orthonormalisation (CUDA cores).
+//
+// Restates blockLutedInnerProduct / blockLutedAxpy / blockLutedOrthonormalise
+// (include/CoarsenedMatrixUpstreamImprovedDirsaveLut.h:70-240, multi-RHS form
+// ...LutMRHS.h:70-236) as per-block complex GEMMs:
+//
+//   project   C_c (R x N)  = F_c^T (R x K) conj(V_c)^T (K x N)   K = bv * dof
+//   promote   F_c (K x R)  = V_c^T (K x N) C_c (N x R)
+//   ortho     V_c <- conj(L^{-1}) V_c  with  L L^dag = V_c V_c^dag  (Cholesky-QR;
+//             the same Q as the reference's modified Gram-Schmidt in exact
+//             arithmetic, since a thin QR with positive diagonal is unique)
+//
+// The basis is kept block-major, basis_blk[c][i][k], k = sb*dof + a with sb the
+// lexicographic in-block site index (CoarseningLookupTableRework.h:156-163),
+// so one block's N x K panel is contiguous.  Fine fields stay in the caller's
+// [site][rhs][dof] layout and are gathered through blk_sites[c][sb].
+#include <algorithm>
+#include <cmath>
+
+#include "gmg_internal.cuh"
+
+namespace gmg {
+
+template <class T> struct ctype;
+template <> struct ctype<double> { typedef double2 t; };
+template <> struct ctype<float> { typedef float2 t; };
+
+template <class Cx> __device__ __forceinline__ Cx cfma(Cx acc, Cx a, Cx b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+  return acc;
+}
+// acc += conj(a) b
+template <class Cx> __device__ __forceinline__ Cx cfma_conj(Cx acc, Cx a, Cx b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(-a.y, b.x, acc.y);
+  return acc;
+}
+
+static int num_sms() {
+  int dev = 0, n = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n;
+}
+
+// ---------------------------------------------------------------------------
+// tables and basis layout
+// ---------------------------------------------------------------------------
+gmg_status agg_build_tables(gmg_agg* h, cudaStream_t s) {
+  const int64_t Vc = h->cdims.vol();
+  std::vector<int32_t> t(Vc * h->bv);
+  for (int64_t sc = 0; sc < Vc; ++sc) {
+    int cc[4];
+    int64_t q = sc;
+    for (int d = 0; d < 4; ++d) { cc[d] = (int)(q % h->cdims.d[d]); q /= h->cdims.d[d]; }
+    for (int sb = 0; sb < h->bv; ++sb) {
+      int cb[4], cf[4];
+      int r = sb;
+      for (int d = 0; d < 4; ++d) { cb[d] = r % h->b[d]; r /= h->b[d]; }
+      for (int d = 0; d < 4; ++d) cf[d] = cc[d] * h->b[d] + cb[d];
+      int64_t sf = 0;
+      for (int d = 3; d >= 0; --d) sf = sf * h->fdims.d[d] + cf[d];
+      t[sc * h->bv + sb] = (int32_t)sf;
+    }
+  }
+  GMG_TRY(h->blk_sites.alloc(t.size() * sizeof(int32_t)));
+  GMG_CUDA(cudaMemcpyAsync(h->blk_sites.p, t.data(), t.size() * sizeof(int32_t),
+                           cudaMemcpyHostToDevice, s));
+  GMG_CUDA(cudaStreamSynchronize(s));
+  return GMG_OK;
+}
+
+// basis [i][site][dof] <-> basis_blk [c][i][sb*dof + a]
+template <bool TO_BLK>
+__global__ void basis_layout_kernel(const double2* __restrict__ src, double2* __restrict__ dst,
+                                    const int32_t* __restrict__ blk_sites, int64_t Vc, int N, int bv,
+                                    int dof, int64_t Vf) {
+  const int64_t K = (int64_t)bv * dof;
+  const int64_t total = Vc * N * K;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = e % K;
+    const int64_t i = (e / K) % N;
+    const int64_t c = e / (K * N);
+    const int64_t sf = blk_sites[c * bv + k / dof];
+    const int64_t fi = (i * Vf + sf) * dof + k % dof;
+    if (TO_BLK) dst[e] = src[fi];
+    else dst[fi] = src[e];
+  }
+}
+
+gmg_status agg_basis_to_blocked(gmg_agg* h, const double* basis_dev, cudaStream_t s) {
+  const int64_t Vc = h->cdims.vol(), Vf = h->fdims.vol();
+  const int64_t total = Vc * h->N * (int64_t)h->bv * h->dof;
+  GMG_TRY(h->basis_blk.alloc(total * sizeof(double2)));
+  const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 64);
+  basis_layout_kernel<true><<<grid, 256, 0, s>>>(reinterpret_cast<const double2*>(basis_dev),
+                                                  h->basis_blk.as<double2>(), h->blk_sites.as<int32_t>(),
+                                                  Vc, h->N, h->bv, h->dof, Vf);
+  GMG_CUDA(cudaGetLastError());
+  h->basis_f_ok = false;
+  return GMG_OK;
+}
+
+gmg_status agg_basis_from_blocked(gmg_agg* h, double* basis_dev, cudaStream_t s) {
+  const int64_t Vc = h->cdims.vol(), Vf = h->fdims.vol();
+  const int64_t total = Vc * h->N * (int64_t)h->bv * h->dof;
+  const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 64);
+  basis_layout_kernel<false><<<grid, 256, 0, s>>>(h->basis_blk.as<double2>(),
+                                                   reinterpret_cast<double2*>(basis_dev),
+                                                   h->blk_sites.as<int32_t>(), Vc, h->N, h->bv, h->dof, Vf);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+__global__ void d2f_kernel(const double2* __restrict__ a, float2* __restrict__ b, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x)
+    b[e] = make_float2((float)a[e].x, (float)a[e].y);
+}
+
+gmg_status agg_prepare_f32(gmg_agg* h, cudaStream_t s) {
+  if (h->basis_f_ok) return GMG_OK;
+  const int64_t n = h->cdims.vol() * h->N * (int64_t)h->bv * h->dof;
+  GMG_TRY(h->basis_blk_f.alloc(n * sizeof(float2)));
+  d2f_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 148 * 64), 256, 0, s>>>(
+      h->basis_blk.as<double2>(), h->basis_blk_f.as<float2>(), n);
+  GMG_CUDA(cudaGetLastError());
+  h->basis_f_ok = true;
+  return GMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// project: coarse[c][r][i] = sum_k conj(V[c][i][k]) F[site(c,k)][r][k % dof]
+// CTA per block; K chunked by KS sites; TR x TB register tiles over (rhs, i).
+// `mask` (nullable, int8 per fine site) restricts the sum to a face / parity
+// subset as the masked LUTs of CoarsenOperator do (...DirsaveLut.h:985-1005).
+// ---------------------------------------------------------------------------
+template <class T, int TR, int TB, int KS>
+__global__ void __launch_bounds__(256) project_kernel(
+    const typename ctype<T>::t* __restrict__ basis, const int32_t* __restrict__ blk_sites,
+    const typename ctype<T>::t* __restrict__ fine, typename ctype<T>::t* __restrict__ coarse,
+    int Vc, int N, int dof, int bv, int nrhs, const int8_t* __restrict__ mask, int accumulate) {
+  typedef typename ctype<T>::t Cx;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int KC = KS * dof;
+  Cx* VT = reinterpret_cast<Cx*>(smem_raw);  // [KC][N]
+  Cx* FT = VT + KC * N;                       // [KC][R]
+  const int R = nrhs;
+  const int NBT = (N + TB - 1) / TB, NRT = (R + TR - 1) / TR;
+  const int ntiles = NBT * NRT;
+  const int t = threadIdx.x, bt = t % NBT, rt = t / NBT;
+  const int64_t K = (int64_t)bv * dof;
+  for (int c = blockIdx.x; c < Vc; c += gridDim.x) {
+    Cx acc[TR][TB];
+#pragma unroll
+    for (int j = 0; j < TR; ++j)
+#pragma unroll
+      for (int i = 0; i < TB; ++i) acc[j][i] = Cx{0, 0};
+    const Cx* Vb = basis + (int64_t)c * N * K;
+    for (int sb0 = 0; sb0 < bv; sb0 += KS) {
+      const int ns = min(KS, bv - sb0);
+      const int kc = ns * dof;
+      __syncthreads();
+      for (int e = t; e < N * kc; e += blockDim.x) {
+        const int i = e / kc, kk = e % kc;
+        VT[kk * N + i] = Vb[(int64_t)i * K + (int64_t)sb0 * dof + kk];
+      }
+      for (int e = t; e < ns * R * dof; e += blockDim.x) {
+        const int sl = e / (R * dof), rem = e % (R * dof);
+        const int r = rem / dof, a = rem % dof;
+        const int sf = blk_sites[(int64_t)c * bv + sb0 + sl];
+        Cx v = fine[((int64_t)sf * nrhs + r) * dof + a];
+        if (mask && !mask[sf]) v = Cx{0, 0};
+        FT[(sl * dof + a) * R + r] = v;
+      }
+      __syncthreads();
+      if (t < ntiles) {
+        for (int kk = 0; kk < kc; ++kk) {
+          Cx a[TB], x[TR];
+#pragma unroll
+          for (int i = 0; i < TB; ++i) {
+            const int ii = bt * TB + i;
+            a[i] = ii < N ? VT[kk * N + ii] : Cx{0, 0};
+          }
+#pragma unroll
+          for (int j = 0; j < TR; ++j) {
+            const int r = rt * TR + j;
+            x[j] = r < R ? FT[kk * R + r] : Cx{0, 0};
+          }
+#pragma unroll
+          for (int j = 0; j < TR; ++j)
+#pragma unroll
+            for (int i = 0; i < TB; ++i) acc[j][i] = cfma_conj(acc[j][i], a[i], x[j]);
+        }
+      }
+    }
+    if (t < ntiles) {
+#pragma unroll
+      for (int j = 0; j < TR; ++j) {
+        const int r = rt * TR + j;
+        if (r >= R) continue;
+#pragma unroll
+        for (int i = 0; i < TB; ++i) {
+          const int ii = bt * TB + i;
+          if (ii >= N) continue;
+          Cx* o = coarse + ((int64_t)c * nrhs + r) * N + ii;
+          if (accumulate) { Cx v = *o; v.x += acc[j][i].x; v.y += acc[j][i].y; *o = v; }
+          else *o = acc[j][i];
+        }
+      }
+    }
+  }
+}
+
+template <class T, int TR, int TB, int KS>
+static gmg_status launch_project(gmg_agg* h, const void* basis, int nrhs, const void* fine,
+                                 void* coarse, const int8_t* mask, int accumulate, cudaStream_t s) {
+  typedef typename ctype<T>::t Cx;
+  const int N = h->N, R = nrhs;
+  const int ntiles = ((N + TB - 1) / TB) * ((R + TR - 1) / TR);
+  GMG_CHECK(ntiles <= 256, GMG_ERR_UNSUPPORTED, "project: nbasis x nrhs too large");
+  const int threads = std::max(32, (ntiles + 31) / 32 * 32);
+  const size_t smem = sizeof(Cx) * (size_t)KS * h->dof * (N + R);
+  GMG_CHECK(smem <= 227 * 1024, GMG_ERR_UNSUPPORTED, "project: shared-memory tile too large");
+  auto kern = project_kernel<T, TR, TB, KS>;
+  GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int Vc = (int)h->cdims.vol();
+  const int grid = std::min(Vc, num_sms() * 16);
+  kern<<<grid, threads, smem, s>>>(reinterpret_cast<const Cx*>(basis), h->blk_sites.as<int32_t>(),
+                                   reinterpret_cast<const Cx*>(fine), reinterpret_cast<Cx*>(coarse),
+                                   Vc, N, h->dof, h->bv, nrhs, mask, accumulate);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status agg_project(gmg_agg* h, int compute, int vec_prec, int nrhs, const void* fine,
+                       void* coarse, const int32_t* mask_unused, cudaStream_t s) {
+  (void)mask_unused;
+  GMG_CHECK(compute == vec_prec, GMG_ERR_UNSUPPORTED, "project: compute and vector precision differ");
+  if (compute == GMG_F64) {
+    if (nrhs >= 4) return launch_project<double, 4, 4, 4>(h, h->basis_blk.p, nrhs, fine, coarse, nullptr, 0, s);
+    return launch_project<double, 1, 2, 4>(h, h->basis_blk.p, nrhs, fine, coarse, nullptr, 0, s);
+  }
+  if (compute == GMG_F32) {
+    GMG_TRY(agg_prepare_f32(h, s));
+    if (nrhs >= 4) return launch_project<float, 4, 4, 4>(h, h->basis_blk_f.p, nrhs, fine, coarse, nullptr, 0, s);
+    return launch_project<float, 1, 2, 4>(h, h->basis_blk_f.p, nrhs, fine, coarse, nullptr, 0, s);
+  }
+  return fail(GMG_ERR_UNSUPPORTED, "project: unsupported precision");
+}
+
+// masked FP64 single-RHS projection used by the coarse-operator construction
+gmg_status agg_project_masked_f64(gmg_agg* h, int nrhs, const double* fine, double* coarse,
+                                  const int8_t* mask, cudaStream_t s) {
+  if (nrhs >= 4) return launch_project<double, 4, 4, 4>(h, h->basis_blk.p, nrhs, fine, coarse, mask, 0, s);
+  return launch_project<double, 1, 2, 4>(h, h->basis_blk.p, nrhs, fine, coarse, mask, 0, s);
+}
+
+// ---------------------------------------------------------------------------
+// promote: F[site(c,k)][r][k%dof] = sum_i V[c][i][k] C[c][r][i]
+// ---------------------------------------------------------------------------
+template <class T, int TK, int TR, int KS>
+__global__ void __launch_bounds__(256) promote_kernel(
+    const typename ctype<T>::t* __restrict__ basis, const int32_t* __restrict__ blk_sites,
+    const typename ctype<T>::t* __restrict__ coarse, typename ctype<T>::t* __restrict__ fine, int Vc,
+    int N, int dof, int bv, int nrhs) {
+  typedef typename ctype<T>::t Cx;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int KC = KS * dof;
+  const int R = nrhs;
+  Cx* CT = reinterpret_cast<Cx*>(smem_raw);  // [N][R]
+  Cx* VS = CT + N * R;                        // [N][KC]
+  const int NKT = KC / TK, NRT = (R + TR - 1) / TR;
+  const int ntiles = NKT * NRT;
+  const int t = threadIdx.x;
+  const int64_t K = (int64_t)bv * dof;
+  for (int c = blockIdx.x; c < Vc; c += gridDim.x) {
+    __syncthreads();
+    for (int e = t; e < N * R; e += blockDim.x) {
+      const int r = e / N, i = e % N;
+      CT[i * R + r] = coarse[((int64_t)c * nrhs + r) * N + i];
+    }
+    const Cx* Vb = basis + (int64_t)c * N * K;
+    for (int sb0 = 0; sb0 < bv; sb0 += KS) {
+      const int ns = min(KS, bv - sb0);
+      const int kc = ns * dof;
+      __syncthreads();
+      for (int e = t; e < N * kc; e += blockDim.x) {
+        const int i = e / kc, kk = e % kc;
+        VS[i * KC + kk] = Vb[(int64_t)i * K + (int64_t)sb0 * dof + kk];
+      }
+      __syncthreads();
+      for (int tile = t; tile < ntiles; tile += blockDim.x) {
+        const int kt = tile % NKT, rt = tile / NKT;
+        if (kt * TK >= kc) continue;
+        Cx acc[TR][TK];
+#pragma unroll
+        for (int j = 0; j < TR; ++j)
+#pragma unroll
+          for (int q = 0; q < TK; ++q) acc[j][q] = Cx{0, 0};
+        for (int i = 0; i < N; ++i) {
+          Cx v[TK], x[TR];
+#pragma unroll
+          for (int q = 0; q < TK; ++q) v[q] = VS[i * KC + kt * TK + q];
+#pragma unroll
+          for (int j = 0; j < TR; ++j) {
+            const int r = rt * TR + j;
+            x[j] = r < R ? CT[i * R + r] : Cx{0, 0};
+          }
+#pragma unroll
+          for (int j = 0; j < TR; ++j)
+#pragma unroll
+            for (int q = 0; q < TK; ++q) acc[j][q] = cfma(acc[j][q], x[j], v[q]);
+        }
+        const int k0 = kt * TK;
+        const int sl = k0 / dof, a0 = k0 % dof;  // TK divides dof: one site per tile
+        const int sf = blk_sites[(int64_t)c * bv + sb0 + sl];
+#pragma unroll
+        for (int j = 0; j < TR; ++j) {
+          const int r = rt * TR + j;
+          if (r >= R) continue;
+          Cx* o = fine + ((int64_t)sf * nrhs + r) * dof + a0;
+#pragma unroll
+          for (int q = 0; q < TK; ++q) o[q] = acc[j][q];
+        }
+      }
+    }
+  }
+}
+
+template <class T, int TK, int TR, int KS>
+static gmg_status launch_promote(gmg_agg* h, const void* basis, int nrhs, const void* coarse,
+                                 void* fine, cudaStream_t s) {
+  typedef typename ctype<T>::t Cx;
+  const int N = h->N, R = nrhs, dof = h->dof;
+  GMG_CHECK(dof % TK == 0, GMG_ERR_UNSUPPORTED, "promote: dof not a multiple of the k tile");
+  const int ntiles = (KS * dof / TK) * ((R + TR - 1) / TR);
+  const int threads = std::min(256, std::max(32, (ntiles + 31) / 32 * 32));
+  const size_t smem = sizeof(Cx) * ((size_t)N * R + (size_t)N * KS * dof);
+  GMG_CHECK(smem <= 227 * 1024, GMG_ERR_UNSUPPORTED, "promote: shared-memory tile too large");
+  auto kern = promote_kernel<T, TK, TR, KS>;
+  GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int Vc = (int)h->cdims.vol();
+  const int grid = std::min(Vc, num_sms() * 16);
+  kern<<<grid, threads, smem, s>>>(reinterpret_cast<const Cx*>(basis), h->blk_sites.as<int32_t>(),
+                                   reinterpret_cast<const Cx*>(coarse), reinterpret_cast<Cx*>(fine),
+                                   Vc, N, dof, h->bv, nrhs);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status agg_promote(gmg_agg* h, int compute, int vec_prec, int nrhs, const void* coarse,
+                       void* fine, cudaStream_t s) {
+  GMG_CHECK(compute == vec_prec, GMG_ERR_UNSUPPORTED, "promote: compute and vector precision differ");
+  const bool tk4 = h->dof % 4 == 0;
+  if (compute == GMG_F64) {
+    if (nrhs >= 4 && tk4) return launch_promote<double, 4, 4, 4>(h, h->basis_blk.p, nrhs, coarse, fine, s);
+    if (tk4) return launch_promote<double, 4, 1, 4>(h, h->basis_blk.p, nrhs, coarse, fine, s);
+    return launch_promote<double, 1, 1, 4>(h, h->basis_blk.p, nrhs, coarse, fine, s);
+  }
+  if (compute == GMG_F32) {
+    GMG_TRY(agg_prepare_f32(h, s));
+    if (nrhs >= 4 && tk4) return launch_promote<float, 4, 4, 4>(h, h->basis_blk_f.p, nrhs, coarse, fine, s);
+    if (tk4) return launch_promote<float, 4, 1, 4>(h, h->basis_blk_f.p, nrhs, coarse, fine, s);
+    return launch_promote<float, 1, 1, 4>(h, h->basis_blk_f.p, nrhs, coarse, fine, s);
+  }
+  return fail(GMG_ERR_UNSUPPORTED, "promote: unsupported precision");
+}
+
+// ---------------------------------------------------------------------------
+// orthonormalise (FP64 Cholesky-QR, one sweep per pass) and orthogonality check
+// ---------------------------------------------------------------------------
+static const int ORTHO_KS = 2;  // sites per K chunk
+
+// G[i][j] = sum_k conj(V[i][k]) V[j][k] into shared memory (N x N)
+__device__ void block_gram(const double2* __restrict__ Vb, int N, int64_t K, int dof, int bv,
+                           double2* VT, double2* G) {
+  const int t = threadIdx.x;
+  const int NT = (N + 3) / 4;
+  const int ntiles = NT * NT;
+  const int ti = t % NT, tj = t / NT;
+  double2 acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = make_double2(0, 0);
+  const int KC = ORTHO_KS * dof;
+  for (int64_t k0 = 0; k0 < K; k0 += KC) {
+    const int kc = (int)((K - k0) < (int64_t)KC ? (K - k0) : (int64_t)KC);
+    __syncthreads();
+    for (int e = t; e < N * kc; e += blockDim.x) {
+      const int i = e / kc, kk = e % kc;
+      VT[kk * N + i] = Vb[(int64_t)i * K + k0 + kk];
+    }
+    __syncthreads();
+    if (t < ntiles) {
+      for (int kk = 0; kk < kc; ++kk) {
+        double2 a[4], b[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int i = ti * 4 + q, j = tj * 4 + q;
+          a[q] = i < N ? VT[kk * N + i] : make_double2(0, 0);
+          b[q] = j < N ? VT[kk * N + j] : make_double2(0, 0);
+        }
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) acc[x][y] = cfma_conj(acc[x][y], a[x], b[y]);
+      }
+    }
+  }
+  __syncthreads();
+  if (t < ntiles) {
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) {
+        const int i = ti * 4 + x, j = tj * 4 + y;
+        if (i < N && j < N) G[i * N + j] = acc[x][y];
+      }
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) ortho_kernel(double2* __restrict__ basis, int Vc, int N,
+                                                    int dof, int bv, int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* G = reinterpret_cast<double2*>(smem_raw);  // [N][N]  Gram, then L
+  double2* Li = G + N * N;                             // [N][N]  conj(L^{-1})
+  double2* VT = Li + N * N;                            // [KC][N] staging
+  const int64_t K = (int64_t)bv * dof;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  for (int c = blockIdx.x; c < Vc; c += gridDim.x) {
+    double2* Vb = basis + (int64_t)c * N * K;
+    block_gram(Vb, N, K, dof, bv, VT, G);
+    // Cholesky G = L L^dag in place (lower triangle), warp 0
+    if (warp == 0) {
+      for (int j = 0; j < N; ++j) {
+        if (lane == 0) {
+          double d = G[j * N + j].x;
+          for (int k = 0; k < j; ++k) d -= G[j * N + k].x * G[j * N + k].x + G[j * N + k].y * G[j * N + k].y;
+          if (!(d > 0.0)) { atomicExch(status, 1); d = 1.0; }
+          G[j * N + j] = make_double2(sqrt(d), 0.0);
+        }
+        __syncwarp();
+        const double dj = G[j * N + j].x;
+        for (int i = j + 1 + lane; i < N; i += 32) {
+          double2 v = G[i * N + j];
+          for (int k = 0; k < j; ++k) {  // v -= L[i][k] conj(L[j][k])
+            const double2 a = G[i * N + k], b = G[j * N + k];
+            v.x -= a.x * b.x + a.y * b.y;
+            v.y -= a.y * b.x - a.x * b.y;
+          }
+          G[i * N + j] = make_double2(v.x / dj, v.y / dj);
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    // L^{-1} column by column (one thread per column), stored conjugated
+    for (int j = t; j < N; j += blockDim.x) {
+      for (int i = 0; i < N; ++i) Li[i * N + j] = make_double2(0, 0);
+      // X[i][j] for i >= j: X[j][j] = 1/L[j][j]; X[i][j] = -(sum_{k=j}^{i-1} L[i][k] X[k][j]) / L[i][i]
+      Li[j * N + j] = make_double2(1.0 / G[j * N + j].x, 0.0);
+      for (int i = j + 1; i < N; ++i) {
+        double2 sacc = make_double2(0, 0);
+        for (int k = j; k < i; ++k) {
+          const double2 a = G[i * N + k], x = Li[k * N + j];
+          sacc.x += a.x * x.x - a.y * x.y;
+          sacc.y += a.x * x.y + a.y * x.x;
+        }
+        const double inv = 1.0 / G[i * N + i].x;
+        Li[i * N + j] = make_double2(-sacc.x * inv, -sacc.y * inv);
+      }
+      for (int i = j; i < N; ++i) Li[i * N + j].y = -Li[i * N + j].y;  // conjugate
+    }
+    __syncthreads();
+    // V <- conj(L^{-1}) V, chunk by chunk (each chunk read fully before it is overwritten)
+    const int KC = ORTHO_KS * dof;
+    for (int64_t k0 = 0; k0 < K; k0 += KC) {
+      const int kc = (int)((K - k0) < (int64_t)KC ? (K - k0) : (int64_t)KC);
+      __syncthreads();
+      for (int e = t; e < N * kc; e += blockDim.x) {
+        const int i = e / kc, kk = e % kc;
+        VT[kk * N + i] = Vb[(int64_t)i * K + k0 + kk];
+      }
+      __syncthreads();
+      for (int e = t; e < N * kc; e += blockDim.x) {
+        const int i = e / kc, kk = e % kc;
+        double2 acc = make_double2(0, 0);
+        for (int j = 0; j <= i; ++j) acc = cfma(acc, Li[i * N + j], VT[kk * N + j]);
+        Vb[(int64_t)i * K + k0 + kk] = acc;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s) {
+  const int N = h->N;
+  const size_t smem = sizeof(double2) * ((size_t)2 * N * N + (size_t)ORTHO_KS * h->dof * N);
+  GMG_CHECK(smem <= 227 * 1024, GMG_ERR_UNSUPPORTED, "orthonormalise: nbasis too large");
+  GMG_CHECK(N <= 64, GMG_ERR_UNSUPPORTED, "orthonormalise: nbasis > 64");
+  GMG_CUDA(cudaFuncSetAttribute(ortho_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  GMG_TRY(h->scratch.alloc(64));
+  GMG_CUDA(cudaMemsetAsync(h->scratch.p, 0, sizeof(int), s));
+  const int Vc = (int)h->cdims.vol();
+  const int grid = std::min(Vc, num_sms() * 8);
+  for (int p = 0; p < passes; ++p) {
+    ortho_kernel<<<grid, 256, smem, s>>>(h->basis_blk.as<double2>(), Vc, N, h->dof, h->bv,
+                                         h->scratch.as<int>());
+    GMG_CUDA(cudaGetLastError());
+  }
+  h->basis_f_ok = false;
+  return GMG_OK;
+}
+
+__global__ void __launch_bounds__(256) ortho_check_kernel(const double2* __restrict__ basis, int Vc,
+                                                          int N, int dof, int bv,
+                                                          unsigned long long* __restrict__ maxerr) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* G = reinterpret_cast<double2*>(smem_raw);
+  double2* VT = G + N * N;
+  const int64_t K = (int64_t)bv * dof;
+  for (int c = blockIdx.x; c < Vc; c += gridDim.x) {
+    block_gram(basis + (int64_t)c * N * K, N, K, dof, bv, VT, G);
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+      const int i = e / N, j = e % N;
+      const double re = G[e].x - (i == j ? 1.0 : 0.0), im = G[e].y;
+      const double err = sqrt(re * re + im * im);
+      atomicMax(maxerr, __double_as_longlong(err));  // non-negative doubles order as integers
+    }
+    __syncthreads();
+  }
+}
+
+gmg_status agg_check_orthogonal(gmg_agg* h, double* max_err, cudaStream_t s) {
+  const int N = h->N;
+  const size_t smem = sizeof(double2) * ((size_t)N * N + (size_t)ORTHO_KS * h->dof * N);
+  GMG_CUDA(cudaFuncSetAttribute(ortho_check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  GMG_TRY(h->scratch.alloc(64));
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(h->scratch.as<char>() + 8);
+  GMG_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), s));
+  const int Vc = (int)h->cdims.vol();
+  ortho_check_kernel<<<std::min(Vc, num_sms() * 8), 256, smem, s>>>(h->basis_blk.as<double2>(), Vc,
+                                                                    N, h->dof, h->bv, d);
+  GMG_CUDA(cudaGetLastError());
+  unsigned long long v = 0;
+  GMG_CUDA(cudaMemcpyAsync(&v, d, sizeof(v), cudaMemcpyDeviceToHost, s));
+  GMG_CUDA(cudaStreamSynchronize(s));
+  double r;
+  memcpy(&r, &v, sizeof(r));
+  *max_err = r;
+  int st = 0;
+  GMG_CUDA(cudaMemcpy(&st, h->scratch.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st) return fail(GMG_ERR_NONFINITE, "orthonormalise: a block Gram matrix was not positive definite");
+  return GMG_OK;
+}
+
+}  // namespace gmg

@@ -1,0 +1,504 @@
+// coarse_mrhs_tc.cu -- multi-RHS coarse stencil on the 5th-generation tensor cores.
+//
+// Restates the multi-RHS coarse operator M / Mdag / Mdir / Mdiag
+// (include/CoarsenedMatrixUpstreamImprovedDirsaveLutMRHS.h:736-947) as, per
+// coarse site x, a sum over the 9 stencil points of complex products
+//
+//     out(x)[r][b] = sum_p sum_bb A_p(x)[b][bb] in(nbr_p(x))[r][bb]
+//
+// decomposed into one real MMA per point and K-step:
+//
+//     D (2N x 2R) += [Ar; Ai] (2N x N)  .  [Xr^T | Xi^T] (N x 2R)
+//     out_r = D[b][r] - D[N+b][R+r],   out_i = D[N+b][r] + D[b][R+r]
+//
+// so the links are read once in their compact (re, im) form and every
+// operand is a straight copy from HBM.  BF16 or FP16 operands, FP32
+// accumulation in tensor memory (TMEM), tcgen05.mma issued by one thread.
+//
+// Kernel structure (one persistent CTA per SM, 6 warps):
+//   warp 0      producer: for each (site, point) stage one bulk copy of the
+//               link tile and one of the neighbour's packed vector tile into
+//               shared memory (cp.async.bulk + mbarrier transaction counts)
+//   warp 1      TMEM allocator + MMA issuer (one elected thread); accumulates
+//               the 9 points of a site into one of two TMEM buffers
+//   warps 2-5   epilogue: tcgen05.ld the accumulator, recombine (re, im) via
+//               shared memory, apply G5C for Mdag, write FP32 output
+// Every mbarrier wait is bounded in time: on time-out the kernel records an
+// error code, stops issuing work, drains its own copies and MMAs, frees TMEM
+// and returns.
+//
+// Global layouts (prepared once per link set / per apply):
+//   links  [V][9][Kc][Mp][8]   halves, Kc = ceil16(N)/8 K-chunks, Mp = 64 or
+//          128 padded rows: rows m < N = Re A[m][.], N <= m < 2N = Im A[m-N][.]
+//   packed [V][Kc][2Rp][8]     halves: rows n < Rp = Re in[r=n][.],
+//          Rp <= n < 2Rp = Im in[r=n-Rp][.]  (Rp = R rounded up to 16)
+// Both are the canonical no-swizzle K-major core-matrix layout
+// (8 rows x 16 B per core matrix): SBO = 128 B, LBO = rows * 16 B.
+#include <algorithm>
+
+#include "gmg_internal.cuh"
+
+namespace gmg {
+
+namespace tc {
+
+constexpr int kWarps = 6;
+constexpr int kThreads = kWarps * 32;
+constexpr int kAccBufs = 2;
+constexpr long long kTimeoutCycles = 4000000000LL;  // ~2 s at 2 GHz
+
+enum : int { ERR_NONE = 0, ERR_TIMEOUT_PRODUCER = 1, ERR_TIMEOUT_MMA = 2, ERR_TIMEOUT_EPILOGUE = 3 };
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait: false after kTimeoutCycles or when another role aborted
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (true) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if (clock64() - t0 > kTimeoutCycles) return false;
+  }
+}
+
+// wait without the abort short-cut (used to drain our own copies / MMAs)
+__device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kTimeoutCycles) return false;
+  return true;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ uint64_t make_desc(const void* smem, uint32_t lbo, uint32_t sbo) {
+  const uint64_t a = (smem_u32(smem) >> 4) & 0x3FFF;
+  uint64_t d = a;
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  // base offset 0, lbo mode 0, layout type 0 = SWIZZLE_NONE
+  return d;
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+        "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+        "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+        "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void named_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// named barrier that also ORs a predicate over the participating threads
+__device__ __forceinline__ bool named_bar_or(int id, int nthreads, bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "r"(id), "r"(nthreads)
+      : "memory");
+  return r != 0;
+}
+
+struct Params {
+  const uint16_t* links;   // [V][9][Kc][Mp][8]
+  const uint16_t* packed;  // [V][Kc][2Rp][8]
+  const int32_t* nbr;      // [9][V]
+  const int32_t* active;   // nullable
+  float2* out;             // [V][nrhs][N]
+  int* err;                // device error word
+  int V, N, nrhs, R, Rp, Kc, Mp, p0, p1, g5, stages, kind;
+};
+
+__global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Params P) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t link_bytes = (uint32_t)P.Kc * P.Mp * 16;
+  const uint32_t vec_bytes = (uint32_t)P.Kc * 2 * P.Rp * 16;
+  const uint32_t stage_bytes = link_bytes + vec_bytes;
+  const int ncolE = 2 * P.Rp + 1;  // padded row of the epilogue staging buffer
+
+  unsigned char* stage_base = smem;
+  float* E = reinterpret_cast<float*>(smem + (size_t)P.stages * stage_bytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(E) +
+                                               (((size_t)P.Mp * ncolE * 4 + 15) / 16) * 16);
+  uint64_t* full = bars;
+  uint64_t* empty = full + P.stages;
+  uint64_t* tfull = empty + P.stages;
+  uint64_t* tempty = tfull + kAccBufs;
+  uint64_t* drain = tempty + kAccBufs;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const uint32_t acc_cols = 2 * P.Rp;
+  uint32_t ncols_alloc = 32;
+  while (ncols_alloc < kAccBufs * acc_cols) ncols_alloc <<= 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < P.stages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < kAccBufs; ++a) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], 128);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(ncols_alloc)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  // sites of this CTA: blockIdx.x, blockIdx.x + gridDim.x, ...
+  const int nsites = (P.V - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int npts = P.p1 - P.p0;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      int issued = 0;
+      for (int i = 0; i < nsites && !*abort_flag; ++i) {
+        const int site = blockIdx.x + i * gridDim.x;
+        for (int p = P.p0; p < P.p1; ++p) {
+          if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) {
+            atomicCAS(P.err, 0, ERR_TIMEOUT_PRODUCER);
+            *abort_flag = 1;
+            break;
+          }
+          unsigned char* st = stage_base + (size_t)stage * stage_bytes;
+          const int nb = __ldg(&P.nbr[(size_t)p * P.V + site]);
+          mbar_expect_tx(&full[stage], stage_bytes);
+          bulk_g2s(st, P.links + ((size_t)site * 9 + p) * (link_bytes / 2), link_bytes, &full[stage]);
+          bulk_g2s(st + link_bytes, P.packed + (size_t)nb * (vec_bytes / 2), vec_bytes, &full[stage]);
+          ++issued;
+          if (++stage == P.stages) { stage = 0; phase ^= 1; }
+        }
+      }
+      // drain: wait for the copies of the last min(issued, stages) stages to land
+      int s = stage;
+      uint32_t ph = phase;
+      for (int k = 0; k < P.stages && k < issued; ++k) {
+        if (--s < 0) { s = P.stages - 1; ph ^= 1; }
+        mbar_drain(&full[s], ph);
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = (1u << 4)                         // D format F32
+                             | ((uint32_t)P.kind << 7)         // A format (0 F16, 1 BF16)
+                             | ((uint32_t)P.kind << 10)        // B format
+                             | ((uint32_t)(2 * P.Rp) >> 3) << 17  // N
+                             | ((uint32_t)P.Mp >> 4) << 24;      // M
+      int stage = 0;
+      uint32_t phase = 0;
+      bool ok = true;
+      int committed = 0;
+      for (int i = 0; i < nsites && ok; ++i) {
+        const int acc = i & 1;
+        const uint32_t aphase = (uint32_t)(i >> 1) & 1;
+        if (!mbar_wait(&tempty[acc], aphase ^ 1, abort_flag)) { ok = false; break; }
+        fence_after();
+        const uint32_t dt = tmem_base + acc * acc_cols;
+        for (int p = 0; p < npts; ++p) {
+          if (!mbar_wait(&full[stage], phase, abort_flag)) { ok = false; break; }
+          fence_after();
+          unsigned char* st = stage_base + (size_t)stage * stage_bytes;
+          for (int ks = 0; ks < P.Kc / 2; ++ks) {
+            const uint64_t ad = make_desc(st + (size_t)(2 * ks) * P.Mp * 16, (uint32_t)P.Mp * 16, 128);
+            const uint64_t bd =
+                make_desc(st + link_bytes + (size_t)(2 * ks) * 2 * P.Rp * 16, (uint32_t)(2 * P.Rp) * 16, 128);
+            mma_f16(dt, ad, bd, idesc, (p > 0 || ks > 0) ? 1u : 0u);
+          }
+          mma_commit(&empty[stage]);
+          ++committed;
+          if (++stage == P.stages) { stage = 0; phase ^= 1; }
+        }
+        if (!ok) break;
+        mma_commit(&tfull[acc]);
+      }
+      if (!ok) {
+        atomicCAS(P.err, 0, ERR_TIMEOUT_MMA);
+        *abort_flag = 1;
+      }
+      // drain our own MMAs before TMEM is freed
+      mma_commit(drain);
+      mbar_drain(drain, 0);
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue (warps 2..5)
+    const int q = warp & 3;                // TMEM sub-partition of this warp
+    const int rows_per_warp = P.Mp / 4;    // 16 (M=64) or 32 (M=128)
+    const int et = threadIdx.x - 64;       // 0..127
+    const int N = P.N, Rp = P.Rp;
+    for (int i = 0; i < nsites; ++i) {
+      const int site = blockIdx.x + i * gridDim.x;
+      const int acc = i & 1;
+      const uint32_t aphase = (uint32_t)(i >> 1) & 1;
+      const bool waited = mbar_wait(&tfull[acc], aphase, abort_flag);
+      // all 128 epilogue threads leave together, or none does
+      if (named_bar_or(1, 128, !waited)) {
+        if (!waited) atomicCAS(P.err, 0, ERR_TIMEOUT_EPILOGUE);
+        *abort_flag = 1;
+        break;
+      }
+      fence_after();
+      const int row = q * rows_per_warp + lane;  // accumulator row held by this thread
+      for (int c0 = 0; c0 < 2 * Rp; c0 += 32) {
+        float v[32];
+        tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + acc * acc_cols + c0, v);
+        if (lane < rows_per_warp && row < 2 * N) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (c0 + j < 2 * Rp) E[row * ncolE + c0 + j] = v[j];
+        }
+      }
+      fence_before();
+      mbar_arrive(&tempty[acc]);
+      named_bar(1, 128);
+      // recombine and store: out[site][slot(r)][b]
+      for (int e = et; e < P.R * N; e += 128) {
+        const int r = e / N, b = e % N;
+        float re = E[b * ncolE + r] - E[(N + b) * ncolE + Rp + r];
+        float im = E[(N + b) * ncolE + r] + E[b * ncolE + Rp + r];
+        if (P.g5 && b >= N / 2) { re = -re; im = -im; }
+        const int slot = P.active ? __ldg(&P.active[r]) : r;
+        P.out[((size_t)site * P.nrhs + slot) * N + b] = make_float2(re, im);
+      }
+      named_bar(1, 128);
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(ncols_alloc)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------- packers
+__device__ __forceinline__ uint16_t to_half_bits(float x, int kind) {
+  if (kind == GMG_BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+  return __half_as_ushort(__float2half_rn(x));
+}
+
+// links (exchange layout, FP64) -> [V][9][Kc][Mp][8] halves
+__global__ void pack_links_kernel(const double2* __restrict__ A, uint4* __restrict__ dst, int V, int N, int Kc,
+                                  int Mp, int kind) {
+  const int64_t total = (int64_t)V * 9 * Kc * Mp;  // one 16-byte row each
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int m = (int)(e % Mp);
+    const int kc = (int)((e / Mp) % Kc);
+    const int p = (int)((e / ((int64_t)Mp * Kc)) % 9);
+    const int64_t s = e / ((int64_t)Mp * Kc * 9);
+    uint16_t h[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int bb = kc * 8 + j;
+      float v = 0.f;
+      if (m < 2 * N && bb < N) {
+        const int b = m < N ? m : m - N;
+        const double2 a = A[(((int64_t)p * V + s) * N + b) * N + bb];
+        v = (float)(m < N ? a.x : a.y);
+      }
+      h[j] = to_half_bits(v, kind);
+    }
+    uint4 o;
+    o.x = h[0] | ((uint32_t)h[1] << 16);
+    o.y = h[2] | ((uint32_t)h[3] << 16);
+    o.z = h[4] | ((uint32_t)h[5] << 16);
+    o.w = h[6] | ((uint32_t)h[7] << 16);
+    dst[e] = o;
+  }
+}
+
+// vectors (FP32 [V][nrhs][N]) -> [V][Kc][2Rp][8] halves, G5C applied on input
+__global__ void pack_vec_kernel(const float2* __restrict__ in, uint4* __restrict__ dst, const int32_t* __restrict__ active,
+                                int V, int N, int nrhs, int R, int Rp, int Kc, int kind, int g5) {
+  const int64_t total = (int64_t)V * Kc * 2 * Rp;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int n = (int)(e % (2 * Rp));
+    const int kc = (int)((e / (2 * Rp)) % Kc);
+    const int64_t s = e / ((int64_t)2 * Rp * Kc);
+    const int r = n < Rp ? n : n - Rp;
+    const bool imag = n >= Rp;
+    uint16_t h[8];
+    if (r < R) {
+      const int slot = active ? active[r] : r;
+      const float2* src = in + ((int64_t)s * nrhs + slot) * N;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int bb = kc * 8 + j;
+        float v = 0.f;
+        if (bb < N) {
+          const float2 x = src[bb];
+          v = imag ? x.y : x.x;
+          if (g5 && bb >= N / 2) v = -v;
+        }
+        h[j] = to_half_bits(v, kind);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) h[j] = 0;
+    }
+    uint4 o;
+    o.x = h[0] | ((uint32_t)h[1] << 16);
+    o.y = h[2] | ((uint32_t)h[3] << 16);
+    o.z = h[4] | ((uint32_t)h[5] << 16);
+    o.w = h[6] | ((uint32_t)h[7] << 16);
+    dst[e] = o;
+  }
+}
+
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+}  // namespace tc
+
+gmg_status coarse_prepare_tc(gmg_coarse* h, int kind, cudaStream_t s) {
+  const int N = h->N;
+  GMG_CHECK(2 * N <= 128, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil needs nbasis <= 64");
+  const int Kc = tc::round_up(N, 16) / 8;
+  const int Mp = 2 * N <= 64 ? 64 : 128;
+  const int V = (int)h->dims.vol();
+  const size_t bytes = (size_t)V * 9 * Kc * Mp * 16;
+  GMG_TRY(h->links_h.buf.alloc(bytes));
+  const int64_t rows = (int64_t)V * 9 * Kc * Mp;
+  tc::pack_links_kernel<<<(int)std::min<int64_t>((rows + 255) / 256, 148 * 64), 256, 0, s>>>(
+      h->links_ref.as<double2>(), h->links_h.buf.as<uint4>(), V, N, Kc, Mp, kind);
+  GMG_CUDA(cudaGetLastError());
+  h->links_h.kind = kind;
+  return GMG_OK;
+}
+
+gmg_status coarse_apply_tc(gmg_coarse* h, int p0, int p1, bool g5, int kind, int nrhs, const float* in,
+                           float* out, const int32_t* active, int n_active, cudaStream_t s) {
+  const int N = h->N;
+  const int R = active ? n_active : nrhs;
+  if (R == 0) return GMG_OK;
+  GMG_CHECK(R <= 128, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil supports at most 128 active RHS");
+  const int Rp = tc::round_up(R, 16);
+  const int Kc = tc::round_up(N, 16) / 8;
+  const int Mp = 2 * N <= 64 ? 64 : 128;
+  const int V = (int)h->dims.vol();
+  // scratch: packed vectors + error word
+  const size_t packed_bytes = (size_t)V * Kc * 2 * Rp * 16;
+  GMG_TRY(h->scratch.alloc(packed_bytes));
+  uint4* packed = h->scratch.as<uint4>();
+  int* err = h->dev_err.as<int>();
+  const int64_t rows = (int64_t)V * Kc * 2 * Rp;
+  tc::pack_vec_kernel<<<(int)std::min<int64_t>((rows + 255) / 256, 148 * 64), 256, 0, s>>>(
+      reinterpret_cast<const float2*>(in), packed, active, V, N, nrhs, R, Rp, Kc, kind, g5 ? 1 : 0);
+  GMG_CUDA(cudaGetLastError());
+
+  const uint32_t stage_bytes = (uint32_t)Kc * Mp * 16 + (uint32_t)Kc * 2 * Rp * 16;
+  const size_t e_bytes = ((size_t)Mp * (2 * Rp + 1) * 4 + 15) / 16 * 16;
+  const size_t fixed = e_bytes + 64 * 8 + 64;
+  const size_t budget = 227 * 1024 - fixed;
+  int stages = (int)std::min<size_t>(32, budget / stage_bytes);
+  GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil: tile does not fit shared memory");
+  const size_t smem = (size_t)stages * stage_bytes + e_bytes + (size_t)(2 * stages + 2 * tc::kAccBufs + 1) * 8 + 16;
+  GMG_CUDA(cudaFuncSetAttribute(tc::coarse_mrhs_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  tc::Params P;
+  P.links = h->links_h.buf.as<uint16_t>();
+  P.packed = reinterpret_cast<const uint16_t*>(packed);
+  P.nbr = h->nbr.as<int32_t>();
+  P.active = active;
+  P.out = reinterpret_cast<float2*>(out);
+  P.err = err;
+  P.V = V;
+  P.N = N;
+  P.nrhs = nrhs;
+  P.R = R;
+  P.Rp = Rp;
+  P.Kc = Kc;
+  P.Mp = Mp;
+  P.p0 = p0;
+  P.p1 = p1;
+  P.g5 = g5 ? 1 : 0;
+  P.stages = stages;
+  P.kind = kind == GMG_BF16 ? 1 : 0;
+  tc::coarse_mrhs_tc_kernel<<<std::min(V, nsm), tc::kThreads, smem, s>>>(P);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+}  // namespace gmg

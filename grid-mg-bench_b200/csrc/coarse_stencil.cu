@@ -1,0 +1,279 @@
+// coarse_stencil.cu -- 9-point coarse Dirac stencil on CUDA cores (FP64 / FP32).
+//
+// Restates CoarsenedMatrix::M / Mdag / MdirCalc / Mdiag
+// (include/CoarsenedMatrixUpstream.h:546-742) and the multi-RHS form
+// (include/CoarsenedMatrixUpstreamImprovedDirsaveLutMRHS.h:736-947):
+//
+//   out(x, r) = sum_{p in [p0,p1)} A_p(x) in(nbr_p(x), r)        (N x N times N)
+//
+// with Mdag = G5C M G5C (sign flip of the upper half of the basis index on
+// load and store, no temporary).  The reference runs one thread per (site,
+// row) and re-reads every link element once per RHS; here one CTA owns a
+// site, stages A_p(x) and the neighbour's R x N tile in shared memory
+// (transposed so that the basis index is the contiguous one), and every
+// thread accumulates a TR x TB register tile of (rhs, row) outputs, so a link
+// element is read from HBM once for all R right-hand sides.
+//
+// Links are kept site-major, [V][9][N][N], so that one site's 9 matrices are
+// one contiguous stream.
+#include <algorithm>
+
+#include "gmg_internal.cuh"
+
+namespace gmg {
+
+template <class T> struct cplx_t;
+template <> struct cplx_t<double> { typedef double2 type; };
+template <> struct cplx_t<float> { typedef float2 type; };
+
+template <class C> __device__ __forceinline__ C cmul_add(C acc, C a, C b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+  return acc;
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion [p][V][N][N] (exchange) -> [V][p][N][N] (site-major)
+// ---------------------------------------------------------------------------
+template <class To>
+__global__ void links_site_major_kernel(const double2* __restrict__ src, To* __restrict__ dst,
+                                        int64_t V, int NN) {
+  const int64_t total = 9 * V * NN;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = k % NN;
+    const int64_t ps = k / NN;
+    const int64_t s = ps % V;
+    const int64_t p = ps / V;
+    const double2 v = src[k];
+    To o;
+    o.x = v.x;
+    o.y = v.y;
+    dst[(s * 9 + p) * NN + e] = o;
+  }
+}
+
+static int grid_for(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  return (int)std::min<int64_t>(std::max<int64_t>(b, 1), 148 * 32);
+}
+
+gmg_status coarse_links_to_site_major(gmg_coarse* h, cudaStream_t s) {
+  const int64_t V = h->dims.vol();
+  const int NN = h->N * h->N;
+  GMG_TRY(h->links_d.alloc(sizeof(double2) * 9 * V * NN));
+  links_site_major_kernel<double2><<<grid_for(9 * V * NN, 256), 256, 0, s>>>(
+      h->links_ref.as<double2>(), h->links_d.as<double2>(), V, NN);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status coarse_prepare_f32(gmg_coarse* h, cudaStream_t s) {
+  const int64_t V = h->dims.vol();
+  const int NN = h->N * h->N;
+  GMG_TRY(h->links_f.alloc(sizeof(float2) * 9 * V * NN));
+  links_site_major_kernel<float2><<<grid_for(9 * V * NN, 256), 256, 0, s>>>(
+      h->links_ref.as<double2>(), h->links_f.as<float2>(), V, NN);
+  GMG_CUDA(cudaGetLastError());
+  h->links_f_ok = true;
+  return GMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the stencil kernel
+// ---------------------------------------------------------------------------
+template <class T, int TR, int TB>
+__global__ void __launch_bounds__(256) coarse_simt_kernel(
+    const typename cplx_t<T>::type* __restrict__ links, const int32_t* __restrict__ nbr,
+    const typename cplx_t<T>::type* __restrict__ in, typename cplx_t<T>::type* __restrict__ out,
+    int V, int N, int nrhs, const int32_t* __restrict__ active, int R, int p0, int p1, int g5) {
+  typedef typename cplx_t<T>::type C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* AT = reinterpret_cast<C*>(smem_raw);  // [N][N]   AT[bb][b] = A[b][bb]
+  C* XT = AT + N * N;                      // [N][R]   XT[bb][r] = in(nbr, r)[bb]
+  const int NBT = (N + TB - 1) / TB;
+  const int NRT = (R + TR - 1) / TR;
+  const int ntiles = NBT * NRT;
+  const int t = threadIdx.x;
+  const int bt = t % NBT, rt = t / NBT;
+  const int half = N / 2;
+
+  for (int site = blockIdx.x; site < V; site += gridDim.x) {
+    C acc[TR][TB];
+#pragma unroll
+    for (int j = 0; j < TR; ++j)
+#pragma unroll
+      for (int i = 0; i < TB; ++i) acc[j][i] = C{0, 0};
+
+    for (int p = p0; p < p1; ++p) {
+      const C* Ap = links + ((int64_t)site * 9 + p) * N * N;
+      const int nb = nbr[(int64_t)p * V + site];
+      __syncthreads();
+      for (int k = t; k < N * N; k += blockDim.x) {
+        const int b = k / N, bb = k % N;
+        AT[bb * N + b] = Ap[k];
+      }
+      for (int k = t; k < R * N; k += blockDim.x) {
+        const int r = k / N, bb = k % N;
+        const int slot = active ? active[r] : r;
+        C v = in[((int64_t)nb * nrhs + slot) * N + bb];
+        if (g5 && bb >= half) { v.x = -v.x; v.y = -v.y; }
+        XT[bb * R + r] = v;
+      }
+      __syncthreads();
+      if (t < ntiles) {
+        for (int bb = 0; bb < N; ++bb) {
+          C a[TB], x[TR];
+#pragma unroll
+          for (int i = 0; i < TB; ++i) {
+            const int b = bt * TB + i;
+            a[i] = b < N ? AT[bb * N + b] : C{0, 0};
+          }
+#pragma unroll
+          for (int j = 0; j < TR; ++j) {
+            const int r = rt * TR + j;
+            x[j] = r < R ? XT[bb * R + r] : C{0, 0};
+          }
+#pragma unroll
+          for (int j = 0; j < TR; ++j)
+#pragma unroll
+            for (int i = 0; i < TB; ++i) acc[j][i] = cmul_add(acc[j][i], a[i], x[j]);
+        }
+      }
+    }
+    if (t < ntiles) {
+#pragma unroll
+      for (int j = 0; j < TR; ++j) {
+        const int r = rt * TR + j;
+        if (r >= R) continue;
+        const int slot = active ? active[r] : r;
+        C* o = out + ((int64_t)site * nrhs + slot) * N;
+#pragma unroll
+        for (int i = 0; i < TB; ++i) {
+          const int b = bt * TB + i;
+          if (b >= N) continue;
+          C v = acc[j][i];
+          if (g5 && b >= half) { v.x = -v.x; v.y = -v.y; }
+          o[b] = v;
+        }
+      }
+    }
+  }
+}
+
+template <class T, int TR, int TB>
+static gmg_status launch_simt(const void* links, const int32_t* nbr, const void* in, void* out,
+                              int V, int N, int nrhs, const int32_t* active, int R, int p0, int p1,
+                              int g5, cudaStream_t s) {
+  typedef typename cplx_t<T>::type C;
+  const int ntiles = ((N + TB - 1) / TB) * ((R + TR - 1) / TR);
+  GMG_CHECK(ntiles <= 256, GMG_ERR_UNSUPPORTED, "coarse apply: nbasis x nrhs tile too large");
+  const int threads = std::max(32, (ntiles + 31) / 32 * 32);
+  const size_t smem = sizeof(C) * ((size_t)N * N + (size_t)N * R);
+  GMG_CHECK(smem <= 227 * 1024, GMG_ERR_UNSUPPORTED, "coarse apply: shared-memory tile too large");
+  auto kern = coarse_simt_kernel<T, TR, TB>;
+  GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, nsm = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  const int grid = std::min(V, nsm * std::max(per_sm, 1) * 4);
+  kern<<<grid, threads, smem, s>>>(reinterpret_cast<const C*>(links), nbr,
+                                   reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), V, N,
+                                   nrhs, active, R, p0, p1, g5);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status coarse_apply_simt(gmg_coarse* h, int p0, int p1, bool g5, int compute, int vec_prec,
+                             int nrhs, const void* in, void* out, const int32_t* active,
+                             int n_active, cudaStream_t s) {
+  const int V = (int)h->dims.vol();
+  const int N = h->N;
+  const int R = active ? n_active : nrhs;
+  if (R == 0) return GMG_OK;
+  const int32_t* nbr = h->nbr.as<int32_t>();
+  if (compute == GMG_F64) {
+    GMG_CHECK(vec_prec == GMG_F64, GMG_ERR_UNSUPPORTED, "F64 compute needs F64 vectors");
+    if (R >= 4) return launch_simt<double, 4, 4>(h->links_d.p, nbr, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
+    return launch_simt<double, 1, 2>(h->links_d.p, nbr, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
+  }
+  if (compute == GMG_F32) {
+    GMG_CHECK(vec_prec == GMG_F32, GMG_ERR_UNSUPPORTED, "F32 compute needs F32 vectors");
+    GMG_CHECK(h->links_f_ok, GMG_ERR_STATE, "F32 links not prepared (gmg_coarse_prepare)");
+    if (R >= 4) return launch_simt<float, 4, 4>(h->links_f.p, nbr, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
+    return launch_simt<float, 1, 2>(h->links_f.p, nbr, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
+  }
+  return fail(GMG_ERR_UNSUPPORTED, "coarse apply: unsupported compute precision for SIMT path");
+}
+
+// ---------------------------------------------------------------------------
+// ConstructRemainingLinks (...DirsaveLut.h:1164-1196) / ForceHermitian
+// (CoarsenedMatrixUpstream.h:956-976) on the exchange layout:
+//   A_{dir}(x)[n1][n2] = S(n1,n2) conj(A_{dir+4}(x + e_dir)[n2][n1])
+// S = -1 iff n1 and n2 lie in different halves (1 if hermitian).
+// ---------------------------------------------------------------------------
+__global__ void construct_remaining_kernel(double2* __restrict__ A, const int32_t* __restrict__ nbr,
+                                           int V, int N, int hermitian) {
+  const int64_t NN = (int64_t)N * N;
+  const int64_t total = 4 * (int64_t)V * NN;
+  const int half = N / 2;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int n2 = (int)(k % N);
+    const int n1 = (int)((k / N) % N);
+    const int64_t s = (k / NN) % V;
+    const int dir = (int)(k / (NN * V));
+    const int sp = nbr[(int64_t)dir * V + s];  // x + e_dir
+    double2 v = A[((int64_t)(dir + 4) * V + sp) * NN + (int64_t)n2 * N + n1];
+    double f = 1.0;
+    if (!hermitian && ((n1 / half + n2 / half) & 1)) f = -1.0;
+    A[((int64_t)dir * V + s) * NN + (int64_t)n1 * N + n2] = make_double2(f * v.x, -f * v.y);
+  }
+}
+
+gmg_status coarse_construct_remaining(gmg_coarse* h, cudaStream_t s) {
+  const int V = (int)h->dims.vol();
+  const int64_t total = 4 * (int64_t)V * h->N * h->N;
+  construct_remaining_kernel<<<grid_for(total, 256), 256, 0, s>>>(
+      h->links_ref.as<double2>(), h->nbr.as<int32_t>(), V, h->N, h->hermitian);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+}  // namespace gmg
+
+// ---------------------------------------------------------------------------
+// Rework layout map for links (Layout_converters.h:49-56): flat [n1][n2] with
+// n = s*Nc_c + c  <->  spin-split [s1][s2][c1][c2].
+// ---------------------------------------------------------------------------
+namespace gmg {
+__global__ void layout_links_kernel(const double2* __restrict__ in, double2* __restrict__ out, int64_t V,
+                                    int N, int ncs, int inverse) {
+  const int ncc = N / ncs;
+  const int64_t NN = (int64_t)N * N;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < V * NN;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = e / NN;
+    const int n1 = (int)((e % NN) / N), n2 = (int)(e % N);
+    const int s1 = n1 / ncc, c1 = n1 % ncc, s2 = n2 / ncc, c2 = n2 % ncc;
+    const int64_t spin = s * NN + ((int64_t)(s1 * ncs + s2) * ncc + c1) * ncc + c2;
+    if (!inverse) out[spin] = in[e];
+    else out[e] = in[spin];
+  }
+}
+}  // namespace gmg
+
+extern "C" gmg_status gmg_layout_links(int64_t V, int nbasis, int ncs, const double* in, double* out,
+                                       int inverse, gmg_stream s) {
+  GMG_CHECK(in && out && in != out, GMG_ERR_ARGUMENT, "gmg_layout_links: bad pointers");
+  GMG_CHECK(V > 0 && nbasis > 0 && ncs > 0 && nbasis % ncs == 0, GMG_ERR_ARGUMENT,
+            "gmg_layout_links: nbasis must be a multiple of the coarse spin count");
+  const int64_t n = V * nbasis * (int64_t)nbasis;
+  gmg::layout_links_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 148 * 32), 256, 0, gmg::S(s)>>>(
+      reinterpret_cast<const double2*>(in), reinterpret_cast<double2*>(out), V, nbasis, ncs, inverse);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}

@@ -1,0 +1,196 @@
+// coarsen.cu -- Galerkin coarse-operator construction on the GPU (FP64).
+//
+// Restates CoarsenedMatrix::CoarsenOperator in its direction-saving form
+// (include/CoarsenedMatrixUpstreamImprovedDirsaveLut.h:927-1097, multi-RHS
+// batching of the fine applies as in ...LutMRHS.h:1004-1101):
+//
+//   for a batch of basis vectors phi_i (the fine operator sees them as RHS):
+//     W_p = Mdir_p phi,               p = 4..7 (disp = -1)
+//     A_p(c)[j][i] = sum_{x in c, x_dir mod b == 0} <v_j(x), W_p(x)>
+//     W_8 = e*M(e phi) + o*M(o phi)   (block even/odd trick, :1053-1067)
+//     A_8(c)[j][i] = sum_{x in c} <v_j(x), W_8(x)>
+//   then A_{+mu}(x) = S o A_{-mu}(x+mu)^dag  (ConstructRemainingLinks, :1164-1196)
+//
+// The fine operator is either the Wilson-clover operator or, for
+// coarse-of-coarse, the coarse stencil of the level above (its MdirCalc is the
+// "fine" Mdir, ...Lut.h:820-860).
+#include <algorithm>
+
+#include "gmg_internal.cuh"
+
+namespace gmg {
+
+gmg_status agg_project_masked_f64(gmg_agg* h, int nrhs, const double* fine, double* coarse,
+                                  const int8_t* mask, cudaStream_t s);
+
+// field[sf][r][a] = basis_blk[c][i0 + r][sb*dof + a]
+__global__ void basis_gather_kernel(const double2* __restrict__ basis_blk, const int32_t* __restrict__ blk_sites,
+                                    double2* __restrict__ field, int64_t Vc, int N, int bv, int dof, int i0,
+                                    int nb) {
+  const int64_t K = (int64_t)bv * dof;
+  const int64_t total = Vc * nb * K;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = e % K;
+    const int r = (int)((e / K) % nb);
+    const int64_t c = e / (K * nb);
+    const int64_t sf = blk_sites[c * bv + k / dof];
+    field[(sf * nb + r) * dof + k % dof] = basis_blk[(c * N + i0 + r) * K + k];
+  }
+}
+
+// out[s][r][a] = mask[s] == want ? in[s][r][a] : 0
+__global__ void mask_select_kernel(const double2* __restrict__ in, double2* __restrict__ out,
+                                   const int8_t* __restrict__ mask, int64_t V, int width, int want) {
+  const int64_t total = V * width;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = e / width;
+    out[e] = (mask[s] == want) ? in[e] : make_double2(0, 0);
+  }
+}
+
+// out = mask ? a : b
+__global__ void mask_merge_kernel(const double2* __restrict__ a, const double2* __restrict__ b,
+                                  double2* __restrict__ out, const int8_t* __restrict__ mask, int64_t V,
+                                  int width) {
+  const int64_t total = V * width;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = mask[e / width] ? a[e] : b[e];
+}
+
+// A_p(c)[j][i0 + r] = proj[c][r][j]
+__global__ void link_scatter_kernel(const double2* __restrict__ proj, double2* __restrict__ A, int64_t Vc,
+                                    int N, int i0, int nb) {
+  const int64_t total = Vc * nb * N;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int j = (int)(e % N);
+    const int r = (int)((e / N) % nb);
+    const int64_t c = e / ((int64_t)N * nb);
+    A[(c * N + j) * N + i0 + r] = proj[e];
+  }
+}
+
+static int gsz(int64_t n) { return (int)std::min<int64_t>(std::max<int64_t>((n + 255) / 256, 1), 148 * 64); }
+
+struct FineOpRef {
+  gmg_wilson* w = nullptr;
+  gmg_coarse* c = nullptr;
+  int dof() const { return w ? 12 : c->N; }
+  const Dims& dims() const { return w ? w->dims : c->dims; }
+  gmg_status mdir(int p, int nb, const double* in, double* out, cudaStream_t s) const {
+    if (w) return wilson_apply(w, GMG_OP_MDIR, p % 4, p < 4 ? 1 : -1, GMG_F64, nb, in, out, s);
+    return coarse_apply_simt(c, p, p + 1, false, GMG_F64, GMG_F64, nb, in, out, nullptr, 0, s);
+  }
+  gmg_status m(int nb, const double* in, double* out, cudaStream_t s) const {
+    if (w) return wilson_apply(w, GMG_OP_M, 0, 0, GMG_F64, nb, in, out, s);
+    return coarse_apply_simt(c, 0, 9, false, GMG_F64, GMG_F64, nb, in, out, nullptr, 0, s);
+  }
+};
+
+static void host_masks(const Dims& f, const int* b, std::vector<int8_t>& out) {
+  // out[0..3]: faces x_dir mod b == 0 (points 4..7); out[4]: even blocks
+  const int64_t V = f.vol();
+  out.assign(5 * V, 0);
+  for (int64_t s = 0; s < V; ++s) {
+    int c[4];
+    int64_t t = s;
+    for (int d = 0; d < 4; ++d) { c[d] = (int)(t % f.d[d]); t /= f.d[d]; }
+    int bcb = 0;
+    for (int d = 0; d < 4; ++d) {
+      out[d * V + s] = (c[d] % b[d]) == 0;
+      bcb += c[d] / b[d];
+    }
+    out[4 * V + s] = (bcb % 2) == 0;
+  }
+}
+
+static gmg_status coarsen_generic(gmg_coarse* out, gmg_agg* agg, const FineOpRef& op, cudaStream_t s) {
+  const Dims& fd = op.dims();
+  const int dof = op.dof();
+  GMG_CHECK(agg->dof == dof, GMG_ERR_SHAPE, "coarsen: aggregation site dof differs from the fine operator");
+  for (int d = 0; d < 4; ++d) {
+    GMG_CHECK(agg->fdims.d[d] == fd.d[d], GMG_ERR_SHAPE, "coarsen: fine lattice differs");
+    GMG_CHECK(agg->cdims.d[d] == out->dims.d[d], GMG_ERR_SHAPE, "coarsen: coarse lattice differs");
+  }
+  GMG_CHECK(agg->N == out->N, GMG_ERR_SHAPE, "coarsen: nbasis differs");
+  GMG_CHECK(agg->basis_set, GMG_ERR_STATE, "coarsen: basis not set");
+  const int N = agg->N;
+  const int64_t Vf = fd.vol(), Vc = out->dims.vol();
+  GMG_TRY(out->links_ref.alloc(sizeof(double2) * 9 * Vc * N * N));
+  GMG_CUDA(cudaMemsetAsync(out->links_ref.p, 0, sizeof(double2) * 9 * Vc * N * N, s));
+
+  // batch of basis vectors treated as right-hand sides (bounded to ~1 GB per field)
+  int nb = N;
+  while (nb > 1 && (double)Vf * nb * dof * 16.0 > 1.0e9) nb = (nb + 1) / 2;
+  const size_t fbytes = sizeof(double2) * (size_t)Vf * nb * dof;
+  DevBuf phi, w1, w2, w3, proj, masks;
+  GMG_TRY(phi.alloc(fbytes));
+  GMG_TRY(w1.alloc(fbytes));
+  GMG_TRY(w2.alloc(fbytes));
+  GMG_TRY(w3.alloc(fbytes));
+  GMG_TRY(proj.alloc(sizeof(double2) * (size_t)Vc * nb * N));
+  std::vector<int8_t> hm;
+  host_masks(fd, agg->b, hm);
+  GMG_TRY(masks.alloc(hm.size()));
+  GMG_CUDA(cudaMemcpyAsync(masks.p, hm.data(), hm.size(), cudaMemcpyHostToDevice, s));
+  const int8_t* face = masks.as<int8_t>();
+  const int8_t* even = face + 4 * Vf;
+  double2* A = out->links_ref.as<double2>();
+  const int width = nb * dof;
+
+  for (int i0 = 0; i0 < N; i0 += nb) {
+    const int cur = std::min(nb, N - i0);
+    const int wdt = cur * dof;
+    basis_gather_kernel<<<gsz(Vc * cur * agg->bv * dof), 256, 0, s>>>(
+        agg->basis_blk.as<double2>(), agg->blk_sites.as<int32_t>(), phi.as<double2>(), Vc, N, agg->bv,
+        dof, i0, cur);
+    GMG_CUDA(cudaGetLastError());
+    for (int p = 4; p < 8; ++p) {
+      GMG_TRY(op.mdir(p, cur, phi.as<double>(), w1.as<double>(), s));
+      GMG_TRY(agg_project_masked_f64(agg, cur, w1.as<double>(), proj.as<double>(), face + (p - 4) * Vf, s));
+      link_scatter_kernel<<<gsz(Vc * cur * N), 256, 0, s>>>(proj.as<double2>(), A + (int64_t)p * Vc * N * N,
+                                                             Vc, N, i0, cur);
+      GMG_CUDA(cudaGetLastError());
+    }
+    // self term
+    mask_select_kernel<<<gsz(Vf * wdt), 256, 0, s>>>(phi.as<double2>(), w1.as<double2>(), even, Vf, wdt, 1);
+    GMG_TRY(op.m(cur, w1.as<double>(), w2.as<double>(), s));   // M(e phi)
+    mask_select_kernel<<<gsz(Vf * wdt), 256, 0, s>>>(phi.as<double2>(), w1.as<double2>(), even, Vf, wdt, 0);
+    GMG_TRY(op.m(cur, w1.as<double>(), w3.as<double>(), s));   // M(o phi)
+    mask_merge_kernel<<<gsz(Vf * wdt), 256, 0, s>>>(w2.as<double2>(), w3.as<double2>(), w1.as<double2>(), even,
+                                                    Vf, wdt);
+    GMG_CUDA(cudaGetLastError());
+    GMG_TRY(agg_project_masked_f64(agg, cur, w1.as<double>(), proj.as<double>(), nullptr, s));
+    link_scatter_kernel<<<gsz(Vc * cur * N), 256, 0, s>>>(proj.as<double2>(), A + (int64_t)8 * Vc * N * N, Vc,
+                                                           N, i0, cur);
+    GMG_CUDA(cudaGetLastError());
+  }
+  (void)width;
+  GMG_TRY(coarse_construct_remaining(out, s));
+  GMG_TRY(coarse_links_to_site_major(out, s));
+  out->links_set = true;
+  out->links_f_ok = false;
+  out->links_h.kind = -1;
+  // temporaries are freed at scope exit: make sure the stream is done with them
+  GMG_CUDA(cudaStreamSynchronize(s));
+  return GMG_OK;
+}
+
+gmg_status coarsen_wilson(gmg_coarse* out, gmg_agg* agg, gmg_wilson* fine, cudaStream_t s) {
+  GMG_CHECK(fine->gauge_set, GMG_ERR_STATE, "coarsen: gauge field not set");
+  FineOpRef op;
+  op.w = fine;
+  return coarsen_generic(out, agg, op, s);
+}
+
+gmg_status coarsen_coarse(gmg_coarse* out, gmg_agg* agg, gmg_coarse* fine, cudaStream_t s) {
+  GMG_CHECK(fine->links_set, GMG_ERR_STATE, "coarsen: fine links not set");
+  FineOpRef op;
+  op.c = fine;
+  return coarsen_generic(out, agg, op, s);
+}
+
+}  // namespace gmg

@@ -1,0 +1,156 @@
+// gmg_internal.cuh -- shared declarations of the libgmg_b200 implementation.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/gmg.h"
+
+namespace gmg {
+
+// ---------------------------------------------------------------------------
+// error handling: every C entry point returns a status; the message of the
+// last failure is kept per host thread.
+// ---------------------------------------------------------------------------
+void set_error(const std::string& msg);
+const char* last_error_cstr();
+gmg_status fail(gmg_status st, const std::string& msg);
+gmg_status cuda_fail(cudaError_t e, const char* what);
+
+#define GMG_CUDA(call)                                     \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return ::gmg::cuda_fail(e_, #call); \
+  } while (0)
+
+#define GMG_CHECK(cond, st, msg)              \
+  do {                                        \
+    if (!(cond)) return ::gmg::fail(st, msg); \
+  } while (0)
+
+#define GMG_TRY(call)                   \
+  do {                                  \
+    gmg_status st_ = (call);            \
+    if (st_ != GMG_OK) return st_;      \
+  } while (0)
+
+inline cudaStream_t S(gmg_stream s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ---------------------------------------------------------------------------
+// lattice helpers
+// ---------------------------------------------------------------------------
+struct Dims {
+  int d[4];
+  int64_t vol() const { return (int64_t)d[0] * d[1] * d[2] * d[3]; }
+};
+
+gmg_status check_dims(const int* dims, const char* what);
+
+// device buffer owned by a handle
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  gmg_status alloc(size_t n);
+  void free();
+  ~DevBuf() { free(); }
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// handles
+// ---------------------------------------------------------------------------
+struct LinksF16 {  // tensor-core link copy (see coarse_mrhs_tc.cu for the layout)
+  DevBuf buf;
+  int kind = -1;  // GMG_BF16 or GMG_F16, -1 = not built
+};
+
+}  // namespace gmg
+
+struct gmg_coarse {
+  gmg::Dims dims;
+  int N = 0;
+  int hermitian = 0;
+  bool links_set = false;
+  gmg::DevBuf nbr;         // int32 [9][V]
+  gmg::DevBuf links_ref;   // complex<double> [9][V][N][N] (exchange layout)
+  gmg::DevBuf links_d;     // complex<double> [V][9][N][N] (site-major, SIMT kernels)
+  gmg::DevBuf links_f;     // complex<float>  [V][9][N][N]
+  bool links_f_ok = false;
+  gmg::LinksF16 links_h;
+  gmg::DevBuf scratch;     // per-handle temporary: packed tensor-core vectors
+  gmg::DevBuf dev_err;     // int: first error code a kernel of this handle recorded
+};
+
+struct gmg_agg {
+  gmg::Dims fdims, cdims;
+  int b[4] = {0, 0, 0, 0};
+  int bv = 0;       // fine sites per block
+  int dof = 0;      // complex dof per fine site
+  int N = 0;
+  bool basis_set = false;
+  gmg::DevBuf blk_sites;  // int32 [Vc][bv]: fine site of in-block index (lexicographic)
+  gmg::DevBuf basis_blk;  // complex<double> [Vc][N][bv*dof]   (block-major copy)
+  gmg::DevBuf basis_blk_f;  // complex<float> same layout
+  bool basis_f_ok = false;
+  gmg::DevBuf scratch;
+};
+
+struct gmg_wilson {
+  gmg::Dims dims;
+  double mass = 0, csw = 0;
+  int apbc = 0;
+  bool gauge_set = false;
+  gmg::DevBuf gauge;      // complex<double> [V][4][3][3]
+  gmg::DevBuf gauge_f;    // complex<float>
+  gmg::DevBuf clover;     // complex<double> [V][2][6][6]
+  gmg::DevBuf clover_f;
+  gmg::DevBuf nbr;        // int32 [9][V]
+};
+
+namespace gmg {
+
+// neighbour table (device) for a lattice
+gmg_status build_neighbors(const Dims& d, DevBuf& nbr, cudaStream_t s);
+void host_neighbors(const Dims& d, int32_t* nbr);
+
+// coarse stencil kernels (coarse_stencil.cu)
+gmg_status coarse_links_to_site_major(gmg_coarse* h, cudaStream_t s);
+gmg_status coarse_prepare_f32(gmg_coarse* h, cudaStream_t s);
+gmg_status coarse_apply_simt(gmg_coarse* h, int p0, int p1, bool g5, int compute, int vec_prec,
+                             int nrhs, const void* in, void* out, const int32_t* active,
+                             int n_active, cudaStream_t s);
+gmg_status coarse_construct_remaining(gmg_coarse* h, cudaStream_t s);
+
+// tensor-core multi-RHS stencil (coarse_mrhs_tc.cu)
+gmg_status coarse_prepare_tc(gmg_coarse* h, int kind, cudaStream_t s);
+gmg_status coarse_apply_tc(gmg_coarse* h, int p0, int p1, bool g5, int kind, int nrhs,
+                           const float* in, float* out, const int32_t* active, int n_active,
+                           cudaStream_t s);
+
+// aggregation kernels (block_ops.cu)
+gmg_status agg_build_tables(gmg_agg* h, cudaStream_t s);
+gmg_status agg_basis_to_blocked(gmg_agg* h, const double* basis_dev, cudaStream_t s);
+gmg_status agg_basis_from_blocked(gmg_agg* h, double* basis_dev, cudaStream_t s);
+gmg_status agg_project(gmg_agg* h, int compute, int vec_prec, int nrhs, const void* fine,
+                       void* coarse, const int32_t* mask_blk, cudaStream_t s);
+gmg_status agg_promote(gmg_agg* h, int compute, int vec_prec, int nrhs, const void* coarse,
+                       void* fine, cudaStream_t s);
+gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s);
+gmg_status agg_check_orthogonal(gmg_agg* h, double* max_err, cudaStream_t s);
+gmg_status agg_prepare_f32(gmg_agg* h, cudaStream_t s);
+
+// fine Wilson-clover (wilson.cu)
+gmg_status wilson_build_clover(gmg_wilson* h, cudaStream_t s);
+gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs,
+                        const void* in, void* out, cudaStream_t s);
+
+// coarse-operator construction (coarsen.cu)
+gmg_status coarsen_wilson(gmg_coarse* out, gmg_agg* agg, gmg_wilson* fine, cudaStream_t s);
+gmg_status coarsen_coarse(gmg_coarse* out, gmg_agg* agg, gmg_coarse* fine, cudaStream_t s);
+
+}  // namespace gmg

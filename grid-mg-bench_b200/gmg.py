@@ -1,0 +1,305 @@
+"""Python binding of libgmg_b200.so (ctypes over the C ABI in include/gmg.h).
+
+Mirrors the reference's class surface so that tests read like the reference's
+own drivers:
+
+  CoarsenedMatrix   M, Mdag, Mdiag, Mdir, MdirAll, CoarsenOperator, links A
+                    (include/CoarsenedMatrixUpstream.h:515-931)
+  Aggregation       Orthogonalise, CheckOrthogonal, ProjectToSubspace,
+                    PromoteFromSubspace, subspace (...LutMRHS.h:293-352)
+  WilsonClover      Op/AdjOp/OpDiag/OpDir of the fine operator
+                    (MdagMLinearOperator over WilsonCloverFermionR)
+
+Vectors are torch CUDA tensors: complex128 (FP64) or complex64 (FP32) with
+shape [sites, nrhs, dof].  There is no CPU fallback: without the built
+library or a GPU every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgmg_b200.so")
+_LIB = None
+
+F64, F32, BF16, F16 = 0, 1, 2, 3
+OP_M, OP_MDAG, OP_MDIAG, OP_MDIR = 0, 1, 2, 3
+PREC = {"f64": F64, "f32": F32, "bf16": BF16, "f16": F16}
+
+
+class GmgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"gmg status {status}: {msg}")
+        self.status = status
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with grid-mg-bench_b200/build.py")
+        _LIB = ctypes.CDLL(LIB_PATH)
+        _LIB.gmg_last_error.restype = ctypes.c_char_p
+        _LIB.gmg_version.restype = ctypes.c_char_p
+    return _LIB
+
+
+def _chk(st):
+    if st != 0:
+        raise GmgError(st, lib().gmg_last_error().decode())
+
+
+def _dims(d):
+    return (ctypes.c_int * 4)(*[int(x) for x in d])
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _vec_prec(t):
+    if t.dtype == torch.complex128:
+        return F64
+    if t.dtype == torch.complex64:
+        return F32
+    raise TypeError(f"vectors must be complex128 or complex64, got {t.dtype}")
+
+
+def _check_vec(t, V, dof, name):
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError(f"{name} must be a contiguous CUDA tensor")
+    if t.dim() != 3 or t.shape[0] != V or t.shape[2] != dof:
+        raise ValueError(f"{name} must have shape [{V}, nrhs, {dof}], got {tuple(t.shape)}")
+
+
+def vol(d):
+    return int(np.prod(d))
+
+
+class CoarsenedMatrix:
+    """CoarsenedMatrix(CoarseGrid, hermitian) over the 9-point coarse stencil."""
+
+    def __init__(self, dims, nbasis, hermitian=0):
+        self.dims = tuple(int(x) for x in dims)
+        self.N = int(nbasis)
+        self.hermitian = int(hermitian)
+        self.V = vol(self.dims)
+        h = ctypes.c_void_p()
+        _chk(lib().gmg_coarse_create(_dims(self.dims), self.N, self.hermitian, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.gmg_coarse_destroy(self._h)
+            self._h = None
+
+    # link fields A[p], exchange layout [9][V][N][N]
+    def set_links(self, A):
+        if isinstance(A, torch.Tensor):
+            A = A.to(torch.complex128).contiguous()
+            _chk(lib().gmg_coarse_set_links(self._h, _ptr(A), 1 if A.is_cuda else 0, _stream()))
+            torch.cuda.current_stream().synchronize()
+        else:
+            a = np.ascontiguousarray(A, dtype=np.complex128)
+            assert a.shape == (9, self.V, self.N, self.N)
+            _chk(lib().gmg_coarse_set_links(self._h, a.ctypes.data_as(ctypes.c_void_p), 0, _stream()))
+
+    def get_links(self):
+        a = np.zeros((9, self.V, self.N, self.N), dtype=np.complex128)
+        _chk(lib().gmg_coarse_get_links(self._h, a.ctypes.data_as(ctypes.c_void_p), 0, _stream()))
+        return a
+
+    def prepare(self, compute):
+        _chk(lib().gmg_coarse_prepare(self._h, PREC.get(compute, compute), _stream()))
+
+    def apply(self, op, inp, out, point=8, compute=None, active=None):
+        _check_vec(inp, self.V, self.N, "in")
+        _check_vec(out, self.V, self.N, "out")
+        vp = _vec_prec(inp)
+        if _vec_prec(out) != vp or out.shape != inp.shape:
+            raise ValueError("in and out must match in shape and dtype")
+        c = vp if compute is None else PREC.get(compute, compute)
+        act = None
+        n_act = 0
+        if active is not None:
+            act = active if isinstance(active, torch.Tensor) else torch.tensor(active, dtype=torch.int32,
+                                                                               device=inp.device)
+            assert act.dtype == torch.int32 and act.is_cuda
+            n_act = act.numel()
+        _chk(lib().gmg_coarse_apply(self._h, op, point, c, vp, inp.shape[1], _ptr(inp), _ptr(out),
+                                    _ptr(act) if act is not None else None, n_act, _stream()))
+        return out
+
+    def M(self, inp, out, **kw):
+        return self.apply(OP_M, inp, out, **kw)
+
+    def Mdag(self, inp, out, **kw):
+        return self.apply(OP_MDAG, inp, out, **kw)
+
+    def Mdiag(self, inp, out, **kw):
+        return self.apply(OP_MDIAG, inp, out, **kw)
+
+    def Mdir(self, inp, out, d, disp, **kw):
+        p = lib().gmg_point_from_dir_disp(4, 1, d, disp)
+        if p < 0:
+            raise ValueError("bad direction / displacement")
+        return self.apply(OP_MDIR, inp, out, point=p, **kw)
+
+    def MdirAll(self, inp, outs, compute=None):
+        assert len(outs) == 8
+        vp = _vec_prec(inp)
+        c = vp if compute is None else PREC.get(compute, compute)
+        arr = (ctypes.c_void_p * 8)(*[o.data_ptr() for o in outs])
+        _chk(lib().gmg_coarse_mdir_all(self._h, c, vp, inp.shape[1], _ptr(inp), arr, _stream()))
+        return outs
+
+    def construct_remaining_links(self):
+        _chk(lib().gmg_coarse_construct_remaining_links(self._h, _stream()))
+
+    def neighbors(self):
+        n = np.zeros((9, self.V), dtype=np.int32)
+        _chk(lib().gmg_coarse_neighbors(self._h, n.ctypes.data_as(ctypes.c_void_p)))
+        return n
+
+    def CoarsenOperator(self, agg, linop):
+        if isinstance(linop, WilsonClover):
+            _chk(lib().gmg_coarsen_wilson(self._h, agg._h, linop._h, _stream()))
+        elif isinstance(linop, CoarsenedMatrix):
+            _chk(lib().gmg_coarsen_coarse(self._h, agg._h, linop._h, _stream()))
+        else:
+            raise TypeError("linop must be WilsonClover or CoarsenedMatrix")
+
+
+class Aggregation:
+    """Aggregation(CoarseGrid, FineGrid): block basis, project / promote / orthonormalise."""
+
+    def __init__(self, fine_dims, coarse_dims, site_dof, nbasis):
+        self.fdims = tuple(int(x) for x in fine_dims)
+        self.cdims = tuple(int(x) for x in coarse_dims)
+        self.dof = int(site_dof)
+        self.N = int(nbasis)
+        self.Vf, self.Vc = vol(self.fdims), vol(self.cdims)
+        h = ctypes.c_void_p()
+        _chk(lib().gmg_agg_create(_dims(self.fdims), _dims(self.cdims), self.dof, self.N, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.gmg_agg_destroy(self._h)
+            self._h = None
+
+    def set_basis(self, B):
+        if isinstance(B, torch.Tensor):
+            B = B.to(torch.complex128).contiguous()
+            _chk(lib().gmg_agg_set_basis(self._h, _ptr(B), 1 if B.is_cuda else 0, _stream()))
+            torch.cuda.current_stream().synchronize()
+        else:
+            b = np.ascontiguousarray(B, dtype=np.complex128)
+            assert b.shape == (self.N, self.Vf, self.dof)
+            _chk(lib().gmg_agg_set_basis(self._h, b.ctypes.data_as(ctypes.c_void_p), 0, _stream()))
+
+    def get_basis(self):
+        b = np.zeros((self.N, self.Vf, self.dof), dtype=np.complex128)
+        _chk(lib().gmg_agg_get_basis(self._h, b.ctypes.data_as(ctypes.c_void_p), 0, _stream()))
+        return b
+
+    def Orthogonalise(self, passes=1):
+        _chk(lib().gmg_agg_orthonormalise(self._h, passes, _stream()))
+
+    def CheckOrthogonal(self):
+        e = ctypes.c_double()
+        _chk(lib().gmg_agg_check_orthogonal(self._h, ctypes.byref(e), _stream()))
+        return e.value
+
+    def ProjectToSubspace(self, fine, coarse, compute=None):
+        _check_vec(fine, self.Vf, self.dof, "fine")
+        _check_vec(coarse, self.Vc, self.N, "coarse")
+        vp = _vec_prec(fine)
+        c = vp if compute is None else PREC.get(compute, compute)
+        _chk(lib().gmg_agg_project(self._h, c, vp, fine.shape[1], _ptr(fine), _ptr(coarse), _stream()))
+        return coarse
+
+    def PromoteFromSubspace(self, coarse, fine, compute=None):
+        _check_vec(fine, self.Vf, self.dof, "fine")
+        _check_vec(coarse, self.Vc, self.N, "coarse")
+        vp = _vec_prec(fine)
+        c = vp if compute is None else PREC.get(compute, compute)
+        _chk(lib().gmg_agg_promote(self._h, c, vp, coarse.shape[1], _ptr(coarse), _ptr(fine), _stream()))
+        return fine
+
+
+class WilsonClover:
+    """Fine Wilson-clover operator: Op (M), AdjOp (Mdag), OpDiag, OpDir."""
+
+    def __init__(self, dims, mass, csw, antiperiodic=False):
+        self.dims = tuple(int(x) for x in dims)
+        self.V = vol(self.dims)
+        h = ctypes.c_void_p()
+        _chk(lib().gmg_wilson_create(_dims(self.dims), ctypes.c_double(mass), ctypes.c_double(csw),
+                                     int(bool(antiperiodic)), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.gmg_wilson_destroy(self._h)
+            self._h = None
+
+    def set_gauge(self, U):
+        u = np.ascontiguousarray(U, dtype=np.complex128)
+        assert u.shape == (self.V, 4, 3, 3)
+        _chk(lib().gmg_wilson_set_gauge(self._h, u.ctypes.data_as(ctypes.c_void_p), 0, _stream()))
+
+    def clover(self):
+        c = np.zeros((self.V, 2, 6, 6), dtype=np.complex128)
+        _chk(lib().gmg_wilson_get_clover(self._h, c.ctypes.data_as(ctypes.c_void_p), 0, _stream()))
+        return c
+
+    def apply(self, op, inp, out, d=0, disp=0):
+        _check_vec(inp, self.V, 12, "in")
+        _check_vec(out, self.V, 12, "out")
+        _chk(lib().gmg_wilson_apply(self._h, op, d, disp, _vec_prec(inp), inp.shape[1], _ptr(inp), _ptr(out),
+                                    _stream()))
+        return out
+
+    def M(self, inp, out):
+        return self.apply(OP_M, inp, out)
+
+    def Mdag(self, inp, out):
+        return self.apply(OP_MDAG, inp, out)
+
+    def Mdiag(self, inp, out):
+        return self.apply(OP_MDIAG, inp, out)
+
+    def Mdir(self, inp, out, d, disp):
+        return self.apply(OP_MDIR, inp, out, d, disp)
+
+
+def lut_build(fine_dims, coarse_dims, mask_kind=-1):
+    b = [f // c for f, c in zip(fine_dims, coarse_dims)]
+    bv = int(np.prod(b))
+    Vc, Vf = vol(coarse_dims), vol(fine_dims)
+    l = np.zeros((Vc, bv), dtype=np.int32)
+    s = np.zeros(Vc, dtype=np.int32)
+    r = np.zeros(Vf, dtype=np.int32)
+    _chk(lib().gmg_lut_build(_dims(fine_dims), _dims(coarse_dims), mask_kind, l.ctypes.data_as(ctypes.c_void_p),
+                             s.ctypes.data_as(ctypes.c_void_p), r.ctypes.data_as(ctypes.c_void_p)))
+    return l, s, r
+
+
+def point_from_dir_disp(ndim, dirs_faster, d, disp):
+    return lib().gmg_point_from_dir_disp(ndim, int(dirs_faster), d, disp)
+
+
+def layout_links(links, ncs, inverse=False):
+    """Device links [V][N][N] (complex128 tensor) flat <-> Rework spin-split layout."""
+    out = torch.empty_like(links)
+    N = links.shape[-1]
+    V = links.numel() // (N * N)
+    _chk(lib().gmg_layout_links(ctypes.c_int64(V), N, ncs, _ptr(links), _ptr(out), int(inverse), _stream()))
+    return out

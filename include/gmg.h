@@ -1,0 +1,194 @@
+/*
+ * gmg.h -- C ABI of the B200-native multigrid hot path (libgmg_b200.so).
+ *
+ * Drop-in boundary for grid-mg-bench's coarse-operator and aggregation
+ * classes.  Every entry point names the reference interface it replaces
+ * (paths inside DanielRichtmann/grid-mg-bench).  Plain pointers and sizes
+ * only; streams are cudaStream_t values passed as `gmg_stream` (NULL = the
+ * legacy default stream).  All calls are stream-ordered and asynchronous
+ * unless stated; calls on one handle are not thread-safe, calls on different
+ * handles are.  Every call returns a gmg_status; gmg_last_error() gives the
+ * message of the last failure on the calling thread.
+ *
+ * Layouts (complex numbers interleaved re, im; sites lexicographic, x fastest):
+ *   fine field       [site][rhs][dof]          dof = 12 (spin-major, colour fastest)
+ *   coarse field     [site][rhs][nbasis]       (the reference's 5-d MRHS layout,
+ *                                               ...LutMRHS.h:767-790, RHS fastest)
+ *   basis            [i][site][dof]            (Aggregation::subspace)
+ *   coarse links     [point][site][b][bb]      (CoarsenedMatrix::A, row-major N x N)
+ *   gauge field      [site][mu][3][3]
+ *   stencil points   p<4: (dir p, +1); 4<=p<8: (dir p-4, -1); p=8: self
+ *                    (GeometryRework.h:54-125, directions-faster order)
+ */
+#ifndef GMG_H
+#define GMG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* gmg_stream;
+
+typedef enum {
+  GMG_OK = 0,
+  GMG_ERR_ARGUMENT = 1,      /* null pointer / out-of-range argument */
+  GMG_ERR_SHAPE = 2,         /* non-conformable sizes (Grid's conformable() abort) */
+  GMG_ERR_STATE = 3,         /* handle not ready (links / basis / gauge not set) */
+  GMG_ERR_CUDA = 4,          /* CUDA runtime error */
+  GMG_ERR_NOMEM = 5,         /* device allocation failed */
+  GMG_ERR_UNSUPPORTED = 6,   /* precision / size combination not built */
+  GMG_ERR_NONFINITE = 7,     /* NaN or Inf detected */
+  GMG_ERR_NOT_CONVERGED = 8, /* iterative solve hit its iteration limit */
+  GMG_ERR_TIMEOUT = 9        /* a bounded device wait ran out */
+} gmg_status;
+
+typedef enum { GMG_F64 = 0, GMG_F32 = 1, GMG_BF16 = 2, GMG_F16 = 3 } gmg_prec;
+
+typedef enum { GMG_OP_M = 0, GMG_OP_MDAG = 1, GMG_OP_MDIAG = 2, GMG_OP_MDIR = 3 } gmg_op;
+
+const char* gmg_last_error(void);
+const char* gmg_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Geometry and lookup tables                                                */
+/* ------------------------------------------------------------------------ */
+
+/* Rework::Geometry::PointFromDirDisp (GeometryRework.h:65-98); -1 on bad input. */
+int gmg_point_from_dir_disp(int ndim, int dirs_faster, int dir, int disp);
+
+/* CoarseningLookupTable::populate (CoarseningLookupTableRework.h:114-179) for
+   mask_kind: -1 = full block, 0..7 = outer face of stencil point p
+   (CoarsenedMatrixUpstream.h:815-821), 9 = even blocks, 10 = odd blocks.
+   Host outputs: lut[Vc][bv] (-1 padded), sizes[Vc], reverse[Vf] (nullable). */
+gmg_status gmg_lut_build(const int fine_dims[4], const int coarse_dims[4], int mask_kind,
+                         int32_t* lut, int32_t* sizes, int32_t* reverse);
+
+/* ------------------------------------------------------------------------ */
+/* Coarse stencil -- CoarsenedMatrix (CoarsenedMatrixUpstream.h:515-753)    */
+/* ------------------------------------------------------------------------ */
+typedef struct gmg_coarse gmg_coarse;
+
+/* CoarsenedMatrix(GridCartesian& CoarseGrid, int hermitian) (CoarsenedMatrixUpstream.h:745-753) */
+gmg_status gmg_coarse_create(const int dims[4], int nbasis, int hermitian, gmg_coarse** h);
+gmg_status gmg_coarse_destroy(gmg_coarse* h);
+
+/* Write / read the public link fields A[p] (CoarsenedMatrixUpstream.h:536, written
+   by the benchmarks at Benchmark_coarse_operator.cc:121-127).  `links` is
+   [9][V][N][N] complex128 on the host (on_device=0) or the device (1).
+   Setting links refreshes every reduced-precision copy already prepared. */
+gmg_status gmg_coarse_set_links(gmg_coarse* h, const double* links, int on_device, gmg_stream s);
+gmg_status gmg_coarse_get_links(gmg_coarse* h, double* links, int on_device, gmg_stream s);
+
+/* Build the link copy used by `compute` (F32, BF16 or F16); F64 needs none. */
+gmg_status gmg_coarse_prepare(gmg_coarse* h, gmg_prec compute, gmg_stream s);
+
+/* M / Mdag / Mdiag / Mdir(point) on nrhs right-hand sides
+   (CoarsenedMatrixUpstream.h:546-742; multi-RHS ...LutMRHS.h:736-947).
+   in, out: device coarse fields [V][nrhs][N] of type vec_prec (F64 or F32).
+   compute: F64 (FP64 links+vectors), F32 (FP32), BF16 / F16 (tensor cores,
+   FP32 accumulation, FP32 vectors).  Mdag is G5C M G5C unless hermitian,
+   fused into the load/store.  active (device int32[n_active], nullable)
+   restricts the apply to those RHS slots; other slots of `out` are untouched. */
+gmg_status gmg_coarse_apply(gmg_coarse* h, gmg_op op, int point, gmg_prec compute,
+                            gmg_prec vec_prec, int nrhs, const void* in, void* out,
+                            const int32_t* active, int n_active, gmg_stream s);
+
+/* MdirAll (CoarsenedMatrixUpstream.h:700-713): out8[p] = A_p in(nbr_p), p < 8. */
+gmg_status gmg_coarse_mdir_all(gmg_coarse* h, gmg_prec compute, gmg_prec vec_prec, int nrhs,
+                               const void* in, void* const* out8, gmg_stream s);
+
+/* ConstructRemainingLinks / ForceHermitian (...DirsaveLut.h:1164-1196,
+   CoarsenedMatrixUpstream.h:956-976): rebuild the 4 forward links from the
+   backward ones, A_{+mu}(x) = S o A_{-mu}(x+mu)^dag (S = 1 if hermitian). */
+gmg_status gmg_coarse_construct_remaining_links(gmg_coarse* h, gmg_stream s);
+
+/* Error code recorded on the device by this handle's tensor-core kernels
+   (0 = none; otherwise a bounded wait ran out and the kernel returned early),
+   read after a device synchronisation and then cleared.  Returns
+   GMG_ERR_TIMEOUT when *code != 0.  No counterpart in the reference, whose
+   kernels cannot time out. */
+gmg_status gmg_coarse_device_error(gmg_coarse* h, int* code);
+
+/* Host copy of the 9-point neighbour table nbr[9][V] (bit-exact index check). */
+gmg_status gmg_coarse_neighbors(gmg_coarse* h, int32_t* nbr);
+
+/* Device pointer of the FP64 links in the exchange layout (valid until destroy). */
+gmg_status gmg_coarse_links_device(gmg_coarse* h, double** links);
+
+/* ------------------------------------------------------------------------ */
+/* Aggregation -- Aggregation (...LutMRHS.h:293-352, AggregationRework.h)    */
+/* ------------------------------------------------------------------------ */
+typedef struct gmg_agg gmg_agg;
+
+/* Aggregation(CoarseGrid, FineGrid, checkerboard) with site_dof = 12 on the
+   fine level or nbasis of the level above for coarse-of-coarse. */
+gmg_status gmg_agg_create(const int fine_dims[4], const int coarse_dims[4], int site_dof,
+                          int nbasis, gmg_agg** h);
+gmg_status gmg_agg_destroy(gmg_agg* h);
+
+/* subspace[i] = basis[i] (public member `subspace`, ...LutMRHS.h:298). */
+gmg_status gmg_agg_set_basis(gmg_agg* h, const double* basis, int on_device, gmg_stream s);
+gmg_status gmg_agg_get_basis(gmg_agg* h, double* basis, int on_device, gmg_stream s);
+
+/* Orthogonalise(check, passes) (...LutMRHS.h:318-325) in FP64: per-block
+   orthonormalisation, `passes` sweeps (blockLutedOrthonormalise, ...Lut.h:172-240). */
+gmg_status gmg_agg_orthonormalise(gmg_agg* h, int passes, gmg_stream s);
+
+/* CheckOrthogonal (...LutMRHS.h:326-340): max over blocks of |B^dag B - 1|_max.
+   Synchronises the stream. */
+gmg_status gmg_agg_check_orthogonal(gmg_agg* h, double* max_err, gmg_stream s);
+
+/* ProjectToSubspace / PromoteFromSubspace (...LutMRHS.h:341-347), i.e.
+   blockLutedInnerProduct / blockLutedAxpy (...Lut.h:70-170) on nrhs RHS.
+   fine [Vf][nrhs][dof], coarse [Vc][nrhs][N], both of type vec_prec (F64/F32);
+   compute F64 or F32. */
+gmg_status gmg_agg_project(gmg_agg* h, gmg_prec compute, gmg_prec vec_prec, int nrhs,
+                           const void* fine, void* coarse, gmg_stream s);
+gmg_status gmg_agg_promote(gmg_agg* h, gmg_prec compute, gmg_prec vec_prec, int nrhs,
+                           const void* coarse, void* fine, gmg_stream s);
+
+/* ------------------------------------------------------------------------ */
+/* Fine Wilson-clover operator (Grid WilsonCloverFermionR through            */
+/* MdagMLinearOperator::{Op,AdjOp,OpDiag,OpDir}, used at                     */
+/* Test_wilsonclover_mg.cc:103-113 and Benchmark_create_coarse_operator.cc)  */
+/* ------------------------------------------------------------------------ */
+typedef struct gmg_wilson gmg_wilson;
+
+gmg_status gmg_wilson_create(const int dims[4], double mass, double csw, int antiperiodic_t,
+                             gmg_wilson** h);
+gmg_status gmg_wilson_destroy(gmg_wilson* h);
+/* Set the gauge field [V][4][3][3] and build the clover term on the device. */
+gmg_status gmg_wilson_set_gauge(gmg_wilson* h, const double* U, int on_device, gmg_stream s);
+/* Clover blocks [V][2][6][6] complex128 to host or device memory. */
+gmg_status gmg_wilson_get_clover(gmg_wilson* h, double* clover, int on_device, gmg_stream s);
+/* op M / Mdag / Mdiag / Mdir(dir, disp); fields [V][nrhs][12] of vec_prec (F64/F32). */
+gmg_status gmg_wilson_apply(gmg_wilson* h, gmg_op op, int dir, int disp, gmg_prec vec_prec,
+                            int nrhs, const void* in, void* out, gmg_stream s);
+
+/* ------------------------------------------------------------------------ */
+/* Galerkin coarse-operator construction                                     */
+/* CoarsenOperator(FineGrid, linop, Aggregation) (CoarsenedMatrixUpstream.h: */
+/* 755-931, ...DirsaveLut.h:927-1097)                                        */
+/* ------------------------------------------------------------------------ */
+
+/* Links of `out` from the fine Wilson-clover operator and the basis of `agg`
+   (backward projections + self term by the block even/odd trick + link
+   reconstruction), FP64. */
+gmg_status gmg_coarsen_wilson(gmg_coarse* out, gmg_agg* agg, gmg_wilson* fine, gmg_stream s);
+/* Coarse-of-coarse: the fine operator is the coarse stencil `fine`. */
+gmg_status gmg_coarsen_coarse(gmg_coarse* out, gmg_agg* agg, gmg_coarse* fine, gmg_stream s);
+
+/* ------------------------------------------------------------------------ */
+/* Rework layout maps (Layout_converters.h:33-139): flat basis index          */
+/* n = s*Nc_c + c <-> (s, c).  Device links [V][N][N], inverse=1 for spin->flat */
+/* ------------------------------------------------------------------------ */
+gmg_status gmg_layout_links(int64_t V, int nbasis, int ncs, const double* in, double* out,
+                            int inverse, gmg_stream s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GMG_H */

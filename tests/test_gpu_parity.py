@@ -1,0 +1,314 @@
+"""GPU parity of the CUDA path (through the C ABI) against the FP64 CPU oracle.
+
+Tolerances are the reference's relative squared deviation |ref-res|^2/|ref|^2
+(include/Benchmark_helpers.h:215-236): 1e-15 for FP64 (src/Benchmark_coarse_operator.cc:81)
+and 1e-7 for FP32; tensor-core forms state their own bound in their tests.
+"""
+import numpy as np
+import pytest
+import torch
+
+import gmg
+import inputs
+import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-15
+TOL32 = 1e-7
+DEV = "cuda:0"
+
+
+def dev(a, dtype=torch.complex128):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV).to(dtype)
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy().astype(np.complex128)
+
+
+# ---------------------------------------------------------------- coarse stencil
+@pytest.fixture(scope="module")
+def coarse44():
+    dims, N = (4, 4, 4, 4), 24
+    r = inputs.rng(stream=101)
+    A = inputs.random_links(dims, N, r)
+    x = inputs.gaussian_field((256, 5, N), r)
+    cm = gmg.CoarsenedMatrix(dims, N)
+    cm.set_links(A)
+    return dims, N, A, x, cm
+
+
+def test_neighbors_bit_exact(coarse44):
+    dims, N, A, x, cm = coarse44
+    assert np.array_equal(cm.neighbors(), orc.coarse_neighbors(dims))
+
+
+def test_links_round_trip(coarse44):
+    dims, N, A, x, cm = coarse44
+    assert np.array_equal(cm.get_links(), A)
+
+
+@pytest.mark.parametrize("nrhs", [1, 2, 5])
+@pytest.mark.parametrize("op", ["M", "Mdag", "Mdiag"])
+def test_coarse_ops_f64(coarse44, nrhs, op):
+    dims, N, A, x, cm = coarse44
+    xs = x[:, :nrhs]
+    code = {"M": orc.OP_M, "Mdag": orc.OP_MDAG, "Mdiag": orc.OP_MDIAG}[op]
+    ref = orc.coarse_apply(dims, A, xs, code)
+    inp = dev(xs)
+    out = torch.zeros_like(inp)
+    getattr(cm, op)(inp, out)
+    assert orc.rel_dev_sq(ref, host(out)) < TOL64
+
+
+def test_coarse_mdir_and_mdirall_f64(coarse44):
+    dims, N, A, x, cm = coarse44
+    inp = dev(x[:, :2])
+    outs = [torch.zeros_like(inp) for _ in range(8)]
+    cm.MdirAll(inp, outs)
+    for p in range(8):
+        ref = orc.coarse_apply(dims, A, x[:, :2], orc.OP_MDIR, point=p)
+        assert orc.rel_dev_sq(ref, host(outs[p])) < TOL64
+        out = torch.zeros_like(inp)
+        cm.Mdir(inp, out, p % 4, 1 if p < 4 else -1)
+        assert orc.rel_dev_sq(ref, host(out)) < TOL64
+
+
+def test_coarse_f32(coarse44):
+    dims, N, A, x, cm = coarse44
+    cm.prepare("f32")
+    for code, name in ((orc.OP_M, "M"), (orc.OP_MDAG, "Mdag")):
+        ref = orc.coarse_apply(dims, A, x, code)
+        inp = dev(x, torch.complex64)
+        out = torch.zeros_like(inp)
+        getattr(cm, name)(inp, out)
+        assert orc.rel_dev_sq(ref, host(out)) < TOL32
+
+
+def test_coarse_active_rhs_subset(coarse44):
+    dims, N, A, x, cm = coarse44
+    inp = dev(x)
+    out = torch.full_like(inp, 7.0)
+    active = [4, 1, 3]
+    cm.M(inp, out, active=active)
+    ref = orc.coarse_apply(dims, A, x, orc.OP_M)
+    got = host(out)
+    for r in range(5):
+        if r in active:
+            assert orc.rel_dev_sq(ref[:, r], got[:, r]) < TOL64
+        else:
+            assert np.all(got[:, r] == 7.0)
+
+
+def test_coarse_hermitian_mdag_is_m():
+    dims, N = (2, 4, 2, 4), 8
+    A = inputs.random_links(dims, N, inputs.rng(stream=102))
+    cm = gmg.CoarsenedMatrix(dims, N, hermitian=1)
+    cm.set_links(A)
+    x = dev(inputs.gaussian_field((64, 3, N), inputs.rng(stream=103)))
+    a, b = torch.zeros_like(x), torch.zeros_like(x)
+    cm.M(x, a)
+    cm.Mdag(x, b)
+    assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("dims,N", [((8, 8, 8, 8), 32), ((4, 4, 4, 4), 40)])
+def test_coarse_mrhs_config_sizes(dims, N):
+    # C2-shaped (8^4, N=32) and C4-shaped (N=40) applies with 8 RHS against the oracle
+    r = inputs.rng(stream=104)
+    A = inputs.random_links(dims, N, r)
+    x = inputs.gaussian_field((int(np.prod(dims)), 8, N), r)
+    cm = gmg.CoarsenedMatrix(dims, N)
+    cm.set_links(A)
+    ref = orc.coarse_apply(dims, A, x, orc.OP_M)
+    out = torch.zeros(x.shape, dtype=torch.complex128, device=DEV)
+    cm.M(dev(x), out)
+    assert orc.rel_dev_sq(ref, host(out)) < TOL64
+
+
+def test_construct_remaining_links_matches_oracle():
+    dims, N = (4, 2, 4, 2), 8
+    A = inputs.gaussian_field((9, 64, N, N), inputs.rng(stream=105))
+    for herm in (0, 1):
+        cm = gmg.CoarsenedMatrix(dims, N, hermitian=herm)
+        cm.set_links(A)
+        cm.construct_remaining_links()
+        ref = orc.construct_remaining_links(dims, A, herm)
+        assert np.array_equal(cm.get_links(), ref)
+
+
+def test_layout_links_matches_oracle():
+    a = inputs.gaussian_field((6, 8, 8), inputs.rng(stream=106))
+    t = dev(a)
+    spin = gmg.layout_links(t, 2)
+    assert np.array_equal(host(spin), orc.layout_link_flat_to_spin(a, 2))
+    assert torch.equal(gmg.layout_links(spin, 2, inverse=True), t)
+
+
+# ------------------------------------------------------------------ aggregation
+@pytest.fixture(scope="module")
+def agg8():
+    fd, cd = (8, 8, 4, 4), (2, 2, 2, 2)
+    h = inputs.gaussian_field((4, int(np.prod(fd)), 12), inputs.rng(stream=111))
+    B0 = orc.chiral_double(h, 0.5)
+    ag = gmg.Aggregation(fd, cd, 12, 8)
+    ag.set_basis(B0)
+    return fd, cd, B0, ag
+
+
+def test_basis_round_trip(agg8):
+    fd, cd, B0, ag = agg8
+    assert np.array_equal(ag.get_basis(), B0)
+
+
+def test_orthonormalise_matches_mgs(agg8):
+    fd, cd, B0, ag = agg8
+    ag2 = gmg.Aggregation(fd, cd, 12, 8)
+    ag2.set_basis(B0)
+    ag2.Orthogonalise(passes=1)
+    got = ag2.get_basis()
+    ref = orc.block_orthonormalise(fd, cd, B0, passes=1)
+    assert orc.rel_dev_sq(ref, got) < 1e-24
+    assert ag2.CheckOrthogonal() < 1e-13
+    ag2.Orthogonalise(passes=2)
+    assert ag2.CheckOrthogonal() < 1e-14
+
+
+@pytest.mark.parametrize("nrhs", [1, 3, 8])
+def test_project_promote_f64(agg8, nrhs):
+    fd, cd, B0, ag = agg8
+    B = orc.block_orthonormalise(fd, cd, B0, passes=1)
+    ag.set_basis(B)
+    f = inputs.gaussian_field((int(np.prod(fd)), nrhs, 12), inputs.rng(stream=112))
+    c = torch.zeros((16, nrhs, 8), dtype=torch.complex128, device=DEV)
+    ag.ProjectToSubspace(dev(f), c)
+    assert orc.rel_dev_sq(orc.block_project(fd, cd, B, f), host(c)) < TOL64
+    vc = inputs.gaussian_field((16, nrhs, 8), inputs.rng(stream=113))
+    fo = torch.zeros((int(np.prod(fd)), nrhs, 12), dtype=torch.complex128, device=DEV)
+    ag.PromoteFromSubspace(dev(vc), fo)
+    assert orc.rel_dev_sq(orc.block_promote(fd, cd, B, vc), host(fo)) < TOL64
+
+
+def test_project_promote_f32(agg8):
+    fd, cd, B0, ag = agg8
+    B = orc.block_orthonormalise(fd, cd, B0, passes=1)
+    ag.set_basis(B)
+    f = inputs.gaussian_field((int(np.prod(fd)), 4, 12), inputs.rng(stream=114))
+    c = torch.zeros((16, 4, 8), dtype=torch.complex64, device=DEV)
+    ag.ProjectToSubspace(dev(f, torch.complex64), c)
+    assert orc.rel_dev_sq(orc.block_project(fd, cd, B, f), host(c)) < TOL32
+    fo = torch.zeros((int(np.prod(fd)), 4, 12), dtype=torch.complex64, device=DEV)
+    ag.PromoteFromSubspace(c, fo)
+    assert orc.rel_dev_sq(orc.block_promote(fd, cd, B, host(c)), host(fo)) < TOL32
+
+
+def test_transfer_identities_gpu(agg8):
+    # P R v_i = v_i and R P v_c = v_c (MultigridPreconditioner.h:352-396)
+    fd, cd, B0, ag = agg8
+    ag.set_basis(B0)
+    ag.Orthogonalise(passes=1)
+    B = ag.get_basis()
+    vi = dev(np.ascontiguousarray(np.transpose(B[:3], (1, 0, 2))))  # 3 basis vectors as RHS
+    c = torch.zeros((16, 3, 8), dtype=torch.complex128, device=DEV)
+    back = torch.zeros_like(vi)
+    ag.ProjectToSubspace(vi, c)
+    ag.PromoteFromSubspace(c, back)
+    assert orc.rel_dev_sq(host(vi), host(back)) < TOL64
+    vc = dev(inputs.gaussian_field((16, 2, 8), inputs.rng(stream=115)))
+    f = torch.zeros((int(np.prod(fd)), 2, 12), dtype=torch.complex128, device=DEV)
+    rp = torch.zeros_like(vc)
+    ag.PromoteFromSubspace(vc, f)
+    ag.ProjectToSubspace(f, rp)
+    assert orc.rel_dev_sq(host(vc), host(rp)) < TOL64
+
+
+# ----------------------------------------------------------------- wilson-clover
+@pytest.fixture(scope="module")
+def wil():
+    dims = (4, 4, 4, 8)
+    U = inputs.hot_gauge(dims, inputs.rng(stream=121))
+    w = gmg.WilsonClover(dims, -0.1, 1.0, antiperiodic=True)
+    w.set_gauge(U)
+    cl = orc.clover_build(dims, U, 1.0)
+    return dims, U, cl, w
+
+
+def test_clover_matches_oracle(wil):
+    dims, U, cl, w = wil
+    assert orc.rel_dev_sq(cl, w.clover()) < TOL64
+
+
+@pytest.mark.parametrize("op", ["M", "Mdag", "Mdiag"])
+def test_wilson_ops_f64(wil, op):
+    dims, U, cl, w = wil
+    x = inputs.gaussian_field((512, 3, 12), inputs.rng(stream=122))
+    code = {"M": orc.OP_M, "Mdag": orc.OP_MDAG, "Mdiag": orc.OP_MDIAG}[op]
+    ref = orc.wilson_clover(dims, U, cl, -0.1, 1, x, code)
+    out = torch.zeros((512, 3, 12), dtype=torch.complex128, device=DEV)
+    getattr(w, op)(dev(x), out)
+    assert orc.rel_dev_sq(ref, host(out)) < TOL64
+
+
+def test_wilson_mdir_f64_and_f32(wil):
+    dims, U, cl, w = wil
+    x = inputs.gaussian_field((512, 2, 12), inputs.rng(stream=123))
+    for d in range(4):
+        for disp in (1, -1):
+            ref = orc.wilson_clover(dims, U, cl, -0.1, 1, x, orc.OP_MDIR, d, disp)
+            out = torch.zeros((512, 2, 12), dtype=torch.complex128, device=DEV)
+            w.Mdir(dev(x), out, d, disp)
+            assert orc.rel_dev_sq(ref, host(out)) < TOL64
+    ref = orc.wilson_clover(dims, U, cl, -0.1, 1, x, orc.OP_M)
+    out = torch.zeros((512, 2, 12), dtype=torch.complex64, device=DEV)
+    w.M(dev(x, torch.complex64), out)
+    assert orc.rel_dev_sq(ref, host(out)) < TOL32
+
+
+# --------------------------------------------------------------- CoarsenOperator
+@pytest.fixture(scope="module")
+def coarsen_setup():
+    fd, cd = (8, 8, 8, 8), (2, 2, 2, 2)
+    U = inputs.hot_gauge(fd, inputs.rng(stream=131))
+    h = inputs.gaussian_field((4, int(np.prod(fd)), 12), inputs.rng(stream=132))
+    B = orc.block_orthonormalise(fd, cd, orc.chiral_double(h, 0.5), passes=1)
+    return fd, cd, U, B
+
+
+@pytest.mark.parametrize("apbc", [0, 1])
+def test_coarsen_wilson_matches_oracle(coarsen_setup, apbc):
+    fd, cd, U, B = coarsen_setup
+    mass = -0.1
+    w = gmg.WilsonClover(fd, mass, 1.0, antiperiodic=apbc)
+    w.set_gauge(U)
+    ag = gmg.Aggregation(fd, cd, 12, 8)
+    ag.set_basis(B)
+    cm = gmg.CoarsenedMatrix(cd, 8)
+    cm.CoarsenOperator(ag, w)
+    cl = orc.clover_build(fd, U, 1.0)
+    ref = orc.coarsen_wilson(fd, cd, B, U, cl, mass, apbc, 0, variant=0)  # Upstream semantics
+    got = cm.get_links()
+    for p in range(9):
+        assert orc.rel_dev_sq(ref[p], got[p]) < TOL64, p
+
+
+def test_coarsen_coarse_matches_oracle(coarsen_setup):
+    fd, cd, U, B = coarsen_setup
+    c1 = (4, 4, 4, 4)
+    h = inputs.gaussian_field((3, int(np.prod(fd)), 12), inputs.rng(stream=133))
+    B1 = orc.block_orthonormalise(fd, c1, orc.chiral_double(h, 0.5), passes=1)
+    cl = orc.clover_build(fd, U, 1.0)
+    A1 = orc.coarsen_wilson(fd, c1, B1, U, cl, -0.1, 0, 0, variant=1)
+    h2 = inputs.gaussian_field((2, 256, 6), inputs.rng(stream=134))
+    B2 = orc.block_orthonormalise(c1, (2, 2, 2, 2), orc.chiral_double(h2, 0.5), passes=1)
+    fine = gmg.CoarsenedMatrix(c1, 6)
+    fine.set_links(A1)
+    ag = gmg.Aggregation(c1, (2, 2, 2, 2), 6, 4)
+    ag.set_basis(B2)
+    cm = gmg.CoarsenedMatrix((2, 2, 2, 2), 4)
+    cm.CoarsenOperator(ag, fine)
+    ref = orc.coarsen_coarse(c1, (2, 2, 2, 2), B2, A1, variant=0)
+    got = cm.get_links()
+    for p in range(9):
+        assert orc.rel_dev_sq(ref[p], got[p]) < TOL64, p
