@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the multi-RHS coarse stencil (the multigrid hot path's Mrhs apply).
+
+Workload: coarse 8^4 lattice, nbasis 32, 32 right-hand sides, one M apply per
+step (the multi-RHS coarse-stencil configuration: coarse operator of a 32^4
+Wilson-clover lattice on 4^4 blocks).  Links are seeded Gaussian with the
+gamma5-hermitian structure a Galerkin coarsening produces, RHS unit Gaussian.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line on rank 0.  `value` is whole-job TFLOP/s (algorithmic
+flops 8 * V * 9 * N^2 * R per apply) with inputs resident in HBM and L2
+flushed between steps; `e2e` is the same metric through the public C ABI call
+with the RHS copied in from pinned host memory and the result copied back every
+step.  --impl reference times the CPU implementation of the path (the FP64
+oracle restatement, all host threads) on bounded site samples of the same
+workload.  Multi-GPU runs are independent replicas (the path has no exchange
+on one GPU per lattice), timed on the device as the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "grid-mg-bench_b200"))
+
+import numpy as np  # noqa: E402
+
+DIMS = (8, 8, 8, 8)
+NBASIS = 32
+NRHS = 32
+V = int(np.prod(DIMS))
+FLOPS = 8.0 * V * 9 * NBASIS * NBASIS * NRHS  # 9.664 GFLOP per apply
+METRIC = "coarse Mrhs stencil M apply throughput (8^4 coarse lattice, nbasis 32, 32 RHS)"
+UNIT = "TFLOP/s"
+VEC_BYTES_F32 = V * NRHS * NBASIS * 8  # one FP32 coarse field of 32 RHS
+# algorithmic bytes of the dominant kernel (tensor-core stencil on packed BF16 input):
+#   BF16 links 9*V*N^2*4 + packed BF16 input V*R*N*4 + FP32 output V*R*N*8
+TC_KERNEL_BYTES = 9 * V * NBASIS * NBASIS * 4 + V * NRHS * NBASIS * 4 + V * NRHS * NBASIS * 8
+# algorithmic bytes of the whole apply (BF16 links + FP32 in + FP32 out)
+APPLY_BYTES = 9 * V * NBASIS * NBASIS * 4 + 2 * VEC_BYTES_F32
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--form", choices=["bf16", "f16"], default="bf16")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="only warm-up + timed applies (for profiler captures); prints a short line")
+    return ap.parse_args()
+
+
+def make_inputs():
+    import inputs
+
+    r = inputs.rng(stream=4242)
+    A = inputs.random_links(DIMS, NBASIS, r)
+    x = inputs.gaussian_field((V, NRHS, NBASIS), r)
+    return A, x
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------- CPU side
+def cpu_sample(A, x, target_s=12.0, max_reps=400):
+    """FP64 oracle apply on all host threads; full applies until ~target_s of work."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    y = np.empty_like(x)
+    orc.coarse_apply_range(DIMS, A, x, y, 0, V)  # warm-up
+    reps, t = 0, 0.0
+    while reps < max_reps and t < target_s:
+        t0 = time.perf_counter()
+        orc.coarse_apply_range(DIMS, A, x, y, 0, V)
+        t += time.perf_counter() - t0
+        reps += 1
+    return {
+        "value": FLOPS * reps / t / 1e12,
+        "unit": UNIT,
+        "cores": os.cpu_count(),
+        "kind": "port",
+        "sample": f"{reps} full M applies (8^4, nbasis 32, 32 RHS, FP64) with the C++/OpenMP oracle, "
+                  f"{t:.1f} s on {os.cpu_count()} threads",
+    }, y
+
+
+def run_reference(args, rank):
+    """CPU implementation of the path (FP64 oracle restatement) on bounded site samples."""
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    A, x = make_inputs()
+    A = np.ascontiguousarray(A)
+    y = np.empty_like(x)
+    t0 = time.perf_counter()
+    orc.coarse_apply_range(DIMS, A, x, y, 0, V)
+    t_full = time.perf_counter() - t0
+    budget = 150.0  # whole run within a few minutes
+    per_step = min(t_full, budget / max(1, args.steps + args.warmup))
+    nsites = max(16, min(V, int(V * per_step / t_full)))
+    for i in range(args.warmup):
+        s0 = (i * nsites) % (V - nsites + 1)
+        orc.coarse_apply_range(DIMS, A, x, y, s0, s0 + nsites)
+    tot = 0.0
+    for i in range(args.steps):
+        s0 = (i * nsites) % (V - nsites + 1)
+        t0 = time.perf_counter()
+        orc.coarse_apply_range(DIMS, A, x, y, s0, s0 + nsites)
+        tot += time.perf_counter() - t0
+    flops = FLOPS * nsites / V * args.steps
+    val = flops / tot / 1e12
+    line = {
+        "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_dict("FP64 CPU restatement of CoarsenedMatrix::M (oracle)"),
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{nsites} of {V} output sites per step (all 32 RHS), FP64, "
+                                   f"{os.cpu_count()} OpenMP threads; Grid, which the reference "
+                                   f"needs, is not installable here"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_dict(form):
+    return {
+        "workload": "multi-RHS coarse stencil M apply: coarse 8^4, nbasis 32, 32 RHS "
+                    "(coarse operator of 32^4 Wilson-clover on 4^4 blocks)",
+        "coarse_dims": list(DIMS), "nbasis": NBASIS, "nrhs": NRHS, "op": "M",
+        "form": form, "l2": "flushed between timed steps (256 MiB write); links exceed L2",
+        "parallelism": "replicas",
+    }
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- GPU side
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+
+    import gmg
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    A, x = make_inputs()
+    cm = gmg.CoarsenedMatrix(DIMS, NBASIS)
+    cm.set_links(A)
+    cm.prepare(args.form)
+    cm.prepare("f32")
+    xin64 = torch.from_numpy(x).to(dev)
+    xin = xin64.to(torch.complex64).contiguous()
+    out = torch.zeros_like(xin)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    # accuracy of each form against the FP64 GPU path (itself pinned to the oracle)
+    ref64 = torch.zeros_like(xin64)
+    cm.M(xin64, ref64)
+    forms = {}
+    for form in (args.form, "f32"):
+        o = torch.zeros_like(xin)
+        cm.M(xin, o, compute=form)
+        torch.cuda.synchronize()
+        err = (torch.linalg.vector_norm(o.to(torch.complex128) - ref64) / torch.linalg.vector_norm(ref64)).item()
+        forms[form] = {"rel_err_vs_fp64": err}
+
+    def step(compute):
+        cm.M(xin, out, compute=compute)
+
+    for _ in range(args.warmup):
+        step(args.form)
+    torch.cuda.synchronize()
+    if args.kernel_only:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            step(args.form)
+        torch.cuda.synchronize()
+        print(json.dumps({"kernel_only": True, "steps": args.steps, "form": args.form}))
+        return 0
+
+    # timed region: K steps, L2 flushed between steps (outside the per-step events)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local) if rank == 0 else None
+    torch.cuda.synchronize()
+    gmg.lib().gmg_profile_enable(1)
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        step(args.form)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    gmg.lib().gmg_profile_enable(0)
+    clocks = sampler.stop() if sampler else None
+    if dist:
+        dist.barrier()
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    import ctypes
+
+    kms, kn = ctypes.c_double(), ctypes.c_int64()
+    gmg.lib().gmg_profile_read(b"coarse_mrhs_tc", ctypes.byref(kms), ctypes.byref(kn))
+    code = np.zeros(1, dtype=np.int32)
+    st = gmg.lib().gmg_coarse_device_error(cm._h, code.ctypes.data_as(ctypes.c_void_p))
+    if st != 0:
+        raise RuntimeError("tensor-core kernel reported a device error: " + gmg.lib().gmg_last_error().decode())
+    tmax = torch.tensor([t_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    t_ms = float(tmax.item())
+    value = world * FLOPS * args.steps / (t_ms * 1e-3) / 1e12
+
+    # other forms (fewer steps): FP32 CUDA-core and FP64 CUDA-core
+    for form, inp, o in (("f32", xin, torch.zeros_like(xin)), ("f64", xin64, torch.zeros_like(xin64))):
+        n = max(5, min(50, args.steps // 10))
+        for _ in range(3):
+            cm.M(inp, o, compute=form)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        tt = 0.0
+        for _ in range(n):
+            flush.fill_(1.0)
+            e0.record(stream)
+            cm.M(inp, o, compute=form)
+            e1.record(stream)
+            e1.synchronize()
+            tt += e0.elapsed_time(e1)
+        forms.setdefault(form, {})["tflops"] = FLOPS * n / (tt * 1e-3) / 1e12
+    forms[args.form]["tflops"] = FLOPS * args.steps / (t_ms * 1e-3) / 1e12 / 1.0
+    forms["f64"]["rel_err_vs_fp64"] = 0.0
+
+    # end to end through the public API with host buffers (pinned), every step
+    host_in = torch.from_numpy(x.astype(np.complex64)).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    dev_in = torch.empty_like(xin)
+    dev_out = torch.empty_like(xin)
+    ne = max(10, min(200, args.steps // 10))
+    for _ in range(3):
+        dev_in.copy_(host_in, non_blocking=True)
+        cm.M(dev_in, dev_out, compute=args.form)
+        host_out.copy_(dev_out, non_blocking=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(ne):
+        dev_in.copy_(host_in, non_blocking=True)
+        cm.M(dev_in, dev_out, compute=args.form)
+        host_out.copy_(dev_out, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e = world * FLOPS * ne / (float(te.item()) * 1e-3) / 1e12
+
+    hbm, src = peaks()
+    kavg_s = (kms.value / max(kn.value, 1)) * 1e-3
+    achieved = TC_KERNEL_BYTES / kavg_s / 1e9 if kn.value else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.form,
+        "data": "synthetic (seeded Gaussian links with gamma5-hermitian structure, unit-Gaussian RHS)",
+        "config": config_dict(f"{args.form} operands on tcgen05 tensor cores, FP32 accumulation, FP32 vectors"),
+        "roofline": {
+            "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": (achieved / hbm) if achieved else None, "traffic": None,
+            "kernel": "coarse_mrhs_tc_kernel", "algorithmic_bytes_per_launch": TC_KERNEL_BYTES,
+            "kernel_ms_avg": kavg_s * 1e3, "launches": kn.value,
+            "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({src})",
+        },
+        "apply_roofline": {"algorithmic_bytes": APPLY_BYTES,
+                           "achieved_gbs": APPLY_BYTES / (t_ms * 1e-3 / args.steps) / 1e9},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": VEC_BYTES_F32,
+                "d2h_bytes_per_step": VEC_BYTES_F32},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+        "forms": forms,
+    }
+    if rank == 0 and world == 1:
+        cpu, _ = cpu_sample(A, x)
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -72,11 +72,22 @@ def build(force=False, verbose_ptxas=False, jobs=None):
                 failed.append(cmd[-3])
     if failed:
         raise RuntimeError("nvcc failed for: " + ", ".join(failed))
+    relinked = False
     if todo or not os.path.exists(LIB) or force:
         cmd = [cc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcuda"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+        relinked = True
+    # host programs over the C++ surface (include/gmg.hpp), linked against the library
+    for src in sorted(glob.glob(os.path.join(HERE, "host", "*.cpp"))):
+        exe = os.path.join(BUILD, os.path.basename(src)[:-4])
+        if force or relinked or _stale(src, exe, hdr_mtime):
+            cmd = [cc, "-O2", "-std=c++17", "-I", INCLUDE, src, "-o", exe, "-L", HERE, "-lgmg_b200",
+                   "-Xlinker", "-rpath=$ORIGIN/..", "-lcudart"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"host program {src} failed to build:\n" + r.stdout + r.stderr)
     return LIB
 
 

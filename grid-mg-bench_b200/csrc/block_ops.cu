@@ -232,6 +232,7 @@ static gmg_status launch_project(gmg_agg* h, const void* basis, int nrhs, const 
   GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int Vc = (int)h->cdims.vol();
   const int grid = std::min(Vc, num_sms() * 16);
+  KernelTimer kt("project", s);
   kern<<<grid, threads, smem, s>>>(reinterpret_cast<const Cx*>(basis), h->blk_sites.as<int32_t>(),
                                    reinterpret_cast<const Cx*>(fine), reinterpret_cast<Cx*>(coarse),
                                    Vc, N, h->dof, h->bv, nrhs, mask, accumulate);
@@ -348,6 +349,7 @@ static gmg_status launch_promote(gmg_agg* h, const void* basis, int nrhs, const 
   GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int Vc = (int)h->cdims.vol();
   const int grid = std::min(Vc, num_sms() * 16);
+  KernelTimer kt("promote", s);
   kern<<<grid, threads, smem, s>>>(reinterpret_cast<const Cx*>(basis), h->blk_sites.as<int32_t>(),
                                    reinterpret_cast<const Cx*>(coarse), reinterpret_cast<Cx*>(fine),
                                    Vc, N, dof, h->bv, nrhs);
@@ -513,6 +515,7 @@ gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s) {
   const int Vc = (int)h->cdims.vol();
   const int grid = std::min(Vc, num_sms() * 8);
   for (int p = 0; p < passes; ++p) {
+    KernelTimer kt("ortho", s);
     ortho_kernel<<<grid, 256, smem, s>>>(h->basis_blk.as<double2>(), Vc, N, h->dof, h->bv,
                                          h->scratch.as<int>());
     GMG_CUDA(cudaGetLastError());

@@ -191,6 +191,7 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
   uint64_t* drain = tempty + kAccBufs;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  int* nbr_s = reinterpret_cast<int*>(tmem_slot + 4);  // [32][9] neighbour indices of the producer
 
   const uint32_t acc_cols = 2 * P.Rp;
   uint32_t ncols_alloc = 32;
@@ -226,27 +227,45 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
 
   if (warp == 0) {
     // ------------------------------------------------------------ producer
-    if (lane == 0) {
-      int stage = 0;
-      uint32_t phase = 0;
-      int issued = 0;
-      for (int i = 0; i < nsites && !*abort_flag; ++i) {
-        const int site = blockIdx.x + i * gridDim.x;
-        for (int p = P.p0; p < P.p1; ++p) {
-          if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) {
-            atomicCAS(P.err, 0, ERR_TIMEOUT_PRODUCER);
-            *abort_flag = 1;
-            break;
+    // The warp stages the neighbour indices of 32 sites at a time in shared
+    // memory (one parallel load), so lane 0 never waits on a dependent global
+    // load between two stages.
+    int stage = 0;
+    uint32_t phase = 0;
+    int issued = 0;
+    bool stop = false;
+    for (int i0 = 0; i0 < nsites && !stop; i0 += 32) {
+      const int cnt = min(32, nsites - i0);
+      __syncwarp();
+      if (lane < cnt) {
+        const int site = blockIdx.x + (i0 + lane) * gridDim.x;
+#pragma unroll
+        for (int p = 0; p < 9; ++p) nbr_s[lane * 9 + p] = __ldg(&P.nbr[(size_t)p * P.V + site]);
+      }
+      __syncwarp();
+      if (lane == 0) {
+        for (int j = 0; j < cnt && !stop; ++j) {
+          const int site = blockIdx.x + (i0 + j) * gridDim.x;
+          for (int p = P.p0; p < P.p1; ++p) {
+            if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) {
+              atomicCAS(P.err, 0, ERR_TIMEOUT_PRODUCER);
+              *abort_flag = 1;
+              stop = true;
+              break;
+            }
+            unsigned char* st = stage_base + (size_t)stage * stage_bytes;
+            const int nb = nbr_s[j * 9 + p];
+            mbar_expect_tx(&full[stage], stage_bytes);
+            bulk_g2s(st, P.links + ((size_t)site * 9 + p) * (link_bytes / 2), link_bytes, &full[stage]);
+            bulk_g2s(st + link_bytes, P.packed + (size_t)nb * (vec_bytes / 2), vec_bytes, &full[stage]);
+            ++issued;
+            if (++stage == P.stages) { stage = 0; phase ^= 1; }
           }
-          unsigned char* st = stage_base + (size_t)stage * stage_bytes;
-          const int nb = __ldg(&P.nbr[(size_t)p * P.V + site]);
-          mbar_expect_tx(&full[stage], stage_bytes);
-          bulk_g2s(st, P.links + ((size_t)site * 9 + p) * (link_bytes / 2), link_bytes, &full[stage]);
-          bulk_g2s(st + link_bytes, P.packed + (size_t)nb * (vec_bytes / 2), vec_bytes, &full[stage]);
-          ++issued;
-          if (++stage == P.stages) { stage = 0; phase ^= 1; }
         }
       }
+      stop = __shfl_sync(0xffffffffu, stop, 0);
+    }
+    if (lane == 0) {
       // drain: wait for the copies of the last min(issued, stages) stages to land
       int s = stage;
       uint32_t ph = phase;
@@ -387,42 +406,65 @@ __global__ void pack_links_kernel(const double2* __restrict__ A, uint4* __restri
   }
 }
 
-// vectors (FP32 [V][nrhs][N]) -> [V][Kc][2Rp][8] halves, G5C applied on input
+// vectors (FP32 [V][nrhs][N]) -> [V][Kc][2Rp][8] halves, G5C applied on input.
+// One thread per (site, K-chunk, rhs), rhs fastest: it reads the 8 complex
+// values of its chunk (64 contiguous bytes) once and writes the real-part row
+// r and the imaginary-part row Rp + r, so reads and writes are both coalesced.
 __global__ void pack_vec_kernel(const float2* __restrict__ in, uint4* __restrict__ dst, const int32_t* __restrict__ active,
-                                int V, int N, int nrhs, int R, int Rp, int Kc, int kind, int g5) {
-  const int64_t total = (int64_t)V * Kc * 2 * Rp;
+                                int V, int N, int nrhs, int R, int Rp, int Kc, int kind, int g5,
+                                int aligned16) {
+  const int64_t total = (int64_t)V * Kc * Rp;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const int n = (int)(e % (2 * Rp));
-    const int kc = (int)((e / (2 * Rp)) % Kc);
-    const int64_t s = e / ((int64_t)2 * Rp * Kc);
-    const int r = n < Rp ? n : n - Rp;
-    const bool imag = n >= Rp;
-    uint16_t h[8];
+    const int r = (int)(e % Rp);
+    const int kc = (int)((e / Rp) % Kc);
+    const int64_t s = e / ((int64_t)Rp * Kc);
+    uint16_t hr[8], hi[8];
     if (r < R) {
       const int slot = active ? active[r] : r;
-      const float2* src = in + ((int64_t)s * nrhs + slot) * N;
+      const float2* src = in + ((int64_t)s * nrhs + slot) * N + kc * 8;
+      float2 x[8];
+      if (aligned16 && (N & 7) == 0) {
+        // `in` is 16-byte aligned (checked on the host) and N, 8*kc are even
+        const float4* s4 = reinterpret_cast<const float4*>(src);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const float4 v = __ldg(s4 + j);
+          x[2 * j] = make_float2(v.x, v.y);
+          x[2 * j + 1] = make_float2(v.z, v.w);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = (kc * 8 + j < N) ? src[j] : make_float2(0.f, 0.f);
+      }
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int bb = kc * 8 + j;
-        float v = 0.f;
+        float re = 0.f, im = 0.f;
         if (bb < N) {
-          const float2 x = src[bb];
-          v = imag ? x.y : x.x;
-          if (g5 && bb >= N / 2) v = -v;
+          re = x[j].x;
+          im = x[j].y;
+          if (g5 && bb >= N / 2) { re = -re; im = -im; }
         }
-        h[j] = to_half_bits(v, kind);
+        hr[j] = to_half_bits(re, kind);
+        hi[j] = to_half_bits(im, kind);
       }
     } else {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) h[j] = 0;
+      for (int j = 0; j < 8; ++j) hr[j] = hi[j] = 0;
     }
     uint4 o;
-    o.x = h[0] | ((uint32_t)h[1] << 16);
-    o.y = h[2] | ((uint32_t)h[3] << 16);
-    o.z = h[4] | ((uint32_t)h[5] << 16);
-    o.w = h[6] | ((uint32_t)h[7] << 16);
-    dst[e] = o;
+    o.x = hr[0] | ((uint32_t)hr[1] << 16);
+    o.y = hr[2] | ((uint32_t)hr[3] << 16);
+    o.z = hr[4] | ((uint32_t)hr[5] << 16);
+    o.w = hr[6] | ((uint32_t)hr[7] << 16);
+    uint4* row = dst + ((int64_t)s * Kc + kc) * 2 * Rp;
+    row[r] = o;
+    o.x = hi[0] | ((uint32_t)hi[1] << 16);
+    o.y = hi[2] | ((uint32_t)hi[3] << 16);
+    o.z = hi[4] | ((uint32_t)hi[5] << 16);
+    o.w = hi[6] | ((uint32_t)hi[7] << 16);
+    row[Rp + r] = o;
   }
 }
 
@@ -461,18 +503,20 @@ gmg_status coarse_apply_tc(gmg_coarse* h, int p0, int p1, bool g5, int kind, int
   GMG_TRY(h->scratch.alloc(packed_bytes));
   uint4* packed = h->scratch.as<uint4>();
   int* err = h->dev_err.as<int>();
-  const int64_t rows = (int64_t)V * Kc * 2 * Rp;
+  const int64_t rows = (int64_t)V * Kc * Rp;
   tc::pack_vec_kernel<<<(int)std::min<int64_t>((rows + 255) / 256, 148 * 64), 256, 0, s>>>(
-      reinterpret_cast<const float2*>(in), packed, active, V, N, nrhs, R, Rp, Kc, kind, g5 ? 1 : 0);
+      reinterpret_cast<const float2*>(in), packed, active, V, N, nrhs, R, Rp, Kc, kind, g5 ? 1 : 0,
+      (reinterpret_cast<uintptr_t>(in) & 15) == 0 ? 1 : 0);
   GMG_CUDA(cudaGetLastError());
 
   const uint32_t stage_bytes = (uint32_t)Kc * Mp * 16 + (uint32_t)Kc * 2 * Rp * 16;
   const size_t e_bytes = ((size_t)Mp * (2 * Rp + 1) * 4 + 15) / 16 * 16;
-  const size_t fixed = e_bytes + 64 * 8 + 64;
+  const size_t fixed = e_bytes + 64 * 8 + 64 + 32 * 9 * 4;
   const size_t budget = 227 * 1024 - fixed;
   int stages = (int)std::min<size_t>(32, budget / stage_bytes);
   GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil: tile does not fit shared memory");
-  const size_t smem = (size_t)stages * stage_bytes + e_bytes + (size_t)(2 * stages + 2 * tc::kAccBufs + 1) * 8 + 16;
+  const size_t smem = (size_t)stages * stage_bytes + e_bytes + (size_t)(2 * stages + 2 * tc::kAccBufs + 1) * 8 + 16 +
+                      32 * 9 * 4;
   GMG_CUDA(cudaFuncSetAttribute(tc::coarse_mrhs_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
@@ -496,7 +540,10 @@ gmg_status coarse_apply_tc(gmg_coarse* h, int p0, int p1, bool g5, int kind, int
   P.g5 = g5 ? 1 : 0;
   P.stages = stages;
   P.kind = kind == GMG_BF16 ? 1 : 0;
-  tc::coarse_mrhs_tc_kernel<<<std::min(V, nsm), tc::kThreads, smem, s>>>(P);
+  {
+    KernelTimer kt("coarse_mrhs_tc", s);
+    tc::coarse_mrhs_tc_kernel<<<std::min(V, nsm), tc::kThreads, smem, s>>>(P);
+  }
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }

@@ -180,6 +180,7 @@ static gmg_status launch_simt(const void* links, const int32_t* nbr, const void*
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
   const int grid = std::min(V, nsm * std::max(per_sm, 1) * 4);
+  KernelTimer kt("coarse_simt", s);
   kern<<<grid, threads, smem, s>>>(reinterpret_cast<const C*>(links), nbr,
                                    reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), V, N,
                                    nrhs, active, R, p0, p1, g5);

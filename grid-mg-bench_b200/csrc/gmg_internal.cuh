@@ -41,6 +41,19 @@ gmg_status cuda_fail(cudaError_t e, const char* what);
 
 inline cudaStream_t S(gmg_stream s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Live timing of one kernel launch (see prof.cu); a no-op unless enabled.
+class KernelTimer {
+ public:
+  KernelTimer(const char* name, cudaStream_t s);
+  ~KernelTimer();
+
+ private:
+  const char* name_;
+  cudaStream_t s_;
+  cudaEvent_t a_ = nullptr, b_ = nullptr;
+  bool active_ = false;
+};
+
 // ---------------------------------------------------------------------------
 // lattice helpers
 // ---------------------------------------------------------------------------

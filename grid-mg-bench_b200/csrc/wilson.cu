@@ -306,6 +306,7 @@ gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, 
   const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
   const int64_t total = (int64_t)V * nrhs;
   const int grid = (int)std::min<int64_t>((total + 127) / 128, 148 * 32);
+  KernelTimer kt("wilson", s);
   if (vec_prec == GMG_F64) {
     wilson_kernel<double><<<grid, 128, 0, s>>>(h->gauge.as<double2>(), h->clover.as<double2>(),
                                                 h->nbr.as<int32_t>(), (const double2*)in, (double2*)out, V,

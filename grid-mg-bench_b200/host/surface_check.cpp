@@ -1,0 +1,163 @@
+// surface_check.cpp -- exercises the C++ class surface (include/gmg.hpp) the way
+// the reference's drivers use CoarsenedMatrix / Aggregation / linear operators.
+//
+// Restates the MG correctness checks of MultiGridPreconditioner::runChecks
+// (include/MultigridPreconditioner.h:311-446) on the GPU implementation:
+//   (1) 0 == (M - (Mdiag + sum_mu Mdir_mu)) v          fine operator
+//   (2) 0 == (1 - P R) v_i                              basis vectors
+//   (3) 0 == (1 - R P) v_c
+//   (4) 0 == (R D P - D_c) v_c                           Galerkin identity
+//   (5) 0 == Im(v_c^dag D_c^dag D_c v_c)                 Mdag is the adjoint
+// Prints one line per check and exits non-zero if any check fails.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+#include "gmg.hpp"
+
+typedef std::complex<double> cplx;
+
+struct DevField {
+  gmg::Field f;
+  DevField(long sites, int nrhs, int dof) {
+    f.sites = sites;
+    f.nrhs = nrhs;
+    f.dof = dof;
+    f.prec = GMG_F64;
+    cudaMalloc(&f.data, bytes());
+    cudaMemset(f.data, 0, bytes());
+  }
+  ~DevField() { cudaFree(f.data); }
+  size_t bytes() const { return sizeof(cplx) * f.sites * f.nrhs * f.dof; }
+  std::vector<cplx> get() const {
+    std::vector<cplx> h(f.sites * f.nrhs * f.dof);
+    cudaMemcpy(h.data(), f.data, bytes(), cudaMemcpyDeviceToHost);
+    return h;
+  }
+  void set(const std::vector<cplx>& h) { cudaMemcpy(f.data, h.data(), bytes(), cudaMemcpyHostToDevice); }
+};
+
+static std::vector<cplx> gaussian(size_t n, std::mt19937_64& g) {
+  std::normal_distribution<double> d(0.0, std::sqrt(0.5));
+  std::vector<cplx> v(n);
+  for (auto& x : v) x = cplx(d(g), d(g));
+  return v;
+}
+
+static double rel_dev(const std::vector<cplx>& a, const std::vector<cplx>& b) {
+  double num = 0, den = 0;
+  for (size_t i = 0; i < a.size(); ++i) {
+    num += std::norm(a[i] - b[i]);
+    den += std::norm(a[i]);
+  }
+  return std::sqrt(num / den);
+}
+
+static bool report(const char* name, double dev, double tol) {
+  const bool ok = dev < tol;
+  std::printf("%-44s deviation %.3e  (tol %.0e)  %s\n", name, dev, tol, ok ? "passed" : "FAILED");
+  return ok;
+}
+
+int main() {
+  const gmg::Coordinate fdims{8, 8, 8, 8}, cdims{2, 2, 2, 2};
+  const long Vf = 4096, Vc = 16;
+  const int nb = 4, N = 2 * nb;
+  std::mt19937_64 gen(1234);
+
+  // random unitary gauge links (Gram-Schmidt of Gaussian 3x3 matrices)
+  std::vector<cplx> U(Vf * 4 * 9);
+  for (long l = 0; l < Vf * 4; ++l) {
+    auto m = gaussian(9, gen);
+    for (int r = 0; r < 3; ++r) {
+      for (int q = 0; q < r; ++q) {
+        cplx d = 0;
+        for (int c = 0; c < 3; ++c) d += std::conj(m[q * 3 + c]) * m[r * 3 + c];
+        for (int c = 0; c < 3; ++c) m[r * 3 + c] -= d * m[q * 3 + c];
+      }
+      double n = 0;
+      for (int c = 0; c < 3; ++c) n += std::norm(m[r * 3 + c]);
+      for (int c = 0; c < 3; ++c) m[r * 3 + c] /= std::sqrt(n);
+    }
+    for (int k = 0; k < 9; ++k) U[l * 9 + k] = m[k];
+  }
+
+  bool ok = true;
+  try {
+    gmg::WilsonCloverFermion D(fdims, -0.2, 1.0, true);
+    D.ImportGauge(reinterpret_cast<const double*>(U.data()), false);
+    gmg::MdagMLinearOperator<gmg::WilsonCloverFermion> FineOp(D);
+
+    // (1) M = Mdiag + sum Mdir
+    DevField v(Vf, 1, 12), Mv(Vf, 1, 12), t(Vf, 1, 12);
+    v.set(gaussian(Vf * 12, gen));
+    FineOp.Op(v.f, Mv.f);
+    FineOp.OpDiag(v.f, t.f);
+    std::vector<cplx> acc = t.get();
+    for (int dir = 0; dir < 4; ++dir)
+      for (int disp : {+1, -1}) {
+        FineOp.OpDir(v.f, t.f, dir, disp);
+        auto h = t.get();
+        for (size_t i = 0; i < acc.size(); ++i) acc[i] += h[i];
+      }
+    ok &= report("M - (Mdiag + sum Mdir)", rel_dev(Mv.get(), acc), 1e-13);
+
+    // basis: nb Gaussian vectors, chirally doubled (G5C, factor 1/2), block-orthonormalised
+    std::vector<cplx> B(N * Vf * 12);
+    auto h = gaussian(nb * Vf * 12, gen);
+    for (int n = 0; n < nb; ++n)
+      for (long s = 0; s < Vf; ++s)
+        for (int a = 0; a < 12; ++a) {
+          const cplx x = h[(n * Vf + s) * 12 + a];
+          B[(n * Vf + s) * 12 + a] = a < 6 ? x : 0.0;
+          B[((n + nb) * Vf + s) * 12 + a] = a < 6 ? 0.0 : x;
+        }
+    gmg::Aggregation Aggs(cdims, fdims, 12, N);
+    Aggs.SetSubspace(reinterpret_cast<const double*>(B.data()), false);
+    Aggs.Orthogonalise(0, 1);
+    ok &= report("CheckOrthogonal max |B^dag B - 1|", Aggs.CheckOrthogonal(), 1e-13);
+
+    gmg::CoarsenedMatrix Dc(cdims, N, 0);
+    Dc.CoarsenOperator(Aggs, D);
+    gmg::MdagMLinearOperator<gmg::CoarsenedMatrix> CoarseOp(Dc);
+
+    // (2) (1 - P R) v_i for the first basis vector
+    std::vector<cplx> Bo(N * Vf * 12);
+    Aggs.GetSubspace(reinterpret_cast<double*>(Bo.data()), false);
+    DevField vi(Vf, 1, 12), back(Vf, 1, 12);
+    DevField c(Vc, 1, N), c2(Vc, 1, N), c3(Vc, 1, N);
+    vi.set(std::vector<cplx>(Bo.begin(), Bo.begin() + Vf * 12));
+    Aggs.ProjectToSubspace(c.f, vi.f);
+    Aggs.PromoteFromSubspace(c.f, back.f);
+    ok &= report("(1 - P R) v_0", rel_dev(vi.get(), back.get()), 1e-13);
+
+    // (3) (1 - R P) v_c
+    c.set(gaussian(Vc * N, gen));
+    Aggs.PromoteFromSubspace(c.f, back.f);
+    Aggs.ProjectToSubspace(c2.f, back.f);
+    ok &= report("(1 - R P) v_c", rel_dev(c.get(), c2.get()), 1e-13);
+
+    // (4) (R D P - D_c) v_c
+    FineOp.Op(back.f, Mv.f);
+    Aggs.ProjectToSubspace(c2.f, Mv.f);
+    CoarseOp.Op(c.f, c3.f);
+    ok &= report("(R D P - D_c) v_c", rel_dev(c2.get(), c3.get()), 1e-12);
+
+    // (5) Im(v_c^dag D_c^dag D_c v_c) / Re(...)
+    CoarseOp.Op(c.f, c2.f);
+    CoarseOp.AdjOp(c2.f, c3.f);
+    auto a = c.get(), b = c3.get();
+    cplx dot = 0;
+    for (size_t i = 0; i < a.size(); ++i) dot += std::conj(a[i]) * b[i];
+    ok &= report("Im(v^dag Dc^dag Dc v) / Re(...)", std::abs(dot.imag()) / std::abs(dot.real()), 1e-12);
+  } catch (const gmg::Error& e) {
+    std::printf("gmg error %d: %s\n", (int)e.status, e.what());
+    return 2;
+  }
+  std::printf("%s\n", ok ? "all checks passed" : "some checks FAILED");
+  return ok ? 0 : 1;
+}

@@ -188,6 +188,17 @@ gmg_status gmg_coarsen_coarse(gmg_coarse* out, gmg_agg* agg, gmg_coarse* fine, g
 gmg_status gmg_layout_links(int64_t V, int nbasis, int ncs, const double* in, double* out,
                             int inverse, gmg_stream s);
 
+/* ------------------------------------------------------------------------ */
+/* Live kernel timing (replaces the reference's Profiler stopwatches,        */
+/* include/Profiler.h:153-296, with CUDA events on the launching stream)     */
+/* ------------------------------------------------------------------------ */
+/* Enable / disable event recording around the hot kernels. */
+gmg_status gmg_profile_enable(int on);
+/* Summed device time and launch count of one kernel since the last read, then
+   reset.  Names: "coarse_mrhs_tc", "coarse_simt", "wilson", "project",
+   "promote", "ortho".  Synchronises the recorded events. */
+gmg_status gmg_profile_read(const char* kernel, double* total_ms, int64_t* launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -161,8 +161,20 @@ extern "C" void orc_coarse_g5(int64_t V, int N, int R, double* v) {
       for (int b = N / 2; b < N; ++b) z[(s * R + r) * N + b] = -z[(s * R + r) * N + b];
 }
 
+extern "C" void orc_coarse_apply_range(const int* dims, int N, int R, const double* links,
+                                       const double* in, double* out, int op, int point, int hermitian,
+                                       int64_t s0, int64_t s1);
+
 extern "C" void orc_coarse_apply(const int* dims, int N, int R, const double* links,
                                  const double* in, double* out, int op, int point, int hermitian) {
+  orc_coarse_apply_range(dims, N, R, links, in, out, op, point, hermitian, 0, volume(dims));
+}
+
+// Same as orc_coarse_apply restricted to output sites [s0, s1) (bounded CPU
+// timing samples); other output sites are left untouched.
+extern "C" void orc_coarse_apply_range(const int* dims, int N, int R, const double* links,
+                                       const double* in, double* out, int op, int point, int hermitian,
+                                       int64_t s0, int64_t s1) {
   const int64_t V = volume(dims);
   const cplx* A = C(links);
   const cplx* x = C(in);
@@ -179,8 +191,8 @@ extern "C" void orc_coarse_apply(const int* dims, int N, int R, const double* li
   int p0 = 0, p1 = NPOINT;
   if (op == 2) { p0 = 8; p1 = 9; }
   if (op == 3) { p0 = point; p1 = point + 1; }
-#pragma omp parallel for
-  for (int64_t s = 0; s < V; ++s) {
+#pragma omp parallel for schedule(static)
+  for (int64_t s = s0; s < s1; ++s) {
     for (int r = 0; r < R; ++r) {
       for (int b = 0; b < N; ++b) {
         cplx res = 0.0;
@@ -193,7 +205,12 @@ extern "C" void orc_coarse_apply(const int* dims, int N, int R, const double* li
       }
     }
   }
-  if (g5) orc_coarse_g5(V, N, R, out);  // G5C(out, out)
+  if (g5) {  // G5C(out, out) on the computed sites
+    cplx* z = C(out);
+    for (int64_t s = s0; s < s1; ++s)
+      for (int r = 0; r < R; ++r)
+        for (int b = N / 2; b < N; ++b) z[(s * R + r) * N + b] = -z[(s * R + r) * N + b];
+  }
 }
 
 // ----------------------------------------------------------------------------

@@ -50,6 +50,9 @@ void orc_block_parity_mask(const int* fdims, const int* cdims, int parity, int8_
 /* coarse stencil (CoarsenedMatrixUpstream.h:546-742) */
 void orc_coarse_apply(const int* dims, int N, int R, const double* links,
                       const double* in, double* out, int op, int point, int hermitian);
+void orc_coarse_apply_range(const int* dims, int N, int R, const double* links,
+                            const double* in, double* out, int op, int point, int hermitian,
+                            int64_t s0, int64_t s1);
 void orc_coarse_g5(int64_t V, int N, int R, double* v);
 
 /* block projection / promotion / orthonormalisation

@@ -102,6 +102,14 @@ def coarse_apply(dims, links, x, op=OP_M, point=8, hermitian=0):
     return y
 
 
+def coarse_apply_range(dims, links, x, y, s0, s1, op=OP_M, point=8, hermitian=0):
+    """In-place y[s0:s1] = op(x) on output sites [s0, s1) (bounded timing samples)."""
+    V, R, N = x.shape
+    lib().orc_coarse_apply_range(_i4(dims), N, R, _p(links), _p(x), _p(y), op, point, hermitian,
+                                 ctypes.c_int64(s0), ctypes.c_int64(s1))
+    return y
+
+
 def block_project(fdims, cdims, basis, fine, mask=None):
     """basis [N][Vf][dof], fine [Vf][R][dof] -> coarse [Vc][R][N]."""
     basis = _c(basis)
