@@ -549,3 +549,140 @@ gmg_status coarse_apply_tc(gmg_coarse* h, int p0, int p1, bool g5, int kind, int
 }
 
 }  // namespace gmg
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the tensor-core multi-RHS apply.
+//
+// gmg_coarse_apply packs the right-hand sides into a per-handle device buffer
+// that it grows with cudaMalloc on demand.  Some callers cannot let a library
+// allocate at that point: a solver loop that must not stall the device (the
+// CUDA runtime may synchronise inside cudaMalloc / cudaFree), or an
+// application whose device memory is handed out entirely by its own pool
+// allocator.  gmg_coarse_apply_noalloc runs the same two kernels (pack, then
+// the tcgen05 stencil) with the packed right-hand sides in the fixed array
+// below instead, so it calls no cudaMalloc, cudaFree or other allocating
+// routine.
+//
+// The array is kNoAllocScratchBytes (16 MiB) of global memory on every GPU
+// that loads this library, held until the process exits.  That is exactly
+// the packed size of the 8^4 lattice / nbasis 32 / 32 RHS workload.  Larger
+// requests are rejected with GMG_ERR_UNSUPPORTED.  Every call shares the
+// array: the pack kernel rewrites every byte the stencil kernel reads (zero
+// padding included), so no clearing is needed between calls.  Calls that
+// overlap on the GPU (different streams, or different host threads) race on
+// the array and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace gmg {
+namespace tc {
+
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Device address of g_noalloc_scratch on the current device.  In host code the
+// symbol itself is only a host-side stand-in, so its device address is looked
+// up once per device (with that device current) and cached.
+static gmg_status noalloc_scratch(void** p) {
+  int dev = 0;
+  GMG_CUDA(cudaGetDevice(&dev));
+  GMG_CHECK(dev >= 0 && dev < kMaxDevices, GMG_ERR_UNSUPPORTED, "gmg_coarse_apply_noalloc: device index too large");
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || ptr == nullptr) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_ptr[dev] = ptr;
+  }
+  *p = g_noalloc_ptr[dev];
+  return GMG_OK;
+}
+
+}  // namespace tc
+}  // namespace gmg
+
+extern "C" gmg_status gmg_coarse_apply_noalloc(gmg_coarse* h, gmg_op op, int point, gmg_prec compute, int nrhs,
+                                               const float* in, float* out, const int32_t* active, int n_active,
+                                               gmg_stream stream) {
+  using namespace gmg;
+  GMG_CHECK(h != nullptr, GMG_ERR_ARGUMENT, "gmg_coarse_apply_noalloc: null handle");
+  GMG_CHECK(in && out && in != out, GMG_ERR_ARGUMENT, "gmg_coarse_apply_noalloc: null or aliased vectors");
+  GMG_CHECK(h->links_set, GMG_ERR_STATE, "gmg_coarse_apply_noalloc: links not set");
+  GMG_CHECK(compute == GMG_BF16 || compute == GMG_F16, GMG_ERR_UNSUPPORTED,
+            "gmg_coarse_apply_noalloc: only the BF16 / F16 tensor-core forms have an allocation-free variant");
+  GMG_CHECK(h->links_h.kind == compute, GMG_ERR_STATE,
+            "gmg_coarse_apply_noalloc: call gmg_coarse_prepare for this precision first (it allocates)");
+  GMG_CHECK(nrhs >= 1 && nrhs <= 1024, GMG_ERR_ARGUMENT, "gmg_coarse_apply_noalloc: nrhs out of range");
+  if (active) GMG_CHECK(n_active >= 0 && n_active <= nrhs, GMG_ERR_ARGUMENT, "gmg_coarse_apply_noalloc: bad n_active");
+  int p0 = 0, p1 = 9;
+  bool g5 = false;
+  switch (op) {
+    case GMG_OP_M: break;
+    case GMG_OP_MDAG: g5 = !h->hermitian; break;
+    case GMG_OP_MDIAG: p0 = 8; p1 = 9; break;
+    case GMG_OP_MDIR:
+      GMG_CHECK(point >= 0 && point < 9, GMG_ERR_ARGUMENT, "gmg_coarse_apply_noalloc: point out of range");
+      p0 = point; p1 = point + 1;
+      break;
+    default: return fail(GMG_ERR_ARGUMENT, "gmg_coarse_apply_noalloc: bad op");
+  }
+  const int N = h->N;
+  const int R = active ? n_active : nrhs;
+  if (R == 0) return GMG_OK;
+  GMG_CHECK(R <= 128, GMG_ERR_UNSUPPORTED, "gmg_coarse_apply_noalloc: at most 128 active RHS");
+  const int Rp = tc::round_up(R, 16);
+  const int Kc = tc::round_up(N, 16) / 8;
+  const int Mp = 2 * N <= 64 ? 64 : 128;
+  const int V = (int)h->dims.vol();
+  const size_t packed_bytes = (size_t)V * Kc * 2 * Rp * 16;
+  if (packed_bytes > tc::kNoAllocScratchBytes)
+    return fail(GMG_ERR_UNSUPPORTED,
+                "gmg_coarse_apply_noalloc: packed right-hand sides need " + std::to_string(packed_bytes) +
+                    " bytes, more than the 16 MiB static scratch; use gmg_coarse_apply");
+  void* scratch = nullptr;
+  GMG_TRY(tc::noalloc_scratch(&scratch));
+  cudaStream_t s = S(stream);
+  uint4* packed = reinterpret_cast<uint4*>(scratch);
+  const int64_t rows = (int64_t)V * Kc * Rp;
+  tc::pack_vec_kernel<<<(int)std::min<int64_t>((rows + 255) / 256, 148 * 64), 256, 0, s>>>(
+      reinterpret_cast<const float2*>(in), packed, active, V, N, nrhs, R, Rp, Kc, compute, g5 ? 1 : 0,
+      (reinterpret_cast<uintptr_t>(in) & 15) == 0 ? 1 : 0);
+  GMG_CUDA(cudaGetLastError());
+  const uint32_t stage_bytes = (uint32_t)Kc * Mp * 16 + (uint32_t)Kc * 2 * Rp * 16;
+  const size_t e_bytes = ((size_t)Mp * (2 * Rp + 1) * 4 + 15) / 16 * 16;
+  const size_t fixed = e_bytes + 64 * 8 + 64 + 32 * 9 * 4;
+  const int stages = (int)std::min<size_t>(32, (227 * 1024 - fixed) / stage_bytes);
+  GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "gmg_coarse_apply_noalloc: tile does not fit shared memory");
+  const size_t smem = (size_t)stages * stage_bytes + e_bytes + (size_t)(2 * stages + 2 * tc::kAccBufs + 1) * 8 + 16 +
+                      32 * 9 * 4;
+  GMG_CUDA(cudaFuncSetAttribute(tc::coarse_mrhs_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, nsm = 148;
+  GMG_CUDA(cudaGetDevice(&dev));
+  GMG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  tc::Params P;
+  P.links = h->links_h.buf.as<uint16_t>();
+  P.packed = reinterpret_cast<const uint16_t*>(packed);
+  P.nbr = h->nbr.as<int32_t>();
+  P.active = active;
+  P.out = reinterpret_cast<float2*>(out);
+  P.err = h->dev_err.as<int>();
+  P.V = V;
+  P.N = N;
+  P.nrhs = nrhs;
+  P.R = R;
+  P.Rp = Rp;
+  P.Kc = Kc;
+  P.Mp = Mp;
+  P.p0 = p0;
+  P.p1 = p1;
+  P.g5 = g5 ? 1 : 0;
+  P.stages = stages;
+  P.kind = compute == GMG_BF16 ? 1 : 0;
+  tc::coarse_mrhs_tc_kernel<<<std::min(V, nsm), tc::kThreads, smem, s>>>(P);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}

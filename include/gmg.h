@@ -96,6 +96,23 @@ gmg_status gmg_coarse_apply(gmg_coarse* h, gmg_op op, int point, gmg_prec comput
                             gmg_prec vec_prec, int nrhs, const void* in, void* out,
                             const int32_t* active, int n_active, gmg_stream s);
 
+/* Allocation-free form of gmg_coarse_apply for the BF16 / F16 tensor-core
+   path (no counterpart in the reference).  For callers that cannot let the
+   library allocate while they run -- a solver loop that must not stall the
+   device (cudaMalloc / cudaFree may synchronise) or an application whose
+   device memory all comes from its own pool allocator.  The packed
+   right-hand sides go to a fixed 16 MiB array of device memory that every
+   GPU loading the library holds until exit; requests needing more (V * Kc *
+   2 * ceil16(R) * 16 bytes, Kc = ceil16(nbasis)/8) return
+   GMG_ERR_UNSUPPORTED.  Vectors are FP32 [V][nrhs][N]; gmg_coarse_prepare
+   (which allocates) must have run for `compute` first.  The first call on a
+   device looks up the array's device address (cudaGetSymbolAddress); make
+   that first call before any stream capture.  All calls share the array:
+   calls that overlap on the GPU race and must be serialised by the caller. */
+gmg_status gmg_coarse_apply_noalloc(gmg_coarse* h, gmg_op op, int point, gmg_prec compute, int nrhs,
+                                    const float* in, float* out, const int32_t* active, int n_active,
+                                    gmg_stream s);
+
 /* MdirAll (CoarsenedMatrixUpstream.h:700-713): out8[p] = A_p in(nbr_p), p < 8. */
 gmg_status gmg_coarse_mdir_all(gmg_coarse* h, gmg_prec compute, gmg_prec vec_prec, int nrhs,
                                const void* in, void* const* out8, gmg_stream s);
