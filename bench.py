@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--form", choices=["bf16", "f16"], default="bf16")
+    ap.add_argument("--suite", action="store_true",
+                    help="per-row measurements (C1, C3, C4, fine operator) instead of the bench line")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed applies (for profiler captures); prints a short line")
     return ap.parse_args()
@@ -202,6 +204,11 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.suite:
+        import suite
+
+        suite.run()
+        return 0
 
     import torch
 

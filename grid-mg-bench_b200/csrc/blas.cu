@@ -1,0 +1,287 @@
+// blas.cu -- per-RHS vector kernels for the multigrid solvers.
+//
+// Fields are [site][rhs][dof] complex (FP64 or FP32).  Every operation acts on
+// each right-hand side separately (per-RHS scalars live on the device), which
+// is what the reference's solvers do one field at a time (Grid's innerProduct,
+// norm2, axpy used by its GMRES / FGMRES / MR, selected at include/Helpers.h:314-341).
+// Reductions accumulate in FP64 whatever the field precision.
+#include <algorithm>
+
+#include "mg_internal.cuh"
+
+namespace gmg {
+namespace blas {
+
+template <class T> struct C2;
+template <> struct C2<double> { typedef double2 t; };
+template <> struct C2<float> { typedef float2 t; };
+
+static int grid1(int64_t n) { return (int)std::min<int64_t>(std::max<int64_t>((n + 255) / 256, 1), 148 * 16); }
+
+// out[(j0+j)*R + r] += sum_s <X_{j0+j}(s, r), Y(s, r)> for j < min(JB, nx - j0)
+// (X_j = X + j*xstride).  Grid (gx, R): blockIdx.y is the RHS, threads walk the
+// sites, then a warp-shuffle + shared-memory reduction and one FP64 atomic per
+// (block, j).  Converged RHS (mask[r] == 0) are skipped.
+template <class T, int JB>
+__global__ void __launch_bounds__(256) multidot_kernel(const typename C2<T>::t* __restrict__ X, int64_t xstride,
+                                                       int j0, int nx, const typename C2<T>::t* __restrict__ Y,
+                                                       int64_t V, int R, int dof, double2* __restrict__ out,
+                                                       const int* __restrict__ mask) {
+  const int r = blockIdx.y;
+  if (mask && !mask[r]) return;
+  const int nj = min(JB, nx - j0);
+  double ar[JB], ai[JB];
+#pragma unroll
+  for (int j = 0; j < JB; ++j) ar[j] = ai[j] = 0.0;
+  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < V; s += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = (s * R + r) * dof;
+    for (int a = 0; a < dof; ++a) {
+      const double yr = Y[e + a].x, yi = Y[e + a].y;
+#pragma unroll
+      for (int j = 0; j < JB; ++j) {
+        if (j < nj) {
+          const typename C2<T>::t x = X[(int64_t)(j0 + j) * xstride + e + a];
+          ar[j] += (double)x.x * yr + (double)x.y * yi;
+          ai[j] += (double)x.x * yi - (double)x.y * yr;
+        }
+      }
+    }
+  }
+  __shared__ double sr[JB][8], si[JB][8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < JB; ++j) {
+    double vr = ar[j], vi = ai[j];
+    for (int o = 16; o > 0; o >>= 1) {
+      vr += __shfl_xor_sync(0xffffffffu, vr, o);
+      vi += __shfl_xor_sync(0xffffffffu, vi, o);
+    }
+    if (lane == 0) { sr[j][w] = vr; si[j][w] = vi; }
+  }
+  __syncthreads();
+  if (threadIdx.x < nj) {
+    double vr = 0, vi = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { vr += sr[threadIdx.x][k]; vi += si[threadIdx.x][k]; }
+    atomicAdd(&out[(j0 + threadIdx.x) * R + r].x, vr);
+    atomicAdd(&out[(j0 + threadIdx.x) * R + r].y, vi);
+  }
+}
+
+// Y(s, r) += sum_j a[j*R + r] X_j(s, r)   (a complex, FP64; X and Y may differ in precision)
+template <class TX, class T>
+__global__ void multiaxpy_kernel(const double2* __restrict__ a, const typename C2<TX>::t* __restrict__ X,
+                                 int64_t xstride, int nx, typename C2<T>::t* __restrict__ Y, int64_t V, int R,
+                                 int dof) {
+  const int64_t n = V * R * dof;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)((e / dof) % R);
+    double yr = Y[e].x, yi = Y[e].y;
+    for (int j = 0; j < nx; ++j) {
+      const double2 c = a[j * R + r];
+      if (c.x == 0.0 && c.y == 0.0) continue;
+      const typename C2<TX>::t x = X[j * xstride + e];
+      yr += c.x * x.x - c.y * x.y;
+      yi += c.x * x.y + c.y * x.x;
+    }
+    Y[e].x = (T)yr;
+    Y[e].y = (T)yi;
+  }
+}
+
+// Y(s, r) = a[r] * X(s, r) + b[r] * Y(s, r)
+template <class T>
+__global__ void axpby_kernel(const double2* __restrict__ a, const typename C2<T>::t* __restrict__ X,
+                             const double2* __restrict__ b, typename C2<T>::t* __restrict__ Y, int64_t V, int R,
+                             int dof) {
+  const int64_t n = V * R * dof;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)((e / dof) % R);
+    const double2 ca = a[r], cb = b[r];
+    const typename C2<T>::t x = X[e], y = Y[e];
+    const double re = ca.x * x.x - ca.y * x.y + cb.x * y.x - cb.y * y.y;
+    const double im = ca.x * x.y + ca.y * x.x + cb.x * y.y + cb.y * y.x;
+    Y[e].x = (T)re;
+    Y[e].y = (T)im;
+  }
+}
+
+template <class Ti, class To>
+__global__ void convert_kernel(const typename C2<Ti>::t* __restrict__ X, typename C2<To>::t* __restrict__ Y, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    Y[e].x = (To)X[e].x;
+    Y[e].y = (To)X[e].y;
+  }
+}
+
+// Chirally doubled basis from a batch of nb vectors X [V][nb][dof]:
+// B[n] = X_n on the upper half of dof, B[n + nb] = X_n on the lower half
+// (performChiralDoublingG5C, include/Benchmark_helpers.h:156-181, up to the
+// factor 1/2 that the following orthonormalisation removes).
+template <class T>
+__global__ void chiral_double_kernel(const typename C2<T>::t* __restrict__ X, double2* __restrict__ B, int64_t V,
+                                     int nb, int dof) {
+  const int64_t n = V * nb * dof;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int a = (int)(e % dof);
+    const int k = (int)((e / dof) % nb);
+    const int64_t s = e / ((int64_t)dof * nb);
+    const double2 v = make_double2(X[e].x, X[e].y);
+    const double2 z = make_double2(0, 0);
+    const bool upper = a < dof / 2;
+    B[((int64_t)k * V + s) * dof + a] = upper ? v : z;
+    B[((int64_t)(k + nb) * V + s) * dof + a] = upper ? z : v;
+  }
+}
+
+}  // namespace blas
+
+// ---------------------------------------------------------------- host wrappers
+gmg_status vec_multidot(const Vec& X0, int nx, int64_t xstride_elems, const Vec& Y, double2* out_dev, const int* mask,
+                        cudaStream_t s) {
+  GMG_CUDA(cudaMemsetAsync(out_dev, 0, sizeof(double2) * nx * Y.R, s));
+  constexpr int JB = 4;
+  const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((Y.V + 255) / 256, (148 * 8 + Y.R - 1) / Y.R));
+  const dim3 grid(gx, Y.R);
+  for (int j0 = 0; j0 < nx; j0 += JB) {
+    if (Y.prec == GMG_F64)
+      blas::multidot_kernel<double, JB><<<grid, 256, 0, s>>>((const double2*)X0.p, xstride_elems, j0, nx,
+                                                             (const double2*)Y.p, Y.V, Y.R, Y.dof, out_dev, mask);
+    else
+      blas::multidot_kernel<float, JB><<<grid, 256, 0, s>>>((const float2*)X0.p, xstride_elems, j0, nx,
+                                                            (const float2*)Y.p, Y.V, Y.R, Y.dof, out_dev, mask);
+    GMG_CUDA(cudaGetLastError());
+  }
+  return GMG_OK;
+}
+
+gmg_status vec_multiaxpy(const double2* a_dev, const Vec& X0, int nx, int64_t xstride_elems, Vec& Y, cudaStream_t s) {
+  const int g = blas::grid1(Y.elems());
+  if (Y.prec == GMG_F64 && X0.prec == GMG_F64)
+    blas::multiaxpy_kernel<double, double><<<g, 256, 0, s>>>(a_dev, (const double2*)X0.p, xstride_elems, nx,
+                                                             (double2*)Y.p, Y.V, Y.R, Y.dof);
+  else if (Y.prec == GMG_F64)
+    blas::multiaxpy_kernel<float, double><<<g, 256, 0, s>>>(a_dev, (const float2*)X0.p, xstride_elems, nx,
+                                                            (double2*)Y.p, Y.V, Y.R, Y.dof);
+  else if (X0.prec == GMG_F32)
+    blas::multiaxpy_kernel<float, float><<<g, 256, 0, s>>>(a_dev, (const float2*)X0.p, xstride_elems, nx,
+                                                           (float2*)Y.p, Y.V, Y.R, Y.dof);
+  else
+    blas::multiaxpy_kernel<double, float><<<g, 256, 0, s>>>(a_dev, (const double2*)X0.p, xstride_elems, nx,
+                                                            (float2*)Y.p, Y.V, Y.R, Y.dof);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status vec_axpby(const double2* a_dev, const Vec& X, const double2* b_dev, Vec& Y, cudaStream_t s) {
+  const int g = blas::grid1(Y.elems());
+  if (Y.prec == GMG_F64)
+    blas::axpby_kernel<double><<<g, 256, 0, s>>>(a_dev, (const double2*)X.p, b_dev, (double2*)Y.p, Y.V, Y.R, Y.dof);
+  else
+    blas::axpby_kernel<float><<<g, 256, 0, s>>>(a_dev, (const float2*)X.p, b_dev, (float2*)Y.p, Y.V, Y.R, Y.dof);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status vec_convert(const Vec& X, Vec& Y, cudaStream_t s) {
+  GMG_CHECK(X.elems() == Y.elems(), GMG_ERR_SHAPE, "convert: size mismatch");
+  const int64_t n = X.elems();
+  const int g = blas::grid1(n);
+  if (X.prec == Y.prec) {
+    GMG_CUDA(cudaMemcpyAsync(Y.p, X.p, X.bytes(), cudaMemcpyDeviceToDevice, s));
+    return GMG_OK;
+  }
+  if (X.prec == GMG_F64)
+    blas::convert_kernel<double, float><<<g, 256, 0, s>>>((const double2*)X.p, (float2*)Y.p, n);
+  else
+    blas::convert_kernel<float, double><<<g, 256, 0, s>>>((const float2*)X.p, (double2*)Y.p, n);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+namespace blas {
+
+// dst[s][r'][a] = src[s][idx[r']][a]  (SCATTER: dst[s][idx[r']][a] = src[s][r'][a])
+template <class T, bool SCATTER>
+__global__ void permute_kernel(const typename C2<T>::t* __restrict__ src, typename C2<T>::t* __restrict__ dst,
+                               const int* __restrict__ idx, int64_t V, int Rs, int Rd, int Rc, int dof) {
+  const int64_t n = V * Rc * dof;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int a = (int)(e % dof);
+    const int rc = (int)((e / dof) % Rc);
+    const int64_t s = e / ((int64_t)dof * Rc);
+    if (SCATTER) dst[(s * Rd + idx[rc]) * dof + a] = src[(s * Rs + rc) * dof + a];
+    else dst[(s * Rd + rc) * dof + a] = src[(s * Rs + idx[rc]) * dof + a];
+  }
+}
+
+// counter-based Gaussian: splitmix64 of (seed, element) -> Box-Muller
+__device__ __forceinline__ uint64_t splitmix(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+template <class T>
+__global__ void gaussian_kernel(typename C2<T>::t* __restrict__ X, int64_t n, uint64_t seed) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t h = splitmix(seed ^ splitmix((uint64_t)e));
+    const double u1 = ((h >> 11) + 1.0) * (1.0 / 9007199254740993.0);  // (0, 1]
+    const double u2 = (double)(splitmix(h) >> 11) * (1.0 / 9007199254740992.0);
+    const double rad = sqrt(-log(u1));  // sqrt(-2 ln u1) * sqrt(1/2)
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    X[e].x = (T)(rad * cs);
+    X[e].y = (T)(rad * sn);
+  }
+}
+
+}  // namespace blas
+
+gmg_status vec_gather(const Vec& src, const int* idx, Vec& dst, cudaStream_t s) {
+  const int64_t n = dst.elems();
+  const int g = blas::grid1(n);
+  if (src.prec == GMG_F64)
+    blas::permute_kernel<double, false><<<g, 256, 0, s>>>((const double2*)src.p, (double2*)dst.p, idx, dst.V, src.R,
+                                                          dst.R, dst.R, dst.dof);
+  else
+    blas::permute_kernel<float, false><<<g, 256, 0, s>>>((const float2*)src.p, (float2*)dst.p, idx, dst.V, src.R,
+                                                         dst.R, dst.R, dst.dof);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status vec_scatter(const Vec& src, const int* idx, Vec& dst, cudaStream_t s) {
+  const int64_t n = src.elems();
+  const int g = blas::grid1(n);
+  if (src.prec == GMG_F64)
+    blas::permute_kernel<double, true><<<g, 256, 0, s>>>((const double2*)src.p, (double2*)dst.p, idx, src.V, src.R,
+                                                         dst.R, src.R, src.dof);
+  else
+    blas::permute_kernel<float, true><<<g, 256, 0, s>>>((const float2*)src.p, (float2*)dst.p, idx, src.V, src.R,
+                                                        dst.R, src.R, src.dof);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status vec_gaussian(Vec& X, uint64_t seed, cudaStream_t s) {
+  const int64_t n = X.elems();
+  const int g = blas::grid1(n);
+  if (X.prec == GMG_F64) blas::gaussian_kernel<double><<<g, 256, 0, s>>>((double2*)X.p, n, seed);
+  else blas::gaussian_kernel<float><<<g, 256, 0, s>>>((float2*)X.p, n, seed);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status vec_chiral_double(const Vec& X, double* basis_dev, cudaStream_t s) {
+  const int64_t n = X.elems();
+  const int g = blas::grid1(n);
+  if (X.prec == GMG_F64)
+    blas::chiral_double_kernel<double><<<g, 256, 0, s>>>((const double2*)X.p, (double2*)basis_dev, X.V, X.R, X.dof);
+  else
+    blas::chiral_double_kernel<float><<<g, 256, 0, s>>>((const float2*)X.p, (double2*)basis_dev, X.V, X.R, X.dof);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+}  // namespace gmg

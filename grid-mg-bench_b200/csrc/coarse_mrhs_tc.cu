@@ -162,6 +162,20 @@ __device__ __forceinline__ bool named_bar_or(int id, int nthreads, bool pred) {
   return r != 0;
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+        "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 struct Params {
   const uint16_t* links;   // [V][9][Kc][Mp][8]
   const uint16_t* packed;  // [V][Kc][2Rp][8]
@@ -169,21 +183,23 @@ struct Params {
   const int32_t* active;   // nullable
   float2* out;             // [V][nrhs][N]
   int* err;                // device error word
-  int V, N, nrhs, R, Rp, Kc, Mp, p0, p1, g5, stages, kind;
+  int V, N, nrhs, R, Rp, Kc, Mp, p0, p1, g5, stages, kind, pps;
 };
 
+// Shared memory: `stages` stages of pps link tiles followed by pps neighbour
+// tiles, then the mbarriers, the TMEM address, the abort flag and the
+// producer's neighbour-index table.
 __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Params P) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t link_bytes = (uint32_t)P.Kc * P.Mp * 16;
-  const uint32_t vec_bytes = (uint32_t)P.Kc * 2 * P.Rp * 16;
-  const uint32_t stage_bytes = link_bytes + vec_bytes;
-  const int ncolE = 2 * P.Rp + 1;  // padded row of the epilogue staging buffer
+  const uint32_t link_bytes = (uint32_t)P.Kc * P.Mp * 16;     // one stencil point of one site
+  const uint32_t vec_bytes = (uint32_t)P.Kc * 2 * P.Rp * 16;  // one neighbour tile
+  const int pps = P.pps;                                      // stencil points per stage
+  const uint32_t stage_bytes = (uint32_t)pps * (link_bytes + vec_bytes);
+  const int ngroups = (P.p1 - P.p0) / pps;                    // pps divides the point count
 
   unsigned char* stage_base = smem;
-  float* E = reinterpret_cast<float*>(smem + (size_t)P.stages * stage_bytes);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(E) +
-                                               (((size_t)P.Mp * ncolE * 4 + 15) / 16) * 16);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)P.stages * stage_bytes);
   uint64_t* full = bars;
   uint64_t* empty = full + P.stages;
   uint64_t* tfull = empty + P.stages;
@@ -223,13 +239,14 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
 
   // sites of this CTA: blockIdx.x, blockIdx.x + gridDim.x, ...
   const int nsites = (P.V - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
-  const int npts = P.p1 - P.p0;
 
   if (warp == 0) {
     // ------------------------------------------------------------ producer
     // The warp stages the neighbour indices of 32 sites at a time in shared
     // memory (one parallel load), so lane 0 never waits on a dependent global
-    // load between two stages.
+    // load between two stages.  One stage = pps consecutive stencil points of
+    // one site: one bulk copy of their (contiguous) link tiles and one per
+    // neighbour tile.
     int stage = 0;
     uint32_t phase = 0;
     int issued = 0;
@@ -246,7 +263,7 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
       if (lane == 0) {
         for (int j = 0; j < cnt && !stop; ++j) {
           const int site = blockIdx.x + (i0 + j) * gridDim.x;
-          for (int p = P.p0; p < P.p1; ++p) {
+          for (int g = 0; g < ngroups; ++g) {
             if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) {
               atomicCAS(P.err, 0, ERR_TIMEOUT_PRODUCER);
               *abort_flag = 1;
@@ -254,10 +271,14 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
               break;
             }
             unsigned char* st = stage_base + (size_t)stage * stage_bytes;
-            const int nb = nbr_s[j * 9 + p];
+            const int pf = P.p0 + g * pps;
             mbar_expect_tx(&full[stage], stage_bytes);
-            bulk_g2s(st, P.links + ((size_t)site * 9 + p) * (link_bytes / 2), link_bytes, &full[stage]);
-            bulk_g2s(st + link_bytes, P.packed + (size_t)nb * (vec_bytes / 2), vec_bytes, &full[stage]);
+            bulk_g2s(st, P.links + ((size_t)site * 9 + pf) * (link_bytes / 2), pps * link_bytes, &full[stage]);
+            for (int pp = 0; pp < pps; ++pp) {
+              const int nb = nbr_s[j * 9 + pf + pp];
+              bulk_g2s(st + pps * link_bytes + pp * vec_bytes, P.packed + (size_t)nb * (vec_bytes / 2), vec_bytes,
+                       &full[stage]);
+            }
             ++issued;
             if (++stage == P.stages) { stage = 0; phase ^= 1; }
           }
@@ -277,33 +298,34 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = (1u << 4)                         // D format F32
-                             | ((uint32_t)P.kind << 7)         // A format (0 F16, 1 BF16)
-                             | ((uint32_t)P.kind << 10)        // B format
+      const uint32_t idesc = (1u << 4)                            // D format F32
+                             | ((uint32_t)P.kind << 7)            // A format (0 F16, 1 BF16)
+                             | ((uint32_t)P.kind << 10)           // B format
                              | ((uint32_t)(2 * P.Rp) >> 3) << 17  // N
-                             | ((uint32_t)P.Mp >> 4) << 24;      // M
+                             | ((uint32_t)P.Mp >> 4) << 24;       // M
       int stage = 0;
       uint32_t phase = 0;
       bool ok = true;
-      int committed = 0;
       for (int i = 0; i < nsites && ok; ++i) {
         const int acc = i & 1;
         const uint32_t aphase = (uint32_t)(i >> 1) & 1;
         if (!mbar_wait(&tempty[acc], aphase ^ 1, abort_flag)) { ok = false; break; }
         fence_after();
         const uint32_t dt = tmem_base + acc * acc_cols;
-        for (int p = 0; p < npts; ++p) {
+        for (int g = 0; g < ngroups; ++g) {
           if (!mbar_wait(&full[stage], phase, abort_flag)) { ok = false; break; }
           fence_after();
           unsigned char* st = stage_base + (size_t)stage * stage_bytes;
-          for (int ks = 0; ks < P.Kc / 2; ++ks) {
-            const uint64_t ad = make_desc(st + (size_t)(2 * ks) * P.Mp * 16, (uint32_t)P.Mp * 16, 128);
-            const uint64_t bd =
-                make_desc(st + link_bytes + (size_t)(2 * ks) * 2 * P.Rp * 16, (uint32_t)(2 * P.Rp) * 16, 128);
-            mma_f16(dt, ad, bd, idesc, (p > 0 || ks > 0) ? 1u : 0u);
+          for (int pp = 0; pp < pps; ++pp) {
+            unsigned char* lt = st + pp * link_bytes;
+            unsigned char* vt = st + pps * link_bytes + pp * vec_bytes;
+            for (int ks = 0; ks < P.Kc / 2; ++ks) {
+              const uint64_t ad = make_desc(lt + (size_t)(2 * ks) * P.Mp * 16, (uint32_t)P.Mp * 16, 128);
+              const uint64_t bd = make_desc(vt + (size_t)(2 * ks) * 2 * P.Rp * 16, (uint32_t)(2 * P.Rp) * 16, 128);
+              mma_f16(dt, ad, bd, idesc, (g > 0 || pp > 0 || ks > 0) ? 1u : 0u);
+            }
           }
           mma_commit(&empty[stage]);
-          ++committed;
           if (++stage == P.stages) { stage = 0; phase ^= 1; }
         }
         if (!ok) break;
@@ -319,45 +341,56 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
     }
   } else {
     // ------------------------------------------------------------ epilogue (warps 2..5)
-    const int q = warp & 3;                // TMEM sub-partition of this warp
-    const int rows_per_warp = P.Mp / 4;    // 16 (M=64) or 32 (M=128)
-    const int et = threadIdx.x - 64;       // 0..127
-    const int N = P.N, Rp = P.Rp;
+    // Link rows are interleaved (2b = Re A[b], 2b+1 = Im A[b]), so accumulator
+    // rows 2b and 2b+1 sit in neighbouring lanes of one warp and the complex
+    // recombination is one lane-pair exchange:
+    //   out_r = D[2b][r] - D[2b+1][Rp+r],   out_i = D[2b][Rp+r] + D[2b+1][r]
+    // The even lane writes r in [c, c+8) of every 16-column chunk, the odd lane [c+8, c+16).
+    const int q = warp & 3;              // TMEM sub-partition of this warp
+    const int rows_per_warp = P.Mp / 4;  // 16 (M=64) or 32 (M=128)
+    const int row = q * rows_per_warp + lane;
+    const int b = row >> 1;
+    const bool odd = row & 1;
+    const bool valid = lane < rows_per_warp && row < 2 * P.N;
+    const float sg = (P.g5 && b >= P.N / 2) ? -1.f : 1.f;
     for (int i = 0; i < nsites; ++i) {
       const int site = blockIdx.x + i * gridDim.x;
       const int acc = i & 1;
       const uint32_t aphase = (uint32_t)(i >> 1) & 1;
       const bool waited = mbar_wait(&tfull[acc], aphase, abort_flag);
-      // all 128 epilogue threads leave together, or none does
-      if (named_bar_or(1, 128, !waited)) {
+      if (!__all_sync(0xffffffffu, waited)) {  // the warp leaves together
         if (!waited) atomicCAS(P.err, 0, ERR_TIMEOUT_EPILOGUE);
         *abort_flag = 1;
         break;
       }
       fence_after();
-      const int row = q * rows_per_warp + lane;  // accumulator row held by this thread
-      for (int c0 = 0; c0 < 2 * Rp; c0 += 32) {
-        float v[32];
-        tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + acc * acc_cols + c0, v);
-        if (lane < rows_per_warp && row < 2 * N) {
+      const uint32_t ta = tmem_base + ((uint32_t)(32 * q) << 16) + acc * acc_cols;
+      float2* orow = P.out + (size_t)site * P.nrhs * P.N + b;
+      for (int c = 0; c < P.Rp; c += 16) {
+        float vr[16], vi[16];
+        tmem_ld16(ta + c, vr);
+        tmem_ld16(ta + P.Rp + c, vi);
+        float pr[8], pi[8];
 #pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (c0 + j < 2 * Rp) E[row * ncolE + c0 + j] = v[j];
+        for (int j = 0; j < 8; ++j) {
+          pr[j] = __shfl_xor_sync(0xffffffffu, odd ? vr[j] : vr[8 + j], 1);
+          pi[j] = __shfl_xor_sync(0xffffffffu, odd ? vi[j] : vi[8 + j], 1);
+        }
+        if (valid) {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int r = c + (odd ? 8 : 0) + j;
+            if (r < P.R) {
+              const float re = odd ? pr[j] - vi[8 + j] : vr[j] - pi[j];
+              const float im = odd ? pi[j] + vr[8 + j] : vi[j] + pr[j];
+              const int slot = P.active ? __ldg(&P.active[r]) : r;
+              orow[(size_t)slot * P.N] = make_float2(sg * re, sg * im);
+            }
+          }
         }
       }
       fence_before();
       mbar_arrive(&tempty[acc]);
-      named_bar(1, 128);
-      // recombine and store: out[site][slot(r)][b]
-      for (int e = et; e < P.R * N; e += 128) {
-        const int r = e / N, b = e % N;
-        float re = E[b * ncolE + r] - E[(N + b) * ncolE + Rp + r];
-        float im = E[(N + b) * ncolE + r] + E[b * ncolE + Rp + r];
-        if (P.g5 && b >= N / 2) { re = -re; im = -im; }
-        const int slot = P.active ? __ldg(&P.active[r]) : r;
-        P.out[((size_t)site * P.nrhs + slot) * N + b] = make_float2(re, im);
-      }
-      named_bar(1, 128);
     }
   }
   fence_before();
@@ -390,10 +423,9 @@ __global__ void pack_links_kernel(const double2* __restrict__ A, uint4* __restri
     for (int j = 0; j < 8; ++j) {
       const int bb = kc * 8 + j;
       float v = 0.f;
-      if (m < 2 * N && bb < N) {
-        const int b = m < N ? m : m - N;
-        const double2 a = A[(((int64_t)p * V + s) * N + b) * N + bb];
-        v = (float)(m < N ? a.x : a.y);
+      if (m < 2 * N && bb < N) {  // interleaved rows: 2b = Re A[b][.], 2b+1 = Im A[b][.]
+        const double2 a = A[(((int64_t)p * V + s) * N + (m >> 1)) * N + bb];
+        v = (float)((m & 1) ? a.y : a.x);
       }
       h[j] = to_half_bits(v, kind);
     }
@@ -488,46 +520,37 @@ gmg_status coarse_prepare_tc(gmg_coarse* h, int kind, cudaStream_t s) {
   return GMG_OK;
 }
 
-gmg_status coarse_apply_tc(gmg_coarse* h, int p0, int p1, bool g5, int kind, int nrhs, const float* in,
-                           float* out, const int32_t* active, int n_active, cudaStream_t s) {
+namespace tc {
+
+// Launch configuration shared by gmg_coarse_apply and gmg_coarse_apply_noalloc:
+// points per stage (3 when enough stages fit, else 1) and the stage count.
+static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int p0, int p1, bool g5, int kind, int nrhs,
+                                 float* out, const int32_t* active, int R, bool timed, cudaStream_t s) {
   const int N = h->N;
-  const int R = active ? n_active : nrhs;
-  if (R == 0) return GMG_OK;
-  GMG_CHECK(R <= 128, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil supports at most 128 active RHS");
-  const int Rp = tc::round_up(R, 16);
-  const int Kc = tc::round_up(N, 16) / 8;
+  const int Rp = round_up(R, 16);
+  const int Kc = round_up(N, 16) / 8;
   const int Mp = 2 * N <= 64 ? 64 : 128;
   const int V = (int)h->dims.vol();
-  // scratch: packed vectors + error word
-  const size_t packed_bytes = (size_t)V * Kc * 2 * Rp * 16;
-  GMG_TRY(h->scratch.alloc(packed_bytes));
-  uint4* packed = h->scratch.as<uint4>();
-  int* err = h->dev_err.as<int>();
-  const int64_t rows = (int64_t)V * Kc * Rp;
-  tc::pack_vec_kernel<<<(int)std::min<int64_t>((rows + 255) / 256, 148 * 64), 256, 0, s>>>(
-      reinterpret_cast<const float2*>(in), packed, active, V, N, nrhs, R, Rp, Kc, kind, g5 ? 1 : 0,
-      (reinterpret_cast<uintptr_t>(in) & 15) == 0 ? 1 : 0);
-  GMG_CUDA(cudaGetLastError());
-
-  const uint32_t stage_bytes = (uint32_t)Kc * Mp * 16 + (uint32_t)Kc * 2 * Rp * 16;
-  const size_t e_bytes = ((size_t)Mp * (2 * Rp + 1) * 4 + 15) / 16 * 16;
-  const size_t fixed = e_bytes + 64 * 8 + 64 + 32 * 9 * 4;
+  const uint32_t per_point = (uint32_t)Kc * Mp * 16 + (uint32_t)Kc * 2 * Rp * 16;
+  const size_t fixed = 80 * 8 + 16 + 32 * 9 * 4;  // barriers (<= 2*32+5), TMEM slot + flag, neighbour table
   const size_t budget = 227 * 1024 - fixed;
-  int stages = (int)std::min<size_t>(32, budget / stage_bytes);
+  const int npts = p1 - p0;
+  int pps = (npts % 3 == 0 && budget / (3 * per_point) >= 4) ? 3 : 1;
+  const uint32_t stage_bytes = pps * per_point;
+  const int stages = (int)std::min<size_t>(32, budget / stage_bytes);
   GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil: tile does not fit shared memory");
-  const size_t smem = (size_t)stages * stage_bytes + e_bytes + (size_t)(2 * stages + 2 * tc::kAccBufs + 1) * 8 + 16 +
-                      32 * 9 * 4;
-  GMG_CUDA(cudaFuncSetAttribute(tc::coarse_mrhs_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t smem = (size_t)stages * stage_bytes + (size_t)(2 * stages + 2 * kAccBufs + 1) * 8 + 16 + 32 * 9 * 4;
+  GMG_CUDA(cudaFuncSetAttribute(coarse_mrhs_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  tc::Params P;
+  GMG_CUDA(cudaGetDevice(&dev));
+  GMG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  Params P;
   P.links = h->links_h.buf.as<uint16_t>();
   P.packed = reinterpret_cast<const uint16_t*>(packed);
   P.nbr = h->nbr.as<int32_t>();
   P.active = active;
   P.out = reinterpret_cast<float2*>(out);
-  P.err = err;
+  P.err = h->dev_err.as<int>();
   P.V = V;
   P.N = N;
   P.nrhs = nrhs;
@@ -540,12 +563,38 @@ gmg_status coarse_apply_tc(gmg_coarse* h, int p0, int p1, bool g5, int kind, int
   P.g5 = g5 ? 1 : 0;
   P.stages = stages;
   P.kind = kind == GMG_BF16 ? 1 : 0;
-  {
+  P.pps = pps;
+  if (timed) {
     KernelTimer kt("coarse_mrhs_tc", s);
-    tc::coarse_mrhs_tc_kernel<<<std::min(V, nsm), tc::kThreads, smem, s>>>(P);
+    coarse_mrhs_tc_kernel<<<std::min(V, nsm), kThreads, smem, s>>>(P);
+  } else {
+    coarse_mrhs_tc_kernel<<<std::min(V, nsm), kThreads, smem, s>>>(P);
   }
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
+}
+
+}  // namespace tc
+
+gmg_status coarse_apply_tc(gmg_coarse* h, int p0, int p1, bool g5, int kind, int nrhs, const float* in,
+                           float* out, const int32_t* active, int n_active, cudaStream_t s) {
+  const int N = h->N;
+  const int R = active ? n_active : nrhs;
+  if (R == 0) return GMG_OK;
+  GMG_CHECK(R <= 128, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil supports at most 128 active RHS");
+  const int Rp = tc::round_up(R, 16);
+  const int Kc = tc::round_up(N, 16) / 8;
+  const int V = (int)h->dims.vol();
+  // scratch: packed vectors
+  const size_t packed_bytes = (size_t)V * Kc * 2 * Rp * 16;
+  GMG_TRY(h->scratch.alloc(packed_bytes));
+  uint4* packed = h->scratch.as<uint4>();
+  const int64_t rows = (int64_t)V * Kc * Rp;
+  tc::pack_vec_kernel<<<(int)std::min<int64_t>((rows + 255) / 256, 148 * 64), 256, 0, s>>>(
+      reinterpret_cast<const float2*>(in), packed, active, V, N, nrhs, R, Rp, Kc, kind, g5 ? 1 : 0,
+      (reinterpret_cast<uintptr_t>(in) & 15) == 0 ? 1 : 0);
+  GMG_CUDA(cudaGetLastError());
+  return tc::launch_stencil(h, packed, p0, p1, g5, kind, nrhs, out, active, R, true, s);
 }
 
 }  // namespace gmg
@@ -636,7 +685,6 @@ extern "C" gmg_status gmg_coarse_apply_noalloc(gmg_coarse* h, gmg_op op, int poi
   GMG_CHECK(R <= 128, GMG_ERR_UNSUPPORTED, "gmg_coarse_apply_noalloc: at most 128 active RHS");
   const int Rp = tc::round_up(R, 16);
   const int Kc = tc::round_up(N, 16) / 8;
-  const int Mp = 2 * N <= 64 ? 64 : 128;
   const int V = (int)h->dims.vol();
   const size_t packed_bytes = (size_t)V * Kc * 2 * Rp * 16;
   if (packed_bytes > tc::kNoAllocScratchBytes)
@@ -652,37 +700,5 @@ extern "C" gmg_status gmg_coarse_apply_noalloc(gmg_coarse* h, gmg_op op, int poi
       reinterpret_cast<const float2*>(in), packed, active, V, N, nrhs, R, Rp, Kc, compute, g5 ? 1 : 0,
       (reinterpret_cast<uintptr_t>(in) & 15) == 0 ? 1 : 0);
   GMG_CUDA(cudaGetLastError());
-  const uint32_t stage_bytes = (uint32_t)Kc * Mp * 16 + (uint32_t)Kc * 2 * Rp * 16;
-  const size_t e_bytes = ((size_t)Mp * (2 * Rp + 1) * 4 + 15) / 16 * 16;
-  const size_t fixed = e_bytes + 64 * 8 + 64 + 32 * 9 * 4;
-  const int stages = (int)std::min<size_t>(32, (227 * 1024 - fixed) / stage_bytes);
-  GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "gmg_coarse_apply_noalloc: tile does not fit shared memory");
-  const size_t smem = (size_t)stages * stage_bytes + e_bytes + (size_t)(2 * stages + 2 * tc::kAccBufs + 1) * 8 + 16 +
-                      32 * 9 * 4;
-  GMG_CUDA(cudaFuncSetAttribute(tc::coarse_mrhs_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int dev = 0, nsm = 148;
-  GMG_CUDA(cudaGetDevice(&dev));
-  GMG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  tc::Params P;
-  P.links = h->links_h.buf.as<uint16_t>();
-  P.packed = reinterpret_cast<const uint16_t*>(packed);
-  P.nbr = h->nbr.as<int32_t>();
-  P.active = active;
-  P.out = reinterpret_cast<float2*>(out);
-  P.err = h->dev_err.as<int>();
-  P.V = V;
-  P.N = N;
-  P.nrhs = nrhs;
-  P.R = R;
-  P.Rp = Rp;
-  P.Kc = Kc;
-  P.Mp = Mp;
-  P.p0 = p0;
-  P.p1 = p1;
-  P.g5 = g5 ? 1 : 0;
-  P.stages = stages;
-  P.kind = compute == GMG_BF16 ? 1 : 0;
-  tc::coarse_mrhs_tc_kernel<<<std::min(V, nsm), tc::kThreads, smem, s>>>(P);
-  GMG_CUDA(cudaGetLastError());
-  return GMG_OK;
+  return tc::launch_stencil(h, packed, p0, p1, g5, compute, nrhs, out, active, R, false, s);
 }

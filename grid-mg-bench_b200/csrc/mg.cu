@@ -1,0 +1,589 @@
+// mg.cu -- multigrid-preconditioned Wilson-clover solve on the GPU.
+//
+// Restates the reference's multigrid driver:
+//   MultiGridPreconditioner::operator() (include/MultigridPreconditioner.h:253-309):
+//       restrict -> K-cycle wrapper solve on the next level, preconditioned by
+//       the next level's cycle -> prolong -> post-smooth (no pre-smoothing)
+//   coarsest level: a GMRES solve (:622-641)
+//   test-vector setup (include/BasisVectors.h:74-149, NullVectorSetupRework.h):
+//       random vectors, an approximate solve A psi = v, chiral doubling,
+//       block orthonormalisation, then CoarsenOperator on every level
+//   outer solve: FGMRES with the MG preconditioner (src/Test_wilsonclover_mg.cc:140,
+//       mixed precision as src/Test_wilsonclover_mg_mp.cc:149-155)
+// with the smoother of the multi-RHS configuration (MR, a fixed number of
+// iterations) and every right-hand side of a batch solved together: vectors
+// are [site][rhs][dof], each RHS keeps its own Krylov coefficients, and the
+// outer solver compacts the batch at every restart so converged RHS drop out.
+// The small per-RHS Krylov algebra (Hessenberg columns, Givens rotations,
+// triangular solves) runs on the host.
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+
+#include "mg_internal.cuh"
+
+typedef std::complex<double> zc;
+
+namespace gmg {
+
+struct MGLevel {
+  int l = 0;
+  Dims dims;
+  int64_t V = 0;
+  int dof = 0;
+  int vprec = GMG_F64;    // vector precision inside the preconditioner
+  int compute = GMG_F64;  // coarse-operator compute form (F64, F32, BF16)
+  gmg_wilson* w = nullptr;  // level 0 (not owned)
+  gmg_coarse* c = nullptr;  // level > 0 (owned)
+  gmg_agg* agg = nullptr;   // aggregation to level l+1 (owned)
+  int m = 0;                // Krylov restart of the solver that runs on this level
+  VecBuf V0, Z0, kw, kt;    // Krylov basis (m+1), flexible directions (m), temporaries
+  VecBuf mr_r, mr_Ar, mr_t; // MR smoother
+  VecBuf bc, xc;            // right-hand side / solution of this level inside the cycle above
+  ~MGLevel() {
+    if (c) gmg_coarse_destroy(c);
+    if (agg) gmg_agg_destroy(agg);
+  }
+};
+
+}  // namespace gmg
+
+struct gmg_mg {
+  gmg_mg_params P;
+  gmg_wilson* fine = nullptr;
+  int Rmax = 0;
+  std::vector<gmg::MGLevel*> L;
+  gmg::DevBuf coef;  // device coefficients (double2)
+  std::vector<zc> hbuf;
+  bool setup_done = false;
+  ~gmg_mg() {
+    for (auto* l : L) delete l;
+  }
+};
+
+namespace gmg {
+namespace {
+
+// ------------------------------------------------------------- small helpers
+gmg_status apply_op(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s) {
+  MGLevel& L = *h->L[l];
+  if (l == 0) return gmg_wilson_apply(L.w, GMG_OP_M, 0, 0, (gmg_prec)in.prec, in.R, in.p, out.p, (gmg_stream)s);
+  const int compute = in.prec == GMG_F64 ? GMG_F64 : L.compute;
+  return gmg_coarse_apply(L.c, GMG_OP_M, 8, (gmg_prec)compute, (gmg_prec)in.prec, in.R, in.p, out.p, nullptr, 0,
+                          (gmg_stream)s);
+}
+
+// host <- per-RHS <X_j, Y> for j < nx
+gmg_status dots(gmg_mg* h, const Vec& X0, int nx, int64_t xstride, const Vec& Y, std::vector<zc>& out,
+                cudaStream_t s) {
+  double2* d = h->coef.as<double2>();
+  GMG_TRY(vec_multidot(X0, nx, xstride, Y, d, nullptr, s));
+  out.resize((size_t)nx * Y.R);
+  GMG_CUDA(cudaMemcpyAsync(out.data(), d, sizeof(double2) * nx * Y.R, cudaMemcpyDeviceToHost, s));
+  GMG_CUDA(cudaStreamSynchronize(s));
+  return GMG_OK;
+}
+
+gmg_status upload(gmg_mg* h, const std::vector<zc>& a, size_t offset_elems, cudaStream_t s) {
+  GMG_CUDA(cudaMemcpyAsync(h->coef.as<double2>() + offset_elems, a.data(), sizeof(double2) * a.size(),
+                           cudaMemcpyHostToDevice, s));
+  GMG_CUDA(cudaStreamSynchronize(s));  // `a` is host scratch reused by the caller
+  return GMG_OK;
+}
+
+// Y = a X + b Y with per-RHS host coefficients
+gmg_status axpby_h(gmg_mg* h, const std::vector<zc>& a, const Vec& X, const std::vector<zc>& b, Vec& Y,
+                   cudaStream_t s) {
+  std::vector<zc> ab(a);
+  ab.insert(ab.end(), b.begin(), b.end());
+  GMG_TRY(upload(h, ab, 0, s));
+  return vec_axpby(h->coef.as<double2>(), X, h->coef.as<double2>() + a.size(), Y, s);
+}
+
+// Y += sum_j c[j*R + r] X_j
+gmg_status multiaxpy_h(gmg_mg* h, const std::vector<zc>& c, const Vec& X0, int nx, int64_t xstride, Vec& Y,
+                       cudaStream_t s) {
+  GMG_TRY(upload(h, c, 0, s));
+  return vec_multiaxpy(h->coef.as<double2>(), X0, nx, xstride, Y, s);
+}
+
+Vec nth(const Vec& base, int j) {
+  Vec v = base;
+  v.p = static_cast<char*>(base.p) + (size_t)j * base.bytes();
+  return v;
+}
+
+gmg_status zero(Vec& v, cudaStream_t s) {
+  GMG_CUDA(cudaMemsetAsync(v.p, 0, v.bytes(), s));
+  return GMG_OK;
+}
+
+gmg_status copyv(const Vec& a, Vec& b, cudaStream_t s) { return vec_convert(a, b, s); }
+
+// ------------------------------------------------------------- MR smoother
+// x <- x + iters steps of minimal residual for A x = b on level l
+gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStream_t s) {
+  MGLevel& L = *h->L[l];
+  const int R = b.R;
+  Vec r = L.mr_r.with_rhs(R), Ar = L.mr_Ar.with_rhs(R), t = L.mr_t.with_rhs(R);
+  std::vector<zc> one(R, 1.0), mone(R, -1.0), d1, d2, al(R), mal(R);
+  GMG_TRY(apply_op(h, l, x, t, s));
+  GMG_TRY(copyv(b, r, s));
+  GMG_TRY(axpby_h(h, mone, t, one, r, s));
+  for (int it = 0; it < iters; ++it) {
+    GMG_TRY(apply_op(h, l, r, Ar, s));
+    GMG_TRY(dots(h, Ar, 1, 0, r, d1, s));
+    GMG_TRY(dots(h, Ar, 1, 0, Ar, d2, s));
+    for (int k = 0; k < R; ++k) {
+      al[k] = d2[k].real() > 0 ? d1[k] / d2[k].real() : 0.0;
+      mal[k] = -al[k];
+    }
+    GMG_TRY(axpby_h(h, al, r, one, x, s));
+    GMG_TRY(axpby_h(h, mal, Ar, one, r, s));
+  }
+  return GMG_OK;
+}
+
+// ------------------------------------------------------------- (F)GMRES
+// Solve A x = b on level l from the initial guess in x; per-RHS relative
+// tolerance tol; at most maxit iterations in cycles of m.  `prec(in, out)`
+// (flexible) is applied when given.  Krylov vectors live on level l's
+// workspace; for level 0 with FP64 vectors the caller supplies them (outer).
+struct Krylov {
+  Vec V0, Z0;   // V: m+1 vectors, Z: m vectors (Z0.p == nullptr -> not flexible)
+  Vec w, t;     // temporaries, precision of V (t: precision of Z)
+  Vec tz;       // Z-precision temporary for the preconditioner input (may equal V precision)
+};
+
+template <class Prec>
+gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m, int maxit, double tol, Prec prec,
+                  bool flexible, int* iters_out, std::vector<double>* relres, cudaStream_t s) {
+  const int R = b.R;
+  Vec V0 = K.V0.with_rhs(R), Z0 = K.Z0.with_rhs(R), w = K.w.with_rhs(R), t = K.t.with_rhs(R), tz = K.tz.with_rhs(R);
+  const int64_t vstride = V0.elems(), zstride = Z0.elems();
+  std::vector<zc> bn;
+  GMG_TRY(dots(h, b, 1, 0, b, bn, s));
+  std::vector<double> bnorm(R);
+  for (int r = 0; r < R; ++r) bnorm[r] = std::sqrt(std::max(bn[r].real(), 1e-300));
+  std::vector<zc> one(R, 1.0), mone(R, -1.0), zeros(R, 0.0);
+  std::vector<double> res(R, 1.0);
+  int iters = 0;
+  std::vector<zc> H((size_t)(m + 1) * m * R), g((size_t)(m + 1) * R), cs((size_t)m * R), sn((size_t)m * R);
+  while (true) {
+    // r0 = b - A x -> V_0
+    Vec v0 = nth(V0, 0);
+    GMG_TRY(apply_op(h, l, x, w, s));
+    GMG_TRY(copyv(b, v0, s));
+    GMG_TRY(axpby_h(h, mone, w, one, v0, s));
+    std::vector<zc> bb;
+    GMG_TRY(dots(h, v0, 1, 0, v0, bb, s));
+    bool all = true;
+    std::vector<zc> inv(R);
+    std::vector<double> beta(R);
+    for (int r = 0; r < R; ++r) {
+      beta[r] = std::sqrt(std::max(bb[r].real(), 0.0));
+      res[r] = beta[r] / bnorm[r];
+      if (res[r] > tol) all = false;
+      inv[r] = beta[r] > 0 ? 1.0 / beta[r] : 0.0;
+    }
+    if (all || iters >= maxit) break;
+    GMG_TRY(axpby_h(h, zeros, v0, inv, v0, s));
+    std::fill(H.begin(), H.end(), zc(0));
+    std::fill(g.begin(), g.end(), zc(0));
+    for (int r = 0; r < R; ++r) g[r] = beta[r];
+    int jl = -1;
+    for (int j = 0; j < m && iters < maxit; ++j) {
+      Vec vj = nth(V0, j);
+      Vec zj = flexible ? nth(Z0, j) : vj;
+      if (flexible) GMG_TRY(prec(vj, zj, tz));
+      if (zj.prec != w.prec) {
+        GMG_TRY(vec_convert(zj, t, s));
+        GMG_TRY(apply_op(h, l, t, w, s));
+      } else {
+        GMG_TRY(apply_op(h, l, zj, w, s));
+      }
+      // classical Gram-Schmidt, twice
+      std::vector<zc> hc, hc2;
+      GMG_TRY(dots(h, V0, j + 1, vstride, w, hc, s));
+      std::vector<zc> neg(hc.size());
+      for (size_t k = 0; k < hc.size(); ++k) neg[k] = -hc[k];
+      GMG_TRY(multiaxpy_h(h, neg, V0, j + 1, vstride, w, s));
+      GMG_TRY(dots(h, V0, j + 1, vstride, w, hc2, s));
+      for (size_t k = 0; k < hc2.size(); ++k) {
+        neg[k] = -hc2[k];
+        hc[k] += hc2[k];
+      }
+      GMG_TRY(multiaxpy_h(h, neg, V0, j + 1, vstride, w, s));
+      std::vector<zc> ww;
+      GMG_TRY(dots(h, w, 1, 0, w, ww, s));
+      Vec vn = nth(V0, j + 1);
+      std::vector<zc> sc(R);
+      for (int r = 0; r < R; ++r) {
+        const double hn = std::sqrt(std::max(ww[r].real(), 0.0));
+        sc[r] = hn > 0 ? 1.0 / hn : 0.0;
+        // Hessenberg column j of RHS r, Givens rotations
+        zc* Hr = &H[(size_t)r * (m + 1) * m];
+        for (int i = 0; i <= j; ++i) Hr[i * m + j] = hc[(size_t)i * R + r];
+        Hr[(j + 1) * m + j] = hn;
+        for (int i = 0; i < j; ++i) {
+          const zc c = cs[(size_t)r * m + i], sgn = sn[(size_t)r * m + i];
+          const zc a = Hr[i * m + j], bq = Hr[(i + 1) * m + j];
+          Hr[i * m + j] = std::conj(c) * a + std::conj(sgn) * bq;
+          Hr[(i + 1) * m + j] = -sgn * a + c * bq;
+        }
+        const zc a = Hr[j * m + j];
+        const double bq = std::abs(Hr[(j + 1) * m + j]);
+        const double den = std::sqrt(std::norm(a) + bq * bq);
+        zc c = 1.0, sgn = 0.0;
+        if (den > 0) {
+          c = a / den;
+          sgn = Hr[(j + 1) * m + j] / den;
+        }
+        cs[(size_t)r * m + j] = c;
+        sn[(size_t)r * m + j] = sgn;
+        Hr[j * m + j] = std::conj(c) * a + std::conj(sgn) * Hr[(j + 1) * m + j];
+        Hr[(j + 1) * m + j] = 0.0;
+        zc* gr = &g[(size_t)r * (m + 1)];
+        const zc gj = gr[j];
+        gr[j] = std::conj(c) * gj;
+        gr[j + 1] = -sgn * gj;
+        res[r] = std::abs(gr[j + 1]) / bnorm[r];
+      }
+      GMG_TRY(copyv(w, vn, s));
+      GMG_TRY(axpby_h(h, zeros, vn, sc, vn, s));
+      ++iters;
+      jl = j;
+      bool conv = true;
+      for (int r = 0; r < R; ++r)
+        if (res[r] > tol) conv = false;
+      if (conv) break;
+    }
+    if (jl < 0) break;
+    // y = H^{-1} g per RHS, x += sum_j y_j Z_j
+    const int n = jl + 1;
+    std::vector<zc> y((size_t)n * R);
+    for (int r = 0; r < R; ++r) {
+      const zc* Hr = &H[(size_t)r * (m + 1) * m];
+      const zc* gr = &g[(size_t)r * (m + 1)];
+      for (int i = n - 1; i >= 0; --i) {
+        zc acc = gr[i];
+        for (int k = i + 1; k < n; ++k) acc -= Hr[i * m + k] * y[(size_t)k * R + r];
+        y[(size_t)i * R + r] = Hr[i * m + i] != zc(0) ? acc / Hr[i * m + i] : zc(0);
+      }
+    }
+    GMG_TRY(multiaxpy_h(h, y, flexible ? Z0 : V0, n, flexible ? zstride : vstride, x, s));
+  }
+  if (iters_out) *iters_out = iters;
+  if (relres) *relres = res;
+  return GMG_OK;
+}
+
+Krylov level_krylov(MGLevel& L) {
+  Krylov K;
+  K.V0 = L.V0;
+  K.Z0 = L.Z0;
+  K.w = L.kw;
+  K.t = L.kt;
+  K.tz = L.kt;
+  return K;
+}
+
+// ------------------------------------------------------------- K-cycle
+gmg_status kcycle(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s);
+
+gmg_status coarse_solve(gmg_mg* h, int lc, const Vec& b, Vec& x, cudaStream_t s) {
+  MGLevel& C = *h->L[lc];
+  const bool coarsest = lc == (int)h->L.size() - 1;
+  const gmg_mg_params& P = h->P;
+  GMG_TRY(zero(x, s));
+  Krylov K = level_krylov(C);
+  if (coarsest) {
+    auto none = [](const Vec&, Vec&, const Vec&) { return GMG_OK; };
+    return fgmres(h, lc, b, x, K, C.m, P.coarsest_iters, P.coarsest_tol, none, false, nullptr, nullptr, s);
+  }
+  auto pc = [h, lc, s](const Vec& in, Vec& out, const Vec&) { return kcycle(h, lc, in, out, s); };
+  return fgmres(h, lc, b, x, K, C.m, P.wrapper_iters, P.wrapper_tol, pc, true, nullptr, nullptr, s);
+}
+
+gmg_status kcycle(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s) {
+  MGLevel& L = *h->L[l];
+  MGLevel& C = *h->L[l + 1];
+  const int R = in.R;
+  Vec bc = C.bc.with_rhs(R), xc = C.xc.with_rhs(R);
+  GMG_TRY(gmg_agg_project(L.agg, (gmg_prec)in.prec, (gmg_prec)in.prec, R, in.p, bc.p, (gmg_stream)s));
+  GMG_TRY(coarse_solve(h, l + 1, bc, xc, s));
+  GMG_TRY(gmg_agg_promote(L.agg, (gmg_prec)in.prec, (gmg_prec)in.prec, R, xc.p, out.p, (gmg_stream)s));
+  return mr_smooth(h, l, in, out, h->P.smoother_iters, s);
+}
+
+// ------------------------------------------------------------- setup
+// `count` consecutive fields of [V][R][dof] in one buffer; the Vec describes the first
+gmg_status alloc_fields(VecBuf& b, int64_t V, int R, int dof, int prec, int count) {
+  b.V = V;
+  b.R = R;
+  b.dof = dof;
+  b.prec = prec;
+  GMG_TRY(b.buf.alloc((size_t)count * b.bytes()));
+  b.p = b.buf.p;
+  return GMG_OK;
+}
+
+// Level workspaces: MR smoother on every level; Krylov basis for the solver
+// that runs on a coarse level (flexible directions only where a K-cycle
+// preconditions it); right-hand side / solution of the cycle above.
+gmg_status alloc_level_ws(MGLevel& L, int R, bool krylov, bool flexible) {
+  const int p = L.vprec;
+  if (krylov) {
+    GMG_TRY(alloc_fields(L.V0, L.V, R, L.dof, p, L.m + 1));
+    if (flexible) GMG_TRY(alloc_fields(L.Z0, L.V, R, L.dof, p, L.m));
+    GMG_TRY(L.kw.alloc(L.V, R, L.dof, p));
+    GMG_TRY(L.kt.alloc(L.V, R, L.dof, p));
+  }
+  GMG_TRY(L.mr_r.alloc(L.V, R, L.dof, p));
+  GMG_TRY(L.mr_Ar.alloc(L.V, R, L.dof, p));
+  GMG_TRY(L.mr_t.alloc(L.V, R, L.dof, p));
+  if (L.l > 0) {
+    GMG_TRY(L.bc.alloc(L.V, R, L.dof, p));
+    GMG_TRY(L.xc.alloc(L.V, R, L.dof, p));
+  }
+  return GMG_OK;
+}
+
+}  // namespace
+}  // namespace gmg
+
+using namespace gmg;
+
+extern "C" gmg_status gmg_mg_params_default(gmg_mg_params* p) {
+  GMG_CHECK(p != nullptr, GMG_ERR_ARGUMENT, "gmg_mg_params_default: null");
+  memset(p, 0, sizeof(*p));
+  p->nlevels = 3;
+  for (int d = 0; d < 4; ++d) {
+    p->block[0][d] = 4;
+    p->block[1][d] = 2;
+  }
+  p->nvec[0] = 12;
+  p->nvec[1] = 16;
+  p->setup_iters = 40;
+  p->smoother_iters = 8;
+  p->wrapper_iters = 10;
+  p->wrapper_tol = 0.1;
+  p->coarsest_iters = 50;
+  p->coarsest_tol = 0.05;
+  p->coarsest_restart = 10;
+  p->outer_restart = 8;
+  p->prec = GMG_F32;
+  p->seed = 1234;
+  return GMG_OK;
+}
+
+extern "C" gmg_status gmg_mg_create(gmg_wilson* fine, const gmg_mg_params* p, int max_rhs, gmg_mg** out) {
+  GMG_CHECK(fine && p && out, GMG_ERR_ARGUMENT, "gmg_mg_create: null argument");
+  *out = nullptr;
+  GMG_CHECK(p->nlevels >= 2 && p->nlevels <= 3, GMG_ERR_ARGUMENT, "gmg_mg_create: nlevels must be 2 or 3");
+  GMG_CHECK(max_rhs >= 1 && max_rhs <= 64, GMG_ERR_ARGUMENT, "gmg_mg_create: max_rhs must be in [1, 64]");
+  GMG_CHECK(p->prec == GMG_F64 || p->prec == GMG_F32 || p->prec == GMG_BF16, GMG_ERR_ARGUMENT,
+            "gmg_mg_create: prec must be F64, F32 or BF16");
+  gmg_mg* h = new gmg_mg();
+  h->P = *p;
+  h->fine = fine;
+  h->Rmax = max_rhs;
+  Dims d = fine->dims;
+  int dof = 12;
+  for (int l = 0; l < p->nlevels; ++l) {
+    MGLevel* L = new MGLevel();
+    L->l = l;
+    L->dims = d;
+    L->V = d.vol();
+    L->dof = dof;
+    L->vprec = p->prec == GMG_F64 ? GMG_F64 : GMG_F32;
+    L->compute = p->prec == GMG_BF16 && l > 0 ? GMG_BF16 : L->vprec;
+    L->w = l == 0 ? fine : nullptr;
+    h->L.push_back(L);
+    if (l + 1 < p->nlevels) {
+      for (int k = 0; k < 4; ++k) {
+        const int b = p->block[l][k];
+        if (b <= 0 || d.d[k] % b != 0) {
+          delete h;
+          return fail(GMG_ERR_SHAPE, "gmg_mg_create: block size does not divide the lattice");
+        }
+        d.d[k] /= b;
+      }
+      dof = 2 * p->nvec[l];
+    }
+  }
+  gmg_status st = h->coef.alloc(sizeof(double2) * 4096);
+  if (st != GMG_OK) {
+    delete h;
+    return st;
+  }
+  *out = h;
+  return GMG_OK;
+}
+
+extern "C" gmg_status gmg_mg_destroy(gmg_mg* h) {
+  if (h) {
+    cudaDeviceSynchronize();
+    delete h;
+  }
+  return GMG_OK;
+}
+
+extern "C" gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream stream) {
+  GMG_CHECK(h != nullptr, GMG_ERR_ARGUMENT, "gmg_mg_setup: null handle");
+  GMG_CHECK(h->fine->gauge_set, GMG_ERR_STATE, "gmg_mg_setup: gauge field not set");
+  cudaStream_t s = S(stream);
+  const gmg_mg_params& P = h->P;
+  const int nl = (int)h->L.size();
+  for (int l = 0; l < nl; ++l) {
+    MGLevel& L = *h->L[l];
+    const bool coarsest = l == nl - 1;
+    L.m = l == 0 ? 0 : (coarsest ? std::max(P.coarsest_restart, 2) : std::max(P.wrapper_iters, 2));
+  }
+  GMG_TRY(alloc_level_ws(*h->L[0], h->Rmax, false, false));
+  for (int l = 0; l + 1 < nl; ++l) {
+    MGLevel& L = *h->L[l];
+    MGLevel& C = *h->L[l + 1];
+    const int nv = P.nvec[l];
+    // test vectors: A psi = v approximately, from random v (BasisVectors.h:94-120),
+    // GMRES(10) with a temporary Krylov basis sized for the nv vectors
+    VecBuf v, psi, sV, sw, st;
+    const int ms = 10;
+    GMG_TRY(v.alloc(L.V, nv, L.dof, L.vprec));
+    GMG_TRY(psi.alloc(L.V, nv, L.dof, L.vprec));
+    GMG_TRY(alloc_fields(sV, L.V, nv, L.dof, L.vprec, ms + 1));
+    GMG_TRY(sw.alloc(L.V, nv, L.dof, L.vprec));
+    GMG_TRY(st.alloc(L.V, nv, L.dof, L.vprec));
+    GMG_TRY(vec_gaussian(v, P.seed * 7919 + l, s));
+    GMG_CUDA(cudaMemsetAsync(psi.p, 0, psi.bytes(), s));
+    Krylov K;
+    K.V0 = sV;
+    K.w = sw;
+    K.t = st;
+    K.tz = st;
+    auto none = [](const Vec&, Vec&, const Vec&) { return GMG_OK; };
+    GMG_TRY(fgmres(h, l, v, psi, K, ms, P.setup_iters, 1e-3, none, false, nullptr, nullptr, s));
+    // chiral doubling -> basis, block orthonormalisation, Galerkin coarsening
+    DevBuf basis;
+    GMG_TRY(basis.alloc(sizeof(double2) * 2 * (size_t)nv * L.V * L.dof));
+    GMG_TRY(vec_chiral_double(psi, basis.as<double>(), s));
+    GMG_TRY(gmg_agg_create(L.dims.d, C.dims.d, L.dof, 2 * nv, &L.agg));
+    GMG_TRY(gmg_agg_set_basis(L.agg, basis.as<double>(), 1, stream));
+    GMG_TRY(gmg_agg_orthonormalise(L.agg, 2, stream));
+    GMG_CUDA(cudaStreamSynchronize(s));
+    GMG_TRY(gmg_coarse_create(C.dims.d, 2 * nv, 0, &C.c));
+    if (l == 0) GMG_TRY(gmg_coarsen_wilson(C.c, L.agg, L.w, stream));
+    else GMG_TRY(gmg_coarsen_coarse(C.c, L.agg, L.c, stream));
+    if (C.vprec == GMG_F32) GMG_TRY(gmg_coarse_prepare(C.c, GMG_F32, stream));
+    if (C.compute == GMG_BF16) GMG_TRY(gmg_coarse_prepare(C.c, GMG_BF16, stream));
+    const bool coarsest = l + 1 == nl - 1;
+    GMG_TRY(alloc_level_ws(C, h->Rmax, true, !coarsest));
+    GMG_CUDA(cudaStreamSynchronize(s));
+  }
+  h->setup_done = true;
+  return GMG_OK;
+}
+
+// Outer FGMRES in FP64 on the fine operator, preconditioned by the K-cycle in
+// the preconditioner precision.  b, x: device FP64 [V][nrhs][12]; x holds the
+// initial guess.  At every restart the still-unconverged RHS are compacted
+// into a contiguous batch, so converged ones drop out of all later work.
+extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double* x, double tol, int maxiter,
+                                   int* iters_out, double* max_relres, gmg_stream stream) {
+  GMG_CHECK(h && b && x, GMG_ERR_ARGUMENT, "gmg_mg_solve: null argument");
+  GMG_CHECK(h->setup_done, GMG_ERR_STATE, "gmg_mg_solve: call gmg_mg_setup first");
+  GMG_CHECK(nrhs >= 1 && nrhs <= h->Rmax, GMG_ERR_ARGUMENT, "gmg_mg_solve: nrhs exceeds max_rhs");
+  GMG_CHECK(tol > 0 && maxiter >= 1, GMG_ERR_ARGUMENT, "gmg_mg_solve: bad tolerance / iteration limit");
+  cudaStream_t s = S(stream);
+  MGLevel& F = *h->L[0];
+  const int m = std::max(h->P.outer_restart, 2);
+  const int zp = F.vprec;
+  // outer workspace for the full batch
+  VecBuf V0, Z0, w, t64, tz, bb, xx, idxv;
+  const int64_t V = F.V;
+  GMG_TRY(V0.alloc(V, nrhs, 12, GMG_F64));
+  V0.buf.free();
+  GMG_TRY(V0.buf.alloc((size_t)(m + 1) * V * nrhs * 12 * 16));
+  V0.p = V0.buf.p;
+  GMG_TRY(Z0.alloc(V, nrhs, 12, zp));
+  Z0.buf.free();
+  GMG_TRY(Z0.buf.alloc((size_t)m * V * nrhs * 12 * Z0.esize()));
+  Z0.p = Z0.buf.p;
+  GMG_TRY(w.alloc(V, nrhs, 12, GMG_F64));
+  GMG_TRY(t64.alloc(V, nrhs, 12, GMG_F64));
+  GMG_TRY(tz.alloc(V, nrhs, 12, zp));
+  GMG_TRY(bb.alloc(V, nrhs, 12, GMG_F64));
+  GMG_TRY(xx.alloc(V, nrhs, 12, GMG_F64));
+  DevBuf idx;
+  GMG_TRY(idx.alloc(sizeof(int) * nrhs));
+  Vec Bfull, Xfull;
+  Bfull.p = const_cast<double*>(b);
+  Bfull.V = V;
+  Bfull.R = nrhs;
+  Bfull.dof = 12;
+  Xfull = Bfull;
+  Xfull.p = x;
+  std::vector<int> active(nrhs);
+  for (int r = 0; r < nrhs; ++r) active[r] = r;
+  std::vector<double> relres(nrhs, 1.0);
+  int total = 0;
+  // per-RHS norms of b for the global convergence criterion
+  std::vector<zc> bnz;
+  GMG_TRY(dots(h, Bfull, 1, 0, Bfull, bnz, s));
+  while (!active.empty() && total < maxiter) {
+    const int Ra = (int)active.size();
+    GMG_CUDA(cudaMemcpyAsync(idx.p, active.data(), sizeof(int) * Ra, cudaMemcpyHostToDevice, s));
+    Vec bA = bb.with_rhs(Ra), xA = xx.with_rhs(Ra);
+    GMG_TRY(vec_gather(Bfull, idx.as<int>(), bA, s));
+    GMG_TRY(vec_gather(Xfull, idx.as<int>(), xA, s));
+    Krylov K;
+    K.V0 = V0.with_rhs(Ra);
+    K.Z0 = Z0.with_rhs(Ra);
+    K.w = w.with_rhs(Ra);
+    K.t = t64.with_rhs(Ra);
+    K.tz = tz.with_rhs(Ra);
+    auto pc = [h, s, &tz, Ra, zp](const Vec& in, Vec& out, const Vec&) -> gmg_status {
+      // in: FP64 Krylov vector; out: Z direction in the preconditioner precision
+      Vec tin = tz.with_rhs(Ra);
+      if (zp != GMG_F64) {
+        GMG_TRY(vec_convert(in, tin, s));
+        return kcycle(h, 0, tin, out, s);
+      }
+      return kcycle(h, 0, in, out, s);
+    };
+    int it = 0;
+    std::vector<double> rr;
+    GMG_TRY(fgmres(h, 0, bA, xA, K, m, std::min(m, maxiter - total), tol, pc, true, &it, &rr, s));
+    GMG_TRY(vec_scatter(xA, idx.as<int>(), Xfull, s));
+    total += std::max(it, 1);
+    // true residuals of the batch decide who stays active
+    Vec rA = w.with_rhs(Ra);
+    GMG_TRY(apply_op(h, 0, xA, rA, s));
+    std::vector<zc> one(Ra, 1.0), mone(Ra, -1.0), rn, bn2;
+    GMG_TRY(axpby_h(h, one, bA, mone, rA, s));
+    GMG_TRY(dots(h, rA, 1, 0, rA, rn, s));
+    std::vector<int> still;
+    for (int k = 0; k < Ra; ++k) {
+      const int r = active[k];
+      relres[r] = std::sqrt(std::max(rn[k].real(), 0.0) / std::max(bnz[r].real(), 1e-300));
+      if (relres[r] > tol) still.push_back(r);
+    }
+    if (it == 0 && still.size() == active.size()) break;  // no progress possible
+    active.swap(still);
+  }
+  GMG_CUDA(cudaStreamSynchronize(s));
+  double mx = 0;
+  for (double v : relres) mx = std::max(mx, v);
+  if (iters_out) *iters_out = total;
+  if (max_relres) *max_relres = mx;
+  if (mx > tol) return fail(GMG_ERR_NOT_CONVERGED, "gmg_mg_solve: not converged within maxiter");
+  return GMG_OK;
+}
+
+extern "C" gmg_status gmg_mg_level(gmg_mg* h, int level, gmg_coarse** op, gmg_agg** agg) {
+  GMG_CHECK(h && level >= 0 && level < (int)h->L.size(), GMG_ERR_ARGUMENT, "gmg_mg_level: bad level");
+  if (op) *op = h->L[level]->c;
+  if (agg) *agg = h->L[level]->agg;
+  return GMG_OK;
+}

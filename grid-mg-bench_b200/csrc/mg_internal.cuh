@@ -1,0 +1,57 @@
+// mg_internal.cuh -- vectors and per-RHS kernels shared by the multigrid solvers.
+#pragma once
+
+#include "gmg_internal.cuh"
+
+namespace gmg {
+
+// A device field [V][R][dof] complex of precision prec (GMG_F64 / GMG_F32).
+struct Vec {
+  void* p = nullptr;
+  int64_t V = 0;
+  int R = 0;
+  int dof = 0;
+  int prec = GMG_F64;
+  int64_t elems() const { return V * (int64_t)R * dof; }
+  size_t esize() const { return prec == GMG_F64 ? 16 : 8; }
+  size_t bytes() const { return (size_t)elems() * esize(); }
+  // the first R' right-hand sides of a buffer laid out for R' RHS (compacted batches)
+  Vec with_rhs(int r) const {
+    Vec v = *this;
+    v.R = r;
+    return v;
+  }
+};
+
+// Owned device field.
+struct VecBuf : Vec {
+  DevBuf buf;
+  gmg_status alloc(int64_t V_, int R_, int dof_, int prec_) {
+    V = V_;
+    R = R_;
+    dof = dof_;
+    prec = prec_;
+    GMG_TRY(buf.alloc(bytes()));
+    p = buf.p;
+    return GMG_OK;
+  }
+};
+
+// out[j*R + r] = <X_j(r), Y(r)> for j < nx, X_j = X0 + j * xstride_elems (complex elements)
+gmg_status vec_multidot(const Vec& X0, int nx, int64_t xstride_elems, const Vec& Y, double2* out_dev, const int* mask,
+                        cudaStream_t s);
+// Y(r) += sum_j a[j*R + r] X_j(r)
+gmg_status vec_multiaxpy(const double2* a_dev, const Vec& X0, int nx, int64_t xstride_elems, Vec& Y, cudaStream_t s);
+// Y(r) = a[r] X(r) + b[r] Y(r)
+gmg_status vec_axpby(const double2* a_dev, const Vec& X, const double2* b_dev, Vec& Y, cudaStream_t s);
+// Y = X with a precision conversion
+gmg_status vec_convert(const Vec& X, Vec& Y, cudaStream_t s);
+// basis [2R][V][dof] (FP64) from X [V][R][dof] by chiral doubling
+gmg_status vec_chiral_double(const Vec& X, double* basis_dev, cudaStream_t s);
+// dst(r') = src(idx[r']) (gather) / dst(idx[r']) = src(r') (scatter), idx on the device
+gmg_status vec_gather(const Vec& src, const int* idx, Vec& dst, cudaStream_t s);
+gmg_status vec_scatter(const Vec& src, const int* idx, Vec& dst, cudaStream_t s);
+// seeded unit-Gaussian field (re, im ~ N(0, 1/2))
+gmg_status vec_gaussian(Vec& X, uint64_t seed, cudaStream_t s);
+
+}  // namespace gmg

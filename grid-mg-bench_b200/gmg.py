@@ -251,6 +251,12 @@ class WilsonClover:
             self._h = None
 
     def set_gauge(self, U):
+        if isinstance(U, torch.Tensor):
+            u = U.to(torch.complex128).contiguous()
+            assert tuple(u.shape) == (self.V, 4, 3, 3)
+            _chk(lib().gmg_wilson_set_gauge(self._h, _ptr(u), 1 if u.is_cuda else 0, _stream()))
+            torch.cuda.current_stream().synchronize()
+            return
         u = np.ascontiguousarray(U, dtype=np.complex128)
         assert u.shape == (self.V, 4, 3, 3)
         _chk(lib().gmg_wilson_set_gauge(self._h, u.ctypes.data_as(ctypes.c_void_p), 0, _stream()))
@@ -278,6 +284,61 @@ class WilsonClover:
 
     def Mdir(self, inp, out, d, disp):
         return self.apply(OP_MDIR, inp, out, d, disp)
+
+
+class MGParams(ctypes.Structure):
+    _fields_ = [("nlevels", ctypes.c_int), ("block", (ctypes.c_int * 4) * 2), ("nvec", ctypes.c_int * 2),
+                ("setup_iters", ctypes.c_int), ("smoother_iters", ctypes.c_int), ("wrapper_iters", ctypes.c_int),
+                ("wrapper_tol", ctypes.c_double), ("coarsest_iters", ctypes.c_int), ("coarsest_tol", ctypes.c_double),
+                ("coarsest_restart", ctypes.c_int), ("outer_restart", ctypes.c_int), ("prec", ctypes.c_int),
+                ("seed", ctypes.c_uint64)]
+
+
+class MultiGrid:
+    """MG-preconditioned FGMRES solve of the fine Wilson-clover operator (MultiGridPreconditioner)."""
+
+    def __init__(self, fine, max_rhs, **params):
+        p = MGParams()
+        _chk(lib().gmg_mg_params_default(ctypes.byref(p)))
+        for k, v in params.items():
+            if k == "block":
+                for i, blk in enumerate(v):
+                    for d in range(4):
+                        p.block[i][d] = blk[d]
+            elif k == "nvec":
+                for i, n in enumerate(v):
+                    p.nvec[i] = n
+            elif k == "prec":
+                p.prec = PREC.get(v, v)
+            else:
+                setattr(p, k, v)
+        self.params = p
+        self.fine = fine
+        h = ctypes.c_void_p()
+        _chk(lib().gmg_mg_create(fine._h, ctypes.byref(p), int(max_rhs), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.gmg_mg_destroy(self._h)
+            self._h = None
+
+    def setup(self):
+        _chk(lib().gmg_mg_setup(self._h, _stream()))
+
+    def solve(self, b, x, tol=1e-10, maxiter=500):
+        """b, x: complex128 CUDA tensors [V, nrhs, 12]; returns (outer iterations, max relative residual)."""
+        _check_vec(b, self.fine.V, 12, "b")
+        _check_vec(x, self.fine.V, 12, "x")
+        it, rr = ctypes.c_int(), ctypes.c_double()
+        _chk(lib().gmg_mg_solve(self._h, b.shape[1], _ptr(b), _ptr(x), ctypes.c_double(tol), int(maxiter),
+                                ctypes.byref(it), ctypes.byref(rr), _stream()))
+        return it.value, rr.value
+
+    def level(self, l):
+        op, ag = ctypes.c_void_p(), ctypes.c_void_p()
+        _chk(lib().gmg_mg_level(self._h, l, ctypes.byref(op), ctypes.byref(ag)))
+        return op, ag
 
 
 def lut_build(fine_dims, coarse_dims, mask_kind=-1):

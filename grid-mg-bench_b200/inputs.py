@@ -112,3 +112,32 @@ def random_links(dims, N, r, scale=None, g5_structure=True, diag_shift=0.0):
     if diag_shift:
         A[8] += diag_shift * np.eye(N)[None]
     return A
+
+
+# ----------------------------------------------------------------------------
+# Device-side generators for the large (32^4) configurations, seeded per stream.
+# Same distributions as above, drawn with torch's Philox generator on the GPU.
+# ----------------------------------------------------------------------------
+def torch_gaussian(shape, seed, device="cuda", dtype=None):
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    re = torch.randn(tuple(shape), generator=g, device=device, dtype=torch.float64)
+    im = torch.randn(tuple(shape), generator=g, device=device, dtype=torch.float64)
+    z = torch.complex(re, im) * (0.5 ** 0.5)
+    return z if dtype is None else z.to(dtype)
+
+
+def torch_smooth_gauge(dims, seed, eps, device="cuda"):
+    """U = exp(i eps H) per link, H traceless Hermitian with Gaussian entries -> [V][4][3][3] complex128."""
+    import torch
+
+    n = vol(dims) * 4
+    a = torch_gaussian((n, 3, 3), seed, device)
+    h = 0.5 * (a + a.conj().transpose(-1, -2))
+    tr = torch.diagonal(h, dim1=-2, dim2=-1).sum(-1) / 3.0
+    h = h - tr[:, None, None] * torch.eye(3, dtype=h.dtype, device=device)
+    w, v = torch.linalg.eigh(h)
+    u = (v * torch.exp(1j * eps * w)[:, None, :]) @ v.conj().transpose(-1, -2)
+    return u.reshape(vol(dims), 4, 3, 3).contiguous()

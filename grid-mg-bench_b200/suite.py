@@ -1,0 +1,198 @@
+"""Per-row measurements of the hot path (run by `bench.py --suite`).
+
+One JSON line per row, each with achieved rates against the measured
+roofline (MEASURED_PEAKS.json) and the kernel time taken from CUDA events on
+the launching stream.  Inputs are seeded synthetic fields with the
+configurations' shapes (coarse links with the gamma5-hermitian structure,
+unit-Gaussian vectors, smooth gauge U = exp(i eps H)).
+
+  C1  coarse M, single RHS, FP64: coarse 4^4, nbasis 24
+  C3  block project / promote (FP64, FP32) and orthonormalise (FP64):
+      fine 32^4, nbasis 32, 32 RHS, 4^4 blocks
+  C4  CoarsenOperator 32^4 -> 8^4 (nbasis 40, Wilson-clover m=-0.3, csw 1,
+      eps 0.3), then coarse-of-coarse 8^4 -> 4^4 (2^4 blocks, nbasis 40)
+  W   fine Wilson-clover M on 32^4, 1 and 12 RHS, FP64 and FP32
+"""
+import ctypes
+import json
+import os
+import time
+
+import numpy as np
+import torch
+
+import gmg
+import inputs
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+L2_FLUSH = 256 << 20
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Timer:
+    """Per-call CUDA-event timing on the current stream with an L2 flush before each call."""
+
+    def __init__(self):
+        self.flush = torch.empty(L2_FLUSH // 4, dtype=torch.float32, device="cuda")
+
+    def run(self, fn, reps=5, warm=2, flush=True):
+        for _ in range(warm):
+            fn()
+        s = torch.cuda.current_stream()
+        tot = 0.0
+        for k in range(reps):
+            if flush:
+                self.flush.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            fn()
+            b.record(s)
+            b.synchronize()
+            tot += a.elapsed_time(b)
+        return tot / reps * 1e-3  # seconds per call
+
+
+def kernel_avg(name):
+    ms, n = ctypes.c_double(), ctypes.c_int64()
+    gmg.lib().gmg_profile_read(name.encode(), ctypes.byref(ms), ctypes.byref(n))
+    return (ms.value / n.value * 1e-3) if n.value else None, n.value
+
+
+def line(row, **kw):
+    d = {"row": row}
+    d.update(kw)
+    print(json.dumps(d), flush=True)
+
+
+def c1(T, hbm):
+    dims, N = (4, 4, 4, 4), 24
+    A = inputs.random_links(dims, N, inputs.rng(stream=501))
+    x = torch.from_numpy(inputs.gaussian_field((256, 1, N), inputs.rng(stream=502))).cuda()
+    cm = gmg.CoarsenedMatrix(dims, N)
+    cm.set_links(A)
+    out = torch.zeros_like(x)
+    flops = 256 * 9 * 8 * N * N
+    byts = (9 * N * N + 2 * N) * 16 * 256
+    t_cold = T.run(lambda: cm.M(x, out), reps=50)
+    t_warm = T.run(lambda: cm.M(x, out), reps=200, flush=False)
+    line("C1 coarse M single RHS FP64 (4^4, nbasis 24)", us_l2_flushed=t_cold * 1e6, us_l2_warm=t_warm * 1e6,
+         gflops_flushed=flops / t_cold / 1e9, gbs_flushed=byts / t_cold / 1e9,
+         frac_hbm_flushed=byts / t_cold / 1e9 / hbm, algorithmic_bytes=byts, algorithmic_flops=flops,
+         note="launch-latency bound: 21 MB of links, 10.6 MFLOP")
+
+
+def c3(T, hbm):
+    fd, cd, N, R = (32, 32, 32, 32), (8, 8, 8, 8), 32, 32
+    Vf, Vc = 32 ** 4, 8 ** 4
+    half = inputs.torch_gaussian((N // 2, Vf, 12), 601)
+    B = torch.zeros((N, Vf, 12), dtype=torch.complex128, device="cuda")
+    B[: N // 2, :, :6] = half[:, :, :6]  # chiral doubling: upper / lower spin halves
+    B[N // 2:, :, 6:] = half[:, :, 6:]
+    del half
+    ag = gmg.Aggregation(fd, cd, 12, N)
+    ag.set_basis(B)
+    del B
+    torch.cuda.empty_cache()
+    t_ortho = T.run(lambda: ag.Orthogonalise(passes=1), reps=2, warm=1)
+    err = ag.CheckOrthogonal()
+    f64 = inputs.torch_gaussian((Vf, R, 12), 602)
+    c64 = torch.zeros((Vc, R, N), dtype=torch.complex128, device="cuda")
+    flops = 8.0 * Vf * 12 * N * R
+    b64 = (N * Vf * 12 + Vf * R * 12 + Vc * R * N) * 16
+    res = {}
+    gmg.lib().gmg_profile_enable(1)
+    t = T.run(lambda: ag.ProjectToSubspace(f64, c64), reps=3, warm=1)
+    res["project_f64"] = (t, kernel_avg("project")[0], b64)
+    t = T.run(lambda: ag.PromoteFromSubspace(c64, f64), reps=3, warm=1)
+    res["promote_f64"] = (t, kernel_avg("promote")[0], b64)
+    f32 = f64.to(torch.complex64)
+    del f64
+    c32 = c64.to(torch.complex64)
+    b32 = b64 // 2
+    t = T.run(lambda: ag.ProjectToSubspace(f32, c32), reps=3, warm=1)
+    res["project_f32"] = (t, kernel_avg("project")[0], b32)
+    t = T.run(lambda: ag.PromoteFromSubspace(c32, f32), reps=3, warm=1)
+    res["promote_f32"] = (t, kernel_avg("promote")[0], b32)
+    gmg.lib().gmg_profile_enable(0)
+    out = {k: {"ms": v[0] * 1e3, "tflops": flops / v[0] / 1e12, "gbs": v[2] / v[0] / 1e9,
+               "frac_hbm": v[2] / v[0] / 1e9 / hbm} for k, v in res.items()}
+    line("C3 block project / promote (32^4, nbasis 32, 32 RHS, 4^4 blocks)", results=out,
+         orthonormalise_ms=t_ortho * 1e3, orthonormalise_max_err=err, algorithmic_flops=flops,
+         algorithmic_bytes_f64=b64)
+
+
+def wilson_and_c4(T, hbm):
+    fd = (32, 32, 32, 32)
+    V = 32 ** 4
+    U = inputs.torch_smooth_gauge(fd, 701, 0.3)
+    w = gmg.WilsonClover(fd, -0.3, 1.0, antiperiodic=True)
+    w.set_gauge(U)
+    del U
+    res = {}
+    for R in (1, 12):
+        for dt, cb in ((torch.complex128, 16), (torch.complex64, 8)):
+            x = inputs.torch_gaussian((V, R, 12), 702, dtype=dt)
+            y = torch.zeros_like(x)
+            t = T.run(lambda: w.M(x, y), reps=5)
+            byts = V * (2 * 12 * R + 36 + 72) * cb  # in + out per RHS, gauge + clover once
+            res[f"R{R}_{'f64' if cb == 16 else 'f32'}"] = {
+                "ms": t * 1e3, "gflops": 1824.0 * V * R / t / 1e9, "gbs": byts / t / 1e9,
+                "frac_hbm": byts / t / 1e9 / hbm}
+            del x, y
+    line("W fine Wilson-clover M (32^4)", results=res,
+         note="flops: 1824 per site per RHS (reference model); bytes: spinor in+out per RHS, gauge 36 + clover 72 complex per site")
+    # C4: CoarsenOperator 32^4 -> 8^4, nbasis 40, then 8^4 -> 4^4
+    N = 40
+    half = inputs.torch_gaussian((N // 2, V, 12), 703)
+    B = torch.zeros((N, V, 12), dtype=torch.complex128, device="cuda")
+    B[: N // 2, :, :6] = half[:, :, :6]
+    B[N // 2:, :, 6:] = half[:, :, 6:]
+    del half
+    ag = gmg.Aggregation(fd, (8, 8, 8, 8), 12, N)
+    ag.set_basis(B)
+    del B
+    torch.cuda.empty_cache()
+    ag.Orthogonalise(passes=1)
+    cm = gmg.CoarsenedMatrix((8, 8, 8, 8), N)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    cm.CoarsenOperator(ag, w)
+    torch.cuda.synchronize()
+    t_c4 = time.perf_counter() - t0
+    h2 = inputs.torch_gaussian((N // 2, 4096, N), 704)
+    B2 = torch.zeros((N, 4096, N), dtype=torch.complex128, device="cuda")
+    B2[: N // 2, :, : N // 2] = h2[:, :, : N // 2]
+    B2[N // 2:, :, N // 2:] = h2[:, :, N // 2:]
+    ag2 = gmg.Aggregation((8, 8, 8, 8), (4, 4, 4, 4), N, N)
+    ag2.set_basis(B2)
+    ag2.Orthogonalise(passes=1)
+    cc = gmg.CoarsenedMatrix((4, 4, 4, 4), N)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    cc.CoarsenOperator(ag2, cm)
+    torch.cuda.synchronize()
+    t_cc = time.perf_counter() - t0
+    proj_flops = 2 * 8.0 * 3072 * N * N * 4096
+    fine_flops = N * V * (4 * 144 + 2 * 1824) * 1.0
+    line("C4 CoarsenOperator 32^4 -> 8^4 (nbasis 40) and 8^4 -> 4^4", seconds=t_c4, coarse_of_coarse_seconds=t_cc,
+         algorithmic_flops=proj_flops + fine_flops, achieved_tflops=(proj_flops + fine_flops) / t_c4 / 1e12,
+         note="FP64; unfused backward Mdir + masked projections per batch of basis vectors")
+
+
+def run():
+    torch.cuda.set_device(0)
+    hbm, src = peaks()
+    T = Timer()
+    c1(T, hbm)
+    c3(T, hbm)
+    torch.cuda.empty_cache()
+    wilson_and_c4(T, hbm)
+    line("peaks", hbm_gbs=hbm, source=src)

@@ -199,6 +199,48 @@ gmg_status gmg_coarsen_wilson(gmg_coarse* out, gmg_agg* agg, gmg_wilson* fine, g
 gmg_status gmg_coarsen_coarse(gmg_coarse* out, gmg_agg* agg, gmg_coarse* fine, gmg_stream s);
 
 /* ------------------------------------------------------------------------ */
+/* Multigrid-preconditioned solve                                            */
+/* MultiGridPreconditioner (MultigridPreconditioner.h:44-660, createMGInstance */
+/* :665-686) with the outer FGMRES of Test_wilsonclover_mg[_mp].cc            */
+/* ------------------------------------------------------------------------ */
+typedef struct gmg_mg gmg_mg;
+
+typedef struct {
+  int nlevels;           /* 2 or 3 (fine + coarse levels), MultiGridParams::nLevels */
+  int block[2][4];       /* aggregation blocks of the transitions 0->1, 1->2 (blockSizes) */
+  int nvec[2];           /* test vectors per transition; nbasis = 2 * nvec (chiral doubling) */
+  int setup_iters;       /* GMRES(10) iterations relaxing the test vectors (setupSolverParams) */
+  int smoother_iters;    /* MR post-smoothing iterations per level */
+  int wrapper_iters;     /* K-cycle FGMRES iterations on intermediate levels (wrapperSolverParams) */
+  double wrapper_tol;
+  int coarsest_iters;    /* GMRES iterations on the coarsest level (coarsestSolverParams) */
+  double coarsest_tol;
+  int coarsest_restart;
+  int outer_restart;     /* outer FGMRES restart length */
+  gmg_prec prec;         /* F64: all FP64; F32: FP32 preconditioner; BF16: FP32 preconditioner with
+                            tensor-core coarse stencils.  The outer FGMRES is always FP64. */
+  uint64_t seed;         /* test-vector seed */
+} gmg_mg_params;
+
+/* Defaults of MultiGridParams (MultigridParams.h:95-113) adapted to the MR smoother. */
+gmg_status gmg_mg_params_default(gmg_mg_params* p);
+/* Levels over the fine operator; solves take up to max_rhs right-hand sides at once. */
+gmg_status gmg_mg_create(gmg_wilson* fine, const gmg_mg_params* p, int max_rhs, gmg_mg** h);
+gmg_status gmg_mg_destroy(gmg_mg* h);
+/* initialSetup (MultigridPreconditioner.h:165-211): test vectors, chiral doubling,
+   block orthonormalisation and CoarsenOperator on every level.  Synchronises. */
+gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream s);
+/* Solve D x = b for nrhs right-hand sides with FP64 FGMRES + MG preconditioner to
+   per-RHS relative residual |b - D x| / |b| <= tol.  b, x: device FP64
+   [V][nrhs][12]; x holds the initial guess.  Converged RHS drop out at every
+   outer restart.  Synchronises; GMG_ERR_NOT_CONVERGED if maxiter is reached. */
+gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double* x, double tol, int maxiter, int* iters,
+                        double* max_relres, gmg_stream s);
+/* The coarse operator of level > 0 and the aggregation from level to level+1
+   (runChecks, MultigridPreconditioner.h:311-446); either may be null. */
+gmg_status gmg_mg_level(gmg_mg* h, int level, gmg_coarse** op, gmg_agg** agg);
+
+/* ------------------------------------------------------------------------ */
 /* Rework layout maps (Layout_converters.h:33-139): flat basis index          */
 /* n = s*Nc_c + c <-> (s, c).  Device links [V][N][N], inverse=1 for spin->flat */
 /* ------------------------------------------------------------------------ */
