@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--form", choices=["bf16", "f16"], default="bf16")
     ap.add_argument("--suite", action="store_true",
                     help="per-row measurements (C1, C3, C4, fine operator) instead of the bench line")
+    ap.add_argument("--rows", default="c1,c3,w_c4,c5", help="suite rows to run")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed applies (for profiler captures); prints a short line")
     return ap.parse_args()
@@ -207,7 +208,7 @@ def main():
     if args.suite:
         import suite
 
-        suite.run()
+        suite.run(tuple(args.rows.split(",")))
         return 0
 
     import torch

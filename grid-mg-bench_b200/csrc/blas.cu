@@ -71,13 +71,15 @@ __global__ void __launch_bounds__(256) multidot_kernel(const typename C2<T>::t* 
 template <class TX, class T>
 __global__ void multiaxpy_kernel(const double2* __restrict__ a, const typename C2<TX>::t* __restrict__ X,
                                  int64_t xstride, int nx, typename C2<T>::t* __restrict__ Y, int64_t V, int R,
-                                 int dof) {
+                                 int dof, double sgn) {
   const int64_t n = V * R * dof;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     const int r = (int)((e / dof) % R);
     double yr = Y[e].x, yi = Y[e].y;
     for (int j = 0; j < nx; ++j) {
-      const double2 c = a[j * R + r];
+      double2 c = a[j * R + r];
+      c.x *= sgn;
+      c.y *= sgn;
       if (c.x == 0.0 && c.y == 0.0) continue;
       const typename C2<TX>::t x = X[j * xstride + e];
       yr += c.x * x.x - c.y * x.y;
@@ -154,20 +156,21 @@ gmg_status vec_multidot(const Vec& X0, int nx, int64_t xstride_elems, const Vec&
   return GMG_OK;
 }
 
-gmg_status vec_multiaxpy(const double2* a_dev, const Vec& X0, int nx, int64_t xstride_elems, Vec& Y, cudaStream_t s) {
+gmg_status vec_multiaxpy(const double2* a_dev, const Vec& X0, int nx, int64_t xstride_elems, Vec& Y, cudaStream_t s,
+                         double sgn) {
   const int g = blas::grid1(Y.elems());
   if (Y.prec == GMG_F64 && X0.prec == GMG_F64)
     blas::multiaxpy_kernel<double, double><<<g, 256, 0, s>>>(a_dev, (const double2*)X0.p, xstride_elems, nx,
-                                                             (double2*)Y.p, Y.V, Y.R, Y.dof);
+                                                             (double2*)Y.p, Y.V, Y.R, Y.dof, sgn);
   else if (Y.prec == GMG_F64)
     blas::multiaxpy_kernel<float, double><<<g, 256, 0, s>>>(a_dev, (const float2*)X0.p, xstride_elems, nx,
-                                                            (double2*)Y.p, Y.V, Y.R, Y.dof);
+                                                            (double2*)Y.p, Y.V, Y.R, Y.dof, sgn);
   else if (X0.prec == GMG_F32)
     blas::multiaxpy_kernel<float, float><<<g, 256, 0, s>>>(a_dev, (const float2*)X0.p, xstride_elems, nx,
-                                                           (float2*)Y.p, Y.V, Y.R, Y.dof);
+                                                           (float2*)Y.p, Y.V, Y.R, Y.dof, sgn);
   else
     blas::multiaxpy_kernel<double, float><<<g, 256, 0, s>>>(a_dev, (const double2*)X0.p, xstride_elems, nx,
-                                                            (float2*)Y.p, Y.V, Y.R, Y.dof);
+                                                            (float2*)Y.p, Y.V, Y.R, Y.dof, sgn);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
@@ -236,7 +239,80 @@ __global__ void gaussian_kernel(typename C2<T>::t* __restrict__ X, int64_t n, ui
   }
 }
 
+// Y(r) = X(r) / sqrt(n[r].x)  (0 where n[r].x == 0); n holds <w, w> from a multidot
+template <class T>
+__global__ void scale_inv_norm_kernel(const double2* __restrict__ n, const typename C2<T>::t* __restrict__ X,
+                                      typename C2<T>::t* __restrict__ Y, int64_t V, int R, int dof) {
+  const int64_t tot = V * R * dof;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)((e / dof) % R);
+    const double nn = n[r].x;
+    const double sc = nn > 0.0 ? rsqrt(nn) : 0.0;
+    Y[e].x = (T)(sc * X[e].x);
+    Y[e].y = (T)(sc * X[e].y);
+  }
+}
+
+// minimal-residual step with per-RHS alpha = <Ar, r> / <Ar, Ar> read from the device:
+// x += alpha r, r -= alpha Ar
+template <class T>
+__global__ void mr_update_kernel(const double2* __restrict__ d1, const double2* __restrict__ d2,
+                                 typename C2<T>::t* __restrict__ x, typename C2<T>::t* __restrict__ r,
+                                 const typename C2<T>::t* __restrict__ Ar, int64_t V, int R, int dof) {
+  const int64_t tot = V * R * dof;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)((e / dof) % R);
+    const double den = d2[k].x;
+    const double ar = den > 0.0 ? d1[k].x / den : 0.0, ai = den > 0.0 ? d1[k].y / den : 0.0;
+    const double rr = r[e].x, ri = r[e].y, qr = Ar[e].x, qi = Ar[e].y;
+    x[e].x = (T)(x[e].x + ar * rr - ai * ri);
+    x[e].y = (T)(x[e].y + ar * ri + ai * rr);
+    r[e].x = (T)(rr - (ar * qr - ai * qi));
+    r[e].y = (T)(ri - (ar * qi + ai * qr));
+  }
+}
+
+// Y(r) = X(r) - Y(r)   (residual from b and A x)
+template <class T>
+__global__ void xmy_kernel(const typename C2<T>::t* __restrict__ X, typename C2<T>::t* __restrict__ Y, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    Y[e].x = X[e].x - Y[e].x;
+    Y[e].y = X[e].y - Y[e].y;
+  }
+}
+
 }  // namespace blas
+
+gmg_status vec_scale_inv_norm(const double2* n_dev, const Vec& X, Vec& Y, cudaStream_t s) {
+  const int g = blas::grid1(Y.elems());
+  if (Y.prec == GMG_F64)
+    blas::scale_inv_norm_kernel<double><<<g, 256, 0, s>>>(n_dev, (const double2*)X.p, (double2*)Y.p, Y.V, Y.R, Y.dof);
+  else
+    blas::scale_inv_norm_kernel<float><<<g, 256, 0, s>>>(n_dev, (const float2*)X.p, (float2*)Y.p, Y.V, Y.R, Y.dof);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s) {
+  const int g = blas::grid1(x.elems());
+  if (x.prec == GMG_F64)
+    blas::mr_update_kernel<double><<<g, 256, 0, s>>>(d1, d2, (double2*)x.p, (double2*)r.p, (const double2*)Ar.p, x.V,
+                                                     x.R, x.dof);
+  else
+    blas::mr_update_kernel<float><<<g, 256, 0, s>>>(d1, d2, (float2*)x.p, (float2*)r.p, (const float2*)Ar.p, x.V, x.R,
+                                                    x.dof);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s) {
+  const int64_t n = Y.elems();
+  const int g = blas::grid1(n);
+  if (Y.prec == GMG_F64) blas::xmy_kernel<double><<<g, 256, 0, s>>>((const double2*)X.p, (double2*)Y.p, n);
+  else blas::xmy_kernel<float><<<g, 256, 0, s>>>((const float2*)X.p, (float2*)Y.p, n);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
 
 gmg_status vec_gather(const Vec& src, const int* idx, Vec& dst, cudaStream_t s) {
   const int64_t n = dst.elems();

@@ -6,30 +6,33 @@
 //
 //     out(x)[r][b] = sum_p sum_bb A_p(x)[b][bb] in(nbr_p(x))[r][bb]
 //
-// decomposed into one real MMA per point and K-step:
+// decomposed into one real MMA per point and K-step, with the link rows
+// interleaved (row 2b = Re A[b][.], row 2b+1 = Im A[b][.]):
 //
-//     D (2N x 2R) += [Ar; Ai] (2N x N)  .  [Xr^T | Xi^T] (N x 2R)
-//     out_r = D[b][r] - D[N+b][R+r],   out_i = D[N+b][r] + D[b][R+r]
+//     D (2N x 2R) += [Re A; Im A] (2N x N)  .  [Xr^T | Xi^T] (N x 2R)
+//     out_r = D[2b][r] - D[2b+1][R+r],   out_i = D[2b][R+r] + D[2b+1][r]
 //
 // so the links are read once in their compact (re, im) form and every
 // operand is a straight copy from HBM.  BF16 or FP16 operands, FP32
 // accumulation in tensor memory (TMEM), tcgen05.mma issued by one thread.
 //
-// Kernel structure (one persistent CTA per SM, 6 warps):
-//   warp 0      producer: for each (site, point) stage one bulk copy of the
-//               link tile and one of the neighbour's packed vector tile into
-//               shared memory (cp.async.bulk + mbarrier transaction counts)
-//   warp 1      TMEM allocator + MMA issuer (one elected thread); accumulates
-//               the 9 points of a site into one of two TMEM buffers
-//   warps 2-5   epilogue: tcgen05.ld the accumulator, recombine (re, im) via
-//               shared memory, apply G5C for Mdag, write FP32 output
+// Kernel structure (one persistent CTA per SM, 11 warps):
+//   warps 0, 10  producers: stage-sequence numbers alternate between them; one
+//                stage = 3 (or 1) stencil points of one site: one bulk copy of
+//                the points' contiguous link tiles and one per neighbour tile
+//                (cp.async.bulk + mbarrier transaction counts)
+//   warp 1       TMEM allocator + MMA issuer (one elected thread); accumulates
+//                the 9 points of a site into one of up to 4 TMEM buffers
+//   warps 2-9    epilogue, two warps per TMEM sub-partition: tcgen05.ld the
+//                accumulator, recombine (re, im) with one lane-pair shuffle,
+//                apply G5C for Mdag, write FP32 output
 // Every mbarrier wait is bounded in time: on time-out the kernel records an
 // error code, stops issuing work, drains its own copies and MMAs, frees TMEM
 // and returns.
 //
 // Global layouts (prepared once per link set / per apply):
 //   links  [V][9][Kc][Mp][8]   halves, Kc = ceil16(N)/8 K-chunks, Mp = 64 or
-//          128 padded rows: rows m < N = Re A[m][.], N <= m < 2N = Im A[m-N][.]
+//          128 rows, interleaved as above, zero-padded beyond 2N
 //   packed [V][Kc][2Rp][8]     halves: rows n < Rp = Re in[r=n][.],
 //          Rp <= n < 2Rp = Im in[r=n-Rp][.]  (Rp = R rounded up to 16)
 // Both are the canonical no-swizzle K-major core-matrix layout
@@ -42,9 +45,10 @@ namespace gmg {
 
 namespace tc {
 
-constexpr int kWarps = 6;
+constexpr int kWarps = 11;  // producer, MMA issuer, 8 epilogue warps (two per TMEM sub-partition), producer
 constexpr int kThreads = kWarps * 32;
-constexpr int kAccBufs = 2;
+constexpr int kAccBufs = 4;  // TMEM accumulator buffers (fewer when 2*Rp columns do not fit 4 times)
+constexpr int kEpiThreads = 256;
 constexpr long long kTimeoutCycles = 4000000000LL;  // ~2 s at 2 GHz
 
 enum : int { ERR_NONE = 0, ERR_TIMEOUT_PRODUCER = 1, ERR_TIMEOUT_MMA = 2, ERR_TIMEOUT_EPILOGUE = 3 };
@@ -176,6 +180,31 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// two 16-column TMEM loads (real-part and imaginary-part columns), one wait
+__device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, float* va, float* vb) {
+  uint32_t a[16], b[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15}, [%16];"
+      : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3]), "=r"(a[4]), "=r"(a[5]), "=r"(a[6]), "=r"(a[7]),
+        "=r"(a[8]), "=r"(a[9]), "=r"(a[10]), "=r"(a[11]), "=r"(a[12]), "=r"(a[13]), "=r"(a[14]),
+        "=r"(a[15])
+      : "r"(ta));
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15}, [%16];"
+      : "=r"(b[0]), "=r"(b[1]), "=r"(b[2]), "=r"(b[3]), "=r"(b[4]), "=r"(b[5]), "=r"(b[6]), "=r"(b[7]),
+        "=r"(b[8]), "=r"(b[9]), "=r"(b[10]), "=r"(b[11]), "=r"(b[12]), "=r"(b[13]), "=r"(b[14]),
+        "=r"(b[15])
+      : "r"(tb));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    va[i] = __uint_as_float(a[i]);
+    vb[i] = __uint_as_float(b[i]);
+  }
+}
+
 struct Params {
   const uint16_t* links;   // [V][9][Kc][Mp][8]
   const uint16_t* packed;  // [V][Kc][2Rp][8]
@@ -207,11 +236,12 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
   uint64_t* drain = tempty + kAccBufs;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  int* nbr_s = reinterpret_cast<int*>(tmem_slot + 4);  // [32][9] neighbour indices of the producer
+  int* nbr_s = reinterpret_cast<int*>(tmem_slot + 4);  // [2][32][9] neighbour indices of the two producers
 
   const uint32_t acc_cols = 2 * P.Rp;
+  const int nacc = (int)min((uint32_t)kAccBufs, 512u / acc_cols);  // >= 2 since Rp <= 128
   uint32_t ncols_alloc = 32;
-  while (ncols_alloc < kAccBufs * acc_cols) ncols_alloc <<= 1;
+  while (ncols_alloc < nacc * acc_cols) ncols_alloc <<= 1;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < P.stages; ++s) {
@@ -220,7 +250,7 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
     }
     for (int a = 0; a < kAccBufs; ++a) {
       mbar_init(&tfull[a], 1);
-      mbar_init(&tempty[a], 128);
+      mbar_init(&tempty[a], kEpiThreads);
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -240,16 +270,18 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
   // sites of this CTA: blockIdx.x, blockIdx.x + gridDim.x, ...
   const int nsites = (P.V - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
 
-  if (warp == 0) {
-    // ------------------------------------------------------------ producer
-    // The warp stages the neighbour indices of 32 sites at a time in shared
-    // memory (one parallel load), so lane 0 never waits on a dependent global
-    // load between two stages.  One stage = pps consecutive stencil points of
-    // one site: one bulk copy of their (contiguous) link tiles and one per
-    // neighbour tile.
-    int stage = 0;
-    uint32_t phase = 0;
-    int issued = 0;
+  if (warp == 0 || warp == kWarps - 1) {
+    // ------------------------------------------------------------ producers
+    // Two producer warps fill alternate stages: stage-sequence number n (one
+    // per group of pps points of one site, in the order the MMA issuer
+    // consumes them) goes to producer n % 2, stage n % stages (stages is even).
+    // Each warp stages the neighbour indices of 32 sites at a time in its own
+    // shared-memory table (one parallel load), so its issuing lane never waits
+    // on a dependent global load between two stages.  One stage = one bulk copy
+    // of the pps (contiguous) link tiles and one per neighbour tile.
+    const int pid = warp == 0 ? 0 : 1;
+    int* my_nbr = nbr_s + pid * 32 * 9;
+    int64_t last = -1;
     bool stop = false;
     for (int i0 = 0; i0 < nsites && !stop; i0 += 32) {
       const int cnt = min(32, nsites - i0);
@@ -257,13 +289,17 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
       if (lane < cnt) {
         const int site = blockIdx.x + (i0 + lane) * gridDim.x;
 #pragma unroll
-        for (int p = 0; p < 9; ++p) nbr_s[lane * 9 + p] = __ldg(&P.nbr[(size_t)p * P.V + site]);
+        for (int p = 0; p < 9; ++p) my_nbr[lane * 9 + p] = __ldg(&P.nbr[(size_t)p * P.V + site]);
       }
       __syncwarp();
       if (lane == 0) {
         for (int j = 0; j < cnt && !stop; ++j) {
           const int site = blockIdx.x + (i0 + j) * gridDim.x;
           for (int g = 0; g < ngroups; ++g) {
+            const int64_t n = (int64_t)(i0 + j) * ngroups + g;
+            if ((int)(n & 1) != pid) continue;
+            const int stage = (int)(n % P.stages);
+            const uint32_t phase = (uint32_t)((n / P.stages) & 1);
             if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) {
               atomicCAS(P.err, 0, ERR_TIMEOUT_PRODUCER);
               *abort_flag = 1;
@@ -275,24 +311,21 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
             mbar_expect_tx(&full[stage], stage_bytes);
             bulk_g2s(st, P.links + ((size_t)site * 9 + pf) * (link_bytes / 2), pps * link_bytes, &full[stage]);
             for (int pp = 0; pp < pps; ++pp) {
-              const int nb = nbr_s[j * 9 + pf + pp];
+              const int nb = my_nbr[j * 9 + pf + pp];
               bulk_g2s(st + pps * link_bytes + pp * vec_bytes, P.packed + (size_t)nb * (vec_bytes / 2), vec_bytes,
                        &full[stage]);
             }
-            ++issued;
-            if (++stage == P.stages) { stage = 0; phase ^= 1; }
+            last = n;
           }
         }
       }
       stop = __shfl_sync(0xffffffffu, stop, 0);
     }
     if (lane == 0) {
-      // drain: wait for the copies of the last min(issued, stages) stages to land
-      int s = stage;
-      uint32_t ph = phase;
-      for (int k = 0; k < P.stages && k < issued; ++k) {
-        if (--s < 0) { s = P.stages - 1; ph ^= 1; }
-        mbar_drain(&full[s], ph);
+      // drain: wait for this producer's copies of the last `stages` sequence numbers to land
+      for (int64_t n = last; n >= 0 && n > last - P.stages; --n) {
+        if ((int)(n & 1) != pid) continue;
+        mbar_drain(&full[n % P.stages], (uint32_t)((n / P.stages) & 1));
       }
     }
   } else if (warp == 1) {
@@ -307,8 +340,8 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
       uint32_t phase = 0;
       bool ok = true;
       for (int i = 0; i < nsites && ok; ++i) {
-        const int acc = i & 1;
-        const uint32_t aphase = (uint32_t)(i >> 1) & 1;
+        const int acc = i % nacc;
+        const uint32_t aphase = (uint32_t)(i / nacc) & 1;
         if (!mbar_wait(&tempty[acc], aphase ^ 1, abort_flag)) { ok = false; break; }
         fence_after();
         const uint32_t dt = tmem_base + acc * acc_cols;
@@ -340,13 +373,15 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
       mbar_drain(drain, 0);
     }
   } else {
-    // ------------------------------------------------------------ epilogue (warps 2..5)
+    // ------------------------------------------------------------ epilogue (warps 2..9)
     // Link rows are interleaved (2b = Re A[b], 2b+1 = Im A[b]), so accumulator
     // rows 2b and 2b+1 sit in neighbouring lanes of one warp and the complex
     // recombination is one lane-pair exchange:
     //   out_r = D[2b][r] - D[2b+1][Rp+r],   out_i = D[2b][Rp+r] + D[2b+1][r]
     // The even lane writes r in [c, c+8) of every 16-column chunk, the odd lane [c+8, c+16).
+    // Two warps share each TMEM sub-partition and take alternate 16-column chunks.
     const int q = warp & 3;              // TMEM sub-partition of this warp
+    const int half = (warp - 2) >> 2;    // 0 or 1: which alternate chunks
     const int rows_per_warp = P.Mp / 4;  // 16 (M=64) or 32 (M=128)
     const int row = q * rows_per_warp + lane;
     const int b = row >> 1;
@@ -355,8 +390,8 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
     const float sg = (P.g5 && b >= P.N / 2) ? -1.f : 1.f;
     for (int i = 0; i < nsites; ++i) {
       const int site = blockIdx.x + i * gridDim.x;
-      const int acc = i & 1;
-      const uint32_t aphase = (uint32_t)(i >> 1) & 1;
+      const int acc = i % nacc;
+      const uint32_t aphase = (uint32_t)(i / nacc) & 1;
       const bool waited = mbar_wait(&tfull[acc], aphase, abort_flag);
       if (!__all_sync(0xffffffffu, waited)) {  // the warp leaves together
         if (!waited) atomicCAS(P.err, 0, ERR_TIMEOUT_EPILOGUE);
@@ -366,10 +401,9 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
       fence_after();
       const uint32_t ta = tmem_base + ((uint32_t)(32 * q) << 16) + acc * acc_cols;
       float2* orow = P.out + (size_t)site * P.nrhs * P.N + b;
-      for (int c = 0; c < P.Rp; c += 16) {
+      for (int c = 16 * half; c < P.Rp; c += 32) {
         float vr[16], vi[16];
-        tmem_ld16(ta + c, vr);
-        tmem_ld16(ta + P.Rp + c, vi);
+        tmem_ld16x2(ta + c, ta + P.Rp + c, vr, vi);
         float pr[8], pi[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -532,14 +566,14 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int p0, int
   const int Mp = 2 * N <= 64 ? 64 : 128;
   const int V = (int)h->dims.vol();
   const uint32_t per_point = (uint32_t)Kc * Mp * 16 + (uint32_t)Kc * 2 * Rp * 16;
-  const size_t fixed = 80 * 8 + 16 + 32 * 9 * 4;  // barriers (<= 2*32+5), TMEM slot + flag, neighbour table
+  const size_t fixed = 80 * 8 + 16 + 2 * 32 * 9 * 4;  // barriers (<= 2*32+9), TMEM slot + flag, neighbour tables
   const size_t budget = 227 * 1024 - fixed;
   const int npts = p1 - p0;
   int pps = (npts % 3 == 0 && budget / (3 * per_point) >= 4) ? 3 : 1;
   const uint32_t stage_bytes = pps * per_point;
-  const int stages = (int)std::min<size_t>(32, budget / stage_bytes);
+  const int stages = (int)std::min<size_t>(32, budget / stage_bytes) & ~1;  // even: two producers
   GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil: tile does not fit shared memory");
-  const size_t smem = (size_t)stages * stage_bytes + (size_t)(2 * stages + 2 * kAccBufs + 1) * 8 + 16 + 32 * 9 * 4;
+  const size_t smem = (size_t)stages * stage_bytes + (size_t)(2 * stages + 2 * kAccBufs + 1) * 8 + 16 + 2 * 32 * 9 * 4;
   GMG_CUDA(cudaFuncSetAttribute(coarse_mrhs_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 148;
   GMG_CUDA(cudaGetDevice(&dev));

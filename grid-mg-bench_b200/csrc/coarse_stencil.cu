@@ -188,6 +188,68 @@ static gmg_status launch_simt(const void* links, const int32_t* nbr, const void*
   return GMG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Single right-hand side (CoarsenedMatrixUpstream.h:572-597 with nrhs = 1).
+// The work per site is 9 GEMVs of N x N, too little for register tiling, and
+// the 4^4 lattices of the coarse levels have only 256 sites.  One CTA per site,
+// one thread per (point, row): the neighbour vectors are staged in shared
+// memory, each thread forms one row product from a contiguous link row, and
+// the 9 partial rows are summed in shared memory.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(576) coarse_1rhs_kernel(const typename cplx_t<T>::type* __restrict__ links,
+                                                          const int32_t* __restrict__ nbr,
+                                                          const typename cplx_t<T>::type* __restrict__ in,
+                                                          typename cplx_t<T>::type* __restrict__ out, int V, int N,
+                                                          int nrhs, int slot, int p0, int p1, int g5) {
+  typedef typename cplx_t<T>::type C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* X = reinterpret_cast<C*>(smem_raw);  // [9][N] neighbour vectors
+  C* part = X + 9 * N;                    // [9][N] partial rows
+  const int t = threadIdx.x;
+  const int p = t / N, b = t % N;  // blockDim = 9 N
+  const int half = N / 2;
+  for (int site = blockIdx.x; site < V; site += gridDim.x) {
+    if (p >= p0 && p < p1) {
+      const int nb = nbr[(int64_t)p * V + site];
+      C v = in[((int64_t)nb * nrhs + slot) * N + b];
+      if (g5 && b >= half) { v.x = -v.x; v.y = -v.y; }
+      X[p * N + b] = v;
+    }
+    __syncthreads();
+    C acc{0, 0};
+    if (p >= p0 && p < p1) {
+      const C* row = links + (((int64_t)site * 9 + p) * N + b) * N;
+      for (int bb = 0; bb < N; ++bb) acc = cmul_add(acc, row[bb], X[p * N + bb]);
+    }
+    part[p * N + b] = acc;
+    __syncthreads();
+    if (t < N) {
+      C o{0, 0};
+      for (int q = p0; q < p1; ++q) {
+        o.x += part[q * N + t].x;
+        o.y += part[q * N + t].y;
+      }
+      if (g5 && t >= half) { o.x = -o.x; o.y = -o.y; }
+      out[((int64_t)site * nrhs + slot) * N + t] = o;
+    }
+    __syncthreads();
+  }
+}
+
+template <class T>
+static gmg_status launch_1rhs(const void* links, const int32_t* nbr, const void* in, void* out, int V, int N,
+                              int nrhs, int slot, int p0, int p1, int g5, cudaStream_t s) {
+  typedef typename cplx_t<T>::type C;
+  const int threads = 9 * N;
+  const size_t smem = sizeof(C) * 18 * (size_t)N;
+  KernelTimer kt("coarse_simt", s);
+  coarse_1rhs_kernel<T><<<V, threads, smem, s>>>(reinterpret_cast<const C*>(links), nbr, reinterpret_cast<const C*>(in),
+                                                 reinterpret_cast<C*>(out), V, N, nrhs, slot, p0, p1, g5);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
 gmg_status coarse_apply_simt(gmg_coarse* h, int p0, int p1, bool g5, int compute, int vec_prec,
                              int nrhs, const void* in, void* out, const int32_t* active,
                              int n_active, cudaStream_t s) {
@@ -196,6 +258,12 @@ gmg_status coarse_apply_simt(gmg_coarse* h, int p0, int p1, bool g5, int compute
   const int R = active ? n_active : nrhs;
   if (R == 0) return GMG_OK;
   const int32_t* nbr = h->nbr.as<int32_t>();
+  if (R == 1 && !active && N <= 64) {
+    if (compute == GMG_F64 && vec_prec == GMG_F64)
+      return launch_1rhs<double>(h->links_d.p, nbr, in, out, V, N, nrhs, 0, p0, p1, g5, s);
+    if (compute == GMG_F32 && vec_prec == GMG_F32 && h->links_f_ok)
+      return launch_1rhs<float>(h->links_f.p, nbr, in, out, V, N, nrhs, 0, p0, p1, g5, s);
+  }
   if (compute == GMG_F64) {
     GMG_CHECK(vec_prec == GMG_F64, GMG_ERR_UNSUPPORTED, "F64 compute needs F64 vectors");
     if (R >= 4) return launch_simt<double, 4, 4>(h->links_d.p, nbr, in, out, V, N, nrhs, active, R, p0, p1, g5, s);

@@ -54,11 +54,13 @@ struct gmg_mg {
   gmg_wilson* fine = nullptr;
   int Rmax = 0;
   std::vector<gmg::MGLevel*> L;
-  gmg::DevBuf coef;  // device coefficients (double2)
-  std::vector<zc> hbuf;
+  gmg::DevBuf coef;        // device coefficients uploaded from the host (double2)
+  gmg::DevBuf dscr;        // device-only per-RHS scalars: dots, norms (double2)
+  double2* hpin = nullptr; // pinned host staging for coefficient transfers
   bool setup_done = false;
   ~gmg_mg() {
     for (auto* l : L) delete l;
+    if (hpin) cudaFreeHost(hpin);
   }
 };
 
@@ -74,31 +76,35 @@ gmg_status apply_op(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s) {
                           (gmg_stream)s);
 }
 
+constexpr int kScalars = 8192;  // double2 slots of h->coef, h->dscr and h->hpin
+
+// host <- n device scalars (one stream synchronisation)
+gmg_status download(gmg_mg* h, const double2* d, int n, std::vector<zc>& out, cudaStream_t s) {
+  GMG_CHECK(n <= kScalars, GMG_ERR_UNSUPPORTED, "mg: too many per-RHS scalars");
+  GMG_CUDA(cudaMemcpyAsync(h->hpin, d, sizeof(double2) * n, cudaMemcpyDeviceToHost, s));
+  GMG_CUDA(cudaStreamSynchronize(s));
+  out.resize(n);
+  for (int k = 0; k < n; ++k) out[k] = zc(h->hpin[k].x, h->hpin[k].y);
+  return GMG_OK;
+}
+
 // host <- per-RHS <X_j, Y> for j < nx
 gmg_status dots(gmg_mg* h, const Vec& X0, int nx, int64_t xstride, const Vec& Y, std::vector<zc>& out,
                 cudaStream_t s) {
-  double2* d = h->coef.as<double2>();
+  double2* d = h->dscr.as<double2>();
   GMG_TRY(vec_multidot(X0, nx, xstride, Y, d, nullptr, s));
-  out.resize((size_t)nx * Y.R);
-  GMG_CUDA(cudaMemcpyAsync(out.data(), d, sizeof(double2) * nx * Y.R, cudaMemcpyDeviceToHost, s));
-  GMG_CUDA(cudaStreamSynchronize(s));
-  return GMG_OK;
+  return download(h, d, nx * Y.R, out, s);
 }
 
+// device coef[offset...] <- a, through the pinned staging buffer.  The copy is
+// asynchronous: every caller reaches a download() (a stream synchronisation)
+// before the staging buffer is written again.
 gmg_status upload(gmg_mg* h, const std::vector<zc>& a, size_t offset_elems, cudaStream_t s) {
-  GMG_CUDA(cudaMemcpyAsync(h->coef.as<double2>() + offset_elems, a.data(), sizeof(double2) * a.size(),
+  GMG_CHECK(a.size() <= (size_t)kScalars, GMG_ERR_UNSUPPORTED, "mg: too many coefficients");
+  for (size_t k = 0; k < a.size(); ++k) h->hpin[k] = make_double2(a[k].real(), a[k].imag());
+  GMG_CUDA(cudaMemcpyAsync(h->coef.as<double2>() + offset_elems, h->hpin, sizeof(double2) * a.size(),
                            cudaMemcpyHostToDevice, s));
-  GMG_CUDA(cudaStreamSynchronize(s));  // `a` is host scratch reused by the caller
   return GMG_OK;
-}
-
-// Y = a X + b Y with per-RHS host coefficients
-gmg_status axpby_h(gmg_mg* h, const std::vector<zc>& a, const Vec& X, const std::vector<zc>& b, Vec& Y,
-                   cudaStream_t s) {
-  std::vector<zc> ab(a);
-  ab.insert(ab.end(), b.begin(), b.end());
-  GMG_TRY(upload(h, ab, 0, s));
-  return vec_axpby(h->coef.as<double2>(), X, h->coef.as<double2>() + a.size(), Y, s);
 }
 
 // Y += sum_j c[j*R + r] X_j
@@ -119,28 +125,23 @@ gmg_status zero(Vec& v, cudaStream_t s) {
   return GMG_OK;
 }
 
-gmg_status copyv(const Vec& a, Vec& b, cudaStream_t s) { return vec_convert(a, b, s); }
 
 // ------------------------------------------------------------- MR smoother
 // x <- x + iters steps of minimal residual for A x = b on level l
+// The step lengths stay on the device: no host synchronisation.
 gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStream_t s) {
   MGLevel& L = *h->L[l];
   const int R = b.R;
-  Vec r = L.mr_r.with_rhs(R), Ar = L.mr_Ar.with_rhs(R), t = L.mr_t.with_rhs(R);
-  std::vector<zc> one(R, 1.0), mone(R, -1.0), d1, d2, al(R), mal(R);
-  GMG_TRY(apply_op(h, l, x, t, s));
-  GMG_TRY(copyv(b, r, s));
-  GMG_TRY(axpby_h(h, mone, t, one, r, s));
+  Vec r = L.mr_r.with_rhs(R), Ar = L.mr_Ar.with_rhs(R);
+  double2* d1 = h->dscr.as<double2>() + kScalars / 2;  // above the Krylov scalars
+  double2* d2 = d1 + R;
+  GMG_TRY(apply_op(h, l, x, r, s));
+  GMG_TRY(vec_xmy(b, r, s));  // r = b - A x
   for (int it = 0; it < iters; ++it) {
     GMG_TRY(apply_op(h, l, r, Ar, s));
-    GMG_TRY(dots(h, Ar, 1, 0, r, d1, s));
-    GMG_TRY(dots(h, Ar, 1, 0, Ar, d2, s));
-    for (int k = 0; k < R; ++k) {
-      al[k] = d2[k].real() > 0 ? d1[k] / d2[k].real() : 0.0;
-      mal[k] = -al[k];
-    }
-    GMG_TRY(axpby_h(h, al, r, one, x, s));
-    GMG_TRY(axpby_h(h, mal, Ar, one, r, s));
+    GMG_TRY(vec_multidot(Ar, 1, 0, r, d1, nullptr, s));
+    GMG_TRY(vec_multidot(Ar, 1, 0, Ar, d2, nullptr, s));
+    GMG_TRY(vec_mr_update(d1, d2, x, r, Ar, s));
   }
   return GMG_OK;
 }
@@ -166,7 +167,6 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
   GMG_TRY(dots(h, b, 1, 0, b, bn, s));
   std::vector<double> bnorm(R);
   for (int r = 0; r < R; ++r) bnorm[r] = std::sqrt(std::max(bn[r].real(), 1e-300));
-  std::vector<zc> one(R, 1.0), mone(R, -1.0), zeros(R, 0.0);
   std::vector<double> res(R, 1.0);
   int iters = 0;
   std::vector<zc> H((size_t)(m + 1) * m * R), g((size_t)(m + 1) * R), cs((size_t)m * R), sn((size_t)m * R);
@@ -174,21 +174,20 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
     // r0 = b - A x -> V_0
     Vec v0 = nth(V0, 0);
     GMG_TRY(apply_op(h, l, x, w, s));
-    GMG_TRY(copyv(b, v0, s));
-    GMG_TRY(axpby_h(h, mone, w, one, v0, s));
+    GMG_TRY(vec_xmy(b, w, s));  // w = b - A x
     std::vector<zc> bb;
-    GMG_TRY(dots(h, v0, 1, 0, v0, bb, s));
+    double2* dn = h->dscr.as<double2>();
+    GMG_TRY(vec_multidot(w, 1, 0, w, dn, nullptr, s));
+    GMG_TRY(download(h, dn, R, bb, s));
     bool all = true;
-    std::vector<zc> inv(R);
     std::vector<double> beta(R);
     for (int r = 0; r < R; ++r) {
       beta[r] = std::sqrt(std::max(bb[r].real(), 0.0));
       res[r] = beta[r] / bnorm[r];
       if (res[r] > tol) all = false;
-      inv[r] = beta[r] > 0 ? 1.0 / beta[r] : 0.0;
     }
     if (all || iters >= maxit) break;
-    GMG_TRY(axpby_h(h, zeros, v0, inv, v0, s));
+    GMG_TRY(vec_scale_inv_norm(dn, w, v0, s));
     std::fill(H.begin(), H.end(), zc(0));
     std::fill(g.begin(), g.end(), zc(0));
     for (int r = 0; r < R; ++r) g[r] = beta[r];
@@ -203,25 +202,25 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
       } else {
         GMG_TRY(apply_op(h, l, zj, w, s));
       }
-      // classical Gram-Schmidt, twice
-      std::vector<zc> hc, hc2;
-      GMG_TRY(dots(h, V0, j + 1, vstride, w, hc, s));
-      std::vector<zc> neg(hc.size());
-      for (size_t k = 0; k < hc.size(); ++k) neg[k] = -hc[k];
-      GMG_TRY(multiaxpy_h(h, neg, V0, j + 1, vstride, w, s));
-      GMG_TRY(dots(h, V0, j + 1, vstride, w, hc2, s));
-      for (size_t k = 0; k < hc2.size(); ++k) {
-        neg[k] = -hc2[k];
-        hc[k] += hc2[k];
-      }
-      GMG_TRY(multiaxpy_h(h, neg, V0, j + 1, vstride, w, s));
-      std::vector<zc> ww;
-      GMG_TRY(dots(h, w, 1, 0, w, ww, s));
+      // classical Gram-Schmidt, twice, with the coefficients kept on the device;
+      // the Hessenberg column comes back to the host in one transfer
+      const size_t nc = (size_t)(j + 1) * R;
+      double2* dh = h->dscr.as<double2>();
+      double2* dh2 = dh + nc;
+      double2* dw = dh2 + nc;
+      GMG_TRY(vec_multidot(V0, j + 1, vstride, w, dh, nullptr, s));
+      GMG_TRY(vec_multiaxpy(dh, V0, j + 1, vstride, w, s, -1.0));
+      GMG_TRY(vec_multidot(V0, j + 1, vstride, w, dh2, nullptr, s));
+      GMG_TRY(vec_multiaxpy(dh2, V0, j + 1, vstride, w, s, -1.0));
+      GMG_TRY(vec_multidot(w, 1, 0, w, dw, nullptr, s));
       Vec vn = nth(V0, j + 1);
-      std::vector<zc> sc(R);
+      GMG_TRY(vec_scale_inv_norm(dw, w, vn, s));
+      std::vector<zc> col;
+      GMG_TRY(download(h, dh, (int)(2 * nc + R), col, s));
+      std::vector<zc> hc(nc);
+      for (size_t k = 0; k < nc; ++k) hc[k] = col[k] + col[nc + k];
       for (int r = 0; r < R; ++r) {
-        const double hn = std::sqrt(std::max(ww[r].real(), 0.0));
-        sc[r] = hn > 0 ? 1.0 / hn : 0.0;
+        const double hn = std::sqrt(std::max(col[2 * nc + r].real(), 0.0));
         // Hessenberg column j of RHS r, Givens rotations
         zc* Hr = &H[(size_t)r * (m + 1) * m];
         for (int i = 0; i <= j; ++i) Hr[i * m + j] = hc[(size_t)i * R + r];
@@ -250,8 +249,6 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
         gr[j + 1] = -sgn * gj;
         res[r] = std::abs(gr[j + 1]) / bnorm[r];
       }
-      GMG_TRY(copyv(w, vn, s));
-      GMG_TRY(axpby_h(h, zeros, vn, sc, vn, s));
       ++iters;
       jl = j;
       bool conv = true;
@@ -413,7 +410,10 @@ extern "C" gmg_status gmg_mg_create(gmg_wilson* fine, const gmg_mg_params* p, in
       dof = 2 * p->nvec[l];
     }
   }
-  gmg_status st = h->coef.alloc(sizeof(double2) * 4096);
+  gmg_status st = h->coef.alloc(sizeof(double2) * kScalars);
+  if (st == GMG_OK) st = h->dscr.alloc(sizeof(double2) * kScalars);
+  if (st == GMG_OK && cudaMallocHost(&h->hpin, sizeof(double2) * kScalars) != cudaSuccess)
+    st = fail(GMG_ERR_NOMEM, "gmg_mg_create: pinned host buffer");
   if (st != GMG_OK) {
     delete h;
     return st;
@@ -560,8 +560,8 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
     // true residuals of the batch decide who stays active
     Vec rA = w.with_rhs(Ra);
     GMG_TRY(apply_op(h, 0, xA, rA, s));
-    std::vector<zc> one(Ra, 1.0), mone(Ra, -1.0), rn, bn2;
-    GMG_TRY(axpby_h(h, one, bA, mone, rA, s));
+    std::vector<zc> rn;
+    GMG_TRY(vec_xmy(bA, rA, s));
     GMG_TRY(dots(h, rA, 1, 0, rA, rn, s));
     std::vector<int> still;
     for (int k = 0; k < Ra; ++k) {

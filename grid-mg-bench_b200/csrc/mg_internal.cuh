@@ -41,7 +41,8 @@ struct VecBuf : Vec {
 gmg_status vec_multidot(const Vec& X0, int nx, int64_t xstride_elems, const Vec& Y, double2* out_dev, const int* mask,
                         cudaStream_t s);
 // Y(r) += sum_j a[j*R + r] X_j(r)
-gmg_status vec_multiaxpy(const double2* a_dev, const Vec& X0, int nx, int64_t xstride_elems, Vec& Y, cudaStream_t s);
+gmg_status vec_multiaxpy(const double2* a_dev, const Vec& X0, int nx, int64_t xstride_elems, Vec& Y, cudaStream_t s,
+                         double sgn = 1.0);
 // Y(r) = a[r] X(r) + b[r] Y(r)
 gmg_status vec_axpby(const double2* a_dev, const Vec& X, const double2* b_dev, Vec& Y, cudaStream_t s);
 // Y = X with a precision conversion
@@ -53,5 +54,11 @@ gmg_status vec_gather(const Vec& src, const int* idx, Vec& dst, cudaStream_t s);
 gmg_status vec_scatter(const Vec& src, const int* idx, Vec& dst, cudaStream_t s);
 // seeded unit-Gaussian field (re, im ~ N(0, 1/2))
 gmg_status vec_gaussian(Vec& X, uint64_t seed, cudaStream_t s);
+// Y(r) = X(r) / sqrt(n[r].x), n from a device multidot
+gmg_status vec_scale_inv_norm(const double2* n_dev, const Vec& X, Vec& Y, cudaStream_t s);
+// MR step with alpha = d1 / d2 (device): x += alpha r, r -= alpha Ar
+gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s);
+// Y = X - Y
+gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s);
 
 }  // namespace gmg

@@ -138,6 +138,18 @@ def torch_smooth_gauge(dims, seed, eps, device="cuda"):
     h = 0.5 * (a + a.conj().transpose(-1, -2))
     tr = torch.diagonal(h, dim1=-2, dim2=-1).sum(-1) / 3.0
     h = h - tr[:, None, None] * torch.eye(3, dtype=h.dtype, device=device)
-    w, v = torch.linalg.eigh(h)
-    u = (v * torch.exp(1j * eps * w)[:, None, :]) @ v.conj().transpose(-1, -2)
+    # exp(i eps H) by scaling and squaring: Taylor series of exp(i eps H / 2^s) to
+    # 18 terms (truncation below 1e-17 for |eps H / 2^s| <= 1/2), then s squarings
+    a = (1j * eps) * h
+    nrm = torch.linalg.matrix_norm(a, ord="fro").max().item()
+    s = max(0, int(np.ceil(np.log2(max(nrm, 1e-30) / 0.5))))
+    a = a / (2.0 ** s)
+    eye = torch.eye(3, dtype=a.dtype, device=device).expand_as(a)
+    u = eye.clone()
+    term = eye.clone()
+    for k in range(1, 19):
+        term = term @ a / k
+        u = u + term
+    for _ in range(s):
+        u = u @ u
     return u.reshape(vol(dims), 4, 3, 3).contiguous()

@@ -187,12 +187,68 @@ def wilson_and_c4(T, hbm):
          note="FP64; unfused backward Mdir + masked projections per batch of basis vectors")
 
 
-def run():
+def c5(nrhs=24, plain_rhs=2):
+    """3-level K-cycle MG-preconditioned FGMRES on 32^4 Wilson-clover (m=-0.35, csw 1, eps 0.3):
+    nbasis 24 on 4^4 blocks, nbasis 32 on 2^4 blocks, MR(8) smoothing; RHS to 1e-10."""
+    fd = (32, 32, 32, 32)
+    V = 32 ** 4
+    U = inputs.torch_smooth_gauge(fd, 801, 0.3)
+    w = gmg.WilsonClover(fd, -0.35, 1.0, antiperiodic=True)
+    w.set_gauge(U)
+    del U
+    b_all = inputs.torch_gaussian((V, nrhs, 12), 802)
+    common = dict(nlevels=3, block=((4, 4, 4, 4), (2, 2, 2, 2)), nvec=(12, 16), smoother_iters=8)
+    out = {}
+    for form, prec, R in (("mixed_bf16_mrhs", "bf16", nrhs), ("mixed_f32_mrhs", "f32", nrhs),
+                          ("plain_f64_single_rhs", "f64", 1)):
+        mg = gmg.MultiGrid(w, R, prec=prec, **common)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        mg.setup()
+        torch.cuda.synchronize()
+        t_setup = time.perf_counter() - t0
+        n_solve = nrhs if R == nrhs else plain_rhs
+        iters, worst, t_solve = [], 0.0, 0.0
+        for k0 in range(0, n_solve, R):
+            b = b_all[:, k0:k0 + R].contiguous()
+            x = torch.zeros_like(b)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            it, rr = mg.solve(b, x, tol=1e-10, maxiter=400)
+            torch.cuda.synchronize()
+            t_solve += time.perf_counter() - t0
+            r = torch.zeros_like(b)
+            w.M(x, r)
+            true = (torch.linalg.vector_norm(b - r, dim=(0, 2)) / torch.linalg.vector_norm(b, dim=(0, 2))).max().item()
+            worst = max(worst, true)
+            iters.append(it)
+            del b, x, r
+        per_rhs = t_solve / n_solve
+        out[form] = {"setup_s": t_setup, "solve_s_measured": t_solve, "rhs_measured": n_solve,
+                     "solve_s_for_all_rhs": per_rhs * nrhs, "outer_iterations": iters,
+                     "max_true_relres": worst}
+        del mg
+        torch.cuda.empty_cache()
+    base = out["plain_f64_single_rhs"]["solve_s_for_all_rhs"]
+    for k in out:
+        out[k]["speedup_vs_plain_f64"] = base / out[k]["solve_s_for_all_rhs"]
+    line("C5 3-level K-cycle MG solve, 32^4 Wilson-clover, 24 RHS to 1e-10", results=out,
+         note=f"plain FP64 single-RHS form timed on {plain_rhs} RHS and scaled to {nrhs}; "
+              "setup (test vectors, orthonormalisation, CoarsenOperator) not included in solve_s")
+
+
+def run(rows=("c1", "c3", "w_c4", "c5")):
     torch.cuda.set_device(0)
     hbm, src = peaks()
     T = Timer()
-    c1(T, hbm)
-    c3(T, hbm)
-    torch.cuda.empty_cache()
-    wilson_and_c4(T, hbm)
+    if "c1" in rows:
+        c1(T, hbm)
+    if "c3" in rows:
+        c3(T, hbm)
+        torch.cuda.empty_cache()
+    if "w_c4" in rows:
+        wilson_and_c4(T, hbm)
+        torch.cuda.empty_cache()
+    if "c5" in rows:
+        c5()
     line("peaks", hbm_gbs=hbm, source=src)
