@@ -104,6 +104,7 @@ gmg_status agg_basis_to_blocked(gmg_agg* h, const double* basis_dev, cudaStream_
                                                   Vc, h->N, h->bv, h->dof, Vf);
   GMG_CUDA(cudaGetLastError());
   h->basis_f_ok = false;
+  h->basis_tc_ok = false;
   return GMG_OK;
 }
 
@@ -243,6 +244,7 @@ static gmg_status launch_project(gmg_agg* h, const void* basis, int nrhs, const 
 gmg_status agg_project(gmg_agg* h, int compute, int vec_prec, int nrhs, const void* fine,
                        void* coarse, const int32_t* mask_unused, cudaStream_t s) {
   (void)mask_unused;
+  if (compute == GMG_BF16 && vec_prec == GMG_F32) return agg_project_tc(h, nrhs, (const float*)fine, (float*)coarse, s);
   GMG_CHECK(compute == vec_prec, GMG_ERR_UNSUPPORTED, "project: compute and vector precision differ");
   if (compute == GMG_F64) {
     if (nrhs >= 4) return launch_project<double, 4, 4, 4>(h, h->basis_blk.p, nrhs, fine, coarse, nullptr, 0, s);
@@ -359,6 +361,7 @@ static gmg_status launch_promote(gmg_agg* h, const void* basis, int nrhs, const 
 
 gmg_status agg_promote(gmg_agg* h, int compute, int vec_prec, int nrhs, const void* coarse,
                        void* fine, cudaStream_t s) {
+  if (compute == GMG_BF16 && vec_prec == GMG_F32) return agg_promote_tc(h, nrhs, (const float*)coarse, (float*)fine, s);
   GMG_CHECK(compute == vec_prec, GMG_ERR_UNSUPPORTED, "promote: compute and vector precision differ");
   const bool tk4 = h->dof % 4 == 0;
   if (compute == GMG_F64) {
@@ -521,6 +524,7 @@ gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s) {
     GMG_CUDA(cudaGetLastError());
   }
   h->basis_f_ok = false;
+  h->basis_tc_ok = false;
   return GMG_OK;
 }
 

@@ -110,7 +110,10 @@ struct gmg_agg {
   gmg::DevBuf basis_blk;  // complex<double> [Vc][N][bv*dof]   (block-major copy)
   gmg::DevBuf basis_blk_f;  // complex<float> same layout
   bool basis_f_ok = false;
+  gmg::DevBuf basis_tc_hi, basis_tc_lo;  // BF16 hi / lo tensor-core packing (block_tc.cu)
+  bool basis_tc_ok = false;
   gmg::DevBuf scratch;
+  gmg::DevBuf dev_err;  // int: error code recorded by the tensor-core kernels
 };
 
 struct gmg_wilson {
@@ -156,6 +159,10 @@ gmg_status agg_promote(gmg_agg* h, int compute, int vec_prec, int nrhs, const vo
 gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s);
 gmg_status agg_check_orthogonal(gmg_agg* h, double* max_err, cudaStream_t s);
 gmg_status agg_prepare_f32(gmg_agg* h, cudaStream_t s);
+// tensor-core projection / promotion (block_tc.cu): FP32 vectors, BF16 hi+lo operands
+gmg_status agg_prepare_tc(gmg_agg* h, cudaStream_t s);
+gmg_status agg_project_tc(gmg_agg* h, int nrhs, const float* fine, float* coarse, cudaStream_t s);
+gmg_status agg_promote_tc(gmg_agg* h, int nrhs, const float* coarse, float* fine, cudaStream_t s);
 
 // fine Wilson-clover (wilson.cu)
 gmg_status wilson_build_clover(gmg_wilson* h, cudaStream_t s);
