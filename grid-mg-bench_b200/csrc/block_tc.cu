@@ -126,17 +126,38 @@ __device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, float* va,
   }
 }
 
-// real / imaginary 16-column chunks summed over `np` partial accumulators `stride` columns apart
-__device__ __forceinline__ void tmem_ld_sum(uint32_t ta, uint32_t tb, uint32_t stride, int np, float* va,
-                                            float* vb) {
-  tmem_ld16x2(ta, tb, va, vb);
-  for (int k = 1; k < np; ++k) {
-    float xa[16], xb[16];
-    tmem_ld16x2(ta + k * stride, tb + k * stride, xa, xb);
+// K-steps of one stage as straight-line code: three MMAs (hi.hi, hi.lo, lo.hi) per
+// 16-deep K-step.  Issuing tcgen05.mma from rolled loops with data-dependent
+// control flow between the instructions measured several times slower per MMA.
+template <int KSTEPS>
+__device__ __forceinline__ void issue_hilo(uint32_t dt, uint64_t ah, uint64_t al, uint64_t bh, uint64_t bl,
+                                           uint32_t a_ks, uint32_t b_ks, uint32_t idesc, bool first) {
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      va[i] += xa[i];
-      vb[i] += xb[i];
+  for (int k = 0; k < KSTEPS; ++k) {
+    mma_bf16(dt, ah + k * a_ks, bh + k * b_ks, idesc, (first && k == 0) ? 0u : 1u);
+    mma_bf16(dt, ah + k * a_ks, bl + k * b_ks, idesc, 1u);
+    mma_bf16(dt, al + k * a_ks, bh + k * b_ks, idesc, 1u);
+  }
+}
+
+__device__ __forceinline__ void issue_hilo_n(int ksteps, uint32_t dt, uint64_t ah, uint64_t al, uint64_t bh,
+                                             uint64_t bl, uint32_t a_ks, uint32_t b_ks, uint32_t idesc, bool first) {
+  switch (ksteps) {
+    case 1: issue_hilo<1>(dt, ah, al, bh, bl, a_ks, b_ks, idesc, first); break;
+    case 2: issue_hilo<2>(dt, ah, al, bh, bl, a_ks, b_ks, idesc, first); break;
+    case 3: issue_hilo<3>(dt, ah, al, bh, bl, a_ks, b_ks, idesc, first); break;
+    case 4: issue_hilo<4>(dt, ah, al, bh, bl, a_ks, b_ks, idesc, first); break;
+    case 5: issue_hilo<5>(dt, ah, al, bh, bl, a_ks, b_ks, idesc, first); break;
+    case 6: issue_hilo<6>(dt, ah, al, bh, bl, a_ks, b_ks, idesc, first); break;
+    case 7: issue_hilo<7>(dt, ah, al, bh, bl, a_ks, b_ks, idesc, first); break;
+    case 8: issue_hilo<8>(dt, ah, al, bh, bl, a_ks, b_ks, idesc, first); break;
+    default: {
+      int k = 0;
+      for (; k + 8 <= ksteps; k += 8)
+        issue_hilo<8>(dt, ah + k * a_ks, al + k * a_ks, bh + k * b_ks, bl + k * b_ks, a_ks, b_ks, idesc,
+                      first && k == 0);
+      for (; k < ksteps; ++k)
+        issue_hilo<1>(dt, ah + k * a_ks, al + k * a_ks, bh + k * b_ks, bl + k * b_ks, a_ks, b_ks, idesc, false);
     }
   }
 }
@@ -155,7 +176,6 @@ struct Params {
   float2* coarse;           // [Vc][nrhs][N] FP32
   int* err;
   int Vc, N, dof, bv, nrhs, R, Rp, Kp, Mp, KS, sps, stages, aligned16;
-  int pacc;  // partial accumulators (independent MMA chains), summed by the epilogue
 };
 
 __global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P) {
@@ -177,9 +197,8 @@ __global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const uint32_t acc_cols = 2 * P.Rp;
-  const uint32_t blk_cols = (uint32_t)P.pacc * acc_cols;
   uint32_t ncols = 32;
-  while (ncols < kAcc * blk_cols) ncols <<= 1;
+  while (ncols < kAcc * acc_cols) ncols <<= 1;
 
   // zero the B tiles once: padding rows (r >= R) and padding K stay zero
   for (size_t k = threadIdx.x; k < (size_t)P.stages * stage_bytes / 16; k += blockDim.x)
@@ -247,9 +266,7 @@ __global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P)
         const uint32_t aph = (uint32_t)(bi / kAcc) & 1;
         if (!mbar_wait(&tempty[acc], aph ^ 1, abort_flag)) { ok = false; break; }
         fence_after();
-        // hi.hi, hi.lo and lo.hi products go to different partial accumulators
-        const uint32_t dt = tmem_base + acc * blk_cols;
-        int j = 0;
+        const uint32_t dt = tmem_base + acc * acc_cols;
         for (int ks = 0; ks < spb; ++ks, ++n) {
           const int stage = (int)(n % P.stages);
           const uint32_t phase = (uint32_t)((n / P.stages) & 1);
@@ -260,19 +277,9 @@ __global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P)
           unsigned char* al = st + a_bytes;
           unsigned char* bh = st + 2 * a_bytes;
           unsigned char* bl = bh + b_bytes;
-          for (int k = 0; k < kc_stage / 2; ++k) {
-            const uint32_t la = (uint32_t)P.Mp * 16, lb = (uint32_t)(2 * P.Rp) * 16;
-            const uint64_t dah = make_desc(ah + (size_t)(2 * k) * P.Mp * 16, la, 128);
-            const uint64_t dal = make_desc(al + (size_t)(2 * k) * P.Mp * 16, la, 128);
-            const uint64_t dbh = make_desc(bh + (size_t)(2 * k) * 2 * P.Rp * 16, lb, 128);
-            const uint64_t dbl = make_desc(bl + (size_t)(2 * k) * 2 * P.Rp * 16, lb, 128);
-            mma_bf16(dt + (uint32_t)(j % P.pacc) * acc_cols, dah, dbh, idesc, j >= P.pacc ? 1u : 0u);
-            ++j;
-            mma_bf16(dt + (uint32_t)(j % P.pacc) * acc_cols, dah, dbl, idesc, j >= P.pacc ? 1u : 0u);
-            ++j;
-            mma_bf16(dt + (uint32_t)(j % P.pacc) * acc_cols, dal, dbh, idesc, j >= P.pacc ? 1u : 0u);
-            ++j;
-          }
+          const uint32_t la = (uint32_t)P.Mp * 16, lb = (uint32_t)(2 * P.Rp) * 16;
+          issue_hilo_n(kc_stage / 2, dt, make_desc(ah, la, 128), make_desc(al, la, 128), make_desc(bh, lb, 128),
+                       make_desc(bl, lb, 128), 2 * P.Mp, 4 * P.Rp, idesc, ks == 0);
           mma_commit(&empty[stage]);
         }
         if (!ok) break;
@@ -351,11 +358,11 @@ __global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P)
         break;
       }
       fence_after();
-      const uint32_t ta = tmem_base + ((uint32_t)(32 * q) << 16) + acc * blk_cols;
+      const uint32_t ta = tmem_base + ((uint32_t)(32 * q) << 16) + acc * acc_cols;
       float2* orow = P.coarse + (size_t)c * P.nrhs * P.N + i;
       for (int c0 = 0; c0 < P.Rp; c0 += 16) {
         float va[16], vb[16];
-        tmem_ld_sum(ta + c0, ta + P.Rp + c0, acc_cols, P.pacc, va, vb);
+        tmem_ld16x2(ta + c0, ta + P.Rp + c0, va, vb);
         float pa[8], pb[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -407,7 +414,6 @@ struct PParams {
   float2* fine;              // [Vf][nrhs][dof]
   int* err;
   int Vc, N, dof, bv, nrhs, R, Rp, K, Kp, Mp, K2, stages;  // K2 = 2N rounded up to 16
-  int pacc;  // partial accumulators (independent MMA chains), summed by the epilogue
 };
 
 constexpr int kPWarps = 6;
@@ -435,9 +441,8 @@ __global__ void __launch_bounds__(kPThreads, 1) promote_tc_kernel(const PParams 
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const uint32_t acc_cols = 2 * P.Rp;
-  const uint32_t tile_cols = (uint32_t)P.pacc * acc_cols;
   uint32_t ncols = 32;
-  while (ncols < 2 * tile_cols) ncols <<= 1;
+  while (ncols < 2 * acc_cols) ncols <<= 1;
   if (threadIdx.x == 0) {
     for (int s = 0; s < P.stages; ++s) {
       mbar_init(&full[s], 1);
@@ -511,21 +516,12 @@ __global__ void __launch_bounds__(kPThreads, 1) promote_tc_kernel(const PParams 
           fence_after();
           unsigned char* ah = smem + (size_t)stage * stage_bytes;
           unsigned char* al = ah + a_bytes;
-          const uint32_t dt = tmem_base + acc * tile_cols;
-          int j = 0;
-          for (int ks = 0; ks < P.K2 / 16; ++ks) {
-            // A: MN-major, 8-dof groups P.Mp*16 bytes apart (SBO), 8-row groups 128 bytes apart (LBO)
-            const uint64_t dah = make_desc(ah + (size_t)ks * 2 * 128, 128, (uint32_t)P.Mp * 16);
-            const uint64_t dal = make_desc(al + (size_t)ks * 2 * 128, 128, (uint32_t)P.Mp * 16);
-            const uint64_t dbh = make_desc(bh + (size_t)(2 * ks) * 2 * P.Rp * 16, (uint32_t)(2 * P.Rp) * 16, 128);
-            const uint64_t dbl = make_desc(bl + (size_t)(2 * ks) * 2 * P.Rp * 16, (uint32_t)(2 * P.Rp) * 16, 128);
-            mma_bf16(dt + (uint32_t)(j % P.pacc) * acc_cols, dah, dbh, idesc, j >= P.pacc ? 1u : 0u);
-            ++j;
-            mma_bf16(dt + (uint32_t)(j % P.pacc) * acc_cols, dah, dbl, idesc, j >= P.pacc ? 1u : 0u);
-            ++j;
-            mma_bf16(dt + (uint32_t)(j % P.pacc) * acc_cols, dal, dbh, idesc, j >= P.pacc ? 1u : 0u);
-            ++j;
-          }
+          const uint32_t dt = tmem_base + acc * acc_cols;
+          // A: MN-major, 8-dof groups P.Mp*16 bytes apart (SBO), 8-row groups 128 bytes apart (LBO);
+          // B: K-major [K2/8 chunks][2Rp rows][8]
+          issue_hilo_n(P.K2 / 16, dt, make_desc(ah, 128, (uint32_t)P.Mp * 16), make_desc(al, 128, (uint32_t)P.Mp * 16),
+                       make_desc(bh, (uint32_t)(2 * P.Rp) * 16, 128), make_desc(bl, (uint32_t)(2 * P.Rp) * 16, 128),
+                       2 * 128 / 16, 2 * 2 * P.Rp, idesc, true);
           mma_commit(&empty[stage]);
           mma_commit(&tfull[acc]);
         }
@@ -597,10 +593,10 @@ __global__ void __launch_bounds__(kPThreads, 1) promote_tc_kernel(const PParams 
         const bool valid = k < P.K;
         const int sb = k / P.dof, a = k % P.dof;
         const int sf = valid ? P.blk_sites[(size_t)c * P.bv + sb] : 0;
-        const uint32_t ta = tmem_base + ((uint32_t)(32 * q) << 16) + acc * tile_cols;
+        const uint32_t ta = tmem_base + ((uint32_t)(32 * q) << 16) + acc * acc_cols;
         for (int c0 = 0; c0 < P.Rp; c0 += 16) {
           float vr[16], vi[16];
-          tmem_ld_sum(ta + c0, ta + P.Rp + c0, acc_cols, P.pacc, vr, vi);
+          tmem_ld16x2(ta + c0, ta + P.Rp + c0, vr, vi);
           if (valid) {
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
@@ -667,14 +663,6 @@ static TcProjGeom tc_geom(const gmg_agg* h) {
   return g;
 }
 
-// Up to 3 partial accumulators (one per hi/lo product) while two of them fit the
-// 512 TMEM columns twice over (double-buffered accumulators).
-static int partial_accumulators(int acc_cols) {
-  int p = 3;
-  while (p > 1 && 2 * p * acc_cols > 512) --p;
-  return p;
-}
-
 gmg_status agg_prepare_tc(gmg_agg* h, cudaStream_t s) {
   if (h->basis_tc_ok) return GMG_OK;
   GMG_CHECK(2 * h->N <= 128, GMG_ERR_UNSUPPORTED, "tensor-core projection needs nbasis <= 64");
@@ -731,7 +719,7 @@ gmg_status agg_project_tc(gmg_agg* h, int nrhs, const float* fine, float* coarse
   P.sps = g.sps;
   P.stages = stages;
   P.aligned16 = ((reinterpret_cast<uintptr_t>(fine) & 15) == 0 && (h->dof % 2) == 0) ? 1 : 0;
-  P.pacc = partial_accumulators(2 * Rp);
+
   {
     KernelTimer kt("project_tc", s);
     ptc::project_tc_kernel<<<std::min(P.Vc, nsm), ptc::kThreads, smem, s>>>(P);
@@ -780,7 +768,7 @@ gmg_status agg_promote_tc(gmg_agg* h, int nrhs, const float* coarse, float* fine
   P.Mp = g.Mp;
   P.K2 = K2;
   P.stages = stages;
-  P.pacc = partial_accumulators(2 * Rp);
+
   {
     KernelTimer kt("promote_tc", s);
     ptc::promote_tc_kernel<<<std::min(P.Vc, nsm), ptc::kPThreads, smem, s>>>(P);

@@ -205,22 +205,6 @@ __device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, float* va,
   }
 }
 
-// real / imaginary 16-column chunks summed over `np` partial accumulators
-// `stride` columns apart (np <= 3), with one wait for all loads
-__device__ __forceinline__ void tmem_ld_sum(uint32_t ta, uint32_t tb, uint32_t stride, int np, float* va,
-                                            float* vb) {
-  tmem_ld16x2(ta, tb, va, vb);
-  for (int k = 1; k < np; ++k) {
-    float xa[16], xb[16];
-    tmem_ld16x2(ta + k * stride, tb + k * stride, xa, xb);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      va[i] += xa[i];
-      vb[i] += xb[i];
-    }
-  }
-}
-
 struct Params {
   const uint16_t* links;   // [V][9][Kc][Mp][8]
   const uint16_t* packed;  // [V][Kc][2Rp][8]
@@ -229,8 +213,32 @@ struct Params {
   float2* out;             // [V][nrhs][N]
   int* err;                // device error word
   int V, N, nrhs, R, Rp, Kc, Mp, p0, p1, g5, stages, kind, pps;
-  int pacc;  // partial accumulators per site (independent MMA chains, summed by the epilogue)
 };
+
+// The MMAs of one stage as straight-line code: PPS points x KH K-steps.  Issuing
+// tcgen05.mma from rolled loops with data-dependent control flow between the
+// instructions measured several times slower per MMA than unrolled sequences.
+template <int PPS, int KH>
+__device__ __forceinline__ void issue_stage(uint32_t dt, uint64_t ad, uint64_t bd, uint32_t a_pt, uint32_t b_pt,
+                                            uint32_t a_ks, uint32_t b_ks, uint32_t idesc, bool first) {
+#pragma unroll
+  for (int pp = 0; pp < PPS; ++pp)
+#pragma unroll
+    for (int ks = 0; ks < KH; ++ks)
+      mma_f16(dt, ad + pp * a_pt + ks * a_ks, bd + pp * b_pt + ks * b_ks, idesc, (first && pp == 0 && ks == 0) ? 0u : 1u);
+}
+
+template <int PPS>
+__device__ __forceinline__ void issue_stage_kh(int kh, uint32_t dt, uint64_t ad, uint64_t bd, uint32_t a_pt,
+                                               uint32_t b_pt, uint32_t a_ks, uint32_t b_ks, uint32_t idesc, bool first) {
+  switch (kh) {
+    case 1: issue_stage<PPS, 1>(dt, ad, bd, a_pt, b_pt, a_ks, b_ks, idesc, first); break;
+    case 2: issue_stage<PPS, 2>(dt, ad, bd, a_pt, b_pt, a_ks, b_ks, idesc, first); break;
+    case 3: issue_stage<PPS, 3>(dt, ad, bd, a_pt, b_pt, a_ks, b_ks, idesc, first); break;
+    default: issue_stage<PPS, 4>(dt, ad, bd, a_pt, b_pt, a_ks, b_ks, idesc, first); break;
+  }
+}
+
 
 // Shared memory: `stages` stages of pps link tiles followed by pps neighbour
 // tiles, then the mbarriers, the TMEM address, the abort flag and the
@@ -255,11 +263,10 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   int* nbr_s = reinterpret_cast<int*>(tmem_slot + 4);  // [2][32][9] neighbour indices of the two producers
 
-  const uint32_t acc_cols = 2 * P.Rp;                 // one partial accumulator
-  const uint32_t site_cols = (uint32_t)P.pacc * acc_cols;  // all partials of one site
-  const int nacc = (int)min((uint32_t)kAccBufs, 512u / site_cols);  // >= 2 (host guarantees)
+  const uint32_t acc_cols = 2 * P.Rp;
+  const int nacc = (int)min((uint32_t)kAccBufs, 512u / acc_cols);  // >= 2 since Rp <= 128
   uint32_t ncols_alloc = 32;
-  while (ncols_alloc < nacc * site_cols) ncols_alloc <<= 1;
+  while (ncols_alloc < nacc * acc_cols) ncols_alloc <<= 1;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < P.stages; ++s) {
@@ -354,9 +361,7 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
                              | ((uint32_t)P.kind << 10)           // B format
                              | ((uint32_t)(2 * P.Rp) >> 3) << 17  // N
                              | ((uint32_t)P.Mp >> 4) << 24;       // M
-      // Descriptors advance by adding 16-byte units to their start-address
-      // field, so one MMA costs a few integer adds on this thread; its
-      // instruction stream, not the tensor core, bounds the issue rate here.
+      // Descriptors advance by adding 16-byte units to their start-address field.
       const uint64_t adesc0 = make_desc(stage_base, (uint32_t)P.Mp * 16, 128);
       const uint64_t bdesc0 = make_desc(stage_base + (size_t)pps * link_bytes, (uint32_t)(2 * P.Rp) * 16, 128);
       const uint32_t st_units = stage_bytes >> 4, a_pt = link_bytes >> 4, b_pt = vec_bytes >> 4;
@@ -370,27 +375,14 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
         const uint32_t aphase = (uint32_t)(i / nacc) & 1;
         if (!mbar_wait(&tempty[acc], aphase ^ 1, abort_flag)) { ok = false; break; }
         fence_after();
-        // consecutive MMAs of a site rotate over P.pacc partial accumulators
-        const uint32_t dt = tmem_base + acc * site_cols;
-        uint32_t dcur = dt, en = 0;
-        int pc = 0;
+        const uint32_t dt = tmem_base + acc * acc_cols;
         for (int g = 0; g < ngroups; ++g) {
           if (!mbar_wait(&full[stage], phase, abort_flag)) { ok = false; break; }
           fence_after();
-          uint64_t ap = adesc0 + st_off, bp = bdesc0 + st_off;
-          for (int pp = 0; pp < pps; ++pp, ap += a_pt, bp += b_pt) {
-            uint64_t ad = ap, bd = bp;
-            for (int ks = 0; ks < kh; ++ks, ad += a_ks, bd += b_ks) {
-              mma_f16(dcur, ad, bd, idesc, en);
-              if (++pc == P.pacc) {
-                pc = 0;
-                dcur = dt;
-                en = 1;
-              } else {
-                dcur += acc_cols;
-              }
-            }
-          }
+          if (pps == 3)
+            issue_stage_kh<3>(kh, dt, adesc0 + st_off, bdesc0 + st_off, a_pt, b_pt, a_ks, b_ks, idesc, g == 0);
+          else
+            issue_stage_kh<1>(kh, dt, adesc0 + st_off, bdesc0 + st_off, a_pt, b_pt, a_ks, b_ks, idesc, g == 0);
           mma_commit(&empty[stage]);
           if (++stage == P.stages) {
             stage = 0;
@@ -438,11 +430,11 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
         break;
       }
       fence_after();
-      const uint32_t ta = tmem_base + ((uint32_t)(32 * q) << 16) + acc * site_cols;
+      const uint32_t ta = tmem_base + ((uint32_t)(32 * q) << 16) + acc * acc_cols;
       float2* orow = P.out + (size_t)site * P.nrhs * P.N + b;
       for (int c = 16 * half; c < P.Rp; c += 32) {
         float vr[16], vi[16];
-        tmem_ld_sum(ta + c, ta + P.Rp + c, acc_cols, P.pacc, vr, vi);
+        tmem_ld16x2(ta + c, ta + P.Rp + c, vr, vi);
         float pr[8], pi[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -637,12 +629,6 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int p0, int
   P.stages = stages;
   P.kind = kind == GMG_BF16 ? 1 : 0;
   P.pps = pps;
-  // partial accumulators: up to 3 independent MMA chains per site, while two
-  // sites' accumulators still fit the 512 TMEM columns
-  const int mmas = npts * (Kc / 2);
-  int pacc = 3;
-  while (pacc > 1 && (pacc > mmas || 512 / (pacc * 2 * Rp) < 2)) --pacc;
-  P.pacc = pacc;
   if (timed) {
     KernelTimer kt("coarse_mrhs_tc", s);
     coarse_mrhs_tc_kernel<<<std::min(V, nsm), kThreads, smem, s>>>(P);

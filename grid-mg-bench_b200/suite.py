@@ -121,9 +121,27 @@ def c3(T, hbm):
     res["project_f32"] = (t, kernel_avg("project")[0], b32)
     t = T.run(lambda: ag.PromoteFromSubspace(c32, f32), reps=3, warm=1)
     res["promote_f32"] = (t, kernel_avg("promote")[0], b32)
+    # tensor-core forms: BF16 hi + lo basis (8 B per complex, as FP32), FP32 vectors
+    t = T.run(lambda: ag.ProjectToSubspace(f32, c32, compute="bf16"), reps=3, warm=1)
+    res["project_bf16x2_tc"] = (t, kernel_avg("project_tc")[0], b32)
+    t = T.run(lambda: ag.PromoteFromSubspace(c32, f32, compute="bf16"), reps=3, warm=1)
+    res["promote_bf16x2_tc"] = (t, kernel_avg("promote_tc")[0], b32)
     gmg.lib().gmg_profile_enable(0)
+    # accuracy of the tensor-core forms against the FP64 kernels on the same inputs
+    errs = {}
+    fx = f32.to(torch.complex128)
+    cref = torch.zeros((Vc, R, N), dtype=torch.complex128, device="cuda")
+    ag.ProjectToSubspace(fx, cref)
+    ag.ProjectToSubspace(f32, c32, compute="bf16")
+    errs["project_bf16x2_tc"] = ((c32.to(torch.complex128) - cref).norm() / cref.norm()).item()
+    ag.PromoteFromSubspace(c32.to(torch.complex128), fx)
+    ag.PromoteFromSubspace(c32, f32, compute="bf16")
+    errs["promote_bf16x2_tc"] = ((f32.to(torch.complex128) - fx).norm() / fx.norm()).item()
+    del fx
     out = {k: {"ms": v[0] * 1e3, "tflops": flops / v[0] / 1e12, "gbs": v[2] / v[0] / 1e9,
                "frac_hbm": v[2] / v[0] / 1e9 / hbm} for k, v in res.items()}
+    for k, e in errs.items():
+        out[k]["rel_err_vs_fp64"] = e
     line("C3 block project / promote (32^4, nbasis 32, 32 RHS, 4^4 blocks)", results=out,
          orthonormalise_ms=t_ortho * 1e3, orthonormalise_max_err=err, algorithmic_flops=flops,
          algorithmic_bytes_f64=b64)
