@@ -130,6 +130,7 @@ gmg_status gmg_coarse_set_links(gmg_coarse* h, const double* links, int on_devic
   GMG_TRY(copy_in(h->links_ref.p, links, bytes, on_device, S(s)));
   GMG_TRY(coarse_links_to_site_major(h, S(s)));
   h->links_set = true;
+  h->self_inv_ok = h->self_inv_f_ok = false;
   if (h->links_f_ok) GMG_TRY(coarse_prepare_f32(h, S(s)));
   if (h->links_h.kind >= 0) GMG_TRY(coarse_prepare_tc(h, h->links_h.kind, S(s)));
   return GMG_OK;
@@ -214,6 +215,7 @@ gmg_status gmg_coarse_construct_remaining_links(gmg_coarse* h, gmg_stream s) {
   GMG_CHECK(h->links_set, GMG_ERR_STATE, "gmg_coarse_construct_remaining_links: links not set");
   GMG_TRY(coarse_construct_remaining(h, S(s)));
   GMG_TRY(coarse_links_to_site_major(h, S(s)));
+  h->self_inv_ok = h->self_inv_f_ok = false;
   if (h->links_f_ok) GMG_TRY(coarse_prepare_f32(h, S(s)));
   if (h->links_h.kind >= 0) GMG_TRY(coarse_prepare_tc(h, h->links_h.kind, S(s)));
   return GMG_OK;

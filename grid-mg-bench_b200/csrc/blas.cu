@@ -360,4 +360,80 @@ gmg_status vec_chiral_double(const Vec& X, double* basis_dev, cudaStream_t s) {
   return GMG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Gram matrix across the RHS columns of a field and a triangular recombination
+// of the columns (global orthonormalisation of a set of lattice vectors kept
+// as the RHS of one field)
+// ---------------------------------------------------------------------------
+namespace blas {
+template <class T>
+__global__ void gram_rhs_kernel(const typename C2<T>::t* __restrict__ X, int64_t V, int R, int dof,
+                                double2* __restrict__ G) {
+  const int a = threadIdx.x / R, b = threadIdx.x % R;  // blockDim = R * R
+  double gr = 0.0, gi = 0.0;
+  for (int64_t s = blockIdx.x; s < V; s += gridDim.x) {
+    const typename C2<T>::t* xa = X + (s * R + a) * dof;
+    const typename C2<T>::t* xb = X + (s * R + b) * dof;
+    for (int k = 0; k < dof; ++k) {  // conj(xa) xb
+      const double ar = xa[k].x, ai = xa[k].y, br = xb[k].x, bi = xb[k].y;
+      gr += ar * br + ai * bi;
+      gi += ar * bi - ai * br;
+    }
+  }
+  atomicAdd(&G[a * R + b].x, gr);
+  atomicAdd(&G[a * R + b].y, gi);
+}
+
+// X[s][a][k] <- sum_{b <= a} T[a * R + b] X[s][b][k]   (R <= 32)
+template <class T>
+__global__ void tri_apply_kernel(const double2* __restrict__ Tm, typename C2<T>::t* __restrict__ X, int64_t V, int R,
+                                 int dof) {
+  const int64_t n = V * dof;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = e / dof;
+    const int k = (int)(e % dof);
+    double xr[32], xi[32];
+    for (int b = 0; b < R; ++b) {
+      xr[b] = X[(s * R + b) * dof + k].x;
+      xi[b] = X[(s * R + b) * dof + k].y;
+    }
+    for (int a = 0; a < R; ++a) {  // inputs are held in registers
+      double yr = 0.0, yi = 0.0;
+      for (int b = 0; b <= a; ++b) {
+        const double2 t = Tm[a * R + b];
+        yr += t.x * xr[b] - t.y * xi[b];
+        yi += t.x * xi[b] + t.y * xr[b];
+      }
+      typename C2<T>::t o;
+      o.x = yr;
+      o.y = yi;
+      X[(s * R + a) * dof + k] = o;
+    }
+  }
+}
+}  // namespace blas
+
+gmg_status vec_gram(const Vec& X, double2* G_dev, cudaStream_t s) {
+  GMG_CHECK(X.R >= 1 && X.R <= 32, GMG_ERR_UNSUPPORTED, "vec_gram: at most 32 vectors");
+  GMG_CUDA(cudaMemsetAsync(G_dev, 0, sizeof(double2) * X.R * X.R, s));
+  const int g = (int)std::min<int64_t>(X.V, 148 * 8);
+  if (X.prec == GMG_F64)
+    blas::gram_rhs_kernel<double><<<g, X.R * X.R, 0, s>>>((const double2*)X.p, X.V, X.R, X.dof, G_dev);
+  else
+    blas::gram_rhs_kernel<float><<<g, X.R * X.R, 0, s>>>((const float2*)X.p, X.V, X.R, X.dof, G_dev);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status vec_tri_apply(const double2* T_dev, Vec& X, cudaStream_t s) {
+  GMG_CHECK(X.R >= 1 && X.R <= 32, GMG_ERR_UNSUPPORTED, "vec_tri_apply: at most 32 vectors");
+  const int g = blas::grid1(X.V * X.dof);
+  if (X.prec == GMG_F64)
+    blas::tri_apply_kernel<double><<<g, 256, 0, s>>>(T_dev, (double2*)X.p, X.V, X.R, X.dof);
+  else
+    blas::tri_apply_kernel<float><<<g, 256, 0, s>>>(T_dev, (float2*)X.p, X.V, X.R, X.dof);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
 }  // namespace gmg

@@ -433,77 +433,115 @@ __device__ void block_gram(const double2* __restrict__ Vb, int N, int64_t K, int
   __syncthreads();
 }
 
+// Cholesky G = L L^dag in place (lower triangle) by warp 0, with `shift` added
+// to the diagonal; returns false (to every thread) when a pivot is not positive.
+__device__ bool block_cholesky(double2* G, int N, double shift, int* fail_s) {
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t == 0) *fail_s = 0;
+  __syncthreads();
+  if (warp == 0) {
+    for (int j = 0; j < N; ++j) {
+      if (lane == 0) {
+        double d = G[j * N + j].x + shift;
+        for (int k = 0; k < j; ++k) d -= G[j * N + k].x * G[j * N + k].x + G[j * N + k].y * G[j * N + k].y;
+        if (!(d > 0.0)) {
+          *fail_s = 1;
+          d = 1.0;
+        }
+        G[j * N + j] = make_double2(sqrt(d), 0.0);
+      }
+      __syncwarp();
+      const double dj = G[j * N + j].x;
+      for (int i = j + 1 + lane; i < N; i += 32) {
+        double2 v = G[i * N + j];
+        for (int k = 0; k < j; ++k) {  // v -= L[i][k] conj(L[j][k])
+          const double2 a = G[i * N + k], b = G[j * N + k];
+          v.x -= a.x * b.x + a.y * b.y;
+          v.y -= a.y * b.x - a.x * b.y;
+        }
+        G[i * N + j] = make_double2(v.x / dj, v.y / dj);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  return *fail_s == 0;
+}
+
+// Block orthonormalisation (blockLutedOrthonormalise, ...Lut.h:172-240: modified
+// Gram-Schmidt per block) as Cholesky QR: each pass forms the block Gram matrix
+// G = V V^dag, factors G = L L^dag and replaces V by L^{-1} V.  The transform is
+// lower triangular in the vector index, so the result is the same orthonormal
+// basis Gram-Schmidt produces.  Cholesky QR loses orthogonality as cond(V)^2;
+// when a factorisation breaks down (smoothed test vectors can be nearly
+// dependent inside a block) that pass is redone with the diagonal shift of
+// shifted Cholesky QR (Fukaya, Kannan, Nakatsukasa, Yamamoto, Yanagisawa,
+// SIAM J. Sci. Comput. 42 (2020)), s = 11 (K N + N (N + 1)) u ||V||_F^2, which
+// always factors, and up to two extra plain passes follow.
 __global__ void __launch_bounds__(256) ortho_kernel(double2* __restrict__ basis, int Vc, int N,
-                                                    int dof, int bv, int* __restrict__ status) {
+                                                    int dof, int bv, int passes, int* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* G = reinterpret_cast<double2*>(smem_raw);  // [N][N]  Gram, then L
   double2* Li = G + N * N;                             // [N][N]  conj(L^{-1})
   double2* VT = Li + N * N;                            // [KC][N] staging
+  __shared__ int fail_s;
+  __shared__ double trace_s;
   const int64_t K = (int64_t)bv * dof;
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int t = threadIdx.x;
   for (int c = blockIdx.x; c < Vc; c += gridDim.x) {
     double2* Vb = basis + (int64_t)c * N * K;
-    block_gram(Vb, N, K, dof, bv, VT, G);
-    // Cholesky G = L L^dag in place (lower triangle), warp 0
-    if (warp == 0) {
-      for (int j = 0; j < N; ++j) {
-        if (lane == 0) {
-          double d = G[j * N + j].x;
-          for (int k = 0; k < j; ++k) d -= G[j * N + k].x * G[j * N + k].x + G[j * N + k].y * G[j * N + k].y;
-          if (!(d > 0.0)) { atomicExch(status, 1); d = 1.0; }
-          G[j * N + j] = make_double2(sqrt(d), 0.0);
+    int extra = 0;
+    for (int pass = 0; pass < passes + extra; ++pass) {
+      block_gram(Vb, N, K, dof, bv, VT, G);
+      if (!block_cholesky(G, N, 0.0, &fail_s)) {
+        block_gram(Vb, N, K, dof, bv, VT, G);
+        if (t == 0) {
+          double tr = 0.0;
+          for (int i = 0; i < N; ++i) tr += G[i * N + i].x;
+          trace_s = tr;
         }
-        __syncwarp();
-        const double dj = G[j * N + j].x;
-        for (int i = j + 1 + lane; i < N; i += 32) {
-          double2 v = G[i * N + j];
-          for (int k = 0; k < j; ++k) {  // v -= L[i][k] conj(L[j][k])
-            const double2 a = G[i * N + k], b = G[j * N + k];
-            v.x -= a.x * b.x + a.y * b.y;
-            v.y -= a.y * b.x - a.x * b.y;
+        __syncthreads();
+        const double shift = 11.0 * ((double)K * N + (double)N * (N + 1)) * 1.1102230246251565e-16 * trace_s;
+        if (!block_cholesky(G, N, shift, &fail_s) && t == 0) atomicExch(status, 1);
+        if (extra < 2) extra = 2;
+      }
+      // L^{-1} column by column (one thread per column), stored conjugated
+      for (int j = t; j < N; j += blockDim.x) {
+        for (int i = 0; i < N; ++i) Li[i * N + j] = make_double2(0, 0);
+        // X[i][j] for i >= j: X[j][j] = 1/L[j][j]; X[i][j] = -(sum_{k=j}^{i-1} L[i][k] X[k][j]) / L[i][i]
+        Li[j * N + j] = make_double2(1.0 / G[j * N + j].x, 0.0);
+        for (int i = j + 1; i < N; ++i) {
+          double2 sacc = make_double2(0, 0);
+          for (int k = j; k < i; ++k) {
+            const double2 a = G[i * N + k], x = Li[k * N + j];
+            sacc.x += a.x * x.x - a.y * x.y;
+            sacc.y += a.x * x.y + a.y * x.x;
           }
-          G[i * N + j] = make_double2(v.x / dj, v.y / dj);
+          const double inv = 1.0 / G[i * N + i].x;
+          Li[i * N + j] = make_double2(-sacc.x * inv, -sacc.y * inv);
         }
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    // L^{-1} column by column (one thread per column), stored conjugated
-    for (int j = t; j < N; j += blockDim.x) {
-      for (int i = 0; i < N; ++i) Li[i * N + j] = make_double2(0, 0);
-      // X[i][j] for i >= j: X[j][j] = 1/L[j][j]; X[i][j] = -(sum_{k=j}^{i-1} L[i][k] X[k][j]) / L[i][i]
-      Li[j * N + j] = make_double2(1.0 / G[j * N + j].x, 0.0);
-      for (int i = j + 1; i < N; ++i) {
-        double2 sacc = make_double2(0, 0);
-        for (int k = j; k < i; ++k) {
-          const double2 a = G[i * N + k], x = Li[k * N + j];
-          sacc.x += a.x * x.x - a.y * x.y;
-          sacc.y += a.x * x.y + a.y * x.x;
-        }
-        const double inv = 1.0 / G[i * N + i].x;
-        Li[i * N + j] = make_double2(-sacc.x * inv, -sacc.y * inv);
-      }
-      for (int i = j; i < N; ++i) Li[i * N + j].y = -Li[i * N + j].y;  // conjugate
-    }
-    __syncthreads();
-    // V <- conj(L^{-1}) V, chunk by chunk (each chunk read fully before it is overwritten)
-    const int KC = ORTHO_KS * dof;
-    for (int64_t k0 = 0; k0 < K; k0 += KC) {
-      const int kc = (int)((K - k0) < (int64_t)KC ? (K - k0) : (int64_t)KC);
-      __syncthreads();
-      for (int e = t; e < N * kc; e += blockDim.x) {
-        const int i = e / kc, kk = e % kc;
-        VT[kk * N + i] = Vb[(int64_t)i * K + k0 + kk];
+        for (int i = j; i < N; ++i) Li[i * N + j].y = -Li[i * N + j].y;  // conjugate
       }
       __syncthreads();
-      for (int e = t; e < N * kc; e += blockDim.x) {
-        const int i = e / kc, kk = e % kc;
-        double2 acc = make_double2(0, 0);
-        for (int j = 0; j <= i; ++j) acc = cfma(acc, Li[i * N + j], VT[kk * N + j]);
-        Vb[(int64_t)i * K + k0 + kk] = acc;
+      // V <- conj(L^{-1}) V, chunk by chunk (each chunk read fully before it is overwritten)
+      const int KC = ORTHO_KS * dof;
+      for (int64_t k0 = 0; k0 < K; k0 += KC) {
+        const int kc = (int)((K - k0) < (int64_t)KC ? (K - k0) : (int64_t)KC);
+        __syncthreads();
+        for (int e = t; e < N * kc; e += blockDim.x) {
+          const int i = e / kc, kk = e % kc;
+          VT[kk * N + i] = Vb[(int64_t)i * K + k0 + kk];
+        }
+        __syncthreads();
+        for (int e = t; e < N * kc; e += blockDim.x) {
+          const int i = e / kc, kk = e % kc;
+          double2 acc = make_double2(0, 0);
+          for (int j = 0; j <= i; ++j) acc = cfma(acc, Li[i * N + j], VT[kk * N + j]);
+          Vb[(int64_t)i * K + k0 + kk] = acc;
+        }
       }
+      __syncthreads();
     }
-    __syncthreads();
   }
 }
 
@@ -517,9 +555,9 @@ gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s) {
   GMG_CUDA(cudaMemsetAsync(h->scratch.p, 0, sizeof(int), s));
   const int Vc = (int)h->cdims.vol();
   const int grid = std::min(Vc, num_sms() * 8);
-  for (int p = 0; p < passes; ++p) {
+  {
     KernelTimer kt("ortho", s);
-    ortho_kernel<<<grid, 256, smem, s>>>(h->basis_blk.as<double2>(), Vc, N, h->dof, h->bv,
+    ortho_kernel<<<grid, 256, smem, s>>>(h->basis_blk.as<double2>(), Vc, N, h->dof, h->bv, passes,
                                          h->scratch.as<int>());
     GMG_CUDA(cudaGetLastError());
   }
@@ -566,7 +604,7 @@ gmg_status agg_check_orthogonal(gmg_agg* h, double* max_err, cudaStream_t s) {
   *max_err = r;
   int st = 0;
   GMG_CUDA(cudaMemcpy(&st, h->scratch.p, sizeof(int), cudaMemcpyDeviceToHost));
-  if (st) return fail(GMG_ERR_NONFINITE, "orthonormalise: a block Gram matrix was not positive definite");
+  if (st) return fail(GMG_ERR_NONFINITE, "orthonormalise: a block Gram matrix was singular even with the shift");
   return GMG_OK;
 }
 

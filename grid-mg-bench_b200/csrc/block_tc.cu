@@ -20,10 +20,11 @@
 //   warp 0      producer: one bulk copy of the basis hi and lo tiles per stage
 //               (the packed basis is stage-contiguous in HBM)
 //   warp 1      TMEM allocation + MMA issue (one thread): 3 MMAs per K-step
-//   warps 2-5   converters: read the FP32 fine vector of the stage's sites, split
+//   warps 2-9   converters: read the FP32 fine vector of the stage's sites (bulk-copied
+//               into the stage by the producer when its rows are 16-byte aligned), split
 //               into hi/lo BF16 and store the B tiles in the canonical K-major
 //               core-matrix layout, then fence.proxy.async + mbarrier arrive
-//   warps 6-9   epilogue: tcgen05.ld, lane-pair (re, im) recombination, FP32 output
+//   warps 10-13 epilogue: tcgen05.ld, lane-pair (re, im) recombination, FP32 output
 // All mbarrier waits are bounded; on time-out the kernel records an error code,
 // drains its copies and MMAs, frees TMEM and returns.
 #include <algorithm>
@@ -33,9 +34,9 @@
 namespace gmg {
 namespace ptc {
 
-constexpr int kWarps = 10;
+constexpr int kWarps = 14;
 constexpr int kThreads = kWarps * 32;
-constexpr int kConvThreads = 128;
+constexpr int kConvThreads = 256;
 constexpr int kEpiThreads = 128;
 constexpr int kAcc = 2;
 constexpr long long kTimeoutCycles = 4000000000LL;
@@ -176,6 +177,7 @@ struct Params {
   float2* coarse;           // [Vc][nrhs][N] FP32
   int* err;
   int Vc, N, dof, bv, nrhs, R, Rp, Kp, Mp, KS, sps, stages, aligned16;
+  int raw;  // 1: the producer bulk-copies each site's FP32 rows into the stage (16-byte aligned rows)
 };
 
 __global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P) {
@@ -184,17 +186,21 @@ __global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P)
   const int kc_stage = P.KS / 8;                               // K-chunks per stage
   const uint32_t a_bytes = (uint32_t)kc_stage * P.Mp * 16;     // one of hi / lo
   const uint32_t b_bytes = (uint32_t)kc_stage * 2 * P.Rp * 16; // one of hi / lo
-  const uint32_t stage_bytes = 2 * a_bytes + 2 * b_bytes;
+  const uint32_t site_bytes = (uint32_t)P.nrhs * P.dof * 8;      // one fine site, all RHS, FP32
+  const uint32_t raw_bytes = P.raw ? (uint32_t)P.sps * site_bytes : 0u;
+  const uint32_t stage_bytes = 2 * a_bytes + 2 * b_bytes + raw_bytes;
   const int spb = P.Kp / P.KS;  // stages per block
 
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)P.stages * stage_bytes);
   uint64_t* full = bars;
   uint64_t* empty = full + P.stages;
-  uint64_t* tfull = empty + P.stages;
+  uint64_t* rawb = empty + P.stages;  // [stages] raw site rows landed (raw mode)
+  uint64_t* tfull = rawb + P.stages;
   uint64_t* tempty = tfull + kAcc;
   uint64_t* drain = tempty + kAcc;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  int* site_tab = reinterpret_cast<int*>(tmem_slot + 4);  // [bv] fine sites of the producer's block (raw mode)
 
   const uint32_t acc_cols = 2 * P.Rp;
   uint32_t ncols = 32;
@@ -207,6 +213,7 @@ __global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P)
     for (int s = 0; s < P.stages; ++s) {
       mbar_init(&full[s], 1 + kConvThreads);
       mbar_init(&empty[s], 1);
+      mbar_init(&rawb[s], 1);
     }
     for (int a = 0; a < kAcc; ++a) {
       mbar_init(&tfull[a], 1);
@@ -232,27 +239,55 @@ __global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P)
 
   if (warp == 0) {
     // ---------------------------------------------------------------- producer: basis tiles
-    if (lane == 0) {
-      int64_t last = -1;
-      for (int64_t n = 0; n < nseq; ++n) {
-        const int stage = (int)(n % P.stages);
-        const uint32_t phase = (uint32_t)((n / P.stages) & 1);
-        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) {
-          atomicCAS(P.err, 0, 1);
-          *abort_flag = 1;
-          break;
-        }
-        const int c = blockIdx.x + (int)(n / spb) * gridDim.x;
-        const int ks = (int)(n % spb);
-        unsigned char* st = smem + (size_t)stage * stage_bytes;
-        const size_t off = ((size_t)c * (P.Kp / 8) + (size_t)ks * kc_stage) * P.Mp * 8;  // halves
-        mbar_expect_tx(&full[stage], 2 * a_bytes);
-        bulk_g2s(st, P.ahi + off, a_bytes, &full[stage]);
-        bulk_g2s(st + a_bytes, P.alo + off, a_bytes, &full[stage]);
-        last = n;
+    // (+ the fine site rows in raw mode).  At the start of each block the warp
+    // loads the block's site table into shared memory in parallel, so the issuing
+    // lane never waits on a dependent global load between copies.
+    int64_t last = -1;
+    bool stop = false;
+    for (int bi = 0; bi < nblk && !stop; ++bi) {
+      const int c = blockIdx.x + bi * gridDim.x;
+      if (P.raw) {
+        __syncwarp();
+        for (int k = lane; k < P.bv; k += 32) site_tab[k] = P.blk_sites[(size_t)c * P.bv + k];
+        __syncwarp();
       }
-      for (int64_t n = last; n >= 0 && n > last - P.stages; --n)
+      if (lane == 0) {
+        for (int ks = 0; ks < spb; ++ks) {
+          const int64_t n = (int64_t)bi * spb + ks;
+          const int stage = (int)(n % P.stages);
+          const uint32_t phase = (uint32_t)((n / P.stages) & 1);
+          if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) {
+            atomicCAS(P.err, 0, 1);
+            *abort_flag = 1;
+            stop = true;
+            break;
+          }
+          unsigned char* st = smem + (size_t)stage * stage_bytes;
+          const size_t off = ((size_t)c * (P.Kp / 8) + (size_t)ks * kc_stage) * P.Mp * 8;  // halves
+          mbar_expect_tx(&full[stage], 2 * a_bytes);
+          bulk_g2s(st, P.ahi + off, a_bytes, &full[stage]);
+          bulk_g2s(st + a_bytes, P.alo + off, a_bytes, &full[stage]);
+          if (P.raw) {
+            // the stage's fine sites: one contiguous [nrhs][dof] FP32 row block each
+            const int s0 = ks * P.sps;
+            const int nsv = min(P.sps, P.bv - s0);
+            unsigned char* rw = st + 2 * a_bytes + 2 * b_bytes;
+            mbar_expect_tx(&rawb[stage], (uint32_t)nsv * site_bytes);
+            for (int sl = 0; sl < nsv; ++sl)
+              bulk_g2s(rw + (size_t)sl * site_bytes,
+                       reinterpret_cast<const unsigned char*>(P.fine) + (size_t)site_tab[s0 + sl] * site_bytes,
+                       site_bytes, &rawb[stage]);
+          }
+          last = n;
+        }
+      }
+      stop = __shfl_sync(0xffffffffu, stop, 0);
+    }
+    if (lane == 0) {
+      for (int64_t n = last; n >= 0 && n > last - P.stages; --n) {
         mbar_drain(&full[n % P.stages], (uint32_t)((n / P.stages) & 1));
+        if (P.raw) mbar_drain(&rawb[n % P.stages], (uint32_t)((n / P.stages) & 1));
+      }
     }
   } else if (warp == 1) {
     // ---------------------------------------------------------------- MMA issue
@@ -292,14 +327,21 @@ __global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P)
       mma_commit(drain);
       mbar_drain(drain, 0);
     }
-  } else if (warp < 6) {
+  } else if (warp < 10) {
     // ---------------------------------------------------------------- converters: B tiles
-    const int t = threadIdx.x - 64;  // 0..127
-    const int pairs = P.sps * P.R;   // (site, rhs) records per stage
+    // Each thread takes (site, rhs) records and splits the record's dof FP32
+    // complex values (dof even) into BF16 hi / lo pairs of the K-major B tiles.
+    // Raw mode reads the records from the stage's bulk-copied site rows; the
+    // direct mode loads them from global memory.
+    const int t = threadIdx.x - 64;  // 0..255
+    const int hd = P.dof / 2;        // complex pairs per (site, rhs) record
+    const int items = P.sps * P.R * hd;
     for (int64_t n = 0; n < nseq; ++n) {
       const int stage = (int)(n % P.stages);
       const uint32_t phase = (uint32_t)((n / P.stages) & 1);
-      if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) {
+      const bool ok = P.raw ? mbar_wait(&rawb[stage], phase, abort_flag)
+                            : mbar_wait(&empty[stage], phase ^ 1, abort_flag);
+      if (!ok) {
         atomicCAS(P.err, 0, 3);
         *abort_flag = 1;
         break;
@@ -309,38 +351,46 @@ __global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P)
       unsigned char* st = smem + (size_t)stage * stage_bytes;
       uint32_t* bh = reinterpret_cast<uint32_t*>(st + 2 * a_bytes);
       uint32_t* bl = reinterpret_cast<uint32_t*>(st + 2 * a_bytes + b_bytes);
-      for (int q = t; q < pairs; q += kConvThreads) {
-        const int sl = q / P.R, r = q % P.R;
+      const unsigned char* rw = st + 2 * a_bytes + 2 * b_bytes;
+      // item = ((sl * R) + r) * hd + a2: consecutive threads read consecutive 16-byte pairs
+      for (int it = t; it < items; it += kConvThreads) {
+        const int a2 = it % hd, rec = it / hd;
+        const int sl = rec / P.R, r = rec % P.R;
         const int sb = ks * P.sps + sl;  // in-block site
-        if (sb >= P.bv) continue;
-        const int sf = P.blk_sites[(size_t)c * P.bv + sb];
-        const float2* src = P.fine + ((size_t)sf * P.nrhs + r) * P.dof;
-        for (int a = 0; a < P.dof; a += 2) {
-          float2 x0, x1;
-          if (P.aligned16) {
-            const float4 v = *reinterpret_cast<const float4*>(src + a);
+        const int a = 2 * a2;
+        float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
+        if (sb < P.bv) {  // else K padding of the block's last stage: zero
+          if (P.raw) {
+            const float4 v = *reinterpret_cast<const float4*>(rw + (size_t)sl * site_bytes + ((size_t)r * P.dof + a) * 8);
             x0 = make_float2(v.x, v.y);
             x1 = make_float2(v.z, v.w);
           } else {
-            x0 = src[a];
-            x1 = src[a + 1];
+            const float2* src = P.fine + ((size_t)P.blk_sites[(size_t)c * P.bv + sb] * P.nrhs + r) * P.dof + a;
+            if (P.aligned16) {
+              const float4 v = *reinterpret_cast<const float4*>(src);
+              x0 = make_float2(v.x, v.y);
+              x1 = make_float2(v.z, v.w);
+            } else {
+              x0 = src[0];
+              x1 = src[1];
+            }
           }
-          const int k = sl * P.dof + a;  // even: k, k+1 share a 16-byte core-matrix row
-          const int chunk = k >> 3, j = k & 7;
-          const float h0r = bf16_round(x0.x), h1r = bf16_round(x1.x), h0i = bf16_round(x0.y), h1i = bf16_round(x1.y);
-          const size_t rre = ((size_t)chunk * 2 * P.Rp + r) * 4 + (j >> 1);           // 32-bit words
-          const size_t rim = ((size_t)chunk * 2 * P.Rp + P.Rp + r) * 4 + (j >> 1);
-          bh[rre] = bf16_pair(h0r, h1r);
-          bh[rim] = bf16_pair(h0i, h1i);
-          bl[rre] = bf16_pair(x0.x - h0r, x1.x - h1r);
-          bl[rim] = bf16_pair(x0.y - h0i, x1.y - h1i);
         }
+        const int k = sl * P.dof + a;  // even: k, k+1 share a 16-byte core-matrix row
+        const int chunk = k >> 3, j = k & 7;
+        const float h0r = bf16_round(x0.x), h1r = bf16_round(x1.x), h0i = bf16_round(x0.y), h1i = bf16_round(x1.y);
+        const size_t rre = ((size_t)chunk * 2 * P.Rp + r) * 4 + (j >> 1);  // 32-bit words
+        const size_t rim = ((size_t)chunk * 2 * P.Rp + P.Rp + r) * 4 + (j >> 1);
+        bh[rre] = bf16_pair(h0r, h1r);
+        bh[rim] = bf16_pair(h0i, h1i);
+        bl[rre] = bf16_pair(x0.x - h0r, x1.x - h1r);
+        bl[rim] = bf16_pair(x0.y - h0i, x1.y - h1i);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&full[stage]);
     }
   } else {
-    // ---------------------------------------------------------------- epilogue (warps 6-9)
+    // ---------------------------------------------------------------- epilogue (warps 10-13)
     const int q = warp & 3;
     const int rows_per_warp = P.Mp / 4;
     const int row = q * rows_per_warp + lane;
@@ -681,16 +731,22 @@ gmg_status agg_prepare_tc(gmg_agg* h, cudaStream_t s) {
 
 gmg_status agg_project_tc(gmg_agg* h, int nrhs, const float* fine, float* coarse, cudaStream_t s) {
   GMG_CHECK(nrhs <= 128, GMG_ERR_UNSUPPORTED, "tensor-core projection: at most 128 RHS");
+  GMG_CHECK(h->dof % 2 == 0, GMG_ERR_UNSUPPORTED, "tensor-core projection: site dof must be even");
   GMG_TRY(agg_prepare_tc(h, s));
   const TcProjGeom g = tc_geom(h);
   const int Rp = (nrhs + 15) / 16 * 16;
   const uint32_t a_bytes = (uint32_t)(g.KS / 8) * g.Mp * 16;
   const uint32_t b_bytes = (uint32_t)(g.KS / 8) * 2 * Rp * 16;
-  const uint32_t stage_bytes = 2 * a_bytes + 2 * b_bytes;
-  const size_t fixed = (2 * 32 + 2 * ptc::kAcc + 1) * 8 + 16;
+  const size_t fixed = (3 * 16 + 2 * ptc::kAcc + 1) * 8 + 16 + (size_t)h->bv * 4;
+  // raw mode: the fine site rows are bulk-copied into the stage (16-byte aligned rows)
+  const uint32_t site_bytes = (uint32_t)nrhs * h->dof * 8;
+  const bool aligned = (reinterpret_cast<uintptr_t>(fine) & 15) == 0 && site_bytes % 16 == 0;
+  const uint32_t raw_stage = (uint32_t)g.sps * site_bytes;
+  int raw = aligned && (2 * a_bytes + 2 * b_bytes + raw_stage) * 2 + fixed <= 227 * 1024 ? 1 : 0;
+  const uint32_t stage_bytes = 2 * a_bytes + 2 * b_bytes + (raw ? raw_stage : 0u);
   int stages = (int)std::min<size_t>(16, (227 * 1024 - fixed) / stage_bytes);
   GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "tensor-core projection: stage does not fit shared memory");
-  const size_t smem = (size_t)stages * stage_bytes + (size_t)(2 * stages + 2 * ptc::kAcc + 1) * 8 + 16;
+  const size_t smem = (size_t)stages * stage_bytes + (size_t)(3 * stages + 2 * ptc::kAcc + 1) * 8 + 16 + (size_t)h->bv * 4;
   GMG_CUDA(cudaFuncSetAttribute(ptc::project_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   if (!h->dev_err.p) {
     GMG_TRY(h->dev_err.alloc(256));
@@ -719,6 +775,7 @@ gmg_status agg_project_tc(gmg_agg* h, int nrhs, const float* fine, float* coarse
   P.sps = g.sps;
   P.stages = stages;
   P.aligned16 = ((reinterpret_cast<uintptr_t>(fine) & 15) == 0 && (h->dof % 2) == 0) ? 1 : 0;
+  P.raw = raw;
 
   {
     KernelTimer kt("project_tc", s);

@@ -18,7 +18,7 @@
 //
 // Kernel structure (one persistent CTA per SM, 11 warps):
 //   warps 0, 10  producers: stage-sequence numbers alternate between them; one
-//                stage = 3 (or 1) stencil points of one site: one bulk copy of
+//                stage = 1-4 stencil points of one site: one bulk copy of
 //                the points' contiguous link tiles and one per neighbour tile
 //                (cp.async.bulk + mbarrier transaction counts)
 //   warp 1       TMEM allocator + MMA issuer (one elected thread); accumulates
@@ -208,7 +208,8 @@ __device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, float* va,
 struct Params {
   const uint16_t* links;   // [V][9][Kc][Mp][8]
   const uint16_t* packed;  // [V][Kc][2Rp][8]
-  const int32_t* nbr;      // [9][V]
+  const int32_t* nbr;      // [9][V]: input index of point p's neighbour of output index o
+  const int32_t* site_map; // [V] link site of output index o (null: o itself)
   const int32_t* active;   // nullable
   float2* out;             // [V][nrhs][N]
   int* err;                // device error word
@@ -262,6 +263,7 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   int* nbr_s = reinterpret_cast<int*>(tmem_slot + 4);  // [2][32][9] neighbour indices of the two producers
+  int* lsite_s = nbr_s + 2 * 32 * 9;                   // [2][32] link sites of the two producers
 
   const uint32_t acc_cols = 2 * P.Rp;
   const int nacc = (int)min((uint32_t)kAccBufs, 512u / acc_cols);  // >= 2 since Rp <= 128
@@ -306,6 +308,7 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
     // of the pps (contiguous) link tiles and one per neighbour tile.
     const int pid = warp == 0 ? 0 : 1;
     int* my_nbr = nbr_s + pid * 32 * 9;
+    int* my_lsite = lsite_s + pid * 32;
     int64_t last = -1;
     bool stop = false;
     for (int i0 = 0; i0 < nsites && !stop; i0 += 32) {
@@ -315,11 +318,12 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
         const int site = blockIdx.x + (i0 + lane) * gridDim.x;
 #pragma unroll
         for (int p = 0; p < 9; ++p) my_nbr[lane * 9 + p] = __ldg(&P.nbr[(size_t)p * P.V + site]);
+        my_lsite[lane] = P.site_map ? __ldg(&P.site_map[site]) : site;
       }
       __syncwarp();
       if (lane == 0) {
         for (int j = 0; j < cnt && !stop; ++j) {
-          const int site = blockIdx.x + (i0 + j) * gridDim.x;
+          const int lsite = my_lsite[j];
           for (int g = 0; g < ngroups; ++g) {
             const int64_t n = (int64_t)(i0 + j) * ngroups + g;
             if ((int)(n & 1) != pid) continue;
@@ -334,7 +338,7 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
             unsigned char* st = stage_base + (size_t)stage * stage_bytes;
             const int pf = P.p0 + g * pps;
             mbar_expect_tx(&full[stage], stage_bytes);
-            bulk_g2s(st, P.links + ((size_t)site * 9 + pf) * (link_bytes / 2), pps * link_bytes, &full[stage]);
+            bulk_g2s(st, P.links + ((size_t)lsite * 9 + pf) * (link_bytes / 2), pps * link_bytes, &full[stage]);
             for (int pp = 0; pp < pps; ++pp) {
               const int nb = my_nbr[j * 9 + pf + pp];
               bulk_g2s(st + pps * link_bytes + pp * vec_bytes, P.packed + (size_t)nb * (vec_bytes / 2), vec_bytes,
@@ -379,10 +383,12 @@ __global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Param
         for (int g = 0; g < ngroups; ++g) {
           if (!mbar_wait(&full[stage], phase, abort_flag)) { ok = false; break; }
           fence_after();
-          if (pps == 3)
-            issue_stage_kh<3>(kh, dt, adesc0 + st_off, bdesc0 + st_off, a_pt, b_pt, a_ks, b_ks, idesc, g == 0);
-          else
-            issue_stage_kh<1>(kh, dt, adesc0 + st_off, bdesc0 + st_off, a_pt, b_pt, a_ks, b_ks, idesc, g == 0);
+          switch (pps) {
+            case 4: issue_stage_kh<4>(kh, dt, adesc0 + st_off, bdesc0 + st_off, a_pt, b_pt, a_ks, b_ks, idesc, g == 0); break;
+            case 3: issue_stage_kh<3>(kh, dt, adesc0 + st_off, bdesc0 + st_off, a_pt, b_pt, a_ks, b_ks, idesc, g == 0); break;
+            case 2: issue_stage_kh<2>(kh, dt, adesc0 + st_off, bdesc0 + st_off, a_pt, b_pt, a_ks, b_ks, idesc, g == 0); break;
+            default: issue_stage_kh<1>(kh, dt, adesc0 + st_off, bdesc0 + st_off, a_pt, b_pt, a_ks, b_ks, idesc, g == 0);
+          }
           mma_commit(&empty[stage]);
           if (++stage == P.stages) {
             stage = 0;
@@ -521,8 +527,9 @@ __global__ void pack_vec_kernel(const float2* __restrict__ in, uint4* __restrict
       const int slot = active ? active[r] : r;
       const float2* src = in + ((int64_t)s * nrhs + slot) * N + kc * 8;
       float2 x[8];
-      if (aligned16 && (N & 7) == 0) {
-        // `in` is 16-byte aligned (checked on the host) and N, 8*kc are even
+      if (aligned16 && (N & 1) == 0 && kc * 8 + 8 <= N) {
+        // `in` is 16-byte aligned (checked on the host), N and 8*kc are even, and the
+        // chunk lies inside the row (the last chunk of N = 24, 40, ... is partial)
         const float4* s4 = reinterpret_cast<const float4*>(src);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -589,22 +596,32 @@ namespace tc {
 
 // Launch configuration shared by gmg_coarse_apply and gmg_coarse_apply_noalloc:
 // points per stage (3 when enough stages fit, else 1) and the stage count.
-static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int p0, int p1, bool g5, int kind, int nrhs,
+// V output sites; site_map (nullable): link site of each output index; nbr [9][V]: input index per point.
+static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, const int32_t* site_map,
+                                 const int32_t* nbr, int p0, int p1, bool g5, int kind, int nrhs,
                                  float* out, const int32_t* active, int R, bool timed, cudaStream_t s) {
   const int N = h->N;
   const int Rp = round_up(R, 16);
   const int Kc = round_up(N, 16) / 8;
   const int Mp = 2 * N <= 64 ? 64 : 128;
-  const int V = (int)h->dims.vol();
   const uint32_t per_point = (uint32_t)Kc * Mp * 16 + (uint32_t)Kc * 2 * Rp * 16;
-  const size_t fixed = 80 * 8 + 16 + 2 * 32 * 9 * 4;  // barriers (<= 2*32+9), TMEM slot + flag, neighbour tables
+  // barriers (<= 2*32+9), TMEM slot + flag, neighbour and link-site tables of the two producers
+  const size_t tables = 2 * 32 * 9 * 4 + 2 * 32 * 4;
+  const size_t fixed = 80 * 8 + 16 + tables;
   const size_t budget = 227 * 1024 - fixed;
   const int npts = p1 - p0;
-  int pps = (npts % 3 == 0 && budget / (3 * per_point) >= 4) ? 3 : 1;
+  // points per stage: the largest of 4, 3, 2 dividing the point count that
+  // still leaves at least 4 stages, else 1
+  int pps = 1;
+  for (int c : {4, 3, 2})
+    if (npts % c == 0 && budget / (c * per_point) >= 4) {
+      pps = c;
+      break;
+    }
   const uint32_t stage_bytes = pps * per_point;
   const int stages = (int)std::min<size_t>(32, budget / stage_bytes) & ~1;  // even: two producers
   GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil: tile does not fit shared memory");
-  const size_t smem = (size_t)stages * stage_bytes + (size_t)(2 * stages + 2 * kAccBufs + 1) * 8 + 16 + 2 * 32 * 9 * 4;
+  const size_t smem = (size_t)stages * stage_bytes + (size_t)(2 * stages + 2 * kAccBufs + 1) * 8 + 16 + tables;
   GMG_CUDA(cudaFuncSetAttribute(coarse_mrhs_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 148;
   GMG_CUDA(cudaGetDevice(&dev));
@@ -612,7 +629,8 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int p0, int
   Params P;
   P.links = h->links_h.buf.as<uint16_t>();
   P.packed = reinterpret_cast<const uint16_t*>(packed);
-  P.nbr = h->nbr.as<int32_t>();
+  P.nbr = nbr;
+  P.site_map = site_map;
   P.active = active;
   P.out = reinterpret_cast<float2*>(out);
   P.err = h->dev_err.as<int>();
@@ -659,7 +677,27 @@ gmg_status coarse_apply_tc(gmg_coarse* h, int p0, int p1, bool g5, int kind, int
       reinterpret_cast<const float2*>(in), packed, active, V, N, nrhs, R, Rp, Kc, kind, g5 ? 1 : 0,
       (reinterpret_cast<uintptr_t>(in) & 15) == 0 ? 1 : 0);
   GMG_CUDA(cudaGetLastError());
-  return tc::launch_stencil(h, packed, p0, p1, g5, kind, nrhs, out, active, R, true, s);
+  return tc::launch_stencil(h, packed, V, nullptr, h->nbr.as<int32_t>(), p0, p1, g5, kind, nrhs, out, active, R,
+                            true, s);
+}
+
+gmg_status coarse_apply_tc_ex(gmg_coarse* h, int V, int V_in, const int32_t* site_map, const int32_t* nbr, int p0,
+                              int p1, bool g5, int kind, int nrhs, const float* in, float* out,
+                              const int32_t* active, int n_active, cudaStream_t s) {
+  const int N = h->N;
+  const int R = active ? n_active : nrhs;
+  if (R == 0) return GMG_OK;
+  GMG_CHECK(R <= 128, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil supports at most 128 active RHS");
+  const int Rp = tc::round_up(R, 16);
+  const int Kc = tc::round_up(N, 16) / 8;
+  GMG_TRY(h->scratch.alloc((size_t)V_in * Kc * 2 * Rp * 16));
+  uint4* packed = h->scratch.as<uint4>();
+  const int64_t rows = (int64_t)V_in * Kc * Rp;
+  tc::pack_vec_kernel<<<(int)std::min<int64_t>((rows + 255) / 256, 148 * 64), 256, 0, s>>>(
+      reinterpret_cast<const float2*>(in), packed, active, V_in, N, nrhs, R, Rp, Kc, kind, g5 ? 1 : 0,
+      (reinterpret_cast<uintptr_t>(in) & 15) == 0 ? 1 : 0);
+  GMG_CUDA(cudaGetLastError());
+  return tc::launch_stencil(h, packed, V, site_map, nbr, p0, p1, g5, kind, nrhs, out, active, R, true, s);
 }
 
 }  // namespace gmg
@@ -765,5 +803,6 @@ extern "C" gmg_status gmg_coarse_apply_noalloc(gmg_coarse* h, gmg_op op, int poi
       reinterpret_cast<const float2*>(in), packed, active, V, N, nrhs, R, Rp, Kc, compute, g5 ? 1 : 0,
       (reinterpret_cast<uintptr_t>(in) & 15) == 0 ? 1 : 0);
   GMG_CUDA(cudaGetLastError());
-  return tc::launch_stencil(h, packed, p0, p1, g5, compute, nrhs, out, active, R, false, s);
+  return tc::launch_stencil(h, packed, V, nullptr, h->nbr.as<int32_t>(), p0, p1, g5, compute, nrhs, out, active, R,
+                            false, s);
 }

@@ -84,9 +84,28 @@ gmg_status coarse_prepare_f32(gmg_coarse* h, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // the stencil kernel
 // ---------------------------------------------------------------------------
+// Link source and site geometry of one apply.  Output index o (V of them: all
+// sites, or the sites of one parity) takes its links from link site
+// site_map[o] (identity when null): matrix (p - pbase) of the link_pts matrices
+// stored per site; its neighbour for point p is input index nbr[p][o] (o
+// itself when nbr is null).  dag applies the conjugate transpose of each matrix.
+struct LinkSel {
+  const void* links;
+  int link_pts, pbase;
+  const int32_t* site_map;
+  const int32_t* nbr;
+  int dag;
+};
+
+template <class C> __device__ __forceinline__ C cconj(C a) {
+  a.y = -a.y;
+  return a;
+}
+
 template <class T, int TR, int TB>
 __global__ void __launch_bounds__(256) coarse_simt_kernel(
-    const typename cplx_t<T>::type* __restrict__ links, const int32_t* __restrict__ nbr,
+    const typename cplx_t<T>::type* __restrict__ links, int link_pts, int pbase, const int32_t* __restrict__ site_map,
+    const int32_t* __restrict__ nbr, int dag,
     const typename cplx_t<T>::type* __restrict__ in, typename cplx_t<T>::type* __restrict__ out,
     int V, int N, int nrhs, const int32_t* __restrict__ active, int R, int p0, int p1, int g5) {
   typedef typename cplx_t<T>::type C;
@@ -101,6 +120,7 @@ __global__ void __launch_bounds__(256) coarse_simt_kernel(
   const int half = N / 2;
 
   for (int site = blockIdx.x; site < V; site += gridDim.x) {
+    const int64_t lsite = site_map ? site_map[site] : site;
     C acc[TR][TB];
 #pragma unroll
     for (int j = 0; j < TR; ++j)
@@ -108,12 +128,16 @@ __global__ void __launch_bounds__(256) coarse_simt_kernel(
       for (int i = 0; i < TB; ++i) acc[j][i] = C{0, 0};
 
     for (int p = p0; p < p1; ++p) {
-      const C* Ap = links + ((int64_t)site * 9 + p) * N * N;
-      const int nb = nbr[(int64_t)p * V + site];
+      const C* Ap = links + (lsite * link_pts + (p - pbase)) * N * N;
+      const int nb = nbr ? nbr[(int64_t)p * V + site] : site;
       __syncthreads();
-      for (int k = t; k < N * N; k += blockDim.x) {
-        const int b = k / N, bb = k % N;
-        AT[bb * N + b] = Ap[k];
+      if (dag) {  // AT[bb][b] = (A^dag)[b][bb] = conj(A[bb][b])
+        for (int k = t; k < N * N; k += blockDim.x) AT[k] = cconj(Ap[k]);
+      } else {
+        for (int k = t; k < N * N; k += blockDim.x) {
+          const int b = k / N, bb = k % N;
+          AT[bb * N + b] = Ap[k];
+        }
       }
       for (int k = t; k < R * N; k += blockDim.x) {
         const int r = k / N, bb = k % N;
@@ -164,7 +188,7 @@ __global__ void __launch_bounds__(256) coarse_simt_kernel(
 }
 
 template <class T, int TR, int TB>
-static gmg_status launch_simt(const void* links, const int32_t* nbr, const void* in, void* out,
+static gmg_status launch_simt(const LinkSel& L, const void* in, void* out,
                               int V, int N, int nrhs, const int32_t* active, int R, int p0, int p1,
                               int g5, cudaStream_t s) {
   typedef typename cplx_t<T>::type C;
@@ -181,7 +205,7 @@ static gmg_status launch_simt(const void* links, const int32_t* nbr, const void*
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
   const int grid = std::min(V, nsm * std::max(per_sm, 1) * 4);
   KernelTimer kt("coarse_simt", s);
-  kern<<<grid, threads, smem, s>>>(reinterpret_cast<const C*>(links), nbr,
+  kern<<<grid, threads, smem, s>>>(reinterpret_cast<const C*>(L.links), L.link_pts, L.pbase, L.site_map, L.nbr, L.dag,
                                    reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), V, N,
                                    nrhs, active, R, p0, p1, g5);
   GMG_CUDA(cudaGetLastError());
@@ -198,7 +222,9 @@ static gmg_status launch_simt(const void* links, const int32_t* nbr, const void*
 // ---------------------------------------------------------------------------
 template <class T>
 __global__ void __launch_bounds__(576) coarse_1rhs_kernel(const typename cplx_t<T>::type* __restrict__ links,
-                                                          const int32_t* __restrict__ nbr,
+                                                          int link_pts, int pbase,
+                                                          const int32_t* __restrict__ site_map,
+                                                          const int32_t* __restrict__ nbr, int dag,
                                                           const typename cplx_t<T>::type* __restrict__ in,
                                                           typename cplx_t<T>::type* __restrict__ out, int V, int N,
                                                           int nrhs, int slot, int p0, int p1, int g5) {
@@ -210,8 +236,9 @@ __global__ void __launch_bounds__(576) coarse_1rhs_kernel(const typename cplx_t<
   const int p = t / N, b = t % N;  // blockDim = 9 N
   const int half = N / 2;
   for (int site = blockIdx.x; site < V; site += gridDim.x) {
+    const int64_t lsite = site_map ? site_map[site] : site;
     if (p >= p0 && p < p1) {
-      const int nb = nbr[(int64_t)p * V + site];
+      const int nb = nbr ? nbr[(int64_t)p * V + site] : site;
       C v = in[((int64_t)nb * nrhs + slot) * N + b];
       if (g5 && b >= half) { v.x = -v.x; v.y = -v.y; }
       X[p * N + b] = v;
@@ -219,8 +246,13 @@ __global__ void __launch_bounds__(576) coarse_1rhs_kernel(const typename cplx_t<
     __syncthreads();
     C acc{0, 0};
     if (p >= p0 && p < p1) {
-      const C* row = links + (((int64_t)site * 9 + p) * N + b) * N;
-      for (int bb = 0; bb < N; ++bb) acc = cmul_add(acc, row[bb], X[p * N + bb]);
+      const C* Mp = links + (lsite * link_pts + (p - pbase)) * N * N;
+      if (dag) {  // row b of A^dag: conj(A[bb][b])
+        for (int bb = 0; bb < N; ++bb) acc = cmul_add(acc, cconj(Mp[(int64_t)bb * N + b]), X[p * N + bb]);
+      } else {
+        const C* row = Mp + (int64_t)b * N;
+        for (int bb = 0; bb < N; ++bb) acc = cmul_add(acc, row[bb], X[p * N + bb]);
+      }
     }
     part[p * N + b] = acc;
     __syncthreads();
@@ -238,44 +270,58 @@ __global__ void __launch_bounds__(576) coarse_1rhs_kernel(const typename cplx_t<
 }
 
 template <class T>
-static gmg_status launch_1rhs(const void* links, const int32_t* nbr, const void* in, void* out, int V, int N,
+static gmg_status launch_1rhs(const LinkSel& L, const void* in, void* out, int V, int N,
                               int nrhs, int slot, int p0, int p1, int g5, cudaStream_t s) {
   typedef typename cplx_t<T>::type C;
   const int threads = 9 * N;
   const size_t smem = sizeof(C) * 18 * (size_t)N;
   KernelTimer kt("coarse_simt", s);
-  coarse_1rhs_kernel<T><<<V, threads, smem, s>>>(reinterpret_cast<const C*>(links), nbr, reinterpret_cast<const C*>(in),
+  coarse_1rhs_kernel<T><<<V, threads, smem, s>>>(reinterpret_cast<const C*>(L.links), L.link_pts, L.pbase, L.site_map,
+                                                 L.nbr, L.dag, reinterpret_cast<const C*>(in),
                                                  reinterpret_cast<C*>(out), V, N, nrhs, slot, p0, p1, g5);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
 
-gmg_status coarse_apply_simt(gmg_coarse* h, int p0, int p1, bool g5, int compute, int vec_prec,
-                             int nrhs, const void* in, void* out, const int32_t* active,
-                             int n_active, cudaStream_t s) {
-  const int V = (int)h->dims.vol();
+// `src`: 0 = the stencil links, 1 = the self-link inverse (one matrix per site,
+// addressed as point 8).  V / site_map / nbr: the output geometry (full grid
+// when site_map is null and nbr is the handle's table).
+gmg_status coarse_apply_simt_ex(gmg_coarse* h, int src, int V, const int32_t* site_map, const int32_t* nbr,
+                                bool dag, int p0, int p1, bool g5, int compute, int vec_prec, int nrhs,
+                                const void* in, void* out, const int32_t* active, int n_active, cudaStream_t s) {
   const int N = h->N;
   const int R = active ? n_active : nrhs;
   if (R == 0) return GMG_OK;
-  const int32_t* nbr = h->nbr.as<int32_t>();
-  if (R == 1 && !active && N <= 64) {
-    if (compute == GMG_F64 && vec_prec == GMG_F64)
-      return launch_1rhs<double>(h->links_d.p, nbr, in, out, V, N, nrhs, 0, p0, p1, g5, s);
-    if (compute == GMG_F32 && vec_prec == GMG_F32 && h->links_f_ok)
-      return launch_1rhs<float>(h->links_f.p, nbr, in, out, V, N, nrhs, 0, p0, p1, g5, s);
-  }
+  LinkSel L{nullptr, src == 1 ? 1 : 9, src == 1 ? 8 : 0, site_map, nbr, dag ? 1 : 0};
   if (compute == GMG_F64) {
     GMG_CHECK(vec_prec == GMG_F64, GMG_ERR_UNSUPPORTED, "F64 compute needs F64 vectors");
-    if (R >= 4) return launch_simt<double, 4, 4>(h->links_d.p, nbr, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
-    return launch_simt<double, 1, 2>(h->links_d.p, nbr, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
-  }
-  if (compute == GMG_F32) {
+    L.links = src == 1 ? h->self_inv.p : h->links_d.p;
+  } else if (compute == GMG_F32) {
     GMG_CHECK(vec_prec == GMG_F32, GMG_ERR_UNSUPPORTED, "F32 compute needs F32 vectors");
-    GMG_CHECK(h->links_f_ok, GMG_ERR_STATE, "F32 links not prepared (gmg_coarse_prepare)");
-    if (R >= 4) return launch_simt<float, 4, 4>(h->links_f.p, nbr, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
-    return launch_simt<float, 1, 2>(h->links_f.p, nbr, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
+    GMG_CHECK(src == 1 ? h->self_inv_f_ok : h->links_f_ok, GMG_ERR_STATE,
+              "F32 links not prepared (gmg_coarse_prepare)");
+    L.links = src == 1 ? h->self_inv_f.p : h->links_f.p;
+  } else {
+    return fail(GMG_ERR_UNSUPPORTED, "coarse apply: unsupported compute precision for SIMT path");
   }
-  return fail(GMG_ERR_UNSUPPORTED, "coarse apply: unsupported compute precision for SIMT path");
+  GMG_CHECK(L.links != nullptr, GMG_ERR_STATE, "coarse apply: link source not built");
+  if (R == 1 && !active && N <= 64) {
+    if (compute == GMG_F64) return launch_1rhs<double>(L, in, out, V, N, nrhs, 0, p0, p1, g5, s);
+    return launch_1rhs<float>(L, in, out, V, N, nrhs, 0, p0, p1, g5, s);
+  }
+  if (compute == GMG_F64) {
+    if (R >= 4) return launch_simt<double, 4, 4>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
+    return launch_simt<double, 1, 2>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
+  }
+  if (R >= 4) return launch_simt<float, 4, 4>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
+  return launch_simt<float, 1, 2>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
+}
+
+gmg_status coarse_apply_simt(gmg_coarse* h, int p0, int p1, bool g5, int compute, int vec_prec,
+                             int nrhs, const void* in, void* out, const int32_t* active,
+                             int n_active, cudaStream_t s) {
+  return coarse_apply_simt_ex(h, 0, (int)h->dims.vol(), nullptr, h->nbr.as<int32_t>(), false, p0, p1, g5, compute,
+                              vec_prec, nrhs, in, out, active, n_active, s);
 }
 
 // ---------------------------------------------------------------------------

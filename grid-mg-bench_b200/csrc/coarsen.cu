@@ -173,6 +173,7 @@ static gmg_status coarsen_generic(gmg_coarse* out, gmg_agg* agg, const FineOpRef
   GMG_TRY(coarse_links_to_site_major(out, s));
   out->links_set = true;
   out->links_f_ok = false;
+  out->self_inv_ok = out->self_inv_f_ok = false;
   out->links_h.kind = -1;
   // temporaries are freed at scope exit: make sure the stream is done with them
   GMG_CUDA(cudaStreamSynchronize(s));

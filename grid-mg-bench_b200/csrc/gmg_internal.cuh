@@ -97,6 +97,13 @@ struct gmg_coarse {
   gmg::LinksF16 links_h;
   gmg::DevBuf scratch;     // per-handle temporary: packed tensor-core vectors
   gmg::DevBuf dev_err;     // int: first error code a kernel of this handle recorded
+  // red-black operator (coarse_rb.cu)
+  gmg::DevBuf self_inv;    // complex<double> [V][N][N]: inverse of the self-stencil link
+  gmg::DevBuf self_inv_f;  // complex<float> copy
+  bool self_inv_ok = false, self_inv_f_ok = false;
+  gmg::DevBuf rb_site;     // int32 [2][V/2]: full site of half index h of parity q
+  gmg::DevBuf rb_nbr;      // int32 [2][9][V/2]: half index (other / same parity) of point p's neighbour
+  bool rb_ok = false;
 };
 
 struct gmg_agg {
@@ -140,6 +147,10 @@ gmg_status coarse_prepare_f32(gmg_coarse* h, cudaStream_t s);
 gmg_status coarse_apply_simt(gmg_coarse* h, int p0, int p1, bool g5, int compute, int vec_prec,
                              int nrhs, const void* in, void* out, const int32_t* active,
                              int n_active, cudaStream_t s);
+// src 0: stencil links, 1: self-link inverse; V / site_map / nbr: output geometry; dag: conjugate-transposed links
+gmg_status coarse_apply_simt_ex(gmg_coarse* h, int src, int V, const int32_t* site_map, const int32_t* nbr,
+                                bool dag, int p0, int p1, bool g5, int compute, int vec_prec, int nrhs,
+                                const void* in, void* out, const int32_t* active, int n_active, cudaStream_t s);
 gmg_status coarse_construct_remaining(gmg_coarse* h, cudaStream_t s);
 
 // tensor-core multi-RHS stencil (coarse_mrhs_tc.cu)
@@ -147,6 +158,11 @@ gmg_status coarse_prepare_tc(gmg_coarse* h, int kind, cudaStream_t s);
 gmg_status coarse_apply_tc(gmg_coarse* h, int p0, int p1, bool g5, int kind, int nrhs,
                            const float* in, float* out, const int32_t* active, int n_active,
                            cudaStream_t s);
+// the same on a sub-geometry: V output sites, site_map (nullable) -> link site, nbr [9][V] -> input index,
+// V_in input sites
+gmg_status coarse_apply_tc_ex(gmg_coarse* h, int V, int V_in, const int32_t* site_map, const int32_t* nbr, int p0,
+                              int p1, bool g5, int kind, int nrhs, const float* in, float* out,
+                              const int32_t* active, int n_active, cudaStream_t s);
 
 // aggregation kernels (block_ops.cu)
 gmg_status agg_build_tables(gmg_agg* h, cudaStream_t s);

@@ -126,6 +126,63 @@ gmg_status zero(Vec& v, cudaStream_t s) {
 }
 
 
+// ------------------------------------------------------------- global orthonormalisation
+// Orthonormalise the R columns of X over the whole lattice, as the reference's
+// test-vector setup does before and after the solves (BasisVectors.h:86-147,
+// setupPre/PostOrthonormalise, MultigridParams.h:103-104): Cholesky QR on the
+// R x R Gram matrix (formed on the device, factored on the host), two passes;
+// a pass whose factorisation breaks down is redone with the shifted-Cholesky
+// diagonal shift and followed by extra plain passes.
+gmg_status global_orthonormalise(gmg_mg* h, Vec& X, cudaStream_t s) {
+  const int R = X.R;
+  double2* G = h->dscr.as<double2>();
+  const double K = (double)X.V * X.dof;
+  int passes = 2;
+  for (int pass = 0; pass < passes; ++pass) {
+    GMG_TRY(vec_gram(X, G, s));
+    std::vector<zc> g;
+    GMG_TRY(download(h, G, R * R, g, s));
+    std::vector<zc> L;
+    auto chol = [&](double shift) -> bool {
+      L.assign((size_t)R * R, zc(0));
+      for (int j = 0; j < R; ++j) {
+        double d = g[(size_t)j * R + j].real() + shift;
+        for (int k = 0; k < j; ++k) d -= std::norm(L[(size_t)j * R + k]);
+        if (!(d > 0.0)) return false;
+        const double dj = std::sqrt(d);
+        L[(size_t)j * R + j] = dj;
+        for (int i = j + 1; i < R; ++i) {  // L[i][j] = (G[i][j] - sum_k L[i][k] conj(L[j][k])) / L[j][j]
+          zc v = g[(size_t)i * R + j];
+          for (int k = 0; k < j; ++k) v -= L[(size_t)i * R + k] * std::conj(L[(size_t)j * R + k]);
+          L[(size_t)i * R + j] = v / dj;
+        }
+      }
+      return true;
+    };
+    if (!chol(0.0)) {
+      double tr = 0.0;
+      for (int i = 0; i < R; ++i) tr += g[(size_t)i * R + i].real();
+      const double shift = 11.0 * (K * R + (double)R * (R + 1)) * 1.1102230246251565e-16 * tr;
+      if (!chol(shift)) return fail(GMG_ERR_NONFINITE, "mg setup: test vectors are linearly dependent");
+      passes = std::min(pass + 3, 5);
+    }
+    // T = conj(L^{-1}) (lower triangular): X(a) <- sum_{b <= a} T[a][b] X(b)
+    std::vector<zc> Li((size_t)R * R, zc(0));
+    for (int j = 0; j < R; ++j) {
+      Li[(size_t)j * R + j] = 1.0 / L[(size_t)j * R + j];
+      for (int i = j + 1; i < R; ++i) {
+        zc acc = 0.0;
+        for (int k = j; k < i; ++k) acc += L[(size_t)i * R + k] * Li[(size_t)k * R + j];
+        Li[(size_t)i * R + j] = -acc / L[(size_t)i * R + i];
+      }
+    }
+    for (auto& v : Li) v = std::conj(v);
+    GMG_TRY(upload(h, Li, 0, s));
+    GMG_TRY(vec_tri_apply(h->coef.as<double2>(), X, s));
+  }
+  return GMG_OK;
+}
+
 // ------------------------------------------------------------- MR smoother
 // x <- x + iters steps of minimal residual for A x = b on level l
 // The step lengths stay on the device: no host synchronisation.
@@ -456,6 +513,7 @@ extern "C" gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream stream) {
     GMG_TRY(sw.alloc(L.V, nv, L.dof, L.vprec));
     GMG_TRY(st.alloc(L.V, nv, L.dof, L.vprec));
     GMG_TRY(vec_gaussian(v, P.seed * 7919 + l, s));
+    GMG_TRY(global_orthonormalise(h, v, s));  // setupPreOrthonormalise
     GMG_CUDA(cudaMemsetAsync(psi.p, 0, psi.bytes(), s));
     Krylov K;
     K.V0 = sV;
@@ -464,6 +522,7 @@ extern "C" gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream stream) {
     K.tz = st;
     auto none = [](const Vec&, Vec&, const Vec&) { return GMG_OK; };
     GMG_TRY(fgmres(h, l, v, psi, K, ms, P.setup_iters, 1e-3, none, false, nullptr, nullptr, s));
+    GMG_TRY(global_orthonormalise(h, psi, s));  // setupPostOrthonormalise
     // chiral doubling -> basis, block orthonormalisation, Galerkin coarsening
     DevBuf basis;
     GMG_TRY(basis.alloc(sizeof(double2) * 2 * (size_t)nv * L.V * L.dof));

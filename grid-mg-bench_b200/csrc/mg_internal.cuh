@@ -60,5 +60,9 @@ gmg_status vec_scale_inv_norm(const double2* n_dev, const Vec& X, Vec& Y, cudaSt
 gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s);
 // Y = X - Y
 gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s);
+// G[a][b] = <X(a), X(b)> over the whole lattice (R <= 32 columns), FP64
+gmg_status vec_gram(const Vec& X, double2* G_dev, cudaStream_t s);
+// X(a) <- sum_{b <= a} T[a][b] X(b)   (lower-triangular recombination of the columns)
+gmg_status vec_tri_apply(const double2* T_dev, Vec& X, cudaStream_t s);
 
 }  // namespace gmg

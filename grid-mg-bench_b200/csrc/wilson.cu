@@ -54,6 +54,12 @@ template <class C> __device__ __forceinline__ C cphase(C a, int code) {
 // gamma_mu row s has one non-zero entry at column perm, value phase code
 __constant__ int c_gperm[4][4] = {{3, 2, 1, 0}, {3, 2, 1, 0}, {2, 3, 0, 1}, {2, 3, 0, 1}};
 __constant__ int c_gphase[4][4] = {{1, 1, 3, 3}, {2, 0, 0, 2}, {1, 3, 3, 1}, {0, 0, 0, 0}};
+// the same tables as constexpr functions: with mu and s known at compile time
+// (unrolled loops) the spinor indices fold and the spinors stay in registers
+__host__ __device__ constexpr int gperm(int mu, int s) { return mu < 2 ? 3 - s : (s ^ 2); }
+__host__ __device__ constexpr int gphase(int mu, int s) {
+  return mu == 0 ? (s < 2 ? 1 : 3) : mu == 1 ? ((s == 0 || s == 3) ? 2 : 0) : mu == 2 ? ((s == 0 || s == 3) ? 1 : 3) : 0;
+}
 
 // accumulate one hop into out[4][3]
 template <class T>
@@ -67,8 +73,8 @@ __device__ __forceinline__ void wilson_hop(typename wt<T>::C out[4][3],
   C h[2][3];
 #pragma unroll
   for (int s = 0; s < 2; ++s) {
-    const int ps = c_gperm[mu][s];
-    const int code = (c_gphase[mu][s] + sgc) & 3;
+    const int ps = gperm(mu, s);
+    const int code = (gphase(mu, s) + sgc) & 3;
 #pragma unroll
     for (int c = 0; c < 3; ++c) h[s][c] = cadd(psi[s * 3 + c], cphase(psi[ps * 3 + c], code));
   }
@@ -94,8 +100,8 @@ __device__ __forceinline__ void wilson_hop(typename wt<T>::C out[4][3],
     }
 #pragma unroll
   for (int s = 2; s < 4; ++s) {
-    const int ps = c_gperm[mu][s];
-    const int code = (c_gphase[mu][s] + sgc) & 3;
+    const int ps = gperm(mu, s);
+    const int code = (gphase(mu, s) + sgc) & 3;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const C v = cphase(uh[ps][a], code);
@@ -105,6 +111,74 @@ __device__ __forceinline__ void wilson_hop(typename wt<T>::C out[4][3],
   }
 }
 
+// One output spinor (site, rhs).  links(p) returns the 3x3 link of hop p
+// (p < 4: U_mu(x), p >= 4: U_mu(x - mu), applied daggered); cl: the site's
+// two 6x6 clover blocks.
+template <class T, class LinkFn>
+__device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict__ cl, LinkFn links,
+                                            const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
+                                            typename wt<T>::C* __restrict__ out, int V, int nrhs, int site, int r,
+                                            T diag, int op, int dir, int disp, int apbc, int tvol, int Lt) {
+  typedef typename wt<T>::C C;
+  const bool g5 = (op == GMG_OP_MDAG);
+  const int tc = site / tvol;
+  C acc[4][3];
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[s][c] = C{0, 0};
+  if (op != GMG_OP_MDIR) {
+    // diagonal: (4 + m) psi + Cl psi, two chiral 6x6 blocks
+    C psi[12];
+    const C* src = in + ((int64_t)site * nrhs + r) * 12;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      psi[k] = src[k];
+      if (g5 && k >= 6) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
+    }
+#pragma unroll
+    for (int blk = 0; blk < 2; ++blk)
+#pragma unroll
+      for (int a = 0; a < 6; ++a) {
+        C v;
+        v.x = diag * psi[blk * 6 + a].x;
+        v.y = diag * psi[blk * 6 + a].y;
+#pragma unroll
+        for (int b = 0; b < 6; ++b) v = cadd(v, cmul(cl[(blk * 6 + a) * 6 + b], psi[blk * 6 + b]));
+        acc[(blk * 6 + a) / 3][(blk * 6 + a) % 3] = v;
+      }
+  }
+  if (op != GMG_OP_MDIAG) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      const int mu = p & 3;
+      const int dsp = p < 4 ? 1 : -1;
+      if (op == GMG_OP_MDIR && (mu != dir || dsp != disp)) continue;
+      const int nb = nbr[(int64_t)p * V + site];
+      T coef = (T)-0.5;
+      if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
+      C psi[12];
+      const C* src = in + ((int64_t)nb * nrhs + r) * 12;
+#pragma unroll
+      for (int k = 0; k < 12; ++k) {
+        psi[k] = src[k];
+        if (g5 && k >= 6) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
+      }
+      wilson_hop<T>(acc, links(p, nb), dsp < 0, psi, mu, dsp, coef);
+    }
+  }
+  C* dst = out + ((int64_t)site * nrhs + r) * 12;
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      C v = acc[s][c];
+      if (g5 && s >= 2) { v.x = -v.x; v.y = -v.y; }
+      dst[s * 3 + c] = v;
+    }
+}
+
+// thread per (site, rhs); links and clover read from global memory (few RHS)
 template <class T>
 __global__ void __launch_bounds__(256) wilson_kernel(
     const typename wt<T>::C* __restrict__ gauge, const typename wt<T>::C* __restrict__ clover,
@@ -113,67 +187,55 @@ __global__ void __launch_bounds__(256) wilson_kernel(
     int apbc, int tvol, int Lt) {
   typedef typename wt<T>::C C;
   const int64_t total = (int64_t)V * nrhs;
-  const bool g5 = (op == GMG_OP_MDAG);
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
     const int site = (int)(e / nrhs);
     const int r = (int)(e % nrhs);
-    const int tc = site / tvol;
-    C acc[4][3];
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) acc[s][c] = C{0, 0};
-    if (op != GMG_OP_MDIR) {
-      // diagonal: (4 + m) psi + Cl psi, two chiral 6x6 blocks
-      C psi[12];
-      const C* src = in + ((int64_t)site * nrhs + r) * 12;
-#pragma unroll
-      for (int k = 0; k < 12; ++k) {
-        psi[k] = src[k];
-        if (g5 && k >= 6) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
-      }
-      const C* cl = clover + (int64_t)site * 72;
-#pragma unroll
-      for (int blk = 0; blk < 2; ++blk)
-#pragma unroll
-        for (int a = 0; a < 6; ++a) {
-          C v;
-          v.x = diag * psi[blk * 6 + a].x;
-          v.y = diag * psi[blk * 6 + a].y;
-#pragma unroll
-          for (int b = 0; b < 6; ++b) v = cadd(v, cmul(cl[(blk * 6 + a) * 6 + b], psi[blk * 6 + b]));
-          acc[(blk * 6 + a) / 3][(blk * 6 + a) % 3] = v;
-        }
+    auto links = [&](int p, int nb) -> const C* {
+      return gauge + ((int64_t)(p < 4 ? site : nb) * 4 + (p & 3)) * 9;
+    };
+    wilson_site<T>(clover + (int64_t)site * 72, links, nbr, in, out, V, nrhs, site, r, diag, op, dir, disp, apbc, tvol,
+                   Lt);
+  }
+}
+
+// Multi-RHS tile: a CTA takes kTileSites consecutive sites and all right-hand
+// sides (rt threads per site, each looping over its RHS); the sites' 8 hop
+// links and clover blocks are staged in shared memory once and read by every
+// RHS of the tile instead of once per RHS from global memory.
+constexpr int kTileSites = 16;
+
+template <class T>
+__global__ void __launch_bounds__(256) wilson_tile_kernel(
+    const typename wt<T>::C* __restrict__ gauge, const typename wt<T>::C* __restrict__ clover,
+    const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
+    typename wt<T>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
+    int apbc, int tvol, int Lt) {
+  typedef typename wt<T>::C C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* Ls = reinterpret_cast<C*>(smem_raw);  // [kTileSites][8][9]: p < 4 U_mu(x), p >= 4 U_mu(x - mu)
+  C* Cs = Ls + kTileSites * 72;            // [kTileSites][72]
+  const int nt = (V + kTileSites - 1) / kTileSites;
+  const int sl = threadIdx.x / rt, rl = threadIdx.x % rt;
+  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+    const int s0 = tile * kTileSites;
+    const int ns = min(kTileSites, V - s0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < ns * 72; k += blockDim.x) {
+      const int j = k / 72, e = k % 72, p = e / 9, m = e % 9;
+      const int site = s0 + j;
+      const int ls = p < 4 ? site : nbr[(int64_t)p * V + site];
+      Ls[k] = gauge[((int64_t)ls * 4 + (p & 3)) * 9 + m];
+      Cs[k] = clover[(int64_t)s0 * 72 + k];
     }
-    if (op != GMG_OP_MDIAG) {
-      for (int p = 0; p < 8; ++p) {
-        const int mu = p & 3;
-        const int dsp = p < 4 ? 1 : -1;
-        if (op == GMG_OP_MDIR && (mu != dir || dsp != disp)) continue;
-        const int nb = nbr[(int64_t)p * V + site];
-        T coef = (T)-0.5;
-        if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
-        C psi[12];
-        const C* src = in + ((int64_t)nb * nrhs + r) * 12;
-#pragma unroll
-        for (int k = 0; k < 12; ++k) {
-          psi[k] = src[k];
-          if (g5 && k >= 6) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
-        }
-        const C* U = gauge + ((int64_t)(dsp > 0 ? site : nb) * 4 + mu) * 9;
-        wilson_hop<T>(acc, U, dsp < 0, psi, mu, dsp, coef);
-      }
+    __syncthreads();
+    if (sl < ns) {
+      const int site = s0 + sl;
+      const C* lsite = Ls + sl * 72;
+      auto links = [&](int p, int) -> const C* { return lsite + p * 9; };
+      for (int r = rl; r < nrhs; r += rt)
+        wilson_site<T>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op, dir, disp, apbc, tvol, Lt);
     }
-    C* dst = out + ((int64_t)site * nrhs + r) * 12;
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        C v = acc[s][c];
-        if (g5 && s >= 2) { v.x = -v.x; v.y = -v.y; }
-        dst[s * 3 + c] = v;
-      }
   }
 }
 
@@ -307,6 +369,30 @@ gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, 
   const int64_t total = (int64_t)V * nrhs;
   const int grid = (int)std::min<int64_t>((total + 127) / 128, 148 * 32);
   KernelTimer kt("wilson", s);
+  if (nrhs >= 4 && op != GMG_OP_MDIR) {
+    // multi-RHS tile: up to 16 threads per site, links and clover in shared memory
+    const int rt = std::min(nrhs, 16);
+    const int threads = kTileSites * rt;
+    const int tiles = (V + kTileSites - 1) / kTileSites;
+    const int g = std::min(tiles, 148 * 16);
+    if (vec_prec == GMG_F64) {
+      const size_t smem = sizeof(double2) * 2 * kTileSites * 72;
+      wilson_tile_kernel<double><<<g, threads, smem, s>>>(h->gauge.as<double2>(), h->clover.as<double2>(),
+                                                          h->nbr.as<int32_t>(), (const double2*)in, (double2*)out, V,
+                                                          nrhs, rt, 4.0 + h->mass, op, dir, disp, h->apbc, tvol,
+                                                          h->dims.d[3]);
+    } else if (vec_prec == GMG_F32) {
+      const size_t smem = sizeof(float2) * 2 * kTileSites * 72;
+      wilson_tile_kernel<float><<<g, threads, smem, s>>>(h->gauge_f.as<float2>(), h->clover_f.as<float2>(),
+                                                         h->nbr.as<int32_t>(), (const float2*)in, (float2*)out, V,
+                                                         nrhs, rt, (float)(4.0 + h->mass), op, dir, disp, h->apbc,
+                                                         tvol, h->dims.d[3]);
+    } else {
+      return fail(GMG_ERR_UNSUPPORTED, "wilson apply: vectors must be F64 or F32");
+    }
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  }
   if (vec_prec == GMG_F64) {
     wilson_kernel<double><<<grid, 128, 0, s>>>(h->gauge.as<double2>(), h->clover.as<double2>(),
                                                 h->nbr.as<int32_t>(), (const double2*)in, (double2*)out, V,

@@ -4,7 +4,9 @@ Mirrors the reference's class surface so that tests read like the reference's
 own drivers:
 
   CoarsenedMatrix   M, Mdag, Mdiag, Mdir, MdirAll, CoarsenOperator, links A
-                    (include/CoarsenedMatrixUpstream.h:515-931)
+                    (include/CoarsenedMatrixUpstream.h:515-931); red-black
+                    Dhop, Meooe[Dag], Mooee[Inv][Dag], InvertSelfStencilPoint
+                    (include/CoarsenedMatrixRework.h:178-245, 617-679)
   Aggregation       Orthogonalise, CheckOrthogonal, ProjectToSubspace,
                     PromoteFromSubspace, subspace (...LutMRHS.h:293-352)
   WilsonClover      Op/AdjOp/OpDiag/OpDir of the fine operator
@@ -26,6 +28,8 @@ _LIB = None
 
 F64, F32, BF16, F16 = 0, 1, 2, 3
 OP_M, OP_MDAG, OP_MDIAG, OP_MDIR = 0, 1, 2, 3
+RB_MEOOE, RB_MEOOE_DAG, RB_MOOEE, RB_MOOEE_DAG, RB_MOOEE_INV, RB_MOOEE_INV_DAG = range(6)
+EVEN, ODD = 0, 1
 PREC = {"f64": F64, "f32": F32, "bf16": BF16, "f16": F16}
 
 
@@ -162,6 +166,60 @@ class CoarsenedMatrix:
     def construct_remaining_links(self):
         _chk(lib().gmg_coarse_construct_remaining_links(self._h, _stream()))
 
+    # ---------------------------------------------------- red-black interface
+    # Half fields: [V/2, nrhs, N], sites of one parity (x+y+z+t) % 2 at half
+    # index x/2 + (Lx/2)(y + Ly(z + Lz t)).
+    def InvertSelfStencilPoint(self):
+        _chk(lib().gmg_coarse_invert_self(self._h, _stream()))
+
+    def _rb(self, op, cb, inp, out, compute):
+        _check_vec(inp, self.V // 2, self.N, "in")
+        _check_vec(out, self.V // 2, self.N, "out")
+        vp = _vec_prec(inp)
+        if _vec_prec(out) != vp or out.shape != inp.shape:
+            raise ValueError("in and out must match in shape and dtype")
+        c = vp if compute is None else PREC.get(compute, compute)
+        _chk(lib().gmg_coarse_apply_rb(self._h, op, int(cb), c, vp, inp.shape[1], _ptr(inp), _ptr(out), _stream()))
+        return out
+
+    def Meooe(self, inp, out, cb, compute=None):
+        """in: half field of parity cb -> out: parity 1 - cb (DhopOE for cb even, DhopEO for odd)."""
+        return self._rb(RB_MEOOE, cb, inp, out, compute)
+
+    def MeooeDag(self, inp, out, cb, compute=None):
+        return self._rb(RB_MEOOE_DAG, cb, inp, out, compute)
+
+    def _mooee(self, op, inp, out, cb, compute):
+        if cb is not None:
+            return self._rb(op, cb, inp, out, compute)
+        _check_vec(inp, self.V, self.N, "in")
+        _check_vec(out, self.V, self.N, "out")
+        vp = _vec_prec(inp)
+        c = vp if compute is None else PREC.get(compute, compute)
+        _chk(lib().gmg_coarse_mooee(self._h, op, c, vp, inp.shape[1], _ptr(inp), _ptr(out), _stream()))
+        return out
+
+    def Mooee(self, inp, out, cb=None, compute=None):
+        """Self point; cb None = full grid, else a half field of parity cb."""
+        return self._mooee(RB_MOOEE, inp, out, cb, compute)
+
+    def MooeeDag(self, inp, out, cb=None, compute=None):
+        return self._mooee(RB_MOOEE_DAG, inp, out, cb, compute)
+
+    def MooeeInv(self, inp, out, cb=None, compute=None):
+        return self._mooee(RB_MOOEE_INV, inp, out, cb, compute)
+
+    def MooeeInvDag(self, inp, out, cb=None, compute=None):
+        return self._mooee(RB_MOOEE_INV_DAG, inp, out, cb, compute)
+
+    def Dhop(self, inp, out, dag=0, compute=None):
+        _check_vec(inp, self.V, self.N, "in")
+        _check_vec(out, self.V, self.N, "out")
+        vp = _vec_prec(inp)
+        c = vp if compute is None else PREC.get(compute, compute)
+        _chk(lib().gmg_coarse_dhop(self._h, int(dag), c, vp, inp.shape[1], _ptr(inp), _ptr(out), _stream()))
+        return out
+
     def neighbors(self):
         n = np.zeros((9, self.V), dtype=np.int32)
         _chk(lib().gmg_coarse_neighbors(self._h, n.ctypes.data_as(ctypes.c_void_p)))
@@ -174,6 +232,19 @@ class CoarsenedMatrix:
             _chk(lib().gmg_coarsen_coarse(self._h, agg._h, linop._h, _stream()))
         else:
             raise TypeError("linop must be WilsonClover or CoarsenedMatrix")
+
+
+def pick_checkerboard(dims, cb, full, half):
+    """Grid's pickCheckerboard on device fields [V, ...] -> [V/2, ...] (complex128 / complex64)."""
+    per = int(np.prod(full.shape[1:])) if full.dim() > 1 else 1
+    _chk(lib().gmg_pick_checkerboard(_dims(dims), int(cb), per, _vec_prec(full), _ptr(full), _ptr(half), _stream()))
+    return half
+
+
+def set_checkerboard(dims, cb, half, full):
+    per = int(np.prod(half.shape[1:])) if half.dim() > 1 else 1
+    _chk(lib().gmg_set_checkerboard(_dims(dims), int(cb), per, _vec_prec(half), _ptr(half), _ptr(full), _stream()))
+    return full
 
 
 class Aggregation:

@@ -8,6 +8,8 @@
 //   (3) 0 == (1 - R P) v_c
 //   (4) 0 == (R D P - D_c) v_c                           Galerkin identity
 //   (5) 0 == Im(v_c^dag D_c^dag D_c v_c)                 Mdag is the adjoint
+// and the red-black identities of src/Test_coarse_red_black.cc:170-482:
+//   (6) M = Dhop + Mdiag   (7) MooeeInv Mooee = 1   (8) M = Meo + Moe + Mee + Moo
 // Prints one line per check and exits non-zero if any check fails.
 #include <cuda_runtime.h>
 
@@ -154,6 +156,43 @@ int main() {
     cplx dot = 0;
     for (size_t i = 0; i < a.size(); ++i) dot += std::conj(a[i]) * b[i];
     ok &= report("Im(v^dag Dc^dag Dc v) / Re(...)", std::abs(dot.imag()) / std::abs(dot.real()), 1e-12);
+
+    // red-black interface (src/Test_coarse_red_black.cc:170-482)
+    // (6) Dhop + Mdiag = M
+    Dc.Dhop(c.f, c2.f, 0);
+    Dc.Mdiag(c.f, c3.f);
+    {
+      auto x = c2.get(), y = c3.get();
+      for (size_t i = 0; i < x.size(); ++i) x[i] += y[i];
+      Dc.M(c.f, c3.f);
+      ok &= report("M - (Dhop + Mdiag)", rel_dev(c3.get(), x), 1e-13);
+    }
+    // (7) MooeeInv Mooee = 1 on each checkerboard, (8) Meo + Moe + Mee + Moo = M
+    Dc.InvertSelfStencilPoint();
+    DevField he(Vc / 2, 1, N), ho(Vc / 2, 1, N), t1(Vc / 2, 1, N), t2(Vc / 2, 1, N), full(Vc, 1, N);
+    gmg::PickCheckerboard(0, cdims, c.f, he.f);
+    gmg::PickCheckerboard(1, cdims, c.f, ho.f);
+    Dc.Mooee(he.f, t1.f, 0);
+    Dc.MooeeInv(t1.f, t2.f, 0);
+    ok &= report("(1 - MooeeInv Mooee) v_e", rel_dev(he.get(), t2.get()), 1e-13);
+    Dc.Meooe(he.f, t1.f, 0);  // -> odd
+    Dc.Mooee(ho.f, t2.f, 1);
+    {
+      auto x = t1.get(), y = t2.get();
+      for (size_t i = 0; i < x.size(); ++i) x[i] += y[i];
+      t1.set(x);
+    }
+    gmg::SetCheckerboard(cdims, t1.f, 1, full.f);
+    Dc.Meooe(ho.f, t1.f, 1);  // -> even
+    Dc.Mooee(he.f, t2.f, 0);
+    {
+      auto x = t1.get(), y = t2.get();
+      for (size_t i = 0; i < x.size(); ++i) x[i] += y[i];
+      t1.set(x);
+    }
+    gmg::SetCheckerboard(cdims, t1.f, 0, full.f);
+    Dc.M(c.f, c3.f);
+    ok &= report("M - (Meo + Moe + Mee + Moo)", rel_dev(c3.get(), full.get()), 1e-13);
   } catch (const gmg::Error& e) {
     std::printf("gmg error %d: %s\n", (int)e.status, e.what());
     return 2;

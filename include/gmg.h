@@ -122,6 +122,52 @@ gmg_status gmg_coarse_mdir_all(gmg_coarse* h, gmg_prec compute, gmg_prec vec_pre
    backward ones, A_{+mu}(x) = S o A_{-mu}(x+mu)^dag (S = 1 if hermitian). */
 gmg_status gmg_coarse_construct_remaining_links(gmg_coarse* h, gmg_stream s);
 
+/* ------------------------------------------------------------------------ */
+/* Red-black (checkerboarded) coarse operator: the Schur interface of        */
+/* Rework::CoarsenedMatrix (CoarsenedMatrixRework.h:178-245, 288-394,        */
+/* 617-679).  A half field holds the sites of one parity q = (x+y+z+t) % 2    */
+/* as [V/2][nrhs][nbasis], half index h = x/2 + (Lx/2)*(y + Ly*(z + Lz*t))    */
+/* (Grid's red-black grid, checkerboarded in x); all extents must be even.   */
+/* ------------------------------------------------------------------------ */
+typedef enum {
+  GMG_RB_MEOOE = 0,         /* out (parity 1-cb) = sum of the 8 hops of in (parity cb): DhopOE / DhopEO */
+  GMG_RB_MEOOE_DAG = 1,     /* G5C Meooe G5C (DhopInternal with dag, :289-346) */
+  GMG_RB_MOOEE = 2,         /* out (parity cb) = A_self in                 (Mooee, :202) */
+  GMG_RB_MOOEE_DAG = 3,     /* adj(A_self) in                              (MooeeDag, :206) */
+  GMG_RB_MOOEE_INV = 4,     /* A_self^-1 in, after gmg_coarse_invert_self  (MooeeInv, :204) */
+  GMG_RB_MOOEE_INV_DAG = 5  /* adj(A_self^-1) in                           (MooeeInvDag, :208) */
+} gmg_rb_op;
+
+/* InvertSelfStencilPoint (CoarsenedMatrixRework.h:642-668): inverse of every
+   site's self-stencil link, on the device in FP64 (Gauss-Jordan, partial
+   pivoting), kept with an FP32 copy.  Synchronises the stream; returns
+   GMG_ERR_NONFINITE if a self link is singular.  Setting or rebuilding the
+   links drops the inverse. */
+gmg_status gmg_coarse_invert_self(gmg_coarse* h, gmg_stream s);
+
+/* Meooe / MeooeDag on half fields (in of parity cb, out of parity 1-cb) and
+   Mooee / MooeeDag / MooeeInv / MooeeInvDag (in and out of parity cb).
+   compute as for gmg_coarse_apply: the BF16 / F16 hops run on the tensor
+   cores (F32 vectors); the self-point ops run in FP32 for those requests. */
+gmg_status gmg_coarse_apply_rb(gmg_coarse* h, gmg_rb_op op, int cb, gmg_prec compute, gmg_prec vec_prec,
+                               int nrhs, const void* in, void* out, gmg_stream s);
+
+/* Dhop (CoarsenedMatrixRework.h:210-217) on the full grid: the 8 hopping
+   points; dag != 0 gives G5C Dhop G5C. */
+gmg_status gmg_coarse_dhop(gmg_coarse* h, int dag, gmg_prec compute, gmg_prec vec_prec, int nrhs,
+                           const void* in, void* out, gmg_stream s);
+
+/* Mooee family on the full grid (op GMG_RB_MOOEE .. GMG_RB_MOOEE_INV_DAG). */
+gmg_status gmg_coarse_mooee(gmg_coarse* h, gmg_rb_op op, gmg_prec compute, gmg_prec vec_prec, int nrhs,
+                            const void* in, void* out, gmg_stream s);
+
+/* Grid's pickCheckerboard / setCheckerboard on device fields [V][per_site]
+   complex (F64 or F32): full -> half of parity cb, and half -> those sites of full. */
+gmg_status gmg_pick_checkerboard(const int dims[4], int cb, int per_site, gmg_prec prec, const void* full,
+                                 void* half, gmg_stream s);
+gmg_status gmg_set_checkerboard(const int dims[4], int cb, int per_site, gmg_prec prec, const void* half,
+                                void* full, gmg_stream s);
+
 /* Error code recorded on the device by this handle's tensor-core kernels
    (0 = none; otherwise a bounded wait ran out and the kernel returned early),
    read after a device synchronisation and then cleared.  Returns

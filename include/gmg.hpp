@@ -51,6 +51,13 @@ struct Field {
   gmg_prec prec = GMG_F64;
 };
 
+// Grid's pickCheckerboard / setCheckerboard on device fields: full (V sites)
+// <-> half (the V/2 sites of parity cb), see gmg_pick_checkerboard.
+inline void PickCheckerboard(int cb, const std::array<int, 4>& dims, const Field& full, Field& half,
+                             gmg_stream s = nullptr);
+inline void SetCheckerboard(const std::array<int, 4>& dims, const Field& half, int cb, Field& full,
+                            gmg_stream s = nullptr);
+
 class LinearOperatorBase {
  public:
   virtual ~LinearOperatorBase() {}
@@ -108,12 +115,40 @@ class CoarsenedMatrix {
 
   void ConstructRemainingLinks() { check(gmg_coarse_construct_remaining_links(h_, stream_)); }
 
+  // Red-black (Schur) interface of Rework::CoarsenedMatrix (CoarsenedMatrixRework.h:178-245).
+  // Half fields hold V/2 sites of one parity; `cb` is the parity of `in`
+  // (Grid's in.Checkerboard()), 0 = Even, 1 = Odd.
+  int ConstEE() const { return 0; }
+  void InvertSelfStencilPoint() { check(gmg_coarse_invert_self(h_, stream_)); }
+  void Dhop(const Field& in, Field& out, int dag) {
+    check(gmg_coarse_dhop(h_, dag, compute_or(in), in.prec, in.nrhs, in.data, out.data, stream_));
+  }
+  void Meooe(const Field& in, Field& out, int cb) { rb(GMG_RB_MEOOE, cb, in, out); }
+  void MeooeDag(const Field& in, Field& out, int cb) { rb(GMG_RB_MEOOE_DAG, cb, in, out); }
+  void DhopOE(const Field& in_even, Field& out_odd, int dag) { rb(dag ? GMG_RB_MEOOE_DAG : GMG_RB_MEOOE, 0, in_even, out_odd); }
+  void DhopEO(const Field& in_odd, Field& out_even, int dag) { rb(dag ? GMG_RB_MEOOE_DAG : GMG_RB_MEOOE, 1, in_odd, out_even); }
+  void Mooee(const Field& in, Field& out, int cb) { rb(GMG_RB_MOOEE, cb, in, out); }
+  void MooeeDag(const Field& in, Field& out, int cb) { rb(GMG_RB_MOOEE_DAG, cb, in, out); }
+  void MooeeInv(const Field& in, Field& out, int cb) { rb(GMG_RB_MOOEE_INV, cb, in, out); }
+  void MooeeInvDag(const Field& in, Field& out, int cb) { rb(GMG_RB_MOOEE_INV_DAG, cb, in, out); }
+  // the full-grid forms of the self-point family
+  void Mooee(const Field& in, Field& out) { mooee(GMG_RB_MOOEE, in, out); }
+  void MooeeDag(const Field& in, Field& out) { mooee(GMG_RB_MOOEE_DAG, in, out); }
+  void MooeeInv(const Field& in, Field& out) { mooee(GMG_RB_MOOEE_INV, in, out); }
+  void MooeeInvDag(const Field& in, Field& out) { mooee(GMG_RB_MOOEE_INV_DAG, in, out); }
+
   // CoarsenOperator(FineGrid, linop, Subspace)
   inline void CoarsenOperator(class Aggregation& agg, class WilsonCloverFermion& fine);
   inline void CoarsenOperator(class Aggregation& agg, CoarsenedMatrix& fine);
 
  private:
   gmg_prec compute_or(const Field& in) const { return compute_ == (gmg_prec)-1 ? in.prec : compute_; }
+  void rb(gmg_rb_op op, int cb, const Field& in, Field& out) {
+    check(gmg_coarse_apply_rb(h_, op, cb, compute_or(in), in.prec, in.nrhs, in.data, out.data, stream_));
+  }
+  void mooee(gmg_rb_op op, const Field& in, Field& out) {
+    check(gmg_coarse_mooee(h_, op, compute_or(in), in.prec, in.nrhs, in.data, out.data, stream_));
+  }
   void apply(gmg_op op, int point, const Field& in, Field& out) {
     check(gmg_coarse_apply(h_, op, point, compute_or(in), in.prec, in.nrhs, in.data, out.data, nullptr, 0,
                            stream_));
@@ -211,5 +246,12 @@ class MdagMLinearOperator : public LinearOperatorBase {
  private:
   Matrix& m_;
 };
+
+inline void PickCheckerboard(int cb, const std::array<int, 4>& dims, const Field& full, Field& half, gmg_stream s) {
+  check(gmg_pick_checkerboard(dims.data(), cb, full.nrhs * full.dof, full.prec, full.data, half.data, s));
+}
+inline void SetCheckerboard(const std::array<int, 4>& dims, const Field& half, int cb, Field& full, gmg_stream s) {
+  check(gmg_set_checkerboard(dims.data(), cb, half.nrhs * half.dof, half.prec, half.data, full.data, s));
+}
 
 }  // namespace gmg

@@ -724,3 +724,169 @@ extern "C" void orc_layout_link_flat_to_spin(int64_t V, int N, int ncs, const do
         C(out)[s * NN + ((s1 * ncs + s2) * ncc + c1) * ncc + c2] = C(in)[s * NN + n1 * N + n2];
       }
 }
+
+// ----------------------------------------------------------------------------
+// Red-black (checkerboarded) coarse operator, Rework::CoarsenedMatrix
+// (CoarsenedMatrixRework.h:178-245 Meooe/Mooee/Dhop, 288-394 DhopInternal,
+// 617-640 MooeeInternal, 642-668 InvertSelfStencilPoint, 670-679 FillHalfCbs).
+//
+// Half fields follow Grid's red-black grid, checkerboarded in x: a site of
+// parity q = (x+y+z+t) % 2 has half index h = x/2 + (Lx/2)*(y + Ly*(z + Lz*t)).
+// ----------------------------------------------------------------------------
+static inline int site_parity(int64_t s, const int* dims) {
+  int c[4];
+  coor_from_index(s, dims, c);
+  return (c[0] + c[1] + c[2] + c[3]) & 1;
+}
+
+static inline int64_t half_index(int64_t s, const int* dims) {
+  int c[4];
+  coor_from_index(s, dims, c);
+  return c[0] / 2 + (int64_t)(dims[0] / 2) * (c[1] + (int64_t)dims[1] * (c[2] + (int64_t)dims[2] * c[3]));
+}
+
+// pickCheckerboard / setCheckerboard on [site][per_site complex] fields
+extern "C" void orc_pick_checkerboard(const int* dims, int cb, int64_t per_site, const double* full, double* half) {
+  const int64_t V = volume(dims);
+  for (int64_t s = 0; s < V; ++s)
+    if (site_parity(s, dims) == cb)
+      for (int64_t k = 0; k < per_site; ++k) C(half)[half_index(s, dims) * per_site + k] = C(full)[s * per_site + k];
+}
+
+extern "C" void orc_set_checkerboard(const int* dims, int cb, int64_t per_site, const double* half, double* full) {
+  const int64_t V = volume(dims);
+  for (int64_t s = 0; s < V; ++s)
+    if (site_parity(s, dims) == cb)
+      for (int64_t k = 0; k < per_site; ++k) C(full)[s * per_site + k] = C(half)[half_index(s, dims) * per_site + k];
+}
+
+// Inverse of each site's N x N self-stencil link (InvertSelfStencilPoint,
+// Eigen's inverse() in the reference): Gauss-Jordan with partial pivoting.
+// A8 and Ainv are [V][N][N] row-major.  Returns the number of singular sites.
+extern "C" int orc_invert_self_links(int64_t V, int N, const double* A8, double* Ainv) {
+  int singular = 0;
+#pragma omp parallel for schedule(static) reduction(+ : singular)
+  for (int64_t s = 0; s < V; ++s) {
+    std::vector<cplx> a(C(A8) + s * N * N, C(A8) + (s + 1) * N * N);
+    std::vector<cplx> inv((size_t)N * N, 0.0);
+    for (int i = 0; i < N; ++i) inv[(size_t)i * N + i] = 1.0;
+    for (int col = 0; col < N; ++col) {
+      int piv = col;
+      for (int r = col + 1; r < N; ++r)
+        if (std::abs(a[(size_t)r * N + col]) > std::abs(a[(size_t)piv * N + col])) piv = r;
+      if (std::abs(a[(size_t)piv * N + col]) == 0.0) {
+        ++singular;
+        break;
+      }
+      if (piv != col)
+        for (int k = 0; k < N; ++k) {
+          std::swap(a[(size_t)piv * N + k], a[(size_t)col * N + k]);
+          std::swap(inv[(size_t)piv * N + k], inv[(size_t)col * N + k]);
+        }
+      const cplx d = 1.0 / a[(size_t)col * N + col];
+      for (int k = 0; k < N; ++k) {
+        a[(size_t)col * N + k] *= d;
+        inv[(size_t)col * N + k] *= d;
+      }
+      for (int r = 0; r < N; ++r) {
+        if (r == col) continue;
+        const cplx f = a[(size_t)r * N + col];
+        if (f == 0.0) continue;
+        for (int k = 0; k < N; ++k) {
+          a[(size_t)r * N + k] -= f * a[(size_t)col * N + k];
+          inv[(size_t)r * N + k] -= f * inv[(size_t)col * N + k];
+        }
+      }
+    }
+    for (int64_t k = 0; k < (int64_t)N * N; ++k) C(Ainv)[s * N * N + k] = inv[k];
+  }
+  return singular;
+}
+
+// Red-black ops on half fields [Vh][R][N].  cb = parity of `in`.
+//   op 0 Meooe       (DhopOE / DhopEO): out (parity 1-cb) = sum_{p<8} A_p in(nbr_p)
+//   op 1 MeooeDag    G5C Meooe G5C (DhopInternal with dag, Galerkin form, :289-346)
+//   op 2 Mooee       out (parity cb) = A_8 in
+//   op 3 MooeeDag    adj(A_8) in          (MooeeInternal, :617-640)
+//   op 4 MooeeInv    A_8^-1 in
+//   op 5 MooeeInvDag adj(A_8^-1) in
+// links [9][V][N][N] (exchange layout), self_inv [V][N][N] (ops 4, 5 only).
+extern "C" void orc_coarse_rb_apply(const int* dims, int N, int R, const double* links, const double* self_inv,
+                                    int op, int cb, const double* in_half, double* out_half) {
+  const int64_t V = volume(dims), NN = (int64_t)N * N;
+  const cplx* A = C(links);
+  const cplx* x = C(in_half);
+  cplx* y = C(out_half);
+  std::vector<int32_t> nbr(NPOINT * V);
+  orc_coarse_neighbors(dims, nbr.data());
+  const bool hop = op <= 1;
+  const int out_par = hop ? 1 - cb : cb;
+  const bool g5 = op == 1;
+  const int half = N / 2;
+#pragma omp parallel for schedule(static)
+  for (int64_t s = 0; s < V; ++s) {
+    if (site_parity(s, dims) != out_par) continue;
+    const int64_t ho = half_index(s, dims);
+    for (int r = 0; r < R; ++r)
+      for (int b = 0; b < N; ++b) {
+        cplx res = 0.0;
+        if (hop) {
+          for (int p = 0; p < 8; ++p) {
+            const cplx* Ap = A + ((int64_t)p * V + s) * NN + (int64_t)b * N;
+            const cplx* nb = x + (half_index(nbr[p * V + s], dims) * R + r) * N;
+            for (int bb = 0; bb < N; ++bb) res += Ap[bb] * (g5 && bb >= half ? -nb[bb] : nb[bb]);
+          }
+          if (g5 && b >= half) res = -res;
+        } else {
+          const cplx* M = (op >= 4) ? C(self_inv) + s * NN : A + ((int64_t)8 * V + s) * NN;
+          const bool dag = (op == 3 || op == 5);
+          const cplx* xi = x + (ho * R + r) * N;
+          for (int bb = 0; bb < N; ++bb) res += (dag ? std::conj(M[(int64_t)bb * N + b]) : M[(int64_t)b * N + bb]) * xi[bb];
+        }
+        y[(ho * R + r) * N + b] = res;
+      }
+  }
+}
+
+// Full-grid Dhop (CoarsenedMatrixRework.h:210-217): the 8 hopping points,
+// dag = G5C Dhop G5C regardless of the hermitian flag (DhopInternal, :289-346).
+extern "C" void orc_coarse_dhop(const int* dims, int N, int R, const double* links, int dag, const double* in,
+                                double* out) {
+  const int64_t V = volume(dims), NN = (int64_t)N * N;
+  const cplx* A = C(links);
+  const cplx* x = C(in);
+  cplx* y = C(out);
+  std::vector<int32_t> nbr(NPOINT * V);
+  orc_coarse_neighbors(dims, nbr.data());
+  const int half = N / 2;
+#pragma omp parallel for schedule(static)
+  for (int64_t s = 0; s < V; ++s)
+    for (int r = 0; r < R; ++r)
+      for (int b = 0; b < N; ++b) {
+        cplx res = 0.0;
+        for (int p = 0; p < 8; ++p) {
+          const cplx* Ap = A + ((int64_t)p * V + s) * NN + (int64_t)b * N;
+          const cplx* nb = x + ((int64_t)nbr[p * V + s] * R + r) * N;
+          for (int bb = 0; bb < N; ++bb) res += Ap[bb] * (dag && bb >= half ? -nb[bb] : nb[bb]);
+        }
+        y[(s * R + r) * N + b] = (dag && b >= half) ? -res : res;
+      }
+}
+
+// Full-grid Mooee family (MooeeInternal on the full grid): op 2..5 as above.
+extern "C" void orc_coarse_mooee(const int* dims, int N, int R, const double* links, const double* self_inv, int op,
+                                 const double* in, double* out) {
+  const int64_t V = volume(dims), NN = (int64_t)N * N;
+#pragma omp parallel for schedule(static)
+  for (int64_t s = 0; s < V; ++s) {
+    const cplx* M = (op >= 4) ? C(self_inv) + s * NN : C(links) + ((int64_t)8 * V + s) * NN;
+    const bool dag = (op == 3 || op == 5);
+    for (int r = 0; r < R; ++r)
+      for (int b = 0; b < N; ++b) {
+        cplx res = 0.0;
+        const cplx* xi = C(in) + (s * R + r) * N;
+        for (int bb = 0; bb < N; ++bb) res += (dag ? std::conj(M[(int64_t)bb * N + b]) : M[(int64_t)b * N + bb]) * xi[bb];
+        C(out)[(s * R + r) * N + b] = res;
+      }
+  }
+}

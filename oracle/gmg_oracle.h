@@ -90,6 +90,17 @@ void orc_construct_remaining_links(const int* dims, int N, double* links, int he
 void orc_layout_vec_flat_to_spin(int64_t V, int N, int ncs, const double* in, double* out);
 void orc_layout_link_flat_to_spin(int64_t V, int N, int ncs, const double* in, double* out);
 
+/* red-black coarse operator (CoarsenedMatrixRework.h:178-245, 288-394, 617-679);
+   half index h = x/2 + (Lx/2)*(y + Ly*(z + Lz*t)) on the sites of one parity */
+void orc_pick_checkerboard(const int* dims, int cb, int64_t per_site, const double* full, double* half);
+void orc_set_checkerboard(const int* dims, int cb, int64_t per_site, const double* half, double* full);
+int  orc_invert_self_links(int64_t V, int N, const double* A8, double* Ainv);
+void orc_coarse_rb_apply(const int* dims, int N, int R, const double* links, const double* self_inv,
+                         int op, int cb, const double* in_half, double* out_half);
+void orc_coarse_dhop(const int* dims, int N, int R, const double* links, int dag, const double* in, double* out);
+void orc_coarse_mooee(const int* dims, int N, int R, const double* links, const double* self_inv, int op,
+                      const double* in, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -230,3 +230,70 @@ def rel_dev_sq(ref, res):
     ref = np.asarray(ref)
     res = np.asarray(res)
     return float(np.sum(np.abs(ref - res) ** 2) / np.sum(np.abs(ref) ** 2))
+
+
+# ----------------------------------------------------------------------------
+# red-black coarse operator (CoarsenedMatrixRework.h:178-245, 288-394, 617-679)
+# ----------------------------------------------------------------------------
+RB_MEOOE, RB_MEOOE_DAG, RB_MOOEE, RB_MOOEE_DAG, RB_MOOEE_INV, RB_MOOEE_INV_DAG = range(6)
+
+
+def pick_checkerboard(dims, cb, full):
+    """full [V][...] -> half [V/2][...] (sites of parity cb, half index x/2 + Lx/2 * (...))."""
+    full = _c(full)
+    per = int(np.prod(full.shape[1:])) if full.ndim > 1 else 1
+    half = np.zeros((full.shape[0] // 2,) + full.shape[1:], dtype=np.complex128)
+    lib().orc_pick_checkerboard(_i4(dims), cb, ctypes.c_int64(per), _p(full), _p(half))
+    return half
+
+
+def set_checkerboard(dims, cb, half, full):
+    """Writes the half field into the parity-cb sites of full (in place)."""
+    half = _c(half)
+    per = int(np.prod(half.shape[1:])) if half.ndim > 1 else 1
+    lib().orc_set_checkerboard(_i4(dims), cb, ctypes.c_int64(per), _p(half), _p(full))
+    return full
+
+
+def invert_self_links(links):
+    """links [9][V][N][N] -> inverse of the self link per site, [V][N][N]."""
+    links = _c(links)
+    V, N = links.shape[1], links.shape[2]
+    a8 = np.ascontiguousarray(links[8])
+    inv = np.zeros_like(a8)
+    lib().orc_invert_self_links.restype = ctypes.c_int
+    bad = lib().orc_invert_self_links(ctypes.c_int64(V), N, _p(a8), _p(inv))
+    if bad:
+        raise ValueError(f"{bad} singular self links")
+    return inv
+
+
+def coarse_rb_apply(dims, links, x_half, op, cb, self_inv=None):
+    """Half field x (parity cb) -> Meooe / Mooee family output half field."""
+    links = _c(links)
+    x_half = _c(x_half)
+    Vh, R, N = x_half.shape
+    y = np.zeros_like(x_half)
+    si = None if self_inv is None else _c(self_inv)
+    lib().orc_coarse_rb_apply(_i4(dims), N, R, _p(links), _p(si), op, cb, _p(x_half), _p(y))
+    return y
+
+
+def coarse_dhop(dims, links, x, dag=0):
+    links = _c(links)
+    x = _c(x)
+    V, R, N = x.shape
+    y = np.zeros_like(x)
+    lib().orc_coarse_dhop(_i4(dims), N, R, _p(links), int(dag), _p(x), _p(y))
+    return y
+
+
+def coarse_mooee(dims, links, x, op, self_inv=None):
+    """Full-grid Mooee family (op RB_MOOEE..RB_MOOEE_INV_DAG)."""
+    links = _c(links)
+    x = _c(x)
+    V, R, N = x.shape
+    y = np.zeros_like(x)
+    si = None if self_inv is None else _c(self_inv)
+    lib().orc_coarse_mooee(_i4(dims), N, R, _p(links), _p(si), op, _p(x), _p(y))
+    return y

@@ -176,6 +176,24 @@ def test_orthonormalise_matches_mgs(agg8):
     assert ag2.CheckOrthogonal() < 1e-14
 
 
+def test_orthonormalise_nearly_dependent_block_vectors(agg8):
+    # smoothed test vectors can be nearly dependent inside a block: v_j = v_0 + 1e-7 noise
+    # (condition number ~1e8, so a plain Cholesky-QR Gram matrix is numerically singular);
+    # the result must still be orthonormal and span the same space as MGS's basis
+    fd, cd, B0, ag = agg8
+    r = inputs.rng(stream=119)
+    B = np.repeat(B0[:1], 8, axis=0) + 1e-7 * inputs.gaussian_field(B0.shape, r)
+    ag2 = gmg.Aggregation(fd, cd, 12, 8)
+    ag2.set_basis(B)
+    ag2.Orthogonalise(passes=2)
+    assert ag2.CheckOrthogonal() < 1e-12
+    got = ag2.get_basis()
+    ref = orc.block_orthonormalise(fd, cd, B, passes=2)
+    # same span block by block: projecting the MGS vectors onto the GPU basis keeps them
+    back = orc.block_promote(fd, cd, got, orc.block_project(fd, cd, got, np.moveaxis(ref, 0, 1)))
+    assert orc.rel_dev_sq(np.moveaxis(ref, 0, 1), back) < 1e-10
+
+
 @pytest.mark.parametrize("nrhs", [1, 3, 8])
 def test_project_promote_f64(agg8, nrhs):
     fd, cd, B0, ag = agg8
@@ -249,6 +267,22 @@ def test_wilson_ops_f64(wil, op):
     out = torch.zeros((512, 3, 12), dtype=torch.complex128, device=DEV)
     getattr(w, op)(dev(x), out)
     assert orc.rel_dev_sq(ref, host(out)) < TOL64
+
+
+@pytest.mark.parametrize("nrhs", [4, 12, 20])
+@pytest.mark.parametrize("op", ["M", "Mdag", "Mdiag"])
+def test_wilson_multi_rhs_tile(wil, nrhs, op):
+    # nrhs >= 4 runs the shared-memory tile kernel (16 sites, up to 16 threads per site)
+    dims, U, cl, w = wil
+    x = inputs.gaussian_field((512, nrhs, 12), inputs.rng(stream=124 + nrhs))
+    code = {"M": orc.OP_M, "Mdag": orc.OP_MDAG, "Mdiag": orc.OP_MDIAG}[op]
+    ref = orc.wilson_clover(dims, U, cl, -0.1, 1, x, code)
+    out = torch.zeros((512, nrhs, 12), dtype=torch.complex128, device=DEV)
+    getattr(w, op)(dev(x), out)
+    assert orc.rel_dev_sq(ref, host(out)) < TOL64
+    out32 = torch.zeros((512, nrhs, 12), dtype=torch.complex64, device=DEV)
+    getattr(w, op)(dev(x, torch.complex64), out32)
+    assert orc.rel_dev_sq(ref, host(out32)) < TOL32
 
 
 def test_wilson_mdir_f64_and_f32(wil):
