@@ -247,7 +247,7 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
     GMG_TRY(vec_scale_inv_norm(dn, w, v0, s));
     std::fill(H.begin(), H.end(), zc(0));
     std::fill(g.begin(), g.end(), zc(0));
-    for (int r = 0; r < R; ++r) g[r] = beta[r];
+    for (int r = 0; r < R; ++r) g[(size_t)r * (m + 1)] = beta[r];  // per-RHS residual vector, [R][m+1]
     int jl = -1;
     for (int j = 0; j < m && iters < maxit; ++j) {
       Vec vj = nth(V0, j);

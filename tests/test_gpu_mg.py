@@ -9,6 +9,8 @@ FP32-preconditioner and the tensor-core (BF16 coarse stencil) forms.  The
 Galerkin identity R D P = D_c (:398-421) is checked on the operators the
 setup built.
 """
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -46,6 +48,13 @@ def test_mg_solve_reaches_1e10(fine, prec, levels):
         kw["block"] = ((2, 2, 2, 2), (2, 2, 2, 2))
     mg = gmg.MultiGrid(w, nrhs, **kw)
     mg.setup()
+    # every test vector of every level made it into an orthonormal block basis
+    # (a zero test vector shows up as a unit error here)
+    for l in range(levels - 1):
+        _, ag = mg.level(l)
+        e = ctypes.c_double()
+        assert gmg.lib().gmg_agg_check_orthogonal(ag, ctypes.byref(e), gmg._stream()) == 0
+        assert e.value < 1e-12, (l, e.value)
     b = torch.from_numpy(inputs.gaussian_field((4096, nrhs, 12), inputs.rng(stream=302))).cuda()
     x = torch.zeros_like(b)
     it, rr = mg.solve(b, x, tol=1e-10, maxiter=300)
