@@ -436,4 +436,120 @@ gmg_status vec_tri_apply(const double2* T_dev, Vec& X, cudaStream_t s) {
   return GMG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// BiCGStab building blocks with per-RHS scalars kept on the device
+// (sc layout per RHS r: sc[0*R+r] rho, [1] alpha, [2] omega, [3] beta)
+// ---------------------------------------------------------------------------
+namespace blas {
+__device__ __forceinline__ double2 zdiv(double2 a, double2 b) {
+  const double n = b.x * b.x + b.y * b.y;
+  if (!(n > 0.0)) return make_double2(0.0, 0.0);
+  return make_double2((a.x * b.x + a.y * b.y) / n, (a.y * b.x - a.x * b.y) / n);
+}
+__device__ __forceinline__ double2 zmul2(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// rho_new = <r0, r>: beta = (rho_new / rho) (alpha / omega), rho = rho_new
+__global__ void bicg_beta_kernel(const double2* __restrict__ rho_new, double2* __restrict__ sc, int R) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  const double2 rho = sc[r], alpha = sc[R + r], omega = sc[2 * R + r];
+  sc[3 * R + r] = zmul2(zdiv(rho_new[r], rho), zdiv(alpha, omega));
+  sc[r] = rho_new[r];
+}
+// alpha = rho / <r0, v>
+__global__ void bicg_alpha_kernel(const double2* __restrict__ r0v, double2* __restrict__ sc, int R) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < R) sc[R + r] = zdiv(sc[r], r0v[r]);
+}
+// omega = <t, s> / <t, t>
+__global__ void bicg_omega_kernel(const double2* __restrict__ ts, const double2* __restrict__ tt, double2* __restrict__ sc,
+                                  int R) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < R) sc[2 * R + r] = zdiv(ts[r], tt[r]);
+}
+
+// p = r + beta (p - omega v)
+template <class T>
+__global__ void bicg_p_kernel(typename C2<T>::t* __restrict__ p, const typename C2<T>::t* __restrict__ r,
+                              const typename C2<T>::t* __restrict__ v, const double2* __restrict__ sc, int64_t V, int R,
+                              int dof) {
+  const int64_t n = V * R * dof;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)((e / dof) % R);
+    const double2 om = sc[2 * R + k], be = sc[3 * R + k];
+    const double2 pv = make_double2(p[e].x, p[e].y), vv = make_double2(v[e].x, v[e].y);
+    const double2 ov = zmul2(om, vv);
+    const double2 q = zmul2(be, make_double2(pv.x - ov.x, pv.y - ov.y));
+    p[e].x = (T)(r[e].x + q.x);
+    p[e].y = (T)(r[e].y + q.y);
+  }
+}
+// s = r - alpha v   (written into r's buffer s)
+template <class T>
+__global__ void bicg_s_kernel(typename C2<T>::t* __restrict__ s_, const typename C2<T>::t* __restrict__ r,
+                              const typename C2<T>::t* __restrict__ v, const double2* __restrict__ sc, int64_t V, int R,
+                              int dof) {
+  const int64_t n = V * R * dof;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)((e / dof) % R);
+    const double2 av = zmul2(sc[R + k], make_double2(v[e].x, v[e].y));
+    s_[e].x = (T)(r[e].x - av.x);
+    s_[e].y = (T)(r[e].y - av.y);
+  }
+}
+// x += alpha p + omega s;  r = s - omega t
+template <class T>
+__global__ void bicg_xr_kernel(typename C2<T>::t* __restrict__ x, typename C2<T>::t* __restrict__ r,
+                               const typename C2<T>::t* __restrict__ p, const typename C2<T>::t* __restrict__ s_,
+                               const typename C2<T>::t* __restrict__ t, const double2* __restrict__ sc, int64_t V, int R,
+                               int dof) {
+  const int64_t n = V * R * dof;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)((e / dof) % R);
+    const double2 al = sc[R + k], om = sc[2 * R + k];
+    const double2 sv = make_double2(s_[e].x, s_[e].y);
+    const double2 ap = zmul2(al, make_double2(p[e].x, p[e].y)), os = zmul2(om, sv);
+    const double2 ot = zmul2(om, make_double2(t[e].x, t[e].y));
+    x[e].x = (T)(x[e].x + ap.x + os.x);
+    x[e].y = (T)(x[e].y + ap.y + os.y);
+    r[e].x = (T)(sv.x - ot.x);
+    r[e].y = (T)(sv.y - ot.y);
+  }
+}
+}  // namespace blas
+
+gmg_status bicg_scalar(int which, const double2* a, const double2* b, double2* sc, int R, cudaStream_t s) {
+  const int g = (R + 127) / 128;
+  if (which == 0) blas::bicg_beta_kernel<<<g, 128, 0, s>>>(a, sc, R);
+  else if (which == 1) blas::bicg_alpha_kernel<<<g, 128, 0, s>>>(a, sc, R);
+  else blas::bicg_omega_kernel<<<g, 128, 0, s>>>(a, b, sc, R);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status bicg_vec(int which, Vec& a, const Vec& b, const Vec& c, const Vec& d, const Vec& e, const double2* sc,
+                    cudaStream_t s) {
+  const int g = blas::grid1(a.elems());
+  const bool f64 = a.prec == GMG_F64;
+  if (which == 0) {  // p = r + beta (p - omega v): a = p, b = r, c = v
+    if (f64) blas::bicg_p_kernel<double><<<g, 256, 0, s>>>((double2*)a.p, (const double2*)b.p, (const double2*)c.p, sc, a.V, a.R, a.dof);
+    else blas::bicg_p_kernel<float><<<g, 256, 0, s>>>((float2*)a.p, (const float2*)b.p, (const float2*)c.p, sc, a.V, a.R, a.dof);
+  } else if (which == 1) {  // s = r - alpha v: a = s, b = r, c = v
+    if (f64) blas::bicg_s_kernel<double><<<g, 256, 0, s>>>((double2*)a.p, (const double2*)b.p, (const double2*)c.p, sc, a.V, a.R, a.dof);
+    else blas::bicg_s_kernel<float><<<g, 256, 0, s>>>((float2*)a.p, (const float2*)b.p, (const float2*)c.p, sc, a.V, a.R, a.dof);
+  } else {  // x += alpha p + omega s; r = s - omega t: a = x, b = r (written), c = p, d = s, e = t
+    Vec& r = const_cast<Vec&>(b);
+    if (f64)
+      blas::bicg_xr_kernel<double><<<g, 256, 0, s>>>((double2*)a.p, (double2*)r.p, (const double2*)c.p, (const double2*)d.p,
+                                                     (const double2*)e.p, sc, a.V, a.R, a.dof);
+    else
+      blas::bicg_xr_kernel<float><<<g, 256, 0, s>>>((float2*)a.p, (float2*)r.p, (const float2*)c.p, (const float2*)d.p,
+                                                    (const float2*)e.p, sc, a.V, a.R, a.dof);
+  }
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
 }  // namespace gmg

@@ -183,6 +183,53 @@ gmg_status global_orthonormalise(gmg_mg* h, Vec& X, cudaStream_t s) {
   return GMG_OK;
 }
 
+// ------------------------------------------------------------- BiCGStab (setup solver)
+// Multi-RHS BiCGStab on A x = b at level l, the reference's setup solver
+// (setupSolverType BiCGSTAB, tolerance 1e-3, 100 iterations,
+// MultigridParams.h:105-107).  The per-RHS scalars rho, alpha, omega, beta stay
+// on the device (h->coef + 4096); residual norms come back every 8 iterations.
+// ws: 6 fields shaped like b (r, r0, p, v, s, t).
+gmg_status bicgstab(gmg_mg* h, int l, const Vec& b, Vec& x, int maxit, double tol, VecBuf* ws, cudaStream_t s) {
+  const int R = b.R;
+  GMG_CHECK(R <= 32, GMG_ERR_UNSUPPORTED, "bicgstab: at most 32 right-hand sides");
+  Vec r = ws[0].with_rhs(R), r0 = ws[1].with_rhs(R), p = ws[2].with_rhs(R), v = ws[3].with_rhs(R),
+      sv = ws[4].with_rhs(R), t = ws[5].with_rhs(R);
+  double2* sc = h->coef.as<double2>() + 4096;  // [4R]: rho, alpha, omega, beta
+  double2* d = h->dscr.as<double2>() + 2048;   // dot products [5R]
+  std::vector<zc> bn;
+  GMG_TRY(dots(h, b, 1, 0, b, bn, s));
+  GMG_TRY(apply_op(h, l, x, r, s));
+  GMG_TRY(vec_xmy(b, r, s));  // r = b - A x
+  GMG_CUDA(cudaMemcpyAsync(r0.p, r.p, r.bytes(), cudaMemcpyDeviceToDevice, s));
+  GMG_TRY(zero(p, s));
+  GMG_TRY(zero(v, s));
+  std::vector<zc> init(4 * (size_t)R, zc(1.0));
+  GMG_TRY(upload(h, init, 4096, s));
+  for (int it = 0; it < maxit; ++it) {
+    GMG_TRY(vec_multidot(r0, 1, 0, r, d, nullptr, s));  // rho_new = <r0, r>
+    GMG_TRY(bicg_scalar(0, d, nullptr, sc, R, s));       // beta, rho
+    GMG_TRY(bicg_vec(0, p, r, v, v, v, sc, s));          // p = r + beta (p - omega v)
+    GMG_TRY(apply_op(h, l, p, v, s));                    // v = A p
+    GMG_TRY(vec_multidot(r0, 1, 0, v, d + R, nullptr, s));
+    GMG_TRY(bicg_scalar(1, d + R, nullptr, sc, R, s));   // alpha = rho / <r0, v>
+    GMG_TRY(bicg_vec(1, sv, r, v, v, v, sc, s));         // s = r - alpha v
+    GMG_TRY(apply_op(h, l, sv, t, s));                   // t = A s
+    GMG_TRY(vec_multidot(t, 1, 0, sv, d + 2 * R, nullptr, s));
+    GMG_TRY(vec_multidot(t, 1, 0, t, d + 3 * R, nullptr, s));
+    GMG_TRY(bicg_scalar(2, d + 2 * R, d + 3 * R, sc, R, s));  // omega = <t, s> / <t, t>
+    GMG_TRY(bicg_vec(2, x, r, p, sv, t, sc, s));         // x += alpha p + omega s; r = s - omega t
+    if ((it + 1) % 8 == 0 || it + 1 == maxit) {
+      std::vector<zc> rn;
+      GMG_TRY(dots(h, r, 1, 0, r, rn, s));
+      bool conv = true;
+      for (int k = 0; k < R; ++k)
+        if (rn[k].real() > tol * tol * bn[k].real()) conv = false;
+      if (conv) break;
+    }
+  }
+  return GMG_OK;
+}
+
 // ------------------------------------------------------------- MR smoother
 // x <- x + iters steps of minimal residual for A x = b on level l
 // The step lengths stay on the device: no host synchronisation.
@@ -419,7 +466,7 @@ extern "C" gmg_status gmg_mg_params_default(gmg_mg_params* p) {
   }
   p->nvec[0] = 12;
   p->nvec[1] = 16;
-  p->setup_iters = 40;
+  p->setup_iters = 100;
   p->smoother_iters = 8;
   p->wrapper_iters = 10;
   p->wrapper_tol = 0.1;
@@ -429,6 +476,17 @@ extern "C" gmg_status gmg_mg_params_default(gmg_mg_params* p) {
   p->outer_restart = 8;
   p->prec = GMG_F32;
   p->seed = 1234;
+  p->setup_solver = 0;
+  p->setup_tol = 1e-3;
+  // Null-vector setup (setupBasisVectorsType nullVectors) rather than the
+  // reference's default single test-vector pass: on 32^4 near the critical mass
+  // one pass of A psi = v leaves the test vectors dominated by bulk modes (the
+  // coarse operator's lowest eigenvalue stayed near 1.9 against 0.04 for the
+  // fine operator, and the K-cycle cut the outer iterations by nothing), while
+  // 100 BiCGStab iterations on A psi = 0 keep the slowly decaying low modes
+  // (28 outer iterations on that configuration).
+  p->setup_passes = 1;
+  p->setup_null = 1;
   return GMG_OK;
 }
 
@@ -505,24 +563,51 @@ extern "C" gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream stream) {
     const int nv = P.nvec[l];
     // test vectors: A psi = v approximately, from random v (BasisVectors.h:94-120),
     // GMRES(10) with a temporary Krylov basis sized for the nv vectors
-    VecBuf v, psi, sV, sw, st;
-    const int ms = 10;
+    // test vectors (BasisVectors::Generate, BasisVectors.h:74-147): random start,
+    // then setup_passes passes of {orthonormalise, solve, orthonormalise}; the
+    // test-vector form solves A psi = v from psi = 0 (inverse iteration), the
+    // null-vector form solves A psi = 0 from psi = v (the slowly decaying low
+    // modes remain)
+    VecBuf v, psi, zsrc;
     GMG_TRY(v.alloc(L.V, nv, L.dof, L.vprec));
     GMG_TRY(psi.alloc(L.V, nv, L.dof, L.vprec));
-    GMG_TRY(alloc_fields(sV, L.V, nv, L.dof, L.vprec, ms + 1));
-    GMG_TRY(sw.alloc(L.V, nv, L.dof, L.vprec));
-    GMG_TRY(st.alloc(L.V, nv, L.dof, L.vprec));
     GMG_TRY(vec_gaussian(v, P.seed * 7919 + l, s));
-    GMG_TRY(global_orthonormalise(h, v, s));  // setupPreOrthonormalise
-    GMG_CUDA(cudaMemsetAsync(psi.p, 0, psi.bytes(), s));
-    Krylov K;
-    K.V0 = sV;
-    K.w = sw;
-    K.t = st;
-    K.tz = st;
-    auto none = [](const Vec&, Vec&, const Vec&) { return GMG_OK; };
-    GMG_TRY(fgmres(h, l, v, psi, K, ms, P.setup_iters, 1e-3, none, false, nullptr, nullptr, s));
-    GMG_TRY(global_orthonormalise(h, psi, s));  // setupPostOrthonormalise
+    if (P.setup_null) {
+      GMG_TRY(zsrc.alloc(L.V, nv, L.dof, L.vprec));
+      GMG_TRY(zero(zsrc, s));
+    }
+    const double stol = P.setup_tol > 0 ? P.setup_tol : 1e-3;
+    const int passes = std::max(P.setup_passes, 1);
+    VecBuf ws[6], sV, sw, st;
+    for (int pass = 0; pass < passes; ++pass) {
+      GMG_TRY(global_orthonormalise(h, v, s));  // setupPreOrthonormalise
+      if (P.setup_null)
+        GMG_CUDA(cudaMemcpyAsync(psi.p, v.p, v.bytes(), cudaMemcpyDeviceToDevice, s));
+      else
+        GMG_CUDA(cudaMemsetAsync(psi.p, 0, psi.bytes(), s));
+      const Vec& src = P.setup_null ? static_cast<const Vec&>(zsrc) : static_cast<const Vec&>(v);
+      if (P.setup_solver == 1) {
+        const int ms = 10;
+        if (!sV.p) {
+          GMG_TRY(alloc_fields(sV, L.V, nv, L.dof, L.vprec, ms + 1));
+          GMG_TRY(sw.alloc(L.V, nv, L.dof, L.vprec));
+          GMG_TRY(st.alloc(L.V, nv, L.dof, L.vprec));
+        }
+        Krylov K;
+        K.V0 = sV;
+        K.w = sw;
+        K.t = st;
+        K.tz = st;
+        auto none = [](const Vec&, Vec&, const Vec&) { return GMG_OK; };
+        GMG_TRY(fgmres(h, l, src, psi, K, ms, P.setup_iters, stol, none, false, nullptr, nullptr, s));
+      } else {
+        if (!ws[0].p)
+          for (auto& f : ws) GMG_TRY(f.alloc(L.V, nv, L.dof, L.vprec));
+        GMG_TRY(bicgstab(h, l, src, psi, P.setup_iters, stol, ws, s));
+      }
+      GMG_TRY(global_orthonormalise(h, psi, s));  // setupPostOrthonormalise
+      if (pass + 1 < passes) GMG_CUDA(cudaMemcpyAsync(v.p, psi.p, psi.bytes(), cudaMemcpyDeviceToDevice, s));
+    }
     // chiral doubling -> basis, block orthonormalisation, Galerkin coarsening
     DevBuf basis;
     GMG_TRY(basis.alloc(sizeof(double2) * 2 * (size_t)nv * L.V * L.dof));

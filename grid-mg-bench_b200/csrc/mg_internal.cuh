@@ -64,5 +64,12 @@ gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s);
 gmg_status vec_gram(const Vec& X, double2* G_dev, cudaStream_t s);
 // X(a) <- sum_{b <= a} T[a][b] X(b)   (lower-triangular recombination of the columns)
 gmg_status vec_tri_apply(const double2* T_dev, Vec& X, cudaStream_t s);
+// BiCGStab steps with per-RHS device scalars sc[4R] = (rho, alpha, omega, beta):
+// bicg_scalar 0: beta / rho from rho_new = a; 1: alpha = rho / a; 2: omega = a / b
+gmg_status bicg_scalar(int which, const double2* a, const double2* b, double2* sc, int R, cudaStream_t s);
+// bicg_vec 0: a(p) = b(r) + beta (a - omega c(v)); 1: a(s) = b(r) - alpha c(v);
+//          2: a(x) += alpha c(p) + omega d(s), b(r) = d(s) - omega e(t)
+gmg_status bicg_vec(int which, Vec& a, const Vec& b, const Vec& c, const Vec& d, const Vec& e, const double2* sc,
+                    cudaStream_t s);
 
 }  // namespace gmg

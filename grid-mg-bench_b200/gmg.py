@@ -362,7 +362,8 @@ class MGParams(ctypes.Structure):
                 ("setup_iters", ctypes.c_int), ("smoother_iters", ctypes.c_int), ("wrapper_iters", ctypes.c_int),
                 ("wrapper_tol", ctypes.c_double), ("coarsest_iters", ctypes.c_int), ("coarsest_tol", ctypes.c_double),
                 ("coarsest_restart", ctypes.c_int), ("outer_restart", ctypes.c_int), ("prec", ctypes.c_int),
-                ("seed", ctypes.c_uint64)]
+                ("seed", ctypes.c_uint64), ("setup_solver", ctypes.c_int), ("setup_tol", ctypes.c_double),
+                ("setup_passes", ctypes.c_int), ("setup_null", ctypes.c_int)]
 
 
 class MultiGrid:

@@ -8,7 +8,8 @@ distributions from numpy's PCG64 seeded with the same integers:
 
   gaussian_field   complex entries with re, im ~ N(0, 1/2)  (E|z|^2 = 1)
   hot_gauge        Haar-random SU(3) links (QR of a Gaussian matrix, phase-fixed)
-  smooth_gauge     U = exp(i * eps * H), H traceless Hermitian with Gaussian entries
+  smooth_gauge     U = exp(i * eps * H), H a traceless Hermitian matrix with unit-variance
+                   Gaussian entries (GUE: E|H_ij|^2 = 1), see gue_traceless
   random_links     Gaussian coarse link matrices, optionally with the
                    gamma5-hermiticity structure that ConstructRemainingLinks
                    produces (CoarsenedMatrixUpstreamImprovedDirsaveLut.h:1164-1196)
@@ -50,13 +51,33 @@ def hot_gauge(dims, r):
     return q.reshape(vol(dims), 4, 3, 3)
 
 
+def gue_traceless(a):
+    """Traceless Hermitian matrices with unit-variance Gaussian entries from complex
+    unit-Gaussian matrices a (E|a_ij|^2 = 1): H = (a + a^dag) / sqrt(2) - tr/3.
+
+    Every entry of H before the trace removal has E|H_ij|^2 = 1 (the Gaussian
+    unitary ensemble), the plain reading of "Gaussian entries".  With this
+    normalisation the smooth gauge field of eps = 0.3 puts the critical mass of
+    the Wilson-clover operator (c_sw = 1, 32^4) near -0.39, so the multigrid
+    configurations' masses (-0.3, -0.35) are near-critical but subcritical; the
+    (a + a^dag) / 2 normalisation (variance 1/2) moves it to about -0.21, past
+    which those masses lie.
+    """
+    import numpy as _np
+    if isinstance(a, _np.ndarray):
+        h = (a + _np.conj(_np.swapaxes(a, -1, -2))) / _np.sqrt(2.0)
+        tr = _np.trace(h, axis1=-2, axis2=-1) / 3.0
+        return h - tr[..., None, None] * _np.eye(3)
+    import torch
+    h = (a + a.conj().transpose(-1, -2)) / np.sqrt(2.0)
+    tr = torch.diagonal(h, dim1=-2, dim2=-1).sum(-1) / 3.0
+    return h - tr[..., None, None] * torch.eye(3, dtype=h.dtype, device=h.device)
+
+
 def smooth_gauge(dims, r, eps):
-    """U = exp(i eps H), H traceless Hermitian with Gaussian entries."""
+    """U = exp(i eps H), H traceless Hermitian with unit-variance Gaussian entries."""
     n = vol(dims) * 4
-    a = gaussian_field((n, 3, 3), r)
-    h = 0.5 * (a + np.conj(np.swapaxes(a, -1, -2)))
-    tr = np.trace(h, axis1=-2, axis2=-1) / 3.0
-    h = h - tr[:, None, None] * np.eye(3)[None]
+    h = gue_traceless(gaussian_field((n, 3, 3), r))
     w, v = np.linalg.eigh(h)
     u = (v * np.exp(1j * eps * w)[:, None, :]) @ np.conj(np.swapaxes(v, -1, -2))
     return u.reshape(vol(dims), 4, 3, 3)
@@ -134,10 +155,7 @@ def torch_smooth_gauge(dims, seed, eps, device="cuda"):
     import torch
 
     n = vol(dims) * 4
-    a = torch_gaussian((n, 3, 3), seed, device)
-    h = 0.5 * (a + a.conj().transpose(-1, -2))
-    tr = torch.diagonal(h, dim1=-2, dim2=-1).sum(-1) / 3.0
-    h = h - tr[:, None, None] * torch.eye(3, dtype=h.dtype, device=device)
+    h = gue_traceless(torch_gaussian((n, 3, 3), seed, device))
     # exp(i eps H) by scaling and squaring: Taylor series of exp(i eps H / 2^s) to
     # 18 terms (truncation below 1e-17 for |eps H / 2^s| <= 1/2), then s squarings
     a = (1j * eps) * h

@@ -255,6 +255,38 @@ def c5(nrhs=24, plain_rhs=2):
               "setup (test vectors, orthonormalisation, CoarsenOperator) not included in solve_s")
 
 
+def profile_rows(rows):
+    """Small cases of the C3 transfers and the fine operator for ncu captures:
+    16^4 fine lattice (nbasis 32 on 4^4 blocks, 32 RHS; Wilson-clover with 12 RHS),
+    each kernel launched once after one untimed warm-up call."""
+    fd, cd, N, R = (16, 16, 16, 16), (4, 4, 4, 4), 32, 32
+    Vf, Vc = 16 ** 4, 4 ** 4
+    if "p_c3" in rows:
+        B = inputs.torch_gaussian((N, Vf, 12), 611)
+        ag = gmg.Aggregation(fd, cd, 12, N)
+        ag.set_basis(B)
+        ag.Orthogonalise(passes=1)
+        f = inputs.torch_gaussian((Vf, R, 12), 612).to(torch.complex64)
+        c = torch.zeros((Vc, R, N), dtype=torch.complex64, device="cuda")
+        for _ in range(2):
+            ag.ProjectToSubspace(f, c, compute="bf16")
+            ag.PromoteFromSubspace(c, f, compute="bf16")
+        torch.cuda.synchronize()
+        line("p_c3 tensor-core project / promote 16^4, nbasis 32, 32 RHS", ok=True)
+    if "p_w" in rows:
+        U = inputs.torch_smooth_gauge(fd, 613, 0.3)
+        w = gmg.WilsonClover(fd, -0.3, 1.0, antiperiodic=True)
+        w.set_gauge(U)
+        x = inputs.torch_gaussian((Vf, 12, 12), 614)
+        y = torch.zeros_like(x)
+        x32, y32 = x.to(torch.complex64), y.to(torch.complex64)
+        for _ in range(2):
+            w.M(x, y)
+            w.M(x32, y32)
+        torch.cuda.synchronize()
+        line("p_w Wilson-clover M 16^4, 12 RHS, FP64 and FP32", ok=True)
+
+
 def run(rows=("c1", "c3", "w_c4", "c5")):
     torch.cuda.set_device(0)
     hbm, src = peaks()
@@ -269,4 +301,7 @@ def run(rows=("c1", "c3", "w_c4", "c5")):
         torch.cuda.empty_cache()
     if "c5" in rows:
         c5()
+    if any(r.startswith("p_") for r in rows):
+        profile_rows(rows)
+        return
     line("peaks", hbm_gbs=hbm, source=src)

@@ -255,7 +255,7 @@ typedef struct {
   int nlevels;           /* 2 or 3 (fine + coarse levels), MultiGridParams::nLevels */
   int block[2][4];       /* aggregation blocks of the transitions 0->1, 1->2 (blockSizes) */
   int nvec[2];           /* test vectors per transition; nbasis = 2 * nvec (chiral doubling) */
-  int setup_iters;       /* GMRES(10) iterations relaxing the test vectors (setupSolverParams) */
+  int setup_iters;       /* setup-solver iterations on A psi = v for the test vectors (setupSolverParams) */
   int smoother_iters;    /* MR post-smoothing iterations per level */
   int wrapper_iters;     /* K-cycle FGMRES iterations on intermediate levels (wrapperSolverParams) */
   double wrapper_tol;
@@ -266,9 +266,16 @@ typedef struct {
   gmg_prec prec;         /* F64: all FP64; F32: FP32 preconditioner; BF16: FP32 preconditioner with
                             tensor-core coarse stencils.  The outer FGMRES is always FP64. */
   uint64_t seed;         /* test-vector seed */
+  int setup_solver;      /* 0: BiCGStab (the reference's default setupSolverType), 1: GMRES(10) */
+  double setup_tol;      /* setup-solver tolerance (setupSolverParams.tolerance, 1e-3) */
+  int setup_passes;      /* passes over the test vectors (setupInitialIter): each pass solves with the
+                            previous pass's vectors (inverse iteration) */
+  int setup_null;        /* 1: null-vector setup (setupBasisVectorsType nullVectors: solve A psi = 0 from
+                            psi = v); 0: test-vector setup (solve A psi = v from psi = 0) */
 } gmg_mg_params;
 
-/* Defaults of MultiGridParams (MultigridParams.h:95-113) adapted to the MR smoother. */
+/* Defaults of MultiGridParams (MultigridParams.h:95-113) adapted to the MR smoother, with the
+   null-vector setup (100 BiCGStab iterations on A psi = 0) instead of one test-vector pass. */
 gmg_status gmg_mg_params_default(gmg_mg_params* p);
 /* Levels over the fine operator; solves take up to max_rhs right-hand sides at once. */
 gmg_status gmg_mg_create(gmg_wilson* fine, const gmg_mg_params* p, int max_rhs, gmg_mg** h);
