@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--suite", action="store_true",
                     help="per-row measurements (C1, C3, C4, fine operator) instead of the bench line")
     ap.add_argument("--rows", default="c1,c3,w_c4,c5", help="suite rows to run")
+    ap.add_argument("--no-mg", action="store_true",
+                    help="skip the 3-level MG solve measurement (32^4 Wilson-clover, 24 RHS) of the JSON line")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed applies (for profiler captures); prints a short line")
     return ap.parse_args()
@@ -68,6 +70,20 @@ def make_inputs():
     A = inputs.random_links(DIMS, NBASIS, r)
     x = inputs.gaussian_field((V, NRHS, NBASIS), r)
     return A, x
+
+
+def ncu_traffic():
+    """DRAM bytes (read + write) of one coarse_mrhs_tc_kernel launch on this workload, from the
+    committed ncu capture summary (profiles/coarse_mrhs_tc_kernel_c2.md), or None."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "coarse_mrhs_tc_kernel_c2.md")
+    try:
+        with open(path) as f:
+            for ln in f:
+                if ln.startswith("traffic_bytes_per_launch:"):
+                    return int(ln.split(":")[1])
+    except OSError:
+        pass
+    return None
 
 
 def peaks():
@@ -348,7 +364,8 @@ def main():
         "config": config_dict(f"{args.form} operands on tcgen05 tensor cores, FP32 accumulation, FP32 vectors"),
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": (achieved / hbm) if achieved else None, "traffic": None,
+            "frac": (achieved / hbm) if achieved else None, "traffic": ncu_traffic(),
+            "traffic_source": "ncu --set full capture, profiles/coarse_mrhs_tc_kernel_c2.md",
             "kernel": "coarse_mrhs_tc_kernel", "algorithmic_bytes_per_launch": TC_KERNEL_BYTES,
             "kernel_ms_avg": kavg_s * 1e3, "launches": kn.value,
             "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({src})",
@@ -364,6 +381,23 @@ def main():
     if rank == 0 and world == 1:
         cpu, _ = cpu_sample(A, x)
         line["cpu_baseline"] = cpu
+    if not args.no_mg:
+        # the MG solve half of the metric: 3-level K-cycle FGMRES on 32^4 Wilson-clover,
+        # 24 RHS to 1e-10, the mixed BF16 multi-RHS form against the plain FP64
+        # single-RHS form (timed on one RHS, scaled to 24); setup not in solve_s
+        torch.cuda.empty_cache()
+        import suite
+
+        mg = suite.c5_measure(nrhs=24, plain_rhs=1, forms=("mixed_bf16_mrhs", "plain_f64_single_rhs"))
+        line["mg_solve"] = {
+            "workload": "3-level K-cycle MG-preconditioned FGMRES, 32^4 Wilson-clover m=-0.35 csw 1, "
+                        "nbasis 24 / 32 on 4^4 / 2^4 blocks, 24 RHS to 1e-10",
+            "unit": "s", "higher_is_better": False,
+            "mixed_bf16_mrhs_s": mg["mixed_bf16_mrhs"]["solve_s_for_all_rhs"],
+            "plain_f64_single_rhs_s": mg["plain_f64_single_rhs"]["solve_s_for_all_rhs"],
+            "speedup_vs_plain_f64": mg["mixed_bf16_mrhs"]["speedup_vs_plain_f64"],
+            "details": mg,
+        }
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

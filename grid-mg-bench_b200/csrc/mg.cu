@@ -412,9 +412,14 @@ gmg_status kcycle(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s) {
   MGLevel& C = *h->L[l + 1];
   const int R = in.R;
   Vec bc = C.bc.with_rhs(R), xc = C.xc.with_rhs(R);
-  GMG_TRY(gmg_agg_project(L.agg, (gmg_prec)in.prec, (gmg_prec)in.prec, R, in.p, bc.p, (gmg_stream)s));
+  // the BF16 form restricts and prolongs on the tensor cores (BF16 hi + lo
+  // operands, FP32 accumulation: about FP32 accuracy)
+  const gmg_prec tc = (h->P.prec == GMG_BF16 && in.prec == GMG_F32 && L.dof % 2 == 0 && C.dof <= 64)
+                          ? GMG_BF16
+                          : (gmg_prec)in.prec;
+  GMG_TRY(gmg_agg_project(L.agg, tc, (gmg_prec)in.prec, R, in.p, bc.p, (gmg_stream)s));
   GMG_TRY(coarse_solve(h, l + 1, bc, xc, s));
-  GMG_TRY(gmg_agg_promote(L.agg, (gmg_prec)in.prec, (gmg_prec)in.prec, R, xc.p, out.p, (gmg_stream)s));
+  GMG_TRY(gmg_agg_promote(L.agg, tc, (gmg_prec)in.prec, R, xc.p, out.p, (gmg_stream)s));
   return mr_smooth(h, l, in, out, h->P.smoother_iters, s);
 }
 
