@@ -394,6 +394,16 @@ gmg_status gmg_wilson_apply(gmg_wilson* h, gmg_op op, int dir, int disp, gmg_pre
   return wilson_apply(h, op, dir, disp, vec_prec, nrhs, in, out, S(s));
 }
 
+gmg_status gmg_wilson_apply_mr(gmg_wilson* h, gmg_prec vec_prec, int nrhs, const void* in, void* out, double* d1,
+                               double* d2, gmg_stream s) {
+  GMG_CHECK(h && in && out && d1 && d2, GMG_ERR_ARGUMENT, "gmg_wilson_apply_mr: null argument");
+  GMG_CHECK(in != out, GMG_ERR_ARGUMENT, "gmg_wilson_apply_mr: in and out must not alias");
+  GMG_CHECK(h->gauge_set, GMG_ERR_STATE, "gmg_wilson_apply_mr: gauge not set");
+  GMG_CHECK(nrhs >= 1 && nrhs <= 1024, GMG_ERR_ARGUMENT, "gmg_wilson_apply_mr: nrhs out of range");
+  GMG_CHECK(vec_prec_ok(vec_prec), GMG_ERR_ARGUMENT, "gmg_wilson_apply_mr: vectors must be F64 or F32");
+  return wilson_apply_mr(h, vec_prec, nrhs, in, out, (double2*)d1, (double2*)d2, S(s));
+}
+
 // ----------------------------------------------------------------- coarsen --
 gmg_status gmg_coarsen_wilson(gmg_coarse* out, gmg_agg* agg, gmg_wilson* fine, gmg_stream s) {
   GMG_CHECK(out && agg && fine, GMG_ERR_ARGUMENT, "gmg_coarsen_wilson: null argument");

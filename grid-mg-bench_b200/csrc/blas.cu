@@ -135,6 +135,172 @@ __global__ void chiral_double_kernel(const typename C2<T>::t* __restrict__ X, do
   }
 }
 
+// ---------------------------------------------------------------------------
+// Row geometry.  A field row is one site: R * dof contiguous complex numbers.
+// With RD = R * dof <= 1024, a block of spb * RD threads takes spb sites per
+// step and every thread owns one fixed (rhs, dof) slot of the row, so the
+// block's loads and stores are contiguous, the RHS index of a thread is
+// computed once, and per-RHS sums reduce inside the block.
+// ---------------------------------------------------------------------------
+struct Row {
+  int RD, spb, threads, grid;
+};
+
+static Row row_geom(int64_t V, int R, int dof) {
+  Row g;
+  g.RD = R * dof;
+  g.spb = g.RD <= 256 ? std::max(1, 256 / g.RD) : 1;
+  g.threads = (g.spb * g.RD + 31) / 32 * 32;
+  g.grid = (int)std::max<int64_t>(1, std::min<int64_t>((V + g.spb - 1) / g.spb, 148 * 16));
+  return g;
+}
+
+// out[(j0+j)*R + r] += sum_s <X_{j0+j}(s, r), Y(s, r)>, j < min(JB, nx - j0).
+// Per-thread partial sums go to shared memory; then one thread per (j, r) adds
+// the partials of the spb * dof threads that own RHS r (no shared-memory
+// atomics: with few RHS every thread would hit the same address) and issues one
+// global FP64 atomic per (block, j, r).
+template <class T, int JB>
+__global__ void __launch_bounds__(1024) multidot_row_kernel(const typename C2<T>::t* __restrict__ X, int64_t xstride,
+                                                            int j0, int nx, const typename C2<T>::t* __restrict__ Y,
+                                                            int64_t V, int R, int dof, int spb,
+                                                            double2* __restrict__ out, const int* __restrict__ mask) {
+  extern __shared__ double part[];  // [JB][2][blockDim]
+  const int RD = R * dof, t = threadIdx.x, NT = blockDim.x;
+  const int so = t / RD, i = t % RD, r = i / dof;
+  const bool act = t < spb * RD && !(mask && !mask[r]);
+  const int nj = min(JB, nx - j0);
+  double ar[JB], ai[JB];
+#pragma unroll
+  for (int j = 0; j < JB; ++j) ar[j] = ai[j] = 0.0;
+  if (act) {
+    for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+      const int64_t e = s * RD + i;
+      const double yr = Y[e].x, yi = Y[e].y;
+#pragma unroll
+      for (int j = 0; j < JB; ++j) {
+        if (j < nj) {
+          const typename C2<T>::t x = X[(int64_t)(j0 + j) * xstride + e];
+          ar[j] += (double)x.x * yr + (double)x.y * yi;
+          ai[j] += (double)x.x * yi - (double)x.y * yr;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < JB; ++j) {
+    part[(2 * j) * NT + t] = ar[j];
+    part[(2 * j + 1) * NT + t] = ai[j];
+  }
+  __syncthreads();
+  // stage 1: fold the spb site slots onto slot 0, one (j, re/im, rhs-dof) per thread
+  if (spb > 1) {
+    for (int k = t; k < 2 * nj * RD; k += NT) {
+      const int jc = k / RD, ii = k % RD;
+      double v = part[jc * NT + ii];
+      for (int o = 1; o < spb; ++o) v += part[jc * NT + o * RD + ii];
+      part[jc * NT + ii] = v;
+    }
+    __syncthreads();
+  }
+  // stage 2: fold the dof components of each rhs
+  for (int k = t; k < nj * R; k += NT) {
+    const int j = k / R, rr = k % R;
+    double vr = 0.0, vi = 0.0;
+    for (int a = 0; a < dof; ++a) {
+      vr += part[(2 * j) * NT + rr * dof + a];
+      vi += part[(2 * j + 1) * NT + rr * dof + a];
+    }
+    atomicAdd(&out[(j0 + j) * R + rr].x, vr);
+    atomicAdd(&out[(j0 + j) * R + rr].y, vi);
+  }
+}
+
+// Y(s, r) += sgn * sum_j a[j*R + r] X_j(s, r), coefficients staged in shared memory
+template <class TX, class T>
+__global__ void __launch_bounds__(1024) multiaxpy_row_kernel(const double2* __restrict__ a,
+                                                             const typename C2<TX>::t* __restrict__ X,
+                                                             int64_t xstride, int nx, typename C2<T>::t* __restrict__ Y,
+                                                             int64_t V, int R, int dof, int spb, double sgn) {
+  extern __shared__ double2 cf[];  // [nx][R]
+  const int RD = R * dof, t = threadIdx.x;
+  const int so = t / RD, i = t % RD, r = i / dof;
+  for (int k = t; k < nx * R; k += blockDim.x) cf[k] = make_double2(sgn * a[k].x, sgn * a[k].y);
+  __syncthreads();
+  if (t >= spb * RD) return;
+  for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+    const int64_t e = s * RD + i;
+    double yr = Y[e].x, yi = Y[e].y;
+    for (int j = 0; j < nx; ++j) {
+      const double2 c = cf[j * R + r];
+      const typename C2<TX>::t x = X[j * xstride + e];
+      yr += c.x * x.x - c.y * x.y;
+      yi += c.x * x.y + c.y * x.x;
+    }
+    Y[e].x = (T)yr;
+    Y[e].y = (T)yi;
+  }
+}
+
+// Y(r) = X(r) / sqrt(n[r].x)
+template <class T>
+__global__ void __launch_bounds__(1024) scale_inv_norm_row_kernel(const double2* __restrict__ n,
+                                                                  const typename C2<T>::t* __restrict__ X,
+                                                                  typename C2<T>::t* __restrict__ Y, int64_t V, int R,
+                                                                  int dof, int spb) {
+  const int RD = R * dof, t = threadIdx.x;
+  if (t >= spb * RD) return;
+  const int so = t / RD, i = t % RD, r = i / dof;
+  const double nn = n[r].x;
+  const double sc = nn > 0.0 ? rsqrt(nn) : 0.0;
+  for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+    const int64_t e = s * RD + i;
+    Y[e].x = (T)(sc * X[e].x);
+    Y[e].y = (T)(sc * X[e].y);
+  }
+}
+
+// MR step: alpha = <Ar, r> / <Ar, Ar>; x += alpha r, r -= alpha Ar
+template <class T>
+__global__ void __launch_bounds__(1024) mr_update_row_kernel(const double2* __restrict__ d1,
+                                                             const double2* __restrict__ d2,
+                                                             typename C2<T>::t* __restrict__ x,
+                                                             typename C2<T>::t* __restrict__ rr_,
+                                                             const typename C2<T>::t* __restrict__ Ar, int64_t V, int R,
+                                                             int dof, int spb) {
+  const int RD = R * dof, t = threadIdx.x;
+  if (t >= spb * RD) return;
+  const int so = t / RD, i = t % RD, k = i / dof;
+  const double den = d2[k].x;
+  const double ar = den > 0.0 ? d1[k].x / den : 0.0, ai = den > 0.0 ? d1[k].y / den : 0.0;
+  for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+    const int64_t e = s * RD + i;
+    const double rr = rr_[e].x, ri = rr_[e].y, qr = Ar[e].x, qi = Ar[e].y;
+    x[e].x = (T)(x[e].x + ar * rr - ai * ri);
+    x[e].y = (T)(x[e].y + ar * ri + ai * rr);
+    rr_[e].x = (T)(rr - (ar * qr - ai * qi));
+    rr_[e].y = (T)(ri - (ar * qi + ai * qr));
+  }
+}
+
+// Y(r) = a[r] X(r) + b[r] Y(r)
+template <class T>
+__global__ void __launch_bounds__(1024) axpby_row_kernel(const double2* __restrict__ a,
+                                                         const typename C2<T>::t* __restrict__ X,
+                                                         const double2* __restrict__ b, typename C2<T>::t* __restrict__ Y,
+                                                         int64_t V, int R, int dof, int spb) {
+  const int RD = R * dof, t = threadIdx.x;
+  if (t >= spb * RD) return;
+  const int so = t / RD, i = t % RD, r = i / dof;
+  const double2 ca = a[r], cb = b[r];
+  for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+    const int64_t e = s * RD + i;
+    const typename C2<T>::t x = X[e], y = Y[e];
+    Y[e].x = (T)(ca.x * x.x - ca.y * x.y + cb.x * y.x - cb.y * y.y);
+    Y[e].y = (T)(ca.x * x.y + ca.y * x.x + cb.x * y.y + cb.y * y.x);
+  }
+}
+
 }  // namespace blas
 
 // ---------------------------------------------------------------- host wrappers
@@ -142,6 +308,26 @@ gmg_status vec_multidot(const Vec& X0, int nx, int64_t xstride_elems, const Vec&
                         cudaStream_t s) {
   GMG_CUDA(cudaMemsetAsync(out_dev, 0, sizeof(double2) * nx * Y.R, s));
   constexpr int JB = 4;
+  if (Y.R * Y.dof <= 1024) {
+    const blas::Row g = blas::row_geom(Y.V, Y.R, Y.dof);
+    const size_t sm = sizeof(double) * 2 * JB * g.threads;
+    if (sm > 48 * 1024) {
+      GMG_CUDA(cudaFuncSetAttribute(blas::multidot_row_kernel<double, JB>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      GMG_CUDA(cudaFuncSetAttribute(blas::multidot_row_kernel<float, JB>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    }
+    for (int j0 = 0; j0 < nx; j0 += JB) {
+      if (Y.prec == GMG_F64)
+        blas::multidot_row_kernel<double, JB><<<g.grid, g.threads, sm, s>>>(
+            (const double2*)X0.p, xstride_elems, j0, nx, (const double2*)Y.p, Y.V, Y.R, Y.dof, g.spb, out_dev, mask);
+      else
+        blas::multidot_row_kernel<float, JB><<<g.grid, g.threads, sm, s>>>(
+            (const float2*)X0.p, xstride_elems, j0, nx, (const float2*)Y.p, Y.V, Y.R, Y.dof, g.spb, out_dev, mask);
+      GMG_CUDA(cudaGetLastError());
+    }
+    return GMG_OK;
+  }
   const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((Y.V + 255) / 256, (148 * 8 + Y.R - 1) / Y.R));
   const dim3 grid(gx, Y.R);
   for (int j0 = 0; j0 < nx; j0 += JB) {
@@ -158,6 +344,24 @@ gmg_status vec_multidot(const Vec& X0, int nx, int64_t xstride_elems, const Vec&
 
 gmg_status vec_multiaxpy(const double2* a_dev, const Vec& X0, int nx, int64_t xstride_elems, Vec& Y, cudaStream_t s,
                          double sgn) {
+  if (Y.R * Y.dof <= 1024 && sizeof(double2) * (size_t)nx * Y.R <= 48 * 1024) {
+    const blas::Row rg = blas::row_geom(Y.V, Y.R, Y.dof);
+    const size_t sm = sizeof(double2) * (size_t)nx * Y.R;
+    if (Y.prec == GMG_F64 && X0.prec == GMG_F64)
+      blas::multiaxpy_row_kernel<double, double><<<rg.grid, rg.threads, sm, s>>>(
+          a_dev, (const double2*)X0.p, xstride_elems, nx, (double2*)Y.p, Y.V, Y.R, Y.dof, rg.spb, sgn);
+    else if (Y.prec == GMG_F64)
+      blas::multiaxpy_row_kernel<float, double><<<rg.grid, rg.threads, sm, s>>>(
+          a_dev, (const float2*)X0.p, xstride_elems, nx, (double2*)Y.p, Y.V, Y.R, Y.dof, rg.spb, sgn);
+    else if (X0.prec == GMG_F32)
+      blas::multiaxpy_row_kernel<float, float><<<rg.grid, rg.threads, sm, s>>>(
+          a_dev, (const float2*)X0.p, xstride_elems, nx, (float2*)Y.p, Y.V, Y.R, Y.dof, rg.spb, sgn);
+    else
+      blas::multiaxpy_row_kernel<double, float><<<rg.grid, rg.threads, sm, s>>>(
+          a_dev, (const double2*)X0.p, xstride_elems, nx, (float2*)Y.p, Y.V, Y.R, Y.dof, rg.spb, sgn);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  }
   const int g = blas::grid1(Y.elems());
   if (Y.prec == GMG_F64 && X0.prec == GMG_F64)
     blas::multiaxpy_kernel<double, double><<<g, 256, 0, s>>>(a_dev, (const double2*)X0.p, xstride_elems, nx,
@@ -176,6 +380,17 @@ gmg_status vec_multiaxpy(const double2* a_dev, const Vec& X0, int nx, int64_t xs
 }
 
 gmg_status vec_axpby(const double2* a_dev, const Vec& X, const double2* b_dev, Vec& Y, cudaStream_t s) {
+  if (Y.R * Y.dof <= 1024) {
+    const blas::Row rg = blas::row_geom(Y.V, Y.R, Y.dof);
+    if (Y.prec == GMG_F64)
+      blas::axpby_row_kernel<double><<<rg.grid, rg.threads, 0, s>>>(a_dev, (const double2*)X.p, b_dev, (double2*)Y.p,
+                                                                     Y.V, Y.R, Y.dof, rg.spb);
+    else
+      blas::axpby_row_kernel<float><<<rg.grid, rg.threads, 0, s>>>(a_dev, (const float2*)X.p, b_dev, (float2*)Y.p,
+                                                                    Y.V, Y.R, Y.dof, rg.spb);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  }
   const int g = blas::grid1(Y.elems());
   if (Y.prec == GMG_F64)
     blas::axpby_kernel<double><<<g, 256, 0, s>>>(a_dev, (const double2*)X.p, b_dev, (double2*)Y.p, Y.V, Y.R, Y.dof);
@@ -284,6 +499,17 @@ __global__ void xmy_kernel(const typename C2<T>::t* __restrict__ X, typename C2<
 }  // namespace blas
 
 gmg_status vec_scale_inv_norm(const double2* n_dev, const Vec& X, Vec& Y, cudaStream_t s) {
+  if (Y.R * Y.dof <= 1024) {
+    const blas::Row rg = blas::row_geom(Y.V, Y.R, Y.dof);
+    if (Y.prec == GMG_F64)
+      blas::scale_inv_norm_row_kernel<double><<<rg.grid, rg.threads, 0, s>>>(n_dev, (const double2*)X.p, (double2*)Y.p,
+                                                                              Y.V, Y.R, Y.dof, rg.spb);
+    else
+      blas::scale_inv_norm_row_kernel<float><<<rg.grid, rg.threads, 0, s>>>(n_dev, (const float2*)X.p, (float2*)Y.p,
+                                                                             Y.V, Y.R, Y.dof, rg.spb);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  }
   const int g = blas::grid1(Y.elems());
   if (Y.prec == GMG_F64)
     blas::scale_inv_norm_kernel<double><<<g, 256, 0, s>>>(n_dev, (const double2*)X.p, (double2*)Y.p, Y.V, Y.R, Y.dof);
@@ -294,6 +520,17 @@ gmg_status vec_scale_inv_norm(const double2* n_dev, const Vec& X, Vec& Y, cudaSt
 }
 
 gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s) {
+  if (x.R * x.dof <= 1024) {
+    const blas::Row rg = blas::row_geom(x.V, x.R, x.dof);
+    if (x.prec == GMG_F64)
+      blas::mr_update_row_kernel<double><<<rg.grid, rg.threads, 0, s>>>(d1, d2, (double2*)x.p, (double2*)r.p,
+                                                                         (const double2*)Ar.p, x.V, x.R, x.dof, rg.spb);
+    else
+      blas::mr_update_row_kernel<float><<<rg.grid, rg.threads, 0, s>>>(d1, d2, (float2*)x.p, (float2*)r.p,
+                                                                        (const float2*)Ar.p, x.V, x.R, x.dof, rg.spb);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  }
   const int g = blas::grid1(x.elems());
   if (x.prec == GMG_F64)
     blas::mr_update_kernel<double><<<g, 256, 0, s>>>(d1, d2, (double2*)x.p, (double2*)r.p, (const double2*)Ar.p, x.V,

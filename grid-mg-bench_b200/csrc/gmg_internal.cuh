@@ -184,6 +184,8 @@ gmg_status agg_promote_tc(gmg_agg* h, int nrhs, const float* coarse, float* fine
 gmg_status wilson_build_clover(gmg_wilson* h, cudaStream_t s);
 gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs,
                         const void* in, void* out, cudaStream_t s);
+gmg_status wilson_apply_mr(gmg_wilson* h, int vec_prec, int nrhs, const void* in, void* out, double2* d1,
+                           double2* d2, cudaStream_t s);
 
 // coarse-operator construction (coarsen.cu)
 gmg_status coarsen_wilson(gmg_coarse* out, gmg_agg* agg, gmg_wilson* fine, cudaStream_t s);

@@ -239,6 +239,222 @@ __global__ void __launch_bounds__(256) wilson_tile_kernel(
   }
 }
 
+// Multi-RHS quad kernel: four lanes per (site, rhs), lane q owning spin q.
+// A quad reads its 12-component record as one contiguous run and consecutive
+// quads hold consecutive right-hand sides, so a warp's loads cover 8 records
+// back to back.  The spin projection (1 -+ gamma_mu) couples spin q with spin
+// perm(q) of the same record: a quad-local shuffle.  Lanes 0 and 1 form the
+// two projected half-spinors and multiply them by the link; lanes 2 and 3
+// take the reconstructed lower spins from lanes perm(q).  The clover couples
+// the two spins of a chiral block: one more shuffle.  Links and clover of the
+// tile's kTileSites sites are staged in shared memory once per tile.
+template <class C>
+__device__ __forceinline__ C shfl_c(C v, int src_lane) {
+  v.x = __shfl_sync(0xffffffffu, v.x, src_lane);
+  v.y = __shfl_sync(0xffffffffu, v.y, src_lane);
+  return v;
+}
+
+template <class T, int MU, bool DAG>
+__device__ __forceinline__ void quad_hop(typename wt<T>::C acc[3], const typename wt<T>::C* __restrict__ U,
+                                         const typename wt<T>::C psi[3], int q, int qbase, T coef) {
+  typedef typename wt<T>::C C;
+  const int sgc = DAG ? 0 : 2;  // projector 1 + sg gamma_mu: sg = -1 forward (code 2), +1 backward
+  // upper half-spinor h[q] = psi_q + phase * psi_perm(q), formed on lanes 0, 1
+  const int pq = gperm(MU, q & 1);
+  C other[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) other[c] = shfl_c(psi[c], qbase + (q < 2 ? gperm(MU, q) : pq));
+  C uh[3];
+  if (q < 2) {
+    const int code = (gphase(MU, q) + sgc) & 3;
+    C h[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) h[c] = cadd(psi[c], cphase(other[c], code));
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      C v{0, 0};
+#pragma unroll
+      for (int b = 0; b < 3; ++b) v = cadd(v, DAG ? cmulc(U[b * 3 + a], h[b]) : cmul(U[a * 3 + b], h[b]));
+      uh[a] = v;
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) uh[a] = C{0, 0};
+  }
+  // lower spins: phase * uh[perm(q)] from lane perm(q) (an upper lane)
+  C low[3];
+  const int src = q < 2 ? q : gperm(MU, q);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) low[a] = shfl_c(uh[a], qbase + src);
+  if (q < 2) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      acc[a].x += coef * uh[a].x;
+      acc[a].y += coef * uh[a].y;
+    }
+  } else {
+    const int code = (gphase(MU, q) + sgc) & 3;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const C v = cphase(low[a], code);
+      acc[a].x += coef * v.x;
+      acc[a].y += coef * v.y;
+    }
+  }
+}
+
+//
+// DOTS (op M or MDAG only): also accumulate, per RHS r, d1[r] += <out, in> and
+// d2[r].x += <out, out> over all sites -- the two inner products of the
+// minimal-residual step -- so the smoother reads neither vector again.  A quad
+// folds its lanes with shuffles, the CTA its sites in shared memory, and the
+// CTA adds its totals to d1 / d2 (zeroed by the caller) once at the end.
+template <class T, bool DOTS>
+__global__ void __launch_bounds__(512) wilson_quad_kernel(
+    const typename wt<T>::C* __restrict__ gauge, const typename wt<T>::C* __restrict__ clover,
+    const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
+    typename wt<T>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
+    int apbc, int tvol, int Lt, double2* __restrict__ d1, double2* __restrict__ d2) {
+  typedef typename wt<T>::C C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* Ls = reinterpret_cast<C*>(smem_raw);  // [kTileSites][8][9]: p < 4 U_mu(x), p >= 4 U_mu(x - mu)
+  C* Cs = Ls + kTileSites * 72;            // [kTileSites][72]
+  double* Ds = reinterpret_cast<double*>(Cs + kTileSites * 72);  // DOTS: [nrhs][3]
+  if (DOTS) {
+    for (int k = threadIdx.x; k < 3 * nrhs; k += blockDim.x) Ds[k] = 0.0;
+  }
+  const bool g5 = (op == GMG_OP_MDAG);
+  const int q = threadIdx.x & 3, qbase = threadIdx.x & 31 & ~3;
+  const int grp = threadIdx.x >> 2;
+  const int sl = grp / rt, rl = grp % rt;
+  const int nt = (V + kTileSites - 1) / kTileSites;
+  const T sg5 = (g5 && q >= 2) ? (T)-1 : (T)1;
+  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+    const int s0 = tile * kTileSites;
+    const int ns = min(kTileSites, V - s0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < ns * 72; k += blockDim.x) {
+      const int j = k / 72, e = k % 72, p = e / 9, m = e % 9;
+      const int st = s0 + j;
+      const int ls = p < 4 ? st : nbr[(int64_t)p * V + st];
+      Ls[k] = gauge[((int64_t)ls * 4 + (p & 3)) * 9 + m];
+      Cs[k] = clover[(int64_t)s0 * 72 + k];
+    }
+    __syncthreads();
+    // a quad with sl >= ns has no site; it still joins the shuffles (all lanes of
+    // a quad agree), reading site s0 harmlessly, and stores nothing
+    const bool active = sl < ns;
+    const int site = s0 + (active ? sl : 0);
+    const int tc = site / tvol;
+    const C* Lsite = Ls + (active ? sl : 0) * 72;
+    for (int r = rl; r < nrhs; r += rt) {
+      C acc[3], cin[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc[c] = C{0, 0};
+      if (op != GMG_OP_MDIR) {
+        const C* src = in + ((int64_t)site * nrhs + r) * 12 + q * 3;
+        C psi[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          cin[c] = src[c];
+          psi[c] = cin[c];
+          psi[c].x *= sg5;
+          psi[c].y *= sg5;
+        }
+        // clover block of this spin's chirality: rows a = (q & 1) * 3 + c, columns over both spins
+        C partner[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) partner[c] = shfl_c(psi[c], qbase + (q ^ 1));
+        const C* cl = Cs + (active ? sl : 0) * 72 + (q >> 1) * 36;
+        const int a0 = (q & 1) * 3;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          C v;
+          v.x = diag * psi[c].x;
+          v.y = diag * psi[c].y;
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            // block columns 0..2 belong to the even spin of the block, 3..5 to the odd one
+            const C lo = (q & 1) ? partner[b] : psi[b];
+            const C hi = (q & 1) ? psi[b] : partner[b];
+            v = cadd(v, cmul(cl[(a0 + c) * 6 + b], lo));
+            v = cadd(v, cmul(cl[(a0 + c) * 6 + 3 + b], hi));
+          }
+          acc[c] = v;
+        }
+      }
+      if (op != GMG_OP_MDIAG) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+          const int mu = p & 3, dsp = p < 4 ? 1 : -1;
+          if (op == GMG_OP_MDIR && (mu != dir || dsp != disp)) continue;
+          const int nb = nbr[(int64_t)p * V + site];
+          T coef = (T)-0.5;
+          if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
+          const C* src = in + ((int64_t)nb * nrhs + r) * 12 + q * 3;
+          C psi[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            psi[c] = src[c];
+            psi[c].x *= sg5;
+            psi[c].y *= sg5;
+          }
+          const C* U = Lsite + p * 9;
+          switch (p) {
+            case 0: quad_hop<T, 0, false>(acc, U, psi, q, qbase, coef); break;
+            case 1: quad_hop<T, 1, false>(acc, U, psi, q, qbase, coef); break;
+            case 2: quad_hop<T, 2, false>(acc, U, psi, q, qbase, coef); break;
+            case 3: quad_hop<T, 3, false>(acc, U, psi, q, qbase, coef); break;
+            case 4: quad_hop<T, 0, true>(acc, U, psi, q, qbase, coef); break;
+            case 5: quad_hop<T, 1, true>(acc, U, psi, q, qbase, coef); break;
+            case 6: quad_hop<T, 2, true>(acc, U, psi, q, qbase, coef); break;
+            default: quad_hop<T, 3, true>(acc, U, psi, q, qbase, coef); break;
+          }
+        }
+      }
+      double pr = 0.0, pi = 0.0, pn = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        acc[c].x *= sg5;
+        acc[c].y *= sg5;
+        if (DOTS) {
+          const double vx = acc[c].x, vy = acc[c].y, ix = cin[c].x, iy = cin[c].y;
+          pr += vx * ix + vy * iy;
+          pi += vx * iy - vy * ix;
+          pn += vx * vx + vy * vy;
+        }
+      }
+      if (active) {
+        C* dst = out + ((int64_t)site * nrhs + r) * 12 + q * 3;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dst[c] = acc[c];
+      }
+      if (DOTS) {
+#pragma unroll
+        for (int m = 1; m <= 2; m <<= 1) {
+          pr += __shfl_xor_sync(0xffffffffu, pr, m);
+          pi += __shfl_xor_sync(0xffffffffu, pi, m);
+          pn += __shfl_xor_sync(0xffffffffu, pn, m);
+        }
+        if (active && q == 0) {
+          atomicAdd(&Ds[3 * r], pr);
+          atomicAdd(&Ds[3 * r + 1], pi);
+          atomicAdd(&Ds[3 * r + 2], pn);
+        }
+      }
+    }
+  }
+  if (DOTS) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < nrhs; k += blockDim.x) {
+      atomicAdd(&d1[k].x, Ds[3 * k]);
+      atomicAdd(&d1[k].y, Ds[3 * k + 1]);
+      atomicAdd(&d2[k].x, Ds[3 * k + 2]);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // clover term from the gauge field (thread per site)
 // ---------------------------------------------------------------------------
@@ -362,6 +578,47 @@ gmg_status wilson_build_clover(gmg_wilson* h, cudaStream_t s) {
   return GMG_OK;
 }
 
+// quad kernel launch: kTileSites sites x rt RHS x 4 spin lanes per CTA, rt the
+// largest divisor of nrhs up to 8 (at most 512 threads)
+template <bool DOTS>
+static gmg_status launch_quad(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs, const void* in,
+                              void* out, double2* d1, double2* d2, cudaStream_t s) {
+  const int V = (int)h->dims.vol();
+  const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
+  int rt = 1;
+  for (int c = std::min(nrhs, 8); c >= 1; --c)
+    if (nrhs % c == 0) {
+      rt = c;
+      break;
+    }
+  const int threads = kTileSites * rt * 4;
+  const int tiles = (V + kTileSites - 1) / kTileSites;
+  // about 2048 resident threads per SM
+  const int g = std::min(tiles, 148 * std::max(1, 2048 / threads));
+  const size_t dots = DOTS ? sizeof(double) * 3 * (size_t)nrhs : 0;
+  if (vec_prec == GMG_F64) {
+    const size_t smem = sizeof(double2) * 2 * kTileSites * 72 + dots;
+    if (smem > 48 * 1024)
+      GMG_CUDA(cudaFuncSetAttribute(wilson_quad_kernel<double, DOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+    wilson_quad_kernel<double, DOTS><<<g, threads, smem, s>>>(
+        h->gauge.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(), (const double2*)in, (double2*)out, V,
+        nrhs, rt, 4.0 + h->mass, op, dir, disp, h->apbc, tvol, h->dims.d[3], d1, d2);
+  } else if (vec_prec == GMG_F32) {
+    const size_t smem = sizeof(float2) * 2 * kTileSites * 72 + dots;
+    if (smem > 48 * 1024)
+      GMG_CUDA(cudaFuncSetAttribute(wilson_quad_kernel<float, DOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+    wilson_quad_kernel<float, DOTS><<<g, threads, smem, s>>>(
+        h->gauge_f.as<float2>(), h->clover_f.as<float2>(), h->nbr.as<int32_t>(), (const float2*)in, (float2*)out, V,
+        nrhs, rt, (float)(4.0 + h->mass), op, dir, disp, h->apbc, tvol, h->dims.d[3], d1, d2);
+  } else {
+    return fail(GMG_ERR_UNSUPPORTED, "wilson apply: vectors must be F64 or F32");
+  }
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
 gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs,
                         const void* in, void* out, cudaStream_t s) {
   const int V = (int)h->dims.vol();
@@ -369,30 +626,7 @@ gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, 
   const int64_t total = (int64_t)V * nrhs;
   const int grid = (int)std::min<int64_t>((total + 127) / 128, 148 * 32);
   KernelTimer kt("wilson", s);
-  if (nrhs >= 4 && op != GMG_OP_MDIR) {
-    // multi-RHS tile: up to 16 threads per site, links and clover in shared memory
-    const int rt = std::min(nrhs, 16);
-    const int threads = kTileSites * rt;
-    const int tiles = (V + kTileSites - 1) / kTileSites;
-    const int g = std::min(tiles, 148 * 16);
-    if (vec_prec == GMG_F64) {
-      const size_t smem = sizeof(double2) * 2 * kTileSites * 72;
-      wilson_tile_kernel<double><<<g, threads, smem, s>>>(h->gauge.as<double2>(), h->clover.as<double2>(),
-                                                          h->nbr.as<int32_t>(), (const double2*)in, (double2*)out, V,
-                                                          nrhs, rt, 4.0 + h->mass, op, dir, disp, h->apbc, tvol,
-                                                          h->dims.d[3]);
-    } else if (vec_prec == GMG_F32) {
-      const size_t smem = sizeof(float2) * 2 * kTileSites * 72;
-      wilson_tile_kernel<float><<<g, threads, smem, s>>>(h->gauge_f.as<float2>(), h->clover_f.as<float2>(),
-                                                         h->nbr.as<int32_t>(), (const float2*)in, (float2*)out, V,
-                                                         nrhs, rt, (float)(4.0 + h->mass), op, dir, disp, h->apbc,
-                                                         tvol, h->dims.d[3]);
-    } else {
-      return fail(GMG_ERR_UNSUPPORTED, "wilson apply: vectors must be F64 or F32");
-    }
-    GMG_CUDA(cudaGetLastError());
-    return GMG_OK;
-  }
+  if (nrhs >= 4) return launch_quad<false>(h, op, dir, disp, vec_prec, nrhs, in, out, nullptr, nullptr, s);
   if (vec_prec == GMG_F64) {
     wilson_kernel<double><<<grid, 128, 0, s>>>(h->gauge.as<double2>(), h->clover.as<double2>(),
                                                 h->nbr.as<int32_t>(), (const double2*)in, (double2*)out, V,
@@ -408,6 +642,16 @@ gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, 
   }
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
+}
+
+// out = M in, and the minimal-residual inner products d1[r] = <out, in>,
+// d2[r].x = <out, out> (d1, d2: nrhs entries each, zeroed here)
+gmg_status wilson_apply_mr(gmg_wilson* h, int vec_prec, int nrhs, const void* in, void* out, double2* d1,
+                           double2* d2, cudaStream_t s) {
+  KernelTimer kt("wilson", s);
+  GMG_CUDA(cudaMemsetAsync(d1, 0, sizeof(double2) * nrhs, s));
+  GMG_CUDA(cudaMemsetAsync(d2, 0, sizeof(double2) * nrhs, s));
+  return launch_quad<true>(h, GMG_OP_M, 0, 0, vec_prec, nrhs, in, out, d1, d2, s);
 }
 
 }  // namespace gmg

@@ -356,6 +356,15 @@ class WilsonClover:
     def Mdir(self, inp, out, d, disp):
         return self.apply(OP_MDIR, inp, out, d, disp)
 
+    def M_mr(self, inp, out):
+        """out = M inp and the MR-step inner products <out, inp>, <out, out> per RHS."""
+        _check_vec(inp, self.V, 12, "in")
+        _check_vec(out, self.V, 12, "out")
+        d = torch.zeros((2, inp.shape[1]), dtype=torch.complex128, device=inp.device)
+        _chk(lib().gmg_wilson_apply_mr(self._h, _vec_prec(inp), inp.shape[1], _ptr(inp), _ptr(out), _ptr(d[0]),
+                                       _ptr(d[1]), _stream()))
+        return d[0], d[1].real
+
 
 class MGParams(ctypes.Structure):
     _fields_ = [("nlevels", ctypes.c_int), ("block", (ctypes.c_int * 4) * 2), ("nvec", ctypes.c_int * 2),

@@ -230,6 +230,12 @@ gmg_status gmg_wilson_get_clover(gmg_wilson* h, double* clover, int on_device, g
 /* op M / Mdag / Mdiag / Mdir(dir, disp); fields [V][nrhs][12] of vec_prec (F64/F32). */
 gmg_status gmg_wilson_apply(gmg_wilson* h, gmg_op op, int dir, int disp, gmg_prec vec_prec,
                             int nrhs, const void* in, void* out, gmg_stream s);
+/* out = M in together with the minimal-residual inner products of the MR
+   smoother step (the smoother solve of include/MultigridPreconditioner.h:
+   264-301): d1[r] = <out_r, in_r>,
+   d2[r] = <out_r, out_r> + 0i, device arrays of nrhs complex128. */
+gmg_status gmg_wilson_apply_mr(gmg_wilson* h, gmg_prec vec_prec, int nrhs, const void* in, void* out,
+                               double* d1, double* d2, gmg_stream s);
 
 /* ------------------------------------------------------------------------ */
 /* Galerkin coarse-operator construction                                     */

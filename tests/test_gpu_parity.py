@@ -269,10 +269,11 @@ def test_wilson_ops_f64(wil, op):
     assert orc.rel_dev_sq(ref, host(out)) < TOL64
 
 
-@pytest.mark.parametrize("nrhs", [4, 12, 20])
+@pytest.mark.parametrize("nrhs", [4, 7, 12, 13, 20])
 @pytest.mark.parametrize("op", ["M", "Mdag", "Mdiag"])
 def test_wilson_multi_rhs_tile(wil, nrhs, op):
-    # nrhs >= 4 runs the shared-memory tile kernel (16 sites, up to 16 threads per site)
+    # nrhs >= 4 runs the quad kernel: 16 sites per tile, 4 spin lanes per (site, RHS),
+    # rt = largest divisor of nrhs up to 8 RHS per pass (13 -> 1, 7 -> 7, 20 -> 5)
     dims, U, cl, w = wil
     x = inputs.gaussian_field((512, nrhs, 12), inputs.rng(stream=124 + nrhs))
     code = {"M": orc.OP_M, "Mdag": orc.OP_MDAG, "Mdiag": orc.OP_MDIAG}[op]
@@ -298,6 +299,37 @@ def test_wilson_mdir_f64_and_f32(wil):
     out = torch.zeros((512, 2, 12), dtype=torch.complex64, device=DEV)
     w.M(dev(x, torch.complex64), out)
     assert orc.rel_dev_sq(ref, host(out)) < TOL32
+
+
+def test_wilson_multi_rhs_mdir(wil):
+    # the quad kernel's single-hop form (CoarsenOperator's Mdir calls, nrhs >= 4)
+    dims, U, cl, w = wil
+    x = inputs.gaussian_field((512, 6, 12), inputs.rng(stream=141))
+    for d in range(4):
+        for disp in (1, -1):
+            ref = orc.wilson_clover(dims, U, cl, -0.1, 1, x, orc.OP_MDIR, d, disp)
+            out = torch.zeros((512, 6, 12), dtype=torch.complex128, device=DEV)
+            w.Mdir(dev(x), out, d, disp)
+            assert orc.rel_dev_sq(ref, host(out)) < TOL64, (d, disp)
+            out32 = torch.zeros((512, 6, 12), dtype=torch.complex64, device=DEV)
+            w.Mdir(dev(x, torch.complex64), out32, d, disp)
+            assert orc.rel_dev_sq(ref, host(out32)) < TOL32, (d, disp)
+
+
+@pytest.mark.parametrize("nrhs", [1, 3, 12])
+def test_wilson_apply_mr_products(wil, nrhs):
+    # M with the minimal-residual inner products formed in the kernel's epilogue
+    dims, U, cl, w = wil
+    x = inputs.gaussian_field((512, nrhs, 12), inputs.rng(stream=150 + nrhs))
+    ref = orc.wilson_clover(dims, U, cl, -0.1, 1, x, orc.OP_M)
+    d1_ref = np.einsum("srk,srk->r", ref.conj(), x)
+    d2_ref = np.einsum("srk,srk->r", ref.conj(), ref).real
+    for dt, tol in ((torch.complex128, TOL64), (torch.complex64, TOL32)):
+        out = torch.zeros((512, nrhs, 12), dtype=dt, device=DEV)
+        d1, d2 = w.M_mr(dev(x, dt), out)
+        assert orc.rel_dev_sq(ref, host(out)) < tol
+        assert np.abs(d1.cpu().numpy() - d1_ref).max() / np.abs(d2_ref).max() < np.sqrt(tol)
+        assert np.abs(d2.cpu().numpy() - d2_ref).max() / np.abs(d2_ref).max() < np.sqrt(tol)
 
 
 # --------------------------------------------------------------- CoarsenOperator
