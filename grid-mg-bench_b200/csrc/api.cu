@@ -394,6 +394,36 @@ gmg_status gmg_wilson_apply(gmg_wilson* h, gmg_op op, int dir, int disp, gmg_pre
   return wilson_apply(h, op, dir, disp, vec_prec, nrhs, in, out, S(s));
 }
 
+gmg_status gmg_wilson_set_kernel(gmg_wilson* h, gmg_wilson_kernel k) {
+  GMG_CHECK(h != nullptr, GMG_ERR_ARGUMENT, "gmg_wilson_set_kernel: null handle");
+  GMG_CHECK(k >= GMG_WILSON_AUTO && k <= GMG_WILSON_STAGED, GMG_ERR_ARGUMENT, "gmg_wilson_set_kernel: bad kernel");
+  h->wforce = (int)k;
+  return GMG_OK;
+}
+
+gmg_status gmg_wilson_tuned_kernel(gmg_wilson* h, gmg_prec vec_prec, int nrhs, int fused_mr, int single_hop,
+                                   gmg_wilson_kernel* k) {
+  GMG_CHECK(h && k, GMG_ERR_ARGUMENT, "gmg_wilson_tuned_kernel: null argument");
+  const int cls = nrhs < 4 ? 0 : nrhs < 8 ? 1 : nrhs < 16 ? 2 : nrhs < 32 ? 3 : 4;
+  const uint64_t key = (uint64_t)vec_prec | ((uint64_t)(fused_mr != 0) << 4) | ((uint64_t)(single_hop != 0) << 5) |
+                       ((uint64_t)cls << 8);
+  auto it = h->wtune.find(key);
+  *k = it == h->wtune.end() ? GMG_WILSON_AUTO : (gmg_wilson_kernel)it->second;
+  return GMG_OK;
+}
+
+gmg_status gmg_wilson_device_error(gmg_wilson* h, int* code) {
+  GMG_CHECK(h && code, GMG_ERR_ARGUMENT, "gmg_wilson_device_error: null argument");
+  *code = 0;
+  GMG_CUDA(cudaDeviceSynchronize());
+  if (!h->dev_err.p) return GMG_OK;
+  GMG_CUDA(cudaMemcpy(code, h->dev_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  GMG_CUDA(cudaMemset(h->dev_err.p, 0, sizeof(int)));
+  if (*code) return fail(GMG_ERR_TIMEOUT, "a staged Wilson kernel gave up waiting for its copies (code " +
+                                             std::to_string(*code) + ")");
+  return GMG_OK;
+}
+
 gmg_status gmg_wilson_apply_mr(gmg_wilson* h, gmg_prec vec_prec, int nrhs, const void* in, void* out, double* d1,
                                double* d2, gmg_stream s) {
   GMG_CHECK(h && in && out && d1 && d2, GMG_ERR_ARGUMENT, "gmg_wilson_apply_mr: null argument");

@@ -17,7 +17,9 @@
 // per (site, rhs); the (1 -+ gamma) projection halves the colour-matrix work
 // (rank-2 projector: lower spins are a phase times the upper ones).
 #include <algorithm>
+#include <vector>
 
+#include "async_copy.cuh"
 #include "gmg_internal.cuh"
 
 namespace gmg {
@@ -114,15 +116,19 @@ __device__ __forceinline__ void wilson_hop(typename wt<T>::C out[4][3],
 // One output spinor (site, rhs).  links(p) returns the 3x3 link of hop p
 // (p < 4: U_mu(x), p >= 4: U_mu(x - mu), applied daggered); cl: the site's
 // two 6x6 clover blocks.
-template <class T, class LinkFn>
+// DOTS (op M or MDAG): also add <out, in> and <out, out> of this (site, r) to
+// Ds[3 r .. 3 r + 2] (shared memory).
+template <class T, class LinkFn, bool DOTS = false>
 __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict__ cl, LinkFn links,
                                             const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
                                             typename wt<T>::C* __restrict__ out, int V, int nrhs, int site, int r,
-                                            T diag, int op, int dir, int disp, int apbc, int tvol, int Lt) {
+                                            T diag, int op, int dir, int disp, int apbc, int tvol, int Lt,
+                                            double* Ds = nullptr) {
   typedef typename wt<T>::C C;
   const bool g5 = (op == GMG_OP_MDAG);
   const int tc = site / tvol;
   C acc[4][3];
+  C cin[12];
 #pragma unroll
   for (int s = 0; s < 4; ++s)
 #pragma unroll
@@ -134,6 +140,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
       psi[k] = src[k];
+      if (DOTS) cin[k] = psi[k];
       if (g5 && k >= 6) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
     }
 #pragma unroll
@@ -168,6 +175,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
     }
   }
   C* dst = out + ((int64_t)site * nrhs + r) * 12;
+  double pr = 0.0, pi = 0.0, pn = 0.0;
 #pragma unroll
   for (int s = 0; s < 4; ++s)
 #pragma unroll
@@ -175,7 +183,18 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
       C v = acc[s][c];
       if (g5 && s >= 2) { v.x = -v.x; v.y = -v.y; }
       dst[s * 3 + c] = v;
+      if (DOTS) {
+        const double vx = v.x, vy = v.y, ix = cin[s * 3 + c].x, iy = cin[s * 3 + c].y;
+        pr += vx * ix + vy * iy;
+        pi += vx * iy - vy * ix;
+        pn += vx * vx + vy * vy;
+      }
     }
+  if (DOTS) {
+    atomicAdd(&Ds[3 * r], pr);
+    atomicAdd(&Ds[3 * r + 1], pi);
+    atomicAdd(&Ds[3 * r + 2], pn);
+  }
 }
 
 // thread per (site, rhs); links and clover read from global memory (few RHS)
@@ -199,22 +218,26 @@ __global__ void __launch_bounds__(256) wilson_kernel(
   }
 }
 
-// Multi-RHS tile: a CTA takes kTileSites consecutive sites and all right-hand
-// sides (rt threads per site, each looping over its RHS); the sites' 8 hop
-// links and clover blocks are staged in shared memory once and read by every
-// RHS of the tile instead of once per RHS from global memory.
 constexpr int kTileSites = 16;
 
-template <class T>
+// Multi-RHS tile kernel: a CTA takes kTileSites consecutive sites and all
+// right-hand sides (rt threads per site, each looping over its RHS); the
+// sites' 8 hop links and clover blocks are staged in shared memory once and
+// read by every RHS of the tile.  Thread per (site, RHS) otherwise, spinors
+// read from global memory.
+template <class T, bool DOTS>
 __global__ void __launch_bounds__(256) wilson_tile_kernel(
-    const typename wt<T>::C* __restrict__ gauge, const typename wt<T>::C* __restrict__ clover,
+    const typename wt<T>::C* __restrict__ hop, const typename wt<T>::C* __restrict__ clover,
     const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
     typename wt<T>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
-    int apbc, int tvol, int Lt) {
+    int apbc, int tvol, int Lt, double2* __restrict__ d1, double2* __restrict__ d2) {
   typedef typename wt<T>::C C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* Ls = reinterpret_cast<C*>(smem_raw);  // [kTileSites][8][9]: p < 4 U_mu(x), p >= 4 U_mu(x - mu)
   C* Cs = Ls + kTileSites * 72;            // [kTileSites][72]
+  double* Ds = reinterpret_cast<double*>(Cs + kTileSites * 72);  // DOTS: [nrhs][3]
+  if (DOTS)
+    for (int k = threadIdx.x; k < 3 * nrhs; k += blockDim.x) Ds[k] = 0.0;
   const int nt = (V + kTileSites - 1) / kTileSites;
   const int sl = threadIdx.x / rt, rl = threadIdx.x % rt;
   for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
@@ -222,10 +245,7 @@ __global__ void __launch_bounds__(256) wilson_tile_kernel(
     const int ns = min(kTileSites, V - s0);
     __syncthreads();
     for (int k = threadIdx.x; k < ns * 72; k += blockDim.x) {
-      const int j = k / 72, e = k % 72, p = e / 9, m = e % 9;
-      const int site = s0 + j;
-      const int ls = p < 4 ? site : nbr[(int64_t)p * V + site];
-      Ls[k] = gauge[((int64_t)ls * 4 + (p & 3)) * 9 + m];
+      Ls[k] = hop[(int64_t)s0 * 72 + k];
       Cs[k] = clover[(int64_t)s0 * 72 + k];
     }
     __syncthreads();
@@ -234,7 +254,16 @@ __global__ void __launch_bounds__(256) wilson_tile_kernel(
       const C* lsite = Ls + sl * 72;
       auto links = [&](int p, int) -> const C* { return lsite + p * 9; };
       for (int r = rl; r < nrhs; r += rt)
-        wilson_site<T>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op, dir, disp, apbc, tvol, Lt);
+        wilson_site<T, decltype(links), DOTS>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op, dir,
+                                              disp, apbc, tvol, Lt, Ds);
+    }
+  }
+  if (DOTS) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < nrhs; k += blockDim.x) {
+      atomicAdd(&d1[k].x, Ds[3 * k]);
+      atomicAdd(&d1[k].y, Ds[3 * k + 1]);
+      atomicAdd(&d2[k].x, Ds[3 * k + 2]);
     }
   }
 }
@@ -456,6 +485,276 @@ __global__ void __launch_bounds__(512) wilson_quad_kernel(
 }
 
 // ---------------------------------------------------------------------------
+// Staged multi-RHS kernel.  A work item is a tile of TS consecutive sites and
+// a chunk of up to kChunk consecutive right-hand sides.  Every distinct
+// neighbour record the tile reads -- (site, chunk) is kChunk x 12 contiguous
+// complex numbers in the [V][nrhs][12] layout -- is brought into its own
+// shared-memory slot by one bulk copy (cp.async.bulk + an mbarrier
+// transaction count), together with the tile's hop links and clover blocks.
+// The spinor stencil then runs from shared memory: no global gathers.
+//
+// Slots and threads are laid out so that shared-memory reads are free of bank
+// conflicts: each slot is padded by 16 bytes (an odd number of 16-byte units)
+// and a quarter warp covers 2 sites x 4 RHS (FP32) or 4 sites x 2 RHS (FP64).
+// Two threads share a (site, RHS): h = 0 applies the forward hops and the
+// upper chiral clover block, h = 1 the backward hops and the lower block; each
+// owns two output spins and the halves meet once through shared memory.
+//
+// The host-built tile plan lists, per tile, the sites of its slots (the TS
+// tile sites first) and per (site, hop) the slot to read; a tile reads at most
+// 7 TS + 4 distinct records (TS own, 6 TS across y, z, t, and at most 4 x
+// halos where the tile starts or ends inside an x row).
+// Tiles are swept chunk by chunk, so the window of records a chunk's sweep
+// revisits (two time slices) stays small enough for L2.
+constexpr int kChunk = 8;
+
+template <class T> struct StageCfg;
+template <> struct StageCfg<float> { static constexpr int TS = 16; };
+template <> struct StageCfg<double> { static constexpr int TS = 8; };
+
+template <class T>
+struct StageGeo {
+  typedef typename wt<T>::C C;
+  static constexpr int TS = StageCfg<T>::TS;
+  static constexpr int SMAX = 7 * TS + 4;
+  static constexpr int SREC = kChunk * 12 * (int)sizeof(C) + 16;  // slot stride (bytes)
+  static constexpr int LREC = 72 * (int)sizeof(C) + 16;           // links / clover stride per site
+  static constexpr int XREC = sizeof(T) == 4 ? 48 : 112;          // half-spinor exchange stride
+  static constexpr int THREADS = TS * kChunk * 2;
+  static constexpr int OFF_SLOTTAB = 16;
+  static constexpr int OFF_SPIN = 16 + 128;
+  static constexpr int OFF_LINKS = OFF_SPIN + SMAX * SREC;
+  static constexpr int OFF_CLOV = OFF_LINKS + TS * LREC;
+  static constexpr int OFF_DOTS = OFF_CLOV + TS * LREC;
+  static_assert(TS * 8 <= 128, "slot table");
+  static_assert(2 * TS * kChunk * XREC <= SMAX * SREC, "exchange buffer");
+  static_assert((SREC / 16) % 2 == 1 && (LREC / 16) % 2 == 1, "odd 16-byte strides");
+};
+
+// lane -> (site within the warp's 4 sites, RHS within the chunk)
+template <class T>
+__device__ __forceinline__ void stage_lane(int lane, int& sw, int& r) {
+  const int qtr = lane >> 3, in = lane & 7;
+  if (sizeof(T) == 4) {
+    sw = ((qtr & 1) << 1) | (in >> 2);
+    r = ((qtr >> 1) << 2) | (in & 3);
+  } else {
+    sw = in >> 1;
+    r = (qtr << 1) | (in & 1);
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void load_spinor(typename wt<T>::C psi[12], const unsigned char* p) {
+  typedef typename wt<T>::C C;
+  if (sizeof(T) == 4) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const float4 v = q[k];
+      psi[2 * k] = C{(T)v.x, (T)v.y};
+      psi[2 * k + 1] = C{(T)v.z, (T)v.w};
+    }
+  } else {
+    const C* q = reinterpret_cast<const C*>(p);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) psi[k] = q[k];
+  }
+}
+
+template <class T, bool DOTS>
+__global__ void __launch_bounds__(StageGeo<T>::THREADS) wilson_stage_kernel(
+    const typename wt<T>::C* __restrict__ hop, const typename wt<T>::C* __restrict__ clover,
+    const int32_t* __restrict__ plan_ns, const int32_t* __restrict__ plan_site,
+    const uint8_t* __restrict__ plan_slot, const typename wt<T>::C* __restrict__ in,
+    typename wt<T>::C* __restrict__ out, int V, int nrhs, T diag, int op, int dir, int disp, int apbc, int tvol,
+    int Lt, double2* __restrict__ d1, double2* __restrict__ d2, int* __restrict__ err) {
+  typedef typename wt<T>::C C;
+  typedef StageGeo<T> G;
+  constexpr int TS = G::TS;
+  extern __shared__ __align__(16) unsigned char sm[];
+  const uint8_t* slottab = sm + G::OFF_SLOTTAB;
+  unsigned char* spin = sm + G::OFF_SPIN;
+  unsigned char* links = sm + G::OFF_LINKS;
+  unsigned char* clov = sm + G::OFF_CLOV;
+  double* Ds = reinterpret_cast<double*>(sm + G::OFF_DOTS);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
+  volatile int* ok_flag = reinterpret_cast<volatile int*>(sm + 8);
+
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int h = t / (TS * kChunk), u = t % (TS * kChunk);
+  int sw, rr;
+  stage_lane<T>(lane, sw, rr);
+  const int j = ((u >> 5) << 2) + sw;  // tile site of this thread
+  const bool g5 = (op == GMG_OP_MDAG);
+  const int ntiles = (V + TS - 1) / TS, nchunks = (nrhs + kChunk - 1) / kChunk;
+  const int64_t items = (int64_t)ntiles * nchunks;
+
+  if (t == 0) ac::mbar_init(bar, 1);
+  if (DOTS)
+    for (int k = t; k < 3 * nrhs; k += blockDim.x) Ds[k] = 0.0;
+  __syncthreads();
+
+  uint32_t phase = 0;
+  for (int64_t item = blockIdx.x; item < items; item += gridDim.x, phase ^= 1) {
+    const int chunk = (int)(item / ntiles), tile = (int)(item % ntiles);
+    const int s0 = tile * TS, nss = min(TS, V - s0);
+    const int r0 = chunk * kChunk, rc = min(kChunk, nrhs - r0);
+    // ---- stage: one bulk copy per slot, per site's links and clover, and the slot table
+    if (warp == 0) {
+      const int ns = plan_ns[tile];
+      const uint32_t rbytes = (uint32_t)(rc * 12 * sizeof(C));
+      if (lane == 0)
+        ac::mbar_expect_tx(bar, ns * rbytes + 2u * nss * 72u * (uint32_t)sizeof(C) + TS * 8u);
+      for (int k = lane; k < ns; k += 32) {
+        const int site = plan_site[(int64_t)tile * G::SMAX + k];
+        ac::bulk_g2s(spin + k * G::SREC, in + ((int64_t)site * nrhs + r0) * 12, rbytes, bar);
+      }
+      for (int k = lane; k < nss; k += 32) {
+        ac::bulk_g2s(links + k * G::LREC, hop + (int64_t)(s0 + k) * 72, 72 * sizeof(C), bar);
+        ac::bulk_g2s(clov + k * G::LREC, clover + (int64_t)(s0 + k) * 72, 72 * sizeof(C), bar);
+      }
+      if (lane == 0) ac::bulk_g2s(sm + G::OFF_SLOTTAB, plan_slot + (int64_t)tile * TS * 8, TS * 8, bar);
+    }
+    if (t == 0) *ok_flag = ac::mbar_wait(bar, phase) ? 1 : 0;
+    __syncthreads();
+    if (!*ok_flag) {
+      // the copies did not land in time: record it, give our own copies a
+      // second bounded wait, and leave (every thread takes this branch)
+      if (t == 0) {
+        atomicCAS(err, 0, 1);
+        ac::mbar_wait(bar, phase);
+      }
+      return;
+    }
+    ac::mbar_try_wait(bar, phase);  // completed: acquire the copied bytes in every thread
+
+    const bool valid = j < nss && rr < rc;
+    C acc[4][3];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc[s][c] = C{0, 0};
+    C cin[6];
+    if (valid) {
+      const int site = s0 + j;
+      if (op != GMG_OP_MDIR) {
+        C psi[12];
+        load_spinor<T>(psi, spin + j * G::SREC + rr * 12 * sizeof(C));
+#pragma unroll
+        for (int k = 0; k < 6; ++k) cin[k] = h ? psi[6 + k] : psi[k];
+        if (g5) {
+#pragma unroll
+          for (int k = 6; k < 12; ++k) psi[k] = C{-psi[k].x, -psi[k].y};
+        }
+        // own chiral block: rows 6h .. 6h + 5 = spins 2h, 2h + 1
+        const C* cl = reinterpret_cast<const C*>(clov + j * G::LREC) + h * 36;
+#pragma unroll
+        for (int a = 0; a < 6; ++a) {
+          C v;
+          const C pa = h ? psi[6 + a] : psi[a];
+          v.x = diag * pa.x;
+          v.y = diag * pa.y;
+#pragma unroll
+          for (int b = 0; b < 6; ++b) v = cadd(v, cmul(cl[a * 6 + b], h ? psi[6 + b] : psi[b]));
+          if (h)
+            acc[2 + a / 3][a % 3] = v;
+          else
+            acc[a / 3][a % 3] = v;
+        }
+      }
+      if (op != GMG_OP_MDIAG) {
+        const int tc = site / tvol;
+        const C* Ls = reinterpret_cast<const C*>(links + j * G::LREC);
+        if (h == 0) {
+#pragma unroll
+          for (int mu = 0; mu < 4; ++mu) {
+            if (op == GMG_OP_MDIR && (mu != dir || disp != 1)) continue;
+            C psi[12];
+            load_spinor<T>(psi, spin + slottab[j * 8 + mu] * G::SREC + rr * 12 * sizeof(C));
+            if (g5) {
+#pragma unroll
+              for (int k = 6; k < 12; ++k) psi[k] = C{-psi[k].x, -psi[k].y};
+            }
+            const T coef = (apbc && mu == 3 && tc == Lt - 1) ? (T)0.5 : (T)-0.5;
+            wilson_hop<T>(acc, Ls + mu * 9, false, psi, mu, 1, coef);
+          }
+        } else {
+#pragma unroll
+          for (int mu = 0; mu < 4; ++mu) {
+            if (op == GMG_OP_MDIR && (mu != dir || disp != -1)) continue;
+            C psi[12];
+            load_spinor<T>(psi, spin + slottab[j * 8 + 4 + mu] * G::SREC + rr * 12 * sizeof(C));
+            if (g5) {
+#pragma unroll
+              for (int k = 6; k < 12; ++k) psi[k] = C{-psi[k].x, -psi[k].y};
+            }
+            const T coef = (apbc && mu == 3 && tc == 0) ? (T)0.5 : (T)-0.5;
+            wilson_hop<T>(acc, Ls + (4 + mu) * 9, true, psi, mu, -1, coef);
+          }
+        }
+      }
+    }
+    // ---- exchange the halves: each thread hands its partner the two spins it does not own
+    __syncthreads();  // every thread is done with the staged slots
+    {
+      C* xo = reinterpret_cast<C*>(spin + (h * TS * kChunk + u) * G::XREC);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) xo[k] = h ? acc[k / 3][k % 3] : acc[2 + k / 3][k % 3];
+    }
+    __syncthreads();
+    if (valid) {
+      const C* xi = reinterpret_cast<const C*>(spin + ((1 - h) * TS * kChunk + u) * G::XREC);
+      C o[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        o[k] = cadd(h ? acc[2 + k / 3][k % 3] : acc[k / 3][k % 3], xi[k]);
+        if (g5 && h) o[k] = C{-o[k].x, -o[k].y};
+      }
+      C* dst = out + ((int64_t)(s0 + j) * nrhs + r0 + rr) * 12 + 6 * h;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) dst[k] = o[k];
+      if (DOTS) {
+        double pr = 0.0, pi = 0.0, pn = 0.0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          const double vx = o[k].x, vy = o[k].y, ix = cin[k].x, iy = cin[k].y;
+          pr += vx * ix + vy * iy;
+          pi += vx * iy - vy * ix;
+          pn += vx * vx + vy * vy;
+        }
+        atomicAdd(&Ds[3 * (r0 + rr)], pr);
+        atomicAdd(&Ds[3 * (r0 + rr) + 1], pi);
+        atomicAdd(&Ds[3 * (r0 + rr) + 2], pn);
+      }
+    }
+    // the next item's bulk copies overwrite what this item wrote and read
+    ac::fence_proxy_async_smem();
+    __syncthreads();
+  }
+  if (DOTS) {
+    __syncthreads();
+    for (int k = t; k < nrhs; k += blockDim.x) {
+      atomicAdd(&d1[k].x, Ds[3 * k]);
+      atomicAdd(&d1[k].y, Ds[3 * k + 1]);
+      atomicAdd(&d2[k].x, Ds[3 * k + 2]);
+    }
+  }
+}
+
+// hop links: hop[x][p] = p < 4 ? U_p(x) : U_{p-4}(x - p)
+template <class C>
+__global__ void hop_links_kernel(const C* __restrict__ gauge, const int32_t* __restrict__ nbr, C* __restrict__ hop,
+                                 int V) {
+  const int64_t n = (int64_t)V * 72;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int site = (int)(e / 72), k = (int)(e % 72), p = k / 9, m = k % 9;
+    const int src = p < 4 ? site : nbr[(int64_t)p * V + site];
+    hop[e] = gauge[((int64_t)src * 4 + (p & 3)) * 9 + m];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // clover term from the gauge field (thread per site)
 // ---------------------------------------------------------------------------
 struct M3 { double2 m[3][3]; };
@@ -575,6 +874,137 @@ gmg_status wilson_build_clover(gmg_wilson* h, cudaStream_t s) {
   d2f_wilson<<<std::min((V * 36 + 255) / 256, 148 * 64), 256, 0, s>>>(h->gauge.as<double2>(),
                                                                        h->gauge_f.as<float2>(), (int64_t)V * 36);
   GMG_CUDA(cudaGetLastError());
+  GMG_TRY(h->hop.alloc(sizeof(double2) * 72 * (size_t)V));
+  GMG_TRY(h->hop_f.alloc(sizeof(float2) * 72 * (size_t)V));
+  const int g = (int)std::min<int64_t>(((int64_t)V * 72 + 255) / 256, 148 * 64);
+  hop_links_kernel<double2><<<g, 256, 0, s>>>(h->gauge.as<double2>(), h->nbr.as<int32_t>(), h->hop.as<double2>(), V);
+  hop_links_kernel<float2><<<g, 256, 0, s>>>(h->gauge_f.as<float2>(), h->nbr.as<int32_t>(), h->hop_f.as<float2>(), V);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+// Tile plan for TS-site tiles: [ntiles] slot counts, [ntiles][7 TS + 4] slot
+// sites (the tile's own sites first), [ntiles][TS][8] slot of each hop.
+// Every out-of-tile neighbour gets its own slot; the count bound 7 TS + 4
+// holds for every lattice (see the staged kernel), and is checked here.
+struct PlanView {
+  const int32_t* ns;
+  const int32_t* site;
+  const uint8_t* slot;
+};
+
+static size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+static PlanView plan_view(const DevBuf& b, int ntiles, int TS) {
+  const int smax = 7 * TS + 4;
+  const unsigned char* p = b.as<unsigned char>();
+  const size_t o1 = align16(sizeof(int32_t) * ntiles);
+  const size_t o2 = o1 + align16(sizeof(int32_t) * (size_t)ntiles * smax);
+  return PlanView{reinterpret_cast<const int32_t*>(p), reinterpret_cast<const int32_t*>(p + o1),
+                  reinterpret_cast<const uint8_t*>(p + o2)};
+}
+
+static gmg_status build_plan(gmg_wilson* h, int which, cudaStream_t s) {
+  if (h->plan_ok[which] >= 0) return GMG_OK;
+  const int TS = which ? 16 : 8, smax = 7 * TS + 4;
+  const int64_t V = h->dims.vol();
+  const int ntiles = (int)((V + TS - 1) / TS);
+  std::vector<int32_t> nbr(9 * V);
+  host_neighbors(h->dims, nbr.data());
+  const size_t o1 = align16(sizeof(int32_t) * ntiles);
+  const size_t o2 = o1 + align16(sizeof(int32_t) * (size_t)ntiles * smax);
+  const size_t bytes = o2 + (size_t)ntiles * TS * 8;
+  std::vector<unsigned char> host(bytes, 0);
+  int32_t* ns = reinterpret_cast<int32_t*>(host.data());
+  int32_t* site = reinterpret_cast<int32_t*>(host.data() + o1);
+  uint8_t* slot = host.data() + o2;
+  bool ok = true;
+  for (int tile = 0; tile < ntiles && ok; ++tile) {
+    const int64_t s0 = (int64_t)tile * TS;
+    const int nss = (int)std::min<int64_t>(TS, V - s0);
+    int32_t* st = site + (size_t)tile * smax;
+    uint8_t* sl = slot + (size_t)tile * TS * 8;
+    int n = nss;
+    for (int j = 0; j < nss; ++j) st[j] = (int32_t)(s0 + j);
+    for (int p = 0; p < 8 && ok; ++p)
+      for (int j = 0; j < nss; ++j) {
+        const int32_t nb = nbr[(size_t)p * V + s0 + j];
+        if (nb >= s0 && nb < s0 + nss) {
+          sl[j * 8 + p] = (uint8_t)(nb - s0);
+        } else if (n < smax) {
+          st[n] = nb;
+          sl[j * 8 + p] = (uint8_t)n;
+          ++n;
+        } else {
+          ok = false;
+          break;
+        }
+      }
+    ns[tile] = n;
+  }
+  if (!ok) {
+    h->plan_ok[which] = 0;
+    return GMG_OK;
+  }
+  GMG_TRY(h->plan[which].alloc(bytes));
+  GMG_CUDA(cudaMemcpyAsync(h->plan[which].p, host.data(), bytes, cudaMemcpyHostToDevice, s));
+  GMG_CUDA(cudaStreamSynchronize(s));  // host goes out of scope
+  h->plan_ok[which] = 1;
+  return GMG_OK;
+}
+
+template <class T, bool DOTS>
+static size_t stage_smem(int nrhs) {
+  return (size_t)StageGeo<T>::OFF_DOTS + (DOTS ? sizeof(double) * 3 * (size_t)nrhs : 0);
+}
+
+// staged kernel launch; *launched = false when the staged path does not apply
+// (no plan for this lattice, unaligned fields, or too little shared memory)
+template <bool DOTS>
+static gmg_status launch_stage(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs, const void* in,
+                               void* out, double2* d1, double2* d2, cudaStream_t s, bool* launched) {
+  *launched = false;
+  if (((uintptr_t)in | (uintptr_t)out) & 15) return GMG_OK;
+  const bool f32 = vec_prec == GMG_F32;
+  if (!f32 && vec_prec != GMG_F64) return GMG_OK;
+  const int which = f32 ? 1 : 0, TS = f32 ? StageGeo<float>::TS : StageGeo<double>::TS;
+  GMG_TRY(build_plan(h, which, s));
+  if (h->plan_ok[which] != 1) return GMG_OK;
+  const size_t smem = f32 ? stage_smem<float, DOTS>(nrhs) : stage_smem<double, DOTS>(nrhs);
+  if (smem > 200 * 1024) return GMG_OK;
+  if (!h->dev_err.p) {
+    GMG_TRY(h->dev_err.alloc(256));
+    GMG_CUDA(cudaMemsetAsync(h->dev_err.p, 0, 256, s));
+  }
+  const int V = (int)h->dims.vol();
+  const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
+  const int ntiles = (V + TS - 1) / TS;
+  const int64_t items = (int64_t)ntiles * ((nrhs + kChunk - 1) / kChunk);
+  const PlanView pv = plan_view(h->plan[which], ntiles, TS);
+  int dev = 0, nsm = 148, occ = 1;
+  GMG_CUDA(cudaGetDevice(&dev));
+  GMG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  if (f32) {
+    auto k = wilson_stage_kernel<float, DOTS>;
+    GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, StageGeo<float>::THREADS, smem));
+    const int g = (int)std::min<int64_t>(items, (int64_t)nsm * std::max(occ, 1));
+    k<<<g, StageGeo<float>::THREADS, smem, s>>>(h->hop_f.as<float2>(), h->clover_f.as<float2>(), pv.ns, pv.site,
+                                                 pv.slot, (const float2*)in, (float2*)out, V, nrhs,
+                                                 (float)(4.0 + h->mass), op, dir, disp, h->apbc, tvol, h->dims.d[3],
+                                                 d1, d2, h->dev_err.as<int>());
+  } else {
+    auto k = wilson_stage_kernel<double, DOTS>;
+    GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, StageGeo<double>::THREADS, smem));
+    const int g = (int)std::min<int64_t>(items, (int64_t)nsm * std::max(occ, 1));
+    k<<<g, StageGeo<double>::THREADS, smem, s>>>(h->hop.as<double2>(), h->clover.as<double2>(), pv.ns, pv.site,
+                                                  pv.slot, (const double2*)in, (double2*)out, V, nrhs, 4.0 + h->mass,
+                                                  op, dir, disp, h->apbc, tvol, h->dims.d[3], d1, d2,
+                                                  h->dev_err.as<int>());
+  }
+  GMG_CUDA(cudaGetLastError());
+  *launched = true;
   return GMG_OK;
 }
 
@@ -619,14 +1049,13 @@ static gmg_status launch_quad(gmg_wilson* h, int op, int dir, int disp, int vec_
   return GMG_OK;
 }
 
-gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs,
-                        const void* in, void* out, cudaStream_t s) {
+// thread per (site, RHS), links and clover from global memory
+static gmg_status launch_site(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs, const void* in,
+                              void* out, cudaStream_t s) {
   const int V = (int)h->dims.vol();
   const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
   const int64_t total = (int64_t)V * nrhs;
   const int grid = (int)std::min<int64_t>((total + 127) / 128, 148 * 32);
-  KernelTimer kt("wilson", s);
-  if (nrhs >= 4) return launch_quad<false>(h, op, dir, disp, vec_prec, nrhs, in, out, nullptr, nullptr, s);
   if (vec_prec == GMG_F64) {
     wilson_kernel<double><<<grid, 128, 0, s>>>(h->gauge.as<double2>(), h->clover.as<double2>(),
                                                 h->nbr.as<int32_t>(), (const double2*)in, (double2*)out, V,
@@ -644,14 +1073,152 @@ gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, 
   return GMG_OK;
 }
 
+// tile kernel: kTileSites sites x min(nrhs, 16) threads per CTA
+template <bool DOTS>
+static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs, const void* in,
+                              void* out, double2* d1, double2* d2, cudaStream_t s) {
+  const int V = (int)h->dims.vol();
+  const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
+  const int rt = std::min(nrhs, 16);
+  const int tiles = (V + kTileSites - 1) / kTileSites;
+  const int g = std::min(tiles, 148 * 16);
+  const size_t dots = DOTS ? sizeof(double) * 3 * (size_t)nrhs : 0;
+  if (vec_prec == GMG_F64) {
+    const size_t smem = sizeof(double2) * 2 * kTileSites * 72 + dots;
+    if (smem > 48 * 1024)
+      GMG_CUDA(cudaFuncSetAttribute(wilson_tile_kernel<double, DOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+    wilson_tile_kernel<double, DOTS><<<g, kTileSites * rt, smem, s>>>(
+        h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(), (const double2*)in, (double2*)out, V,
+        nrhs, rt, 4.0 + h->mass, op, dir, disp, h->apbc, tvol, h->dims.d[3], d1, d2);
+  } else if (vec_prec == GMG_F32) {
+    const size_t smem = sizeof(float2) * 2 * kTileSites * 72 + dots;
+    if (smem > 48 * 1024)
+      GMG_CUDA(cudaFuncSetAttribute(wilson_tile_kernel<float, DOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+    wilson_tile_kernel<float, DOTS><<<g, kTileSites * rt, smem, s>>>(
+        h->hop_f.as<float2>(), h->clover_f.as<float2>(), h->nbr.as<int32_t>(), (const float2*)in, (float2*)out, V,
+        nrhs, rt, (float)(4.0 + h->mass), op, dir, disp, h->apbc, tvol, h->dims.d[3], d1, d2);
+  } else {
+    return fail(GMG_ERR_UNSUPPORTED, "wilson apply: vectors must be F64 or F32");
+  }
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+// One launch of kernel variant v; *launched = false when v does not apply.
+static gmg_status run_variant(gmg_wilson* h, int v, bool dots, int op, int dir, int disp, int vec_prec, int nrhs,
+                              const void* in, void* out, double2* d1, double2* d2, cudaStream_t s, bool* launched) {
+  *launched = true;
+  switch (v) {
+    case GMG_WILSON_SITE:
+      if (dots) break;
+      return launch_site(h, op, dir, disp, vec_prec, nrhs, in, out, s);
+    case GMG_WILSON_TILE:
+      return dots ? launch_tile<true>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s)
+                  : launch_tile<false>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s);
+    case GMG_WILSON_QUAD:
+      return dots ? launch_quad<true>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s)
+                  : launch_quad<false>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s);
+    case GMG_WILSON_STAGED:
+      return dots ? launch_stage<true>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, launched)
+                  : launch_stage<false>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, launched);
+    default:
+      break;
+  }
+  *launched = false;
+  return GMG_OK;
+}
+
+// Autotuned dispatch.  The kernel variant is chosen per (vector precision,
+// fused products or not, single-hop op or not, nrhs class) by timing every
+// applicable variant once on the call that first meets the key (CUDA events
+// on the caller's stream; not while the stream is being captured) and is
+// cached in the handle.  The nrhs classes (1-3, 4-7, 8-15, 16-31, 32+) keep a
+// batch that shrinks as right-hand sides converge from re-tuning at every size.
+static gmg_status wilson_dispatch(gmg_wilson* h, bool dots, int op, int dir, int disp, int vec_prec, int nrhs,
+                                  const void* in, void* out, double2* d1, double2* d2, cudaStream_t s) {
+  auto zero_dots = [&]() -> gmg_status {
+    if (dots) {
+      GMG_CUDA(cudaMemsetAsync(d1, 0, sizeof(double2) * nrhs, s));
+      GMG_CUDA(cudaMemsetAsync(d2, 0, sizeof(double2) * nrhs, s));
+    }
+    return GMG_OK;
+  };
+  bool launched = false;
+  if (h->wforce >= 0) {
+    GMG_TRY(zero_dots());
+    GMG_TRY(run_variant(h, h->wforce, dots, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, &launched));
+    if (launched) return GMG_OK;
+    // a forced variant that does not apply falls through to the tuned choice
+  }
+  const int cls = nrhs < 4 ? 0 : nrhs < 8 ? 1 : nrhs < 16 ? 2 : nrhs < 32 ? 3 : 4;
+  const uint64_t key = (uint64_t)vec_prec | ((uint64_t)dots << 4) | ((uint64_t)(op == GMG_OP_MDIR) << 5) |
+                       ((uint64_t)cls << 8);
+  auto it = h->wtune.find(key);
+  if (it != h->wtune.end()) {
+    GMG_TRY(zero_dots());
+    GMG_TRY(run_variant(h, it->second, dots, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, &launched));
+    if (launched) return GMG_OK;
+  }
+  std::vector<int> cand;
+  if (!dots && nrhs < 4) cand.push_back(GMG_WILSON_SITE);
+  cand.push_back(GMG_WILSON_TILE);
+  cand.push_back(GMG_WILSON_QUAD);
+  if (nrhs >= 4) cand.push_back(GMG_WILSON_STAGED);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  GMG_CUDA(cudaStreamIsCapturing(s, &cap));
+  int best = nrhs >= 4 ? GMG_WILSON_TILE : (dots ? GMG_WILSON_QUAD : GMG_WILSON_SITE);
+  if (cap == cudaStreamCaptureStatusNone) {
+    cudaEvent_t e0, e1;
+    GMG_CUDA(cudaEventCreate(&e0));
+    GMG_CUDA(cudaEventCreate(&e1));
+    float best_ms = 1e30f;
+    gmg_status st = GMG_OK;
+    for (int v : cand) {
+      bool ok = false;
+      st = run_variant(h, v, dots, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, &ok);  // warm-up
+      if (st != GMG_OK) break;
+      if (!ok) continue;
+      if (cudaEventRecord(e0, s) != cudaSuccess) break;
+      for (int k = 0; k < 2 && st == GMG_OK; ++k)
+        st = run_variant(h, v, dots, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, &ok);
+      if (st != GMG_OK || cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = v;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    GMG_TRY(st);
+    GMG_CUDA(cudaGetLastError());
+    h->wtune[key] = best;
+  }
+  GMG_TRY(zero_dots());
+  GMG_TRY(run_variant(h, best, dots, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, &launched));
+  if (!launched) return fail(GMG_ERR_UNSUPPORTED, "wilson apply: no kernel variant applies");
+  return GMG_OK;
+}
+
+gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs,
+                        const void* in, void* out, cudaStream_t s) {
+  if (vec_prec != GMG_F64 && vec_prec != GMG_F32)
+    return fail(GMG_ERR_UNSUPPORTED, "wilson apply: vectors must be F64 or F32");
+  KernelTimer kt("wilson", s);
+  return wilson_dispatch(h, false, op, dir, disp, vec_prec, nrhs, in, out, nullptr, nullptr, s);
+}
+
 // out = M in, and the minimal-residual inner products d1[r] = <out, in>,
 // d2[r].x = <out, out> (d1, d2: nrhs entries each, zeroed here)
 gmg_status wilson_apply_mr(gmg_wilson* h, int vec_prec, int nrhs, const void* in, void* out, double2* d1,
                            double2* d2, cudaStream_t s) {
+  if (vec_prec != GMG_F64 && vec_prec != GMG_F32)
+    return fail(GMG_ERR_UNSUPPORTED, "wilson apply: vectors must be F64 or F32");
   KernelTimer kt("wilson", s);
-  GMG_CUDA(cudaMemsetAsync(d1, 0, sizeof(double2) * nrhs, s));
-  GMG_CUDA(cudaMemsetAsync(d2, 0, sizeof(double2) * nrhs, s));
-  return launch_quad<true>(h, GMG_OP_M, 0, 0, vec_prec, nrhs, in, out, d1, d2, s);
+  return wilson_dispatch(h, true, GMG_OP_M, 0, 0, vec_prec, nrhs, in, out, d1, d2, s);
 }
 
 }  // namespace gmg

@@ -356,6 +356,23 @@ class WilsonClover:
     def Mdir(self, inp, out, d, disp):
         return self.apply(OP_MDIR, inp, out, d, disp)
 
+    KERNELS = {"auto": -1, "site": 0, "tile": 1, "quad": 2, "staged": 3}
+
+    def set_kernel(self, name):
+        """Force a kernel variant ("site", "tile", "quad", "staged") or "auto"."""
+        _chk(lib().gmg_wilson_set_kernel(self._h, self.KERNELS[name]))
+
+    def tuned_kernel(self, prec, nrhs, fused_mr=False, single_hop=False):
+        k = ctypes.c_int()
+        _chk(lib().gmg_wilson_tuned_kernel(self._h, PREC[prec], nrhs, int(fused_mr), int(single_hop),
+                                           ctypes.byref(k)))
+        return {v: n for n, v in self.KERNELS.items()}[k.value]
+
+    def device_error(self):
+        code = ctypes.c_int()
+        st = lib().gmg_wilson_device_error(self._h, ctypes.byref(code))
+        return st, code.value
+
     def M_mr(self, inp, out):
         """out = M inp and the MR-step inner products <out, inp>, <out, out> per RHS."""
         _check_vec(inp, self.V, 12, "in")

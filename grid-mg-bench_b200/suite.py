@@ -159,14 +159,20 @@ def wilson_and_c4(T, hbm):
         for dt, cb in ((torch.complex128, 16), (torch.complex64, 8)):
             x = inputs.torch_gaussian((V, R, 12), 702, dtype=dt)
             y = torch.zeros_like(x)
-            t = T.run(lambda: w.M(x, y), reps=5)
             byts = V * (2 * 12 * R + 36 + 72) * cb  # in + out per RHS, gauge + clover once
-            res[f"R{R}_{'f64' if cb == 16 else 'f32'}"] = {
+            prec = "f64" if cb == 16 else "f32"
+            per = {}
+            for variant in (("site", "tile", "quad") if R < 4 else ("tile", "quad", "staged")):
+                w.set_kernel(variant)
+                per[variant] = round(T.run(lambda: w.M(x, y), reps=5) * 1e3, 3)
+            w.set_kernel("auto")
+            t = T.run(lambda: w.M(x, y), reps=5)
+            res[f"R{R}_{prec}"] = {
                 "ms": t * 1e3, "gflops": 1824.0 * V * R / t / 1e9, "gbs": byts / t / 1e9,
-                "frac_hbm": byts / t / 1e9 / hbm}
+                "frac_hbm": byts / t / 1e9 / hbm, "tuned": w.tuned_kernel(prec, R), "ms_per_variant": per}
             del x, y
     line("W fine Wilson-clover M (32^4)", results=res,
-         note="flops: 1824 per site per RHS (reference model); bytes: spinor in+out per RHS, gauge 36 + clover 72 complex per site")
+         note="flops: 1824 per site per RHS (reference model); bytes: spinor in+out per RHS, gauge 36 + clover 72 complex per site; 'tuned' is the autotuner's pick")
     # C4: CoarsenOperator 32^4 -> 8^4, nbasis 40, then 8^4 -> 4^4
     N = 40
     half = inputs.torch_gaussian((N // 2, V, 12), 703)

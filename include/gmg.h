@@ -234,6 +234,29 @@ gmg_status gmg_wilson_apply(gmg_wilson* h, gmg_op op, int dir, int disp, gmg_pre
    smoother step (the smoother solve of include/MultigridPreconditioner.h:
    264-301): d1[r] = <out_r, in_r>,
    d2[r] = <out_r, out_r> + 0i, device arrays of nrhs complex128. */
+/* Kernel variants of the multi-RHS Wilson-clover apply.  By default the
+   variant is autotuned: every applicable one is timed once per (vector
+   precision, fused MR products or not, single-hop op or not, nrhs class) on
+   the first call that meets the key, and the fastest is kept in the handle.
+   gmg_wilson_set_kernel forces one (GMG_WILSON_AUTO restores tuning); a forced
+   variant that does not apply to a call falls back to the tuned choice. */
+typedef enum {
+  GMG_WILSON_AUTO = -1,
+  GMG_WILSON_SITE = 0,    /* thread per (site, RHS), operands from global memory */
+  GMG_WILSON_TILE = 1,    /* 16-site tiles, links and clover staged in shared memory */
+  GMG_WILSON_QUAD = 2,    /* four lanes per (site, RHS), one per spin, quad shuffles */
+  GMG_WILSON_STAGED = 3   /* neighbour records bulk-copied into shared memory per tile and RHS chunk */
+} gmg_wilson_kernel;
+gmg_status gmg_wilson_set_kernel(gmg_wilson* h, gmg_wilson_kernel k);
+/* The variant the tuner chose for a key, or GMG_WILSON_AUTO when not tuned yet. */
+gmg_status gmg_wilson_tuned_kernel(gmg_wilson* h, gmg_prec vec_prec, int nrhs, int fused_mr, int single_hop,
+                                   gmg_wilson_kernel* k);
+
+/* Device error word of this handle's staged (bulk-copy) kernels: 0, or 1 when
+   a kernel gave up waiting for its copies; read after a device
+   synchronisation and then cleared.  Returns GMG_ERR_TIMEOUT when *code != 0.
+   No counterpart in the reference. */
+gmg_status gmg_wilson_device_error(gmg_wilson* h, int* code);
 gmg_status gmg_wilson_apply_mr(gmg_wilson* h, gmg_prec vec_prec, int nrhs, const void* in, void* out,
                                double* d1, double* d2, gmg_stream s);
 

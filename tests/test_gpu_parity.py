@@ -269,12 +269,25 @@ def test_wilson_ops_f64(wil, op):
     assert orc.rel_dev_sq(ref, host(out)) < TOL64
 
 
+@pytest.fixture
+def forced(wil):
+    """Force a Wilson kernel variant for one test, back to autotuning after it."""
+    w = wil[3]
+    yield w.set_kernel
+    w.set_kernel("auto")
+
+
+VARIANTS = ["site", "tile", "quad", "staged"]
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("nrhs", [4, 7, 12, 13, 20])
 @pytest.mark.parametrize("op", ["M", "Mdag", "Mdiag"])
-def test_wilson_multi_rhs_tile(wil, nrhs, op):
-    # nrhs >= 4 runs the quad kernel: 16 sites per tile, 4 spin lanes per (site, RHS),
-    # rt = largest divisor of nrhs up to 8 RHS per pass (13 -> 1, 7 -> 7, 20 -> 5)
+def test_wilson_multi_rhs_variants(wil, forced, variant, nrhs, op):
+    # tile: 16 sites x min(nrhs, 16) threads; quad: rt = largest divisor of nrhs
+    # up to 8 (13 -> 1, 7 -> 7, 20 -> 5); staged: chunks of 8 RHS (12 -> 8 + 4)
     dims, U, cl, w = wil
+    forced(variant)
     x = inputs.gaussian_field((512, nrhs, 12), inputs.rng(stream=124 + nrhs))
     code = {"M": orc.OP_M, "Mdag": orc.OP_MDAG, "Mdiag": orc.OP_MDIAG}[op]
     ref = orc.wilson_clover(dims, U, cl, -0.1, 1, x, code)
@@ -284,6 +297,16 @@ def test_wilson_multi_rhs_tile(wil, nrhs, op):
     out32 = torch.zeros((512, nrhs, 12), dtype=torch.complex64, device=DEV)
     getattr(w, op)(dev(x, torch.complex64), out32)
     assert orc.rel_dev_sq(ref, host(out32)) < TOL32
+
+
+def test_wilson_autotuner_records_a_choice(wil):
+    dims, U, cl, w = wil
+    x = dev(inputs.gaussian_field((512, 12, 12), inputs.rng(stream=171)), torch.complex64)
+    out = torch.zeros_like(x)
+    w.M(x, out)
+    assert w.tuned_kernel("f32", 12) in ("site", "tile", "quad", "staged")
+    ref = orc.wilson_clover(dims, U, cl, -0.1, 1, host(x).astype(np.complex128), orc.OP_M)
+    assert orc.rel_dev_sq(ref, host(out)) < TOL32
 
 
 def test_wilson_mdir_f64_and_f32(wil):
@@ -301,9 +324,34 @@ def test_wilson_mdir_f64_and_f32(wil):
     assert orc.rel_dev_sq(ref, host(out)) < TOL32
 
 
-def test_wilson_multi_rhs_mdir(wil):
-    # the quad kernel's single-hop form (CoarsenOperator's Mdir calls, nrhs >= 4)
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("dims,nrhs", [((6, 4, 2, 4), 9), ((2, 2, 2, 2), 4), ((10, 2, 2, 2), 16)])
+def test_wilson_odd_lattices(dims, nrhs, variant):
+    # tiles that start and end inside x rows (x halos), lattices of extent 2
+    # (both hops of a direction reach the same site), a partial last RHS chunk
+    V = int(np.prod(dims))
+    U = inputs.hot_gauge(dims, inputs.rng(stream=161))
+    w = gmg.WilsonClover(dims, -0.2, 1.0, antiperiodic=True)
+    w.set_gauge(U)
+    w.set_kernel(variant)
+    cl = orc.clover_build(dims, U, 1.0)
+    x = inputs.gaussian_field((V, nrhs, 12), inputs.rng(stream=162))
+    for op, code in (("M", orc.OP_M), ("Mdag", orc.OP_MDAG)):
+        ref = orc.wilson_clover(dims, U, cl, -0.2, 1, x, code)
+        out = torch.zeros((V, nrhs, 12), dtype=torch.complex128, device=DEV)
+        getattr(w, op)(dev(x), out)
+        assert orc.rel_dev_sq(ref, host(out)) < TOL64, op
+        out32 = torch.zeros((V, nrhs, 12), dtype=torch.complex64, device=DEV)
+        getattr(w, op)(dev(x, torch.complex64), out32)
+        assert orc.rel_dev_sq(ref, host(out32)) < TOL32, op
+    assert w.device_error() == (0, 0)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_wilson_multi_rhs_mdir(wil, forced, variant):
+    # the single-hop form (CoarsenOperator's Mdir calls, nrhs >= 4) of every variant
     dims, U, cl, w = wil
+    forced(variant)
     x = inputs.gaussian_field((512, 6, 12), inputs.rng(stream=141))
     for d in range(4):
         for disp in (1, -1):
@@ -316,10 +364,13 @@ def test_wilson_multi_rhs_mdir(wil):
             assert orc.rel_dev_sq(ref, host(out32)) < TOL32, (d, disp)
 
 
+@pytest.mark.parametrize("variant", ["tile", "quad", "staged"])
 @pytest.mark.parametrize("nrhs", [1, 3, 12])
-def test_wilson_apply_mr_products(wil, nrhs):
+def test_wilson_apply_mr_products(wil, forced, variant, nrhs):
     # M with the minimal-residual inner products formed in the kernel's epilogue
+    # (staged needs nrhs >= 4 and falls back to the tuned choice below that)
     dims, U, cl, w = wil
+    forced(variant)
     x = inputs.gaussian_field((512, nrhs, 12), inputs.rng(stream=150 + nrhs))
     ref = orc.wilson_clover(dims, U, cl, -0.1, 1, x, orc.OP_M)
     d1_ref = np.einsum("srk,srk->r", ref.conj(), x)
