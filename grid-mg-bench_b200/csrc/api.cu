@@ -408,7 +408,9 @@ gmg_status gmg_wilson_tuned_kernel(gmg_wilson* h, gmg_prec vec_prec, int nrhs, i
   const uint64_t key = (uint64_t)vec_prec | ((uint64_t)(fused_mr != 0) << 4) | ((uint64_t)(single_hop != 0) << 5) |
                        ((uint64_t)cls << 8);
   auto it = h->wtune.find(key);
-  *k = it == h->wtune.end() ? GMG_WILSON_AUTO : (gmg_wilson_kernel)it->second;
+  // internal register-budget sub-variants (ids >= 16) of the tile kernel report as TILE
+  *k = it == h->wtune.end() ? GMG_WILSON_AUTO
+                            : (gmg_wilson_kernel)(it->second >= 16 ? (int)GMG_WILSON_TILE : it->second);
   return GMG_OK;
 }
 

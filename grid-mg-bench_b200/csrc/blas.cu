@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(1024) mr_update_row_kernel(const double2* __re
                                                              typename C2<T>::t* __restrict__ x,
                                                              typename C2<T>::t* __restrict__ rr_,
                                                              const typename C2<T>::t* __restrict__ Ar, int64_t V, int R,
-                                                             int dof, int spb) {
+                                                             int dof, int spb, bool update_r) {
   const int RD = R * dof, t = threadIdx.x;
   if (t >= spb * RD) return;
   const int so = t / RD, i = t % RD, k = i / dof;
@@ -275,11 +275,14 @@ __global__ void __launch_bounds__(1024) mr_update_row_kernel(const double2* __re
   const double ar = den > 0.0 ? d1[k].x / den : 0.0, ai = den > 0.0 ? d1[k].y / den : 0.0;
   for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
     const int64_t e = s * RD + i;
-    const double rr = rr_[e].x, ri = rr_[e].y, qr = Ar[e].x, qi = Ar[e].y;
+    const double rr = rr_[e].x, ri = rr_[e].y;
     x[e].x = (T)(x[e].x + ar * rr - ai * ri);
     x[e].y = (T)(x[e].y + ar * ri + ai * rr);
-    rr_[e].x = (T)(rr - (ar * qr - ai * qi));
-    rr_[e].y = (T)(ri - (ar * qi + ai * qr));
+    if (update_r) {
+      const double qr = Ar[e].x, qi = Ar[e].y;
+      rr_[e].x = (T)(rr - (ar * qr - ai * qi));
+      rr_[e].y = (T)(ri - (ar * qi + ai * qr));
+    }
   }
 }
 
@@ -473,17 +476,20 @@ __global__ void scale_inv_norm_kernel(const double2* __restrict__ n, const typen
 template <class T>
 __global__ void mr_update_kernel(const double2* __restrict__ d1, const double2* __restrict__ d2,
                                  typename C2<T>::t* __restrict__ x, typename C2<T>::t* __restrict__ r,
-                                 const typename C2<T>::t* __restrict__ Ar, int64_t V, int R, int dof) {
+                                 const typename C2<T>::t* __restrict__ Ar, int64_t V, int R, int dof, bool update_r) {
   const int64_t tot = V * R * dof;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
     const int k = (int)((e / dof) % R);
     const double den = d2[k].x;
     const double ar = den > 0.0 ? d1[k].x / den : 0.0, ai = den > 0.0 ? d1[k].y / den : 0.0;
-    const double rr = r[e].x, ri = r[e].y, qr = Ar[e].x, qi = Ar[e].y;
+    const double rr = r[e].x, ri = r[e].y;
     x[e].x = (T)(x[e].x + ar * rr - ai * ri);
     x[e].y = (T)(x[e].y + ar * ri + ai * rr);
-    r[e].x = (T)(rr - (ar * qr - ai * qi));
-    r[e].y = (T)(ri - (ar * qi + ai * qr));
+    if (update_r) {
+      const double qr = Ar[e].x, qi = Ar[e].y;
+      r[e].x = (T)(rr - (ar * qr - ai * qi));
+      r[e].y = (T)(ri - (ar * qi + ai * qr));
+    }
   }
 }
 
@@ -519,25 +525,26 @@ gmg_status vec_scale_inv_norm(const double2* n_dev, const Vec& X, Vec& Y, cudaSt
   return GMG_OK;
 }
 
-gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s) {
+gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s,
+                         bool update_r) {
   if (x.R * x.dof <= 1024) {
     const blas::Row rg = blas::row_geom(x.V, x.R, x.dof);
     if (x.prec == GMG_F64)
       blas::mr_update_row_kernel<double><<<rg.grid, rg.threads, 0, s>>>(d1, d2, (double2*)x.p, (double2*)r.p,
-                                                                         (const double2*)Ar.p, x.V, x.R, x.dof, rg.spb);
+                                                                         (const double2*)Ar.p, x.V, x.R, x.dof, rg.spb, update_r);
     else
       blas::mr_update_row_kernel<float><<<rg.grid, rg.threads, 0, s>>>(d1, d2, (float2*)x.p, (float2*)r.p,
-                                                                        (const float2*)Ar.p, x.V, x.R, x.dof, rg.spb);
+                                                                        (const float2*)Ar.p, x.V, x.R, x.dof, rg.spb, update_r);
     GMG_CUDA(cudaGetLastError());
     return GMG_OK;
   }
   const int g = blas::grid1(x.elems());
   if (x.prec == GMG_F64)
     blas::mr_update_kernel<double><<<g, 256, 0, s>>>(d1, d2, (double2*)x.p, (double2*)r.p, (const double2*)Ar.p, x.V,
-                                                     x.R, x.dof);
+                                                     x.R, x.dof, update_r);
   else
     blas::mr_update_kernel<float><<<g, 256, 0, s>>>(d1, d2, (float2*)x.p, (float2*)r.p, (const float2*)Ar.p, x.V, x.R,
-                                                    x.dof);
+                                                    x.dof, update_r);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }

@@ -254,7 +254,8 @@ gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStre
       GMG_TRY(vec_multidot(Ar, 1, 0, r, d1, nullptr, s));
       GMG_TRY(vec_multidot(Ar, 1, 0, Ar, d2, nullptr, s));
     }
-    GMG_TRY(vec_mr_update(d1, d2, x, r, Ar, s));
+    // the residual of the last step is never read
+    GMG_TRY(vec_mr_update(d1, d2, x, r, Ar, s, it + 1 < iters));
   }
   return GMG_OK;
 }
@@ -315,40 +316,18 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
       } else {
         GMG_TRY(apply_op(h, l, zj, w, s));
       }
-      // classical Gram-Schmidt with the coefficients kept on the device; the
-      // Hessenberg column comes back to the host in one transfer.  Small levels
-      // always take the second pass (CGS2: no extra host round trip).  On the
-      // fine level, where every pass over the basis is a pass over HBM, the
-      // second pass runs only when the first one cancelled more than half of
-      // |w|^2 for some RHS (the Daniel-Gragg-Kaufman-Stewart criterion,
-      // |w'| < |w| / sqrt 2, with |w'|^2 = |w|^2 - sum_i |h_i|^2).
+      // classical Gram-Schmidt, twice, with the coefficients kept on the device;
+      // the Hessenberg column comes back to the host in one transfer.  (With a
+      // good preconditioner w = A z_j is close to v_j, the first pass cancels
+      // most of w, and a selective second pass would run on every step.)
       const size_t nc = (size_t)(j + 1) * R;
       double2* dh = h->dscr.as<double2>();
       double2* dh2 = dh + nc;
       double2* dw = dh2 + nc;
-      bool second = true;
-      if (l == 0) {
-        GMG_TRY(vec_multidot(w, 1, 0, w, dw, nullptr, s));
-        GMG_TRY(vec_multidot(V0, j + 1, vstride, w, dh, nullptr, s));
-        std::vector<zc> c1;
-        GMG_TRY(download(h, dh, (int)(2 * nc + R), c1, s));
-        second = false;
-        for (int r = 0; r < R; ++r) {
-          double proj = 0.0;
-          for (int i = 0; i <= j; ++i) proj += std::norm(c1[(size_t)i * R + r]);
-          const double w2 = c1[2 * nc + r].real();
-          if (w2 - proj < 0.5 * w2) second = true;
-        }
-      } else {
-        GMG_TRY(vec_multidot(V0, j + 1, vstride, w, dh, nullptr, s));
-      }
+      GMG_TRY(vec_multidot(V0, j + 1, vstride, w, dh, nullptr, s));
       GMG_TRY(vec_multiaxpy(dh, V0, j + 1, vstride, w, s, -1.0));
-      if (second) {
-        GMG_TRY(vec_multidot(V0, j + 1, vstride, w, dh2, nullptr, s));
-        GMG_TRY(vec_multiaxpy(dh2, V0, j + 1, vstride, w, s, -1.0));
-      } else {
-        GMG_CUDA(cudaMemsetAsync(dh2, 0, sizeof(double2) * nc, s));
-      }
+      GMG_TRY(vec_multidot(V0, j + 1, vstride, w, dh2, nullptr, s));
+      GMG_TRY(vec_multiaxpy(dh2, V0, j + 1, vstride, w, s, -1.0));
       GMG_TRY(vec_multidot(w, 1, 0, w, dw, nullptr, s));
       Vec vn = nth(V0, j + 1);
       GMG_TRY(vec_scale_inv_norm(dw, w, vn, s));

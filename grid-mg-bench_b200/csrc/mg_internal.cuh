@@ -57,7 +57,9 @@ gmg_status vec_gaussian(Vec& X, uint64_t seed, cudaStream_t s);
 // Y(r) = X(r) / sqrt(n[r].x), n from a device multidot
 gmg_status vec_scale_inv_norm(const double2* n_dev, const Vec& X, Vec& Y, cudaStream_t s);
 // MR step with alpha = d1 / d2 (device): x += alpha r, r -= alpha Ar
-gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s);
+// x += a r, and r -= a Ar unless update_r is false, a = <Ar, r> / <Ar, Ar> per RHS
+gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s,
+                         bool update_r = true);
 // Y = X - Y
 gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s);
 // G[a][b] = <X(a), X(b)> over the whole lattice (R <= 32 columns), FP64

@@ -116,14 +116,45 @@ __device__ __forceinline__ void wilson_hop(typename wt<T>::C out[4][3],
 // One output spinor (site, rhs).  links(p) returns the 3x3 link of hop p
 // (p < 4: U_mu(x), p >= 4: U_mu(x - mu), applied daggered); cl: the site's
 // two 6x6 clover blocks.
+// 12 complex numbers of one (site, RHS) record: 16-byte accesses when VEC
+// (the record start is 16-byte aligned), else one per complex number
+template <class T, bool VEC>
+__device__ __forceinline__ void ld12(typename wt<T>::C v[12], const typename wt<T>::C* __restrict__ p) {
+  if (VEC && sizeof(T) == 4) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const float4 a = q[k];
+      v[2 * k].x = a.x;
+      v[2 * k].y = a.y;
+      v[2 * k + 1].x = a.z;
+      v[2 * k + 1].y = a.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 12; ++k) v[k] = p[k];
+  }
+}
+template <class T, bool VEC>
+__device__ __forceinline__ void st12(typename wt<T>::C* __restrict__ p, const typename wt<T>::C v[12]) {
+  if (VEC && sizeof(T) == 4) {
+    float4* q = reinterpret_cast<float4*>(p);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) q[k] = make_float4(v[2 * k].x, v[2 * k].y, v[2 * k + 1].x, v[2 * k + 1].y);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 12; ++k) p[k] = v[k];
+  }
+}
+
 // DOTS (op M or MDAG): also add <out, in> and <out, out> of this (site, r) to
-// Ds[3 r .. 3 r + 2] (shared memory).
-template <class T, class LinkFn, bool DOTS = false>
+// dsum[0..1] and dsum[2].  VEC: 16-byte spinor accesses.
+template <class T, class LinkFn, bool DOTS = false, bool VEC = false>
 __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict__ cl, LinkFn links,
                                             const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
                                             typename wt<T>::C* __restrict__ out, int V, int nrhs, int site, int r,
                                             T diag, int op, int dir, int disp, int apbc, int tvol, int Lt,
-                                            double* Ds = nullptr) {
+                                            double* dsum = nullptr) {
   typedef typename wt<T>::C C;
   const bool g5 = (op == GMG_OP_MDAG);
   const int tc = site / tvol;
@@ -136,11 +167,9 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
   if (op != GMG_OP_MDIR) {
     // diagonal: (4 + m) psi + Cl psi, two chiral 6x6 blocks
     C psi[12];
-    const C* src = in + ((int64_t)site * nrhs + r) * 12;
+    ld12<T, VEC>(psi, in + ((int64_t)site * nrhs + r) * 12);
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
-      psi[k] = src[k];
-      if (DOTS) cin[k] = psi[k];
       if (g5 && k >= 6) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
     }
 #pragma unroll
@@ -165,35 +194,39 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
       T coef = (T)-0.5;
       if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
       C psi[12];
-      const C* src = in + ((int64_t)nb * nrhs + r) * 12;
+      ld12<T, VEC>(psi, in + ((int64_t)nb * nrhs + r) * 12);
+      if (g5) {
 #pragma unroll
-      for (int k = 0; k < 12; ++k) {
-        psi[k] = src[k];
-        if (g5 && k >= 6) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
+        for (int k = 6; k < 12; ++k) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
       }
       wilson_hop<T>(acc, links(p, nb), dsp < 0, psi, mu, dsp, coef);
     }
   }
-  C* dst = out + ((int64_t)site * nrhs + r) * 12;
-  double pr = 0.0, pi = 0.0, pn = 0.0;
+  // per-record partial products in T (12 terms), accumulated in FP64 by the caller
+  T pr = 0, pi = 0, pn = 0;
+  C ov[12];
+  // the input record again for the products (re-read rather than kept live
+  // through the hops: registers decide the occupancy of this kernel)
+  if (DOTS) ld12<T, VEC>(cin, in + ((int64_t)site * nrhs + r) * 12);
 #pragma unroll
   for (int s = 0; s < 4; ++s)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       C v = acc[s][c];
       if (g5 && s >= 2) { v.x = -v.x; v.y = -v.y; }
-      dst[s * 3 + c] = v;
+      ov[s * 3 + c] = v;
       if (DOTS) {
-        const double vx = v.x, vy = v.y, ix = cin[s * 3 + c].x, iy = cin[s * 3 + c].y;
-        pr += vx * ix + vy * iy;
-        pi += vx * iy - vy * ix;
-        pn += vx * vx + vy * vy;
+        const T ix = cin[s * 3 + c].x, iy = cin[s * 3 + c].y;
+        pr += v.x * ix + v.y * iy;
+        pi += v.x * iy - v.y * ix;
+        pn += v.x * v.x + v.y * v.y;
       }
     }
+  st12<T, VEC>(out + ((int64_t)site * nrhs + r) * 12, ov);
   if (DOTS) {
-    atomicAdd(&Ds[3 * r], pr);
-    atomicAdd(&Ds[3 * r + 1], pi);
-    atomicAdd(&Ds[3 * r + 2], pn);
+    dsum[0] += pr;
+    dsum[1] += pi;
+    dsum[2] += pn;
   }
 }
 
@@ -225,8 +258,8 @@ constexpr int kTileSites = 16;
 // sites' 8 hop links and clover blocks are staged in shared memory once and
 // read by every RHS of the tile.  Thread per (site, RHS) otherwise, spinors
 // read from global memory.
-template <class T, bool DOTS>
-__global__ void __launch_bounds__(256) wilson_tile_kernel(
+template <class T, bool DOTS, int MINB>
+__global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
     const typename wt<T>::C* __restrict__ hop, const typename wt<T>::C* __restrict__ clover,
     const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
     typename wt<T>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
@@ -240,6 +273,8 @@ __global__ void __launch_bounds__(256) wilson_tile_kernel(
     for (int k = threadIdx.x; k < 3 * nrhs; k += blockDim.x) Ds[k] = 0.0;
   const int nt = (V + kTileSites - 1) / kTileSites;
   const int sl = threadIdx.x / rt, rl = threadIdx.x % rt;
+  const bool two = nrhs <= 2 * rt;
+  double da[3] = {0.0, 0.0, 0.0}, db[3] = {0.0, 0.0, 0.0};
   for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
     const int s0 = tile * kTileSites;
     const int ns = min(kTileSites, V - s0);
@@ -253,12 +288,39 @@ __global__ void __launch_bounds__(256) wilson_tile_kernel(
       const int site = s0 + sl;
       const C* lsite = Ls + sl * 72;
       auto links = [&](int p, int) -> const C* { return lsite + p * 9; };
-      for (int r = rl; r < nrhs; r += rt)
-        wilson_site<T, decltype(links), DOTS>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op, dir,
-                                              disp, apbc, tvol, Lt, Ds);
+      // with two RHS or fewer per thread (rl, rl + rt) the thread owns them for
+      // the whole launch and its products stay in registers until the end
+      int k = 0;
+      for (int r = rl; r < nrhs; r += rt, ++k) {
+        double dt[3] = {0.0, 0.0, 0.0};
+        wilson_site<T, decltype(links), DOTS, true>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op,
+                                                    dir, disp, apbc, tvol, Lt, dt);
+        if (DOTS) {
+          if (two) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              if (k == 0)
+                da[c] += dt[c];
+              else
+                db[c] += dt[c];
+            }
+          } else {
+            atomicAdd(&Ds[3 * r], dt[0]);
+            atomicAdd(&Ds[3 * r + 1], dt[1]);
+            atomicAdd(&Ds[3 * r + 2], dt[2]);
+          }
+        }
+      }
     }
   }
   if (DOTS) {
+    if (two) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (rl < nrhs) atomicAdd(&Ds[3 * rl + c], da[c]);
+        if (rl + rt < nrhs) atomicAdd(&Ds[3 * (rl + rt) + c], db[c]);
+      }
+    }
     __syncthreads();
     for (int k = threadIdx.x; k < nrhs; k += blockDim.x) {
       atomicAdd(&d1[k].x, Ds[3 * k]);
@@ -1073,8 +1135,9 @@ static gmg_status launch_site(gmg_wilson* h, int op, int dir, int disp, int vec_
   return GMG_OK;
 }
 
-// tile kernel: kTileSites sites x min(nrhs, 16) threads per CTA
-template <bool DOTS>
+// tile kernel: kTileSites sites x min(nrhs, 16) threads per CTA; MINB: CTAs
+// per SM the register allocation must allow (FP32: 2 or 3)
+template <bool DOTS, int MINB = 2>
 static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs, const void* in,
                               void* out, double2* d1, double2* d2, cudaStream_t s) {
   const int V = (int)h->dims.vol();
@@ -1086,17 +1149,17 @@ static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_
   if (vec_prec == GMG_F64) {
     const size_t smem = sizeof(double2) * 2 * kTileSites * 72 + dots;
     if (smem > 48 * 1024)
-      GMG_CUDA(cudaFuncSetAttribute(wilson_tile_kernel<double, DOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      GMG_CUDA(cudaFuncSetAttribute(wilson_tile_kernel<double, DOTS, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
-    wilson_tile_kernel<double, DOTS><<<g, kTileSites * rt, smem, s>>>(
+    wilson_tile_kernel<double, DOTS, 2><<<g, kTileSites * rt, smem, s>>>(
         h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(), (const double2*)in, (double2*)out, V,
         nrhs, rt, 4.0 + h->mass, op, dir, disp, h->apbc, tvol, h->dims.d[3], d1, d2);
   } else if (vec_prec == GMG_F32) {
     const size_t smem = sizeof(float2) * 2 * kTileSites * 72 + dots;
     if (smem > 48 * 1024)
-      GMG_CUDA(cudaFuncSetAttribute(wilson_tile_kernel<float, DOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
-    wilson_tile_kernel<float, DOTS><<<g, kTileSites * rt, smem, s>>>(
+      GMG_CUDA(cudaFuncSetAttribute(wilson_tile_kernel<float, DOTS, MINB>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    wilson_tile_kernel<float, DOTS, MINB><<<g, kTileSites * rt, smem, s>>>(
         h->hop_f.as<float2>(), h->clover_f.as<float2>(), h->nbr.as<int32_t>(), (const float2*)in, (float2*)out, V,
         nrhs, rt, (float)(4.0 + h->mass), op, dir, disp, h->apbc, tvol, h->dims.d[3], d1, d2);
   } else {
@@ -1105,6 +1168,10 @@ static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
+
+// internal variant id: a second register budget of the tile kernel, tuned
+// alongside the public variants and reported as GMG_WILSON_TILE
+constexpr int kTileOcc3 = 16;
 
 // One launch of kernel variant v; *launched = false when v does not apply.
 static gmg_status run_variant(gmg_wilson* h, int v, bool dots, int op, int dir, int disp, int vec_prec, int nrhs,
@@ -1115,8 +1182,13 @@ static gmg_status run_variant(gmg_wilson* h, int v, bool dots, int op, int dir, 
       if (dots) break;
       return launch_site(h, op, dir, disp, vec_prec, nrhs, in, out, s);
     case GMG_WILSON_TILE:
+      if (((uintptr_t)in | (uintptr_t)out) & 15) break;  // 16-byte spinor accesses
       return dots ? launch_tile<true>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s)
                   : launch_tile<false>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s);
+    case kTileOcc3:  // the tile kernel with registers capped for 3 CTAs per SM (FP32)
+      if ((((uintptr_t)in | (uintptr_t)out) & 15) || vec_prec != GMG_F32) break;
+      return dots ? launch_tile<true, 3>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s)
+                  : launch_tile<false, 3>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s);
     case GMG_WILSON_QUAD:
       return dots ? launch_quad<true>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s)
                   : launch_quad<false>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s);
@@ -1164,6 +1236,7 @@ static gmg_status wilson_dispatch(gmg_wilson* h, bool dots, int op, int dir, int
   std::vector<int> cand;
   if (!dots && nrhs < 4) cand.push_back(GMG_WILSON_SITE);
   cand.push_back(GMG_WILSON_TILE);
+  if (vec_prec == GMG_F32) cand.push_back(kTileOcc3);
   cand.push_back(GMG_WILSON_QUAD);
   if (nrhs >= 4) cand.push_back(GMG_WILSON_STAGED);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
