@@ -6,6 +6,7 @@
 // norm2, axpy used by its GMRES / FGMRES / MR, selected at include/Helpers.h:314-341).
 // Reductions accumulate in FP64 whatever the field precision.
 #include <algorithm>
+#include <type_traits>
 
 #include "mg_internal.cuh"
 
@@ -242,6 +243,116 @@ __global__ void __launch_bounds__(1024) multiaxpy_row_kernel(const double2* __re
   }
 }
 
+// Y(s, r) += sgn * sum_j a[j*R + r] X_j(s, r) and, in the same sweep over the
+// updated Y, MODE 1: out[j*R + r] += <X_j(r), Y(r)> for j < nx (the next
+// Gram-Schmidt pass's coefficients), MODE 2: out[r] += <Y(r), Y(r)> (the norm
+// of the new Krylov vector).  nx <= kAxDotMaxJ (every restart length the MG
+// levels use); MODE 1 keeps a site's X_j values in registers between the
+// update and the products, so it runs at most kAxDot1Threads threads per block
+// (MODE 2 needs no X after the update and runs up to kAxDotThreads).
+constexpr int kAxDotMaxJ = 10;
+constexpr int kAxDotThreads = 768;
+constexpr int kAxDot1Threads = 384;
+
+template <class TX, class T, int MODE, int MJ = kAxDotMaxJ>
+__global__ void __launch_bounds__(MODE == 1 ? kAxDot1Threads : kAxDotThreads) multiaxpy_dot_row_kernel(const double2* __restrict__ a,
+                                                                 const typename C2<TX>::t* __restrict__ X,
+                                                                 int64_t xstride, int nx,
+                                                                 typename C2<T>::t* __restrict__ Y, int64_t V, int R,
+                                                                 int dof, int spb, double sgn,
+                                                                 double2* __restrict__ out) {
+  extern __shared__ double2 smd[];
+  double2* cf = smd;                                        // [nx][R]
+  double* part = reinterpret_cast<double*>(smd + kAxDotMaxJ * R);  // [8][NT]
+  const int RD = R * dof, t = threadIdx.x, NT = blockDim.x;
+  const int so = t / RD, i = t % RD, r = i / dof;
+  for (int k = t; k < nx * R; k += NT) cf[k] = make_double2(sgn * a[k].x, sgn * a[k].y);
+  __syncthreads();
+  const bool act = t < spb * RD;
+  double ar[MODE == 1 ? MJ : 1], ai[MODE == 1 ? MJ : 1];
+#pragma unroll
+  for (int j = 0; j < (MODE == 1 ? MJ : 1); ++j) ar[j] = ai[j] = 0.0;
+  if (act) {
+    for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+      const int64_t e = s * RD + i;
+      double yr = Y[e].x, yi = Y[e].y;
+      if (MODE == 1) {
+        // MODE 1 is instantiated for the exact basis count (MJ == nx): the
+        // loads carry no guard and all issue before the first use
+        typename C2<TX>::t xv[MJ];
+#pragma unroll
+        for (int j = 0; j < MJ; ++j) xv[j] = X[j * xstride + e];
+#pragma unroll
+        for (int j = 0; j < MJ; ++j) {
+          const double2 c = cf[j * R + r];
+          yr += c.x * xv[j].x - c.y * xv[j].y;
+          yi += c.x * xv[j].y + c.y * xv[j].x;
+        }
+#pragma unroll
+        for (int j = 0; j < MJ; ++j) {
+          ar[j] += xv[j].x * yr + xv[j].y * yi;
+          ai[j] += xv[j].x * yi - xv[j].y * yr;
+        }
+      } else {
+        for (int j = 0; j < nx; ++j) {
+          const typename C2<TX>::t x = X[j * xstride + e];
+          const double2 c = cf[j * R + r];
+          yr += c.x * x.x - c.y * x.y;
+          yi += c.x * x.y + c.y * x.x;
+        }
+      }
+      Y[e].x = (T)yr;
+      Y[e].y = (T)yi;
+      if (MODE == 1) {
+      } else {
+        ar[0] += yr * yr + yi * yi;
+      }
+    }
+  }
+  // block reduction in chunks of 4 products: fold the spb site slots, then the
+  // dof components of each RHS, then one global atomic per (j, r) and block
+  const int nprod = MODE == 1 ? nx : 1;
+#pragma unroll
+  for (int j0 = 0; j0 < (MODE == 1 ? MJ : 1); j0 += 4) {
+    if (j0 >= nprod) break;
+    const int nj = min(4, nprod - j0);
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = j0 + q;
+      double vr = 0.0, vi = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < (MODE == 1 ? MJ : 1); ++jj)
+        if (jj == j) {
+          vr = ar[jj];
+          vi = ai[jj];
+        }
+      part[(2 * q) * NT + t] = act ? vr : 0.0;
+      part[(2 * q + 1) * NT + t] = act ? vi : 0.0;
+    }
+    __syncthreads();
+    if (spb > 1) {
+      for (int k = t; k < 2 * nj * RD; k += NT) {
+        const int jc = k / RD, ii = k % RD;
+        double v = part[jc * NT + ii];
+        for (int o = 1; o < spb; ++o) v += part[jc * NT + o * RD + ii];
+        part[jc * NT + ii] = v;
+      }
+      __syncthreads();
+    }
+    for (int k = t; k < nj * R; k += NT) {
+      const int q = k / R, rr = k % R;
+      double vr = 0.0, vi = 0.0;
+      for (int d = 0; d < dof; ++d) {
+        vr += part[(2 * q) * NT + rr * dof + d];
+        vi += part[(2 * q + 1) * NT + rr * dof + d];
+      }
+      atomicAdd(&out[(j0 + q) * R + rr].x, vr);
+      if (MODE == 1) atomicAdd(&out[(j0 + q) * R + rr].y, vi);
+    }
+  }
+}
+
 // Y(r) = X(r) / sqrt(n[r].x)
 template <class T>
 __global__ void __launch_bounds__(1024) scale_inv_norm_row_kernel(const double2* __restrict__ n,
@@ -320,12 +431,15 @@ gmg_status vec_multidot(const Vec& X0, int nx, int64_t xstride_elems, const Vec&
       GMG_CUDA(cudaFuncSetAttribute(blas::multidot_row_kernel<float, JB>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     }
+    // one resident wave of blocks: every block ends in nj * R global atomics on
+    // the same nj * R addresses, so more blocks than fit at once only add contention
+    const int grid = std::min(g.grid, 148 * std::max(1, 2048 / g.threads));
     for (int j0 = 0; j0 < nx; j0 += JB) {
       if (Y.prec == GMG_F64)
-        blas::multidot_row_kernel<double, JB><<<g.grid, g.threads, sm, s>>>(
+        blas::multidot_row_kernel<double, JB><<<grid, g.threads, sm, s>>>(
             (const double2*)X0.p, xstride_elems, j0, nx, (const double2*)Y.p, Y.V, Y.R, Y.dof, g.spb, out_dev, mask);
       else
-        blas::multidot_row_kernel<float, JB><<<g.grid, g.threads, sm, s>>>(
+        blas::multidot_row_kernel<float, JB><<<grid, g.threads, sm, s>>>(
             (const float2*)X0.p, xstride_elems, j0, nx, (const float2*)Y.p, Y.V, Y.R, Y.dof, g.spb, out_dev, mask);
       GMG_CUDA(cudaGetLastError());
     }
@@ -523,6 +637,50 @@ gmg_status vec_scale_inv_norm(const double2* n_dev, const Vec& X, Vec& Y, cudaSt
     blas::scale_inv_norm_kernel<float><<<g, 256, 0, s>>>(n_dev, (const float2*)X.p, (float2*)Y.p, Y.V, Y.R, Y.dof);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
+}
+
+// Fused Gram-Schmidt sweep: Y += sgn * sum_j a_j X_j, then out = (mode 1)
+// <X_j, Y> for j < nx, or (mode 2) <Y, Y>, both over the updated Y.  Falls back
+// to separate passes where the fused kernel does not apply.
+gmg_status vec_multiaxpy_dot(const double2* a_dev, const Vec& X0, int nx, int64_t xstride_elems, Vec& Y,
+                             cudaStream_t s, double sgn, double2* out_dev, int mode) {
+  const bool fused = nx <= blas::kAxDotMaxJ && X0.prec == Y.prec &&
+                     Y.R * Y.dof <= (mode == 1 ? blas::kAxDot1Threads : blas::kAxDotThreads);
+  if (!fused) {
+    GMG_TRY(vec_multiaxpy(a_dev, X0, nx, xstride_elems, Y, s, sgn));
+    return mode == 1 ? vec_multidot(X0, nx, xstride_elems, Y, out_dev, nullptr, s)
+                     : vec_multidot(Y, 1, 0, Y, out_dev, nullptr, s);
+  }
+  GMG_CUDA(cudaMemsetAsync(out_dev, 0, sizeof(double2) * (mode == 1 ? nx : 1) * Y.R, s));
+  const blas::Row g = blas::row_geom(Y.V, Y.R, Y.dof);
+  const size_t sm = sizeof(double2) * blas::kAxDotMaxJ * Y.R + sizeof(double) * 8 * g.threads;
+  const int grid = std::min(g.grid, 148 * std::max(1, 2048 / g.threads));
+  auto launch = [&](auto kern, const auto* X, auto* Yp) -> gmg_status {
+    if (sm > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<grid, g.threads, sm, s>>>(a_dev, X, xstride_elems, nx, Yp, Y.V, Y.R, Y.dof, g.spb, sgn, out_dev);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  };
+  // mode 1 holds nx X values and 2 nx products per thread: one instantiation per nx
+  auto run = [&](const auto* X, auto* Yp) -> gmg_status {
+    typedef std::remove_const_t<std::remove_pointer_t<decltype(X)>> C;
+    typedef std::conditional_t<std::is_same<C, double2>::value, double, float> Tb;
+    if (mode == 2) return launch(blas::multiaxpy_dot_row_kernel<Tb, Tb, 2>, X, Yp);
+    switch (nx) {
+      case 1: return launch(blas::multiaxpy_dot_row_kernel<Tb, Tb, 1, 1>, X, Yp);
+      case 2: return launch(blas::multiaxpy_dot_row_kernel<Tb, Tb, 1, 2>, X, Yp);
+      case 3: return launch(blas::multiaxpy_dot_row_kernel<Tb, Tb, 1, 3>, X, Yp);
+      case 4: return launch(blas::multiaxpy_dot_row_kernel<Tb, Tb, 1, 4>, X, Yp);
+      case 5: return launch(blas::multiaxpy_dot_row_kernel<Tb, Tb, 1, 5>, X, Yp);
+      case 6: return launch(blas::multiaxpy_dot_row_kernel<Tb, Tb, 1, 6>, X, Yp);
+      case 7: return launch(blas::multiaxpy_dot_row_kernel<Tb, Tb, 1, 7>, X, Yp);
+      case 8: return launch(blas::multiaxpy_dot_row_kernel<Tb, Tb, 1, 8>, X, Yp);
+      case 9: return launch(blas::multiaxpy_dot_row_kernel<Tb, Tb, 1, 9>, X, Yp);
+      default: return launch(blas::multiaxpy_dot_row_kernel<Tb, Tb, 1, 10>, X, Yp);
+    }
+  };
+  if (Y.prec == GMG_F64) return run((const double2*)X0.p, (double2*)Y.p);
+  return run((const float2*)X0.p, (float2*)Y.p);
 }
 
 gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s,

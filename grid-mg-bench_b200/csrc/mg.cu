@@ -324,11 +324,11 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
       double2* dh = h->dscr.as<double2>();
       double2* dh2 = dh + nc;
       double2* dw = dh2 + nc;
+      // pass 1: dh = V^H w; then w -= V dh fused with pass 2's dh2 = V^H w;
+      // then w -= V dh2 fused with dw = |w|^2
       GMG_TRY(vec_multidot(V0, j + 1, vstride, w, dh, nullptr, s));
-      GMG_TRY(vec_multiaxpy(dh, V0, j + 1, vstride, w, s, -1.0));
-      GMG_TRY(vec_multidot(V0, j + 1, vstride, w, dh2, nullptr, s));
-      GMG_TRY(vec_multiaxpy(dh2, V0, j + 1, vstride, w, s, -1.0));
-      GMG_TRY(vec_multidot(w, 1, 0, w, dw, nullptr, s));
+      GMG_TRY(vec_multiaxpy_dot(dh, V0, j + 1, vstride, w, s, -1.0, dh2, 1));
+      GMG_TRY(vec_multiaxpy_dot(dh2, V0, j + 1, vstride, w, s, -1.0, dw, 2));
       Vec vn = nth(V0, j + 1);
       GMG_TRY(vec_scale_inv_norm(dw, w, vn, s));
       std::vector<zc> col;

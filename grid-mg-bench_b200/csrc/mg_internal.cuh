@@ -43,6 +43,10 @@ gmg_status vec_multidot(const Vec& X0, int nx, int64_t xstride_elems, const Vec&
 // Y(r) += sum_j a[j*R + r] X_j(r)
 gmg_status vec_multiaxpy(const double2* a_dev, const Vec& X0, int nx, int64_t xstride_elems, Vec& Y, cudaStream_t s,
                          double sgn = 1.0);
+// Y += sgn * sum_j a[j*R + r] X_j, then out = <X_j, Y> per (j, r) (mode 1) or
+// <Y, Y> per r (mode 2) over the updated Y, in one sweep where possible
+gmg_status vec_multiaxpy_dot(const double2* a_dev, const Vec& X0, int nx, int64_t xstride_elems, Vec& Y,
+                             cudaStream_t s, double sgn, double2* out_dev, int mode);
 // Y(r) = a[r] X(r) + b[r] Y(r)
 gmg_status vec_axpby(const double2* a_dev, const Vec& X, const double2* b_dev, Vec& Y, cudaStream_t s);
 // Y = X with a precision conversion
