@@ -244,7 +244,8 @@ __device__ __forceinline__ void issue_stage_kh(int kh, uint32_t dt, uint64_t ad,
 // Shared memory: `stages` stages of pps link tiles followed by pps neighbour
 // tiles, then the mbarriers, the TMEM address, the abort flag and the
 // producer's neighbour-index table.
-__global__ void __launch_bounds__(kThreads, 1) coarse_mrhs_tc_kernel(const Params P) {
+template <int CTAS>  // CTAs per SM the register budget allows (1 or 2)
+__global__ void __launch_bounds__(kThreads, CTAS) coarse_mrhs_tc_kernel(const Params P) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t link_bytes = (uint32_t)P.Kc * P.Mp * 16;     // one stencil point of one site
@@ -608,21 +609,36 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, cons
   // barriers (<= 2*32+9), TMEM slot + flag, neighbour and link-site tables of the two producers
   const size_t tables = 2 * 32 * 9 * 4 + 2 * 32 * 4;
   const size_t fixed = 80 * 8 + 16 + tables;
-  const size_t budget = 227 * 1024 - fixed;
   const int npts = p1 - p0;
-  // points per stage: the largest of 4, 3, 2 dividing the point count that
-  // still leaves at least 4 stages, else 1
-  int pps = 1;
-  for (int c : {4, 3, 2})
-    if (npts % c == 0 && budget / (c * per_point) >= 4) {
-      pps = c;
-      break;
-    }
-  const uint32_t stage_bytes = pps * per_point;
-  const int stages = (int)std::min<size_t>(32, budget / stage_bytes) & ~1;  // even: two producers
+  // Two CTAs per SM (two MMA-issuing threads, two independent site chains)
+  // when both CTAs' TMEM accumulators fit the SM's 512 columns and each keeps
+  // at least 4 stages in half the shared memory; else one CTA with all of it.
+  const uint32_t acc_cols = 2 * (uint32_t)Rp;
+  const uint32_t nacc = std::min<uint32_t>(kAccBufs, 512u / acc_cols);
+  uint32_t ncols = 32;
+  while (ncols < nacc * acc_cols) ncols <<= 1;
+  int ctas = 1, pps = 1, stages = 0;
+  uint32_t stage_bytes = 0;
+  for (int c2 : {2, 1}) {
+    if (c2 == 2 && 2 * ncols > 512) continue;
+    const size_t budget = (c2 == 2 ? 233472 / 2 - 1024 : 227 * 1024) - fixed;
+    // points per stage: the largest of 4, 3, 2 dividing the point count that
+    // still leaves at least 4 stages, else 1
+    pps = 1;
+    for (int c : {4, 3, 2})
+      if (npts % c == 0 && budget / (c * per_point) >= 4) {
+        pps = c;
+        break;
+      }
+    stage_bytes = pps * per_point;
+    stages = (int)std::min<size_t>(32, budget / stage_bytes) & ~1;  // even: two producers
+    ctas = c2;
+    if (c2 == 1 || stages >= 4) break;
+  }
   GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil: tile does not fit shared memory");
   const size_t smem = (size_t)stages * stage_bytes + (size_t)(2 * stages + 2 * kAccBufs + 1) * 8 + 16 + tables;
-  GMG_CUDA(cudaFuncSetAttribute(coarse_mrhs_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  auto kern = ctas == 2 ? coarse_mrhs_tc_kernel<2> : coarse_mrhs_tc_kernel<1>;
+  GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 148;
   GMG_CUDA(cudaGetDevice(&dev));
   GMG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -647,11 +663,12 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, cons
   P.stages = stages;
   P.kind = kind == GMG_BF16 ? 1 : 0;
   P.pps = pps;
+  const int grid = std::min(V, nsm * ctas);
   if (timed) {
     KernelTimer kt("coarse_mrhs_tc", s);
-    coarse_mrhs_tc_kernel<<<std::min(V, nsm), kThreads, smem, s>>>(P);
+    kern<<<grid, kThreads, smem, s>>>(P);
   } else {
-    coarse_mrhs_tc_kernel<<<std::min(V, nsm), kThreads, smem, s>>>(P);
+    kern<<<grid, kThreads, smem, s>>>(P);
   }
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
