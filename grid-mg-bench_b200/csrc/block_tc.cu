@@ -16,7 +16,7 @@
 // products hi.hi + hi.lo + lo.hi accumulate in FP32 in tensor memory, which keeps the
 // result at about FP32 accuracy while reading the basis at BF16 cost per part.
 //
-// Kernel (one persistent CTA per SM, blocks c = blockIdx.x, +gridDim.x, ...):
+// Kernel (one or two persistent CTAs per SM, blocks c = blockIdx.x, +gridDim.x, ...):
 //   warp 0      producer: one bulk copy of the basis hi and lo tiles per stage
 //               (the packed basis is stage-contiguous in HBM)
 //   warp 1      TMEM allocation + MMA issue (one thread): 3 MMAs per K-step
@@ -180,7 +180,8 @@ struct Params {
   int raw;  // 1: the producer bulk-copies each site's FP32 rows into the stage (16-byte aligned rows)
 };
 
-__global__ void __launch_bounds__(kThreads, 1) project_tc_kernel(const Params P) {
+template <int CTAS>  // CTAs per SM the register budget allows (1 or 2)
+__global__ void __launch_bounds__(kThreads, CTAS) project_tc_kernel(const Params P) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int kc_stage = P.KS / 8;                               // K-chunks per stage
@@ -470,7 +471,8 @@ constexpr int kPWarps = 6;
 constexpr int kPThreads = kPWarps * 32;
 constexpr int kTileM = 128;
 
-__global__ void __launch_bounds__(kPThreads, 1) promote_tc_kernel(const PParams P) {
+template <int CTAS>
+__global__ void __launch_bounds__(kPThreads, CTAS) promote_tc_kernel(const PParams P) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ctile = kTileM / 8;                         // K-chunks (8 fine dofs) per M tile
@@ -742,12 +744,26 @@ gmg_status agg_project_tc(gmg_agg* h, int nrhs, const float* fine, float* coarse
   const uint32_t site_bytes = (uint32_t)nrhs * h->dof * 8;
   const bool aligned = (reinterpret_cast<uintptr_t>(fine) & 15) == 0 && site_bytes % 16 == 0;
   const uint32_t raw_stage = (uint32_t)g.sps * site_bytes;
-  int raw = aligned && (2 * a_bytes + 2 * b_bytes + raw_stage) * 2 + fixed <= 227 * 1024 ? 1 : 0;
-  const uint32_t stage_bytes = 2 * a_bytes + 2 * b_bytes + (raw ? raw_stage : 0u);
-  int stages = (int)std::min<size_t>(16, (227 * 1024 - fixed) / stage_bytes);
+  // two CTAs per SM (twice the converter and MMA warps) when both TMEM
+  // accumulators fit the SM's 512 columns and each CTA keeps 3 stages in half
+  // the shared memory; else one CTA with all of it
+  uint32_t ncols = 32;
+  while (ncols < ptc::kAcc * 2 * (uint32_t)Rp) ncols <<= 1;
+  int ctas = 1, raw = 0, stages = 0;
+  uint32_t stage_bytes = 0;
+  for (int c2 : {2, 1}) {
+    if (c2 == 2 && 2 * ncols > 512) continue;
+    const size_t cap = c2 == 2 ? 233472 / 2 - 1024 : 227 * 1024;
+    raw = aligned && (2 * a_bytes + 2 * b_bytes + raw_stage) * 2 + fixed <= cap ? 1 : 0;
+    stage_bytes = 2 * a_bytes + 2 * b_bytes + (raw ? raw_stage : 0u);
+    stages = (int)std::min<size_t>(16, (cap - fixed) / stage_bytes);
+    ctas = c2;
+    if (c2 == 1 || stages >= 3) break;
+  }
   GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "tensor-core projection: stage does not fit shared memory");
   const size_t smem = (size_t)stages * stage_bytes + (size_t)(3 * stages + 2 * ptc::kAcc + 1) * 8 + 16 + (size_t)h->bv * 4;
-  GMG_CUDA(cudaFuncSetAttribute(ptc::project_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  auto kern = ctas == 2 ? ptc::project_tc_kernel<2> : ptc::project_tc_kernel<1>;
+  GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   if (!h->dev_err.p) {
     GMG_TRY(h->dev_err.alloc(256));
     GMG_CUDA(cudaMemsetAsync(h->dev_err.p, 0, 256, s));
@@ -779,7 +795,7 @@ gmg_status agg_project_tc(gmg_agg* h, int nrhs, const float* fine, float* coarse
 
   {
     KernelTimer kt("project_tc", s);
-    ptc::project_tc_kernel<<<std::min(P.Vc, nsm), ptc::kThreads, smem, s>>>(P);
+    kern<<<std::min(P.Vc, nsm * ctas), ptc::kThreads, smem, s>>>(P);
   }
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
@@ -795,10 +811,23 @@ gmg_status agg_promote_tc(gmg_agg* h, int nrhs, const float* coarse, float* fine
   const uint32_t b_bytes = (uint32_t)(K2 / 8) * 2 * Rp * 16;
   const size_t fixed = 4 * (size_t)b_bytes + (2 * 16 + 10 + 1) * 8 + 16;
   GMG_CHECK(fixed < 227 * 1024, GMG_ERR_UNSUPPORTED, "tensor-core promotion: coarse tile does not fit");
-  const int stages = (int)std::min<size_t>(16, (227 * 1024 - fixed) / (2 * a_bytes));
+  // two CTAs per SM when both TMEM accumulators fit and each keeps 2 stages in
+  // half the shared memory; else one CTA with all of it
+  uint32_t ncols = 32;
+  while (ncols < 2 * 2 * (uint32_t)Rp) ncols <<= 1;
+  int ctas = 1, stages = 0;
+  for (int c2 : {2, 1}) {
+    if (c2 == 2 && 2 * ncols > 512) continue;
+    const size_t cap = c2 == 2 ? 233472 / 2 - 1024 : 227 * 1024;
+    if (fixed >= cap) continue;
+    stages = (int)std::min<size_t>(16, (cap - fixed) / (2 * a_bytes));
+    ctas = c2;
+    if (c2 == 1 || stages >= 2) break;
+  }
   GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "tensor-core promotion: stage does not fit shared memory");
   const size_t smem = (size_t)stages * 2 * a_bytes + 4 * (size_t)b_bytes + (size_t)(2 * stages + 10 + 1) * 8 + 16;
-  GMG_CUDA(cudaFuncSetAttribute(ptc::promote_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  auto kern = ctas == 2 ? ptc::promote_tc_kernel<2> : ptc::promote_tc_kernel<1>;
+  GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   if (!h->dev_err.p) {
     GMG_TRY(h->dev_err.alloc(256));
     GMG_CUDA(cudaMemsetAsync(h->dev_err.p, 0, 256, s));
@@ -828,7 +857,7 @@ gmg_status agg_promote_tc(gmg_agg* h, int nrhs, const float* coarse, float* fine
 
   {
     KernelTimer kt("promote_tc", s);
-    ptc::promote_tc_kernel<<<std::min(P.Vc, nsm), ptc::kPThreads, smem, s>>>(P);
+    kern<<<std::min(P.Vc, nsm * ctas), ptc::kPThreads, smem, s>>>(P);
   }
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
