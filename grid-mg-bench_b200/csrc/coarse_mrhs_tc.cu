@@ -38,6 +38,7 @@
 // Both are the canonical no-swizzle K-major core-matrix layout
 // (8 rows x 16 B per core matrix): SBO = 128 B, LBO = rows * 16 B.
 #include <algorithm>
+#include <mutex>
 
 #include "gmg_internal.cuh"
 
@@ -520,8 +521,10 @@ __global__ void pack_vec_kernel(const float2* __restrict__ in, uint4* __restrict
   const int64_t total = (int64_t)V * Kc * Rp;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const int r = (int)(e % Rp);
-    const int kc = (int)((e / Rp) % Kc);
+    // K chunk fastest: the Kc threads of one (site, RHS) read its row of N
+    // complex numbers contiguously; a warp's writes are Kc runs of 16 B x RHS
+    const int kc = (int)(e % Kc);
+    const int r = (int)((e / Kc) % Rp);
     const int64_t s = e / ((int64_t)Rp * Kc);
     uint16_t hr[8], hi[8];
     if (r < R) {
@@ -595,6 +598,8 @@ gmg_status coarse_prepare_tc(gmg_coarse* h, int kind, cudaStream_t s) {
 
 namespace tc {
 
+constexpr int kMaxAttrDevices = 64;
+
 // Launch configuration shared by gmg_coarse_apply and gmg_coarse_apply_noalloc:
 // points per stage (3 when enough stages fit, else 1) and the stage count.
 // V output sites; site_map (nullable): link site of each output index; nbr [9][V]: input index per point.
@@ -638,10 +643,25 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, cons
   GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil: tile does not fit shared memory");
   const size_t smem = (size_t)stages * stage_bytes + (size_t)(2 * stages + 2 * kAccBufs + 1) * 8 + 16 + tables;
   auto kern = ctas == 2 ? coarse_mrhs_tc_kernel<2> : coarse_mrhs_tc_kernel<1>;
-  GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int dev = 0, nsm = 148;
+  // per device: the SM count, and the largest shared-memory size each kernel
+  // instantiation was opened to (the attribute only grows, so it is set again
+  // only for a larger request)
+  int dev = 0;
   GMG_CUDA(cudaGetDevice(&dev));
-  GMG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  static int nsm_of[kMaxAttrDevices] = {0};
+  static size_t smem_of[kMaxAttrDevices][2] = {{0}};
+  GMG_CHECK(dev < kMaxAttrDevices, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil: device index too large");
+  static std::mutex attr_mu;  // handles used from different host threads share these tables
+  int nsm = 0;
+  {
+    std::lock_guard<std::mutex> g(attr_mu);
+    if (!nsm_of[dev]) GMG_CUDA(cudaDeviceGetAttribute(&nsm_of[dev], cudaDevAttrMultiProcessorCount, dev));
+    nsm = nsm_of[dev];
+    if (smem_of[dev][ctas - 1] < smem) {
+      GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      smem_of[dev][ctas - 1] = smem;
+    }
+  }
   Params P;
   P.links = h->links_h.buf.as<uint16_t>();
   P.packed = reinterpret_cast<const uint16_t*>(packed);

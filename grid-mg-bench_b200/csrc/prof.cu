@@ -21,14 +21,29 @@ struct Rec {
 std::mutex g_mu;
 bool g_on = false;
 std::map<std::string, Rec> g_recs;
+std::vector<cudaEvent_t> g_pool;  // events returned by gmg_profile_read, reused
+
+cudaEvent_t take_event() {
+  {
+    std::lock_guard<std::mutex> g(g_mu);
+    if (!g_pool.empty()) {
+      cudaEvent_t e = g_pool.back();
+      g_pool.pop_back();
+      return e;
+    }
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
 }  // namespace
 
 bool prof_enabled() { return g_on; }
 
 KernelTimer::KernelTimer(const char* name, cudaStream_t s) : name_(name), s_(s) {
   if (!g_on) return;
-  cudaEventCreate(&a_);
-  cudaEventCreate(&b_);
+  a_ = take_event();
+  b_ = take_event();
   cudaEventRecord(a_, s_);
   active_ = true;
 }
@@ -62,8 +77,13 @@ extern "C" gmg_status gmg_profile_read(const char* kernel, double* total_ms, int
     GMG_CUDA(cudaEventSynchronize(e.second));
     GMG_CUDA(cudaEventElapsedTime(&ms, e.first, e.second));
     t += ms;
-    cudaEventDestroy(e.first);
-    cudaEventDestroy(e.second);
+  }
+  {
+    std::lock_guard<std::mutex> g(gmg::g_mu);
+    for (auto& e : ev) {
+      gmg::g_pool.push_back(e.first);
+      gmg::g_pool.push_back(e.second);
+    }
   }
   *total_ms = t;
   *launches = (int64_t)ev.size();
