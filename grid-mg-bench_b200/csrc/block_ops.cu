@@ -142,11 +142,14 @@ gmg_status agg_prepare_f32(gmg_agg* h, cudaStream_t s) {
 // `mask` (nullable, int8 per fine site) restricts the sum to a face / parity
 // subset as the masked LUTs of CoarsenOperator do (...DirsaveLut.h:985-1005).
 // ---------------------------------------------------------------------------
+// `sel` (nullable, nsel entries): the in-block site indices the sum runs over,
+// the same for every block (a face of the block); without it all bv sites.
 template <class T, int TR, int TB, int KS>
 __global__ void __launch_bounds__(256) project_kernel(
     const typename ctype<T>::t* __restrict__ basis, const int32_t* __restrict__ blk_sites,
     const typename ctype<T>::t* __restrict__ fine, typename ctype<T>::t* __restrict__ coarse,
-    int Vc, int N, int dof, int bv, int nrhs, const int8_t* __restrict__ mask, int accumulate) {
+    int Vc, int N, int dof, int bv, int nrhs, const int8_t* __restrict__ mask, int accumulate,
+    const int32_t* __restrict__ sel, int nsel) {
   typedef typename ctype<T>::t Cx;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int KC = KS * dof;
@@ -164,18 +167,21 @@ __global__ void __launch_bounds__(256) project_kernel(
 #pragma unroll
       for (int i = 0; i < TB; ++i) acc[j][i] = Cx{0, 0};
     const Cx* Vb = basis + (int64_t)c * N * K;
-    for (int sb0 = 0; sb0 < bv; sb0 += KS) {
-      const int ns = min(KS, bv - sb0);
+    const int nsites = sel ? nsel : bv;
+    for (int sb0 = 0; sb0 < nsites; sb0 += KS) {
+      const int ns = min(KS, nsites - sb0);
       const int kc = ns * dof;
       __syncthreads();
       for (int e = t; e < N * kc; e += blockDim.x) {
         const int i = e / kc, kk = e % kc;
-        VT[kk * N + i] = Vb[(int64_t)i * K + (int64_t)sb0 * dof + kk];
+        const int sl = kk / dof, a = kk % dof;
+        const int sb = sel ? sel[sb0 + sl] : sb0 + sl;
+        VT[kk * N + i] = Vb[(int64_t)i * K + (int64_t)sb * dof + a];
       }
       for (int e = t; e < ns * R * dof; e += blockDim.x) {
         const int sl = e / (R * dof), rem = e % (R * dof);
         const int r = rem / dof, a = rem % dof;
-        const int sf = blk_sites[(int64_t)c * bv + sb0 + sl];
+        const int sf = blk_sites[(int64_t)c * bv + (sel ? sel[sb0 + sl] : sb0 + sl)];
         Cx v = fine[((int64_t)sf * nrhs + r) * dof + a];
         if (mask && !mask[sf]) v = Cx{0, 0};
         FT[(sl * dof + a) * R + r] = v;
@@ -221,7 +227,8 @@ __global__ void __launch_bounds__(256) project_kernel(
 
 template <class T, int TR, int TB, int KS>
 static gmg_status launch_project(gmg_agg* h, const void* basis, int nrhs, const void* fine,
-                                 void* coarse, const int8_t* mask, int accumulate, cudaStream_t s) {
+                                 void* coarse, const int8_t* mask, int accumulate, cudaStream_t s,
+                                 const int32_t* sel = nullptr, int nsel = 0) {
   typedef typename ctype<T>::t Cx;
   const int N = h->N, R = nrhs;
   const int ntiles = ((N + TB - 1) / TB) * ((R + TR - 1) / TR);
@@ -236,7 +243,7 @@ static gmg_status launch_project(gmg_agg* h, const void* basis, int nrhs, const 
   KernelTimer kt("project", s);
   kern<<<grid, threads, smem, s>>>(reinterpret_cast<const Cx*>(basis), h->blk_sites.as<int32_t>(),
                                    reinterpret_cast<const Cx*>(fine), reinterpret_cast<Cx*>(coarse),
-                                   Vc, N, h->dof, h->bv, nrhs, mask, accumulate);
+                                   Vc, N, h->dof, h->bv, nrhs, mask, accumulate, sel, nsel);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
@@ -256,6 +263,16 @@ gmg_status agg_project(gmg_agg* h, int compute, int vec_prec, int nrhs, const vo
     return launch_project<float, 1, 2, 4>(h, h->basis_blk_f.p, nrhs, fine, coarse, nullptr, 0, s);
   }
   return fail(GMG_ERR_UNSUPPORTED, "project: unsupported precision");
+}
+
+// FP64 projection over a subset of every block's sites (sel: nsel in-block
+// indices on the device, the same for all blocks), used for the face terms of
+// the coarse-operator construction
+gmg_status agg_project_sel_f64(gmg_agg* h, int nrhs, const double* fine, double* coarse, const int32_t* sel,
+                               int nsel, cudaStream_t s) {
+  if (nrhs >= 4)
+    return launch_project<double, 4, 4, 4>(h, h->basis_blk.p, nrhs, fine, coarse, nullptr, 0, s, sel, nsel);
+  return launch_project<double, 1, 2, 4>(h, h->basis_blk.p, nrhs, fine, coarse, nullptr, 0, s, sel, nsel);
 }
 
 // masked FP64 single-RHS projection used by the coarse-operator construction

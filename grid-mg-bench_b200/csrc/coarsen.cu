@@ -22,6 +22,8 @@ namespace gmg {
 
 gmg_status agg_project_masked_f64(gmg_agg* h, int nrhs, const double* fine, double* coarse,
                                   const int8_t* mask, cudaStream_t s);
+gmg_status agg_project_sel_f64(gmg_agg* h, int nrhs, const double* fine, double* coarse, const int32_t* sel,
+                               int nsel, cudaStream_t s);
 
 // field[sf][r][a] = basis_blk[c][i0 + r][sb*dof + a]
 __global__ void basis_gather_kernel(const double2* __restrict__ basis_blk, const int32_t* __restrict__ blk_sites,
@@ -122,9 +124,14 @@ static gmg_status coarsen_generic(gmg_coarse* out, gmg_agg* agg, const FineOpRef
   GMG_TRY(out->links_ref.alloc(sizeof(double2) * 9 * Vc * N * N));
   GMG_CUDA(cudaMemsetAsync(out->links_ref.p, 0, sizeof(double2) * 9 * Vc * N * N, s));
 
-  // batch of basis vectors treated as right-hand sides (bounded to ~1 GB per field)
+  // batch of basis vectors treated as right-hand sides: the projections reuse
+  // each basis panel across the batch, so the batch is as large as four fields
+  // of it allow in a third of the free device memory (at most 16 GB)
+  size_t free_b = 0, total_b = 0;
+  GMG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const double cap = std::min(16.0e9, (double)free_b / 3.0) / 4.0;
   int nb = N;
-  while (nb > 1 && (double)Vf * nb * dof * 16.0 > 1.0e9) nb = (nb + 1) / 2;
+  while (nb > 1 && (double)Vf * nb * dof * 16.0 > cap) nb = (nb + 1) / 2;
   const size_t fbytes = sizeof(double2) * (size_t)Vf * nb * dof;
   DevBuf phi, w1, w2, w3, proj, masks;
   GMG_TRY(phi.alloc(fbytes));
@@ -137,6 +144,25 @@ static gmg_status coarsen_generic(gmg_coarse* out, gmg_agg* agg, const FineOpRef
   GMG_TRY(masks.alloc(hm.size()));
   GMG_CUDA(cudaMemcpyAsync(masks.p, hm.data(), hm.size(), cudaMemcpyHostToDevice, s));
   const int8_t* face = masks.as<int8_t>();
+  // in-block indices of each backward face (local x_mu == 0): the face
+  // projections sum over those sites only, the same sites the face masks keep
+  std::vector<int32_t> hsel;
+  int nsel[4];
+  for (int d = 0; d < 4; ++d) {
+    nsel[d] = 0;
+    for (int k = 0; k < agg->bv; ++k) {
+      int t = k, lc[4];
+      for (int q = 0; q < 4; ++q) { lc[q] = t % agg->b[q]; t /= agg->b[q]; }
+      if (lc[d] == 0) {
+        hsel.push_back(k);
+        ++nsel[d];
+      }
+    }
+  }
+  DevBuf sel;
+  GMG_TRY(sel.alloc(sizeof(int32_t) * hsel.size()));
+  GMG_CUDA(cudaMemcpyAsync(sel.p, hsel.data(), sizeof(int32_t) * hsel.size(), cudaMemcpyHostToDevice, s));
+  const int sel_off[4] = {0, nsel[0], nsel[0] + nsel[1], nsel[0] + nsel[1] + nsel[2]};
   const int8_t* even = face + 4 * Vf;
   double2* A = out->links_ref.as<double2>();
   const int width = nb * dof;
@@ -150,7 +176,8 @@ static gmg_status coarsen_generic(gmg_coarse* out, gmg_agg* agg, const FineOpRef
     GMG_CUDA(cudaGetLastError());
     for (int p = 4; p < 8; ++p) {
       GMG_TRY(op.mdir(p, cur, phi.as<double>(), w1.as<double>(), s));
-      GMG_TRY(agg_project_masked_f64(agg, cur, w1.as<double>(), proj.as<double>(), face + (p - 4) * Vf, s));
+      GMG_TRY(agg_project_sel_f64(agg, cur, w1.as<double>(), proj.as<double>(), sel.as<int32_t>() + sel_off[p - 4],
+                                  nsel[p - 4], s));
       link_scatter_kernel<<<gsz(Vc * cur * N), 256, 0, s>>>(proj.as<double2>(), A + (int64_t)p * Vc * N * N,
                                                              Vc, N, i0, cur);
       GMG_CUDA(cudaGetLastError());
