@@ -126,10 +126,11 @@ static gmg_status coarsen_generic(gmg_coarse* out, gmg_agg* agg, const FineOpRef
 
   // batch of basis vectors treated as right-hand sides: the projections reuse
   // each basis panel across the batch, so the batch is as large as four fields
-  // of it allow in a third of the free device memory (at most 16 GB)
+  // of it allow in a third of the free device memory (at most 40 GB: the
+  // whole basis of 40 vectors at 32^4)
   size_t free_b = 0, total_b = 0;
   GMG_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  const double cap = std::min(16.0e9, (double)free_b / 3.0) / 4.0;
+  const double cap = std::min(40.0e9, (double)free_b / 3.0) / 4.0;
   int nb = N;
   while (nb > 1 && (double)Vf * nb * dof * 16.0 > cap) nb = (nb + 1) / 2;
   const size_t fbytes = sizeof(double2) * (size_t)Vf * nb * dof;

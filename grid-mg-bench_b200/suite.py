@@ -185,12 +185,17 @@ def wilson_and_c4(T, hbm):
     del B
     torch.cuda.empty_cache()
     ag.Orthogonalise(passes=1)
-    cm = gmg.CoarsenedMatrix((8, 8, 8, 8), N)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    cm.CoarsenOperator(ag, w)
-    torch.cuda.synchronize()
-    t_c4 = time.perf_counter() - t0
+    # the first call also tunes the fine-operator kernels for its batch size
+    t_first = None
+    for _ in range(2):
+        cm = gmg.CoarsenedMatrix((8, 8, 8, 8), N)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cm.CoarsenOperator(ag, w)
+        torch.cuda.synchronize()
+        t_c4 = time.perf_counter() - t0
+        if t_first is None:
+            t_first = t_c4
     h2 = inputs.torch_gaussian((N // 2, 4096, N), 704)
     B2 = torch.zeros((N, 4096, N), dtype=torch.complex128, device="cuda")
     B2[: N // 2, :, : N // 2] = h2[:, :, : N // 2]
@@ -206,9 +211,10 @@ def wilson_and_c4(T, hbm):
     t_cc = time.perf_counter() - t0
     proj_flops = 2 * 8.0 * 3072 * N * N * 4096
     fine_flops = N * V * (4 * 144 + 2 * 1824) * 1.0
-    line("C4 CoarsenOperator 32^4 -> 8^4 (nbasis 40) and 8^4 -> 4^4", seconds=t_c4, coarse_of_coarse_seconds=t_cc,
+    line("C4 CoarsenOperator 32^4 -> 8^4 (nbasis 40) and 8^4 -> 4^4", seconds=t_c4, first_call_seconds=t_first,
+         coarse_of_coarse_seconds=t_cc,
          algorithmic_flops=proj_flops + fine_flops, achieved_tflops=(proj_flops + fine_flops) / t_c4 / 1e12,
-         note="FP64; unfused backward Mdir + masked projections per batch of basis vectors")
+         note="FP64; backward Mdir + face-site projections per batch of basis vectors; seconds: second call")
 
 
 def c5_measure(nrhs=24, plain_rhs=2, forms=("mixed_bf16_mrhs", "mixed_f32_mrhs", "plain_f64_single_rhs")):
