@@ -355,13 +355,18 @@ def main():
 
     hbm, src = peaks()
     kavg_s = (kms.value / max(kn.value, 1)) * 1e-3
+    tc_ctas, tc_pps = ctypes.c_int(), ctypes.c_int()
+    gmg.lib().gmg_coarse_tuned_shape(cm._h, NRHS, 9, gmg.PREC[args.form], ctypes.byref(tc_ctas),
+                                     ctypes.byref(tc_pps))
     achieved = TC_KERNEL_BYTES / kavg_s / 1e9 if kn.value else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.form,
         "data": "synthetic (seeded Gaussian links with gamma5-hermitian structure, unit-Gaussian RHS)",
-        "config": config_dict(f"{args.form} operands on tcgen05 tensor cores, FP32 accumulation, FP32 vectors"),
+        "config": dict(config_dict(f"{args.form} operands on tcgen05 tensor cores, FP32 accumulation, FP32 vectors"),
+                       tile={"ctas_per_sm": tc_ctas.value, "points_per_stage": tc_pps.value,
+                             "chosen_by": "autotuner (first apply times every shape that fits)"}),
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None, "traffic": ncu_traffic(),

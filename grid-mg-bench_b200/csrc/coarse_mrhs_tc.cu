@@ -600,9 +600,44 @@ namespace tc {
 
 constexpr int kMaxAttrDevices = 64;
 
-// Launch configuration shared by gmg_coarse_apply and gmg_coarse_apply_noalloc:
-// points per stage (3 when enough stages fit, else 1) and the stage count.
+// Launch shape of the stencil: CTAs per SM (1 or 2), stencil points per stage
+// and the stage count that fills the shared memory of one CTA.
+struct Shape {
+  int ctas = 0, pps = 0, stages = 0;
+  uint32_t stage_bytes = 0;
+  size_t smem = 0;
+};
+
+// barriers (<= 2*32+9), TMEM slot + flag, neighbour and link-site tables of the two producers
+constexpr size_t kTables = 2 * 32 * 9 * 4 + 2 * 32 * 4;
+constexpr size_t kFixed = 80 * 8 + 16 + kTables;
+
+// the shape (ctas, pps) when it fits: TMEM accumulators of all CTAs of an SM in
+// its 512 columns, at least 2 stages (an even count: two producers)
+static bool make_shape(int ctas, int pps, int npts, uint32_t per_point, uint32_t ncols, Shape* out) {
+  if (npts % pps) return false;
+  if ((uint32_t)ctas * ncols > 512) return false;
+  const size_t cap = ctas == 2 ? 233472 / 2 - 1024 : 227 * 1024;
+  const uint32_t stage_bytes = (uint32_t)pps * per_point;
+  const int stages = (int)std::min<size_t>(32, (cap - kFixed) / stage_bytes) & ~1;
+  if (stages < 2) return false;
+  out->ctas = ctas;
+  out->pps = pps;
+  out->stages = stages;
+  out->stage_bytes = stage_bytes;
+  out->smem = (size_t)stages * stage_bytes + (size_t)(2 * stages + 2 * kAccBufs + 1) * 8 + 16 + kTables;
+  return true;
+}
+
+// Launch configuration shared by gmg_coarse_apply and gmg_coarse_apply_noalloc.
 // V output sites; site_map (nullable): link site of each output index; nbr [9][V]: input index per point.
+// The shape is autotuned: the first call of a handle for a key (nbasis, padded
+// RHS count, output volume, point count, operand kind, site map or not) times
+// every shape that fits (one warm-up and two timed launches each, CUDA events
+// on the caller's stream) and keeps the fastest; calls while the stream is
+// being captured, and calls with `timed` false (the allocation-free entry),
+// use the kept shape or, before there is one, the largest points-per-stage with
+// 4 stages at two CTAs per SM.
 static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, const int32_t* site_map,
                                  const int32_t* nbr, int p0, int p1, bool g5, int kind, int nrhs,
                                  float* out, const int32_t* active, int R, bool timed, cudaStream_t s) {
@@ -611,41 +646,12 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, cons
   const int Kc = round_up(N, 16) / 8;
   const int Mp = 2 * N <= 64 ? 64 : 128;
   const uint32_t per_point = (uint32_t)Kc * Mp * 16 + (uint32_t)Kc * 2 * Rp * 16;
-  // barriers (<= 2*32+9), TMEM slot + flag, neighbour and link-site tables of the two producers
-  const size_t tables = 2 * 32 * 9 * 4 + 2 * 32 * 4;
-  const size_t fixed = 80 * 8 + 16 + tables;
   const int npts = p1 - p0;
-  // Two CTAs per SM (two MMA-issuing threads, two independent site chains)
-  // when both CTAs' TMEM accumulators fit the SM's 512 columns and each keeps
-  // at least 4 stages in half the shared memory; else one CTA with all of it.
   const uint32_t acc_cols = 2 * (uint32_t)Rp;
   const uint32_t nacc = std::min<uint32_t>(kAccBufs, 512u / acc_cols);
   uint32_t ncols = 32;
   while (ncols < nacc * acc_cols) ncols <<= 1;
-  int ctas = 1, pps = 1, stages = 0;
-  uint32_t stage_bytes = 0;
-  for (int c2 : {2, 1}) {
-    if (c2 == 2 && 2 * ncols > 512) continue;
-    const size_t budget = (c2 == 2 ? 233472 / 2 - 1024 : 227 * 1024) - fixed;
-    // points per stage: the largest of 4, 3, 2 dividing the point count that
-    // still leaves at least 4 stages, else 1
-    pps = 1;
-    for (int c : {4, 3, 2})
-      if (npts % c == 0 && budget / (c * per_point) >= 4) {
-        pps = c;
-        break;
-      }
-    stage_bytes = pps * per_point;
-    stages = (int)std::min<size_t>(32, budget / stage_bytes) & ~1;  // even: two producers
-    ctas = c2;
-    if (c2 == 1 || stages >= 4) break;
-  }
-  GMG_CHECK(stages >= 2, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil: tile does not fit shared memory");
-  const size_t smem = (size_t)stages * stage_bytes + (size_t)(2 * stages + 2 * kAccBufs + 1) * 8 + 16 + tables;
-  auto kern = ctas == 2 ? coarse_mrhs_tc_kernel<2> : coarse_mrhs_tc_kernel<1>;
-  // per device: the SM count, and the largest shared-memory size each kernel
-  // instantiation was opened to (the attribute only grows, so it is set again
-  // only for a larger request)
+
   int dev = 0;
   GMG_CUDA(cudaGetDevice(&dev));
   static int nsm_of[kMaxAttrDevices] = {0};
@@ -657,11 +663,8 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, cons
     std::lock_guard<std::mutex> g(attr_mu);
     if (!nsm_of[dev]) GMG_CUDA(cudaDeviceGetAttribute(&nsm_of[dev], cudaDevAttrMultiProcessorCount, dev));
     nsm = nsm_of[dev];
-    if (smem_of[dev][ctas - 1] < smem) {
-      GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      smem_of[dev][ctas - 1] = smem;
-    }
   }
+
   Params P;
   P.links = h->links_h.buf.as<uint16_t>();
   P.packed = reinterpret_cast<const uint16_t*>(packed);
@@ -680,18 +683,88 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, cons
   P.p0 = p0;
   P.p1 = p1;
   P.g5 = g5 ? 1 : 0;
-  P.stages = stages;
   P.kind = kind == GMG_BF16 ? 1 : 0;
-  P.pps = pps;
-  const int grid = std::min(V, nsm * ctas);
+
+  // one launch of shape sh (the shared-memory attribute of each instantiation
+  // only grows, so it is set again only for a larger request)
+  auto launch = [&](const Shape& sh) -> gmg_status {
+    auto kern = sh.ctas == 2 ? coarse_mrhs_tc_kernel<2> : coarse_mrhs_tc_kernel<1>;
+    {
+      std::lock_guard<std::mutex> g(attr_mu);
+      if (smem_of[dev][sh.ctas - 1] < sh.smem) {
+        GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
+        smem_of[dev][sh.ctas - 1] = sh.smem;
+      }
+    }
+    Params Q = P;
+    Q.stages = sh.stages;
+    Q.pps = sh.pps;
+    kern<<<std::min(V, nsm * sh.ctas), kThreads, sh.smem, s>>>(Q);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  };
+
+  const uint64_t key = (uint64_t)N | ((uint64_t)Rp << 8) | ((uint64_t)npts << 16) | ((uint64_t)P.kind << 20) |
+                       ((uint64_t)(site_map != nullptr) << 21) | ((uint64_t)V << 24);
+  Shape sh;
+  bool have = h->tc_force && make_shape(h->tc_force >> 8, h->tc_force & 0xff, npts, per_point, ncols, &sh);
+  auto it = h->tc_shape.find(key);
+  if (!have)
+    have = it != h->tc_shape.end() && make_shape(it->second >> 8, it->second & 0xff, npts, per_point, ncols, &sh);
+  if (!have) {
+    // candidates: every (ctas, pps) that fits, the heuristic choice first
+    Shape cand[8];
+    int ncand = 0;
+    for (int c2 : {2, 1})
+      for (int pp : {4, 3, 2, 1}) {
+        Shape t;
+        if (make_shape(c2, pp, npts, per_point, ncols, &t) && (pp == 1 || t.stages >= 4)) cand[ncand++] = t;
+      }
+    GMG_CHECK(ncand > 0, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil: tile does not fit shared memory");
+    sh = cand[0];
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    GMG_CUDA(cudaStreamIsCapturing(s, &cap));
+    if (timed && cap == cudaStreamCaptureStatusNone && ncand > 1) {
+      cudaEvent_t e0, e1;
+      GMG_CUDA(cudaEventCreate(&e0));
+      GMG_CUDA(cudaEventCreate(&e1));
+      float best = 1e30f;
+      gmg_status st = GMG_OK;
+      for (int ci = 0; ci < ncand; ++ci) {
+        const Shape& c = cand[ci];
+        st = launch(c);  // warm-up
+        if (st != GMG_OK) break;
+        cudaEventRecord(e0, s);
+        for (int k = 0; k < 2 && st == GMG_OK; ++k) st = launch(c);
+        if (st != GMG_OK) break;
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+          best = ms;
+          sh = c;
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      GMG_TRY(st);
+      h->tc_shape[key] = ((uint32_t)sh.ctas << 8) | (uint32_t)sh.pps;
+    }
+  }
   if (timed) {
     KernelTimer kt("coarse_mrhs_tc", s);
-    kern<<<grid, kThreads, smem, s>>>(P);
-  } else {
-    kern<<<grid, kThreads, smem, s>>>(P);
+    return launch(sh);
   }
-  GMG_CUDA(cudaGetLastError());
-  return GMG_OK;
+  return launch(sh);
+}
+
+// the tuned shape of a key, for reports: ctas << 8 | pps, or 0 when not tuned
+static uint32_t tuned_shape(gmg_coarse* h, int R, int npts, int kind) {
+  const uint64_t key = (uint64_t)h->N | ((uint64_t)round_up(R, 16) << 8) | ((uint64_t)npts << 16) |
+                       ((uint64_t)(kind == GMG_BF16 ? 1 : 0) << 20) | ((uint64_t)h->dims.vol() << 24);
+  auto it = h->tc_shape.find(key);
+  return it == h->tc_shape.end() ? 0u : it->second;
 }
 
 }  // namespace tc
@@ -793,6 +866,24 @@ static gmg_status noalloc_scratch(void** p) {
 
 }  // namespace tc
 }  // namespace gmg
+
+extern "C" gmg_status gmg_coarse_set_shape(gmg_coarse* h, int ctas, int points_per_stage) {
+  GMG_CHECK(h != nullptr, GMG_ERR_ARGUMENT, "gmg_coarse_set_shape: null handle");
+  GMG_CHECK((ctas == 0 && points_per_stage == 0) ||
+                ((ctas == 1 || ctas == 2) && points_per_stage >= 1 && points_per_stage <= 4),
+            GMG_ERR_ARGUMENT, "gmg_coarse_set_shape: ctas must be 1 or 2, points per stage 1 to 4 (0, 0: autotune)");
+  h->tc_force = ((uint32_t)ctas << 8) | (uint32_t)points_per_stage;
+  return GMG_OK;
+}
+
+extern "C" gmg_status gmg_coarse_tuned_shape(gmg_coarse* h, int nrhs, int npoints, gmg_prec compute, int* ctas,
+                                             int* points_per_stage) {
+  GMG_CHECK(h && ctas && points_per_stage, GMG_ERR_ARGUMENT, "gmg_coarse_tuned_shape: null argument");
+  const uint32_t v = gmg::tc::tuned_shape(h, nrhs, npoints, (int)compute);
+  *ctas = (int)(v >> 8);
+  *points_per_stage = (int)(v & 0xff);
+  return GMG_OK;
+}
 
 extern "C" gmg_status gmg_coarse_apply_noalloc(gmg_coarse* h, gmg_op op, int point, gmg_prec compute, int nrhs,
                                                const float* in, float* out, const int32_t* active, int n_active,

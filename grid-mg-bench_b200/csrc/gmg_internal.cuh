@@ -98,6 +98,8 @@ struct gmg_coarse {
   gmg::LinksF16 links_h;
   gmg::DevBuf scratch;     // per-handle temporary: packed tensor-core vectors
   gmg::DevBuf dev_err;     // int: first error code a kernel of this handle recorded
+  std::map<uint64_t, uint32_t> tc_shape;  // autotuned tensor-core stencil shape per key (ctas << 8 | pps)
+  uint32_t tc_force = 0;                  // forced shape (ctas << 8 | pps), 0: autotuned
   // red-black operator (coarse_rb.cu)
   gmg::DevBuf self_inv;    // complex<double> [V][N][N]: inverse of the self-stencil link
   gmg::DevBuf self_inv_f;  // complex<float> copy

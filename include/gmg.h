@@ -96,6 +96,19 @@ gmg_status gmg_coarse_apply(gmg_coarse* h, gmg_op op, int point, gmg_prec comput
                             gmg_prec vec_prec, int nrhs, const void* in, void* out,
                             const int32_t* active, int n_active, gmg_stream s);
 
+/* The launch shape the autotuner chose for the tensor-core stencil of this
+   handle: CTAs per SM and stencil points per stage, for an apply of nrhs
+   right-hand sides over npoints stencil points (9 for M) in `compute`
+   (GMG_BF16 / GMG_F16); 0, 0 before the first such apply.  The first apply
+   of each (nbasis, padded nrhs, volume, point count, operand kind) times every
+   shape that fits and keeps the fastest.  No counterpart in the reference. */
+gmg_status gmg_coarse_tuned_shape(gmg_coarse* h, int nrhs, int npoints, gmg_prec compute, int* ctas,
+                                  int* points_per_stage);
+/* Force the tensor-core stencil shape of this handle (CTAs per SM 1 or 2,
+   points per stage 1-4); 0, 0 restores autotuning.  A forced shape that does
+   not fit a call (the point count not a multiple of it, TMEM or shared memory
+   too small) falls back to the tuned one.  No counterpart in the reference. */
+gmg_status gmg_coarse_set_shape(gmg_coarse* h, int ctas, int points_per_stage);
 /* Allocation-free form of gmg_coarse_apply for the BF16 / F16 tensor-core
    path (no counterpart in the reference).  For callers that cannot let the
    library allocate while they run -- a solver loop that must not stall the

@@ -103,3 +103,39 @@ def test_tc_full_c2_size_against_fp64_gpu():
     a, b = 0.7 - 0.2j, -1.3 + 0.5j
     lin = run(cm, a * x + b * y, orc.OP_M, "bf16")
     assert orc.rel_dev_sq(a * got + b * run(cm, y, orc.OP_M, "bf16"), lin) < 4 * TOL["bf16"]
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (1, 3), (2, 1), (2, 3), (2, 4), (1, 2)])
+def test_tc_every_launch_shape(shape):
+    # every (CTAs per SM, points per stage) shape the autotuner may pick gives
+    # the oracle's result; a shape that does not divide the point count (4 or 2
+    # for the 9 points of M) falls back to the tuned one
+    dims, N, R = (4, 4, 4, 4), 32, 24
+    r = inputs.rng(stream=240 + 3 * shape[0] + shape[1])
+    A = inputs.random_links(dims, N, r)
+    x = inputs.gaussian_field((256, R, N), r)
+    cm = gmg.CoarsenedMatrix(dims, N)
+    cm.set_links(A)
+    cm.prepare("bf16")
+    assert gmg.lib().gmg_coarse_set_shape(cm._h, shape[0], shape[1]) == 0
+    ref = orc.coarse_apply(dims, A, x, orc.OP_M)
+    assert orc.rel_dev_sq(ref, run(cm, x, orc.OP_M, "bf16")) < TOL["bf16"]
+    assert gmg.lib().gmg_coarse_set_shape(cm._h, 0, 0) == 0
+
+
+def test_tc_autotuner_records_a_shape():
+    import ctypes
+    dims, N, R = (4, 4, 4, 4), 32, 32
+    r = inputs.rng(stream=251)
+    A = inputs.random_links(dims, N, r)
+    x = inputs.gaussian_field((256, R, N), r)
+    cm = gmg.CoarsenedMatrix(dims, N)
+    cm.set_links(A)
+    cm.prepare("bf16")
+    ref = orc.coarse_apply(dims, A, x, orc.OP_M)
+    assert orc.rel_dev_sq(ref, run(cm, x, orc.OP_M, "bf16")) < TOL["bf16"]
+    ctas, pps = ctypes.c_int(), ctypes.c_int()
+    assert gmg.lib().gmg_coarse_tuned_shape(cm._h, R, 9, gmg.BF16, ctypes.byref(ctas), ctypes.byref(pps)) == 0
+    assert ctas.value in (1, 2) and pps.value in (1, 3), (ctas.value, pps.value)
+    # a second call reuses the kept shape and gives the same result
+    assert orc.rel_dev_sq(ref, run(cm, x, orc.OP_M, "bf16")) < TOL["bf16"]
