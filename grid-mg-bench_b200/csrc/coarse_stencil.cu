@@ -269,13 +269,100 @@ __global__ void __launch_bounds__(576) coarse_1rhs_kernel(const typename cplx_t<
   }
 }
 
+// Single RHS with the site's links staged in shared memory: the CTA first
+// copies the (p1 - p0) N x N link matrices of its site with cp.async (every
+// 16-byte chunk in flight at once: one memory round trip instead of a
+// dependent chain per row), then thread (p, b) forms row b of point p from
+// shared memory, starting
+// its row at column (b + k) mod N so that the 16-byte reads of a quarter warp
+// fall in distinct banks (N a multiple of 8).
+template <class T>
+__global__ void __launch_bounds__(576) coarse_1rhs_smem_kernel(const typename cplx_t<T>::type* __restrict__ links,
+                                                               int link_pts, int pbase,
+                                                               const int32_t* __restrict__ site_map,
+                                                               const int32_t* __restrict__ nbr, int dag,
+                                                               const typename cplx_t<T>::type* __restrict__ in,
+                                                               typename cplx_t<T>::type* __restrict__ out, int V,
+                                                               int N, int nrhs, int slot, int p0, int p1, int g5) {
+  typedef typename cplx_t<T>::type C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int np = p1 - p0, NN = N * N;
+  C* Ls = reinterpret_cast<C*>(smem_raw);  // [np][N][N]
+  C* X = Ls + (size_t)np * NN;             // [9][N] neighbour vectors
+  C* part = X + 9 * N;                     // [9][N] partial rows
+  const int t = threadIdx.x;
+  const int p = t / N, b = t % N;  // blockDim = 9 N
+  const int half = N / 2;
+  for (int site = blockIdx.x; site < V; site += gridDim.x) {
+    const int64_t lsite = site_map ? site_map[site] : site;
+    // every 16-byte chunk of the site's links in flight at once (cp.async),
+    // one wait for all of them
+    const unsigned char* src = reinterpret_cast<const unsigned char*>(links + (lsite * link_pts + (p0 - pbase)) * NN);
+    const int nchunk = (int)(np * NN * sizeof(C) / 16);
+    const uint32_t dst0 = (uint32_t)__cvta_generic_to_shared(Ls);
+    for (int e = t; e < nchunk; e += blockDim.x)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst0 + 16u * e), "l"(src + 16 * (size_t)e)
+                   : "memory");
+    asm volatile("cp.async.commit_group;\n cp.async.wait_group 0;" ::: "memory");
+    if (p >= p0 && p < p1) {
+      const int nb = nbr ? nbr[(int64_t)p * V + site] : site;
+      C v = in[((int64_t)nb * nrhs + slot) * N + b];
+      if (g5 && b >= half) { v.x = -v.x; v.y = -v.y; }
+      X[p * N + b] = v;
+    }
+    __syncthreads();
+    C acc{0, 0};
+    if (p >= p0 && p < p1) {
+      const C* Mp = Ls + (size_t)(p - p0) * NN;
+      const C* xp = X + p * N;
+      int bb = b;
+      if (dag) {  // row b of A^dag: conj(A[bb][b])
+        for (int k = 0; k < N; ++k) {
+          acc = cmul_add(acc, cconj(Mp[bb * N + b]), xp[bb]);
+          bb = bb + 1 == N ? 0 : bb + 1;
+        }
+      } else {
+        const C* row = Mp + b * N;
+        for (int k = 0; k < N; ++k) {
+          acc = cmul_add(acc, row[bb], xp[bb]);
+          bb = bb + 1 == N ? 0 : bb + 1;
+        }
+      }
+    }
+    part[p * N + b] = acc;
+    __syncthreads();
+    if (t < N) {
+      C o{0, 0};
+      for (int q = p0; q < p1; ++q) {
+        o.x += part[q * N + t].x;
+        o.y += part[q * N + t].y;
+      }
+      if (g5 && t >= half) { o.x = -o.x; o.y = -o.y; }
+      out[((int64_t)site * nrhs + slot) * N + t] = o;
+    }
+    __syncthreads();
+  }
+}
+
 template <class T>
 static gmg_status launch_1rhs(const LinkSel& L, const void* in, void* out, int V, int N,
                               int nrhs, int slot, int p0, int p1, int g5, cudaStream_t s) {
   typedef typename cplx_t<T>::type C;
   const int threads = 9 * N;
-  const size_t smem = sizeof(C) * 18 * (size_t)N;
   KernelTimer kt("coarse_simt", s);
+  // links staged in shared memory when they fit two CTAs per SM
+  const size_t smem_staged = sizeof(C) * ((size_t)(p1 - p0) * N * N + 18 * (size_t)N);
+  if (N % 8 == 0 && smem_staged <= 100 * 1024) {
+    if (smem_staged > 48 * 1024)
+      GMG_CUDA(cudaFuncSetAttribute(coarse_1rhs_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_staged));
+    coarse_1rhs_smem_kernel<T><<<V, threads, smem_staged, s>>>(
+        reinterpret_cast<const C*>(L.links), L.link_pts, L.pbase, L.site_map, L.nbr, L.dag,
+        reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), V, N, nrhs, slot, p0, p1, g5);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  }
+  const size_t smem = sizeof(C) * 18 * (size_t)N;
   coarse_1rhs_kernel<T><<<V, threads, smem, s>>>(reinterpret_cast<const C*>(L.links), L.link_pts, L.pbase, L.site_map,
                                                  L.nbr, L.dag, reinterpret_cast<const C*>(in),
                                                  reinterpret_cast<C*>(out), V, N, nrhs, slot, p0, p1, g5);
