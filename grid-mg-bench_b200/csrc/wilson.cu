@@ -1135,14 +1135,23 @@ static gmg_status launch_site(gmg_wilson* h, int op, int dir, int disp, int vec_
   return GMG_OK;
 }
 
-// tile kernel: kTileSites sites x min(nrhs, 16) threads per CTA; MINB: CTAs
+// tile kernel: kTileSites sites x rt threads per CTA (rt <= 16); MINB: CTAs
 // per SM the register allocation must allow (FP32: 2 or 3)
 template <bool DOTS, int MINB = 2>
 static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs, const void* in,
                               void* out, double2* d1, double2* d2, cudaStream_t s) {
   const int V = (int)h->dims.vol();
   const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
-  const int rt = std::min(nrhs, 16);
+  // threads per site: the largest divisor of nrhs up to 16, so that every
+  // thread of a site handles the same number of RHS (24 -> 12 x 2); nrhs
+  // without a divisor of 8 or more above 16 uses 16 (the last round uneven)
+  int rt = 1;
+  for (int c = std::min(nrhs, 16); c >= 1; --c)
+    if (nrhs % c == 0) {
+      rt = c;
+      break;
+    }
+  if (nrhs > 16 && rt < 8) rt = 16;
   const int tiles = (V + kTileSites - 1) / kTileSites;
   const int g = std::min(tiles, 148 * 16);
   const size_t dots = DOTS ? sizeof(double) * 3 * (size_t)nrhs : 0;

@@ -281,7 +281,7 @@ VARIANTS = ["site", "tile", "quad", "staged"]
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
-@pytest.mark.parametrize("nrhs", [4, 7, 12, 13, 20])
+@pytest.mark.parametrize("nrhs", [4, 7, 12, 13, 17, 20, 24])
 @pytest.mark.parametrize("op", ["M", "Mdag", "Mdiag"])
 def test_wilson_multi_rhs_variants(wil, forced, variant, nrhs, op):
     # tile: 16 sites x min(nrhs, 16) threads; quad: rt = largest divisor of nrhs
