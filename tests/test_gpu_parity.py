@@ -209,6 +209,24 @@ def test_project_promote_f64(agg8, nrhs):
     assert orc.rel_dev_sq(orc.block_promote(fd, cd, B, vc), host(fo)) < TOL64
 
 
+@pytest.mark.parametrize("fd,cd,dof,N,R", [((8, 8, 8, 8), (2, 2, 2, 2), 12, 24, 12),
+                                          ((8, 8, 8, 8), (4, 4, 4, 4), 12, 40, 20),
+                                          ((4, 4, 4, 4), (2, 2, 2, 2), 16, 16, 4),
+                                          ((4, 4, 4, 4), (2, 2, 2, 2), 40, 40, 40)])
+def test_project_f64_shapes(fd, cd, dof, N, R):
+    # FP64 projections of fine-site (dof 12) and coarse-site (dof 16, 40)
+    # aggregations: several K chunks per block, register tiles cut by nbasis
+    # and nrhs that are not multiples of the tile
+    Vf = int(np.prod(fd))
+    B = inputs.gaussian_field((N, Vf, dof), inputs.rng(stream=180 + N))
+    ag = gmg.Aggregation(fd, cd, dof, N)
+    ag.set_basis(B)
+    f = inputs.gaussian_field((Vf, R, dof), inputs.rng(stream=181 + R))
+    c = torch.zeros((int(np.prod(cd)), R, N), dtype=torch.complex128, device=DEV)
+    ag.ProjectToSubspace(dev(f), c)
+    assert orc.rel_dev_sq(orc.block_project(fd, cd, B, f), host(c)) < TOL64
+
+
 def test_project_promote_f32(agg8):
     fd, cd, B0, ag = agg8
     B = orc.block_orthonormalise(fd, cd, B0, passes=1)
