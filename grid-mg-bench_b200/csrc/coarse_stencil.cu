@@ -466,7 +466,33 @@ __global__ void layout_links_kernel(const double2* __restrict__ in, double2* __r
     else out[e] = in[spin];
   }
 }
+
+// vectors: flat index n = s * Nc_c + c <-> spin form [s][c] (Layout_converters.h:92-139)
+__global__ void layout_vectors_kernel(const double2* __restrict__ in, double2* __restrict__ out, int64_t rows,
+                                      int N, int ncs, int inverse) {
+  const int ncc = N / ncs;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < rows * N;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = e / N;
+    const int n = (int)(e % N), sp = n / ncc, c = n % ncc;
+    const int64_t spin = row * N + (int64_t)sp * ncc + c;  // [row][s][c]: the same order as the flat index
+    if (!inverse) out[spin] = in[e];
+    else out[e] = in[spin];
+  }
+}
 }  // namespace gmg
+
+extern "C" gmg_status gmg_layout_vectors(int64_t rows, int nbasis, int ncs, const double* in, double* out,
+                                         int inverse, gmg_stream s) {
+  GMG_CHECK(in && out && in != out, GMG_ERR_ARGUMENT, "gmg_layout_vectors: bad pointers");
+  GMG_CHECK(rows > 0 && nbasis > 0 && ncs > 0 && nbasis % ncs == 0, GMG_ERR_ARGUMENT,
+            "gmg_layout_vectors: nbasis must be a multiple of the coarse spin count");
+  const int64_t n = rows * nbasis;
+  gmg::layout_vectors_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 148 * 32), 256, 0, gmg::S(s)>>>(
+      reinterpret_cast<const double2*>(in), reinterpret_cast<double2*>(out), rows, nbasis, ncs, inverse);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
 
 extern "C" gmg_status gmg_layout_links(int64_t V, int nbasis, int ncs, const double* in, double* out,
                                        int inverse, gmg_stream s) {

@@ -455,6 +455,15 @@ def point_from_dir_disp(ndim, dirs_faster, d, disp):
     return lib().gmg_point_from_dir_disp(ndim, int(dirs_faster), d, disp)
 
 
+def layout_vectors(vecs, ncs, inverse=False):
+    """Device coarse vectors [..][N] (complex128 tensor) flat <-> Rework spin-split layout."""
+    out = torch.empty_like(vecs)
+    N = vecs.shape[-1]
+    rows = vecs.numel() // N
+    _chk(lib().gmg_layout_vectors(ctypes.c_int64(rows), N, ncs, _ptr(vecs), _ptr(out), int(inverse), _stream()))
+    return out
+
+
 def layout_links(links, ncs, inverse=False):
     """Device links [V][N][N] (complex128 tensor) flat <-> Rework spin-split layout."""
     out = torch.empty_like(links)

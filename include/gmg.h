@@ -341,6 +341,14 @@ gmg_status gmg_mg_level(gmg_mg* h, int level, gmg_coarse** op, gmg_agg** agg);
 /* ------------------------------------------------------------------------ */
 gmg_status gmg_layout_links(int64_t V, int nbasis, int ncs, const double* in, double* out,
                             int inverse, gmg_stream s);
+/* Rework layout map of coarse vectors (Layout_converters.h:92-139): flat
+   basis index n = s*Nc_c + c <-> (s, c), rows = sites x nrhs.  In the
+   lexicographic [row][N] buffers of this library both forms have the same
+   memory order, so the map is a copy; it is kept as an entry so that an
+   adapter converting Grid fields calls it where the reference calls
+   convertLayout. */
+gmg_status gmg_layout_vectors(int64_t rows, int nbasis, int ncs, const double* in, double* out,
+                              int inverse, gmg_stream s);
 
 /* ------------------------------------------------------------------------ */
 /* Live kernel timing (replaces the reference's Profiler stopwatches,        */

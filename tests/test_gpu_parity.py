@@ -147,6 +147,14 @@ def test_layout_links_matches_oracle():
     assert torch.equal(gmg.layout_links(spin, 2, inverse=True), t)
 
 
+def test_layout_vectors_matches_oracle():
+    v = inputs.gaussian_field((16, 3, 24), inputs.rng(stream=107))
+    t = dev(v)
+    spin = gmg.layout_vectors(t, 2)
+    assert np.array_equal(host(spin).reshape(-1, 24), orc.layout_vec_flat_to_spin(v.reshape(-1, 24), 2))
+    assert torch.equal(gmg.layout_vectors(spin, 2, inverse=True), t)
+
+
 # ------------------------------------------------------------------ aggregation
 @pytest.fixture(scope="module")
 def agg8():
