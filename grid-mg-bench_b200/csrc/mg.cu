@@ -21,6 +21,8 @@
 #include <cstring>
 #include <vector>
 
+#include <map>
+
 #include "mg_internal.cuh"
 
 typedef std::complex<double> zc;
@@ -41,6 +43,11 @@ struct MGLevel {
   VecBuf V0, Z0, kw, kt;    // Krylov basis (m+1), flexible directions (m), temporaries
   VecBuf mr_r, mr_Ar, mr_t; // MR smoother
   VecBuf bc, xc;            // right-hand side / solution of this level inside the cycle above
+  // device state of this level's solver inside a captured K-cycle: Hessenberg
+  // [R][m+1][m], rhs g [R][m+1], Givens cs / sn [R][m], residual estimates [R],
+  // solution coefficients y [m][R], counters {iterations, steps of the cycle},
+  // |b|^2 and |r0|^2 per RHS
+  DevBuf gH, gG, gCs, gSn, gRes, gY, gCtr, gBn, gBeta;
   ~MGLevel() {
     if (c) gmg_coarse_destroy(c);
     if (agg) gmg_agg_destroy(agg);
@@ -62,7 +69,16 @@ struct gmg_mg {
   gmg::VecBuf oV0, oZ0, ow, ot64, otz, obb, oxx;
   gmg::DevBuf oidx;
   bool outer_ready = false;
+  // captured K-cycle graphs per active-batch size (params.graph), their output
+  // buffer and the capture streams of the nested conditional bodies
+  std::map<int, cudaGraphExec_t> kgraph;
+  gmg::VecBuf ogz;
+  cudaStream_t cap_st[8] = {};
+  bool graph_broken = false;
   ~gmg_mg() {
+    for (auto& g : kgraph) cudaGraphExecDestroy(g.second);
+    for (auto& st : cap_st)
+      if (st) cudaStreamDestroy(st);
     for (auto* l : L) delete l;
     if (hpin) cudaFreeHost(hpin);
   }
@@ -435,6 +451,327 @@ gmg_status kcycle(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s) {
   return mr_smooth(h, l, in, out, h->P.smoother_iters, s);
 }
 
+// ------------------------------------------------------------- captured K-cycle
+// The coarse-level solvers of a K-cycle captured as a CUDA graph.  The
+// Hessenberg column, the Givens rotations and the convergence test of every
+// RHS run in small device kernels (one thread per RHS) instead of on the host;
+// every Arnoldi step and every restart cycle is a conditional IF node, switched
+// on by the kernel that ends the step before it (or starts the cycle) while the
+// tolerance and the iteration limit are not met, so a replay takes the same
+// early exits as the host-driven solver.  The step index is fixed in each
+// captured body, so the existing vector kernels are captured unchanged.
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 zconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 zadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 zsub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double zabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ double2 zdiv(double2 a, double2 b) {
+  const double d = zabs2(b);
+  return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+
+// start of a restart cycle: g = |r0| e_0, residual estimates, step counter 0;
+// the first step runs while some RHS is above tol and iterations remain
+__global__ void cycle_init_kernel(const double2* __restrict__ beta2, const double2* __restrict__ bn2, int R, int m,
+                                  double2* __restrict__ g, double* __restrict__ res, double tol, int* __restrict__ ctr,
+                                  int maxit, cudaGraphConditionalHandle first_step) {
+  const int r = threadIdx.x;
+  int ok = 1;
+  if (r < R) {
+    const double beta = sqrt(fmax(beta2[r].x, 0.0)), bn = sqrt(fmax(bn2[r].x, 1e-300));
+    double2* gr = g + (size_t)r * (m + 1);
+    gr[0] = make_double2(beta, 0.0);
+    for (int k = 1; k <= m; ++k) gr[k] = make_double2(0.0, 0.0);
+    res[r] = beta / bn;
+    ok = res[r] <= tol;
+  }
+  const int conv = __syncthreads_and(ok);
+  if (r == 0) {
+    ctr[1] = 0;
+    cudaGraphSetConditional(first_step, (!conv && ctr[0] < maxit) ? 1u : 0u);
+  }
+}
+
+// end of Arnoldi step j: Hessenberg column j = the two Gram-Schmidt passes'
+// coefficients and |w|, previous rotations, a new rotation, the residual
+// estimate; the next step runs while some RHS is above tol and iterations remain
+__global__ void arnoldi_step_kernel(const double2* __restrict__ dh, const double2* __restrict__ dh2,
+                                    const double2* __restrict__ dw, int j, int m, int R, double2* __restrict__ H,
+                                    double2* __restrict__ g, double2* __restrict__ cs, double2* __restrict__ sn,
+                                    double* __restrict__ res, const double2* __restrict__ bn2, double tol,
+                                    int* __restrict__ ctr, int maxit, cudaGraphConditionalHandle next_step,
+                                    int has_next) {
+  const int r = threadIdx.x;
+  int ok = 1;
+  if (r < R) {
+    double2* Hr = H + (size_t)r * (m + 1) * m;
+    for (int i = 0; i <= j; ++i) Hr[i * m + j] = zadd(dh[(size_t)i * R + r], dh2[(size_t)i * R + r]);
+    Hr[(j + 1) * m + j] = make_double2(sqrt(fmax(dw[r].x, 0.0)), 0.0);
+    for (int i = 0; i < j; ++i) {
+      const double2 c = cs[r * m + i], sg = sn[r * m + i];
+      const double2 a = Hr[i * m + j], bq = Hr[(i + 1) * m + j];
+      Hr[i * m + j] = zadd(zmul(zconj(c), a), zmul(zconj(sg), bq));
+      Hr[(i + 1) * m + j] = zsub(zmul(c, bq), zmul(sg, a));
+    }
+    const double2 a = Hr[j * m + j], hn = Hr[(j + 1) * m + j];
+    const double den = sqrt(zabs2(a) + zabs2(hn));
+    double2 c = make_double2(1.0, 0.0), sg = make_double2(0.0, 0.0);
+    if (den > 0.0) {
+      c = make_double2(a.x / den, a.y / den);
+      sg = make_double2(hn.x / den, hn.y / den);
+    }
+    cs[r * m + j] = c;
+    sn[r * m + j] = sg;
+    Hr[j * m + j] = zadd(zmul(zconj(c), a), zmul(zconj(sg), hn));
+    Hr[(j + 1) * m + j] = make_double2(0.0, 0.0);
+    double2* gr = g + (size_t)r * (m + 1);
+    const double2 gj = gr[j];
+    gr[j] = zmul(zconj(c), gj);
+    gr[j + 1] = make_double2(-(sg.x * gj.x - sg.y * gj.y), -(sg.x * gj.y + sg.y * gj.x));
+    res[r] = sqrt(zabs2(gr[j + 1])) / sqrt(fmax(bn2[r].x, 1e-300));
+    ok = res[r] <= tol;
+  }
+  const int conv = __syncthreads_and(ok);
+  if (r == 0) {
+    ctr[0] += 1;
+    ctr[1] = j + 1;
+    if (has_next) cudaGraphSetConditional(next_step, (!conv && ctr[0] < maxit) ? 1u : 0u);
+  }
+}
+
+// end of a restart cycle: y = H^-1 g over the steps taken (zero beyond), and
+// the next cycle runs when this one took a step and iterations remain (it
+// starts from the true residual, as the host-driven solver does)
+__global__ void cycle_finish_kernel(const double2* __restrict__ H, const double2* __restrict__ g, int R, int m,
+                                    const int* __restrict__ ctr, int maxit, double2* __restrict__ y,
+                                    cudaGraphConditionalHandle next_cycle, int has_next) {
+  const int r = threadIdx.x;
+  const int n = ctr[1];
+  if (r < R) {
+    const double2* Hr = H + (size_t)r * (m + 1) * m;
+    const double2* gr = g + (size_t)r * (m + 1);
+    for (int i = n - 1; i >= 0; --i) {
+      double2 acc = gr[i];
+      for (int k = i + 1; k < n; ++k) acc = zsub(acc, zmul(Hr[i * m + k], y[(size_t)k * R + r]));
+      const double2 d = Hr[i * m + i];
+      y[(size_t)i * R + r] = (d.x != 0.0 || d.y != 0.0) ? zdiv(acc, d) : make_double2(0.0, 0.0);
+    }
+    for (int i = n; i < m; ++i) y[(size_t)i * R + r] = make_double2(0.0, 0.0);
+  }
+  if (r == 0 && has_next) cudaGraphSetConditional(next_cycle, (n > 0 && ctr[0] < maxit) ? 1u : 0u);
+}
+
+// a conditional handle of the graph that stream s is capturing
+gmg_status cap_handle(cudaStream_t s, cudaGraphConditionalHandle* hnd) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  GMG_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr));
+  GMG_CHECK(st == cudaStreamCaptureStatusActive, GMG_ERR_STATE, "mg graph: stream is not capturing");
+  GMG_CUDA(cudaGraphConditionalHandleCreate(hnd, g, 0, cudaGraphCondAssignDefault));
+  return GMG_OK;
+}
+
+// an IF node on hnd at the capture point of s; its body is captured on body_s
+gmg_status cap_if_begin(cudaStream_t s, cudaGraphConditionalHandle hnd, cudaStream_t body_s) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  GMG_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = hnd;
+  p.conditional.type = cudaGraphCondTypeIf;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  GMG_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+  GMG_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  GMG_CUDA(cudaStreamBeginCaptureToGraph(body_s, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal));
+  return GMG_OK;
+}
+
+gmg_status cap_if_end(cudaStream_t body_s) {
+  cudaGraph_t g = nullptr;
+  GMG_CUDA(cudaStreamEndCapture(body_s, &g));
+  return GMG_OK;
+}
+
+// the restarted (F)GMRES of level l inside a captured K-cycle, on the capture
+// stream of nesting depth d; prec(in, out, tz, depth) captures the preconditioner
+template <class Prec>
+gmg_status fgmres_cap(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m, int maxit, double tol,
+                      Prec prec, bool flexible, int d) {
+  MGLevel& L = *h->L[l];
+  GMG_CHECK(d + 2 < 8, GMG_ERR_UNSUPPORTED, "mg graph: solvers nested too deep");
+  cudaStream_t s = h->cap_st[d];
+  const int R = b.R;
+  Vec V0 = K.V0.with_rhs(R), Z0 = K.Z0.with_rhs(R), w = K.w.with_rhs(R), t = K.t.with_rhs(R), tz = K.tz.with_rhs(R);
+  const int64_t vstride = V0.elems(), zstride = Z0.elems();
+  double2* bn2 = L.gBn.as<double2>();
+  double2* beta2 = L.gBeta.as<double2>();
+  int* ctr = L.gCtr.as<int>();
+  double2 *H = L.gH.as<double2>(), *G = L.gG.as<double2>(), *CS = L.gCs.as<double2>(), *SN = L.gSn.as<double2>();
+  double2* Y = L.gY.as<double2>();
+  double* RES = L.gRes.as<double>();
+  const int threads = (R + 31) / 32 * 32;
+  GMG_TRY(vec_multidot(b, 1, 0, b, bn2, nullptr, s));
+  GMG_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(int), s));
+  const int ncyc = std::max(1, (maxit + m - 1) / m);
+  std::vector<cudaGraphConditionalHandle> hcyc(ncyc, 0);
+  for (int c = 1; c < ncyc; ++c) GMG_TRY(cap_handle(s, &hcyc[c]));
+  for (int c = 0; c < ncyc; ++c) {
+    cudaStream_t sc = s;
+    int dc = d;
+    if (c > 0) {
+      GMG_TRY(cap_if_begin(s, hcyc[c], h->cap_st[d + 1]));
+      sc = h->cap_st[d + 1];
+      dc = d + 1;
+    }
+    // r0 = b - A x, |r0|, v_0
+    Vec v0 = nth(V0, 0);
+    GMG_TRY(apply_op(h, l, x, w, sc));
+    GMG_TRY(vec_xmy(b, w, sc));
+    GMG_TRY(vec_multidot(w, 1, 0, w, beta2, nullptr, sc));
+    std::vector<cudaGraphConditionalHandle> hit(m, 0);
+    for (int j = 0; j < m; ++j) GMG_TRY(cap_handle(sc, &hit[j]));
+    cycle_init_kernel<<<1, threads, 0, sc>>>(beta2, bn2, R, m, G, RES, tol, ctr, maxit, hit[0]);
+    GMG_CUDA(cudaGetLastError());
+    GMG_TRY(vec_scale_inv_norm(beta2, w, v0, sc));
+    for (int j = 0; j < m; ++j) {
+      cudaStream_t si = h->cap_st[dc + 1];
+      GMG_TRY(cap_if_begin(sc, hit[j], si));
+      Vec vj = nth(V0, j);
+      Vec zj = flexible ? nth(Z0, j) : vj;
+      if (flexible) GMG_TRY(prec(vj, zj, tz, dc + 1));
+      if (zj.prec != w.prec) {
+        GMG_TRY(vec_convert(zj, t, si));
+        GMG_TRY(apply_op(h, l, t, w, si));
+      } else {
+        GMG_TRY(apply_op(h, l, zj, w, si));
+      }
+      const size_t nc = (size_t)(j + 1) * R;
+      double2* dh = h->dscr.as<double2>();
+      double2* dh2 = dh + nc;
+      double2* dw = dh2 + nc;
+      GMG_TRY(vec_multidot(V0, j + 1, vstride, w, dh, nullptr, si));
+      GMG_TRY(vec_multiaxpy_dot(dh, V0, j + 1, vstride, w, si, -1.0, dh2, 1));
+      GMG_TRY(vec_multiaxpy_dot(dh2, V0, j + 1, vstride, w, si, -1.0, dw, 2));
+      Vec vn = nth(V0, j + 1);
+      GMG_TRY(vec_scale_inv_norm(dw, w, vn, si));
+      arnoldi_step_kernel<<<1, threads, 0, si>>>(dh, dh2, dw, j, m, R, H, G, CS, SN, RES, bn2, tol, ctr, maxit,
+                                                 j + 1 < m ? hit[j + 1] : hit[j], j + 1 < m ? 1 : 0);
+      GMG_CUDA(cudaGetLastError());
+      GMG_TRY(cap_if_end(si));
+    }
+    cycle_finish_kernel<<<1, threads, 0, sc>>>(H, G, R, m, ctr, maxit, Y, c + 1 < ncyc ? hcyc[c + 1] : hit[0],
+                                               c + 1 < ncyc ? 1 : 0);
+    GMG_CUDA(cudaGetLastError());
+    GMG_TRY(vec_multiaxpy(Y, flexible ? Z0 : V0, m, flexible ? zstride : vstride, x, sc, 1.0));
+    if (c > 0) GMG_TRY(cap_if_end(sc));
+  }
+  return GMG_OK;
+}
+
+gmg_status kcycle_cap(gmg_mg* h, int l, const Vec& in, Vec& out, int d);
+
+gmg_status coarse_solve_cap(gmg_mg* h, int lc, const Vec& b, Vec& x, int d) {
+  MGLevel& C = *h->L[lc];
+  const bool coarsest = lc == (int)h->L.size() - 1;
+  const gmg_mg_params& P = h->P;
+  GMG_TRY(zero(x, h->cap_st[d]));
+  Krylov K = level_krylov(C);
+  if (coarsest) {
+    auto none = [](const Vec&, Vec&, const Vec&, int) { return GMG_OK; };
+    return fgmres_cap(h, lc, b, x, K, C.m, P.coarsest_iters, P.coarsest_tol, none, false, d);
+  }
+  auto pc = [h, lc](const Vec& in, Vec& out, const Vec&, int dd) { return kcycle_cap(h, lc, in, out, dd); };
+  return fgmres_cap(h, lc, b, x, K, C.m, P.wrapper_iters, P.wrapper_tol, pc, true, d);
+}
+
+// kcycle() on the capture stream of depth d
+gmg_status kcycle_cap(gmg_mg* h, int l, const Vec& in, Vec& out, int d) {
+  MGLevel& L = *h->L[l];
+  MGLevel& C = *h->L[l + 1];
+  cudaStream_t s = h->cap_st[d];
+  const int R = in.R;
+  Vec bc = C.bc.with_rhs(R), xc = C.xc.with_rhs(R);
+  const gmg_prec tc = (h->P.prec == GMG_BF16 && in.prec == GMG_F32 && L.dof % 2 == 0 && C.dof <= 64)
+                          ? GMG_BF16
+                          : (gmg_prec)in.prec;
+  GMG_TRY(gmg_agg_project(L.agg, tc, (gmg_prec)in.prec, R, in.p, bc.p, (gmg_stream)s));
+  GMG_TRY(coarse_solve_cap(h, l + 1, bc, xc, d));
+  GMG_TRY(gmg_agg_promote(L.agg, tc, (gmg_prec)in.prec, R, xc.p, out.p, (gmg_stream)s));
+  return mr_smooth(h, l, in, out, h->P.smoother_iters, s);
+}
+
+// device state of the coarse-level solvers for max_rhs RHS (allocated before any capture)
+gmg_status graph_state(gmg_mg* h) {
+  const int R = h->Rmax;
+  for (size_t l = 1; l < h->L.size(); ++l) {
+    MGLevel& L = *h->L[l];
+    const int m = L.m;
+    if (L.gH.p) continue;
+    GMG_TRY(L.gH.alloc(sizeof(double2) * (size_t)R * (m + 1) * m));
+    GMG_TRY(L.gG.alloc(sizeof(double2) * (size_t)R * (m + 1)));
+    GMG_TRY(L.gCs.alloc(sizeof(double2) * (size_t)R * m));
+    GMG_TRY(L.gSn.alloc(sizeof(double2) * (size_t)R * m));
+    GMG_TRY(L.gRes.alloc(sizeof(double) * (size_t)R));
+    GMG_TRY(L.gY.alloc(sizeof(double2) * (size_t)R * m));
+    GMG_TRY(L.gCtr.alloc(sizeof(int) * 4));
+    GMG_TRY(L.gBn.alloc(sizeof(double2) * (size_t)R));
+    GMG_TRY(L.gBeta.alloc(sizeof(double2) * (size_t)R));
+    // the captured cycle combines all m Krylov / flexible directions with
+    // zero coefficients beyond the steps taken: keep them finite
+    GMG_CUDA(cudaMemset(L.V0.p, 0, L.V0.buf.bytes));
+    if (L.Z0.p) GMG_CUDA(cudaMemset(L.Z0.p, 0, L.Z0.buf.bytes));
+  }
+  for (auto& st : h->cap_st)
+    if (!st) GMG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  return GMG_OK;
+}
+
+// capture kcycle(0) on fixed buffers (input h->otz, output h->ogz) for R RHS
+gmg_status build_kcycle_graph(gmg_mg* h, int R, cudaGraphExec_t* exec) {
+  *exec = nullptr;
+  GMG_TRY(graph_state(h));
+  cudaStream_t s0 = h->cap_st[0];
+  Vec in = h->otz.with_rhs(R), out = h->ogz.with_rhs(R);
+  GMG_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+  gmg_status st = kcycle_cap(h, 0, in, out, 0);
+  cudaGraph_t g = nullptr;
+  // end every capture still open (an error inside a body leaves it open)
+  for (int d = 7; d >= 1; --d) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (h->cap_st[d] && cudaStreamIsCapturing(h->cap_st[d], &cs) == cudaSuccess &&
+        cs != cudaStreamCaptureStatusNone) {
+      cudaGraph_t gb = nullptr;
+      cudaStreamEndCapture(h->cap_st[d], &gb);
+    }
+  }
+  const cudaError_t e = cudaStreamEndCapture(s0, &g);
+  if (st != GMG_OK) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return st;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(GMG_ERR_CUDA, std::string("mg graph: capture failed: ") + cudaGetErrorString(e));
+  }
+  const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    cudaGetLastError();
+    *exec = nullptr;
+    return fail(GMG_ERR_CUDA, std::string("mg graph: instantiation failed: ") + cudaGetErrorString(ei));
+  }
+  return GMG_OK;
+}
+
 // ------------------------------------------------------------- setup
 // `count` consecutive fields of [V][R][dof] in one buffer; the Vec describes the first
 gmg_status alloc_fields(VecBuf& b, int64_t V, int R, int dof, int prec, int count) {
@@ -486,6 +823,7 @@ gmg_status outer_workspace(gmg_mg* h) {
   GMG_TRY(h->obb.alloc(V, R, 12, GMG_F64));
   GMG_TRY(h->oxx.alloc(V, R, 12, GMG_F64));
   GMG_TRY(h->oidx.alloc(sizeof(int) * R));
+  if (h->P.graph && zp != GMG_F64) GMG_TRY(h->ogz.alloc(V, R, 12, zp));
   h->outer_ready = true;
   return GMG_OK;
 }
@@ -550,6 +888,7 @@ extern "C" gmg_status gmg_mg_params_default(gmg_mg_params* p) {
   // (28 outer iterations on that configuration).
   p->setup_passes = 1;
   p->setup_null = 1;
+  p->graph = 0;
   return GMG_OK;
 }
 
@@ -614,6 +953,10 @@ extern "C" gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream stream) {
   cudaStream_t s = S(stream);
   const gmg_mg_params& P = h->P;
   const int nl = (int)h->L.size();
+  // captured cycles refer to the operators and buffers a new setup replaces
+  for (auto& g : h->kgraph) cudaGraphExecDestroy(g.second);
+  h->kgraph.clear();
+  h->graph_broken = false;
   for (int l = 0; l < nl; ++l) {
     MGLevel& L = *h->L[l];
     const bool coarsest = l == nl - 1;
@@ -741,11 +1084,25 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
     auto pc = [h, s, &tz, Ra, zp](const Vec& in, Vec& out, const Vec&) -> gmg_status {
       // in: FP64 Krylov vector; out: Z direction in the preconditioner precision
       Vec tin = tz.with_rhs(Ra);
-      if (zp != GMG_F64) {
-        GMG_TRY(vec_convert(in, tin, s));
-        return kcycle(h, 0, tin, out, s);
+      if (zp == GMG_F64) return kcycle(h, 0, in, out, s);
+      GMG_TRY(vec_convert(in, tin, s));
+      if (!h->P.graph || h->graph_broken || Ra > 1024) return kcycle(h, 0, tin, out, s);
+      auto it = h->kgraph.find(Ra);
+      if (it == h->kgraph.end()) {
+        // first cycle of this batch size: host-driven (it also builds every
+        // buffer and tuning key the cycle needs), then captured for the next ones
+        GMG_TRY(kcycle(h, 0, tin, out, s));
+        GMG_CUDA(cudaStreamSynchronize(s));
+        cudaGraphExec_t ex = nullptr;
+        if (build_kcycle_graph(h, Ra, &ex) == GMG_OK)
+          h->kgraph[Ra] = ex;
+        else
+          h->graph_broken = true;  // keep the host-driven cycle
+        return GMG_OK;
       }
-      return kcycle(h, 0, in, out, s);
+      GMG_CUDA(cudaGraphLaunch(it->second, s));
+      GMG_CUDA(cudaMemcpyAsync(out.p, h->ogz.p, out.bytes(), cudaMemcpyDeviceToDevice, s));
+      return GMG_OK;
     };
     int it = 0;
     std::vector<double> rr;
@@ -773,6 +1130,13 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
   if (iters_out) *iters_out = total;
   if (max_relres) *max_relres = mx;
   if (mx > tol) return fail(GMG_ERR_NOT_CONVERGED, "gmg_mg_solve: not converged within maxiter");
+  return GMG_OK;
+}
+
+extern "C" gmg_status gmg_mg_graphs(gmg_mg* h, int* graphs, int* fell_back) {
+  GMG_CHECK(h && graphs && fell_back, GMG_ERR_ARGUMENT, "gmg_mg_graphs: null argument");
+  *graphs = (int)h->kgraph.size();
+  *fell_back = h->graph_broken ? 1 : 0;
   return GMG_OK;
 }
 

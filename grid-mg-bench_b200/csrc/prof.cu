@@ -42,6 +42,8 @@ bool prof_enabled() { return g_on; }
 
 KernelTimer::KernelTimer(const char* name, cudaStream_t s) : name_(name), s_(s) {
   if (!g_on) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s_, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;  // not in graphs
   a_ = take_event();
   b_ = take_event();
   cudaEventRecord(a_, s_);

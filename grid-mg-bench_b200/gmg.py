@@ -389,7 +389,7 @@ class MGParams(ctypes.Structure):
                 ("wrapper_tol", ctypes.c_double), ("coarsest_iters", ctypes.c_int), ("coarsest_tol", ctypes.c_double),
                 ("coarsest_restart", ctypes.c_int), ("outer_restart", ctypes.c_int), ("prec", ctypes.c_int),
                 ("seed", ctypes.c_uint64), ("setup_solver", ctypes.c_int), ("setup_tol", ctypes.c_double),
-                ("setup_passes", ctypes.c_int), ("setup_null", ctypes.c_int)]
+                ("setup_passes", ctypes.c_int), ("setup_null", ctypes.c_int), ("graph", ctypes.c_int)]
 
 
 class MultiGrid:
@@ -423,6 +423,12 @@ class MultiGrid:
 
     def setup(self):
         _chk(lib().gmg_mg_setup(self._h, _stream()))
+
+    def graphs(self):
+        """(captured K-cycle graphs, 1 if a capture failed and the host-driven cycle was kept)."""
+        n, fb = ctypes.c_int(), ctypes.c_int()
+        _chk(lib().gmg_mg_graphs(self._h, ctypes.byref(n), ctypes.byref(fb)))
+        return n.value, fb.value
 
     def solve(self, b, x, tol=1e-10, maxiter=500):
         """b, x: complex128 CUDA tensors [V, nrhs, 12]; returns (outer iterations, max relative residual)."""

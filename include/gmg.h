@@ -314,6 +314,13 @@ typedef struct {
                             previous pass's vectors (inverse iteration) */
   int setup_null;        /* 1: null-vector setup (setupBasisVectorsType nullVectors: solve A psi = 0 from
                             psi = v); 0: test-vector setup (solve A psi = v from psi = 0) */
+  int graph;             /* 1: replay the K-cycle preconditioner as a CUDA graph.  The coarse-level
+                            solvers keep their Hessenberg / Givens state on the device; each restart
+                            cycle and each Arnoldi step is a conditional (IF) node that a device kernel
+                            switches on while the level's tolerance and iteration limit are not met,
+                            so the replay takes the same early exits as the host-driven cycle.  One
+                            graph per active-batch size, captured after one host-driven cycle of that
+                            size.  0: host-driven cycle (one host synchronisation per Arnoldi step). */
 } gmg_mg_params;
 
 /* Defaults of MultiGridParams (MultigridParams.h:95-113) adapted to the MR smoother, with the
@@ -331,6 +338,10 @@ gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream s);
    outer restart.  Synchronises; GMG_ERR_NOT_CONVERGED if maxiter is reached. */
 gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double* x, double tol, int maxiter, int* iters,
                         double* max_relres, gmg_stream s);
+/* Captured K-cycle graphs of this handle (params.graph): how many (one per
+   active-batch size met so far) and whether a capture failed, in which case
+   the solver kept the host-driven cycle.  No counterpart in the reference. */
+gmg_status gmg_mg_graphs(gmg_mg* h, int* graphs, int* fell_back);
 /* The coarse operator of level > 0 and the aggregation from level to level+1
    (runChecks, MultigridPreconditioner.h:311-446); either may be null. */
 gmg_status gmg_mg_level(gmg_mg* h, int level, gmg_coarse** op, gmg_agg** agg);

@@ -62,6 +62,31 @@ def test_mg_solve_reaches_1e10(fine, prec, levels):
     assert true_relres(w, b, x) <= 2e-10, (it, rr)
 
 
+@pytest.mark.parametrize("prec,levels", [("f32", 2), ("f32", 3), ("bf16", 3)])
+def test_mg_graph_captured_cycle(fine, prec, levels):
+    # the K-cycle replayed as a CUDA graph (coarse-level Givens on the device,
+    # conditional nodes for the early exits) reaches the same tolerance in the
+    # same number of outer iterations as the host-driven cycle
+    dims, w = fine
+    nrhs = 4
+    kw = dict(nlevels=levels, nvec=(6, 6), setup_iters=30, prec=prec, coarsest_iters=30, wrapper_iters=6)
+    kw["block"] = ((4, 4, 4, 4), (2, 2, 2, 2)) if levels == 2 else ((2, 2, 2, 2), (2, 2, 2, 2))
+    b = torch.from_numpy(inputs.gaussian_field((4096, nrhs, 12), inputs.rng(stream=304))).cuda()
+    its = {}
+    for graph in (0, 1):
+        mg = gmg.MultiGrid(w, nrhs, graph=graph, **kw)
+        mg.setup()
+        x = torch.zeros_like(b)
+        it, rr = mg.solve(b, x, tol=1e-10, maxiter=300)
+        assert rr <= 1e-10
+        assert true_relres(w, b, x) <= 2e-10, (graph, it, rr)
+        its[graph] = it
+        if graph:
+            n, fell_back = mg.graphs()
+            assert n >= 1 and fell_back == 0, (n, fell_back)
+    assert abs(its[1] - its[0]) <= 1, its
+
+
 def test_mg_galerkin_identity_on_setup_operators(fine):
     dims, w = fine
     mg = gmg.MultiGrid(w, 2, nlevels=2, block=((4, 4, 4, 4), (2, 2, 2, 2)), nvec=(6, 6), prec="f64")
