@@ -218,7 +218,7 @@ def wilson_and_c4(T, hbm):
 
 
 def c5_measure(nrhs=24, plain_rhs=2,
-               forms=("mixed_bf16_mrhs", "mixed_bf16_mrhs_graph", "mixed_f32_mrhs", "plain_f64_single_rhs")):
+               forms=("mixed_bf16_mrhs", "mixed_bf16_mrhs_graph", "mixed_f32_mrhs", "plain_f64_single_rhs"), L=32):
     """3-level K-cycle MG-preconditioned FGMRES on 32^4 Wilson-clover (m=-0.35, csw 1, eps 0.3,
     antiperiodic t): nbasis 24 on 4^4 blocks, nbasis 32 on 2^4 blocks, MR(8) smoothing;
     `nrhs` Gaussian RHS to a true relative residual of 1e-10.  The plain FP64 single-RHS
@@ -226,8 +226,8 @@ def c5_measure(nrhs=24, plain_rhs=2,
     replays the K-cycle as a captured CUDA graph; its first solve also captures the graph
     (after one host-driven cycle per batch size) and is reported separately, the timed one
     is the second solve on the same handle."""
-    fd = (32, 32, 32, 32)
-    V = 32 ** 4
+    fd = (L, L, L, L)
+    V = L ** 4
     U = inputs.torch_smooth_gauge(fd, 801, 0.3)
     w = gmg.WilsonClover(fd, -0.35, 1.0, antiperiodic=True)
     w.set_gauge(U)
@@ -294,6 +294,14 @@ def c5(nrhs=24, plain_rhs=2):
               "setup (null vectors, orthonormalisation, CoarsenOperator) not included in solve_s")
 
 
+def c5_small(nrhs=24):
+    """The C5 solver on a 16^4 lattice (coarse levels of 256 and 16 sites), where
+    the coarse solves are latency-bound: host-driven vs graph-replayed K-cycle."""
+    out = c5_measure(nrhs, 1, forms=("mixed_bf16_mrhs", "mixed_bf16_mrhs_graph"), L=16)
+    line("C5s same 3-level MG on 16^4 Wilson-clover, 24 RHS to 1e-10: host-driven vs graph-replayed K-cycle",
+         results=out, note="graph form: second solve on the handle (the first also captures)")
+
+
 def profile_rows(rows):
     """Small cases of the C3 transfers and the fine operator for ncu captures:
     16^4 fine lattice (nbasis 32 on 4^4 blocks, 32 RHS; Wilson-clover with 24 RHS)."""
@@ -348,6 +356,8 @@ def run(rows=("c1", "c3", "w_c4", "c5")):
         torch.cuda.empty_cache()
     if "c5" in rows:
         c5()
+    if "c5s" in rows:
+        c5_small()
     if any(r.startswith("p_") for r in rows):
         profile_rows(rows)
         return
