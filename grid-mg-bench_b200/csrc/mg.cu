@@ -888,7 +888,7 @@ extern "C" gmg_status gmg_mg_params_default(gmg_mg_params* p) {
   // (28 outer iterations on that configuration).
   p->setup_passes = 1;
   p->setup_null = 1;
-  p->graph = 0;
+  p->graph = 1;
   return GMG_OK;
 }
 

@@ -320,7 +320,8 @@ typedef struct {
                             switches on while the level's tolerance and iteration limit are not met,
                             so the replay takes the same early exits as the host-driven cycle.  One
                             graph per active-batch size, captured after one host-driven cycle of that
-                            size.  0: host-driven cycle (one host synchronisation per Arnoldi step). */
+                            size (default).  0: host-driven cycle (one host synchronisation per
+                            Arnoldi step).  The FP64 preconditioner form is always host-driven. */
 } gmg_mg_params;
 
 /* Defaults of MultiGridParams (MultigridParams.h:95-113) adapted to the MR smoother, with the
