@@ -87,6 +87,26 @@ def test_mg_graph_captured_cycle(fine, prec, levels):
     assert abs(its[1] - its[0]) <= 1, its
 
 
+def test_mg_graph_after_compaction(fine):
+    # RHS that converge early drop out at the first outer restart; the smaller
+    # batch gets its own captured cycle, and every RHS still reaches 1e-10
+    dims, w = fine
+    nrhs = 4
+    mg = gmg.MultiGrid(w, nrhs, nlevels=3, block=((2, 2, 2, 2), (2, 2, 2, 2)), nvec=(6, 6), setup_iters=30,
+                       prec="f32", coarsest_iters=30, wrapper_iters=6, outer_restart=4)
+    mg.setup()
+    b = torch.from_numpy(inputs.gaussian_field((4096, nrhs, 12), inputs.rng(stream=305))).cuda()
+    x = torch.zeros_like(b)
+    mg.solve(b, x, tol=1e-10, maxiter=300)
+    assert mg.graphs() == (1, 0)
+    x[:, 2:] = 0  # RHS 0 and 1 start converged
+    it, rr = mg.solve(b, x, tol=1e-10, maxiter=300)
+    assert rr <= 1e-10
+    assert true_relres(w, b, x) <= 2e-10, it
+    n, fell_back = mg.graphs()
+    assert n == 2 and fell_back == 0, (n, fell_back)
+
+
 def test_mg_galerkin_identity_on_setup_operators(fine):
     dims, w = fine
     mg = gmg.MultiGrid(w, 2, nlevels=2, block=((4, 4, 4, 4), (2, 2, 2, 2)), nvec=(6, 6), prec="f64")
