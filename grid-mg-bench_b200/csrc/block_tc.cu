@@ -168,6 +168,16 @@ __device__ __forceinline__ uint32_t bf16_pair(float a, float b) {
          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b)) << 16);
 }
 __device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+// hi = round-to-nearest BF16 of (a, b) packed in one word (low half: a), and
+// the lo parts a - hi_a, b - hi_b packed the same way; the BF16 -> FP32 of hi
+// is a 16-bit shift
+__device__ __forceinline__ void bf16_hilo_pair(float a, float b, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  const float ha = __uint_as_float(hi << 16), hb = __uint_as_float(hi & 0xffff0000u);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(a - ha, b - hb);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
 
 struct Params {
   const uint16_t* ahi;      // packed basis, hi part: [Vc][Kp/8][Mp][8]
@@ -337,6 +347,9 @@ __global__ void __launch_bounds__(kThreads, CTAS) project_tc_kernel(const Params
     const int t = threadIdx.x - 64;  // 0..255
     const int hd = P.dof / 2;        // complex pairs per (site, rhs) record
     const int items = P.sps * P.R * hd;
+    // per-item step of kConvThreads items in (a2, r, sl) digits
+    const int da2 = kConvThreads % hd, drec = kConvThreads / hd;
+    const int dr = drec % P.R, dsl = drec / P.R;
     for (int64_t n = 0; n < nseq; ++n) {
       const int stage = (int)(n % P.stages);
       const uint32_t phase = (uint32_t)((n / P.stages) & 1);
@@ -353,10 +366,11 @@ __global__ void __launch_bounds__(kThreads, CTAS) project_tc_kernel(const Params
       uint32_t* bh = reinterpret_cast<uint32_t*>(st + 2 * a_bytes);
       uint32_t* bl = reinterpret_cast<uint32_t*>(st + 2 * a_bytes + b_bytes);
       const unsigned char* rw = st + 2 * a_bytes + 2 * b_bytes;
-      // item = ((sl * R) + r) * hd + a2: consecutive threads read consecutive 16-byte pairs
+      // item = ((sl * R) + r) * hd + a2: consecutive threads read consecutive 16-byte pairs;
+      // (a2, r, sl) advance by carries instead of divisions per item
+      int a2 = t % hd, rec0 = t / hd;
+      int r = rec0 % P.R, sl = rec0 / P.R;
       for (int it = t; it < items; it += kConvThreads) {
-        const int a2 = it % hd, rec = it / hd;
-        const int sl = rec / P.R, r = rec % P.R;
         const int sb = ks * P.sps + sl;  // in-block site
         const int a = 2 * a2;
         float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
@@ -379,13 +393,26 @@ __global__ void __launch_bounds__(kThreads, CTAS) project_tc_kernel(const Params
         }
         const int k = sl * P.dof + a;  // even: k, k+1 share a 16-byte core-matrix row
         const int chunk = k >> 3, j = k & 7;
-        const float h0r = bf16_round(x0.x), h1r = bf16_round(x1.x), h0i = bf16_round(x0.y), h1i = bf16_round(x1.y);
         const size_t rre = ((size_t)chunk * 2 * P.Rp + r) * 4 + (j >> 1);  // 32-bit words
         const size_t rim = ((size_t)chunk * 2 * P.Rp + P.Rp + r) * 4 + (j >> 1);
-        bh[rre] = bf16_pair(h0r, h1r);
-        bh[rim] = bf16_pair(h0i, h1i);
-        bl[rre] = bf16_pair(x0.x - h0r, x1.x - h1r);
-        bl[rim] = bf16_pair(x0.y - h0i, x1.y - h1i);
+        uint32_t hre, lre, him, lim;
+        bf16_hilo_pair(x0.x, x1.x, hre, lre);
+        bf16_hilo_pair(x0.y, x1.y, him, lim);
+        bh[rre] = hre;
+        bh[rim] = him;
+        bl[rre] = lre;
+        bl[rim] = lim;
+        a2 += da2;
+        r += dr;
+        if (a2 >= hd) {
+          a2 -= hd;
+          ++r;
+        }
+        sl += dsl;
+        if (r >= P.R) {
+          r -= P.R;
+          ++sl;
+        }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&full[stage]);
