@@ -480,6 +480,15 @@ __device__ __forceinline__ uint16_t to_half_bits(float x, int kind) {
   if (kind == GMG_BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(x));
   return __half_as_ushort(__float2half_rn(x));
 }
+// (a, b) rounded to the 16-bit kind with one paired conversion; a in the low half
+__device__ __forceinline__ uint32_t to_half_pair(float a, float b, int kind) {
+  if (kind == GMG_BF16) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+  }
+  const __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
 
 // links (exchange layout, FP64) -> [V][9][Kc][Mp][8] halves
 __global__ void pack_links_kernel(const double2* __restrict__ A, uint4* __restrict__ dst, int V, int N, int Kc,
@@ -526,7 +535,7 @@ __global__ void pack_vec_kernel(const float2* __restrict__ in, uint4* __restrict
     const int kc = (int)(e % Kc);
     const int r = (int)((e / Kc) % Rp);
     const int64_t s = e / ((int64_t)Rp * Kc);
-    uint16_t hr[8], hi[8];
+    uint32_t pr[4], pi[4];
     if (r < R) {
       const int slot = active ? active[r] : r;
       const float2* src = in + ((int64_t)s * nrhs + slot) * N + kc * 8;
@@ -545,34 +554,30 @@ __global__ void pack_vec_kernel(const float2* __restrict__ in, uint4* __restrict
 #pragma unroll
         for (int j = 0; j < 8; ++j) x[j] = (kc * 8 + j < N) ? src[j] : make_float2(0.f, 0.f);
       }
+      float re[8], im[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int bb = kc * 8 + j;
-        float re = 0.f, im = 0.f;
+        re[j] = 0.f;
+        im[j] = 0.f;
         if (bb < N) {
-          re = x[j].x;
-          im = x[j].y;
-          if (g5 && bb >= N / 2) { re = -re; im = -im; }
+          re[j] = x[j].x;
+          im[j] = x[j].y;
+          if (g5 && bb >= N / 2) { re[j] = -re[j]; im[j] = -im[j]; }
         }
-        hr[j] = to_half_bits(re, kind);
-        hi[j] = to_half_bits(im, kind);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        pr[j] = to_half_pair(re[2 * j], re[2 * j + 1], kind);
+        pi[j] = to_half_pair(im[2 * j], im[2 * j + 1], kind);
       }
     } else {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) hr[j] = hi[j] = 0;
+      for (int j = 0; j < 4; ++j) pr[j] = pi[j] = 0;
     }
-    uint4 o;
-    o.x = hr[0] | ((uint32_t)hr[1] << 16);
-    o.y = hr[2] | ((uint32_t)hr[3] << 16);
-    o.z = hr[4] | ((uint32_t)hr[5] << 16);
-    o.w = hr[6] | ((uint32_t)hr[7] << 16);
     uint4* row = dst + ((int64_t)s * Kc + kc) * 2 * Rp;
-    row[r] = o;
-    o.x = hi[0] | ((uint32_t)hi[1] << 16);
-    o.y = hi[2] | ((uint32_t)hi[3] << 16);
-    o.z = hi[4] | ((uint32_t)hi[5] << 16);
-    o.w = hi[6] | ((uint32_t)hi[7] << 16);
-    row[Rp + r] = o;
+    row[r] = make_uint4(pr[0], pr[1], pr[2], pr[3]);
+    row[Rp + r] = make_uint4(pi[0], pi[1], pi[2], pi[3]);
   }
 }
 
