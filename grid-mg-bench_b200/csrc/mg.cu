@@ -43,6 +43,7 @@ struct MGLevel {
   VecBuf V0, Z0, kw, kt;    // Krylov basis (m+1), flexible directions (m), temporaries
   VecBuf mr_r, mr_Ar, mr_t; // MR smoother
   VecBuf bc, xc;            // right-hand side / solution of this level inside the cycle above
+  VecBuf tv;                // test vectors (nvec[l]) the basis to level l+1 is built from
   // device state of this level's solver inside a captured K-cycle: Hessenberg
   // [R][m+1][m], rhs g [R][m+1], Givens cs / sn [R][m], residual estimates [R],
   // solution coefficients y [m][R], counters {iterations, steps of the cycle},
@@ -852,6 +853,48 @@ gmg_status pretune_fine(gmg_mg* h, cudaStream_t s) {
   return GMG_OK;
 }
 
+// recreateOperators of one transition (MultigridPreconditioner.h:458-477):
+// chiral doubling of level l's test vectors into the 2 nvec basis, block
+// orthonormalisation (Aggregation::Create), Galerkin coarsening into level
+// l+1's operator and its reduced-precision copies.  The handles are created on
+// first use and refilled afterwards, so their addresses stay valid.
+gmg_status recreate_level(gmg_mg* h, int l, cudaStream_t s) {
+  MGLevel& L = *h->L[l];
+  MGLevel& C = *h->L[l + 1];
+  const int nv = h->P.nvec[l];
+  const gmg_stream stream = (gmg_stream)s;
+  DevBuf basis;
+  GMG_TRY(basis.alloc(sizeof(double2) * 2 * (size_t)nv * L.V * L.dof));
+  GMG_TRY(vec_chiral_double(L.tv, basis.as<double>(), s));
+  if (!L.agg) GMG_TRY(gmg_agg_create(L.dims.d, C.dims.d, L.dof, 2 * nv, &L.agg));
+  GMG_TRY(gmg_agg_set_basis(L.agg, basis.as<double>(), 1, stream));
+  GMG_TRY(gmg_agg_orthonormalise(L.agg, 2, stream));
+  GMG_CUDA(cudaStreamSynchronize(s));
+  if (!C.c) GMG_TRY(gmg_coarse_create(C.dims.d, 2 * nv, 0, &C.c));
+  if (l == 0) GMG_TRY(gmg_coarsen_wilson(C.c, L.agg, L.w, stream));
+  else GMG_TRY(gmg_coarsen_coarse(C.c, L.agg, L.c, stream));
+  if (C.vprec == GMG_F32) GMG_TRY(gmg_coarse_prepare(C.c, GMG_F32, stream));
+  if (C.compute == GMG_BF16) GMG_TRY(gmg_coarse_prepare(C.c, GMG_BF16, stream));
+  GMG_CUDA(cudaStreamSynchronize(s));
+  return GMG_OK;
+}
+
+// right-hand sides [s0, s0 + n) of src -> [d0, d0 + n) of dst (same sites,
+// dof and precision; the RHS index is the middle one of [V][R][dof])
+gmg_status copy_rhs(const Vec& src, int s0, const Vec& dst, int d0, int n, cudaStream_t s) {
+  const size_t col = (size_t)src.dof * src.esize();
+  GMG_CUDA(cudaMemcpy2DAsync(static_cast<char*>(dst.p) + d0 * col, dst.R * col,
+                             static_cast<const char*>(src.p) + s0 * col, src.R * col, n * col, (size_t)src.V,
+                             cudaMemcpyDeviceToDevice, s));
+  return GMG_OK;
+}
+
+void drop_graphs(gmg_mg* h) {
+  for (auto& g : h->kgraph) cudaGraphExecDestroy(g.second);
+  h->kgraph.clear();
+  h->graph_broken = false;
+}
+
 }  // namespace
 }  // namespace gmg
 
@@ -889,6 +932,8 @@ extern "C" gmg_status gmg_mg_params_default(gmg_mg_params* p) {
   p->setup_passes = 1;
   p->setup_null = 1;
   p->graph = 1;
+  p->refine_iters[0] = p->refine_iters[1] = 0;
+  p->recursive_updates = 1;
   return GMG_OK;
 }
 
@@ -953,10 +998,9 @@ extern "C" gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream stream) {
   cudaStream_t s = S(stream);
   const gmg_mg_params& P = h->P;
   const int nl = (int)h->L.size();
+  h->setup_done = false;
   // captured cycles refer to the operators and buffers a new setup replaces
-  for (auto& g : h->kgraph) cudaGraphExecDestroy(g.second);
-  h->kgraph.clear();
-  h->graph_broken = false;
+  drop_graphs(h);
   for (int l = 0; l < nl; ++l) {
     MGLevel& L = *h->L[l];
     const bool coarsest = l == nl - 1;
@@ -967,14 +1011,13 @@ extern "C" gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream stream) {
     MGLevel& L = *h->L[l];
     MGLevel& C = *h->L[l + 1];
     const int nv = P.nvec[l];
-    // test vectors: A psi = v approximately, from random v (BasisVectors.h:94-120),
-    // GMRES(10) with a temporary Krylov basis sized for the nv vectors
     // test vectors (BasisVectors::Generate, BasisVectors.h:74-147): random start,
     // then setup_passes passes of {orthonormalise, solve, orthonormalise}; the
     // test-vector form solves A psi = v from psi = 0 (inverse iteration), the
     // null-vector form solves A psi = 0 from psi = v (the slowly decaying low
     // modes remain)
-    VecBuf v, psi, zsrc;
+    VecBuf v, zsrc;
+    VecBuf& psi = L.tv;  // kept for the refinement setup
     GMG_TRY(v.alloc(L.V, nv, L.dof, L.vprec));
     GMG_TRY(psi.alloc(L.V, nv, L.dof, L.vprec));
     GMG_TRY(vec_gaussian(v, P.seed * 7919 + l, s));
@@ -1015,18 +1058,7 @@ extern "C" gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream stream) {
       if (pass + 1 < passes) GMG_CUDA(cudaMemcpyAsync(v.p, psi.p, psi.bytes(), cudaMemcpyDeviceToDevice, s));
     }
     // chiral doubling -> basis, block orthonormalisation, Galerkin coarsening
-    DevBuf basis;
-    GMG_TRY(basis.alloc(sizeof(double2) * 2 * (size_t)nv * L.V * L.dof));
-    GMG_TRY(vec_chiral_double(psi, basis.as<double>(), s));
-    GMG_TRY(gmg_agg_create(L.dims.d, C.dims.d, L.dof, 2 * nv, &L.agg));
-    GMG_TRY(gmg_agg_set_basis(L.agg, basis.as<double>(), 1, stream));
-    GMG_TRY(gmg_agg_orthonormalise(L.agg, 2, stream));
-    GMG_CUDA(cudaStreamSynchronize(s));
-    GMG_TRY(gmg_coarse_create(C.dims.d, 2 * nv, 0, &C.c));
-    if (l == 0) GMG_TRY(gmg_coarsen_wilson(C.c, L.agg, L.w, stream));
-    else GMG_TRY(gmg_coarsen_coarse(C.c, L.agg, L.c, stream));
-    if (C.vprec == GMG_F32) GMG_TRY(gmg_coarse_prepare(C.c, GMG_F32, stream));
-    if (C.compute == GMG_BF16) GMG_TRY(gmg_coarse_prepare(C.c, GMG_BF16, stream));
+    GMG_TRY(recreate_level(h, l, s));
     const bool coarsest = l + 1 == nl - 1;
     GMG_TRY(alloc_level_ws(C, h->Rmax, true, !coarsest));
     GMG_CUDA(cudaStreamSynchronize(s));
@@ -1034,6 +1066,60 @@ extern "C" gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream stream) {
   GMG_TRY(outer_workspace(h));
   GMG_TRY(pretune_fine(h, s));
   h->setup_done = true;
+  return GMG_OK;
+}
+
+// refinementSetup (MultigridPreconditioner.h:213-251) with the test-vector
+// form of BasisVectors::Generate (BasisVectors.h:74-147): the solver is the
+// level's own preconditioner (OperatorFunctionWrapper over operator(),
+// :253-309), applied from psi = 0 to each test vector; updateBasisVector
+// (:479-501) and recreateOperators (:458-477) are the callbacks.  The
+// reference applies the preconditioner to one vector at a time; the operators
+// do not change within a pass, so the vectors go through the K-cycle as one
+// multi-RHS batch (max_rhs at a time) with the same result per vector up to
+// the batch's shared iteration count on the coarse levels.
+extern "C" gmg_status gmg_mg_refine(gmg_mg* h, gmg_stream stream) {
+  GMG_CHECK(h != nullptr, GMG_ERR_ARGUMENT, "gmg_mg_refine: null handle");
+  GMG_CHECK(h->setup_done, GMG_ERR_STATE, "gmg_mg_refine: call gmg_mg_setup first");
+  cudaStream_t s = S(stream);
+  const gmg_mg_params& P = h->P;
+  const int nl = (int)h->L.size();
+  for (int l = 0; l + 1 < nl; ++l) {
+    const int iters = P.refine_iters[l];
+    // a level without refinement iterations does not recurse (:214, :246)
+    if (iters <= 0) break;
+    drop_graphs(h);
+    MGLevel& L = *h->L[l];
+    MGLevel& C = *h->L[l + 1];
+    const int nv = P.nvec[l];
+    const int Rc = std::min(nv, h->Rmax);
+    VecBuf a, b;
+    GMG_TRY(a.alloc(L.V, Rc, L.dof, L.vprec));
+    GMG_TRY(b.alloc(L.V, Rc, L.dof, L.vprec));
+    // updateBasisVector reaches level l+1's test vectors when that level has
+    // an aggregation below it (the coarsest level keeps none, :653)
+    const bool update_next = P.recursive_updates && l + 2 < nl;
+    for (int it = 0; it < iters; ++it) {
+      GMG_TRY(global_orthonormalise(h, L.tv, s));  // setupPreOrthonormalise
+      for (int k0 = 0; k0 < nv; k0 += Rc) {
+        const int n = std::min(Rc, nv - k0);
+        Vec in = a.with_rhs(n), out = b.with_rhs(n);
+        GMG_TRY(copy_rhs(L.tv, k0, in, 0, n, s));
+        GMG_TRY(kcycle(h, l, in, out, s));  // psi = MG(v) from psi = 0
+        GMG_TRY(copy_rhs(out, 0, L.tv, k0, n, s));
+        // level l+1's vector k <- its solution inside this application (_FineSol)
+        const int nu = update_next ? std::min(n, P.nvec[l + 1] - k0) : 0;
+        if (nu > 0) GMG_TRY(copy_rhs(C.xc.with_rhs(n), 0, C.tv, k0, nu, s));
+      }
+      GMG_TRY(global_orthonormalise(h, L.tv, s));  // setupPostOrthonormalise
+      // recreateOperators(setupRecursiveUpdates)
+      for (int q = l; q + 1 < nl; ++q) {
+        GMG_TRY(recreate_level(h, q, s));
+        if (!P.recursive_updates) break;
+      }
+    }
+  }
+  GMG_CUDA(cudaStreamSynchronize(s));
   return GMG_OK;
 }
 

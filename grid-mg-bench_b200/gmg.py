@@ -389,7 +389,8 @@ class MGParams(ctypes.Structure):
                 ("wrapper_tol", ctypes.c_double), ("coarsest_iters", ctypes.c_int), ("coarsest_tol", ctypes.c_double),
                 ("coarsest_restart", ctypes.c_int), ("outer_restart", ctypes.c_int), ("prec", ctypes.c_int),
                 ("seed", ctypes.c_uint64), ("setup_solver", ctypes.c_int), ("setup_tol", ctypes.c_double),
-                ("setup_passes", ctypes.c_int), ("setup_null", ctypes.c_int), ("graph", ctypes.c_int)]
+                ("setup_passes", ctypes.c_int), ("setup_null", ctypes.c_int), ("graph", ctypes.c_int),
+                ("refine_iters", ctypes.c_int * 2), ("recursive_updates", ctypes.c_int)]
 
 
 class MultiGrid:
@@ -403,9 +404,10 @@ class MultiGrid:
                 for i, blk in enumerate(v):
                     for d in range(4):
                         p.block[i][d] = blk[d]
-            elif k == "nvec":
+            elif k in ("nvec", "refine_iters"):
+                arr = getattr(p, k)
                 for i, n in enumerate(v):
-                    p.nvec[i] = n
+                    arr[i] = n
             elif k == "prec":
                 p.prec = PREC.get(v, v)
             else:
@@ -423,6 +425,10 @@ class MultiGrid:
 
     def setup(self):
         _chk(lib().gmg_mg_setup(self._h, _stream()))
+
+    def refine(self):
+        """refinementSetup: params.refine_iters passes per transition (see gmg_mg_refine)."""
+        _chk(lib().gmg_mg_refine(self._h, _stream()))
 
     def graphs(self):
         """(captured K-cycle graphs, 1 if a capture failed and the host-driven cycle was kept)."""

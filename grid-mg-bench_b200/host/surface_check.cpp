@@ -10,9 +10,14 @@
 //   (5) 0 == Im(v_c^dag D_c^dag D_c v_c)                 Mdag is the adjoint
 // and the red-black identities of src/Test_coarse_red_black.cc:170-482:
 //   (6) M = Dhop + Mdiag   (7) MooeeInv Mooee = 1   (8) M = Meo + Moe + Mee + Moo
+// and the MG driver of src/Test_wilsonclover_mg.cc:115-140 (initialSetup,
+// refinementSetup, outer FGMRES):
+//   (9) |b - D x| / |b| of the solve after the refinement setup
+//   (10) (R D P - D_c) v_c on the operators the refinement rebuilt
 // Prints one line per check and exits non-zero if any check fails.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -193,6 +198,52 @@ int main() {
     gmg::SetCheckerboard(cdims, t1.f, 0, full.f);
     Dc.M(c.f, c3.f);
     ok &= report("M - (Meo + Moe + Mee + Moo)", rel_dev(c3.get(), full.get()), 1e-13);
+
+    // MG driver: 2 levels, test-vector setup, one refinement pass
+    gmg_mg_params P = gmg::MultiGridPreconditioner::Params();
+    P.nlevels = 2;
+    P.nvec[0] = 4;
+    P.setup_iters = 30;
+    P.setup_null = 0;
+    P.coarsest_iters = 30;
+    P.refine_iters[0] = 1;
+    gmg::MultiGridPreconditioner MG(D, P, 2);
+    MG.initialSetup();
+    MG.refinementSetup();
+    DevField bb(Vf, 2, 12), xx(Vf, 2, 12), r(Vf, 2, 12);
+    auto bh = gaussian(Vf * 2 * 12, gen);
+    bb.set(bh);
+    double rr = 0;
+    const int its = MG.Solve(bb.f, xx.f, 1e-10, 300, &rr);
+    FineOp.Op(xx.f, r.f);
+    {
+      auto Dx = r.get();
+      double worst = 0;
+      for (int k = 0; k < 2; ++k) {
+        double num = 0, den = 0;
+        for (long s2 = 0; s2 < Vf; ++s2)
+          for (int a2 = 0; a2 < 12; ++a2) {
+            const size_t i = ((size_t)s2 * 2 + k) * 12 + a2;
+            num += std::norm(bh[i] - Dx[i]);
+            den += std::norm(bh[i]);
+          }
+        worst = std::max(worst, std::sqrt(num / den));
+      }
+      std::printf("MG solve after refinementSetup: %d outer iterations\n", its);
+      ok &= report("|b - D x| / |b| after refinementSetup", worst, 2e-10);
+    }
+    {
+      gmg_agg* ag = MG.Aggregates(0);
+      gmg_coarse* op = MG.CoarseMatrix(1);
+      const int Nm = 2 * P.nvec[0];
+      DevField vc(Vc, 1, Nm), rc(Vc, 1, Nm), dc(Vc, 1, Nm), pf(Vf, 1, 12), dpf(Vf, 1, 12);
+      vc.set(gaussian(Vc * Nm, gen));
+      gmg::check(gmg_agg_promote(ag, GMG_F64, GMG_F64, 1, vc.f.data, pf.f.data, nullptr));
+      FineOp.Op(pf.f, dpf.f);
+      gmg::check(gmg_agg_project(ag, GMG_F64, GMG_F64, 1, dpf.f.data, rc.f.data, nullptr));
+      gmg::check(gmg_coarse_apply(op, GMG_OP_M, 8, GMG_F64, GMG_F64, 1, vc.f.data, dc.f.data, nullptr, 0, nullptr));
+      ok &= report("(R D P - D_c) v_c after refinementSetup", rel_dev(rc.get(), dc.get()), 1e-12);
+    }
   } catch (const gmg::Error& e) {
     std::printf("gmg error %d: %s\n", (int)e.status, e.what());
     return 2;

@@ -322,6 +322,11 @@ typedef struct {
                             graph per active-batch size, captured after one host-driven cycle of that
                             size (default).  0: host-driven cycle (one host synchronisation per
                             Arnoldi step).  The FP64 preconditioner form is always host-driven. */
+  int refine_iters[2];   /* refinement setup iterations of the transitions 0->1, 1->2
+                            (setupRefinementIter, default {0, 0}); run by gmg_mg_refine */
+  int recursive_updates; /* 1: the refinement of a level also replaces the next level's test vectors
+                            by its coarse solutions and rebuilds every coarser operator
+                            (setupRecursiveUpdates, default 1) */
 } gmg_mg_params;
 
 /* Defaults of MultiGridParams (MultigridParams.h:95-113) adapted to the MR smoother, with the
@@ -333,6 +338,18 @@ gmg_status gmg_mg_destroy(gmg_mg* h);
 /* initialSetup (MultigridPreconditioner.h:165-211): test vectors, chiral doubling,
    block orthonormalisation and CoarsenOperator on every level.  Synchronises. */
 gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream s);
+/* refinementSetup (MultigridPreconditioner.h:213-251, BasisVectors.h:74-147 with
+   testVectorSetup): for each transition l in order, refine_iters[l] passes of
+   {orthonormalise the level's test vectors; replace each by the level-l
+   preconditioner (restrict, K-cycle, prolong, smooth) applied to it; with
+   recursive_updates, replace the next level's test vector k by the coarse
+   solution of that application; orthonormalise; rebuild the aggregation and
+   coarse operator of level l (and of every coarser level with
+   recursive_updates)}.  As in the reference, a transition with no iterations
+   ends the refinement (coarser transitions are not refined).  The test vectors
+   of a batch go through the K-cycle together (up to max_rhs at a time).
+   Synchronises; operator and aggregation handles keep their addresses. */
+gmg_status gmg_mg_refine(gmg_mg* h, gmg_stream s);
 /* Solve D x = b for nrhs right-hand sides with FP64 FGMRES + MG preconditioner to
    per-RHS relative residual |b - D x| / |b| <= tol.  b, x: device FP64
    [V][nrhs][12]; x holds the initial guess.  Converged RHS drop out at every

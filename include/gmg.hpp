@@ -15,6 +15,10 @@
 //   gmg::LinearOperatorBase   Op / AdjOp / HermOp / OpDiag / OpDir / OpDirAll
 //   gmg::MdagMLinearOperator  Grid's MdagMLinearOperator<Matrix, Field> over any
 //                             of the sparse matrices above
+//   gmg::MultiGridPreconditioner
+//                             MultiGridPreconditioner (include/MultigridPreconditioner.h:44-660):
+//                             initialSetup, refinementSetup, and the outer
+//                             FGMRES solve of Test_wilsonclover_mg[_mp].cc
 //
 // Fields are device buffers described by gmg::Field (pointer, sites, nrhs,
 // dof, precision); the library never owns them.  Errors throw gmg::Error
@@ -245,6 +249,55 @@ class MdagMLinearOperator : public LinearOperatorBase {
 
  private:
   Matrix& m_;
+};
+
+// The multigrid hierarchy over the fine Wilson-clover matrix.  Parameters
+// are MultiGridParams (MultigridParams.h:95-113) as gmg_mg_params; Params()
+// gives the defaults.  Solve() runs the FP64 outer FGMRES preconditioned by
+// the K-cycle on device fields [V][nrhs][12] (F64) and returns the outer
+// iteration count.
+class MultiGridPreconditioner {
+ public:
+  static gmg_mg_params Params() {
+    gmg_mg_params p;
+    check(gmg_mg_params_default(&p));
+    return p;
+  }
+  MultiGridPreconditioner(WilsonCloverFermion& fine, const gmg_mg_params& p, int max_rhs, gmg_stream s = nullptr)
+      : stream_(s) {
+    check(gmg_mg_create(fine.handle(), &p, max_rhs, &h_));
+  }
+  ~MultiGridPreconditioner() { gmg_mg_destroy(h_); }
+  MultiGridPreconditioner(const MultiGridPreconditioner&) = delete;
+  MultiGridPreconditioner& operator=(const MultiGridPreconditioner&) = delete;
+  gmg_mg* handle() const { return h_; }
+
+  void initialSetup() { check(gmg_mg_setup(h_, stream_)); }
+  void refinementSetup() { check(gmg_mg_refine(h_, stream_)); }
+  int Solve(const Field& b, Field& x, double tol, int maxiter, double* max_relres = nullptr) {
+    int it = 0;
+    double rr = 0;
+    check(gmg_mg_solve(h_, b.nrhs, static_cast<const double*>(b.data), static_cast<double*>(x.data), tol, maxiter,
+                       &it, &rr, stream_));
+    if (max_relres) *max_relres = rr;
+    return it;
+  }
+  // the coarse operator of level > 0 and the aggregation from level to level+1
+  // (owned by the hierarchy)
+  gmg_coarse* CoarseMatrix(int level) {
+    gmg_coarse* op = nullptr;
+    check(gmg_mg_level(h_, level, &op, nullptr));
+    return op;
+  }
+  gmg_agg* Aggregates(int level) {
+    gmg_agg* agg = nullptr;
+    check(gmg_mg_level(h_, level, nullptr, &agg));
+    return agg;
+  }
+
+ private:
+  gmg_stream stream_;
+  gmg_mg* h_ = nullptr;
 };
 
 inline void PickCheckerboard(int cb, const std::array<int, 4>& dims, const Field& full, Field& half, gmg_stream s) {

@@ -88,3 +88,30 @@ def test_bad_arguments_return_status(lib):
     ok = (ctypes.c_int * 4)(4, 4, 4, 4)
     assert lib.gmg_coarse_create(ok, 7, 0, ctypes.byref(h)) == 1  # odd nbasis
     assert lib.gmg_lut_build(ok, (ctypes.c_int * 4)(3, 4, 4, 4), -1, None, None, None) == 1
+
+
+def test_mg_params_layout_and_defaults(lib, tmp_path):
+    # the Python binding's gmg_mg_params matches the C layout field by field,
+    # and the defaults carry MultiGridParams' refinement defaults
+    # (MultigridParams.h:99, :105: setupRefinementIter {0, 0},
+    # setupRecursiveUpdates true)
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "grid-mg-bench_b200"))
+    import gmg
+    fields = [f[0] for f in gmg.MGParams._fields_]
+    src = tmp_path / "layout.c"
+    body = "".join(f'  printf("%zu\\n", offsetof(gmg_mg_params, {f}));\n' for f in fields)
+    src.write_text('#include <stdio.h>\n#include "gmg.h"\nint main(void) {\n'
+                   '  printf("%zu\\n", sizeof(gmg_mg_params));\n' + body + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [ctypes.sizeof(gmg.MGParams)] + [getattr(gmg.MGParams, f).offset for f in fields]
+    assert got == want
+    p = gmg.MGParams()
+    lib.gmg_mg_params_default.argtypes = [ctypes.c_void_p]
+    assert lib.gmg_mg_params_default(ctypes.addressof(p)) == 0
+    assert list(p.refine_iters) == [0, 0] and p.recursive_updates == 1
+    assert p.nlevels == 3 and list(p.nvec) == [12, 16] and p.graph == 1
+    # the refinement checks its handle before touching the device
+    assert lib.gmg_mg_refine(None, None) != 0
