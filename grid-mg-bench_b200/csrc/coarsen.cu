@@ -208,11 +208,134 @@ static gmg_status coarsen_generic(gmg_coarse* out, gmg_agg* agg, const FineOpRef
   return GMG_OK;
 }
 
+// Workspace of the Wilson-clover coarsening, built on the first call and kept
+// in the aggregation: the batch size comes from the free memory then (two
+// fields of it in a third of it, at most 40 GB), the face lists and block
+// parities from the geometry.
+static gmg_status coarsen_workspace(gmg_agg* agg, cudaStream_t s) {
+  if (agg->cw_nb > 0) return GMG_OK;
+  const Dims& fd = agg->fdims;
+  const int64_t Vf = fd.vol(), Vc = agg->cdims.vol();
+  const int N = agg->N, dof = agg->dof;
+  size_t free_b = 0, total_b = 0;
+  GMG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const double cap = std::min(40.0e9, (double)free_b / 3.0) / 2.0;
+  int nb = N;
+  while (nb > 1 && (double)Vf * nb * dof * 16.0 > cap) nb = (nb + 1) / 2;
+  const size_t fbytes = sizeof(double2) * (size_t)Vf * nb * dof;
+  GMG_TRY(agg->cw_phi.alloc(fbytes));
+  GMG_TRY(agg->cw_w.alloc(fbytes));
+  GMG_TRY(agg->cw_proj.alloc(sizeof(double2) * (size_t)Vc * nb * N));
+  std::vector<int32_t> face, sel;
+  std::vector<int8_t> bpar(Vf);
+  for (int d = 0; d < 4; ++d) {
+    agg->cw_nface[d] = 0;
+    for (int64_t x = 0; x < Vf; ++x) {
+      int64_t t = x;
+      int c = 0;
+      for (int q = 0; q <= d; ++q) {
+        c = (int)(t % fd.d[q]);
+        t /= fd.d[q];
+      }
+      if (c % agg->b[d] == 0) {
+        face.push_back((int32_t)x);
+        ++agg->cw_nface[d];
+      }
+    }
+    agg->cw_nsel[d] = 0;
+    for (int k = 0; k < agg->bv; ++k) {
+      int t = k, lc[4];
+      for (int q = 0; q < 4; ++q) {
+        lc[q] = t % agg->b[q];
+        t /= agg->b[q];
+      }
+      if (lc[d] == 0) {
+        sel.push_back(k);
+        ++agg->cw_nsel[d];
+      }
+    }
+  }
+  for (int64_t x = 0; x < Vf; ++x) {
+    int64_t t = x;
+    int par = 0;
+    for (int q = 0; q < 4; ++q) {
+      par += (int)(t % fd.d[q]) / agg->b[q];
+      t /= fd.d[q];
+    }
+    bpar[x] = (int8_t)(par & 1);
+  }
+  GMG_TRY(agg->cw_face.alloc(sizeof(int32_t) * face.size()));
+  GMG_TRY(agg->cw_sel.alloc(sizeof(int32_t) * sel.size()));
+  GMG_TRY(agg->cw_bpar.alloc(bpar.size()));
+  GMG_CUDA(cudaMemcpyAsync(agg->cw_face.p, face.data(), sizeof(int32_t) * face.size(), cudaMemcpyHostToDevice, s));
+  GMG_CUDA(cudaMemcpyAsync(agg->cw_sel.p, sel.data(), sizeof(int32_t) * sel.size(), cudaMemcpyHostToDevice, s));
+  GMG_CUDA(cudaMemcpyAsync(agg->cw_bpar.p, bpar.data(), bpar.size(), cudaMemcpyHostToDevice, s));
+  GMG_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
+  agg->cw_nb = nb;
+  return GMG_OK;
+}
+
+// CoarsenOperator over the Wilson-clover operator.  Per batch of basis
+// vectors: the backward hop Mdir_p evaluated on the face sites only (the only
+// sites its face projection reads), and the self term e D e + o D o as one
+// pass of the operator with the hops between blocks of opposite parity left
+// out.  Both give, at every site the projections read, the same sums in the
+// same order as the masked full-lattice form of coarsen_generic.
+static gmg_status coarsen_wilson_faces(gmg_coarse* out, gmg_agg* agg, gmg_wilson* w, cudaStream_t s) {
+  const int dof = 12;
+  GMG_CHECK(agg->dof == dof, GMG_ERR_SHAPE, "coarsen: aggregation site dof differs from the fine operator");
+  for (int d = 0; d < 4; ++d) {
+    GMG_CHECK(agg->fdims.d[d] == w->dims.d[d], GMG_ERR_SHAPE, "coarsen: fine lattice differs");
+    GMG_CHECK(agg->cdims.d[d] == out->dims.d[d], GMG_ERR_SHAPE, "coarsen: coarse lattice differs");
+  }
+  GMG_CHECK(agg->N == out->N, GMG_ERR_SHAPE, "coarsen: nbasis differs");
+  GMG_CHECK(agg->basis_set, GMG_ERR_STATE, "coarsen: basis not set");
+  const int N = agg->N;
+  const int64_t Vc = out->dims.vol();
+  GMG_TRY(out->links_ref.alloc(sizeof(double2) * 9 * Vc * N * N));
+  GMG_CUDA(cudaMemsetAsync(out->links_ref.p, 0, sizeof(double2) * 9 * Vc * N * N, s));
+  GMG_TRY(coarsen_workspace(agg, s));
+  const int nb = agg->cw_nb;
+  double* phi = agg->cw_phi.as<double>();
+  double* wf = agg->cw_w.as<double>();
+  double* proj = agg->cw_proj.as<double>();
+  const int32_t* face = agg->cw_face.as<int32_t>();
+  const int32_t* sel = agg->cw_sel.as<int32_t>();
+  double2* A = out->links_ref.as<double2>();
+  for (int i0 = 0; i0 < N; i0 += nb) {
+    const int cur = std::min(nb, N - i0);
+    basis_gather_kernel<<<gsz(Vc * cur * agg->bv * dof), 256, 0, s>>>(
+        agg->basis_blk.as<double2>(), agg->blk_sites.as<int32_t>(), reinterpret_cast<double2*>(phi), Vc, N,
+        agg->bv, dof, i0, cur);
+    GMG_CUDA(cudaGetLastError());
+    int fo = 0, so = 0;
+    for (int d = 0; d < 4; ++d) {
+      GMG_TRY(wilson_apply_sel(w, GMG_OP_MDIR, d, -1, cur, phi, wf, face + fo, agg->cw_nface[d], nullptr, s));
+      GMG_TRY(agg_project_sel_f64(agg, cur, wf, proj, sel + so, agg->cw_nsel[d], s));
+      link_scatter_kernel<<<gsz(Vc * cur * N), 256, 0, s>>>(reinterpret_cast<const double2*>(proj),
+                                                             A + (int64_t)(4 + d) * Vc * N * N, Vc, N, i0, cur);
+      GMG_CUDA(cudaGetLastError());
+      fo += agg->cw_nface[d];
+      so += agg->cw_nsel[d];
+    }
+    GMG_TRY(wilson_apply_sel(w, GMG_OP_M, 0, 0, cur, phi, wf, nullptr, 0, agg->cw_bpar.as<int8_t>(), s));
+    GMG_TRY(agg_project_masked_f64(agg, cur, wf, proj, nullptr, s));
+    link_scatter_kernel<<<gsz(Vc * cur * N), 256, 0, s>>>(reinterpret_cast<const double2*>(proj),
+                                                           A + (int64_t)8 * Vc * N * N, Vc, N, i0, cur);
+    GMG_CUDA(cudaGetLastError());
+  }
+  GMG_TRY(coarse_construct_remaining(out, s));
+  GMG_TRY(coarse_links_to_site_major(out, s));
+  out->links_set = true;
+  out->links_f_ok = false;
+  out->self_inv_ok = out->self_inv_f_ok = false;
+  out->links_h.kind = -1;
+  return GMG_OK;
+}
+
 gmg_status coarsen_wilson(gmg_coarse* out, gmg_agg* agg, gmg_wilson* fine, cudaStream_t s) {
   GMG_CHECK(fine->gauge_set, GMG_ERR_STATE, "coarsen: gauge field not set");
-  FineOpRef op;
-  op.w = fine;
-  return coarsen_generic(out, agg, op, s);
+  return coarsen_wilson_faces(out, agg, fine, s);
 }
 
 gmg_status coarsen_coarse(gmg_coarse* out, gmg_agg* agg, gmg_coarse* fine, cudaStream_t s) {

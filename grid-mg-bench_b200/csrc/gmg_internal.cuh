@@ -124,6 +124,13 @@ struct gmg_agg {
   bool basis_tc_ok = false;
   gmg::DevBuf scratch;
   gmg::DevBuf dev_err;  // int: error code recorded by the tensor-core kernels
+  // CoarsenOperator workspace over the Wilson-clover operator (coarsen.cu),
+  // kept between calls: fine fields of one batch of cw_nb basis vectors, the
+  // projection output, per direction the fine sites of the backward faces
+  // (global, cw_face) and their in-block indices (cw_sel), block parity per site
+  gmg::DevBuf cw_phi, cw_w, cw_proj, cw_face, cw_sel, cw_bpar;
+  int cw_nb = 0;
+  int cw_nface[4] = {0, 0, 0, 0}, cw_nsel[4] = {0, 0, 0, 0};
 };
 
 struct gmg_wilson {
@@ -194,6 +201,8 @@ gmg_status agg_promote_tc(gmg_agg* h, int nrhs, const float* coarse, float* fine
 
 // fine Wilson-clover (wilson.cu)
 gmg_status wilson_build_clover(gmg_wilson* h, cudaStream_t s);
+gmg_status wilson_apply_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, const double* in, double* out,
+                            const int32_t* sel, int nsel, const int8_t* bpar, cudaStream_t s);
 gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs,
                         const void* in, void* out, cudaStream_t s);
 gmg_status wilson_apply_mr(gmg_wilson* h, int vec_prec, int nrhs, const void* in, void* out, double2* d1,

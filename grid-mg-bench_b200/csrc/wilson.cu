@@ -148,13 +148,16 @@ __device__ __forceinline__ void st12(typename wt<T>::C* __restrict__ p, const ty
 }
 
 // DOTS (op M or MDAG): also add <out, in> and <out, out> of this (site, r) to
-// dsum[0..1] and dsum[2].  VEC: 16-byte spinor accesses.
+// dsum[0..1] and dsum[2].  VEC: 16-byte spinor accesses.  bpar (per-site
+// block parity, null for the plain operator): hops whose neighbour has the
+// other parity are left out, which gives e D e + o D o of the coarsening's
+// self term in one pass.
 template <class T, class LinkFn, bool DOTS = false, bool VEC = false>
 __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict__ cl, LinkFn links,
                                             const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
                                             typename wt<T>::C* __restrict__ out, int V, int nrhs, int site, int r,
                                             T diag, int op, int dir, int disp, int apbc, int tvol, int Lt,
-                                            double* dsum = nullptr) {
+                                            double* dsum = nullptr, const int8_t* __restrict__ bpar = nullptr) {
   typedef typename wt<T>::C C;
   const bool g5 = (op == GMG_OP_MDAG);
   const int tc = site / tvol;
@@ -191,6 +194,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
       const int dsp = p < 4 ? 1 : -1;
       if (op == GMG_OP_MDIR && (mu != dir || dsp != disp)) continue;
       const int nb = nbr[(int64_t)p * V + site];
+      if (bpar && bpar[nb] != bpar[site]) continue;
       T coef = (T)-0.5;
       if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
       C psi[12];
@@ -258,12 +262,17 @@ constexpr int kTileSites = 16;
 // sites' 8 hop links and clover blocks are staged in shared memory once and
 // read by every RHS of the tile.  Thread per (site, RHS) otherwise, spinors
 // read from global memory.
-template <class T, bool DOTS, int MINB>
+// SEL (the coarsening's forms, compiled separately): the tiles run over the
+// nsel sites of the list `sel` (all V sites when null) and only those are
+// written; a single-hop op stages only its link; bpar restricts the hops to
+// neighbours of the same block parity (see wilson_site).
+template <class T, bool DOTS, int MINB, bool SEL = false>
 __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
     const typename wt<T>::C* __restrict__ hop, const typename wt<T>::C* __restrict__ clover,
     const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
     typename wt<T>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
-    int apbc, int tvol, int Lt, double2* __restrict__ d1, double2* __restrict__ d2) {
+    int apbc, int tvol, int Lt, double2* __restrict__ d1, double2* __restrict__ d2,
+    const int32_t* __restrict__ sel = nullptr, int nsel = 0, const int8_t* __restrict__ bpar = nullptr) {
   typedef typename wt<T>::C C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* Ls = reinterpret_cast<C*>(smem_raw);  // [kTileSites][8][9]: p < 4 U_mu(x), p >= 4 U_mu(x - mu)
@@ -271,21 +280,36 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
   double* Ds = reinterpret_cast<double*>(Cs + kTileSites * 72);  // DOTS: [nrhs][3]
   if (DOTS)
     for (int k = threadIdx.x; k < 3 * nrhs; k += blockDim.x) Ds[k] = 0.0;
-  const int nt = (V + kTileSites - 1) / kTileSites;
+  const int nsites = (SEL && sel) ? nsel : V;
+  const int nt = (nsites + kTileSites - 1) / kTileSites;
   const int sl = threadIdx.x / rt, rl = threadIdx.x % rt;
   const bool two = nrhs <= 2 * rt;
   double da[3] = {0.0, 0.0, 0.0}, db[3] = {0.0, 0.0, 0.0};
   for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
     const int s0 = tile * kTileSites;
-    const int ns = min(kTileSites, V - s0);
+    const int ns = min(kTileSites, nsites - s0);
     __syncthreads();
-    for (int k = threadIdx.x; k < ns * 72; k += blockDim.x) {
-      Ls[k] = hop[(int64_t)s0 * 72 + k];
-      Cs[k] = clover[(int64_t)s0 * 72 + k];
+    if (!SEL) {
+      for (int k = threadIdx.x; k < ns * 72; k += blockDim.x) {
+        Ls[k] = hop[(int64_t)s0 * 72 + k];
+        Cs[k] = clover[(int64_t)s0 * 72 + k];
+      }
+    } else if (op == GMG_OP_MDIR) {
+      const int pl = (disp > 0 ? 0 : 4) + dir;
+      for (int k = threadIdx.x; k < ns * 9; k += blockDim.x) {
+        const int64_t st = sel ? sel[s0 + k / 9] : s0 + k / 9;
+        Ls[(k / 9) * 72 + pl * 9 + k % 9] = hop[st * 72 + pl * 9 + k % 9];
+      }
+    } else {
+      for (int k = threadIdx.x; k < ns * 72; k += blockDim.x) {
+        const int64_t st = sel ? sel[s0 + k / 72] : s0 + k / 72;
+        Ls[k] = hop[st * 72 + k % 72];
+        Cs[k] = clover[st * 72 + k % 72];
+      }
     }
     __syncthreads();
     if (sl < ns) {
-      const int site = s0 + sl;
+      const int site = (SEL && sel) ? sel[s0 + sl] : s0 + sl;
       const C* lsite = Ls + sl * 72;
       auto links = [&](int p, int) -> const C* { return lsite + p * 9; };
       // with two RHS or fewer per thread (rl, rl + rt) the thread owns them for
@@ -294,7 +318,7 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
       for (int r = rl; r < nrhs; r += rt, ++k) {
         double dt[3] = {0.0, 0.0, 0.0};
         wilson_site<T, decltype(links), DOTS, true>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op,
-                                                    dir, disp, apbc, tvol, Lt, dt);
+                                                    dir, disp, apbc, tvol, Lt, dt, SEL ? bpar : nullptr);
         if (DOTS) {
           if (two) {
 #pragma unroll
@@ -1282,6 +1306,36 @@ static gmg_status wilson_dispatch(gmg_wilson* h, bool dots, int op, int dir, int
   GMG_TRY(zero_dots());
   GMG_TRY(run_variant(h, best, dots, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, &launched));
   if (!launched) return fail(GMG_ERR_UNSUPPORTED, "wilson apply: no kernel variant applies");
+  return GMG_OK;
+}
+
+// The coarsening's forms of the FP64 operator (tile kernel, SEL instance):
+// op on the nsel sites of `sel` only (all sites when null; the other sites of
+// `out` are not written), and with bpar the hops restricted to neighbours of
+// the same block parity.
+gmg_status wilson_apply_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, const double* in, double* out,
+                            const int32_t* sel, int nsel, const int8_t* bpar, cudaStream_t s) {
+  const int V = (int)h->dims.vol();
+  const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
+  int rt = 1;
+  for (int c = std::min(nrhs, 16); c >= 1; --c)
+    if (nrhs % c == 0) {
+      rt = c;
+      break;
+    }
+  if (nrhs > 16 && rt < 8) rt = 16;
+  const int nsites = sel ? nsel : V;
+  if (nsites == 0) return GMG_OK;
+  const int tiles = (nsites + kTileSites - 1) / kTileSites;
+  const int g = std::min(tiles, 148 * 16);
+  const size_t smem = sizeof(double2) * 2 * kTileSites * 72;
+  auto k = wilson_tile_kernel<double, false, 2, true>;
+  if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  KernelTimer kt("wilson", s);
+  k<<<g, kTileSites * rt, smem, s>>>(h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(),
+                                     (const double2*)in, (double2*)out, V, nrhs, rt, 4.0 + h->mass, op, dir, disp,
+                                     h->apbc, tvol, h->dims.d[3], nullptr, nullptr, sel, nsel, bpar);
+  GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
 

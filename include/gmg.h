@@ -281,7 +281,11 @@ gmg_status gmg_wilson_apply_mr(gmg_wilson* h, gmg_prec vec_prec, int nrhs, const
 
 /* Links of `out` from the fine Wilson-clover operator and the basis of `agg`
    (backward projections + self term by the block even/odd trick + link
-   reconstruction), FP64. */
+   reconstruction), FP64.  The backward hops are evaluated on the face sites
+   only, and the self term as one operator pass without the hops between
+   blocks of opposite parity.  The first call keeps a workspace in `agg` (two
+   fine fields of a batch of basis vectors, at most 40 GB, sized from the free
+   memory then) that later calls reuse; it is freed with `agg`.  Asynchronous. */
 gmg_status gmg_coarsen_wilson(gmg_coarse* out, gmg_agg* agg, gmg_wilson* fine, gmg_stream s);
 /* Coarse-of-coarse: the fine operator is the coarse stencil `fine`. */
 gmg_status gmg_coarsen_coarse(gmg_coarse* out, gmg_agg* agg, gmg_coarse* fine, gmg_stream s);

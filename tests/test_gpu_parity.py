@@ -436,6 +436,28 @@ def test_coarsen_wilson_matches_oracle(coarsen_setup, apbc):
         assert orc.rel_dev_sq(ref[p], got[p]) < TOL64, p
 
 
+def test_coarsen_wilson_anisotropic_blocks_and_reuse():
+    # blocks of a different extent per direction (each backward face its own
+    # site list), and a second call on the same aggregation with a new basis
+    # (the workspace kept from the first call) against the oracle both times
+    fd, cd = (8, 4, 8, 8), (2, 2, 4, 2)
+    U = inputs.hot_gauge(fd, inputs.rng(stream=135))
+    w = gmg.WilsonClover(fd, -0.2, 1.0, antiperiodic=1)
+    w.set_gauge(U)
+    cl = orc.clover_build(fd, U, 1.0)
+    ag = gmg.Aggregation(fd, cd, 12, 6)
+    for stream in (136, 137):
+        h = inputs.gaussian_field((3, int(np.prod(fd)), 12), inputs.rng(stream=stream))
+        B = orc.block_orthonormalise(fd, cd, orc.chiral_double(h, 0.5), passes=1)
+        ag.set_basis(B)
+        cm = gmg.CoarsenedMatrix(cd, 6)
+        cm.CoarsenOperator(ag, w)
+        ref = orc.coarsen_wilson(fd, cd, B, U, cl, -0.2, 1, 0, variant=0)
+        got = cm.get_links()
+        for p in range(9):
+            assert orc.rel_dev_sq(ref[p], got[p]) < TOL64, (stream, p)
+
+
 def test_coarsen_coarse_matches_oracle(coarsen_setup):
     fd, cd, U, B = coarsen_setup
     c1 = (4, 4, 4, 4)
