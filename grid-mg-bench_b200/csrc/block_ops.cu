@@ -248,12 +248,157 @@ static gmg_status launch_project(gmg_agg* h, const void* basis, int nrhs, const 
   return GMG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// FP64 projection of spin-colour fields (dof 12, nrhs >= 4), pipelined: the
+// same sums as project_kernel, with
+//   - the next KS-site chunk of basis and fine field copied into the second
+//     shared-memory buffer (cp.async, 16 B per complex number, written
+//     straight into the transposed [k][N] / [k][R] tiles) while the current
+//     one is multiplied, so the global loads no longer stall the FMA loop;
+//   - basis rows and RHS interleaved over the threads (thread (bt, rt) owns
+//     rows bt + NBT i and RHS rt + NRT j), so the 16-byte shared loads of
+//     neighbouring threads fall on consecutive banks;
+//   - the chunk's index arithmetic on compile-time strides.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N_>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N_) : "memory"); }
+
+template <int DOF, int KS, int TR, int TB>
+__global__ void __launch_bounds__(128) project_f64_pipe_kernel(
+    const double2* __restrict__ basis, const int32_t* __restrict__ blk_sites, const double2* __restrict__ fine,
+    double2* __restrict__ coarse, int Vc, int N, int bv, int nrhs, const int32_t* __restrict__ sel, int nsel) {
+  constexpr int KC = KS * DOF;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int R = nrhs;
+  double2* buf0 = reinterpret_cast<double2*>(smem_raw);  // per buffer: VT [KC][N], FT [KC][R]
+  const int bufsz = KC * (N + R);
+  const int NBT = (N + TB - 1) / TB, NRT = (R + TR - 1) / TR;
+  const int ntiles = NBT * NRT;
+  const int t = threadIdx.x, bt = t % NBT, rt = t / NBT;
+  const int64_t K = (int64_t)bv * DOF;
+  const int nsites = sel ? nsel : bv;
+  const int nch = (nsites + KS - 1) / KS;
+  for (int c = blockIdx.x; c < Vc; c += gridDim.x) {
+    const double2* Vb = basis + (int64_t)c * N * K;
+    // copies of chunk ch into buffer b (sites beyond nsites are skipped; the
+    // multiply loop stops at the chunk's own length)
+    auto issue = [&](int ch, int b) {
+      double2* VT = buf0 + b * bufsz;
+      double2* FT = VT + KC * N;
+      const int sb0 = ch * KS;
+      const int ns = min(KS, nsites - sb0);
+      for (int e = t; e < N * KC; e += blockDim.x) {
+        const int i = e / KC, kk = e % KC;
+        const int sl = kk / DOF, a = kk % DOF;
+        if (sl < ns) {
+          const int sb = sel ? sel[sb0 + sl] : sb0 + sl;
+          cp_async16(VT + kk * N + i, Vb + (int64_t)i * K + (int64_t)sb * DOF + a);
+        }
+      }
+      for (int sl = 0; sl < ns; ++sl) {
+        const int64_t sf = blk_sites[(int64_t)c * bv + (sel ? sel[sb0 + sl] : sb0 + sl)];
+        const double2* src = fine + sf * nrhs * DOF;
+        for (int e = t; e < R * DOF; e += blockDim.x) {
+          const int r = e / DOF, a = e % DOF;
+          cp_async16(FT + (sl * DOF + a) * R + r, src + e);
+        }
+      }
+      cp_async_commit();
+    };
+    double2 acc[TR][TB];
+#pragma unroll
+    for (int j = 0; j < TR; ++j)
+#pragma unroll
+      for (int i = 0; i < TB; ++i) acc[j][i] = make_double2(0.0, 0.0);
+    __syncthreads();  // the previous block's last chunk is no longer read
+    issue(0, 0);
+    for (int ch = 0; ch < nch; ++ch) {
+      if (ch + 1 < nch) {
+        issue(ch + 1, (ch + 1) & 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
+      const double2* VT = buf0 + (ch & 1) * bufsz;
+      const double2* FT = VT + KC * N;
+      const int kc = min(KS, nsites - ch * KS) * DOF;
+      if (t < ntiles) {
+        for (int kk = 0; kk < kc; ++kk) {
+          double2 a[TB], x[TR];
+#pragma unroll
+          for (int i = 0; i < TB; ++i) {
+            const int ii = bt + NBT * i;
+            a[i] = ii < N ? VT[kk * N + ii] : make_double2(0.0, 0.0);
+          }
+#pragma unroll
+          for (int j = 0; j < TR; ++j) {
+            const int r = rt + NRT * j;
+            x[j] = r < R ? FT[kk * R + r] : make_double2(0.0, 0.0);
+          }
+#pragma unroll
+          for (int j = 0; j < TR; ++j)
+#pragma unroll
+            for (int i = 0; i < TB; ++i) acc[j][i] = cfma_conj(acc[j][i], a[i], x[j]);
+        }
+      }
+      __syncthreads();  // buffer (ch & 1) is refilled by the issue of chunk ch + 2
+    }
+    if (t < ntiles) {
+#pragma unroll
+      for (int j = 0; j < TR; ++j) {
+        const int r = rt + NRT * j;
+        if (r >= R) continue;
+#pragma unroll
+        for (int i = 0; i < TB; ++i) {
+          const int ii = bt + NBT * i;
+          if (ii < N) coarse[((int64_t)c * nrhs + r) * N + ii] = acc[j][i];
+        }
+      }
+    }
+  }
+}
+
+// the pipelined FP64 projection when it applies (dof 12, 4 <= nrhs, tiles and
+// two buffers within limits); *launched = false otherwise
+static gmg_status launch_project_f64_pipe(gmg_agg* h, int nrhs, const void* fine, void* coarse, const int32_t* sel,
+                                          int nsel, cudaStream_t s, bool* launched) {
+  constexpr int KS = 2, TR = 4, TB = 4;
+  *launched = false;
+  const int N = h->N, R = nrhs;
+  if (h->dof != 12 || R < 4 || (reinterpret_cast<uintptr_t>(fine) & 15)) return GMG_OK;
+  const int ntiles = ((N + TB - 1) / TB) * ((R + TR - 1) / TR);
+  if (ntiles > 128) return GMG_OK;
+  const size_t smem = sizeof(double2) * 2 * (size_t)KS * 12 * (N + R);
+  if (smem > 200 * 1024) return GMG_OK;
+  auto kern = project_f64_pipe_kernel<12, KS, TR, TB>;
+  GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int Vc = (int)h->cdims.vol();
+  const int grid = std::min(Vc, num_sms() * 16);
+  KernelTimer kt("project", s);
+  kern<<<grid, 128, smem, s>>>(h->basis_blk.as<double2>(), h->blk_sites.as<int32_t>(),
+                               reinterpret_cast<const double2*>(fine), reinterpret_cast<double2*>(coarse), Vc, N,
+                               h->bv, nrhs, sel, nsel);
+  GMG_CUDA(cudaGetLastError());
+  *launched = true;
+  return GMG_OK;
+}
+
 gmg_status agg_project(gmg_agg* h, int compute, int vec_prec, int nrhs, const void* fine,
                        void* coarse, const int32_t* mask_unused, cudaStream_t s) {
   (void)mask_unused;
   if (compute == GMG_BF16 && vec_prec == GMG_F32) return agg_project_tc(h, nrhs, (const float*)fine, (float*)coarse, s);
   GMG_CHECK(compute == vec_prec, GMG_ERR_UNSUPPORTED, "project: compute and vector precision differ");
   if (compute == GMG_F64) {
+    bool done = false;
+    GMG_TRY(launch_project_f64_pipe(h, nrhs, fine, coarse, nullptr, 0, s, &done));
+    if (done) return GMG_OK;
     if (nrhs >= 4) return launch_project<double, 4, 4, 4>(h, h->basis_blk.p, nrhs, fine, coarse, nullptr, 0, s);
     return launch_project<double, 1, 2, 4>(h, h->basis_blk.p, nrhs, fine, coarse, nullptr, 0, s);
   }
@@ -270,6 +415,9 @@ gmg_status agg_project(gmg_agg* h, int compute, int vec_prec, int nrhs, const vo
 // the coarse-operator construction
 gmg_status agg_project_sel_f64(gmg_agg* h, int nrhs, const double* fine, double* coarse, const int32_t* sel,
                                int nsel, cudaStream_t s) {
+  bool done = false;
+  GMG_TRY(launch_project_f64_pipe(h, nrhs, fine, coarse, sel, nsel, s, &done));
+  if (done) return GMG_OK;
   if (nrhs >= 4)
     return launch_project<double, 4, 4, 4>(h, h->basis_blk.p, nrhs, fine, coarse, nullptr, 0, s, sel, nsel);
   return launch_project<double, 1, 2, 4>(h, h->basis_blk.p, nrhs, fine, coarse, nullptr, 0, s, sel, nsel);
@@ -278,6 +426,11 @@ gmg_status agg_project_sel_f64(gmg_agg* h, int nrhs, const double* fine, double*
 // masked FP64 single-RHS projection used by the coarse-operator construction
 gmg_status agg_project_masked_f64(gmg_agg* h, int nrhs, const double* fine, double* coarse,
                                   const int8_t* mask, cudaStream_t s) {
+  if (!mask) {
+    bool done = false;
+    GMG_TRY(launch_project_f64_pipe(h, nrhs, fine, coarse, nullptr, 0, s, &done));
+    if (done) return GMG_OK;
+  }
   if (nrhs >= 4) return launch_project<double, 4, 4, 4>(h, h->basis_blk.p, nrhs, fine, coarse, mask, 0, s);
   return launch_project<double, 1, 2, 4>(h, h->basis_blk.p, nrhs, fine, coarse, mask, 0, s);
 }

@@ -220,11 +220,15 @@ def test_project_promote_f64(agg8, nrhs):
 @pytest.mark.parametrize("fd,cd,dof,N,R", [((8, 8, 8, 8), (2, 2, 2, 2), 12, 24, 12),
                                           ((8, 8, 8, 8), (4, 4, 4, 4), 12, 40, 20),
                                           ((4, 4, 4, 4), (2, 2, 2, 2), 16, 16, 4),
-                                          ((4, 4, 4, 4), (2, 2, 2, 2), 40, 40, 40)])
+                                          ((4, 4, 4, 4), (2, 2, 2, 2), 40, 40, 40),
+                                          ((8, 8, 8, 8), (2, 2, 2, 2), 12, 40, 40),
+                                          ((8, 8, 8, 8), (4, 4, 4, 4), 12, 10, 7),
+                                          ((6, 4, 4, 4), (2, 4, 4, 4), 12, 6, 5)])
 def test_project_f64_shapes(fd, cd, dof, N, R):
     # FP64 projections of fine-site (dof 12) and coarse-site (dof 16, 40)
     # aggregations: several K chunks per block, register tiles cut by nbasis
-    # and nrhs that are not multiples of the tile
+    # and nrhs that are not multiples of the tile, and a block of 3 sites (the
+    # pipelined kernel's last chunk of a block shorter than the others)
     Vf = int(np.prod(fd))
     B = inputs.gaussian_field((N, Vf, dof), inputs.rng(stream=180 + N))
     ag = gmg.Aggregation(fd, cd, dof, N)
