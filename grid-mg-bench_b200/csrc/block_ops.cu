@@ -269,44 +269,48 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N_>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N_) : "memory"); }
 
-template <int DOF, int KS, int TR, int TB>
-__global__ void __launch_bounds__(128) project_f64_pipe_kernel(
+template <int DOF, int KS, int TR, int TB, int NT>
+__global__ void __launch_bounds__(NT, 384 / NT) project_f64_pipe_kernel(
     const double2* __restrict__ basis, const int32_t* __restrict__ blk_sites, const double2* __restrict__ fine,
     double2* __restrict__ coarse, int Vc, int N, int bv, int nrhs, const int32_t* __restrict__ sel, int nsel) {
   constexpr int KC = KS * DOF;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int R = nrhs;
-  double2* buf0 = reinterpret_cast<double2*>(smem_raw);  // per buffer: VT [KC][N], FT [KC][R]
-  const int bufsz = KC * (N + R);
   const int NBT = (N + TB - 1) / TB, NRT = (R + TR - 1) / TR;
+  // tile widths padded to whole register tiles; the pad columns are zeroed
+  // once and never copied to, so the multiply loop needs no bounds tests
+  const int Np = NBT * TB, Rq = NRT * TR;
+  double2* buf0 = reinterpret_cast<double2*>(smem_raw);  // per buffer: VT [KC][Np], FT [KC][Rq]
+  const int bufsz = KC * (Np + Rq);
   const int ntiles = NBT * NRT;
   const int t = threadIdx.x, bt = t % NBT, rt = t / NBT;
   const int64_t K = (int64_t)bv * DOF;
   const int nsites = sel ? nsel : bv;
   const int nch = (nsites + KS - 1) / KS;
+  for (int e = t; e < 2 * bufsz; e += NT) buf0[e] = make_double2(0.0, 0.0);
   for (int c = blockIdx.x; c < Vc; c += gridDim.x) {
     const double2* Vb = basis + (int64_t)c * N * K;
     // copies of chunk ch into buffer b (sites beyond nsites are skipped; the
     // multiply loop stops at the chunk's own length)
     auto issue = [&](int ch, int b) {
       double2* VT = buf0 + b * bufsz;
-      double2* FT = VT + KC * N;
+      double2* FT = VT + KC * Np;
       const int sb0 = ch * KS;
       const int ns = min(KS, nsites - sb0);
-      for (int e = t; e < N * KC; e += blockDim.x) {
+      for (int e = t; e < N * KC; e += NT) {
         const int i = e / KC, kk = e % KC;
         const int sl = kk / DOF, a = kk % DOF;
         if (sl < ns) {
           const int sb = sel ? sel[sb0 + sl] : sb0 + sl;
-          cp_async16(VT + kk * N + i, Vb + (int64_t)i * K + (int64_t)sb * DOF + a);
+          cp_async16(VT + kk * Np + i, Vb + (int64_t)i * K + (int64_t)sb * DOF + a);
         }
       }
       for (int sl = 0; sl < ns; ++sl) {
         const int64_t sf = blk_sites[(int64_t)c * bv + (sel ? sel[sb0 + sl] : sb0 + sl)];
         const double2* src = fine + sf * nrhs * DOF;
-        for (int e = t; e < R * DOF; e += blockDim.x) {
+        for (int e = t; e < R * DOF; e += NT) {
           const int r = e / DOF, a = e % DOF;
-          cp_async16(FT + (sl * DOF + a) * R + r, src + e);
+          cp_async16(FT + (sl * DOF + a) * Rq + r, src + e);
         }
       }
       cp_async_commit();
@@ -316,7 +320,7 @@ __global__ void __launch_bounds__(128) project_f64_pipe_kernel(
     for (int j = 0; j < TR; ++j)
 #pragma unroll
       for (int i = 0; i < TB; ++i) acc[j][i] = make_double2(0.0, 0.0);
-    __syncthreads();  // the previous block's last chunk is no longer read
+    __syncthreads();  // zeroing done / the previous block's last chunk is no longer read
     issue(0, 0);
     for (int ch = 0; ch < nch; ++ch) {
       if (ch + 1 < nch) {
@@ -326,22 +330,17 @@ __global__ void __launch_bounds__(128) project_f64_pipe_kernel(
         cp_async_wait<0>();
       }
       __syncthreads();
-      const double2* VT = buf0 + (ch & 1) * bufsz;
-      const double2* FT = VT + KC * N;
+      const double2* va = buf0 + (ch & 1) * bufsz + bt;
+      const double2* xa = buf0 + (ch & 1) * bufsz + KC * Np + rt;
       const int kc = min(KS, nsites - ch * KS) * DOF;
       if (t < ntiles) {
+#pragma unroll 1
         for (int kk = 0; kk < kc; ++kk) {
           double2 a[TB], x[TR];
 #pragma unroll
-          for (int i = 0; i < TB; ++i) {
-            const int ii = bt + NBT * i;
-            a[i] = ii < N ? VT[kk * N + ii] : make_double2(0.0, 0.0);
-          }
+          for (int i = 0; i < TB; ++i) a[i] = va[kk * Np + NBT * i];
 #pragma unroll
-          for (int j = 0; j < TR; ++j) {
-            const int r = rt + NRT * j;
-            x[j] = r < R ? FT[kk * R + r] : make_double2(0.0, 0.0);
-          }
+          for (int j = 0; j < TR; ++j) x[j] = xa[kk * Rq + NRT * j];
 #pragma unroll
           for (int j = 0; j < TR; ++j)
 #pragma unroll
@@ -365,27 +364,42 @@ __global__ void __launch_bounds__(128) project_f64_pipe_kernel(
   }
 }
 
-// the pipelined FP64 projection when it applies (dof 12, 4 <= nrhs, tiles and
-// two buffers within limits); *launched = false otherwise
-static gmg_status launch_project_f64_pipe(gmg_agg* h, int nrhs, const void* fine, void* coarse, const int32_t* sel,
-                                          int nsel, cudaStream_t s, bool* launched) {
-  constexpr int KS = 2, TR = 4, TB = 4;
-  *launched = false;
+template <int KS, int TR, int TB, int NT>
+static gmg_status launch_pipe(gmg_agg* h, int nrhs, const void* fine, void* coarse, const int32_t* sel, int nsel,
+                              cudaStream_t s) {
   const int N = h->N, R = nrhs;
-  if (h->dof != 12 || R < 4 || (reinterpret_cast<uintptr_t>(fine) & 15)) return GMG_OK;
-  const int ntiles = ((N + TB - 1) / TB) * ((R + TR - 1) / TR);
-  if (ntiles > 128) return GMG_OK;
-  const size_t smem = sizeof(double2) * 2 * (size_t)KS * 12 * (N + R);
-  if (smem > 200 * 1024) return GMG_OK;
-  auto kern = project_f64_pipe_kernel<12, KS, TR, TB>;
+  const int Np = (N + TB - 1) / TB * TB, Rq = (R + TR - 1) / TR * TR;
+  const size_t smem = sizeof(double2) * 2 * (size_t)KS * 12 * (Np + Rq);
+  auto kern = project_f64_pipe_kernel<12, KS, TR, TB, NT>;
   GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int Vc = (int)h->cdims.vol();
   const int grid = std::min(Vc, num_sms() * 16);
   KernelTimer kt("project", s);
-  kern<<<grid, 128, smem, s>>>(h->basis_blk.as<double2>(), h->blk_sites.as<int32_t>(),
-                               reinterpret_cast<const double2*>(fine), reinterpret_cast<double2*>(coarse), Vc, N,
-                               h->bv, nrhs, sel, nsel);
+  kern<<<grid, NT, smem, s>>>(h->basis_blk.as<double2>(), h->blk_sites.as<int32_t>(),
+                              reinterpret_cast<const double2*>(fine), reinterpret_cast<double2*>(coarse), Vc, N, h->bv,
+                              nrhs, sel, nsel);
   GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+// the pipelined FP64 projection when it applies (dof 12, 4 <= nrhs, tiles and
+// two buffers within limits); *launched = false otherwise.  5 x 5 register
+// tiles on 64 threads when they fill more than one warp with nbasis and nrhs
+// up to 40 (the coarsening's 40 x 40: 64 threads, no idle lanes), else 4 x 4
+// on 128 threads.
+static gmg_status launch_project_f64_pipe(gmg_agg* h, int nrhs, const void* fine, void* coarse, const int32_t* sel,
+                                          int nsel, cudaStream_t s, bool* launched) {
+  *launched = false;
+  const int N = h->N, R = nrhs;
+  if (h->dof != 12 || R < 4 || (reinterpret_cast<uintptr_t>(fine) & 15)) return GMG_OK;
+  const int t5 = ((N + 4) / 5) * ((R + 4) / 5);
+  if (N <= 40 && R <= 40 && t5 > 32) {
+    GMG_TRY((launch_pipe<1, 5, 5, 64>(h, nrhs, fine, coarse, sel, nsel, s)));
+  } else {
+    const int t4 = ((N + 3) / 4) * ((R + 3) / 4);
+    if (t4 > 128 || sizeof(double2) * 2 * 2 * 12 * (size_t)(N + R + 6) > 200 * 1024) return GMG_OK;
+    GMG_TRY((launch_pipe<2, 4, 4, 128>(h, nrhs, fine, coarse, sel, nsel, s)));
+  }
   *launched = true;
   return GMG_OK;
 }

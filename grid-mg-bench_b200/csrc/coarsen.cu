@@ -227,7 +227,7 @@ static gmg_status coarsen_workspace(gmg_agg* agg, cudaStream_t s) {
   GMG_TRY(agg->cw_w.alloc(fbytes));
   GMG_TRY(agg->cw_proj.alloc(sizeof(double2) * (size_t)Vc * nb * N));
   std::vector<int32_t> face, sel;
-  std::vector<int8_t> bpar(Vf);
+  std::vector<uint8_t> bpar(Vf), hskip(Vf);
   for (int d = 0; d < 4; ++d) {
     agg->cw_nface[d] = 0;
     for (int64_t x = 0; x < Vf; ++x) {
@@ -262,14 +262,28 @@ static gmg_status coarsen_workspace(gmg_agg* agg, cudaStream_t s) {
       par += (int)(t % fd.d[q]) / agg->b[q];
       t /= fd.d[q];
     }
-    bpar[x] = (int8_t)(par & 1);
+    bpar[x] = (uint8_t)(par & 1);
+  }
+  // hop p = (mu = p mod 4, +1 for p < 4, -1 otherwise), periodic neighbours
+  int64_t stride[4] = {1, 1, 1, 1};
+  for (int q = 1; q < 4; ++q) stride[q] = stride[q - 1] * fd.d[q - 1];
+  for (int64_t x = 0; x < Vf; ++x) {
+    uint8_t m = 0;
+    for (int p = 0; p < 8; ++p) {
+      const int mu = p & 3;
+      const int xm = (int)((x / stride[mu]) % fd.d[mu]);
+      const int ym = (xm + (p < 4 ? 1 : fd.d[mu] - 1)) % fd.d[mu];
+      const int64_t y = x + (int64_t)(ym - xm) * stride[mu];
+      if (bpar[y] != bpar[x]) m |= (uint8_t)(1u << p);
+    }
+    hskip[x] = m;
   }
   GMG_TRY(agg->cw_face.alloc(sizeof(int32_t) * face.size()));
   GMG_TRY(agg->cw_sel.alloc(sizeof(int32_t) * sel.size()));
-  GMG_TRY(agg->cw_bpar.alloc(bpar.size()));
+  GMG_TRY(agg->cw_hskip.alloc(hskip.size()));
   GMG_CUDA(cudaMemcpyAsync(agg->cw_face.p, face.data(), sizeof(int32_t) * face.size(), cudaMemcpyHostToDevice, s));
   GMG_CUDA(cudaMemcpyAsync(agg->cw_sel.p, sel.data(), sizeof(int32_t) * sel.size(), cudaMemcpyHostToDevice, s));
-  GMG_CUDA(cudaMemcpyAsync(agg->cw_bpar.p, bpar.data(), bpar.size(), cudaMemcpyHostToDevice, s));
+  GMG_CUDA(cudaMemcpyAsync(agg->cw_hskip.p, hskip.data(), hskip.size(), cudaMemcpyHostToDevice, s));
   GMG_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
   agg->cw_nb = nb;
   return GMG_OK;
@@ -310,7 +324,7 @@ static gmg_status coarsen_wilson_faces(gmg_coarse* out, gmg_agg* agg, gmg_wilson
     GMG_CUDA(cudaGetLastError());
     int fo = 0, so = 0;
     for (int d = 0; d < 4; ++d) {
-      GMG_TRY(wilson_apply_sel(w, GMG_OP_MDIR, d, -1, cur, phi, wf, face + fo, agg->cw_nface[d], nullptr, s));
+      GMG_TRY(wilson_apply_face(w, 4 + d, cur, phi, wf, face + fo, agg->cw_nface[d], s));
       GMG_TRY(agg_project_sel_f64(agg, cur, wf, proj, sel + so, agg->cw_nsel[d], s));
       link_scatter_kernel<<<gsz(Vc * cur * N), 256, 0, s>>>(reinterpret_cast<const double2*>(proj),
                                                              A + (int64_t)(4 + d) * Vc * N * N, Vc, N, i0, cur);
@@ -318,7 +332,7 @@ static gmg_status coarsen_wilson_faces(gmg_coarse* out, gmg_agg* agg, gmg_wilson
       fo += agg->cw_nface[d];
       so += agg->cw_nsel[d];
     }
-    GMG_TRY(wilson_apply_sel(w, GMG_OP_M, 0, 0, cur, phi, wf, nullptr, 0, agg->cw_bpar.as<int8_t>(), s));
+    GMG_TRY(wilson_apply_sel(w, GMG_OP_M, 0, 0, cur, phi, wf, nullptr, 0, agg->cw_hskip.as<uint8_t>(), s));
     GMG_TRY(agg_project_masked_f64(agg, cur, wf, proj, nullptr, s));
     link_scatter_kernel<<<gsz(Vc * cur * N), 256, 0, s>>>(reinterpret_cast<const double2*>(proj),
                                                            A + (int64_t)8 * Vc * N * N, Vc, N, i0, cur);

@@ -127,8 +127,9 @@ struct gmg_agg {
   // CoarsenOperator workspace over the Wilson-clover operator (coarsen.cu),
   // kept between calls: fine fields of one batch of cw_nb basis vectors, the
   // projection output, per direction the fine sites of the backward faces
-  // (global, cw_face) and their in-block indices (cw_sel), block parity per site
-  gmg::DevBuf cw_phi, cw_w, cw_proj, cw_face, cw_sel, cw_bpar;
+  // (global, cw_face) and their in-block indices (cw_sel), and per site the
+  // hops (bit p) whose neighbour lies in a block of the other parity (cw_hskip)
+  gmg::DevBuf cw_phi, cw_w, cw_proj, cw_face, cw_sel, cw_hskip;
   int cw_nb = 0;
   int cw_nface[4] = {0, 0, 0, 0}, cw_nsel[4] = {0, 0, 0, 0};
 };
@@ -201,8 +202,10 @@ gmg_status agg_promote_tc(gmg_agg* h, int nrhs, const float* coarse, float* fine
 
 // fine Wilson-clover (wilson.cu)
 gmg_status wilson_build_clover(gmg_wilson* h, cudaStream_t s);
+gmg_status wilson_apply_face(gmg_wilson* h, int p, int nrhs, const double* in, double* out, const int32_t* sel,
+                             int nsel, cudaStream_t s);
 gmg_status wilson_apply_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, const double* in, double* out,
-                            const int32_t* sel, int nsel, const int8_t* bpar, cudaStream_t s);
+                            const int32_t* sel, int nsel, const uint8_t* hskip, cudaStream_t s);
 gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs,
                         const void* in, void* out, cudaStream_t s);
 gmg_status wilson_apply_mr(gmg_wilson* h, int vec_prec, int nrhs, const void* in, void* out, double2* d1,

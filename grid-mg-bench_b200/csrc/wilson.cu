@@ -148,16 +148,16 @@ __device__ __forceinline__ void st12(typename wt<T>::C* __restrict__ p, const ty
 }
 
 // DOTS (op M or MDAG): also add <out, in> and <out, out> of this (site, r) to
-// dsum[0..1] and dsum[2].  VEC: 16-byte spinor accesses.  bpar (per-site
-// block parity, null for the plain operator): hops whose neighbour has the
-// other parity are left out, which gives e D e + o D o of the coarsening's
-// self term in one pass.
+// dsum[0..1] and dsum[2].  VEC: 16-byte spinor accesses.  skip: hops p with
+// bit p set are left out (0 for the plain operator); with the bits of the
+// hops to blocks of the other parity this gives e D e + o D o of the
+// coarsening's self term in one pass.
 template <class T, class LinkFn, bool DOTS = false, bool VEC = false>
 __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict__ cl, LinkFn links,
                                             const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
                                             typename wt<T>::C* __restrict__ out, int V, int nrhs, int site, int r,
                                             T diag, int op, int dir, int disp, int apbc, int tvol, int Lt,
-                                            double* dsum = nullptr, const int8_t* __restrict__ bpar = nullptr) {
+                                            double* dsum = nullptr, int skip = 0) {
   typedef typename wt<T>::C C;
   const bool g5 = (op == GMG_OP_MDAG);
   const int tc = site / tvol;
@@ -193,8 +193,8 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
       const int mu = p & 3;
       const int dsp = p < 4 ? 1 : -1;
       if (op == GMG_OP_MDIR && (mu != dir || dsp != disp)) continue;
+      if (skip & (1 << p)) continue;
       const int nb = nbr[(int64_t)p * V + site];
-      if (bpar && bpar[nb] != bpar[site]) continue;
       T coef = (T)-0.5;
       if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
       C psi[12];
@@ -262,9 +262,9 @@ constexpr int kTileSites = 16;
 // sites' 8 hop links and clover blocks are staged in shared memory once and
 // read by every RHS of the tile.  Thread per (site, RHS) otherwise, spinors
 // read from global memory.
-// SEL (the coarsening's forms, compiled separately): the tiles run over the
-// nsel sites of the list `sel` (all V sites when null) and only those are
-// written; a single-hop op stages only its link; bpar restricts the hops to
+// SEL (the coarsening's self term, compiled separately): the tiles run over
+// the nsel sites of the list `sel` (all V sites when null) and only those are
+// written; hskip (per site, bit p: leave hop p out) restricts the hops to
 // neighbours of the same block parity (see wilson_site).
 template <class T, bool DOTS, int MINB, bool SEL = false>
 __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
     const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
     typename wt<T>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
     int apbc, int tvol, int Lt, double2* __restrict__ d1, double2* __restrict__ d2,
-    const int32_t* __restrict__ sel = nullptr, int nsel = 0, const int8_t* __restrict__ bpar = nullptr) {
+    const int32_t* __restrict__ sel = nullptr, int nsel = 0, const uint8_t* __restrict__ hskip = nullptr) {
   typedef typename wt<T>::C C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* Ls = reinterpret_cast<C*>(smem_raw);  // [kTileSites][8][9]: p < 4 U_mu(x), p >= 4 U_mu(x - mu)
@@ -294,12 +294,6 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
         Ls[k] = hop[(int64_t)s0 * 72 + k];
         Cs[k] = clover[(int64_t)s0 * 72 + k];
       }
-    } else if (op == GMG_OP_MDIR) {
-      const int pl = (disp > 0 ? 0 : 4) + dir;
-      for (int k = threadIdx.x; k < ns * 9; k += blockDim.x) {
-        const int64_t st = sel ? sel[s0 + k / 9] : s0 + k / 9;
-        Ls[(k / 9) * 72 + pl * 9 + k % 9] = hop[st * 72 + pl * 9 + k % 9];
-      }
     } else {
       for (int k = threadIdx.x; k < ns * 72; k += blockDim.x) {
         const int64_t st = sel ? sel[s0 + k / 72] : s0 + k / 72;
@@ -310,6 +304,7 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
     __syncthreads();
     if (sl < ns) {
       const int site = (SEL && sel) ? sel[s0 + sl] : s0 + sl;
+      const int skip = (SEL && hskip) ? hskip[site] : 0;
       const C* lsite = Ls + sl * 72;
       auto links = [&](int p, int) -> const C* { return lsite + p * 9; };
       // with two RHS or fewer per thread (rl, rl + rt) the thread owns them for
@@ -318,7 +313,7 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
       for (int r = rl; r < nrhs; r += rt, ++k) {
         double dt[3] = {0.0, 0.0, 0.0};
         wilson_site<T, decltype(links), DOTS, true>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op,
-                                                    dir, disp, apbc, tvol, Lt, dt, SEL ? bpar : nullptr);
+                                                    dir, disp, apbc, tvol, Lt, dt, skip);
         if (DOTS) {
           if (two) {
 #pragma unroll
@@ -1309,12 +1304,123 @@ static gmg_status wilson_dispatch(gmg_wilson* h, bool dots, int op, int dir, int
   return GMG_OK;
 }
 
+// Single-hop operator (Mdir of stencil point p) on a list of sites, FP64, for
+// the coarsening's face terms.  A CTA takes S = blockDim / nrhs sites: their
+// neighbour records (all RHS, 12 components each, contiguous in memory) come
+// into shared memory with coalesced loads, one thread per (site, RHS) applies
+// the hop from there into its own slot, and the results leave through the
+// same buffer with coalesced stores.  Slots are padded to 13 complex numbers so
+// that the 16-byte reads of consecutive RHS fall on different banks.  The
+// arithmetic is wilson_hop's, as in wilson_site with op GMG_OP_MDIR.
+constexpr int kFacePad = 13;
+
+template <int MU>
+__device__ __forceinline__ void face_hop(double2 acc[4][3], const double2* __restrict__ U, const double2* psi,
+                                         int disp, double coef) {
+  wilson_hop<double>(acc, U, disp < 0, psi, MU, disp, coef);
+}
+
+__global__ void __launch_bounds__(256) wilson_face_hop_kernel(
+    const double2* __restrict__ hop, const int32_t* __restrict__ nbr, const double2* __restrict__ in,
+    double2* __restrict__ out, int V, int nrhs, const int32_t* __restrict__ sel, int nsel, int p, int apbc,
+    int tvol, int Lt) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int R = nrhs, W = nrhs * 12;
+  const int S = blockDim.x / R;
+  double2* rec = reinterpret_cast<double2*>(smem_raw);  // [S][R][kFacePad]
+  int* sidx = reinterpret_cast<int*>(rec + (size_t)S * R * kFacePad);
+  int* nidx = sidx + S;
+  const int mu = p & 3, disp = p < 4 ? 1 : -1;
+  const int t = threadIdx.x, q = t / R, r = t % R;
+  const int ntl = (nsel + S - 1) / S;
+  for (int tile = blockIdx.x; tile < ntl; tile += gridDim.x) {
+    const int s0 = tile * S, ns = min(S, nsel - s0);
+    __syncthreads();  // the previous tile's stores have read rec, sidx
+    if (t < ns) {
+      const int st = sel[s0 + t];
+      sidx[t] = st;
+      nidx[t] = nbr[(int64_t)p * V + st];
+    }
+    __syncthreads();
+    // one flat loop over the tile's records: its loads are independent and
+    // issue back to back
+#pragma unroll 4
+    for (int k = t; k < ns * W; k += blockDim.x) {
+      const int qq = k / W, e = k - qq * W;
+      rec[qq * R * kFacePad + (e / 12) * kFacePad + e % 12] = in[(int64_t)nidx[qq] * W + e];
+    }
+    __syncthreads();
+    if (q < ns) {
+      const int site = sidx[q];
+      double2* my = rec + (q * R + r) * kFacePad;
+      double2 psi[12];
+#pragma unroll
+      for (int a = 0; a < 12; ++a) psi[a] = my[a];
+      double2 acc[4][3];
+#pragma unroll
+      for (int s2 = 0; s2 < 4; ++s2)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[s2][c] = make_double2(0.0, 0.0);
+      const int tc = site / tvol;
+      double coef = -0.5;
+      if (apbc && mu == 3 && ((disp > 0 && tc == Lt - 1) || (disp < 0 && tc == 0))) coef = 0.5;
+      const double2* U = hop + (int64_t)site * 72 + p * 9;
+      switch (mu) {
+        case 0: face_hop<0>(acc, U, psi, disp, coef); break;
+        case 1: face_hop<1>(acc, U, psi, disp, coef); break;
+        case 2: face_hop<2>(acc, U, psi, disp, coef); break;
+        default: face_hop<3>(acc, U, psi, disp, coef); break;
+      }
+#pragma unroll
+      for (int s2 = 0; s2 < 4; ++s2)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) my[s2 * 3 + c] = acc[s2][c];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = t; k < ns * W; k += blockDim.x) {
+      const int qq = k / W, e = k - qq * W;
+      out[(int64_t)sidx[qq] * W + e] = rec[qq * R * kFacePad + (e / 12) * kFacePad + e % 12];
+    }
+  }
+}
+
+// out = Mdir_p in on the nsel sites of `sel` (FP64, nrhs <= 64); the other
+// sites of `out` are not written
+gmg_status wilson_apply_face(gmg_wilson* h, int p, int nrhs, const double* in, double* out, const int32_t* sel,
+                             int nsel, cudaStream_t s) {
+  GMG_CHECK(nrhs >= 1 && nrhs <= 64, GMG_ERR_UNSUPPORTED, "wilson face hop: nrhs must be in [1, 64]");
+  GMG_CHECK(p >= 0 && p < 8, GMG_ERR_ARGUMENT, "wilson face hop: bad stencil point");
+  if (nsel == 0) return GMG_OK;
+  const int V = (int)h->dims.vol();
+  const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
+  const int S = std::max(1, 256 / nrhs);
+  const int threads = S * nrhs;
+  const size_t smem = sizeof(double2) * (size_t)S * nrhs * kFacePad + sizeof(int) * 2 * S;
+  if (smem > 48 * 1024)
+    GMG_CUDA(cudaFuncSetAttribute(wilson_face_hop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // one resident wave of CTAs looping over the tiles
+  int occ = 1, dev = 0, nsm = 148;
+  GMG_CUDA(cudaGetDevice(&dev));
+  GMG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wilson_face_hop_kernel, threads, smem));
+  const int tiles = (nsel + S - 1) / S;
+  const int g = std::min(tiles, nsm * std::max(occ, 1));
+  KernelTimer kt("wilson", s);
+  wilson_face_hop_kernel<<<g, threads, smem, s>>>(h->hop.as<double2>(), h->nbr.as<int32_t>(),
+                                                   reinterpret_cast<const double2*>(in),
+                                                   reinterpret_cast<double2*>(out), V, nrhs, sel, nsel, p, h->apbc,
+                                                   tvol, h->dims.d[3]);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
 // The coarsening's forms of the FP64 operator (tile kernel, SEL instance):
 // op on the nsel sites of `sel` only (all sites when null; the other sites of
-// `out` are not written), and with bpar the hops restricted to neighbours of
-// the same block parity.
+// `out` are not written), and with hskip (per site, bit p set: leave hop p
+// out) the hops restricted to neighbours of the same block parity.
 gmg_status wilson_apply_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, const double* in, double* out,
-                            const int32_t* sel, int nsel, const int8_t* bpar, cudaStream_t s) {
+                            const int32_t* sel, int nsel, const uint8_t* hskip, cudaStream_t s) {
   const int V = (int)h->dims.vol();
   const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
   int rt = 1;
@@ -1334,7 +1440,7 @@ gmg_status wilson_apply_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, 
   KernelTimer kt("wilson", s);
   k<<<g, kTileSites * rt, smem, s>>>(h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(),
                                      (const double2*)in, (double2*)out, V, nrhs, rt, 4.0 + h->mass, op, dir, disp,
-                                     h->apbc, tvol, h->dims.d[3], nullptr, nullptr, sel, nsel, bpar);
+                                     h->apbc, tvol, h->dims.d[3], nullptr, nullptr, sel, nsel, hskip);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
