@@ -303,8 +303,9 @@ def c5_small(nrhs=24):
 
 
 def profile_rows(rows):
-    """Small cases of the C3 transfers and the fine operator for ncu captures:
-    16^4 fine lattice (nbasis 32 on 4^4 blocks, 32 RHS; Wilson-clover with 24 RHS)."""
+    """Small cases of the C3 transfers, the fine operator and the C4 construction
+    for ncu captures: 16^4 fine lattice (nbasis 32 on 4^4 blocks, 32 RHS;
+    Wilson-clover with 24 RHS; CoarsenOperator with nbasis 40)."""
     fd, cd, N, R = (16, 16, 16, 16), (4, 4, 4, 4), 32, 32
     Vf, Vc = 16 ** 4, 4 ** 4
     if "p_c3" in rows:
@@ -340,6 +341,26 @@ def profile_rows(rows):
         torch.cuda.synchronize()
         line("p_w Wilson-clover 16^4, 24 RHS: FP32 M with MR products, FP64 M", ok=True,
              tuned={"f32_mr": w.tuned_kernel("f32", 24, fused_mr=True), "f64": w.tuned_kernel("f64", 24)})
+    if "p_c4" in rows:
+        # CoarsenOperator 16^4 -> 4^4, nbasis 40 (the C4 construction on a
+        # sixteenth of its volume): two calls, each with 4 face hops, one
+        # self-term operator pass and 5 FP64 projections of 40 RHS
+        N4 = 40
+        U = inputs.torch_smooth_gauge(fd, 615, 0.3)
+        w = gmg.WilsonClover(fd, -0.3, 1.0, antiperiodic=True)
+        w.set_gauge(U)
+        half = inputs.torch_gaussian((N4 // 2, Vf, 12), 616)
+        B = torch.zeros((N4, Vf, 12), dtype=torch.complex128, device="cuda")
+        B[: N4 // 2, :, :6] = half[:, :, :6]
+        B[N4 // 2:, :, 6:] = half[:, :, 6:]
+        ag = gmg.Aggregation(fd, cd, 12, N4)
+        ag.set_basis(B)
+        ag.Orthogonalise(passes=1)
+        cm = gmg.CoarsenedMatrix(cd, N4)
+        for _ in range(2):
+            cm.CoarsenOperator(ag, w)
+        torch.cuda.synchronize()
+        line("p_c4 CoarsenOperator 16^4 -> 4^4, nbasis 40", ok=True)
 
 
 def run(rows=("c1", "c3", "w_c4", "c5")):
