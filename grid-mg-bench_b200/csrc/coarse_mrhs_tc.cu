@@ -322,6 +322,10 @@ __global__ void __launch_bounds__(kThreads, CTAS) coarse_mrhs_tc_kernel(const Pa
         for (int p = 0; p < 9; ++p) my_nbr[lane * 9 + p] = __ldg(&P.nbr[(size_t)p * P.V + site]);
         my_lsite[lane] = P.site_map ? __ldg(&P.site_map[site]) : site;
       }
+      // launched as a programmatic dependent of the vector pack: everything
+      // above overlaps the pack's tail; the packed vectors are read only
+      // after the pack grid has completed (a no-op for a plain launch)
+      if (i0 == 0) asm volatile("griddepcontrol.wait;" ::: "memory");
       __syncwarp();
       if (lane == 0) {
         for (int j = 0; j < cnt && !stop; ++j) {
@@ -527,6 +531,9 @@ __global__ void pack_links_kernel(const double2* __restrict__ A, uint4* __restri
 __global__ void pack_vec_kernel(const float2* __restrict__ in, uint4* __restrict__ dst, const int32_t* __restrict__ active,
                                 int V, int N, int nrhs, int R, int Rp, int Kc, int kind, int g5,
                                 int aligned16) {
+  // the stencil launched after this kernel may start its prologue now (it
+  // waits for this grid's completion before reading the packed vectors)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int64_t total = (int64_t)V * Kc * Rp;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
@@ -715,8 +722,21 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, cons
     Params Q = P;
     Q.stages = sh.stages;
     Q.pps = sh.pps;
-    kern<<<std::min(V, nsm * sh.ctas), kThreads, sh.smem, s>>>(Q);
-    GMG_CUDA(cudaGetLastError());
+    // programmatic dependent launch on the pack that precedes every stencil
+    // launch (not inside a stream capture: captured cycles keep plain edges)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    GMG_CUDA(cudaStreamIsCapturing(s, &cs));
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(std::min(V, nsm * sh.ctas));
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = sh.smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = cs == cudaStreamCaptureStatusNone ? 1 : 0;
+    GMG_CUDA(cudaLaunchKernelEx(&cfg, kern, Q));
     return GMG_OK;
   };
 
