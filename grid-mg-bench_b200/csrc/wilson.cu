@@ -1320,7 +1320,7 @@ __device__ __forceinline__ void face_hop(double2 acc[4][3], const double2* __res
   wilson_hop<double>(acc, U, disp < 0, psi, MU, disp, coef);
 }
 
-__global__ void __launch_bounds__(256) wilson_face_hop_kernel(
+__global__ void __launch_bounds__(256, 3) wilson_face_hop_kernel(
     const double2* __restrict__ hop, const int32_t* __restrict__ nbr, const double2* __restrict__ in,
     double2* __restrict__ out, int V, int nrhs, const int32_t* __restrict__ sel, int nsel, int p, int apbc,
     int tvol, int Lt) {
@@ -1343,8 +1343,8 @@ __global__ void __launch_bounds__(256) wilson_face_hop_kernel(
     }
     __syncthreads();
     // one flat loop over the tile's records: its loads are independent and
-    // issue back to back
-#pragma unroll 4
+    // issue back to back (12 per thread for 40 RHS)
+#pragma unroll 12
     for (int k = t; k < ns * W; k += blockDim.x) {
       const int qq = k / W, e = k - qq * W;
       rec[qq * R * kFacePad + (e / 12) * kFacePad + e % 12] = in[(int64_t)nidx[qq] * W + e];
@@ -1377,7 +1377,7 @@ __global__ void __launch_bounds__(256) wilson_face_hop_kernel(
         for (int c = 0; c < 3; ++c) my[s2 * 3 + c] = acc[s2][c];
     }
     __syncthreads();
-#pragma unroll 4
+#pragma unroll 12
     for (int k = t; k < ns * W; k += blockDim.x) {
       const int qq = k / W, e = k - qq * W;
       out[(int64_t)sidx[qq] * W + e] = rec[qq * R * kFacePad + (e / 12) * kFacePad + e % 12];
@@ -1399,6 +1399,10 @@ gmg_status wilson_apply_face(gmg_wilson* h, int p, int nrhs, const double* in, d
   const size_t smem = sizeof(double2) * (size_t)S * nrhs * kFacePad + sizeof(int) * 2 * S;
   if (smem > 48 * 1024)
     GMG_CUDA(cudaFuncSetAttribute(wilson_face_hop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // all of the unified L1 / shared array as shared memory: three CTAs of
+  // 50 KB per SM, as many as the register bound allows (two with the default
+  // split)
+  GMG_CUDA(cudaFuncSetAttribute(wilson_face_hop_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   // one resident wave of CTAs looping over the tiles
   int occ = 1, dev = 0, nsm = 148;
   GMG_CUDA(cudaGetDevice(&dev));
