@@ -590,9 +590,10 @@ __global__ void pack_vec_kernel(const float2* __restrict__ in, uint4* __restrict
 
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
-// pack the vectors of one apply (G5C on input when g5).  (A variant with one
-// thread per 16 input bytes and 4-byte stores measured 23 us against 15 us for
-// this one on the 8^4 x 32 x 32 apply.)
+// pack the vectors of one apply (G5C on input when g5).  (Two variants did not
+// beat this one on the 8^4 x 32 x 32 apply, 15.5 us: one thread per 16 input
+// bytes with 4-byte stores, 23 us; two chunks per thread with all eight loads
+// issued first, 15.7 us.)
 inline void launch_pack(const float* in, uint4* packed, const int32_t* active, int V, int N, int nrhs, int R,
                         int Rp, int Kc, int kind, bool g5, cudaStream_t s) {
   const int64_t rows = (int64_t)V * Kc * Rp;
