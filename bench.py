@@ -120,6 +120,17 @@ def cpu_sample(A, x, target_s=12.0, max_reps=400):
     }, y
 
 
+def max_over_ranks(v, dist, device):
+    """The largest of every rank's v (a device time in ms): the job ends with its slowest rank."""
+    if dist is None:
+        return float(v)
+    import torch
+
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args, rank):
     """CPU implementation of the path (FP64 oracle restatement) on bounded site samples."""
     if rank != 0:
@@ -314,10 +325,7 @@ def main():
     st = gmg.lib().gmg_coarse_device_error(cm._h, code.ctypes.data_as(ctypes.c_void_p))
     if st != 0:
         raise RuntimeError("tensor-core kernel reported a device error: " + gmg.lib().gmg_last_error().decode())
-    tmax = torch.tensor([t_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    t_ms = float(tmax.item())
+    t_ms = max_over_ranks(t_ms, dist, dev)
     value = world * FLOPS * args.steps / (t_ms * 1e-3) / 1e12
 
     # other forms (fewer steps): FP32 CUDA-core and FP64 CUDA-core
@@ -385,10 +393,8 @@ def main():
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2e_run(ne, e0, e1)
-    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e = world * FLOPS * ne / (float(te.item()) * 1e-3) / 1e12
+    te = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+    e2e = world * FLOPS * ne / (te * 1e-3) / 1e12
 
     hbm, src = peaks()
     kavg_s = (kms.value / max(kn.value, 1)) * 1e-3
