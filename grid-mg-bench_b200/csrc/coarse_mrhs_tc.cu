@@ -764,21 +764,27 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, cons
     if (timed && cap == cudaStreamCaptureStatusNone && ncand > 1) {
       cudaEvent_t e0, e1;
       GMG_CUDA(cudaEventCreate(&e0));
-      GMG_CUDA(cudaEventCreate(&e1));
+      const cudaError_t ce = cudaEventCreate(&e1);
+      if (ce != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_fail(ce, "cudaEventCreate");
+      }
       float best = 1e30f;
       gmg_status st = GMG_OK;
-      for (int ci = 0; ci < ncand; ++ci) {
+      // a failed event call leaves the timing unknown: the heuristic shape
+      // is used for this call and nothing is stored for the key
+      bool timing_ok = true;
+      for (int ci = 0; ci < ncand && timing_ok; ++ci) {
         const Shape& c = cand[ci];
         st = launch(c);  // warm-up
         if (st != GMG_OK) break;
-        cudaEventRecord(e0, s);
+        timing_ok = cudaEventRecord(e0, s) == cudaSuccess;
         for (int k = 0; k < 2 && st == GMG_OK; ++k) st = launch(c);
         if (st != GMG_OK) break;
-        cudaEventRecord(e1, s);
-        cudaEventSynchronize(e1);
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) {
+        timing_ok = timing_ok && cudaEventRecord(e1, s) == cudaSuccess &&
+                    cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+        if (timing_ok && ms < best) {
           best = ms;
           sh = c;
         }
@@ -786,7 +792,12 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, cons
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       GMG_TRY(st);
-      h->tc_shape[key] = ((uint32_t)sh.ctas << 8) | (uint32_t)sh.pps;
+      if (timing_ok) {
+        h->tc_shape[key] = ((uint32_t)sh.ctas << 8) | (uint32_t)sh.pps;
+      } else {
+        (void)cudaGetLastError();  // reset the error state the failed event call left behind
+        sh = cand[0];
+      }
     }
   }
   if (timed) {
@@ -868,33 +879,25 @@ gmg_status coarse_apply_tc_ex(gmg_coarse* h, int V, int V_in, const int32_t* sit
 // overlap on the GPU (different streams, or different host threads) race on
 // the array and must be serialised by the caller.
 // ---------------------------------------------------------------------------
-#include <mutex>
-
 namespace gmg {
 namespace tc {
 
 constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_ptr[kMaxDevices] = {nullptr};
-
 // Device address of g_noalloc_scratch on the current device.  In host code the
 // symbol itself is only a host-side stand-in, so its device address is looked
-// up once per device (with that device current) and cached.
+// up with that device current.  The lookup is repeated on every call rather
+// than cached: after a cudaDeviceReset (or any other re-creation of the
+// primary context) the module is loaded again and a cached address would point
+// into freed memory.  Once the module is loaded the lookup allocates nothing;
+// the first lookup on a device may load it, which is when the array is
+// committed.
 static gmg_status noalloc_scratch(void** p) {
-  int dev = 0;
-  GMG_CUDA(cudaGetDevice(&dev));
-  GMG_CHECK(dev >= 0 && dev < kMaxDevices, GMG_ERR_UNSUPPORTED, "gmg_coarse_apply_noalloc: device index too large");
-  std::lock_guard<std::mutex> g(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess || ptr == nullptr) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-    g_noalloc_ptr[dev] = ptr;
-  }
-  *p = g_noalloc_ptr[dev];
+  void* ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  if (e != cudaSuccess || ptr == nullptr) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+  *p = ptr;
   return GMG_OK;
 }
 

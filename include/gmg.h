@@ -118,10 +118,14 @@ gmg_status gmg_coarse_set_shape(gmg_coarse* h, int ctas, int points_per_stage);
    GPU loading the library holds until exit; requests needing more (V * Kc *
    2 * ceil16(R) * 16 bytes, Kc = ceil16(nbasis)/8) return
    GMG_ERR_UNSUPPORTED.  Vectors are FP32 [V][nrhs][N]; gmg_coarse_prepare
-   (which allocates) must have run for `compute` first.  The first call on a
-   device looks up the array's device address (cudaGetSymbolAddress); make
-   that first call before any stream capture.  All calls share the array:
-   calls that overlap on the GPU race and must be serialised by the caller. */
+   (which allocates) must have run for `compute` first.  Every call looks up
+   the array's device address on the current device (cudaGetSymbolAddress),
+   which allocates nothing once the library's device code is loaded; with
+   lazy module loading (the CUDA default) the first call on a device may load
+   it and so commit the 16 MiB at that moment.  A caller that must not
+   allocate mid-run makes one warm-up call at setup, before any stream
+   capture.  All calls share the array: calls that overlap on the GPU race
+   and must be serialised by the caller. */
 gmg_status gmg_coarse_apply_noalloc(gmg_coarse* h, gmg_op op, int point, gmg_prec compute, int nrhs,
                                     const float* in, float* out, const int32_t* active, int n_active,
                                     gmg_stream s);

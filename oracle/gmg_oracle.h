@@ -54,6 +54,8 @@ void orc_coarse_apply_range(const int* dims, int N, int R, const double* links,
                             const double* in, double* out, int op, int point, int hermitian,
                             int64_t s0, int64_t s1);
 void orc_coarse_g5(int64_t V, int N, int R, double* v);
+/* OpenMP threads of the parallel loops (n <= 0: all); returns the previous count */
+int  orc_set_threads(int n);
 
 /* block projection / promotion / orthonormalisation
    (CoarsenedMatrixUpstreamImprovedDirsaveLut.h:70-240) */

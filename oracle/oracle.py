@@ -102,6 +102,11 @@ def coarse_apply(dims, links, x, op=OP_M, point=8, hermitian=0):
     return y
 
 
+def set_threads(n):
+    """OpenMP threads of the oracle's parallel loops (n <= 0: all host threads); returns the previous count."""
+    return lib().orc_set_threads(int(n))
+
+
 def coarse_apply_range(dims, links, x, y, s0, s1, op=OP_M, point=8, hermitian=0):
     """In-place y[s0:s1] = op(x) on output sites [s0, s1) (bounded timing samples)."""
     V, R, N = x.shape
