@@ -279,6 +279,17 @@ gmg_status gmg_agg_destroy(gmg_agg* h) {
   return GMG_OK;
 }
 
+gmg_status gmg_agg_set_coarsen_batch(gmg_agg* h, int max_batch) {
+  GMG_CHECK(h != nullptr, GMG_ERR_ARGUMENT, "gmg_agg_set_coarsen_batch: null handle");
+  GMG_CHECK(max_batch >= 0, GMG_ERR_ARGUMENT, "gmg_agg_set_coarsen_batch: negative batch");
+  if (max_batch != h->cw_max_batch) {
+    GMG_CUDA(cudaDeviceSynchronize());  // the kept workspace may still be in use
+    h->cw_max_batch = max_batch;
+    h->cw_nb = 0;  // the workspace is rebuilt for the new batch on the next construction
+  }
+  return GMG_OK;
+}
+
 gmg_status gmg_agg_set_basis(gmg_agg* h, const double* basis, int on_device, gmg_stream s) {
   GMG_CHECK(h && basis, GMG_ERR_ARGUMENT, "gmg_agg_set_basis: null argument");
   const size_t bytes = sizeof(double2) * (size_t)h->N * h->fdims.vol() * h->dof;

@@ -117,18 +117,23 @@ __global__ void convert_kernel(const typename C2<Ti>::t* __restrict__ X, typenam
 }
 
 // Chirally doubled basis from a batch of nb vectors X [V][nb][dof]:
-// B[n] = X_n on the upper half of dof, B[n + nb] = X_n on the lower half
-// (performChiralDoublingG5C, include/Benchmark_helpers.h:156-181, up to the
-// factor 1/2 that the following orthonormalisation removes).
+// B[n] = f (1 + G5) X_n and B[n + nb] = f (1 - G5) X_n with G5 = +1 on the
+// upper half of the site's dof and -1 on the lower half (gamma5 =
+// diag(1,1,-1,-1) on spin-colour, G5C on coarse vectors): 2 f X_n on one half,
+// zero on the other.  f = 1/2 is performChiralDoublingG5C
+// (include/Benchmark_helpers.h:156-181), f = 1 the G5R5 form (:130-154); the
+// setup uses f = 1/2 (any factor is removed by the block orthonormalisation
+// that follows).
 template <class T>
 __global__ void chiral_double_kernel(const typename C2<T>::t* __restrict__ X, double2* __restrict__ B, int64_t V,
-                                     int nb, int dof) {
+                                     int nb, int dof, double f) {
   const int64_t n = V * nb * dof;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     const int a = (int)(e % dof);
     const int k = (int)((e / dof) % nb);
     const int64_t s = e / ((int64_t)dof * nb);
-    const double2 v = make_double2(X[e].x, X[e].y);
+    const double m = 2.0 * f;
+    const double2 v = make_double2(m * (double)X[e].x, m * (double)X[e].y);
     const double2 z = make_double2(0, 0);
     const bool upper = a < dof / 2;
     B[((int64_t)k * V + s) * dof + a] = upper ? v : z;
@@ -751,13 +756,15 @@ gmg_status vec_gaussian(Vec& X, uint64_t seed, cudaStream_t s) {
   return GMG_OK;
 }
 
-gmg_status vec_chiral_double(const Vec& X, double* basis_dev, cudaStream_t s) {
+gmg_status vec_chiral_double(const Vec& X, double* basis_dev, cudaStream_t s, double factor) {
   const int64_t n = X.elems();
   const int g = blas::grid1(n);
   if (X.prec == GMG_F64)
-    blas::chiral_double_kernel<double><<<g, 256, 0, s>>>((const double2*)X.p, (double2*)basis_dev, X.V, X.R, X.dof);
+    blas::chiral_double_kernel<double>
+        <<<g, 256, 0, s>>>((const double2*)X.p, (double2*)basis_dev, X.V, X.R, X.dof, factor);
   else
-    blas::chiral_double_kernel<float><<<g, 256, 0, s>>>((const float2*)X.p, (double2*)basis_dev, X.V, X.R, X.dof);
+    blas::chiral_double_kernel<float>
+        <<<g, 256, 0, s>>>((const float2*)X.p, (double2*)basis_dev, X.V, X.R, X.dof, factor);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
@@ -955,3 +962,19 @@ gmg_status bicg_vec(int which, Vec& a, const Vec& b, const Vec& c, const Vec& d,
 }
 
 }  // namespace gmg
+
+extern "C" gmg_status gmg_chiral_double(int64_t V, int dof, int nvec, gmg_prec prec, const void* vecs, double factor,
+                                        double* basis, gmg_stream stream) {
+  using namespace gmg;
+  GMG_CHECK(vecs && basis, GMG_ERR_ARGUMENT, "gmg_chiral_double: null argument");
+  GMG_CHECK(V >= 1 && dof >= 2 && dof % 2 == 0 && nvec >= 1 && nvec <= 4096, GMG_ERR_ARGUMENT,
+            "gmg_chiral_double: V >= 1, an even dof >= 2 and 1 <= nvec <= 4096 required");
+  GMG_CHECK(prec == GMG_F64 || prec == GMG_F32, GMG_ERR_ARGUMENT, "gmg_chiral_double: vectors must be F64 or F32");
+  Vec X;
+  X.p = const_cast<void*>(vecs);
+  X.V = V;
+  X.R = nvec;
+  X.dof = dof;
+  X.prec = prec;
+  return vec_chiral_double(X, basis, S(stream), factor);
+}

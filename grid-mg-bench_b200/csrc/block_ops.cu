@@ -6,10 +6,8 @@
 //
 //   project   C_c (R x N)  = F_c^T (R x K) conj(V_c)^T (K x N)   K = bv * dof
 //   promote   F_c (K x R)  = V_c^T (K x N) C_c (N x R)
-//   ortho     V_c <- conj(L^{-1}) V_c  with  L L^dag = V_c V_c^dag  (Cholesky-QR;
-//             the same Q as the reference's modified Gram-Schmidt in exact
-//             arithmetic, since a thin QR with positive diagonal is unique)
 //
+// (the block orthonormalisation is in ortho.cu)
 // The basis is kept block-major, basis_blk[c][i][k], k = sb*dof + a with sb the
 // lexicographic in-block site index (CoarseningLookupTableRework.h:156-163),
 // so one block's N x K panel is contiguous.  Fine fields stay in the caller's
@@ -560,236 +558,6 @@ gmg_status agg_promote(gmg_agg* h, int compute, int vec_prec, int nrhs, const vo
     return launch_promote<float, 1, 1, 4>(h, h->basis_blk_f.p, nrhs, coarse, fine, s);
   }
   return fail(GMG_ERR_UNSUPPORTED, "promote: unsupported precision");
-}
-
-// ---------------------------------------------------------------------------
-// orthonormalise (FP64 Cholesky-QR, one sweep per pass) and orthogonality check
-// ---------------------------------------------------------------------------
-static const int ORTHO_KS = 2;  // sites per K chunk
-
-// G[i][j] = sum_k conj(V[i][k]) V[j][k] into shared memory (N x N)
-__device__ void block_gram(const double2* __restrict__ Vb, int N, int64_t K, int dof, int bv,
-                           double2* VT, double2* G) {
-  const int t = threadIdx.x;
-  const int NT = (N + 3) / 4;
-  const int ntiles = NT * NT;
-  const int ti = t % NT, tj = t / NT;
-  double2 acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = make_double2(0, 0);
-  const int KC = ORTHO_KS * dof;
-  for (int64_t k0 = 0; k0 < K; k0 += KC) {
-    const int kc = (int)((K - k0) < (int64_t)KC ? (K - k0) : (int64_t)KC);
-    __syncthreads();
-    for (int e = t; e < N * kc; e += blockDim.x) {
-      const int i = e / kc, kk = e % kc;
-      VT[kk * N + i] = Vb[(int64_t)i * K + k0 + kk];
-    }
-    __syncthreads();
-    if (t < ntiles) {
-      for (int kk = 0; kk < kc; ++kk) {
-        double2 a[4], b[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int i = ti * 4 + q, j = tj * 4 + q;
-          a[q] = i < N ? VT[kk * N + i] : make_double2(0, 0);
-          b[q] = j < N ? VT[kk * N + j] : make_double2(0, 0);
-        }
-#pragma unroll
-        for (int x = 0; x < 4; ++x)
-#pragma unroll
-          for (int y = 0; y < 4; ++y) acc[x][y] = cfma_conj(acc[x][y], a[x], b[y]);
-      }
-    }
-  }
-  __syncthreads();
-  if (t < ntiles) {
-#pragma unroll
-    for (int x = 0; x < 4; ++x)
-#pragma unroll
-      for (int y = 0; y < 4; ++y) {
-        const int i = ti * 4 + x, j = tj * 4 + y;
-        if (i < N && j < N) G[i * N + j] = acc[x][y];
-      }
-  }
-  __syncthreads();
-}
-
-// Cholesky G = L L^dag in place (lower triangle) by warp 0, with `shift` added
-// to the diagonal; returns false (to every thread) when a pivot is not positive.
-__device__ bool block_cholesky(double2* G, int N, double shift, int* fail_s) {
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  if (t == 0) *fail_s = 0;
-  __syncthreads();
-  if (warp == 0) {
-    for (int j = 0; j < N; ++j) {
-      if (lane == 0) {
-        double d = G[j * N + j].x + shift;
-        for (int k = 0; k < j; ++k) d -= G[j * N + k].x * G[j * N + k].x + G[j * N + k].y * G[j * N + k].y;
-        if (!(d > 0.0)) {
-          *fail_s = 1;
-          d = 1.0;
-        }
-        G[j * N + j] = make_double2(sqrt(d), 0.0);
-      }
-      __syncwarp();
-      const double dj = G[j * N + j].x;
-      for (int i = j + 1 + lane; i < N; i += 32) {
-        double2 v = G[i * N + j];
-        for (int k = 0; k < j; ++k) {  // v -= L[i][k] conj(L[j][k])
-          const double2 a = G[i * N + k], b = G[j * N + k];
-          v.x -= a.x * b.x + a.y * b.y;
-          v.y -= a.y * b.x - a.x * b.y;
-        }
-        G[i * N + j] = make_double2(v.x / dj, v.y / dj);
-      }
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-  return *fail_s == 0;
-}
-
-// Block orthonormalisation (blockLutedOrthonormalise, ...Lut.h:172-240: modified
-// Gram-Schmidt per block) as Cholesky QR: each pass forms the block Gram matrix
-// G = V V^dag, factors G = L L^dag and replaces V by L^{-1} V.  The transform is
-// lower triangular in the vector index, so the result is the same orthonormal
-// basis Gram-Schmidt produces.  Cholesky QR loses orthogonality as cond(V)^2;
-// when a factorisation breaks down (smoothed test vectors can be nearly
-// dependent inside a block) that pass is redone with the diagonal shift of
-// shifted Cholesky QR (Fukaya, Kannan, Nakatsukasa, Yamamoto, Yanagisawa,
-// SIAM J. Sci. Comput. 42 (2020)), s = 11 (K N + N (N + 1)) u ||V||_F^2, which
-// always factors, and up to two extra plain passes follow.
-__global__ void __launch_bounds__(256) ortho_kernel(double2* __restrict__ basis, int Vc, int N,
-                                                    int dof, int bv, int passes, int* __restrict__ status) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* G = reinterpret_cast<double2*>(smem_raw);  // [N][N]  Gram, then L
-  double2* Li = G + N * N;                             // [N][N]  conj(L^{-1})
-  double2* VT = Li + N * N;                            // [KC][N] staging
-  __shared__ int fail_s;
-  __shared__ double trace_s;
-  const int64_t K = (int64_t)bv * dof;
-  const int t = threadIdx.x;
-  for (int c = blockIdx.x; c < Vc; c += gridDim.x) {
-    double2* Vb = basis + (int64_t)c * N * K;
-    int extra = 0;
-    for (int pass = 0; pass < passes + extra; ++pass) {
-      block_gram(Vb, N, K, dof, bv, VT, G);
-      if (!block_cholesky(G, N, 0.0, &fail_s)) {
-        block_gram(Vb, N, K, dof, bv, VT, G);
-        if (t == 0) {
-          double tr = 0.0;
-          for (int i = 0; i < N; ++i) tr += G[i * N + i].x;
-          trace_s = tr;
-        }
-        __syncthreads();
-        const double shift = 11.0 * ((double)K * N + (double)N * (N + 1)) * 1.1102230246251565e-16 * trace_s;
-        if (!block_cholesky(G, N, shift, &fail_s) && t == 0) atomicExch(status, 1);
-        if (extra < 2) extra = 2;
-      }
-      // L^{-1} column by column (one thread per column), stored conjugated
-      for (int j = t; j < N; j += blockDim.x) {
-        for (int i = 0; i < N; ++i) Li[i * N + j] = make_double2(0, 0);
-        // X[i][j] for i >= j: X[j][j] = 1/L[j][j]; X[i][j] = -(sum_{k=j}^{i-1} L[i][k] X[k][j]) / L[i][i]
-        Li[j * N + j] = make_double2(1.0 / G[j * N + j].x, 0.0);
-        for (int i = j + 1; i < N; ++i) {
-          double2 sacc = make_double2(0, 0);
-          for (int k = j; k < i; ++k) {
-            const double2 a = G[i * N + k], x = Li[k * N + j];
-            sacc.x += a.x * x.x - a.y * x.y;
-            sacc.y += a.x * x.y + a.y * x.x;
-          }
-          const double inv = 1.0 / G[i * N + i].x;
-          Li[i * N + j] = make_double2(-sacc.x * inv, -sacc.y * inv);
-        }
-        for (int i = j; i < N; ++i) Li[i * N + j].y = -Li[i * N + j].y;  // conjugate
-      }
-      __syncthreads();
-      // V <- conj(L^{-1}) V, chunk by chunk (each chunk read fully before it is overwritten)
-      const int KC = ORTHO_KS * dof;
-      for (int64_t k0 = 0; k0 < K; k0 += KC) {
-        const int kc = (int)((K - k0) < (int64_t)KC ? (K - k0) : (int64_t)KC);
-        __syncthreads();
-        for (int e = t; e < N * kc; e += blockDim.x) {
-          const int i = e / kc, kk = e % kc;
-          VT[kk * N + i] = Vb[(int64_t)i * K + k0 + kk];
-        }
-        __syncthreads();
-        for (int e = t; e < N * kc; e += blockDim.x) {
-          const int i = e / kc, kk = e % kc;
-          double2 acc = make_double2(0, 0);
-          for (int j = 0; j <= i; ++j) acc = cfma(acc, Li[i * N + j], VT[kk * N + j]);
-          Vb[(int64_t)i * K + k0 + kk] = acc;
-        }
-      }
-      __syncthreads();
-    }
-  }
-}
-
-gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s) {
-  const int N = h->N;
-  const size_t smem = sizeof(double2) * ((size_t)2 * N * N + (size_t)ORTHO_KS * h->dof * N);
-  GMG_CHECK(smem <= 227 * 1024, GMG_ERR_UNSUPPORTED, "orthonormalise: nbasis too large");
-  GMG_CHECK(N <= 64, GMG_ERR_UNSUPPORTED, "orthonormalise: nbasis > 64");
-  GMG_CUDA(cudaFuncSetAttribute(ortho_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  GMG_TRY(h->scratch.alloc(64));
-  GMG_CUDA(cudaMemsetAsync(h->scratch.p, 0, sizeof(int), s));
-  const int Vc = (int)h->cdims.vol();
-  const int grid = std::min(Vc, num_sms() * 8);
-  {
-    KernelTimer kt("ortho", s);
-    ortho_kernel<<<grid, 256, smem, s>>>(h->basis_blk.as<double2>(), Vc, N, h->dof, h->bv, passes,
-                                         h->scratch.as<int>());
-    GMG_CUDA(cudaGetLastError());
-  }
-  h->basis_f_ok = false;
-  h->basis_tc_ok = false;
-  return GMG_OK;
-}
-
-__global__ void __launch_bounds__(256) ortho_check_kernel(const double2* __restrict__ basis, int Vc,
-                                                          int N, int dof, int bv,
-                                                          unsigned long long* __restrict__ maxerr) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* G = reinterpret_cast<double2*>(smem_raw);
-  double2* VT = G + N * N;
-  const int64_t K = (int64_t)bv * dof;
-  for (int c = blockIdx.x; c < Vc; c += gridDim.x) {
-    block_gram(basis + (int64_t)c * N * K, N, K, dof, bv, VT, G);
-    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
-      const int i = e / N, j = e % N;
-      const double re = G[e].x - (i == j ? 1.0 : 0.0), im = G[e].y;
-      const double err = sqrt(re * re + im * im);
-      atomicMax(maxerr, __double_as_longlong(err));  // non-negative doubles order as integers
-    }
-    __syncthreads();
-  }
-}
-
-gmg_status agg_check_orthogonal(gmg_agg* h, double* max_err, cudaStream_t s) {
-  const int N = h->N;
-  const size_t smem = sizeof(double2) * ((size_t)N * N + (size_t)ORTHO_KS * h->dof * N);
-  GMG_CUDA(cudaFuncSetAttribute(ortho_check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  GMG_TRY(h->scratch.alloc(64));
-  unsigned long long* d = reinterpret_cast<unsigned long long*>(h->scratch.as<char>() + 8);
-  GMG_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), s));
-  const int Vc = (int)h->cdims.vol();
-  ortho_check_kernel<<<std::min(Vc, num_sms() * 8), 256, smem, s>>>(h->basis_blk.as<double2>(), Vc,
-                                                                    N, h->dof, h->bv, d);
-  GMG_CUDA(cudaGetLastError());
-  unsigned long long v = 0;
-  GMG_CUDA(cudaMemcpyAsync(&v, d, sizeof(v), cudaMemcpyDeviceToHost, s));
-  GMG_CUDA(cudaStreamSynchronize(s));
-  double r;
-  memcpy(&r, &v, sizeof(r));
-  *max_err = r;
-  int st = 0;
-  GMG_CUDA(cudaMemcpy(&st, h->scratch.p, sizeof(int), cudaMemcpyDeviceToHost));
-  if (st) return fail(GMG_ERR_NONFINITE, "orthonormalise: a block Gram matrix was singular even with the shift");
-  return GMG_OK;
 }
 
 }  // namespace gmg

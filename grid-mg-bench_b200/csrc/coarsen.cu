@@ -133,6 +133,7 @@ static gmg_status coarsen_generic(gmg_coarse* out, gmg_agg* agg, const FineOpRef
   const double cap = std::min(40.0e9, (double)free_b / 3.0) / 4.0;
   int nb = N;
   while (nb > 1 && (double)Vf * nb * dof * 16.0 > cap) nb = (nb + 1) / 2;
+  if (agg->cw_max_batch > 0) nb = std::min(nb, agg->cw_max_batch);
   const size_t fbytes = sizeof(double2) * (size_t)Vf * nb * dof;
   DevBuf phi, w1, w2, w3, proj, masks;
   GMG_TRY(phi.alloc(fbytes));
@@ -222,6 +223,7 @@ static gmg_status coarsen_workspace(gmg_agg* agg, cudaStream_t s) {
   const double cap = std::min(40.0e9, (double)free_b / 3.0) / 2.0;
   int nb = N;
   while (nb > 1 && (double)Vf * nb * dof * 16.0 > cap) nb = (nb + 1) / 2;
+  if (agg->cw_max_batch > 0) nb = std::min(nb, agg->cw_max_batch);
   const size_t fbytes = sizeof(double2) * (size_t)Vf * nb * dof;
   GMG_TRY(agg->cw_phi.alloc(fbytes));
   GMG_TRY(agg->cw_w.alloc(fbytes));

@@ -123,6 +123,7 @@ struct gmg_agg {
   gmg::DevBuf basis_tc_hi, basis_tc_lo;  // BF16 hi / lo tensor-core packing (block_tc.cu)
   bool basis_tc_ok = false;
   gmg::DevBuf scratch;
+  gmg::DevBuf ortho_ws;  // orthonormalisation workspace (ortho.cu): status, per-block flags, Cholesky factors
   gmg::DevBuf dev_err;  // int: error code recorded by the tensor-core kernels
   // CoarsenOperator workspace over the Wilson-clover operator (coarsen.cu),
   // kept between calls: fine fields of one batch of cw_nb basis vectors, the
@@ -131,6 +132,7 @@ struct gmg_agg {
   // hops (bit p) whose neighbour lies in a block of the other parity (cw_hskip)
   gmg::DevBuf cw_phi, cw_w, cw_proj, cw_face, cw_sel, cw_hskip;
   int cw_nb = 0;
+  int cw_max_batch = 0;  // cap on basis vectors per CoarsenOperator batch (0: from free memory)
   int cw_nface[4] = {0, 0, 0, 0}, cw_nsel[4] = {0, 0, 0, 0};
 };
 
@@ -192,6 +194,7 @@ gmg_status agg_project(gmg_agg* h, int compute, int vec_prec, int nrhs, const vo
                        void* coarse, const int32_t* mask_blk, cudaStream_t s);
 gmg_status agg_promote(gmg_agg* h, int compute, int vec_prec, int nrhs, const void* coarse,
                        void* fine, cudaStream_t s);
+// block orthonormalisation and its check (ortho.cu)
 gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s);
 gmg_status agg_check_orthogonal(gmg_agg* h, double* max_err, cudaStream_t s);
 gmg_status agg_prepare_f32(gmg_agg* h, cudaStream_t s);

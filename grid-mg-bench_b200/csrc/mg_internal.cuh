@@ -52,7 +52,8 @@ gmg_status vec_axpby(const double2* a_dev, const Vec& X, const double2* b_dev, V
 // Y = X with a precision conversion
 gmg_status vec_convert(const Vec& X, Vec& Y, cudaStream_t s);
 // basis [2R][V][dof] (FP64) from X [V][R][dof] by chiral doubling
-gmg_status vec_chiral_double(const Vec& X, double* basis_dev, cudaStream_t s);
+// basis [2 R][V][dof] FP64 = factor (1 +- G5) X from the R vectors of X
+gmg_status vec_chiral_double(const Vec& X, double* basis_dev, cudaStream_t s, double factor = 0.5);
 // dst(r') = src(idx[r']) (gather) / dst(idx[r']) = src(r') (scatter), idx on the device
 gmg_status vec_gather(const Vec& src, const int* idx, Vec& dst, cudaStream_t s);
 gmg_status vec_scatter(const Vec& src, const int* idx, Vec& dst, cudaStream_t s);

@@ -265,6 +265,10 @@ class Aggregation:
             _LIB.gmg_agg_destroy(self._h)
             self._h = None
 
+    def set_coarsen_batch(self, max_batch):
+        """Cap the basis vectors per CoarsenOperator batch (0: sized from free memory)."""
+        _chk(lib().gmg_agg_set_coarsen_batch(self._h, int(max_batch)))
+
     def set_basis(self, B):
         if isinstance(B, torch.Tensor):
             B = B.to(torch.complex128).contiguous()
@@ -449,6 +453,17 @@ class MultiGrid:
         op, ag = ctypes.c_void_p(), ctypes.c_void_p()
         _chk(lib().gmg_mg_level(self._h, l, ctypes.byref(op), ctypes.byref(ag)))
         return op, ag
+
+
+def chiral_double(vecs, factor=1.0):
+    """Chirally doubled basis [2 nvec][V][dof] complex128 from vecs [V][nvec][dof]
+    (complex128 or complex64 on the GPU): factor (1 + G5) v_n, then factor (1 - G5) v_n
+    (performChiralDoublingG5C with factor 1/2, G5R5 with factor 1)."""
+    V, nvec, dof = vecs.shape
+    out = torch.empty((2 * nvec, V, dof), dtype=torch.complex128, device=vecs.device)
+    _chk(lib().gmg_chiral_double(ctypes.c_int64(V), dof, nvec, _vec_prec(vecs), _ptr(vecs),
+                                 ctypes.c_double(factor), _ptr(out), _stream()))
+    return out
 
 
 def lut_build(fine_dims, coarse_dims, mask_kind=-1):

@@ -209,6 +209,16 @@ gmg_status gmg_agg_create(const int fine_dims[4], const int coarse_dims[4], int 
                           int nbasis, gmg_agg** h);
 gmg_status gmg_agg_destroy(gmg_agg* h);
 
+/* Upper bound on the basis vectors the coarse-operator construction treats as
+   one batch of right-hand sides of the fine operator (0, the default: as many
+   as two fine fields of the batch in a third of the free device memory allow,
+   at most 40 GB).  A smaller batch trades speed for memory; the links do not
+   depend on it.  No counterpart in the reference, which applies the fine
+   operator to one basis vector at a time (CoarsenedMatrixUpstream.h:835-844)
+   or to batches of Ls vectors, the extent of the fifth (RHS) dimension
+   (...LutMRHS.h:1004-1101). */
+gmg_status gmg_agg_set_coarsen_batch(gmg_agg* h, int max_batch);
+
 /* subspace[i] = basis[i] (public member `subspace`, ...LutMRHS.h:298). */
 gmg_status gmg_agg_set_basis(gmg_agg* h, const double* basis, int on_device, gmg_stream s);
 gmg_status gmg_agg_get_basis(gmg_agg* h, double* basis, int on_device, gmg_stream s);
@@ -229,6 +239,17 @@ gmg_status gmg_agg_project(gmg_agg* h, gmg_prec compute, gmg_prec vec_prec, int 
                            const void* fine, void* coarse, gmg_stream s);
 gmg_status gmg_agg_promote(gmg_agg* h, gmg_prec compute, gmg_prec vec_prec, int nrhs,
                            const void* coarse, void* fine, gmg_stream s);
+
+/* Chiral doubling of nvec vectors into a 2 nvec basis
+   (performChiralDoublingG5C, include/Benchmark_helpers.h:156-181, factor 1/2;
+   performChiralDoublingG5R5, :130-154, factor 1): basis[n] = factor (1 + G5)
+   v_n and basis[n + nvec] = factor (1 - G5) v_n, G5 = +1 on the upper half of
+   the site dof (gamma5 of the chiral basis on spin-colour, G5C on coarse
+   vectors).  vecs: device [V][nvec][dof] of prec (F64 / F32, the multi-RHS
+   layout of the setup solves); basis: device [2 nvec][V][dof] complex128,
+   the layout of gmg_agg_set_basis. */
+gmg_status gmg_chiral_double(int64_t V, int dof, int nvec, gmg_prec prec, const void* vecs, double factor,
+                             double* basis, gmg_stream s);
 
 /* ------------------------------------------------------------------------ */
 /* Fine Wilson-clover operator (Grid WilsonCloverFermionR through            */

@@ -202,6 +202,63 @@ def test_orthonormalise_nearly_dependent_block_vectors(agg8):
     assert orc.rel_dev_sq(np.moveaxis(ref, 0, 1), back) < 1e-10
 
 
+@pytest.mark.parametrize("fd,cd,dof,N", [
+    ((8, 8, 8, 8), (2, 2, 2, 2), 12, 24),   # 4^4 blocks (K = 3072), nbasis 24
+    ((8, 8, 8, 8), (2, 2, 2, 2), 12, 32),   # nbasis 32
+    ((8, 8, 8, 8), (2, 2, 2, 2), 12, 40),   # nbasis 40 (the two-kernel path's largest)
+    ((4, 4, 4, 4), (2, 2, 2, 2), 40, 40),   # coarse level: 2^4 blocks of dof 40 (K = 640)
+    ((4, 4, 4, 4), (1, 2, 2, 2), 24, 48),   # nbasis 48: the one-CTA-per-block path
+    ((4, 4, 2, 2), (2, 2, 1, 1), 12, 6),    # small nbasis, partial last chunk (K = 96)
+])
+def test_orthonormalise_sizes_match_mgs(fd, cd, dof, N):
+    # Cholesky QR on the GPU against the oracle's modified Gram-Schmidt
+    # (blockLutedOrthonormalise) on chirally doubled Gaussian vectors, one and
+    # two passes, and the orthogonality check (CheckOrthogonal)
+    h = inputs.gaussian_field((N // 2, int(np.prod(fd)), dof), inputs.rng(stream=190 + N + dof))
+    B0 = orc.chiral_double(h, 0.5)
+    ag = gmg.Aggregation(fd, cd, dof, N)
+    ag.set_basis(B0)
+    assert ag.CheckOrthogonal() > 0.5
+    ag.Orthogonalise(passes=1)
+    ref = orc.block_orthonormalise(fd, cd, B0, passes=1)
+    assert orc.rel_dev_sq(ref, ag.get_basis()) < 1e-24
+    assert ag.CheckOrthogonal() < 1e-13
+    ag.set_basis(B0)
+    ag.Orthogonalise(passes=2)
+    ref2 = orc.block_orthonormalise(fd, cd, B0, passes=2)
+    assert orc.rel_dev_sq(ref2, ag.get_basis()) < 1e-24
+    assert ag.CheckOrthogonal() < 1e-14
+
+
+def test_orthonormalise_shift_only_where_needed():
+    # one block of 16 holds nearly dependent vectors (plain Cholesky QR breaks
+    # down there and the shifted factorisation plus two extra passes run for it
+    # alone); the other blocks must come out as the plain passes leave them
+    fd, cd, N = (8, 8, 8, 8), (2, 2, 2, 2), 24
+    V = int(np.prod(fd))
+    h = inputs.gaussian_field((N // 2, V, 12), inputs.rng(stream=195))
+    B0 = orc.chiral_double(h, 0.5)
+    lut = gmg.lut_build(fd, cd)[0]
+    sites = lut[5]  # block 5
+    noise = 1e-7 * inputs.gaussian_field((N, len(sites), 12), inputs.rng(stream=196))
+    B0[:, sites] = B0[:1, sites] + noise
+    B0[N // 2:, sites, :6] = 0.0  # keep the chiral structure of the doubled basis
+    B0[:N // 2, sites, 6:] = 0.0
+    ag = gmg.Aggregation(fd, cd, 12, N)
+    ag.set_basis(B0)
+    ag.Orthogonalise(passes=1)
+    assert ag.CheckOrthogonal() < 1e-12
+    got = ag.get_basis()
+    ref = orc.block_orthonormalise(fd, cd, B0, passes=1)
+    other = np.setdiff1d(np.arange(V), sites)
+    assert orc.rel_dev_sq(ref[:, other], got[:, other]) < 1e-24
+    # block 5: same span as the Gram-Schmidt basis
+    sub = got[:, sites]
+    proj = np.einsum("ik,jk->ij", sub.reshape(N, -1).conj(), ref[:, sites].reshape(N, -1))
+    back = np.einsum("ij,ik->jk", proj, sub.reshape(N, -1))
+    assert orc.rel_dev_sq(ref[:, sites].reshape(N, -1), back) < 1e-10
+
+
 @pytest.mark.parametrize("nrhs", [1, 3, 8])
 def test_project_promote_f64(agg8, nrhs):
     fd, cd, B0, ag = agg8
@@ -286,6 +343,27 @@ def wil():
 def test_clover_matches_oracle(wil):
     dims, U, cl, w = wil
     assert orc.rel_dev_sq(cl, w.clover()) < TOL64
+
+
+def test_clover_known_answer_uniform_abelian_field():
+    # the device-built clover term on a uniform U(1) field (B01 = 2 pi / 8 in the
+    # (0,1) plane, B23 = -2 pi / 8 in the (2,3) plane, identity colour) equals
+    # the analytic -(c_sw/2) (sin B01 sigma_01 + sin B23 sigma_23) x 1_colour
+    dims, csw = (8, 2, 8, 2), 1.3
+    V = int(np.prod(dims))
+    b01, b23 = 2 * np.pi / 8, -2 * np.pi / 8
+    U = np.zeros((V, 4, 3, 3), dtype=np.complex128)
+    for s in range(V):
+        x0, x2 = s % 8, (s // 16) % 8
+        for mu, ph in enumerate((1.0, np.exp(1j * b01 * x0), 1.0, np.exp(1j * b23 * x2))):
+            U[s, mu] = ph * np.eye(3)
+    g = [orc.gamma(mu) for mu in range(4)]
+    sig = lambda a, b: 0.5j * (g[a] @ g[b] - g[b] @ g[a])  # noqa: E731
+    full = np.kron(-0.5 * csw * (np.sin(b01) * sig(0, 1) + np.sin(b23) * sig(2, 3)), np.eye(3))
+    expect = np.stack([full[:6, :6], full[6:, 6:]])
+    w = gmg.WilsonClover(dims, -0.2, csw, antiperiodic=0)
+    w.set_gauge(U)
+    assert np.abs(w.clover() - expect[None]).max() < 1e-14
 
 
 @pytest.mark.parametrize("op", ["M", "Mdag", "Mdiag"])
@@ -411,6 +489,27 @@ def test_wilson_apply_mr_products(wil, forced, variant, nrhs):
         assert orc.rel_dev_sq(ref, host(out)) < tol
         assert np.abs(d1.cpu().numpy() - d1_ref).max() / np.abs(d2_ref).max() < np.sqrt(tol)
         assert np.abs(d2.cpu().numpy() - d2_ref).max() / np.abs(d2_ref).max() < np.sqrt(tol)
+
+
+# ------------------------------------------------------------- chiral doubling
+@pytest.mark.parametrize("dof", [12, 24])
+@pytest.mark.parametrize("factor", [0.5, 1.0])
+def test_chiral_double_matches_oracle(dof, factor):
+    # performChiralDoublingG5C (factor 1/2) and the G5R5 form (factor 1) on
+    # spin-colour vectors (dof 12) and coarse vectors (dof 24), the setup's
+    # multi-RHS input layout [V][nvec][dof], F64 and F32 inputs
+    V, nvec = 300, 5
+    h = inputs.gaussian_field((nvec, V, dof), inputs.rng(stream=160 + dof))
+    ref = orc.chiral_double(h, factor)
+    x = np.ascontiguousarray(h.transpose(1, 0, 2))
+    got = gmg.chiral_double(dev(x), factor)
+    assert np.array_equal(ref, host(got))  # sign selection and one product per element: exact
+    x32 = dev(x, torch.complex64)
+    got32 = host(gmg.chiral_double(x32, factor))
+    ref32 = orc.chiral_double(x32.cpu().numpy().astype(np.complex128).transpose(1, 0, 2), factor)
+    assert np.array_equal(ref32, got32)
+    # the halves sum back to factor * 2 v (undoChiralDoubling up to the factor)
+    assert np.allclose(got32[:nvec] + got32[nvec:], 2 * factor * x32.cpu().numpy().transpose(1, 0, 2), atol=0)
 
 
 # --------------------------------------------------------------- CoarsenOperator

@@ -318,3 +318,64 @@ def test_layout_maps():
     for n1 in range(N):
         for n2 in range(N):
             assert y[:, n1 // 4, n2 // 4, n1 % 4, n2 % 4].tolist() == a[:, n1, n2].tolist()
+
+
+# DeGrand-Rossi chiral basis (the basis Grid uses), written out from its definition
+_I = 1j
+_GAMMA_DR = [
+    np.array([[0, 0, 0, _I], [0, 0, _I, 0], [0, -_I, 0, 0], [-_I, 0, 0, 0]]),
+    np.array([[0, 0, 0, -1], [0, 0, 1, 0], [0, 1, 0, 0], [-1, 0, 0, 0]], dtype=complex),
+    np.array([[0, 0, _I, 0], [0, 0, 0, -_I], [-_I, 0, 0, 0], [0, _I, 0, 0]]),
+    np.array([[0, 0, 1, 0], [0, 0, 0, 1], [1, 0, 0, 0], [0, 1, 0, 0]], dtype=complex),
+]
+
+
+def _abelian_gauge(dims, n01, n23):
+    """U(1) x identity-colour links with a uniform field strength: U_1(x) = exp(i B01 x_0),
+    U_3(x) = exp(i B23 x_2), U_0 = U_2 = 1, with B01 = 2 pi n01 / L_0 and B23 = 2 pi n23 / L_2
+    (whole flux quanta, so the field is uniform across the periodic boundary too).
+    Every plaquette in the (0,1) plane is exp(i B01), in the (2,3) plane exp(i B23),
+    in the other four planes 1."""
+    V = int(np.prod(dims))
+    U = np.zeros((V, 4, 3, 3), dtype=np.complex128)
+    b01, b23 = 2 * np.pi * n01 / dims[0], 2 * np.pi * n23 / dims[2]
+    for s in range(V):
+        x0 = s % dims[0]
+        x2 = (s // (dims[0] * dims[1])) % dims[2]
+        ph = [1.0, np.exp(1j * b01 * x0), 1.0, np.exp(1j * b23 * x2)]
+        for mu in range(4):
+            U[s, mu] = ph[mu] * np.eye(3)
+    return U, b01, b23
+
+
+@pytest.mark.parametrize("n01,n23", [(1, 0), (1, 1), (1, -1), (2, 1)])
+def test_clover_known_answer_uniform_abelian_field(n01, n23):
+    # Clover term on an analytic background: the clover-leaf field strength of a
+    # uniform U(1) field is F_{mu nu} = (Q - Q^dag)/(8i) = sin(B_{mu nu}) exactly
+    # (four equal leaves exp(i B)), so Cl = -(c_sw/2) sum_{mu<nu} sigma_{mu nu} F_{mu nu}
+    # with sigma_{mu nu} = (i/2)[gamma_mu, gamma_nu] is
+    #   Cl = -(c_sw/2) (sin B01 sigma_01 + sin B23 sigma_23) (x) 1_colour
+    # at every site: this pins the normalisation (1/8 of the leaf sum, 1/2 of
+    # c_sw) and the sign.  In the chiral basis sigma_01 = diag(1,-1,1,-1) and
+    # sigma_23 = diag(-1,1,1,-1), so a self-dual field (B01 = B23) leaves the
+    # gamma5 = +1 block untouched and an anti-self-dual one the gamma5 = -1 block.
+    dims, csw, m = (8, 2, 8, 2), 1.3, -0.2
+    for mu in range(4):
+        assert np.array_equal(orc.gamma(mu), _GAMMA_DR[mu])
+    U, b01, b23 = _abelian_gauge(dims, n01, n23)
+    cl = orc.clover_build(dims, U, csw)
+    sig01 = 0.5j * (_GAMMA_DR[0] @ _GAMMA_DR[1] - _GAMMA_DR[1] @ _GAMMA_DR[0])
+    sig23 = 0.5j * (_GAMMA_DR[2] @ _GAMMA_DR[3] - _GAMMA_DR[3] @ _GAMMA_DR[2])
+    spin = -0.5 * csw * (np.sin(b01) * sig01 + np.sin(b23) * sig23)
+    full = np.kron(spin, np.eye(3))  # index 3 * spin + colour
+    expect = np.stack([full[:6, :6], full[6:, 6:]])
+    assert np.abs(full[:6, 6:]).max() == 0 and np.abs(full[6:, :6]).max() == 0
+    assert np.abs(cl - expect[None]).max() < 1e-14
+    if n01 == n23:
+        assert np.abs(cl[:, 0]).max() < 1e-14 and np.abs(cl[:, 1]).max() > 0.1
+    if n01 == -n23:
+        assert np.abs(cl[:, 1]).max() < 1e-14 and np.abs(cl[:, 0]).max() > 0.1
+    # Mdiag on a Gaussian spinor field = (4 + m) x + Cl x
+    x = inputs.gaussian_field((int(np.prod(dims)), 2, 12), inputs.rng(stream=77))
+    y = orc.wilson_clover(dims, U, cl, m, 0, x, orc.OP_MDIAG)
+    assert np.abs(y - ((4 + m) * x + np.einsum("ab,srb->sra", full, x))).max() < 1e-13
