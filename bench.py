@@ -60,6 +60,9 @@ def parse():
                     help="skip the 3-level MG solve measurement (32^4 Wilson-clover, 24 RHS) of the JSON line")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed applies (for profiler captures); prints a short line")
+    ap.add_argument("--flush", choices=["write+read", "write"], default="write+read",
+                    help="L2 flush between timed steps: 256 MiB written then another 256 MiB read (the default: "
+                         "the written lines are written back before the step), or the write alone")
     return ap.parse_args()
 
 
@@ -174,7 +177,8 @@ def run_reference(args, rank):
         "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": config_dict("FP64 CPU restatement of CoarsenedMatrix::M (oracle)"),
+        "data": "synthetic", "config": config_dict(),
+        "form": "FP64 CPU restatement of CoarsenedMatrix::M (the oracle, C++/OpenMP)",
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                          "sample": f"{nsites} of {V} output sites per step (all 32 RHS), FP64, "
                                    f"{os.cpu_count()} OpenMP threads; Grid, which the reference "
@@ -185,12 +189,14 @@ def run_reference(args, rank):
     return 0
 
 
-def config_dict(form):
+def config_dict():
+    """The workload, the same for both arms (how each arm computes it is in `form` and `dtype`)."""
     return {
         "workload": "multi-RHS coarse stencil M apply: coarse 8^4, nbasis 32, 32 RHS "
                     "(coarse operator of 32^4 Wilson-clover on 4^4 blocks)",
         "coarse_dims": list(DIMS), "nbasis": NBASIS, "nrhs": NRHS, "op": "M",
-        "form": form, "l2": "flushed between timed steps (256 MiB write); links exceed L2",
+        "l2": "flushed between timed steps: 256 MiB written, then 256 MiB of a second buffer read, so that the "
+              "flush's dirty lines are written back before the step starts; inputs and links are not in L2",
         "parallelism": "replicas",
     }
 
@@ -273,7 +279,18 @@ def main():
     xin = xin64.to(torch.complex64).contiguous()
     out = torch.zeros_like(xin)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    flush_rd = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    flush_sum = torch.empty((), dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream()
+
+    def l2_flush(k, mode=None):
+        """Evict the step's operands from L2: write 256 MiB; then (write+read) read another
+        256 MiB, which writes the written lines back to DRAM before the step instead of
+        during it (a write-only flush leaves ~126 MB of dirty lines that the next step's
+        first kernel pays to evict)."""
+        flush.fill_(float(k))
+        if (mode or args.flush) == "write+read":
+            torch.sum(flush_rd, dim=0, out=flush_sum)
 
     # accuracy of each form against the FP64 GPU path (itself pinned to the oracle)
     ref64 = torch.zeros_like(xin64)
@@ -293,8 +310,8 @@ def main():
         step(args.form)
     torch.cuda.synchronize()
     if args.kernel_only:
-        for _ in range(args.steps):
-            flush.fill_(1.0)
+        for k in range(args.steps):
+            l2_flush(k)
             step(args.form)
         torch.cuda.synchronize()
         print(json.dumps({"kernel_only": True, "steps": args.steps, "form": args.form}))
@@ -311,21 +328,29 @@ def main():
     sampler = ClockSampler(local) if rank == 0 else None
     torch.cuda.synchronize()
     for k in range(args.steps):
-        flush.fill_(float(k))
+        l2_flush(k)
         ev[k][0].record(stream)
         step(args.form)
         ev[k][1].record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop() if sampler else None
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    # the same steps after a write-only flush, for comparison (not the value)
+    for k in range(args.steps):
+        l2_flush(k, "write")
+        ev[k][0].record(stream)
+        step(args.form)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    t_write_only = sum(a.elapsed_time(b) for a, b in ev)
     if dist:
         dist.barrier()
-    t_ms = sum(a.elapsed_time(b) for a, b in ev)
     import ctypes
 
     # kernel-duration pass: the same K steps with the per-kernel events on
     gmg.lib().gmg_profile_enable(1)
     for k in range(args.steps):
-        flush.fill_(float(k))
+        l2_flush(k)
         step(args.form)
     torch.cuda.synchronize()
     gmg.lib().gmg_profile_enable(0)
@@ -347,8 +372,8 @@ def main():
             cm.M(inp, o, compute=form)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         tt = 0.0
-        for _ in range(n):
-            flush.fill_(1.0)
+        for kk in range(n):
+            l2_flush(kk)
             e0.record(stream)
             cm.M(inp, o, compute=form)
             e1.record(stream)
@@ -363,50 +388,79 @@ def main():
     # over three streams so that step k+1's copy-in and step k-1's copy-out
     # (separate copy engines) overlap step k's apply; every step still moves
     # its whole input and result across PCIe.
-    host_in = torch.from_numpy(x.astype(np.complex64)).pin_memory()
-    host_out = torch.empty_like(host_in).pin_memory()
-    dev_in = [torch.empty_like(xin) for _ in range(2)]
-    dev_out = [torch.empty_like(xin) for _ in range(2)]
     s_in, s_cmp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
     ne = max(10, min(200, args.steps // 10))
 
-    def e2e_run(nsteps, e0=None, e1=None):
-        ev_in = [torch.cuda.Event() for _ in range(nsteps)]
-        ev_cmp = [torch.cuda.Event() for _ in range(nsteps)]
-        ev_out = [torch.cuda.Event() for _ in range(nsteps)]
-        s_in.wait_stream(torch.cuda.current_stream())
-        if e0 is not None:
-            e0.record(s_in)
-        for k in range(nsteps):
-            b = k % 2
-            with torch.cuda.stream(s_in):
-                if k >= 2:
-                    s_in.wait_event(ev_cmp[k - 2])  # dev_in[b] no longer read
-                dev_in[b].copy_(host_in, non_blocking=True)
-                ev_in[k].record(s_in)
-            with torch.cuda.stream(s_cmp):
-                s_cmp.wait_event(ev_in[k])
-                if k >= 2:
-                    s_cmp.wait_event(ev_out[k - 2])  # dev_out[b] copied out
-                cm.M(dev_in[b], dev_out[b], compute=args.form)
-                ev_cmp[k].record(s_cmp)
-            with torch.cuda.stream(s_out):
-                s_out.wait_event(ev_cmp[k])
-                host_out.copy_(dev_out[b], non_blocking=True)
-                ev_out[k].record(s_out)
-        s_out.wait_stream(s_in)
-        s_out.wait_stream(s_cmp)
-        if e1 is not None:
-            e1.record(s_out)
-        torch.cuda.synchronize()
+    def e2e_measure(compute, xhost):
+        host_in = torch.from_numpy(xhost).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        dev_in = [torch.empty(host_in.shape, dtype=host_in.dtype, device=dev) for _ in range(2)]
+        dev_out = [torch.empty_like(d) for d in dev_in]
 
-    e2e_run(3)
-    if dist:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2e_run(ne, e0, e1)
-    te = max_over_ranks(e0.elapsed_time(e1), dist, dev)
-    e2e = world * FLOPS * ne / (te * 1e-3) / 1e12
+        def run(nsteps, e0=None, e1=None):
+            ev_in = [torch.cuda.Event() for _ in range(nsteps)]
+            ev_cmp = [torch.cuda.Event() for _ in range(nsteps)]
+            ev_out = [torch.cuda.Event() for _ in range(nsteps)]
+            s_in.wait_stream(torch.cuda.current_stream())
+            if e0 is not None:
+                e0.record(s_in)
+            for k in range(nsteps):
+                b = k % 2
+                with torch.cuda.stream(s_in):
+                    if k >= 2:
+                        s_in.wait_event(ev_cmp[k - 2])  # dev_in[b] no longer read
+                    dev_in[b].copy_(host_in, non_blocking=True)
+                    ev_in[k].record(s_in)
+                with torch.cuda.stream(s_cmp):
+                    s_cmp.wait_event(ev_in[k])
+                    if k >= 2:
+                        s_cmp.wait_event(ev_out[k - 2])  # dev_out[b] copied out
+                    cm.M(dev_in[b], dev_out[b], compute=compute)
+                    ev_cmp[k].record(s_cmp)
+                with torch.cuda.stream(s_out):
+                    s_out.wait_event(ev_cmp[k])
+                    host_out.copy_(dev_out[b], non_blocking=True)
+                    ev_out[k].record(s_out)
+            s_out.wait_stream(s_in)
+            s_out.wait_stream(s_cmp)
+            if e1 is not None:
+                e1.record(s_out)
+            torch.cuda.synchronize()
+
+        run(3)
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        run(ne, e0, e1)
+        te = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+        return world * FLOPS * ne / (te * 1e-3) / 1e12, int(host_in.numel() * host_in.element_size())
+
+    e2e, e2e_bytes = e2e_measure(args.form, x.astype(np.complex64))
+    # the same apply in FP64 (links and vectors), the reference's own arithmetic:
+    # device-timed steps (L2 flushed) and end to end with complex128 host buffers
+    n64 = max(5, min(100, args.steps))
+    o64 = torch.zeros_like(xin64)
+    for _ in range(3):
+        cm.M(xin64, o64, compute="f64")
+    ev64 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n64)]
+    torch.cuda.synchronize()
+    for k in range(n64):
+        l2_flush(k)
+        ev64[k][0].record(stream)
+        cm.M(xin64, o64, compute="f64")
+        ev64[k][1].record(stream)
+    torch.cuda.synchronize()
+    t64 = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev64), dist, dev)
+    e2e64, e2e64_bytes = e2e_measure("f64", x)
+    f64_leg = {
+        "value": world * FLOPS * n64 / (t64 * 1e-3) / 1e12, "unit": UNIT, "steps": n64,
+        "ms_per_step": t64 / n64, "dtype": "f64",
+        "form": "FP64 links and vectors on the CUDA cores (coarse_simt_kernel), the arithmetic of the reference "
+                "and of its CPU arm",
+        "e2e": {"value": e2e64, "unit": UNIT, "h2d_bytes_per_step": e2e64_bytes, "d2h_bytes_per_step": e2e64_bytes,
+                "how": "public gmg_coarse_apply (compute F64) with pinned complex128 host input/output every step, "
+                       "double-buffered as the headline e2e"},
+    }
 
     hbm, src = peaks()
     kavg_s = (kms.value / max(kn.value, 1)) * 1e-3
@@ -419,9 +473,10 @@ def main():
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.form,
         "data": "synthetic (seeded Gaussian links with gamma5-hermitian structure, unit-Gaussian RHS)",
-        "config": dict(config_dict(f"{args.form} operands on tcgen05 tensor cores, FP32 accumulation, FP32 vectors"),
-                       tile={"ctas_per_sm": tc_ctas.value, "points_per_stage": tc_pps.value,
-                             "chosen_by": "autotuner (first apply times every shape that fits)"}),
+        "config": config_dict(),
+        "form": f"{args.form} operands on tcgen05 tensor cores, FP32 accumulation, FP32 vectors",
+        "tile": {"ctas_per_sm": tc_ctas.value, "points_per_stage": tc_pps.value,
+                 "chosen_by": "autotuner (first apply times every shape that fits)"},
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None, "traffic": TC_KERNEL_TRAFFIC,
@@ -436,32 +491,42 @@ def main():
         },
         "apply_roofline": {"algorithmic_bytes": APPLY_BYTES,
                            "achieved_gbs": APPLY_BYTES / (t_ms * 1e-3 / args.steps) / 1e9},
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": VEC_BYTES_F32,
-                "d2h_bytes_per_step": VEC_BYTES_F32,
+        "l2_flush": {"mode": args.flush,
+                     "write_only_flush_ms_per_step": t_write_only / args.steps,
+                     "note": "the same steps timed after a write-only flush, whose dirty lines the step evicts"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": e2e_bytes,
+                "d2h_bytes_per_step": e2e_bytes,
                 "how": "public gmg_coarse_apply with pinned host input/output every step; double-buffered on "
                        "three streams: step k+1's copy-in and step k-1's copy-out overlap step k"},
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
         "forms": forms,
+        "f64_leg": f64_leg,
     }
     if rank == 0 and world == 1:
         cpu, _ = cpu_sample(A, x)
         line["cpu_baseline"] = cpu
     if not args.no_mg:
         # the MG solve half of the metric: 3-level K-cycle FGMRES on 32^4 Wilson-clover,
-        # 24 RHS to 1e-10, the mixed BF16 multi-RHS form against the plain FP64
-        # single-RHS form (timed on one RHS, scaled to 24); setup not in solve_s
+        # 24 RHS to 1e-10: the mixed BF16 multi-RHS form with the K-cycle replayed as a
+        # CUDA graph (timed on its second solve; the first also captures), the same
+        # form host-driven, and the plain FP64 single-RHS form on all 24 RHS one at a
+        # time; setup not in the solve times
         torch.cuda.empty_cache()
         import suite
 
-        mg = suite.c5_measure(nrhs=24, plain_rhs=1, forms=("mixed_bf16_mrhs", "plain_f64_single_rhs"))
+        mg = suite.c5_measure(nrhs=24, plain_rhs=24,
+                              forms=("mixed_bf16_mrhs_graph", "mixed_bf16_mrhs", "plain_f64_single_rhs"))
         line["mg_solve"] = {
             "workload": "3-level K-cycle MG-preconditioned FGMRES, 32^4 Wilson-clover m=-0.35 csw 1, "
                         "nbasis 24 / 32 on 4^4 / 2^4 blocks, 24 RHS to 1e-10",
             "unit": "s", "higher_is_better": False,
-            "mixed_bf16_mrhs_s": mg["mixed_bf16_mrhs"]["solve_s_for_all_rhs"],
+            "mixed_bf16_mrhs_graph_s": mg["mixed_bf16_mrhs_graph"]["solve_s_for_all_rhs"],
+            "mixed_bf16_mrhs_graph_first_solve_s": mg["mixed_bf16_mrhs_graph"]["first_solve_s"],
+            "mixed_bf16_mrhs_host_driven_s": mg["mixed_bf16_mrhs"]["solve_s_for_all_rhs"],
             "plain_f64_single_rhs_s": mg["plain_f64_single_rhs"]["solve_s_for_all_rhs"],
-            "speedup_vs_plain_f64": mg["mixed_bf16_mrhs"]["speedup_vs_plain_f64"],
+            "plain_f64_rhs_measured": mg["plain_f64_single_rhs"]["rhs_measured"],
+            "speedup_vs_plain_f64": mg["mixed_bf16_mrhs_graph"]["speedup_vs_plain_f64"],
             "details": mg,
         }
     if rank == 0:

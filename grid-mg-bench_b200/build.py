@@ -33,7 +33,8 @@ def nvcc():
 
 
 def _headers():
-    return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    return (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h")) +
+            glob.glob(os.path.join(INCLUDE, "*.hpp")))
 
 
 def _stale(src, obj, hdr_mtime):

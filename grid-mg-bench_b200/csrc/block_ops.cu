@@ -103,6 +103,8 @@ gmg_status agg_basis_to_blocked(gmg_agg* h, const double* basis_dev, cudaStream_
   GMG_CUDA(cudaGetLastError());
   h->basis_f_ok = false;
   h->basis_tc_ok = false;
+  // a new basis: the failure flag of the previous orthonormalisation no longer applies
+  if (h->ortho_ws.p) GMG_CUDA(cudaMemsetAsync(h->ortho_ws.p, 0, sizeof(int), s));
   return GMG_OK;
 }
 

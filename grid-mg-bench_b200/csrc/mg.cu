@@ -76,6 +76,10 @@ struct gmg_mg {
   gmg::VecBuf ogz;
   cudaStream_t cap_st[8] = {};
   bool graph_broken = false;
+  // per-RHS outcome of the last solve: the outer iteration count at which the
+  // RHS left the active batch (its true residual below tol), and that residual
+  std::vector<int> last_iters;
+  std::vector<double> last_relres;
   ~gmg_mg() {
     for (auto& g : kgraph) cudaGraphExecDestroy(g.second);
     for (auto& st : cap_st)
@@ -1151,6 +1155,7 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
   std::vector<int> active(nrhs);
   for (int r = 0; r < nrhs; ++r) active[r] = r;
   std::vector<double> relres(nrhs, 1.0);
+  std::vector<int> conv_it(nrhs, 0);
   int total = 0;
   // per-RHS norms of b for the global convergence criterion
   std::vector<zc> bnz;
@@ -1205,6 +1210,7 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
     for (int k = 0; k < Ra; ++k) {
       const int r = active[k];
       relres[r] = std::sqrt(std::max(rn[k].real(), 0.0) / std::max(bnz[r].real(), 1e-300));
+      conv_it[r] = total;
       if (relres[r] > tol) still.push_back(r);
     }
     if (it == 0 && still.size() == active.size()) break;  // no progress possible
@@ -1215,7 +1221,20 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
   for (double v : relres) mx = std::max(mx, v);
   if (iters_out) *iters_out = total;
   if (max_relres) *max_relres = mx;
+  h->last_iters = conv_it;
+  h->last_relres = relres;
   if (mx > tol) return fail(GMG_ERR_NOT_CONVERGED, "gmg_mg_solve: not converged within maxiter");
+  return GMG_OK;
+}
+
+extern "C" gmg_status gmg_mg_solve_stats(gmg_mg* h, int nrhs, int* iters, double* relres) {
+  GMG_CHECK(h && iters && relres, GMG_ERR_ARGUMENT, "gmg_mg_solve_stats: null argument");
+  GMG_CHECK(nrhs == (int)h->last_iters.size(), GMG_ERR_SHAPE,
+            "gmg_mg_solve_stats: nrhs differs from the last solve's");
+  for (int r = 0; r < nrhs; ++r) {
+    iters[r] = h->last_iters[r];
+    relres[r] = h->last_relres[r];
+  }
   return GMG_OK;
 }
 

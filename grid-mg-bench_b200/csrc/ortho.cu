@@ -21,19 +21,22 @@
 // s = 11 (K N + N (N + 1)) u ||V_c||_F^2, which always factors, and that block
 // gets two extra plain passes.
 //
-// Two kernels per pass:
-//   gram_chol_kernel   CTA per block (persistent over blocks): the Gram matrix
-//                      from FP64 register tiles over the lower block triangle,
-//                      fed by a cp.async double buffer of K-chunks, then the
-//                      Cholesky factor in shared memory; writes conj(L) and
-//                      1 / diag(L) packed (row i: i + 1 entries) per block.
-//   tri_solve_kernel   thread per column of V_c: the N entries of the column in
-//                      registers, forward substitution against conj(L) held in
-//                      shared memory (every thread reads the same entry: a
-//                      broadcast), the column written back in place.
+// Three kernels per pass (nbasis up to 40):
+//   gram_kernel      CTA per block (persistent over blocks): the Gram matrix
+//                    from FP64 register tiles over the lower block triangle, fed
+//                    by a three-stage cp.async pipeline of K-chunks with one
+//                    barrier per chunk; writes the packed lower triangle.
+//   factor_kernel    warp per block: the Cholesky factor in shared memory, lane
+//                    i owning row i; the shifted retry re-reads the Gram matrix;
+//                    writes conj(L) and 1 / diag(L) packed (row i: i + 1 entries).
+//   tri_solve_kernel thread per column of V_c: the column in registers, forward
+//                    substitution against conj(L) in shared memory (every thread
+//                    reads the same entry: a broadcast), the column written back
+//                    in place; the next column batch is copied into shared
+//                    memory (cp.async) while the current one is solved.
 // Traffic per pass: the basis read twice and written once (3 x 8 B x 2 x N x K
-// per block); flops 8 K N (N + 1) / 2 for the Gram matrix (lower triangle) and
-// the same for the substitution.
+// per block) plus the small factors; flops 8 K N (N + 1) / 2 for the Gram
+// matrix (lower triangle) and the same for the substitution.
 //
 // Layout: basis_blk [c][i][k] complex128, k = sb * dof + a (one block's panel
 // contiguous).
@@ -47,9 +50,12 @@ namespace gmg {
 namespace ortho {
 
 constexpr int kThreads = 256;
-constexpr int kKC = 64;        // K values per staged chunk
-constexpr int kMaxKG = 16;     // K-interleaved groups of tile threads
-constexpr int kSolveMax = 40;  // largest nbasis of the two-kernel path
+constexpr int kKC = 64;         // K values per pipeline stage (at most)
+constexpr int kStages = 3;      // cp.async pipeline depth of the Gram kernel
+constexpr int kMaxKG = 16;      // K-interleaved groups of tile threads
+constexpr int kSolveMax = 40;   // largest nbasis of the three-kernel path
+constexpr int kFactorWarps = 4;  // blocks (one per warp) per factor CTA
+constexpr int kSolveThreads = 128;  // columns per solve chunk (three CTAs per SM at 170 registers)
 
 __device__ __forceinline__ double2 cfma_conj(double2 acc, double2 a, double2 b) {  // acc += conj(a) b
   acc.x = fma(a.x, b.x, acc.x);
@@ -71,11 +77,12 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // Tile geometry of the Gram matrix for nbasis N: NT tiles per side, tile (ti, tj)
 // owning rows ti + NT q and columns tj + NT r (q, r < 4), only ti >= tj (the
 // others are conjugate transposes); KG groups of tile threads take interleaved
-// K entries of a chunk.  Staging tiles are [kKC][Np] complex with Np = 4 NT + 1
-// (the odd row length spreads the transposed 16-byte writes over the banks).
+// K entries of a chunk of KC = KG * floor(kKC / KG) entries (equal shares).
+// Staging tiles are [kKC][Np] complex with Np = 4 NT + 1 (the odd row length
+// spreads the transposed 16-byte writes over the banks).
 struct Geo {
-  int N, NT, Np, ntiles, KG;
-  size_t stage_bytes, red_bytes, g_bytes, smem;
+  int N, NT, Np, ntiles, KG, KC;
+  size_t stage_bytes, red_bytes, smem;
 };
 
 inline Geo geometry(int N) {
@@ -85,120 +92,318 @@ inline Geo geometry(int N) {
   g.Np = 4 * g.NT + 1;
   g.ntiles = g.NT * (g.NT + 1) / 2;
   g.KG = std::max(1, std::min(kMaxKG, kThreads / g.ntiles));
-  g.stage_bytes = sizeof(double2) * 2 * kKC * (size_t)g.Np;
+  g.KC = g.KG * std::max(1, kKC / g.KG);
+  g.stage_bytes = sizeof(double2) * kStages * kKC * (size_t)g.Np;
   g.red_bytes = sizeof(double2) * 16 * (size_t)g.KG * g.ntiles;
-  g.g_bytes = sizeof(double2) * (size_t)N * N + sizeof(double) * N;
-  g.smem = std::max(g.stage_bytes, g.red_bytes) + g.g_bytes;
+  g.smem = std::max(g.stage_bytes, g.red_bytes);
   return g;
 }
 
 struct Params {
-  double2* basis;          // [Vc][N][K]
-  double2* lfac;           // [Vc][N (N + 1) / 2]: conj(L[i][j]) for j < i, (1 / L[i][i], 0) for j = i
-  int* need;               // [Vc]: 1 once a block needed the shifted factorisation
-  int* status;             // 1 when a shifted factorisation failed too
+  double2* basis;              // [Vc][N][K]
+  double2* gram;               // [Vc][N (N + 1) / 2]: G[i][j], j <= i
+  double2* lfac;               // [Vc][N (N + 1) / 2]: conj(L[i][j]) for j < i, (1 / L[i][i], 0) for j = i
+  int* need;                   // [Vc]: 1 once a block needed the shifted factorisation
+  int* status;                 // 1 when a shifted factorisation failed too
   unsigned long long* maxerr;  // check mode: max |G - 1| (as the bits of a non-negative double)
-  int Vc, N, K, NT, Np, ntiles, KG;
+  int Vc, N, K, NT, Np, ntiles, KG, KC;
   int pass, passes;
 };
 
-// Gram matrix of block c into G (lower triangle, row-major N x N).  All threads
-// call it; `stage` holds two chunk buffers, then the per-group partial tiles.
-__device__ void block_gram(const Params& P, const double2* __restrict__ Vb, double2* stage, double2* G) {
+__device__ __forceinline__ bool block_active(const Params& P, int c) { return P.pass < P.passes || P.need[c] != 0; }
+
+// Gram matrices of the blocks (packed lower triangles into P.gram), or in
+// CHECK mode the largest |G - 1| over all blocks into P.maxerr.
+template <bool CHECK>
+__global__ void __launch_bounds__(kThreads, 2) gram_kernel(Params P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* stage = reinterpret_cast<double2*>(smem_raw);  // [kStages][kKC][Np], then the partial tiles
   const int t = threadIdx.x;
-  const int NT = P.NT, Np = P.Np, N = P.N, K = P.K;
+  const int NT = P.NT, Np = P.Np, N = P.N, K = P.K, KC = P.KC, KG = P.KG;
   const int tile = t % P.ntiles, grp = t / P.ntiles;
-  const bool active = grp < P.KG;
+  const bool active = grp < KG;
   int ti = 0;
   while ((ti + 1) * (ti + 2) / 2 <= tile) ++ti;
   const int tj = tile - ti * (ti + 1) / 2;
-  double2 acc[4][4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int r = 0; r < 4; ++r) acc[q][r] = make_double2(0.0, 0.0);
-  const int nch = (K + kKC - 1) / kKC;
-  auto issue = [&](int ch) {
-    double2* buf = stage + (ch & 1) * kKC * Np;
-    const int k0 = ch * kKC;
-    const int kc = min(kKC, K - k0);
-    for (int e = t; e < N * kKC; e += kThreads) {
-      const int i = e / kKC, kk = e % kKC;
-      if (kk < kc) cp_async16(buf + kk * Np + i, Vb + (int64_t)i * K + k0 + kk);
-    }
-    cp_async_commit();
-  };
-  __syncthreads();  // the previous user of `stage` (reduction or solve) is done
-  issue(0);
-  for (int ch = 0; ch < nch; ++ch) {
-    if (ch + 1 < nch) {
-      issue(ch + 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
-    if (active) {
-      const double2* buf = stage + (ch & 1) * kKC * Np;
-      const int kc = min(kKC, K - ch * kKC);
-#pragma unroll 2
-      for (int kk = grp; kk < kc; kk += P.KG) {
-        double2 a[4], b[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) a[q] = buf[kk * Np + ti + NT * q];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) b[r] = buf[kk * Np + tj + NT * r];
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-          for (int r = 0; r < 4; ++r) acc[q][r] = cfma_conj(acc[q][r], a[q], b[r]);
+  const int nch = (K + KC - 1) / KC;
+  double mx = 0.0;
+  for (int c = blockIdx.x; c < P.Vc; c += gridDim.x) {
+    if (!CHECK && !block_active(P, c)) continue;  // uniform over the CTA
+    const double2* Vb = P.basis + (int64_t)c * N * K;
+    auto issue = [&](int ch) {
+      if (ch < nch) {
+        double2* buf = stage + (ch % kStages) * kKC * Np;
+        const int k0 = ch * KC;
+        const int kc = min(KC, K - k0);
+        for (int e = t; e < N * KC; e += kThreads) {
+          const int i = e / KC, kk = e - i * KC;
+          if (kk < kc) cp_async16(buf + kk * Np + i, Vb + (int64_t)i * K + k0 + kk);
+        }
       }
-    }
-    __syncthreads();  // buffer (ch & 1) is refilled by the issue of chunk ch + 2
-  }
-  // partial tiles of every group, then the sum over groups per lower entry
-  if (active) {
-    double2* red = stage + ((size_t)grp * P.ntiles + tile) * 16;
+      cp_async_commit();  // an empty group past the last chunk keeps the group count uniform
+    };
+    double2 acc[4][4];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
 #pragma unroll
-      for (int r = 0; r < 4; ++r) red[q * 4 + r] = acc[q][r];
-  }
-  __syncthreads();
-  for (int e = t; e < N * N; e += kThreads) {
-    const int i = e / N, j = e % N;
-    if (j > i) continue;
-    const int qi = i / NT, ti2 = i % NT, rj = j / NT, tj2 = j % NT;
-    double2 s = make_double2(0.0, 0.0);
-    if (ti2 >= tj2) {
-      const double2* src = stage + (size_t)(ti2 * (ti2 + 1) / 2 + tj2) * 16 + qi * 4 + rj;
-      for (int g = 0; g < P.KG; ++g) {
-        const double2 v = src[(size_t)g * P.ntiles * 16];
-        s.x += v.x;
-        s.y += v.y;
-      }
-    } else {  // the conjugate of entry (j, i), held by tile (tj2, ti2)
-      const double2* src = stage + (size_t)(tj2 * (tj2 + 1) / 2 + ti2) * 16 + rj * 4 + qi;
-      for (int g = 0; g < P.KG; ++g) {
-        const double2 v = src[(size_t)g * P.ntiles * 16];
-        s.x += v.x;
-        s.y -= v.y;
+      for (int r = 0; r < 4; ++r) acc[q][r] = make_double2(0.0, 0.0);
+    __syncthreads();  // the previous block's reduction no longer reads `stage`
+#pragma unroll
+    for (int sidx = 0; sidx < kStages - 1; ++sidx) issue(sidx);
+    for (int ch = 0; ch < nch; ++ch) {
+      cp_async_wait<kStages - 2>();  // this thread's copies of chunk ch have landed
+      __syncthreads();               // everyone's have; chunk ch - 1 is no longer read
+      issue(ch + kStages - 1);       // into the buffer chunk ch - 1 used
+      if (active) {
+        const double2* buf = stage + (ch % kStages) * kKC * Np;
+        const int kc = min(KC, K - ch * KC);
+#pragma unroll 2
+        for (int kk = grp; kk < kc; kk += KG) {
+          double2 a[4], b[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) a[q] = buf[kk * Np + ti + NT * q];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) b[r] = buf[kk * Np + tj + NT * r];
+          // conj(a) b in two sweeps over the 16 accumulators, so that the two
+          // dependent FMAs of each component are 32 instructions apart
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              acc[q][r].x = fma(a[q].x, b[r].x, acc[q][r].x);
+              acc[q][r].y = fma(a[q].x, b[r].y, acc[q][r].y);
+            }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              acc[q][r].x = fma(a[q].y, b[r].y, acc[q][r].x);
+              acc[q][r].y = fma(-a[q].y, b[r].x, acc[q][r].y);
+            }
+        }
       }
     }
-    G[i * N + j] = s;
+    cp_async_wait<0>();
+    __syncthreads();  // all chunks consumed: `stage` takes the partial tiles
+    if (active) {
+      double2* red = stage + ((size_t)grp * P.ntiles + tile) * 16;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) red[q * 4 + r] = acc[q][r];
+    }
+    __syncthreads();
+    double2* Gc = P.gram + (int64_t)c * (N * (N + 1) / 2);
+    for (int e = t; e < N * N; e += kThreads) {
+      const int i = e / N, j = e - (e / N) * N;
+      if (j > i) continue;
+      const int qi = i / NT, ti2 = i - qi * NT, rj = j / NT, tj2 = j - rj * NT;
+      double2 sum = make_double2(0.0, 0.0);
+      if (ti2 >= tj2) {
+        const double2* src = stage + (size_t)(ti2 * (ti2 + 1) / 2 + tj2) * 16 + qi * 4 + rj;
+        for (int g = 0; g < KG; ++g) {
+          const double2 v = src[(size_t)g * P.ntiles * 16];
+          sum.x += v.x;
+          sum.y += v.y;
+        }
+      } else {  // the conjugate of entry (j, i), held by tile (tj2, ti2)
+        const double2* src = stage + (size_t)(tj2 * (tj2 + 1) / 2 + ti2) * 16 + rj * 4 + qi;
+        for (int g = 0; g < KG; ++g) {
+          const double2 v = src[(size_t)g * P.ntiles * 16];
+          sum.x += v.x;
+          sum.y -= v.y;
+        }
+      }
+      if (CHECK) {
+        const double re = sum.x - (i == j ? 1.0 : 0.0);
+        mx = fmax(mx, sqrt(re * re + sum.y * sum.y));
+      } else {
+        Gc[i * (i + 1) / 2 + j] = sum;
+      }
+    }
   }
-  __syncthreads();
+  if (CHECK) atomicMax(P.maxerr, (unsigned long long)__double_as_longlong(mx));  // non-negative doubles order as integers
 }
 
-// Cholesky G + shift I = L L^dag in place (strict lower triangle of G; the
-// diagonal goes to diag[]).  Returns false to every thread when a pivot is not
-// positive (that pivot is replaced by 1 so that the factor stays finite).
+// Cholesky factor of one block's Gram matrix by one warp: G + shift I = L L^dag,
+// rows in shared memory at stride N + 1 (lane i owns rows i and i + 32), the
+// strict lower triangle of L in place of G, the diagonal in diag[].  Returns
+// false when a pivot is not positive (replaced by 1 so that L stays finite).
+__device__ bool warp_cholesky(double2* G, double* diag, int N, double shift) {
+  const int lane = threadIdx.x & 31, Sp = N + 1;
+  bool ok = true;
+  for (int j = 0; j < N; ++j) {
+    double d = G[j * Sp + j].x + shift;
+    if (!(d > 0.0)) {
+      ok = false;
+      d = 1.0;
+    }
+    const double dj = sqrt(d), inv = 1.0 / dj;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int i = lane + 32 * h;
+      if (i > j && i < N) {
+        const double2 v = G[i * Sp + j];
+        G[i * Sp + j] = make_double2(v.x * inv, v.y * inv);
+      }
+    }
+    if (lane == 0) diag[j] = dj;
+    __syncwarp();
+    // trailing update G[i][k] -= L[i][j] conj(L[k][j]), j < k <= i: lane i walks
+    // k in step with the other lanes, so L[k][j] is one broadcast read
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int i = lane + 32 * h;
+      if (i > j && i < N) {
+        const double2 a = G[i * Sp + j];
+#pragma unroll 4
+        for (int k = j + 1; k <= i; ++k) {
+          const double2 b = G[k * Sp + j];
+          double2 g = G[i * Sp + k];
+          g.x -= a.x * b.x + a.y * b.y;
+          g.y -= a.y * b.x - a.x * b.y;
+          G[i * Sp + k] = g;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  return ok;
+}
+
+__global__ void __launch_bounds__(32 * kFactorWarps) factor_kernel(Params P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int N = P.N, Sp = N + 1, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int c = blockIdx.x * kFactorWarps + w;
+  if (c >= P.Vc || !block_active(P, c)) return;  // whole warps leave; no block-wide barrier follows
+  double2* G = reinterpret_cast<double2*>(smem_raw) + (size_t)w * N * Sp;
+  double* diag = reinterpret_cast<double*>(reinterpret_cast<double2*>(smem_raw) + (size_t)kFactorWarps * N * Sp) +
+                 (size_t)w * N;
+  const int nl = N * (N + 1) / 2;
+  const double2* Gc = P.gram + (int64_t)c * nl;
+  auto load = [&]() {
+    for (int i = 0; i < N; ++i)
+      for (int j = lane; j <= i; j += 32) G[i * Sp + j] = Gc[i * (i + 1) / 2 + j];
+    __syncwarp();
+  };
+  load();
+  bool ok = warp_cholesky(G, diag, N, 0.0);
+  if (!ok) {
+    // shifted Cholesky QR on the same Gram matrix, and two extra passes for this block
+    load();
+    double tr = 0.0;
+    for (int i = lane; i < N; i += 32) tr += G[i * Sp + i].x;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) tr += __shfl_xor_sync(0xffffffffu, tr, off);
+    const double shift = 11.0 * ((double)P.K * N + (double)N * (N + 1)) * 1.1102230246251565e-16 * tr;
+    ok = warp_cholesky(G, diag, N, shift);
+    if (lane == 0) {
+      P.need[c] = 1;
+      if (!ok) atomicExch(P.status, 1);
+    }
+  }
+  double2* Lc = P.lfac + (int64_t)c * nl;
+  for (int i = 0; i < N; ++i)
+    for (int j = lane; j <= i; j += 32) {
+      const double2 v = G[i * Sp + j];
+      Lc[i * (i + 1) / 2 + j] = j < i ? make_double2(v.x, -v.y) : make_double2(1.0 / diag[i], 0.0);
+    }
+}
+
+// W = conj(L)^{-1} V for every column of every block: thread per column, the
+// column in registers (NMAX entries, rows >= N unused), conj(L) in shared
+// memory; the CTA walks the blocks of its grid stride and every 256-column
+// chunk of each, with the next chunk's columns copied into shared memory while
+// the current chunk is solved.
+template <int NMAX>
+__global__ void __launch_bounds__(kSolveThreads) tri_solve_kernel(Params P) {
+  constexpr int NTS = kSolveThreads;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* pre = reinterpret_cast<double2*>(smem_raw);  // [NMAX][NTS]: the prefetched columns
+  double2* L = pre + NMAX * NTS;                        // packed conj(L) of the current block
+  const int N = P.N, K = P.K, t = threadIdx.x;
+  const int nl = N * (N + 1) / 2;
+  const int chunks = (K + NTS - 1) / NTS;
+  // this CTA's work items (block, chunk) in order, skipping inactive blocks
+  auto next_block = [&](int c) {
+    for (; c < P.Vc; c += gridDim.x)
+      if (block_active(P, c)) return c;
+    return P.Vc;
+  };
+  auto prefetch = [&](int c, int ch) {
+    const int k = ch * NTS + t;
+    if (c < P.Vc && k < K) {
+      const double2* col = P.basis + (int64_t)c * N * K + k;
+#pragma unroll
+      for (int i = 0; i < NMAX; ++i)
+        if (i < N) cp_async16(pre + i * NTS + t, col + (int64_t)i * K);
+    }
+    cp_async_commit();
+  };
+  int c = next_block(blockIdx.x), ch = 0;
+  int lc = -1;  // the block whose factor is in L
+  prefetch(c, ch);
+  while (c < P.Vc) {
+    // the item after this one
+    int nc = c, nch = ch + 1;
+    if (nch == chunks) {
+      nc = next_block(c + gridDim.x);
+      nch = 0;
+    }
+    if (c != lc) {
+      __syncthreads();  // every thread is done with the previous block's factor
+      const double2* src = P.lfac + (int64_t)c * nl;
+      for (int e = t; e < nl; e += NTS) L[e] = src[e];
+      __syncthreads();
+      lc = c;
+    }
+    cp_async_wait<0>();  // this thread's columns of the current item (its own slots only)
+    const int k = ch * NTS + t;
+    double2 w[NMAX];
+#pragma unroll
+    for (int i = 0; i < NMAX; ++i) w[i] = (i < N && k < K) ? pre[i * NTS + t] : make_double2(0.0, 0.0);
+    prefetch(nc, nch);  // the slots are free again: copy the next item's columns meanwhile
+    if (k < K) {
+#pragma unroll
+      for (int i = 0; i < NMAX; ++i) {
+        if (i < N) {
+          // four partial sums (j mod 4) shorten the dependent chains
+          const double2* Li = L + i * (i + 1) / 2;
+          double2 sp[4] = {w[i], make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+#pragma unroll
+          for (int j = 0; j < i; ++j) {  // s -= conj(L[i][j]) w[j]
+            const double2 a = Li[j];
+            double2& s = sp[j & 3];
+            s.x = fma(-a.x, w[j].x, s.x);
+            s.x = fma(a.y, w[j].y, s.x);
+            s.y = fma(-a.x, w[j].y, s.y);
+            s.y = fma(-a.y, w[j].x, s.y);
+          }
+          const double inv = Li[i].x;
+          w[i] = make_double2(((sp[0].x + sp[1].x) + (sp[2].x + sp[3].x)) * inv,
+                              ((sp[0].y + sp[1].y) + (sp[2].y + sp[3].y)) * inv);
+        }
+      }
+      double2* col = P.basis + (int64_t)c * N * K + k;
+#pragma unroll
+      for (int i = 0; i < NMAX; ++i)
+        if (i < N) col[(int64_t)i * K] = w[i];
+    }
+    c = nc;
+    ch = nch;
+  }
+  cp_async_wait<0>();
+}
+
+// Cholesky G + shift I = L L^dag in place by the whole CTA (strict lower
+// triangle of G, row-major N x N; the diagonal goes to diag[]); false to every
+// thread when a pivot is not positive (replaced by 1).  Used by the one-CTA-
+// per-block path below.
 __device__ bool block_cholesky(double2* G, double* diag, int N, double shift, int* fail_s) {
   const int t = threadIdx.x;
   if (t == 0) *fail_s = 0;
   __syncthreads();
   for (int j = 0; j < N; ++j) {
-    // column j: every thread takes the pivot from G[j][j] (final after step j - 1)
     double d = G[j * N + j].x + shift;
     const bool bad = !(d > 0.0);
     if (bad) d = 1.0;
@@ -212,7 +417,6 @@ __device__ bool block_cholesky(double2* G, double* diag, int N, double shift, in
       if (bad) *fail_s = 1;
     }
     __syncthreads();
-    // trailing update G[i][k] -= L[i][j] conj(L[k][j]), j < k <= i
     const int m = N - j - 1;
     for (int e = t; e < m * (m + 1) / 2; e += kThreads) {
       int ii = (int)((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
@@ -229,113 +433,6 @@ __device__ bool block_cholesky(double2* G, double* diag, int N, double shift, in
     __syncthreads();
   }
   return *fail_s == 0;
-}
-
-template <bool CHECK>
-__global__ void __launch_bounds__(kThreads, 2) gram_chol_kernel(Params P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int N = P.N;
-  const size_t st_a = (size_t)2 * kKC * P.Np, st_b = (size_t)16 * P.KG * P.ntiles;
-  const size_t stage_elems = st_a > st_b ? st_a : st_b;  // double2 units
-  double2* stage = reinterpret_cast<double2*>(smem_raw);
-  double2* G = stage + stage_elems;
-  double* diag = reinterpret_cast<double*>(G + (size_t)N * N);
-  __shared__ int fail_s;
-  __shared__ double trace_s;
-  const int t = threadIdx.x;
-  for (int c = blockIdx.x; c < P.Vc; c += gridDim.x) {
-    if (!CHECK && P.pass >= P.passes && P.need[c] == 0) continue;  // extra passes: broken-down blocks only
-    const double2* Vb = P.basis + (int64_t)c * N * P.K;
-    block_gram(P, Vb, stage, G);
-    if (CHECK) {
-      double m = 0.0;
-      for (int e = t; e < N * N; e += kThreads) {
-        const int i = e / N, j = e % N;
-        if (j > i) continue;
-        const double re = G[e].x - (i == j ? 1.0 : 0.0), im = G[e].y;
-        m = fmax(m, sqrt(re * re + im * im));
-      }
-      atomicMax(P.maxerr, (unsigned long long)__double_as_longlong(m));  // non-negative doubles order as integers
-      continue;
-    }
-    bool ok = block_cholesky(G, diag, N, 0.0, &fail_s);
-    if (!ok) {
-      // shifted Cholesky QR on the same Gram matrix (formed again: the failed
-      // factorisation overwrote it), then two extra plain passes for this block
-      block_gram(P, Vb, stage, G);
-      if (t == 0) {
-        double tr = 0.0;
-        for (int i = 0; i < N; ++i) tr += G[i * N + i].x;
-        trace_s = tr;
-      }
-      __syncthreads();
-      const double shift = 11.0 * ((double)P.K * N + (double)N * (N + 1)) * 1.1102230246251565e-16 * trace_s;
-      ok = block_cholesky(G, diag, N, shift, &fail_s);
-      if (t == 0) {
-        P.need[c] = 1;
-        if (!ok) atomicExch(P.status, 1);
-      }
-    }
-    // packed conj(L) with the reciprocal diagonal
-    double2* Lc = P.lfac + (int64_t)c * (N * (N + 1) / 2);
-    for (int e = t; e < N * N; e += kThreads) {
-      const int i = e / N, j = e % N;
-      if (j > i) continue;
-      const double2 v = G[e];
-      Lc[i * (i + 1) / 2 + j] = j < i ? make_double2(v.x, -v.y) : make_double2(1.0 / diag[i], 0.0);
-    }
-    __syncthreads();  // G and diag are rewritten for the next block
-  }
-}
-
-// W = conj(L)^{-1} V for every column of every block: thread per column, the
-// column in registers (NMAX entries, rows >= N unused), conj(L) in shared memory.
-template <int NMAX>
-__global__ void __launch_bounds__(kThreads) tri_solve_kernel(Params P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* L = reinterpret_cast<double2*>(smem_raw);  // packed, N (N + 1) / 2
-  const int N = P.N, K = P.K;
-  const int nL = N * (N + 1) / 2;
-  const int chunks = (K + kThreads - 1) / kThreads;
-  const int64_t items = (int64_t)P.Vc * chunks;
-  int prev_c = -1;
-  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
-    const int c = (int)(it / chunks);
-    const int k = (int)(it % chunks) * kThreads + threadIdx.x;
-    if (P.pass >= P.passes && P.need[c] == 0) continue;  // uniform over the CTA
-    if (c != prev_c) {
-      __syncthreads();
-      const double2* src = P.lfac + (int64_t)c * nL;
-      for (int e = threadIdx.x; e < nL; e += kThreads) L[e] = src[e];
-      __syncthreads();
-      prev_c = c;
-    }
-    if (k >= K) continue;
-    double2* col = P.basis + (int64_t)c * N * K + k;
-    double2 w[NMAX];
-#pragma unroll
-    for (int i = 0; i < NMAX; ++i) w[i] = i < N ? col[(int64_t)i * K] : make_double2(0.0, 0.0);
-#pragma unroll
-    for (int i = 0; i < NMAX; ++i) {
-      if (i < N) {
-        const double2* Li = L + i * (i + 1) / 2;
-        double2 s = w[i];
-#pragma unroll
-        for (int j = 0; j < i; ++j) {  // s -= conj(L[i][j]) w[j]
-          const double2 a = Li[j];
-          s.x = fma(-a.x, w[j].x, s.x);
-          s.x = fma(a.y, w[j].y, s.x);
-          s.y = fma(-a.x, w[j].y, s.y);
-          s.y = fma(-a.y, w[j].x, s.y);
-        }
-        const double inv = Li[i].x;
-        w[i] = make_double2(s.x * inv, s.y * inv);
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < NMAX; ++i)
-      if (i < N) col[(int64_t)i * K] = w[i];
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -471,48 +568,64 @@ static int num_sms() {
   return n;
 }
 
-// workspace: [status int + max error][need int Vc][conj(L) Vc x N (N + 1) / 2]
-static gmg_status workspace(gmg_agg* h, int** status, unsigned long long** maxerr, int** need, double2** lfac) {
+// workspace: [status int + max error][need int Vc][Gram Vc x N (N + 1) / 2][conj(L) same]
+static gmg_status workspace(gmg_agg* h, Params* P) {
   const int64_t Vc = h->cdims.vol();
   const size_t head = 256, need_b = (size_t)(Vc * sizeof(int) + 255) / 256 * 256;
   const size_t lf_b = sizeof(double2) * (size_t)Vc * (h->N * (h->N + 1) / 2);
-  GMG_TRY(h->ortho_ws.alloc(head + need_b + lf_b));
+  const void* before = h->ortho_ws.p;
+  GMG_TRY(h->ortho_ws.alloc(head + need_b + 2 * lf_b));
   char* p = h->ortho_ws.as<char>();
-  *status = reinterpret_cast<int*>(p);
-  *maxerr = reinterpret_cast<unsigned long long*>(p + 8);
-  *need = reinterpret_cast<int*>(p + head);
-  *lfac = reinterpret_cast<double2*>(p + head + need_b);
+  if (p != before) GMG_CUDA(cudaMemset(p, 0, head));  // fresh memory: no failure recorded yet
+  const Geo g = geometry(h->N);
+  P->basis = h->basis_blk.as<double2>();
+  P->status = reinterpret_cast<int*>(p);
+  P->maxerr = reinterpret_cast<unsigned long long*>(p + 8);
+  P->need = reinterpret_cast<int*>(p + head);
+  P->gram = reinterpret_cast<double2*>(p + head + need_b);
+  P->lfac = reinterpret_cast<double2*>(p + head + need_b + lf_b);
+  P->Vc = (int)Vc;
+  P->N = h->N;
+  P->K = h->bv * h->dof;
+  P->NT = g.NT;
+  P->Np = g.Np;
+  P->ntiles = g.ntiles;
+  P->KG = g.KG;
+  P->KC = g.KC;
+  P->pass = 0;
+  P->passes = 1;
   return GMG_OK;
 }
 
-static Params params(gmg_agg* h, const Geo& g, int* status, unsigned long long* maxerr, int* need, double2* lfac) {
-  Params P;
-  P.basis = h->basis_blk.as<double2>();
-  P.lfac = lfac;
-  P.need = need;
-  P.status = status;
-  P.maxerr = maxerr;
-  P.Vc = (int)h->cdims.vol();
-  P.N = h->N;
-  P.K = h->bv * h->dof;
-  P.NT = g.NT;
-  P.Np = g.Np;
-  P.ntiles = g.ntiles;
-  P.KG = g.KG;
-  P.pass = 0;
-  P.passes = 1;
-  return P;
+template <bool CHECK>
+static gmg_status launch_gram(const Params& P, cudaStream_t s) {
+  const Geo g = geometry(P.N);
+  GMG_CHECK(g.smem <= 227 * 1024, GMG_ERR_UNSUPPORTED, "orthonormalise: tile does not fit shared memory");
+  GMG_CUDA(cudaFuncSetAttribute(gram_kernel<CHECK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
+  int per_sm = 1;
+  GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gram_kernel<CHECK>, kThreads, g.smem));
+  const int grid = std::min(P.Vc, num_sms() * std::max(per_sm, 1));
+  gram_kernel<CHECK><<<grid, kThreads, g.smem, s>>>(P);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+static gmg_status launch_factor(const Params& P, cudaStream_t s) {
+  const size_t smem = (sizeof(double2) * (size_t)P.N * (P.N + 1) + sizeof(double) * P.N) * kFactorWarps;
+  GMG_CUDA(cudaFuncSetAttribute(factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  factor_kernel<<<(P.Vc + kFactorWarps - 1) / kFactorWarps, 32 * kFactorWarps, smem, s>>>(P);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
 }
 
 template <int NMAX>
 static gmg_status launch_solve(const Params& P, cudaStream_t s) {
-  const size_t smem = sizeof(double2) * (size_t)(P.N * (P.N + 1) / 2);
-  const int chunks = (P.K + kThreads - 1) / kThreads;
-  const int64_t items = (int64_t)P.Vc * chunks;
+  const size_t smem = sizeof(double2) * ((size_t)NMAX * kSolveThreads + (size_t)P.N * (P.N + 1) / 2);
+  GMG_CUDA(cudaFuncSetAttribute(tri_solve_kernel<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 1;
-  GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tri_solve_kernel<NMAX>, kThreads, smem));
-  const int grid = (int)std::min<int64_t>(items, (int64_t)num_sms() * std::max(per_sm, 1) * 4);
-  tri_solve_kernel<NMAX><<<grid, kThreads, smem, s>>>(P);
+  GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tri_solve_kernel<NMAX>, kSolveThreads, smem));
+  const int grid = std::min(P.Vc, num_sms() * std::max(per_sm, 1));
+  tri_solve_kernel<NMAX><<<grid, kSolveThreads, smem, s>>>(P);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
@@ -530,12 +643,10 @@ static gmg_status solve(const Params& P, cudaStream_t s) {
 gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s) {
   using namespace ortho;
   const int N = h->N;
-  int *status, *need;
-  unsigned long long* maxerr;
-  double2* lfac;
-  GMG_TRY(workspace(h, &status, &maxerr, &need, &lfac));
-  const int Vc = (int)h->cdims.vol();
-  GMG_CUDA(cudaMemsetAsync(status, 0, sizeof(int), s));
+  Params P;
+  GMG_TRY(workspace(h, &P));
+  const int Vc = P.Vc;
+  GMG_CUDA(cudaMemsetAsync(P.status, 0, sizeof(int), s));
   if (N > kSolveMax) {
     GMG_CHECK(N <= 64, GMG_ERR_UNSUPPORTED, "orthonormalise: nbasis > 64");
     const size_t smem = sizeof(double2) * ((size_t)2 * N * N + (size_t)kBigKS * h->dof * N) +
@@ -544,24 +655,17 @@ gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s) {
     GMG_CUDA(cudaFuncSetAttribute(big_ortho_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     KernelTimer kt("ortho", s);
     big_ortho_kernel<<<std::min(Vc, num_sms() * 8), kThreads, smem, s>>>(h->basis_blk.as<double2>(), Vc, N, h->dof,
-                                                                        h->bv, passes, status);
+                                                                        h->bv, passes, P.status);
     GMG_CUDA(cudaGetLastError());
   } else {
-    const Geo g = geometry(N);
-    GMG_CHECK(g.smem <= 227 * 1024, GMG_ERR_UNSUPPORTED, "orthonormalise: tile does not fit shared memory");
-    GMG_CUDA(cudaFuncSetAttribute(gram_chol_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
-    GMG_CUDA(cudaMemsetAsync(need, 0, sizeof(int) * Vc, s));
-    Params P = params(h, g, status, maxerr, need, lfac);
+    GMG_CUDA(cudaMemsetAsync(P.need, 0, sizeof(int) * Vc, s));
     P.passes = passes;
-    int per_sm = 1;
-    GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gram_chol_kernel<false>, kThreads, g.smem));
-    const int grid = std::min(Vc, num_sms() * std::max(per_sm, 1));
     KernelTimer kt("ortho", s);
     // passes + 2 rounds: the last two only touch blocks that needed the shift
     for (int pass = 0; pass < passes + 2; ++pass) {
       P.pass = pass;
-      gram_chol_kernel<false><<<grid, kThreads, g.smem, s>>>(P);
-      GMG_CUDA(cudaGetLastError());
+      GMG_TRY(launch_gram<false>(P, s));
+      GMG_TRY(launch_factor(P, s));
       GMG_TRY(solve(P, s));
     }
   }
@@ -572,25 +676,14 @@ gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s) {
 
 gmg_status agg_check_orthogonal(gmg_agg* h, double* max_err, cudaStream_t s) {
   using namespace ortho;
-  const int N = h->N;
-  int *status, *need;
-  unsigned long long* maxerr;
-  double2* lfac;
-  GMG_TRY(workspace(h, &status, &maxerr, &need, &lfac));
-  const Geo g = geometry(N);
-  GMG_CHECK(g.smem <= 227 * 1024, GMG_ERR_UNSUPPORTED, "check orthogonal: tile does not fit shared memory");
-  GMG_CUDA(cudaFuncSetAttribute(gram_chol_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
-  GMG_CUDA(cudaMemsetAsync(maxerr, 0, sizeof(unsigned long long), s));
-  const int Vc = (int)h->cdims.vol();
-  Params P = params(h, g, status, maxerr, need, lfac);
-  int per_sm = 1;
-  GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gram_chol_kernel<true>, kThreads, g.smem));
-  gram_chol_kernel<true><<<std::min(Vc, num_sms() * std::max(per_sm, 1)), kThreads, g.smem, s>>>(P);
-  GMG_CUDA(cudaGetLastError());
+  Params P;
+  GMG_TRY(workspace(h, &P));
+  GMG_CUDA(cudaMemsetAsync(P.maxerr, 0, sizeof(unsigned long long), s));
+  GMG_TRY(launch_gram<true>(P, s));
   unsigned long long v = 0;
   int st = 0;
-  GMG_CUDA(cudaMemcpyAsync(&v, maxerr, sizeof(v), cudaMemcpyDeviceToHost, s));
-  GMG_CUDA(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  GMG_CUDA(cudaMemcpyAsync(&v, P.maxerr, sizeof(v), cudaMemcpyDeviceToHost, s));
+  GMG_CUDA(cudaMemcpyAsync(&st, P.status, sizeof(int), cudaMemcpyDeviceToHost, s));
   GMG_CUDA(cudaStreamSynchronize(s));
   double r;
   memcpy(&r, &v, sizeof(r));

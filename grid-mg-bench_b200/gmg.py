@@ -119,6 +119,19 @@ class CoarsenedMatrix:
         _chk(lib().gmg_coarse_get_links(self._h, a.ctypes.data_as(ctypes.c_void_p), 0, _stream()))
         return a
 
+    def get_links_spins(self, point, ncoarse_spins=2):
+        """Rework link field Y_[point] as [V][Ns_c][Ns_c][Nc_c][Nc_c] complex128."""
+        nc = self.N // ncoarse_spins
+        y = np.zeros((self.V, ncoarse_spins, ncoarse_spins, nc, nc), dtype=np.complex128)
+        _chk(lib().gmg_coarse_get_links_spins(self._h, int(ncoarse_spins), int(point),
+                                              y.ctypes.data_as(ctypes.c_void_p), 0, _stream()))
+        return y
+
+    def set_links_spins(self, Y, ncoarse_spins=2):
+        y = np.ascontiguousarray(Y, dtype=np.complex128)
+        _chk(lib().gmg_coarse_set_links_spins(self._h, int(ncoarse_spins), y.ctypes.data_as(ctypes.c_void_p), 0,
+                                              _stream()))
+
     def prepare(self, compute):
         _chk(lib().gmg_coarse_prepare(self._h, PREC.get(compute, compute), _stream()))
 
@@ -264,6 +277,24 @@ class Aggregation:
         if getattr(self, "_h", None) and _LIB is not None:
             _LIB.gmg_agg_destroy(self._h)
             self._h = None
+
+    def set_subspace_spins(self, vecs, ncoarse_spins=2):
+        """Rework subspace in: vecs [nbasis / ncoarse_spins][Vf][dof] (complex128, host or device)."""
+        if isinstance(vecs, torch.Tensor):
+            v = vecs.to(torch.complex128).contiguous()
+            _chk(lib().gmg_agg_set_subspace_spins(self._h, int(ncoarse_spins), _ptr(v), 1 if v.is_cuda else 0,
+                                                  _stream()))
+            torch.cuda.current_stream().synchronize()
+        else:
+            v = np.ascontiguousarray(vecs, dtype=np.complex128)
+            _chk(lib().gmg_agg_set_subspace_spins(self._h, int(ncoarse_spins), v.ctypes.data_as(ctypes.c_void_p), 0,
+                                                  _stream()))
+
+    def get_subspace_spins(self, ncoarse_spins=2):
+        v = np.zeros((self.N // ncoarse_spins, self.Vf, self.dof), dtype=np.complex128)
+        _chk(lib().gmg_agg_get_subspace_spins(self._h, int(ncoarse_spins), v.ctypes.data_as(ctypes.c_void_p), 0,
+                                              _stream()))
+        return v
 
     def set_coarsen_batch(self, max_batch):
         """Cap the basis vectors per CoarsenOperator batch (0: sized from free memory)."""
@@ -448,6 +479,15 @@ class MultiGrid:
         _chk(lib().gmg_mg_solve(self._h, b.shape[1], _ptr(b), _ptr(x), ctypes.c_double(tol), int(maxiter),
                                 ctypes.byref(it), ctypes.byref(rr), _stream()))
         return it.value, rr.value
+
+    def solve_stats(self, nrhs):
+        """Per-RHS (outer iterations until it left the active batch, final true relative residual)
+        of the last solve."""
+        it = np.zeros(nrhs, dtype=np.int32)
+        rr = np.zeros(nrhs, dtype=np.float64)
+        _chk(lib().gmg_mg_solve_stats(self._h, int(nrhs), it.ctypes.data_as(ctypes.c_void_p),
+                                      rr.ctypes.data_as(ctypes.c_void_p)))
+        return it, rr
 
     def level(self, l):
         op, ag = ctypes.c_void_p(), ctypes.c_void_p()

@@ -14,6 +14,14 @@
 // refinementSetup, outer FGMRES):
 //   (9) |b - D x| / |b| of the solve after the refinement setup
 //   (10) (R D P - D_c) v_c on the operators the refinement rebuilt
+// and the Rework (two-spin, policy-typed) surface of include/gmg_rework.hpp the
+// way src/Benchmark_create_coarse_operator.cc:355-467 checks it:
+//   (11) the Upstream subspace with its chiral doubling undone, copied into the
+//        two-spin aggregation, comes back unchanged and orthonormal
+//   (12) Y_[p] of the two-spin CoarsenOperator against A[p] of the Upstream
+//        one through the layout map (convertLayout), every point
+//   (13) the two-spin M / Mdag / Meooe / MooeeInv Mooee on the same coarse fields
+//   (14) Create(basis vectors) gives an orthonormal two-spin subspace
 // Prints one line per check and exits non-zero if any check fails.
 #include <cuda_runtime.h>
 
@@ -24,7 +32,7 @@
 #include <random>
 #include <vector>
 
-#include "gmg.hpp"
+#include "gmg_rework.hpp"
 
 typedef std::complex<double> cplx;
 
@@ -243,6 +251,66 @@ int main() {
       gmg::check(gmg_agg_project(ag, GMG_F64, GMG_F64, 1, dpf.f.data, rc.f.data, nullptr));
       gmg::check(gmg_coarse_apply(op, GMG_OP_M, 8, GMG_F64, GMG_F64, 1, vc.f.data, dc.f.data, nullptr, 0, nullptr));
       ok &= report("(R D P - D_c) v_c after refinementSetup", rel_dev(rc.get(), dc.get()), 1e-12);
+    }
+    // ------------------------------------------------------------ Rework surface
+    {
+      typedef gmg::Rework::WilsonTwoSpinPolicy<nb> Policy;
+      const gmg::Coordinate rbdims{cdims[0] / 2, cdims[1], cdims[2], cdims[3]};
+      // (11) undoChiralDoublingG5C of the Upstream subspace (Bo), copied into the two-spin aggregation
+      std::vector<cplx> undone(nb * Vf * 12);
+      for (int n = 0; n < nb; ++n)
+        for (long k = 0; k < Vf * 12; ++k) undone[n * Vf * 12 + k] = Bo[n * Vf * 12 + k] + Bo[(n + nb) * Vf * 12 + k];
+      gmg::Rework::Aggregation<Policy> TwoSpinAggs(cdims, fdims, 0, 1);
+      TwoSpinAggs.SetSubspace(reinterpret_cast<const double*>(undone.data()), false);
+      std::vector<cplx> back2(nb * Vf * 12);
+      TwoSpinAggs.GetSubspace(reinterpret_cast<double*>(back2.data()), false);
+      ok &= report("two-spin Subspace() round trip", rel_dev(undone, back2), 1e-16);
+      ok &= report("two-spin CheckOrthogonal", TwoSpinAggs.CheckOrthogonal(), 1e-13);
+
+      // (12) two-spin CoarsenOperator (speed level 1) against the Upstream links
+      gmg::Rework::CoarsenedMatrix<Policy> TwoSpinCMat(cdims, rbdims, 1, 0);
+      TwoSpinCMat.CoarsenOperator(fdims, FineOp, TwoSpinAggs);
+      std::vector<cplx> A(9 * Vc * N * N), Y(Vc * N * N);
+      Dc.GetLinks(reinterpret_cast<double*>(A.data()), false);
+      double worst = 0;
+      for (int p = 0; p < 9; ++p) {
+        TwoSpinCMat.GetLinks(p, reinterpret_cast<double*>(Y.data()), false);
+        // convertLayout: Y(s1, s2)(c1, c2) = A(s1 nb + c1, s2 nb + c2)
+        std::vector<cplx> flat(Vc * N * N);
+        for (long st = 0; st < Vc; ++st)
+          for (int s1 = 0; s1 < 2; ++s1)
+            for (int s2 = 0; s2 < 2; ++s2)
+              for (int c1 = 0; c1 < nb; ++c1)
+                for (int c2 = 0; c2 < nb; ++c2)
+                  flat[(st * N + s1 * nb + c1) * N + s2 * nb + c2] =
+                      Y[(((st * 2 + s1) * 2 + s2) * nb + c1) * nb + c2];
+        std::vector<cplx> ref(A.begin() + (long)p * Vc * N * N, A.begin() + (long)(p + 1) * Vc * N * N);
+        worst = std::max(worst, rel_dev(ref, flat));
+      }
+      ok &= report("two-spin Y_[p] vs Upstream A[p], all points", worst, 1e-14);
+
+      // (13) the operators on the same coarse fields
+      DevField y1(Vc, 1, N), y2(Vc, 1, N);
+      TwoSpinCMat.M(c.f, y1.f);
+      Dc.M(c.f, y2.f);
+      ok &= report("two-spin M vs Upstream M", rel_dev(y2.get(), y1.get()), 1e-14);
+      TwoSpinCMat.Mdag(c.f, y1.f);
+      Dc.Mdag(c.f, y2.f);
+      ok &= report("two-spin Mdag vs Upstream Mdag", rel_dev(y2.get(), y1.get()), 1e-14);
+      DevField e1(Vc / 2, 1, N), e2(Vc / 2, 1, N), o1(Vc / 2, 1, N);
+      he.f.checkerboard = 0;
+      TwoSpinCMat.Meooe(he.f, o1.f);  // even -> odd
+      Dc.Meooe(he.f, t1.f, 0);
+      ok &= report("two-spin Meooe (Even in) vs Upstream", rel_dev(t1.get(), o1.get()), 1e-14);
+      if (o1.f.checkerboard != 1) ok &= report("two-spin Meooe sets the output checkerboard", 1.0, 0.5);
+      TwoSpinCMat.Mooee(he.f, e1.f);
+      TwoSpinCMat.MooeeInv(e1.f, e2.f);
+      ok &= report("two-spin (1 - MooeeInv Mooee) v_e", rel_dev(he.get(), e2.get()), 1e-13);
+
+      // (14) Create(MGBasisVectors): copy in and orthogonalise (two passes)
+      gmg::Rework::Aggregation<Policy> Created(cdims, fdims);
+      const double err = Created.Create(reinterpret_cast<const double*>(h.data()), false);
+      ok &= report("two-spin Create: CheckOrthogonal", err, 1e-13);
     }
   } catch (const gmg::Error& e) {
     std::printf("gmg error %d: %s\n", (int)e.status, e.what());

@@ -142,9 +142,16 @@ def c3(T, hbm):
                "frac_hbm": v[2] / v[0] / 1e9 / hbm} for k, v in res.items()}
     for k, e in errs.items():
         out[k]["rel_err_vs_fp64"] = e
+    # orthonormalisation: algorithmic bytes = basis read + written once (FP64),
+    # flops = 8 K N^2 Vc (the Gram-Schmidt inner products and updates)
+    ob = 2 * N * Vf * 12 * 16
+    of = 8.0 * 3072 * N * N * Vc
+    ortho = {"ms": t_ortho * 1e3, "max_err": err, "algorithmic_bytes": ob, "gbs": ob / t_ortho / 1e9,
+             "frac_hbm": ob / t_ortho / 1e9 / hbm, "algorithmic_flops": of, "tflops_fp64": of / t_ortho / 1e12,
+             "traffic_model_bytes": 3 * N * Vf * 12 * 16,
+             "note": "one pass: Gram + Cholesky kernel (basis read), forward-substitution kernel (read + write)"}
     line("C3 block project / promote (32^4, nbasis 32, 32 RHS, 4^4 blocks)", results=out,
-         orthonormalise_ms=t_ortho * 1e3, orthonormalise_max_err=err, algorithmic_flops=flops,
-         algorithmic_bytes_f64=b64)
+         orthonormalise=ortho, algorithmic_flops=flops, algorithmic_bytes_f64=b64)
 
 
 def wilson_and_c4(T, hbm):
@@ -217,12 +224,14 @@ def wilson_and_c4(T, hbm):
          note="FP64; backward Mdir + face-site projections per batch of basis vectors; seconds: second call")
 
 
-def c5_measure(nrhs=24, plain_rhs=2,
+def c5_measure(nrhs=24, plain_rhs=24,
                forms=("mixed_bf16_mrhs", "mixed_bf16_mrhs_graph", "mixed_f32_mrhs", "plain_f64_single_rhs"), L=32):
     """3-level K-cycle MG-preconditioned FGMRES on 32^4 Wilson-clover (m=-0.35, csw 1, eps 0.3,
     antiperiodic t): nbasis 24 on 4^4 blocks, nbasis 32 on 2^4 blocks, MR(8) smoothing;
     `nrhs` Gaussian RHS to a true relative residual of 1e-10.  The plain FP64 single-RHS
-    form is timed on `plain_rhs` RHS, one at a time, and scaled to `nrhs`.  The graph form
+    form is timed on `plain_rhs` RHS, one at a time (scaled to `nrhs` when fewer).
+    `outer_iterations_per_rhs` lists, per RHS, the outer FGMRES iterations after which it
+    left the active batch (its true residual below the tolerance).  The graph form
     replays the K-cycle as a captured CUDA graph; its first solve also captures the graph
     (after one host-driven cycle per batch size) and is reported separately, the timed one
     is the second solve on the same handle."""
@@ -269,11 +278,11 @@ def c5_measure(nrhs=24, plain_rhs=2,
             w.M(x, r)
             true = (torch.linalg.vector_norm(b - r, dim=(0, 2)) / torch.linalg.vector_norm(b, dim=(0, 2))).max().item()
             worst = max(worst, true)
-            iters.append(it)
+            iters.extend(int(v) for v in mg.solve_stats(b.shape[1])[0])
             del b, x, r
         per_rhs = t_solve / n_solve
         out[form] = {"setup_s": t_setup, "solve_s_measured": t_solve, "rhs_measured": n_solve,
-                     "solve_s_for_all_rhs": per_rhs * nrhs, "outer_iterations": iters,
+                     "solve_s_for_all_rhs": per_rhs * nrhs, "outer_iterations_per_rhs": iters,
                      "max_true_relres": worst}
         if graph:
             out[form]["first_solve_s"] = t_first
@@ -287,10 +296,10 @@ def c5_measure(nrhs=24, plain_rhs=2,
     return out
 
 
-def c5(nrhs=24, plain_rhs=2):
+def c5(nrhs=24, plain_rhs=24):
     out = c5_measure(nrhs, plain_rhs)
     line("C5 3-level K-cycle MG solve, 32^4 Wilson-clover, 24 RHS to 1e-10", results=out,
-         note=f"plain FP64 single-RHS form timed on {plain_rhs} RHS and scaled to {nrhs}; "
+         note=f"plain FP64 single-RHS form timed on {plain_rhs} RHS one at a time; "
               "setup (null vectors, orthonormalisation, CoarsenOperator) not included in solve_s")
 
 
@@ -320,6 +329,17 @@ def profile_rows(rows):
             ag.PromoteFromSubspace(c, f, compute="bf16")
         torch.cuda.synchronize()
         line("p_c3 tensor-core project / promote 16^4, nbasis 32, 32 RHS", ok=True)
+    if "p_ortho" in rows:
+        # block orthonormalisation 16^4, nbasis 32 on 4^4 blocks (basis 403 MB):
+        # one pass of the Gram + Cholesky kernel and the forward substitution
+        B = inputs.torch_gaussian((N, Vf, 12), 617)
+        ag = gmg.Aggregation(fd, cd, 12, N)
+        ag.set_basis(B)
+        del B
+        ag.Orthogonalise(passes=1)
+        ag.Orthogonalise(passes=1)
+        torch.cuda.synchronize()
+        line("p_ortho orthonormalise 16^4, nbasis 32, 4^4 blocks", ok=True, max_err=ag.CheckOrthogonal())
     if "p_w" in rows:
         # the two fine-operator forms of the C5 solve at 24 RHS: M with the fused
         # MR products in FP32 (smoother) and M in FP64 (outer FGMRES); the first

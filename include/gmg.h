@@ -385,6 +385,13 @@ gmg_status gmg_mg_refine(gmg_mg* h, gmg_stream s);
    outer restart.  Synchronises; GMG_ERR_NOT_CONVERGED if maxiter is reached. */
 gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double* x, double tol, int maxiter, int* iters,
                         double* max_relres, gmg_stream s);
+/* Per-RHS outcome of the last gmg_mg_solve on this handle (nrhs must be that
+   solve's): iters[r], the outer iteration count after which RHS r left the
+   active batch (its true relative residual at or below tol; the last count
+   reached if it never did), and relres[r], that true relative residual.  No
+   counterpart: the reference solves one RHS per solver call and times it
+   (Test_wilsonclover_mg.cc:140-151). */
+gmg_status gmg_mg_solve_stats(gmg_mg* h, int nrhs, int* iters, double* relres);
 /* Captured K-cycle graphs of this handle (params.graph): how many (one per
    active-batch size met so far) and whether a capture failed, in which case
    the solver kept the host-driven cycle.  No counterpart in the reference. */
@@ -407,6 +414,33 @@ gmg_status gmg_layout_links(int64_t V, int nbasis, int ncs, const double* in, do
    convertLayout. */
 gmg_status gmg_layout_vectors(int64_t rows, int nbasis, int ncs, const double* in, double* out,
                               int inverse, gmg_stream s);
+
+/* ------------------------------------------------------------------------ */
+/* Two-spin (Rework) forms of the subspace and of the links                  */
+/* (CoarseningPolicyRework.h:56-109, AggregationRework.h:75-146,             */
+/* CoarsenedMatrixRework.h:60-101).  The Rework classes keep                 */
+/* Nc_c = nbasis / ncoarse_spins basis vectors; coarse component (s, c) is   */
+/* the projection on the part of vector c on the s-th of ncoarse_spins equal */
+/* slices of the fine site dof (the two chiralities of a Wilson spinor, the  */
+/* G5C halves of a coarse vector).  This library stores that as the doubled  */
+/* basis with flat index n = s * Nc_c + c, so coarse vectors are the same    */
+/* memory in both forms; subspace and links are converted by these entries.  */
+/* ------------------------------------------------------------------------ */
+/* subspace_[c] = vecs[c] (Rework::Aggregation::Create's copy, :127-146):
+   vecs [Nc_c][Vf][dof] complex128; basis vector s * Nc_c + c becomes the
+   part of vecs[c] on dof slice s (zero elsewhere). */
+gmg_status gmg_agg_set_subspace_spins(gmg_agg* h, int ncoarse_spins, const double* vecs, int on_device,
+                                      gmg_stream s);
+/* Rework::Aggregation::Subspace() (:75-76): vecs[c] = sum_s basis[s * Nc_c + c]. */
+gmg_status gmg_agg_get_subspace_spins(gmg_agg* h, int ncoarse_spins, double* vecs, int on_device, gmg_stream s);
+/* Rework::CoarsenedMatrix::Y_[point] (:70): links [V][Ns_c][Ns_c][Nc_c][Nc_c]
+   complex128, Y(s1, s2)(c1, c2) = A_point[s1 Nc_c + c1][s2 Nc_c + c2]
+   (convertLayout, Layout_converters.h:33-90). */
+gmg_status gmg_coarse_get_links_spins(gmg_coarse* h, int ncoarse_spins, int point, double* links, int on_device,
+                                      gmg_stream s);
+/* All nine Y_[p] in that form, [9][V][Ns_c][Ns_c][Nc_c][Nc_c] (as gmg_coarse_set_links). */
+gmg_status gmg_coarse_set_links_spins(gmg_coarse* h, int ncoarse_spins, const double* links, int on_device,
+                                      gmg_stream s);
 
 /* ------------------------------------------------------------------------ */
 /* Live kernel timing (replaces the reference's Profiler stopwatches,        */

@@ -53,6 +53,7 @@ struct Field {
   int nrhs = 1;
   int dof = 0;
   gmg_prec prec = GMG_F64;
+  int checkerboard = -1;  // half fields: the parity of their sites (0 Even, 1 Odd), as Grid's Checkerboard()
 };
 
 // Grid's pickCheckerboard / setCheckerboard on device fields: full (V sites)
@@ -241,6 +242,7 @@ template <class Matrix>
 class MdagMLinearOperator : public LinearOperatorBase {
  public:
   explicit MdagMLinearOperator(Matrix& m) : m_(m) {}
+  Matrix& matrix() { return m_; }
   void Op(const Field& in, Field& out) override { m_.M(in, out); }
   void AdjOp(const Field& in, Field& out) override { m_.Mdag(in, out); }
   void OpDiag(const Field& in, Field& out) override { m_.Mdiag(in, out); }

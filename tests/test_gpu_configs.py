@@ -23,7 +23,9 @@ Cases:
     configuration's second level) on 8^4 -> 4^4 -> 2^4;
   - the construction in several batches of basis vectors (forced smaller than
     the basis, uneven last batch), for the Wilson-clover and the coarse fine
-    operator.
+    operator;
+  - the two-spin (Rework) subspace and link forms against the Upstream ones,
+    on a Wilson-clover and on a coarse fine level.
 """
 import numpy as np
 import pytest
@@ -156,3 +158,48 @@ def test_coarsen_in_forced_batches(batch):
     cc.CoarsenOperator(ag2, fine)
     _check_links(orc.coarsen_coarse(c1, (2, 2, 2, 2), B2, A1, variant=0), cc.get_links(),
                  f"coarse-of-coarse, batches of {batch}")
+
+
+@pytest.mark.parametrize("level", ["fine", "coarse"])
+def test_two_spin_surface_matches_upstream(level):
+    # The Rework (two-spin) forms through the C ABI, as
+    # src/Benchmark_create_coarse_operator.cc:355-467 checks them: the Upstream
+    # subspace with its chiral doubling undone goes into the two-spin subspace
+    # (and comes back unchanged), the coarse operator built from it has
+    # Y_[p] = convertLayout(A[p]) for every point, and the links set in the
+    # two-spin form read back in the flat one
+    if level == "fine":
+        fd, cd, dof, nvec = (8, 8, 8, 8), (2, 2, 2, 2), 12, 6
+    else:
+        fd, cd, dof, nvec = (4, 4, 4, 4), (2, 2, 2, 2), 8, 5
+    V = int(np.prod(fd))
+    h = inputs.gaussian_field((nvec, V, dof), inputs.rng(stream=185))
+    up = orc.block_orthonormalise(fd, cd, orc.chiral_double(h, 0.5), passes=1)
+    undone = orc.undo_chiral_double(up)
+    ag2 = gmg.Aggregation(fd, cd, dof, 2 * nvec)
+    ag2.set_subspace_spins(undone, 2)
+    assert np.array_equal(ag2.get_basis(), up)  # the chiral halves have disjoint supports: exact
+    assert np.array_equal(ag2.get_subspace_spins(2), undone)
+    if level == "fine":
+        U = inputs.hot_gauge(fd, inputs.rng(stream=186))
+        w = gmg.WilsonClover(fd, -0.1, 1.0, antiperiodic=1)
+        w.set_gauge(U)
+        cm = gmg.CoarsenedMatrix(cd, 2 * nvec)
+        cm.CoarsenOperator(ag2, w)
+        ref = orc.coarsen_wilson(fd, cd, up, U, orc.clover_build(fd, U, 1.0), -0.1, 1, 0, variant=0)
+    else:
+        fine = gmg.CoarsenedMatrix(fd, dof)
+        A1 = inputs.random_links(fd, dof, inputs.rng(stream=187))
+        fine.set_links(A1)
+        cm = gmg.CoarsenedMatrix(cd, 2 * nvec)
+        cm.CoarsenOperator(ag2, fine)
+        ref = orc.coarsen_coarse(fd, cd, up, A1, variant=0)
+    got = cm.get_links()
+    _check_links(ref, got, f"two-spin subspace, {level} level")
+    Y = np.stack([cm.get_links_spins(p, 2) for p in range(9)])
+    for p in range(9):
+        want = orc.layout_link_flat_to_spin(got[p], 2).reshape(Y[p].shape)
+        assert np.array_equal(want, Y[p])
+    cm2 = gmg.CoarsenedMatrix(cd, 2 * nvec)
+    cm2.set_links_spins(Y, 2)
+    assert np.array_equal(cm2.get_links(), got)

@@ -231,16 +231,18 @@ def test_orthonormalise_sizes_match_mgs(fd, cd, dof, N):
 
 
 def test_orthonormalise_shift_only_where_needed():
-    # one block of 16 holds nearly dependent vectors (plain Cholesky QR breaks
-    # down there and the shifted factorisation plus two extra passes run for it
-    # alone); the other blocks must come out as the plain passes leave them
+    # one block of 16 holds nearly dependent vectors, v_j = v_0 + 1e-9 noise
+    # (the Gram matrix's condition number ~1e18 is beyond FP64, so plain
+    # Cholesky QR breaks down there and the shifted factorisation plus two
+    # extra plain passes run for that block alone); the other blocks must come
+    # out as the plain pass leaves them
     fd, cd, N = (8, 8, 8, 8), (2, 2, 2, 2), 24
     V = int(np.prod(fd))
     h = inputs.gaussian_field((N // 2, V, 12), inputs.rng(stream=195))
     B0 = orc.chiral_double(h, 0.5)
     lut = gmg.lut_build(fd, cd)[0]
     sites = lut[5]  # block 5
-    noise = 1e-7 * inputs.gaussian_field((N, len(sites), 12), inputs.rng(stream=196))
+    noise = 1e-9 * inputs.gaussian_field((N, len(sites), 12), inputs.rng(stream=196))
     B0[:, sites] = B0[:1, sites] + noise
     B0[N // 2:, sites, :6] = 0.0  # keep the chiral structure of the doubled basis
     B0[:N // 2, sites, 6:] = 0.0
