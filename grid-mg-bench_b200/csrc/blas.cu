@@ -19,6 +19,27 @@ template <> struct C2<float> { typedef float2 t; };
 
 static int grid1(int64_t n) { return (int)std::min<int64_t>(std::max<int64_t>((n + 255) / 256, 1), 148 * 16); }
 
+// The RHS index of element e of a [V][R][dof] field along a grid-stride loop,
+// without a 64-bit division per element: q = e mod (R dof) advances by the
+// stride modulo R dof, and r = q / dof is a multiply-high by ceil(2^32 / dof)
+// (exact for q < 2^32 / dof, far above R dof here).
+struct RhsWalk {
+  int64_t e;
+  uint32_t q, rd, dq, m;
+  __device__ __forceinline__ RhsWalk(int64_t e0, int64_t stride, int R, int dof)
+      : e(e0), rd((uint32_t)R * (uint32_t)dof) {
+    q = (uint32_t)(e0 % rd);
+    dq = (uint32_t)(stride % rd);
+    m = 0xFFFFFFFFu / (uint32_t)dof + 1u;
+  }
+  __device__ __forceinline__ int r() const { return (int)__umulhi(q, m); }
+  __device__ __forceinline__ void next(int64_t stride) {
+    e += stride;
+    q += dq;
+    if (q >= rd) q -= rd;
+  }
+};
+
 // out[(j0+j)*R + r] += sum_s <X_{j0+j}(s, r), Y(s, r)> for j < min(JB, nx - j0)
 // (X_j = X + j*xstride).  Grid (gx, R): blockIdx.y is the RHS, threads walk the
 // sites, then a warp-shuffle + shared-memory reduction and one FP64 atomic per
@@ -74,8 +95,10 @@ __global__ void multiaxpy_kernel(const double2* __restrict__ a, const typename C
                                  int64_t xstride, int nx, typename C2<T>::t* __restrict__ Y, int64_t V, int R,
                                  int dof, double sgn) {
   const int64_t n = V * R * dof;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int r = (int)((e / dof) % R);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (RhsWalk w(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride, R, dof); w.e < n; w.next(stride)) {
+    const int64_t e = w.e;
+    const int r = w.r();
     double yr = Y[e].x, yi = Y[e].y;
     for (int j = 0; j < nx; ++j) {
       double2 c = a[j * R + r];
@@ -97,8 +120,10 @@ __global__ void axpby_kernel(const double2* __restrict__ a, const typename C2<T>
                              const double2* __restrict__ b, typename C2<T>::t* __restrict__ Y, int64_t V, int R,
                              int dof) {
   const int64_t n = V * R * dof;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int r = (int)((e / dof) % R);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (RhsWalk w(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride, R, dof); w.e < n; w.next(stride)) {
+    const int64_t e = w.e;
+    const int r = w.r();
     const double2 ca = a[r], cb = b[r];
     const typename C2<T>::t x = X[e], y = Y[e];
     const double re = ca.x * x.x - ca.y * x.y + cb.x * y.x - cb.y * y.y;
@@ -581,8 +606,10 @@ template <class T>
 __global__ void scale_inv_norm_kernel(const double2* __restrict__ n, const typename C2<T>::t* __restrict__ X,
                                       typename C2<T>::t* __restrict__ Y, int64_t V, int R, int dof) {
   const int64_t tot = V * R * dof;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-    const int r = (int)((e / dof) % R);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (RhsWalk w(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride, R, dof); w.e < tot; w.next(stride)) {
+    const int64_t e = w.e;
+    const int r = w.r();
     const double nn = n[r].x;
     const double sc = nn > 0.0 ? rsqrt(nn) : 0.0;
     Y[e].x = (T)(sc * X[e].x);
@@ -597,8 +624,10 @@ __global__ void mr_update_kernel(const double2* __restrict__ d1, const double2* 
                                  typename C2<T>::t* __restrict__ x, typename C2<T>::t* __restrict__ r,
                                  const typename C2<T>::t* __restrict__ Ar, int64_t V, int R, int dof, bool update_r) {
   const int64_t tot = V * R * dof;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)((e / dof) % R);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (RhsWalk w(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride, R, dof); w.e < tot; w.next(stride)) {
+    const int64_t e = w.e;
+    const int k = w.r();
     const double den = d2[k].x;
     const double ar = den > 0.0 ? d1[k].x / den : 0.0, ai = den > 0.0 ? d1[k].y / den : 0.0;
     const double rr = r[e].x, ri = r[e].y;
@@ -885,8 +914,10 @@ __global__ void bicg_p_kernel(typename C2<T>::t* __restrict__ p, const typename 
                               const typename C2<T>::t* __restrict__ v, const double2* __restrict__ sc, int64_t V, int R,
                               int dof) {
   const int64_t n = V * R * dof;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)((e / dof) % R);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (RhsWalk w(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride, R, dof); w.e < n; w.next(stride)) {
+    const int64_t e = w.e;
+    const int k = w.r();
     const double2 om = sc[2 * R + k], be = sc[3 * R + k];
     const double2 pv = make_double2(p[e].x, p[e].y), vv = make_double2(v[e].x, v[e].y);
     const double2 ov = zmul2(om, vv);
@@ -901,8 +932,10 @@ __global__ void bicg_s_kernel(typename C2<T>::t* __restrict__ s_, const typename
                               const typename C2<T>::t* __restrict__ v, const double2* __restrict__ sc, int64_t V, int R,
                               int dof) {
   const int64_t n = V * R * dof;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)((e / dof) % R);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (RhsWalk w(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride, R, dof); w.e < n; w.next(stride)) {
+    const int64_t e = w.e;
+    const int k = w.r();
     const double2 av = zmul2(sc[R + k], make_double2(v[e].x, v[e].y));
     s_[e].x = (T)(r[e].x - av.x);
     s_[e].y = (T)(r[e].y - av.y);
@@ -915,8 +948,10 @@ __global__ void bicg_xr_kernel(typename C2<T>::t* __restrict__ x, typename C2<T>
                                const typename C2<T>::t* __restrict__ t, const double2* __restrict__ sc, int64_t V, int R,
                                int dof) {
   const int64_t n = V * R * dof;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)((e / dof) % R);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (RhsWalk w(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride, R, dof); w.e < n; w.next(stride)) {
+    const int64_t e = w.e;
+    const int k = w.r();
     const double2 al = sc[R + k], om = sc[2 * R + k];
     const double2 sv = make_double2(s_[e].x, s_[e].y);
     const double2 ap = zmul2(al, make_double2(p[e].x, p[e].y)), os = zmul2(om, sv);

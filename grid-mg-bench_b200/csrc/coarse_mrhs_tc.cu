@@ -313,6 +313,10 @@ __global__ void __launch_bounds__(kThreads, CTAS) coarse_mrhs_tc_kernel(const Pa
     int* my_lsite = lsite_s + pid * 32;
     int64_t last = -1;
     bool stop = false;
+    // the first `stages` sequence numbers fill stages that have never been used:
+    // their link tiles (which do not depend on the pack) are requested before
+    // the wait on the pack grid, and only their neighbour tiles after it
+    const int64_t npre = min((int64_t)P.stages, (int64_t)nsites * ngroups);
     for (int i0 = 0; i0 < nsites && !stop; i0 += 32) {
       const int cnt = min(32, nsites - i0);
       __syncwarp();
@@ -322,10 +326,24 @@ __global__ void __launch_bounds__(kThreads, CTAS) coarse_mrhs_tc_kernel(const Pa
         for (int p = 0; p < 9; ++p) my_nbr[lane * 9 + p] = __ldg(&P.nbr[(size_t)p * P.V + site]);
         my_lsite[lane] = P.site_map ? __ldg(&P.site_map[site]) : site;
       }
-      // launched as a programmatic dependent of the vector pack: everything
-      // above overlaps the pack's tail; the packed vectors are read only
-      // after the pack grid has completed (a no-op for a plain launch)
-      if (i0 == 0) asm volatile("griddepcontrol.wait;" ::: "memory");
+      if (i0 == 0) {
+        __syncwarp();
+        if (lane == 0) {
+          // npre <= stages <= 32 and ngroups >= 1, so these sites are in this first table
+          for (int64_t n = pid; n < npre; n += 2) {
+            const int j = (int)(n / ngroups), g = (int)(n % ngroups);
+            const int stage = (int)n;
+            const int pf = P.p0 + g * pps;
+            mbar_expect_tx(&full[stage], stage_bytes);
+            bulk_g2s(stage_base + (size_t)stage * stage_bytes,
+                     P.links + ((size_t)my_lsite[j] * 9 + pf) * (link_bytes / 2), pps * link_bytes, &full[stage]);
+          }
+        }
+        // launched as a programmatic dependent of the vector pack: everything
+        // above overlaps the pack's tail; the packed vectors are read only
+        // after the pack grid has completed (a no-op for a plain launch)
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+      }
       __syncwarp();
       if (lane == 0) {
         for (int j = 0; j < cnt && !stop; ++j) {
@@ -335,16 +353,18 @@ __global__ void __launch_bounds__(kThreads, CTAS) coarse_mrhs_tc_kernel(const Pa
             if ((int)(n & 1) != pid) continue;
             const int stage = (int)(n % P.stages);
             const uint32_t phase = (uint32_t)((n / P.stages) & 1);
-            if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) {
-              atomicCAS(P.err, 0, ERR_TIMEOUT_PRODUCER);
-              *abort_flag = 1;
-              stop = true;
-              break;
-            }
             unsigned char* st = stage_base + (size_t)stage * stage_bytes;
             const int pf = P.p0 + g * pps;
-            mbar_expect_tx(&full[stage], stage_bytes);
-            bulk_g2s(st, P.links + ((size_t)lsite * 9 + pf) * (link_bytes / 2), pps * link_bytes, &full[stage]);
+            if (n >= npre) {
+              if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) {
+                atomicCAS(P.err, 0, ERR_TIMEOUT_PRODUCER);
+                *abort_flag = 1;
+                stop = true;
+                break;
+              }
+              mbar_expect_tx(&full[stage], stage_bytes);
+              bulk_g2s(st, P.links + ((size_t)lsite * 9 + pf) * (link_bytes / 2), pps * link_bytes, &full[stage]);
+            }
             for (int pp = 0; pp < pps; ++pp) {
               const int nb = my_nbr[j * 9 + pf + pp];
               bulk_g2s(st + pps * link_bytes + pp * vec_bytes, P.packed + (size_t)nb * (vec_bytes / 2), vec_bytes,
@@ -525,27 +545,40 @@ __global__ void pack_links_kernel(const double2* __restrict__ A, uint4* __restri
 }
 
 // vectors (FP32 [V][nrhs][N]) -> [V][Kc][2Rp][8] halves, G5C applied on input.
-// One thread per (site, K-chunk, rhs), rhs fastest: it reads the 8 complex
-// values of its chunk (64 contiguous bytes) once and writes the real-part row
-// r and the imaginary-part row Rp + r, so reads and writes are both coalesced.
-__global__ void pack_vec_kernel(const float2* __restrict__ in, uint4* __restrict__ dst, const int32_t* __restrict__ active,
-                                int V, int N, int nrhs, int R, int Rp, int Kc, int kind, int g5,
-                                int aligned16) {
+// One thread per (site, K-chunk, rhs), K chunk fastest: the Kc threads of one
+// (site, RHS) read its row of N complex numbers contiguously (a warp reads 2 KB
+// in one run) and each writes the real-part row r and the imaginary-part row
+// Rp + r of its chunk, so a warp's writes are whole 128-byte runs.  Indices are
+// 32-bit with the chunk count a compile-time constant: one 32-bit division per
+// item (64-bit divisions, expanded in software, had made the kernel
+// instruction-bound).
+// vectors (FP32 [V][nrhs][N]) -> [V][Kc][2Rp][8] halves, G5C applied on input.
+// One thread per (site, K-chunk, rhs), K chunk fastest: the Kc threads of one
+// (site, RHS) read its row of N complex numbers contiguously (a warp reads 2 KB
+// in one run) and each writes the real-part row r and the imaginary-part row
+// Rp + r of its chunk, so a warp's writes are whole 128-byte runs.  Indices are
+// 32-bit with the chunk count a compile-time constant: one 32-bit division per
+// item (64-bit divisions, expanded in software, had made the kernel
+// instruction-bound).  Two items per thread, both loaded before either is
+// stored, measured slower (14.3 against 12.4 us on 8^4 x 32 x 32).
+template <int KC>
+__global__ void __launch_bounds__(256) pack_vec_kernel(const float2* __restrict__ in, uint4* __restrict__ dst,
+                                                       const int32_t* __restrict__ active, int V, int N, int nrhs,
+                                                       int R, int Rp, int kind, int g5, int aligned16) {
   // the stencil launched after this kernel may start its prologue now (it
   // waits for this grid's completion before reading the packed vectors)
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  const int64_t total = (int64_t)V * Kc * Rp;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    // K chunk fastest: the Kc threads of one (site, RHS) read its row of N
-    // complex numbers contiguously; a warp's writes are Kc runs of 16 B x RHS
-    const int kc = (int)(e % Kc);
-    const int r = (int)((e / Kc) % Rp);
-    const int64_t s = e / ((int64_t)Rp * Kc);
+  const uint32_t per_site = (uint32_t)KC * Rp;
+  const uint32_t total = (uint32_t)V * per_site;
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const uint32_t s = e / per_site;
+    const uint32_t rem = e - s * per_site;
+    const int kc = (int)(rem % KC);
+    const int r = (int)(rem / KC);
     uint32_t pr[4], pi[4];
     if (r < R) {
-      const int slot = active ? active[r] : r;
-      const float2* src = in + ((int64_t)s * nrhs + slot) * N + kc * 8;
+      const int slot = active ? __ldg(&active[r]) : r;
+      const float2* src = in + ((size_t)s * nrhs + slot) * N + kc * 8;
       float2 x[8];
       if (aligned16 && (N & 1) == 0 && kc * 8 + 8 <= N) {
         // `in` is 16-byte aligned (checked on the host), N and 8*kc are even, and the
@@ -582,7 +615,7 @@ __global__ void pack_vec_kernel(const float2* __restrict__ in, uint4* __restrict
 #pragma unroll
       for (int j = 0; j < 4; ++j) pr[j] = pi[j] = 0;
     }
-    uint4* row = dst + ((int64_t)s * Kc + kc) * 2 * Rp;
+    uint4* row = dst + ((size_t)s * KC + kc) * 2 * Rp;
     row[r] = make_uint4(pr[0], pr[1], pr[2], pr[3]);
     row[Rp + r] = make_uint4(pi[0], pi[1], pi[2], pi[3]);
   }
@@ -594,12 +627,22 @@ inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 // beat this one on the 8^4 x 32 x 32 apply, 15.5 us: one thread per 16 input
 // bytes with 4-byte stores, 23 us; two chunks per thread with all eight loads
 // issued first, 15.7 us.)
-inline void launch_pack(const float* in, uint4* packed, const int32_t* active, int V, int N, int nrhs, int R,
-                        int Rp, int Kc, int kind, bool g5, cudaStream_t s) {
+inline gmg_status launch_pack(const float* in, uint4* packed, const int32_t* active, int V, int N, int nrhs,
+                              int R, int Rp, int Kc, int kind, bool g5, cudaStream_t s) {
   const int64_t rows = (int64_t)V * Kc * Rp;
-  pack_vec_kernel<<<(int)std::min<int64_t>((rows + 255) / 256, 148 * 64), 256, 0, s>>>(
-      reinterpret_cast<const float2*>(in), packed, active, V, N, nrhs, R, Rp, Kc, kind, g5 ? 1 : 0,
-      (reinterpret_cast<uintptr_t>(in) & 15) == 0 ? 1 : 0);
+  GMG_CHECK(rows < ((int64_t)1 << 31), GMG_ERR_UNSUPPORTED,
+            "tensor-core coarse stencil: coarse volume x packed RHS rows exceeds 2^31");
+  const int grid = (int)std::min<int64_t>((rows + 255) / 256, 148 * 64);
+  const float2* src = reinterpret_cast<const float2*>(in);
+  const int a16 = (reinterpret_cast<uintptr_t>(in) & 15) == 0 ? 1 : 0;
+  switch (Kc) {  // Kc = ceil16(N) / 8: 2, 4, 6 or 8 for N <= 64
+    case 2: pack_vec_kernel<2><<<grid, 256, 0, s>>>(src, packed, active, V, N, nrhs, R, Rp, kind, g5, a16); break;
+    case 4: pack_vec_kernel<4><<<grid, 256, 0, s>>>(src, packed, active, V, N, nrhs, R, Rp, kind, g5, a16); break;
+    case 6: pack_vec_kernel<6><<<grid, 256, 0, s>>>(src, packed, active, V, N, nrhs, R, Rp, kind, g5, a16); break;
+    default: pack_vec_kernel<8><<<grid, 256, 0, s>>>(src, packed, active, V, N, nrhs, R, Rp, kind, g5, a16); break;
+  }
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
 }
 
 }  // namespace tc
@@ -832,8 +875,7 @@ gmg_status coarse_apply_tc(gmg_coarse* h, int p0, int p1, bool g5, int kind, int
   uint4* packed = h->scratch.as<uint4>();
   {
     KernelTimer kt("pack_vec", s);
-    tc::launch_pack(in, packed, active, V, N, nrhs, R, Rp, Kc, kind, g5, s);
-    GMG_CUDA(cudaGetLastError());
+    GMG_TRY(tc::launch_pack(in, packed, active, V, N, nrhs, R, Rp, Kc, kind, g5, s));
   }
   return tc::launch_stencil(h, packed, V, nullptr, h->nbr.as<int32_t>(), p0, p1, g5, kind, nrhs, out, active, R,
                             true, s);
@@ -850,8 +892,7 @@ gmg_status coarse_apply_tc_ex(gmg_coarse* h, int V, int V_in, const int32_t* sit
   const int Kc = tc::round_up(N, 16) / 8;
   GMG_TRY(h->scratch.alloc((size_t)V_in * Kc * 2 * Rp * 16));
   uint4* packed = h->scratch.as<uint4>();
-  tc::launch_pack(in, packed, active, V_in, N, nrhs, R, Rp, Kc, kind, g5, s);
-  GMG_CUDA(cudaGetLastError());
+  GMG_TRY(tc::launch_pack(in, packed, active, V_in, N, nrhs, R, Rp, Kc, kind, g5, s));
   return tc::launch_stencil(h, packed, V, site_map, nbr, p0, p1, g5, kind, nrhs, out, active, R, true, s);
 }
 
@@ -963,8 +1004,7 @@ extern "C" gmg_status gmg_coarse_apply_noalloc(gmg_coarse* h, gmg_op op, int poi
   GMG_TRY(tc::noalloc_scratch(&scratch));
   cudaStream_t s = S(stream);
   uint4* packed = reinterpret_cast<uint4*>(scratch);
-  tc::launch_pack(static_cast<const float*>(in), packed, active, V, N, nrhs, R, Rp, Kc, compute, g5, s);
-  GMG_CUDA(cudaGetLastError());
+  GMG_TRY(tc::launch_pack(static_cast<const float*>(in), packed, active, V, N, nrhs, R, Rp, Kc, compute, g5, s));
   return tc::launch_stencil(h, packed, V, nullptr, h->nbr.as<int32_t>(), p0, p1, g5, compute, nrhs, out, active, R,
                             false, s);
 }

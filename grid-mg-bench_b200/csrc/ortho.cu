@@ -664,8 +664,15 @@ gmg_status agg_orthonormalise(gmg_agg* h, int passes, cudaStream_t s) {
     // passes + 2 rounds: the last two only touch blocks that needed the shift
     for (int pass = 0; pass < passes + 2; ++pass) {
       P.pass = pass;
-      GMG_TRY(launch_gram<false>(P, s));
-      GMG_TRY(launch_factor(P, s));
+      {
+        KernelTimer k1("ortho_gram", s);
+        GMG_TRY(launch_gram<false>(P, s));
+      }
+      {
+        KernelTimer k2("ortho_factor", s);
+        GMG_TRY(launch_factor(P, s));
+      }
+      KernelTimer k3("ortho_solve", s);
       GMG_TRY(solve(P, s));
     }
   }

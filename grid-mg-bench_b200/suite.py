@@ -103,6 +103,15 @@ def c3(T, hbm):
     torch.cuda.empty_cache()
     t_ortho = T.run(lambda: ag.Orthogonalise(passes=1), reps=2, warm=1)
     err = ag.CheckOrthogonal()
+    # per-kernel times of one more pass (events on the stream; the two extra rounds are near-empty)
+    gmg.lib().gmg_profile_enable(1)
+    ag.Orthogonalise(passes=1)
+    torch.cuda.synchronize()
+    gmg.lib().gmg_profile_enable(0)
+    ortho_kernels = {}
+    for kname in ("ortho_gram", "ortho_factor", "ortho_solve"):
+        ms_, n_ = kernel_avg(kname)
+        ortho_kernels[kname] = {"ms_total": (ms_ or 0.0) * n_ * 1e3, "launches": n_}
     f64 = inputs.torch_gaussian((Vf, R, 12), 602)
     c64 = torch.zeros((Vc, R, N), dtype=torch.complex128, device="cuda")
     flops = 8.0 * Vf * 12 * N * R
@@ -148,7 +157,7 @@ def c3(T, hbm):
     of = 8.0 * 3072 * N * N * Vc
     ortho = {"ms": t_ortho * 1e3, "max_err": err, "algorithmic_bytes": ob, "gbs": ob / t_ortho / 1e9,
              "frac_hbm": ob / t_ortho / 1e9 / hbm, "algorithmic_flops": of, "tflops_fp64": of / t_ortho / 1e12,
-             "traffic_model_bytes": 3 * N * Vf * 12 * 16,
+             "traffic_model_bytes": 3 * N * Vf * 12 * 16, "kernels": ortho_kernels,
              "note": "one pass: Gram + Cholesky kernel (basis read), forward-substitution kernel (read + write)"}
     line("C3 block project / promote (32^4, nbasis 32, 32 RHS, 4^4 blocks)", results=out,
          orthonormalise=ortho, algorithmic_flops=flops, algorithmic_bytes_f64=b64)
