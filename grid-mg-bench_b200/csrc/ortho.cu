@@ -22,10 +22,11 @@
 // gets two extra plain passes.
 //
 // Three kernels per pass (nbasis up to 40):
-//   gram_kernel      CTA per block (persistent over blocks): the Gram matrix
-//                    from FP64 register tiles over the lower block triangle, fed
-//                    by a three-stage cp.async pipeline of K-chunks with one
-//                    barrier per chunk; writes the packed lower triangle.
+//   gram_kernel      CTA per block (persistent over blocks): the Gram matrix on
+//                    the FP64 tensor cores (mma m8n8k4 over the lower 8 x 8 tiles
+//                    of the real panel's Gram matrix), fed by a three-stage
+//                    cp.async pipeline of K-chunks with one barrier per chunk;
+//                    writes the packed lower triangle.
 //   factor_kernel    warp per block: the Cholesky factor in shared memory, lane
 //                    i owning row i; the shifted retry re-reads the Gram matrix;
 //                    writes conj(L) and 1 / diag(L) packed (row i: i + 1 entries).
@@ -33,7 +34,11 @@
 //                    substitution against conj(L) in shared memory (every thread
 //                    reads the same entry: a broadcast), the column written back
 //                    in place; the next column batch is copied into shared
-//                    memory (cp.async) while the current one is solved.
+//                    memory (cp.async) while the current one is solved.  (The
+//                    same product as a block-lower-triangular real GEMM on the
+//                    FP64 tensor cores, with T = conj(L)^{-1} formed explicitly,
+//                    measured slower: 3.88 against 3.48 ms at 32^4 x 32, bound by
+//                    the shared-memory reads of T's fragments.)
 // Traffic per pass: the basis read twice and written once (3 x 8 B x 2 x N x K
 // per block) plus the small factors; flops 8 K N (N + 1) / 2 for the Gram
 // matrix (lower triangle) and the same for the substitution.
@@ -52,10 +57,8 @@ namespace ortho {
 constexpr int kThreads = 256;
 constexpr int kKC = 64;         // K values per pipeline stage (at most)
 constexpr int kStages = 3;      // cp.async pipeline depth of the Gram kernel
-constexpr int kMaxKG = 16;      // K-interleaved groups of tile threads
 constexpr int kSolveMax = 40;   // largest nbasis of the three-kernel path
 constexpr int kFactorWarps = 4;  // blocks (one per warp) per factor CTA
-constexpr int kSolveThreads = 128;  // columns per solve chunk (three CTAs per SM at 170 registers)
 
 __device__ __forceinline__ double2 cfma_conj(double2 acc, double2 a, double2 b) {  // acc += conj(a) b
   acc.x = fma(a.x, b.x, acc.x);
@@ -74,28 +77,40 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N_>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N_) : "memory"); }
 
-// Tile geometry of the Gram matrix for nbasis N: NT tiles per side, tile (ti, tj)
-// owning rows ti + NT q and columns tj + NT r (q, r < 4), only ti >= tj (the
-// others are conjugate transposes); KG groups of tile threads take interleaved
-// K entries of a chunk of KC = KG * floor(kKC / KG) entries (equal shares).
-// Staging tiles are [kKC][Np] complex with Np = 4 NT + 1 (the odd row length
-// spreads the transposed 16-byte writes over the banks).
+// Geometry of the Gram kernel for nbasis N.  The block panel is staged as
+// [KC][Np] complex (k-major), which read as doubles is the real 2N x KC panel W
+// with rows 2i = Re v_i, 2i + 1 = Im v_i (rows 2N .. 8 NT - 1 zero).  Its real
+// Gram matrix P = W W^T is formed with FP64 tensor-core MMAs (m8n8k4) over 8 x 8
+// tiles: NT = ceil(N / 4) row tiles, the NT (NT + 1) / 2 lower tiles split over
+// ntw "tile warps" (warp w takes the tile rows w and NT - 1 - w, so every warp
+// has NT + 1 tiles) and K split over kgw groups of them.  Np = 4 mod 8 (16-byte
+// units) puts the 32 lanes' fragment reads of one k-step on distinct bank
+// pairs.  KC (a multiple of 4 kgw) and three stages fit two CTAs per SM.
+constexpr int kMaxNT = 10;  // nbasis <= 40 on this path
 struct Geo {
-  int N, NT, Np, ntiles, KG, KC;
-  size_t stage_bytes, red_bytes, smem;
+  int N, NT, Np, ntw, kgw, KC, ntiles;
+  size_t stage_bytes, pbuf_bytes, smem;
 };
 
 inline Geo geometry(int N) {
   Geo g;
   g.N = N;
   g.NT = (N + 3) / 4;
-  g.Np = 4 * g.NT + 1;
+  g.Np = 4 * g.NT + (g.NT % 2 == 0 ? 4 : 0);
+  g.ntw = (g.NT + 1) / 2;
+  g.kgw = std::max(1, 8 / g.ntw);
   g.ntiles = g.NT * (g.NT + 1) / 2;
-  g.KG = std::max(1, std::min(kMaxKG, kThreads / g.ntiles));
-  g.KC = g.KG * std::max(1, kKC / g.KG);
-  g.stage_bytes = sizeof(double2) * kStages * kKC * (size_t)g.Np;
-  g.red_bytes = sizeof(double2) * 16 * (size_t)g.KG * g.ntiles;
-  g.smem = std::max(g.stage_bytes, g.red_bytes);
+  g.KC = 32;
+  for (int kc : {64, 48, 32}) {
+    if ((kc / 4) % g.kgw) continue;
+    if (sizeof(double2) * kStages * (size_t)kc * g.Np <= 112 * 1024) {
+      g.KC = kc;
+      break;
+    }
+  }
+  g.stage_bytes = sizeof(double2) * kStages * (size_t)g.KC * g.Np;
+  g.pbuf_bytes = sizeof(double) * 64 * (size_t)g.kgw * g.ntiles;
+  g.smem = std::max(g.stage_bytes, g.pbuf_bytes);
   return g;
 }
 
@@ -106,48 +121,94 @@ struct Params {
   int* need;                   // [Vc]: 1 once a block needed the shifted factorisation
   int* status;                 // 1 when a shifted factorisation failed too
   unsigned long long* maxerr;  // check mode: max |G - 1| (as the bits of a non-negative double)
-  int Vc, N, K, NT, Np, ntiles, KG, KC;
+  int Vc, N, K, Np, ntw, kgw, KC, ntiles;
   int pass, passes;
 };
 
 __device__ __forceinline__ bool block_active(const Params& P, int c) { return P.pass < P.passes || P.need[c] != 0; }
 
+// D (8 x 8, two elements per lane) += A (8 x 4) B (4 x 8), FP64 tensor cores
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// The k-steps of one chunk for the warp whose tile rows are TW and NT - 1 - TW:
+// per step of 4 k values one fragment load per tile row it needs and one MMA
+// per tile, all indices compile-time.
+template <int NT, int TW>
+__device__ __forceinline__ void gram_steps(double (&acc)[NT + 1][2], const double* fb, int stride_d, int grp, int nk4,
+                                           int kgw) {
+  constexpr int I1 = TW, I2 = NT - 1 - TW;
+  for (int k4 = grp; k4 < nk4; k4 += kgw) {
+    const double* f = fb + 4 * k4 * stride_d;
+    double fr[I2 + 1];
+#pragma unroll
+    for (int X = 0; X <= I2; ++X) fr[X] = f[8 * X];
+#pragma unroll
+    for (int J = 0; J <= I1; ++J) dmma(acc[J], fr[I1], fr[J]);
+    if (I2 != I1) {
+#pragma unroll
+      for (int J = 0; J <= I2; ++J) dmma(acc[I1 + 1 + J], fr[I2], fr[J]);
+    }
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ void gram_steps_tw(int tw, double (&acc)[NT + 1][2], const double* fb, int stride_d, int grp,
+                                              int nk4, int kgw) {
+  switch (tw) {
+    case 0: gram_steps<NT, 0>(acc, fb, stride_d, grp, nk4, kgw); break;
+    case 1: if (NT > 2) gram_steps<NT, (NT > 2 ? 1 : 0)>(acc, fb, stride_d, grp, nk4, kgw); break;
+    case 2: if (NT > 4) gram_steps<NT, (NT > 4 ? 2 : 0)>(acc, fb, stride_d, grp, nk4, kgw); break;
+    case 3: if (NT > 6) gram_steps<NT, (NT > 6 ? 3 : 0)>(acc, fb, stride_d, grp, nk4, kgw); break;
+    default: if (NT > 8) gram_steps<NT, (NT > 8 ? 4 : 0)>(acc, fb, stride_d, grp, nk4, kgw); break;
+  }
+}
+
 // Gram matrices of the blocks (packed lower triangles into P.gram), or in
 // CHECK mode the largest |G - 1| over all blocks into P.maxerr.
-template <bool CHECK>
+template <int NT, bool CHECK>
 __global__ void __launch_bounds__(kThreads, 2) gram_kernel(Params P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* stage = reinterpret_cast<double2*>(smem_raw);  // [kStages][kKC][Np], then the partial tiles
-  const int t = threadIdx.x;
-  const int NT = P.NT, Np = P.Np, N = P.N, K = P.K, KC = P.KC, KG = P.KG;
-  const int tile = t % P.ntiles, grp = t / P.ntiles;
-  const bool active = grp < KG;
-  int ti = 0;
-  while ((ti + 1) * (ti + 2) / 2 <= tile) ++ti;
-  const int tj = tile - ti * (ti + 1) / 2;
+  double2* stage = reinterpret_cast<double2*>(smem_raw);  // [kStages][KC][Np], then the P tiles
+  double* pbuf = reinterpret_cast<double*>(smem_raw);
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int Np = P.Np, N = P.N, K = P.K, KC = P.KC, kgw = P.kgw, ntw = P.ntw;
+  const int stride_d = 2 * Np;  // doubles per staged k row
+  const int tw = w % ntw, grp = w / ntw;
+  const bool active = grp < kgw;
+  const int I1 = tw, I2 = NT - 1 - tw;  // this warp's tile rows (the same when NT is odd and tw is the middle)
   const int nch = (K + KC - 1) / KC;
+  const int stage_elems = kStages * KC * Np;
+  // zero the staging buffers once: rows i >= N and k rows past the end of a
+  // partial last chunk must read as zero
+  for (int e = t; e < stage_elems; e += kThreads) stage[e] = make_double2(0.0, 0.0);
+  __syncthreads();
   double mx = 0.0;
   for (int c = blockIdx.x; c < P.Vc; c += gridDim.x) {
     if (!CHECK && !block_active(P, c)) continue;  // uniform over the CTA
     const double2* Vb = P.basis + (int64_t)c * N * K;
     auto issue = [&](int ch) {
       if (ch < nch) {
-        double2* buf = stage + (ch % kStages) * kKC * Np;
+        double2* buf = stage + (ch % kStages) * KC * Np;
         const int k0 = ch * KC;
         const int kc = min(KC, K - k0);
         for (int e = t; e < N * KC; e += kThreads) {
           const int i = e / KC, kk = e - i * KC;
           if (kk < kc) cp_async16(buf + kk * Np + i, Vb + (int64_t)i * K + k0 + kk);
         }
+        // a partial last chunk: the k rows up to the next multiple of 4 read as zero
+        const int kc4 = (kc + 3) & ~3;
+        for (int e = t; e < (kc4 - kc) * Np; e += kThreads) buf[(kc + e / Np) * Np + e % Np] = make_double2(0.0, 0.0);
       }
       cp_async_commit();  // an empty group past the last chunk keeps the group count uniform
     };
-    double2 acc[4][4];
+    double acc[NT + 1][2];
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-      for (int r = 0; r < 4; ++r) acc[q][r] = make_double2(0.0, 0.0);
-    __syncthreads();  // the previous block's reduction no longer reads `stage`
+    for (int q = 0; q <= NT; ++q) acc[q][0] = acc[q][1] = 0.0;
+    __syncthreads();  // the previous block's P tiles are no longer read
 #pragma unroll
     for (int sidx = 0; sidx < kStages - 1; ++sidx) issue(sidx);
     for (int ch = 0; ch < nch; ++ch) {
@@ -155,72 +216,63 @@ __global__ void __launch_bounds__(kThreads, 2) gram_kernel(Params P) {
       __syncthreads();               // everyone's have; chunk ch - 1 is no longer read
       issue(ch + kStages - 1);       // into the buffer chunk ch - 1 used
       if (active) {
-        const double2* buf = stage + (ch % kStages) * kKC * Np;
-        const int kc = min(KC, K - ch * KC);
-#pragma unroll 2
-        for (int kk = grp; kk < kc; kk += KG) {
-          double2 a[4], b[4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) a[q] = buf[kk * Np + ti + NT * q];
-#pragma unroll
-          for (int r = 0; r < 4; ++r) b[r] = buf[kk * Np + tj + NT * r];
-          // conj(a) b in two sweeps over the 16 accumulators, so that the two
-          // dependent FMAs of each component are 32 instructions apart
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              acc[q][r].x = fma(a[q].x, b[r].x, acc[q][r].x);
-              acc[q][r].y = fma(a[q].x, b[r].y, acc[q][r].y);
-            }
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              acc[q][r].x = fma(a[q].y, b[r].y, acc[q][r].x);
-              acc[q][r].y = fma(-a[q].y, b[r].x, acc[q][r].y);
-            }
-        }
+        const double* buf = reinterpret_cast<const double*>(stage + (ch % kStages) * KC * Np);
+        const int nk4 = (min(KC, K - ch * KC) + 3) >> 2;
+        // lane (r, q) = (lane / 4, lane % 4): A / B fragment element W[8 X + r][k + q]
+        const double* fb = buf + (lane & 3) * stride_d + (lane >> 2);
+        gram_steps_tw<NT>(tw, acc, fb, stride_d, grp, nk4, kgw);
       }
     }
     cp_async_wait<0>();
-    __syncthreads();  // all chunks consumed: `stage` takes the partial tiles
+    __syncthreads();  // all chunks consumed: the stage area takes the P tiles
     if (active) {
-      double2* red = stage + ((size_t)grp * P.ntiles + tile) * 16;
+      // tile (I, J) of group grp: element (m, n) at pbuf[((grp * ntiles + I (I + 1) / 2 + J) * 8 + m) * 8 + n];
+      // this lane holds (m, n) = (lane / 4, 2 (lane % 4) + {0, 1}); tile slot q of the accumulators is
+      // (I1, q) for q <= I1, (I2, q - I1 - 1) after
+      const int off = (lane >> 2) * 8 + 2 * (lane & 3);
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) red[q * 4 + r] = acc[q][r];
+      for (int q = 0; q <= NT; ++q) {
+        const int I = q <= I1 ? I1 : I2, J = q <= I1 ? q : q - I1 - 1;
+        if (q <= I1 || (I2 != I1 && J <= I2)) {
+          double* d = pbuf + ((size_t)(grp * P.ntiles + I * (I + 1) / 2 + J) * 64) + off;
+          d[0] = acc[q][0];
+          d[1] = acc[q][1];
+        }
+      }
     }
     __syncthreads();
+    // P(R, R') for R >= R', summed over the K groups
+    auto pel = [&](int R, int R2) {
+      if (R < R2) {
+        const int tmp = R;
+        R = R2;
+        R2 = tmp;
+      }
+      const int I = R >> 3, J = R2 >> 3;
+      const double* src = pbuf + (size_t)(I * (I + 1) / 2 + J) * 64 + (R & 7) * 8 + (R2 & 7);
+      double v = 0.0;
+      for (int g = 0; g < kgw; ++g) v += src[(size_t)g * P.ntiles * 64];
+      return v;
+    };
     double2* Gc = P.gram + (int64_t)c * (N * (N + 1) / 2);
     for (int e = t; e < N * N; e += kThreads) {
       const int i = e / N, j = e - (e / N) * N;
       if (j > i) continue;
-      const int qi = i / NT, ti2 = i - qi * NT, rj = j / NT, tj2 = j - rj * NT;
-      double2 sum = make_double2(0.0, 0.0);
-      if (ti2 >= tj2) {
-        const double2* src = stage + (size_t)(ti2 * (ti2 + 1) / 2 + tj2) * 16 + qi * 4 + rj;
-        for (int g = 0; g < KG; ++g) {
-          const double2 v = src[(size_t)g * P.ntiles * 16];
-          sum.x += v.x;
-          sum.y += v.y;
-        }
-      } else {  // the conjugate of entry (j, i), held by tile (tj2, ti2)
-        const double2* src = stage + (size_t)(tj2 * (tj2 + 1) / 2 + ti2) * 16 + rj * 4 + qi;
-        for (int g = 0; g < KG; ++g) {
-          const double2 v = src[(size_t)g * P.ntiles * 16];
-          sum.x += v.x;
-          sum.y -= v.y;
-        }
-      }
+      const double gr = pel(2 * i, 2 * j) + pel(2 * i + 1, 2 * j + 1);
+      const double gi = i == j ? 0.0 : pel(2 * i, 2 * j + 1) - pel(2 * i + 1, 2 * j);
       if (CHECK) {
-        const double re = sum.x - (i == j ? 1.0 : 0.0);
-        mx = fmax(mx, sqrt(re * re + sum.y * sum.y));
+        const double re = gr - (i == j ? 1.0 : 0.0);
+        mx = fmax(mx, sqrt(re * re + gi * gi));
       } else {
-        Gc[i * (i + 1) / 2 + j] = sum;
+        Gc[i * (i + 1) / 2 + j] = make_double2(gr, gi);
       }
     }
+    __syncthreads();  // P tiles read: zero the staging rows i >= N again for the next block
+    if (N < 4 * NT)
+      for (int e = t; e < kStages * KC * (4 * NT - N); e += kThreads) {
+        const int row = e / (4 * NT - N), col = N + e % (4 * NT - N);
+        stage[row * Np + col] = make_double2(0.0, 0.0);
+      }
   }
   if (CHECK) atomicMax(P.maxerr, (unsigned long long)__double_as_longlong(mx));  // non-negative doubles order as integers
 }
@@ -309,6 +361,8 @@ __global__ void __launch_bounds__(32 * kFactorWarps) factor_kernel(Params P) {
       Lc[i * (i + 1) / 2 + j] = j < i ? make_double2(v.x, -v.y) : make_double2(1.0 / diag[i], 0.0);
     }
 }
+
+constexpr int kSolveThreads = 128;  // columns per solve chunk (three CTAs per SM at 170 registers)
 
 // W = conj(L)^{-1} V for every column of every block: thread per column, the
 // column in registers (NMAX entries, rows >= N unused), conj(L) in shared
@@ -561,6 +615,26 @@ __global__ void __launch_bounds__(kThreads) big_ortho_kernel(double2* __restrict
   }
 }
 
+// the orthogonality check above nbasis 40: one CTA per block, max |G - 1|
+__global__ void __launch_bounds__(kThreads) big_check_kernel(const double2* __restrict__ basis, int Vc, int N, int dof,
+                                                             int bv, unsigned long long* __restrict__ maxerr) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* G = reinterpret_cast<double2*>(smem_raw);  // [N][N]
+  double2* VT = G + N * N;                             // [KC][N] staging
+  const int64_t K = (int64_t)bv * dof;
+  double mx = 0.0;
+  for (int c = blockIdx.x; c < Vc; c += gridDim.x) {
+    big_gram(basis + (int64_t)c * N * K, N, K, dof, VT, G);
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+      const int i = e / N, j = e % N;
+      const double re = G[e].x - (i == j ? 1.0 : 0.0), im = G[e].y;
+      mx = fmax(mx, sqrt(re * re + im * im));
+    }
+    __syncthreads();
+  }
+  atomicMax(maxerr, (unsigned long long)__double_as_longlong(mx));
+}
+
 static int num_sms() {
   int dev = 0, n = 148;
   cudaGetDevice(&dev);
@@ -587,27 +661,45 @@ static gmg_status workspace(gmg_agg* h, Params* P) {
   P->Vc = (int)Vc;
   P->N = h->N;
   P->K = h->bv * h->dof;
-  P->NT = g.NT;
   P->Np = g.Np;
-  P->ntiles = g.ntiles;
-  P->KG = g.KG;
+  P->ntw = g.ntw;
+  P->kgw = g.kgw;
   P->KC = g.KC;
+  P->ntiles = g.ntiles;
   P->pass = 0;
   P->passes = 1;
+  return GMG_OK;
+}
+
+template <int NT, bool CHECK>
+static gmg_status launch_gram_nt(const Params& P, const Geo& g, cudaStream_t s) {
+  auto kern = gram_kernel<NT, CHECK>;
+  GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
+  int per_sm = 1;
+  GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, g.smem));
+  const int grid = std::min(P.Vc, num_sms() * std::max(per_sm, 1));
+  kern<<<grid, kThreads, g.smem, s>>>(P);
+  GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
 
 template <bool CHECK>
 static gmg_status launch_gram(const Params& P, cudaStream_t s) {
   const Geo g = geometry(P.N);
+  GMG_CHECK(g.NT <= kMaxNT, GMG_ERR_UNSUPPORTED, "orthonormalise: nbasis above the tensor-core Gram path");
   GMG_CHECK(g.smem <= 227 * 1024, GMG_ERR_UNSUPPORTED, "orthonormalise: tile does not fit shared memory");
-  GMG_CUDA(cudaFuncSetAttribute(gram_kernel<CHECK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
-  int per_sm = 1;
-  GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gram_kernel<CHECK>, kThreads, g.smem));
-  const int grid = std::min(P.Vc, num_sms() * std::max(per_sm, 1));
-  gram_kernel<CHECK><<<grid, kThreads, g.smem, s>>>(P);
-  GMG_CUDA(cudaGetLastError());
-  return GMG_OK;
+  switch (g.NT) {
+    case 1: return launch_gram_nt<1, CHECK>(P, g, s);
+    case 2: return launch_gram_nt<2, CHECK>(P, g, s);
+    case 3: return launch_gram_nt<3, CHECK>(P, g, s);
+    case 4: return launch_gram_nt<4, CHECK>(P, g, s);
+    case 5: return launch_gram_nt<5, CHECK>(P, g, s);
+    case 6: return launch_gram_nt<6, CHECK>(P, g, s);
+    case 7: return launch_gram_nt<7, CHECK>(P, g, s);
+    case 8: return launch_gram_nt<8, CHECK>(P, g, s);
+    case 9: return launch_gram_nt<9, CHECK>(P, g, s);
+    default: return launch_gram_nt<10, CHECK>(P, g, s);
+  }
 }
 
 static gmg_status launch_factor(const Params& P, cudaStream_t s) {
@@ -686,7 +778,16 @@ gmg_status agg_check_orthogonal(gmg_agg* h, double* max_err, cudaStream_t s) {
   Params P;
   GMG_TRY(workspace(h, &P));
   GMG_CUDA(cudaMemsetAsync(P.maxerr, 0, sizeof(unsigned long long), s));
-  GMG_TRY(launch_gram<true>(P, s));
+  if (h->N > kSolveMax) {
+    const size_t smem = sizeof(double2) * ((size_t)h->N * h->N + (size_t)kBigKS * h->dof * h->N);
+    GMG_CHECK(smem <= 227 * 1024, GMG_ERR_UNSUPPORTED, "check orthogonal: nbasis x site dof too large");
+    GMG_CUDA(cudaFuncSetAttribute(big_check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    big_check_kernel<<<std::min(P.Vc, num_sms() * 8), kThreads, smem, s>>>(h->basis_blk.as<double2>(), P.Vc, h->N,
+                                                                          h->dof, h->bv, P.maxerr);
+    GMG_CUDA(cudaGetLastError());
+  } else {
+    GMG_TRY(launch_gram<true>(P, s));
+  }
   unsigned long long v = 0;
   int st = 0;
   GMG_CUDA(cudaMemcpyAsync(&v, P.maxerr, sizeof(v), cudaMemcpyDeviceToHost, s));
