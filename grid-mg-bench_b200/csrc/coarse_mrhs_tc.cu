@@ -621,6 +621,106 @@ __global__ void __launch_bounds__(256) pack_vec_kernel(const float2* __restrict_
   }
 }
 
+// The same packing with coalesced loads, for all RHS (no active list), N a
+// multiple of 8 and a 16-byte aligned input.  A warp takes 256 consecutive
+// complex numbers of the input (2 KB): load j of lane l is the 16 bytes at
+// complex 64 j + 2 l, so each load instruction of the warp reads 512
+// contiguous bytes.  A 4 x 4 transpose inside each quad of lanes (two
+// shuffle stages) then gives lane k of quad q the 8 consecutive complex
+// numbers 64 k + 8 q .. + 7: one packed chunk, which it converts and stores
+// as the generic kernel does.  Rows r >= nrhs of the padded RHS dimension and
+// the chunks kc >= N / 8 (b >= N) are written as zeros by a second loop.
+template <int KC>
+__global__ void __launch_bounds__(256) pack_vec_coalesced_kernel(const float4* __restrict__ in,
+                                                                 uint4* __restrict__ dst, int V, int N, int nrhs,
+                                                                 int Rp, int kind, int g5) {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const uint32_t total = (uint32_t)V * (uint32_t)nrhs * (uint32_t)N;  // complex numbers, < 2^31
+  const int lane = threadIdx.x & 31, k = lane & 3, q = lane >> 2;
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 256u; base < total;
+       base += nwarps * 256u) {
+    float4 x[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t c = base + 64u * j + 2u * lane;
+      x[j] = c < total ? __ldg(in + (c >> 1)) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    // transpose (register j, lane k) within the quad: x[m] <- lane m's x[k]
+#pragma unroll
+    for (int b = 2; b >= 1; b >>= 1) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (j & b) continue;
+        const bool hi = (k & b) != 0;
+        const float4 send = hi ? x[j] : x[j ^ b];
+        float4 got;
+        got.x = __shfl_xor_sync(0xffffffffu, send.x, b);
+        got.y = __shfl_xor_sync(0xffffffffu, send.y, b);
+        got.z = __shfl_xor_sync(0xffffffffu, send.z, b);
+        got.w = __shfl_xor_sync(0xffffffffu, send.w, b);
+        if (hi)
+          x[j] = got;
+        else
+          x[j ^ b] = got;
+      }
+    }
+    const uint32_t c0 = base + 64u * k + 8u * q;
+    if (c0 < total) {
+      const uint32_t row = c0 / (uint32_t)N;  // site * nrhs + r
+      const int b0 = (int)(c0 - row * (uint32_t)N);
+      const uint32_t s = row / (uint32_t)nrhs;
+      const int r = (int)(row - s * (uint32_t)nrhs);
+      float re[8], im[8];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        re[2 * m] = x[m].x;
+        im[2 * m] = x[m].y;
+        re[2 * m + 1] = x[m].z;
+        im[2 * m + 1] = x[m].w;
+      }
+      if (g5) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          if (b0 + i >= N / 2) {
+            re[i] = -re[i];
+            im[i] = -im[i];
+          }
+      }
+      uint32_t pr[4], pi[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        pr[m] = to_half_pair(re[2 * m], re[2 * m + 1], kind);
+        pi[m] = to_half_pair(im[2 * m], im[2 * m + 1], kind);
+      }
+      uint4* rowp = dst + ((size_t)s * KC + (b0 >> 3)) * 2 * Rp;
+      rowp[r] = make_uint4(pr[0], pr[1], pr[2], pr[3]);
+      rowp[Rp + r] = make_uint4(pi[0], pi[1], pi[2], pi[3]);
+    }
+  }
+  // zeros: padded rows r in [nrhs, Rp) of every chunk, and chunks kc >= N / 8 of rows r < nrhs
+  const int kfull = N / 8, npad = Rp - nrhs;
+  const uint32_t per_site = (uint32_t)KC * npad + (uint32_t)(KC - kfull) * nrhs;
+  const uint32_t zitems = (uint32_t)V * per_site;
+  const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < zitems; e += gridDim.x * blockDim.x) {
+    const uint32_t s = e / per_site;
+    const int rem = (int)(e - s * per_site);
+    int kc, r;
+    if (rem < KC * npad) {
+      kc = rem / npad;
+      r = nrhs + (rem - kc * npad);
+    } else {
+      const int t = rem - KC * npad;
+      kc = kfull + t / nrhs;
+      r = t - (kc - kfull) * nrhs;
+    }
+    uint4* rowp = dst + ((size_t)s * KC + kc) * 2 * Rp;
+    rowp[r] = z;
+    rowp[Rp + r] = z;
+  }
+}
+
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 // pack the vectors of one apply (G5C on input when g5).  (Two variants did not
@@ -635,6 +735,20 @@ inline gmg_status launch_pack(const float* in, uint4* packed, const int32_t* act
   const int grid = (int)std::min<int64_t>((rows + 255) / 256, 148 * 64);
   const float2* src = reinterpret_cast<const float2*>(in);
   const int a16 = (reinterpret_cast<uintptr_t>(in) & 15) == 0 ? 1 : 0;
+  const int64_t total = (int64_t)V * nrhs * N;
+  if (!active && R == nrhs && N % 8 == 0 && a16 && total < ((int64_t)1 << 31)) {
+    // one warp per 256 input complex numbers, 8 warps per CTA
+    const int cgrid = (int)std::min<int64_t>((total + 2047) / 2048, 148 * 32);
+    const float4* s4 = reinterpret_cast<const float4*>(in);
+    switch (Kc) {
+      case 2: pack_vec_coalesced_kernel<2><<<cgrid, 256, 0, s>>>(s4, packed, V, N, nrhs, Rp, kind, g5); break;
+      case 4: pack_vec_coalesced_kernel<4><<<cgrid, 256, 0, s>>>(s4, packed, V, N, nrhs, Rp, kind, g5); break;
+      case 6: pack_vec_coalesced_kernel<6><<<cgrid, 256, 0, s>>>(s4, packed, V, N, nrhs, Rp, kind, g5); break;
+      default: pack_vec_coalesced_kernel<8><<<cgrid, 256, 0, s>>>(s4, packed, V, N, nrhs, Rp, kind, g5); break;
+    }
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  }
   switch (Kc) {  // Kc = ceil16(N) / 8: 2, 4, 6 or 8 for N <= 64
     case 2: pack_vec_kernel<2><<<grid, 256, 0, s>>>(src, packed, active, V, N, nrhs, R, Rp, kind, g5, a16); break;
     case 4: pack_vec_kernel<4><<<grid, 256, 0, s>>>(src, packed, active, V, N, nrhs, R, Rp, kind, g5, a16); break;

@@ -146,12 +146,16 @@ struct gmg_wilson {
   gmg::DevBuf clover;     // complex<double> [V][2][6][6]
   gmg::DevBuf clover_f;
   gmg::DevBuf nbr;        // int32 [9][V]
-  // staged multi-RHS kernel: hop links [V][8][3][3] (p < 4: U_mu(x), p >= 4:
-  // U_mu(x - mu)), and per tile-size plans of the neighbour records a tile
-  // of consecutive sites reads (built once per lattice)
+  // hop links [V][8][3][3] (p < 4: U_mu(x), p >= 4: U_mu(x - mu)^dagger) for
+  // the tile, staged and face-hop kernels
   gmg::DevBuf hop, hop_f;
-  gmg::DevBuf plan[2];    // [0]: 8-site tiles, [1]: 16-site tiles
-  int plan_ok[2] = {-1, -1};
+  // plans of the pipelined staged kernel, by z block of the tile order: the
+  // neighbour records each 4-site tile reads, tiles in processing order
+  struct PipePlan {
+    gmg::DevBuf buf;
+    int smax = 0;         // most slots any tile uses; 0: the lattice has no plan
+  };
+  std::map<int, PipePlan> pplans;
   gmg::DevBuf dev_err;    // device error word of the staged kernel
   int wforce = -1;                  // forced kernel variant (gmg_wilson_kernel), -1: autotuned
   std::map<uint64_t, int> wtune;    // autotuned variant per (precision, products, op class, nrhs class)

@@ -114,13 +114,41 @@ __device__ __forceinline__ void wilson_hop(typename wt<T>::C out[4][3],
 }
 
 // One output spinor (site, rhs).  links(p) returns the 3x3 link of hop p
-// (p < 4: U_mu(x), p >= 4: U_mu(x - mu), applied daggered); cl: the site's
+// (p < 4: U_mu(x), p >= 4: U_mu(x - mu), applied daggered unless LDAG says the
+// links come daggered already); cl: the site's
 // two 6x6 clover blocks.
-// 12 complex numbers of one (site, RHS) record: 16-byte accesses when VEC
-// (the record start is 16-byte aligned), else one per complex number
-template <class T, bool VEC>
+// 12 complex numbers of one (site, RHS) record.  VEC 2: 32-byte accesses
+// (ld/st .v8.f32 / .v4.f64; the record start is 32-byte aligned), so that
+// every access covers one whole 32-byte sector; VEC 1: 16-byte accesses (the
+// record start is 16-byte aligned); VEC 0: one access per complex number.
+template <class T, int VEC>
 __device__ __forceinline__ void ld12(typename wt<T>::C v[12], const typename wt<T>::C* __restrict__ p) {
-  if (VEC && sizeof(T) == 4) {
+  if (VEC == 2 && sizeof(T) == 4) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float r[8];
+      asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                   : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]), "=f"(r[7])
+                   : "l"(reinterpret_cast<const float*>(p) + 8 * k));
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        v[4 * k + i].x = (T)r[2 * i];
+        v[4 * k + i].y = (T)r[2 * i + 1];
+      }
+    }
+  } else if (VEC == 2) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      double r[4];
+      asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+                   : "=d"(r[0]), "=d"(r[1]), "=d"(r[2]), "=d"(r[3])
+                   : "l"(reinterpret_cast<const double*>(p) + 4 * k));
+      v[2 * k].x = (T)r[0];
+      v[2 * k].y = (T)r[1];
+      v[2 * k + 1].x = (T)r[2];
+      v[2 * k + 1].y = (T)r[3];
+    }
+  } else if (VEC == 1 && sizeof(T) == 4) {
     const float4* q = reinterpret_cast<const float4*>(p);
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
@@ -135,9 +163,24 @@ __device__ __forceinline__ void ld12(typename wt<T>::C v[12], const typename wt<
     for (int k = 0; k < 12; ++k) v[k] = p[k];
   }
 }
-template <class T, bool VEC>
+template <class T, int VEC>
 __device__ __forceinline__ void st12(typename wt<T>::C* __restrict__ p, const typename wt<T>::C v[12]) {
-  if (VEC && sizeof(T) == 4) {
+  if (VEC == 2 && sizeof(T) == 4) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(reinterpret_cast<float*>(p) + 8 * k),
+                   "f"((float)v[4 * k].x), "f"((float)v[4 * k].y), "f"((float)v[4 * k + 1].x),
+                   "f"((float)v[4 * k + 1].y), "f"((float)v[4 * k + 2].x), "f"((float)v[4 * k + 2].y),
+                   "f"((float)v[4 * k + 3].x), "f"((float)v[4 * k + 3].y)
+                   : "memory");
+  } else if (VEC == 2) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(reinterpret_cast<double*>(p) + 4 * k),
+                   "d"((double)v[2 * k].x), "d"((double)v[2 * k].y), "d"((double)v[2 * k + 1].x),
+                   "d"((double)v[2 * k + 1].y)
+                   : "memory");
+  } else if (VEC == 1 && sizeof(T) == 4) {
     float4* q = reinterpret_cast<float4*>(p);
 #pragma unroll
     for (int k = 0; k < 6; ++k) q[k] = make_float4(v[2 * k].x, v[2 * k].y, v[2 * k + 1].x, v[2 * k + 1].y);
@@ -152,7 +195,7 @@ __device__ __forceinline__ void st12(typename wt<T>::C* __restrict__ p, const ty
 // bit p set are left out (0 for the plain operator); with the bits of the
 // hops to blocks of the other parity this gives e D e + o D o of the
 // coarsening's self term in one pass.
-template <class T, class LinkFn, bool DOTS = false, bool VEC = false>
+template <class T, class LinkFn, bool DOTS = false, int VEC = 0, bool LDAG = false, bool PF = false>
 __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict__ cl, LinkFn links,
                                             const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
                                             typename wt<T>::C* __restrict__ out, int V, int nrhs, int site, int r,
@@ -167,6 +210,49 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
   for (int s = 0; s < 4; ++s)
 #pragma unroll
     for (int c = 0; c < 3; ++c) acc[s][c] = C{0, 0};
+  if (PF && (op == GMG_OP_M || op == GMG_OP_MDAG)) {
+    // the full operator with the neighbour records software-pipelined: the
+    // eight neighbour indices first, then each hop's record is requested one
+    // hop ahead (the first one before the clover term), so that a record's
+    // latency overlaps the previous hop's arithmetic
+    int nbs[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) nbs[p] = nbr[(int64_t)p * V + site];
+    C psi[12], nxt[12];
+    ld12<T, VEC>(psi, in + ((int64_t)site * nrhs + r) * 12);
+    ld12<T, VEC>(nxt, in + ((int64_t)nbs[0] * nrhs + r) * 12);
+#pragma unroll
+    for (int k = 6; k < 12; ++k)
+      if (g5) psi[k] = C{-psi[k].x, -psi[k].y};
+#pragma unroll
+    for (int blk = 0; blk < 2; ++blk)
+#pragma unroll
+      for (int a = 0; a < 6; ++a) {
+        C v;
+        v.x = diag * psi[blk * 6 + a].x;
+        v.y = diag * psi[blk * 6 + a].y;
+#pragma unroll
+        for (int b = 0; b < 6; ++b) v = cadd(v, cmul(cl[(blk * 6 + a) * 6 + b], psi[blk * 6 + b]));
+        acc[(blk * 6 + a) / 3][(blk * 6 + a) % 3] = v;
+      }
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      const int mu = p & 3;
+      const int dsp = p < 4 ? 1 : -1;
+      C cur[12];
+#pragma unroll
+      for (int k = 0; k < 12; ++k) cur[k] = nxt[k];
+      if (p < 7) ld12<T, VEC>(nxt, in + ((int64_t)nbs[p < 7 ? p + 1 : 7] * nrhs + r) * 12);
+      if (skip & (1 << p)) continue;
+      T coef = (T)-0.5;
+      if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
+      if (g5) {
+#pragma unroll
+        for (int k = 6; k < 12; ++k) cur[k] = C{-cur[k].x, -cur[k].y};
+      }
+      wilson_hop<T>(acc, links(p, nbs[p]), dsp < 0 && !LDAG, cur, mu, dsp, coef);
+    }
+  } else {
   if (op != GMG_OP_MDIR) {
     // diagonal: (4 + m) psi + Cl psi, two chiral 6x6 blocks
     C psi[12];
@@ -203,8 +289,9 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
 #pragma unroll
         for (int k = 6; k < 12; ++k) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
       }
-      wilson_hop<T>(acc, links(p, nb), dsp < 0, psi, mu, dsp, coef);
+      wilson_hop<T>(acc, links(p, nb), dsp < 0 && !LDAG, psi, mu, dsp, coef);
     }
+  }
   }
   // per-record partial products in T (12 terms), accumulated in FP64 by the caller
   T pr = 0, pi = 0, pn = 0;
@@ -266,16 +353,21 @@ constexpr int kTileSites = 16;
 // the nsel sites of the list `sel` (all V sites when null) and only those are
 // written; hskip (per site, bit p: leave hop p out) restricts the hops to
 // neighbours of the same block parity (see wilson_site).
-template <class T, bool DOTS, int MINB, bool SEL = false>
+// bz > 0 (L0 a multiple of kTileSites, all sites): tile k of the loop is the
+// k-th in (z / bz, t, z mod bz, y, x) order, so that the records tiles share
+// with their t and z neighbours are still in L2 when those are processed.
+// PF: the neighbour records are software-pipelined (see wilson_site).
+template <class T, bool DOTS, int MINB, bool SEL = false, int VEC = 1, bool PF = false>
 __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
     const typename wt<T>::C* __restrict__ hop, const typename wt<T>::C* __restrict__ clover,
     const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
     typename wt<T>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
     int apbc, int tvol, int Lt, double2* __restrict__ d1, double2* __restrict__ d2,
-    const int32_t* __restrict__ sel = nullptr, int nsel = 0, const uint8_t* __restrict__ hskip = nullptr) {
+    const int32_t* __restrict__ sel = nullptr, int nsel = 0, const uint8_t* __restrict__ hskip = nullptr,
+    int L0 = 0, int L1 = 0, int bz = 0) {
   typedef typename wt<T>::C C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* Ls = reinterpret_cast<C*>(smem_raw);  // [kTileSites][8][9]: p < 4 U_mu(x), p >= 4 U_mu(x - mu)
+  C* Ls = reinterpret_cast<C*>(smem_raw);  // [kTileSites][8][9]: p < 4 U_mu(x), p >= 4 U_mu(x - mu)^dagger
   C* Cs = Ls + kTileSites * 72;            // [kTileSites][72]
   double* Ds = reinterpret_cast<double*>(Cs + kTileSites * 72);  // DOTS: [nrhs][3]
   if (DOTS)
@@ -286,7 +378,19 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
   const bool two = nrhs <= 2 * rt;
   double da[3] = {0.0, 0.0, 0.0}, db[3] = {0.0, 0.0, 0.0};
   for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
-    const int s0 = tile * kTileSites;
+    int s0 = tile * kTileSites;
+    if (!SEL && bz > 0) {
+      int k = tile;
+      const int nxt = L0 / kTileSites;
+      const int xt = k % nxt;
+      k /= nxt;
+      const int y = k % L1;
+      k /= L1;
+      const int zi = k % bz;
+      k /= bz;
+      const int t = k % Lt, z = (k / Lt) * bz + zi;
+      s0 = xt * kTileSites + L0 * (y + L1 * z) + tvol * t;
+    }
     const int ns = min(kTileSites, nsites - s0);
     __syncthreads();
     if (!SEL) {
@@ -312,7 +416,7 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
       int k = 0;
       for (int r = rl; r < nrhs; r += rt, ++k) {
         double dt[3] = {0.0, 0.0, 0.0};
-        wilson_site<T, decltype(links), DOTS, true>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op,
+        wilson_site<T, decltype(links), DOTS, VEC, true, PF>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op,
                                                     dir, disp, apbc, tvol, Lt, dt, skip);
         if (DOTS) {
           if (two) {
@@ -566,72 +670,117 @@ __global__ void __launch_bounds__(512) wilson_quad_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// Staged multi-RHS kernel.  A work item is a tile of TS consecutive sites and
-// a chunk of up to kChunk consecutive right-hand sides.  Every distinct
-// neighbour record the tile reads -- (site, chunk) is kChunk x 12 contiguous
-// complex numbers in the [V][nrhs][12] layout -- is brought into its own
-// shared-memory slot by one bulk copy (cp.async.bulk + an mbarrier
-// transaction count), together with the tile's hop links and clover blocks.
-// The spinor stencil then runs from shared memory: no global gathers.
+// Pipelined staged multi-RHS kernel (variant GMG_WILSON_STAGED).
 //
-// Slots and threads are laid out so that shared-memory reads are free of bank
-// conflicts: each slot is padded by 16 bytes (an odd number of 16-byte units)
-// and a quarter warp covers 2 sites x 4 RHS (FP32) or 4 sites x 2 RHS (FP64).
-// Two threads share a (site, RHS): h = 0 applies the forward hops and the
-// upper chiral clover block, h = 1 the backward hops and the lower block; each
-// owns two output spins and the halves meet once through shared memory.
+// A work item is a tile of kPipeTS = 4 consecutive sites and a chunk of up to
+// CMAX consecutive right-hand sides.  Every distinct neighbour record of the
+// tile -- (site, chunk) is chunk x 12 complex numbers, contiguous in the
+// [V][nrhs][12] layout -- is brought into its own shared-memory slot by one
+// bulk copy (cp.async.bulk), together with the tile's hop links, clover
+// blocks and plan entry.  One producer warp fills a ring of stages, each
+// tracked by an mbarrier transaction count (full[s]); the consumer warps
+// compute from a full stage and release it (empty[s]), so the copies of the
+// next stages overlap the arithmetic of this one.  CTAs are persistent (one
+// per SM) and walk the items in plan order: tiles sorted by (z block, t, z,
+// y, x), so that a record shared with the t and z neighbours of its site is
+// still in L2 when they are processed.
 //
-// The host-built tile plan lists, per tile, the sites of its slots (the TS
-// tile sites first) and per (site, hop) the slot to read; a tile reads at most
-// 7 TS + 4 distinct records (TS own, 6 TS across y, z, t, and at most 4 x
-// halos where the tile starts or ends inside an x row).
-// Tiles are swept chunk by chunk, so the window of records a chunk's sweep
-// revisits (two time slices) stays small enough for L2.
-constexpr int kChunk = 8;
+// Consumer lanes: lane bit 4 is the role h.  h = 0 applies the four forward
+// hops and the upper chiral clover block, h = 1 the four backward hops and
+// the lower block.  Both roles run one instruction stream (the backward hop
+// links are stored daggered, and the projector's sign is a factor), and the
+// two halves of an output record meet through one shuffle exchange.  The
+// other lane bits pick (site, RHS) so that the 16-byte shared-memory reads of
+// a quarter warp fall on distinct banks: 2 sites x 4 RHS (FP32) or 4 sites x
+// 2 RHS (FP64), with the slots padded to an odd number of 16-byte units.
+constexpr int kPipeTS = 4;
+constexpr int kPipeSMax = 7 * kPipeTS + 4;
+constexpr int kPipeMaxStages = 4;
+constexpr int kPipeHead = 256;  // mbarriers at the start of the dynamic shared memory
 
-template <class T> struct StageCfg;
-template <> struct StageCfg<float> { static constexpr int TS = 16; };
-template <> struct StageCfg<double> { static constexpr int TS = 8; };
+// plan entry of one tile (48 bytes, copied into the stage with the records)
+struct PipeTile {
+  int32_t s0, ns, nss, pad;
+  uint8_t slot[kPipeTS * 8];  // slot of the record of hop p of tile site j: slot[j * 8 + p]
+};
+static_assert(sizeof(PipeTile) == 48, "plan entry size");
+
+// CMAX: RHS per chunk; WARPS: consumer warps of one group (16 (site, RHS)
+// items per warp); GMAX: most consumer groups, each computing its own stage
+template <class T> struct PipeCfg;
+// (several groups measured slower: the stages' bulk copies, not the
+// arithmetic, bound this kernel, and more groups leave fewer stages to fill)
+template <> struct PipeCfg<float> { static constexpr int CMAX = 24, WARPS = 6, GMAX = 1; };
+template <> struct PipeCfg<double> { static constexpr int CMAX = 16, WARPS = 4, GMAX = 1; };
 
 template <class T>
-struct StageGeo {
+struct PipeGeo {
   typedef typename wt<T>::C C;
-  static constexpr int TS = StageCfg<T>::TS;
-  static constexpr int SMAX = 7 * TS + 4;
-  static constexpr int SREC = kChunk * 12 * (int)sizeof(C) + 16;  // slot stride (bytes)
-  static constexpr int LREC = 72 * (int)sizeof(C) + 16;           // links / clover stride per site
-  static constexpr int XREC = sizeof(T) == 4 ? 48 : 112;          // half-spinor exchange stride
-  static constexpr int THREADS = TS * kChunk * 2;
-  static constexpr int OFF_SLOTTAB = 16;
-  static constexpr int OFF_SPIN = 16 + 128;
-  static constexpr int OFF_LINKS = OFF_SPIN + SMAX * SREC;
-  static constexpr int OFF_CLOV = OFF_LINKS + TS * LREC;
-  static constexpr int OFF_DOTS = OFF_CLOV + TS * LREC;
-  static_assert(TS * 8 <= 128, "slot table");
-  static_assert(2 * TS * kChunk * XREC <= SMAX * SREC, "exchange buffer");
-  static_assert((SREC / 16) % 2 == 1 && (LREC / 16) % 2 == 1, "odd 16-byte strides");
+  static constexpr int LREC = 72 * (int)sizeof(C) + 16;  // links / clover stride per site
+  static constexpr int OFF_LINKS = 48;
+  static constexpr int OFF_CLOV = OFF_LINKS + kPipeTS * LREC;
+  static constexpr int OFF_SLOTS = OFF_CLOV + kPipeTS * LREC;
+  static constexpr int MAX_THREADS = (PipeCfg<T>::WARPS * PipeCfg<T>::GMAX + 1) * 32;
+  static_assert((LREC / 16) % 2 == 1, "odd 16-byte stride");
+  static_assert(PipeCfg<T>::WARPS * 16 == kPipeTS * PipeCfg<T>::CMAX, "16 (site, RHS) items per warp");
+  // slot stride for a chunk of ch RHS: an odd number of 16-byte units
+  __host__ __device__ static int srec(int ch) { return ch * 12 * (int)sizeof(C) + 16; }
+  __host__ __device__ static int stage_bytes(int ch, int smax) { return OFF_SLOTS + smax * srec(ch); }
 };
 
-// lane -> (site within the warp's 4 sites, RHS within the chunk)
-template <class T>
-__device__ __forceinline__ void stage_lane(int lane, int& sw, int& r) {
-  const int qtr = lane >> 3, in = lane & 7;
-  if (sizeof(T) == 4) {
-    sw = ((qtr & 1) << 1) | (in >> 2);
-    r = ((qtr >> 1) << 2) | (in & 3);
-  } else {
-    sw = in >> 1;
-    r = (qtr << 1) | (in & 1);
+// One hop with a compile-time direction for either role: the projected
+// half spinor (1 + sgn gamma_MU) psi, times the link U (already daggered for
+// backward hops), accumulated with coef into the upper spins and, through the
+// projector's rank-2 structure, into the lower ones.  sgn = -1 for the
+// forward hop (disp +1), +1 for the backward hop.
+template <class T, int MU>
+__device__ __forceinline__ void pipe_hop(typename wt<T>::C acc[4][3], const typename wt<T>::C* __restrict__ U,
+                                         const typename wt<T>::C psi[12], T sgn, T coef) {
+  typedef typename wt<T>::C C;
+  C hh[2][3];
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const int ps = gperm(MU, s), code = gphase(MU, s) & 3;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const C v = cphase(psi[ps * 3 + c], code);
+      hh[s][c] = C{psi[s * 3 + c].x + sgn * v.x, psi[s * 3 + c].y + sgn * v.y};
+    }
+  }
+  C uh[2][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const C u0 = U[a * 3], u1 = U[a * 3 + 1], u2 = U[a * 3 + 2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) uh[s][a] = cadd(cadd(cmul(u0, hh[s][0]), cmul(u1, hh[s][1])), cmul(u2, hh[s][2]));
+  }
+#pragma unroll
+  for (int s = 0; s < 2; ++s)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      acc[s][a].x += coef * uh[s][a].x;
+      acc[s][a].y += coef * uh[s][a].y;
+    }
+  const T cl = coef * sgn;
+#pragma unroll
+  for (int s = 2; s < 4; ++s) {
+    const int ps = gperm(MU, s), code = gphase(MU, s) & 3;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const C v = cphase(uh[ps][a], code);
+      acc[s][a].x += cl * v.x;
+      acc[s][a].y += cl * v.y;
+    }
   }
 }
 
 template <class T>
-__device__ __forceinline__ void load_spinor(typename wt<T>::C psi[12], const unsigned char* p) {
+__device__ __forceinline__ void load_spinor(typename wt<T>::C* psi, const unsigned char* p, int n) {
   typedef typename wt<T>::C C;
   if (sizeof(T) == 4) {
     const float4* q = reinterpret_cast<const float4*>(p);
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
+    for (int k = 0; k < n / 2; ++k) {
       const float4 v = q[k];
       psi[2 * k] = C{(T)v.x, (T)v.y};
       psi[2 * k + 1] = C{(T)v.z, (T)v.w};
@@ -639,183 +788,217 @@ __device__ __forceinline__ void load_spinor(typename wt<T>::C psi[12], const uns
   } else {
     const C* q = reinterpret_cast<const C*>(p);
 #pragma unroll
-    for (int k = 0; k < 12; ++k) psi[k] = q[k];
+    for (int k = 0; k < n; ++k) psi[k] = q[k];
   }
 }
 
-template <class T, bool DOTS>
-__global__ void __launch_bounds__(StageGeo<T>::THREADS) wilson_stage_kernel(
-    const typename wt<T>::C* __restrict__ hop, const typename wt<T>::C* __restrict__ clover,
-    const int32_t* __restrict__ plan_ns, const int32_t* __restrict__ plan_site,
-    const uint8_t* __restrict__ plan_slot, const typename wt<T>::C* __restrict__ in,
-    typename wt<T>::C* __restrict__ out, int V, int nrhs, T diag, int op, int dir, int disp, int apbc, int tvol,
-    int Lt, double2* __restrict__ d1, double2* __restrict__ d2, int* __restrict__ err) {
+// the hop of direction MU of role h (p = 4 h + MU), unless left out
+template <class T, int MU, bool SKIP>
+__device__ __forceinline__ void pipe_role_hop(typename wt<T>::C acc[4][3], const unsigned char* slots, int srec,
+                                              const uint8_t* tab, const typename wt<T>::C* Ls, int rr, int h,
+                                              T sgn, bool g5, int op, int dir, int disp, int skipb, bool tedge,
+                                              int apbc) {
   typedef typename wt<T>::C C;
-  typedef StageGeo<T> G;
-  constexpr int TS = G::TS;
-  extern __shared__ __align__(16) unsigned char sm[];
-  const uint8_t* slottab = sm + G::OFF_SLOTTAB;
-  unsigned char* spin = sm + G::OFF_SPIN;
-  unsigned char* links = sm + G::OFF_LINKS;
-  unsigned char* clov = sm + G::OFF_CLOV;
-  double* Ds = reinterpret_cast<double*>(sm + G::OFF_DOTS);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
-  volatile int* ok_flag = reinterpret_cast<volatile int*>(sm + 8);
+  if (op == GMG_OP_MDIR && (MU != dir || disp != (h ? -1 : 1))) return;
+  if (SKIP && ((skipb >> (4 * h + MU)) & 1)) return;
+  C psi[12];
+  load_spinor<T>(psi, slots + tab[MU] * srec + rr * 12 * (int)sizeof(C), 12);
+  if (g5) {
+#pragma unroll
+    for (int k = 6; k < 12; ++k) psi[k] = C{-psi[k].x, -psi[k].y};
+  }
+  const T coef = (apbc && MU == 3 && tedge) ? (T)0.5 : (T)-0.5;
+  pipe_hop<T, MU>(acc, Ls + (4 * h + MU) * 9, psi, sgn, coef);
+}
 
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int h = t / (TS * kChunk), u = t % (TS * kChunk);
-  int sw, rr;
-  stage_lane<T>(lane, sw, rr);
-  const int j = ((u >> 5) << 2) + sw;  // tile site of this thread
-  const bool g5 = (op == GMG_OP_MDAG);
-  const int ntiles = (V + TS - 1) / TS, nchunks = (nrhs + kChunk - 1) / kChunk;
-  const int64_t items = (int64_t)ntiles * nchunks;
+template <class T, bool DOTS, bool SKIP>
+__global__ void __launch_bounds__(PipeGeo<T>::MAX_THREADS, 1) wilson_pipe_kernel(
+    const typename wt<T>::C* __restrict__ hop, const typename wt<T>::C* __restrict__ clover,
+    const PipeTile* __restrict__ tiles, const int32_t* __restrict__ tsites, const typename wt<T>::C* __restrict__ in,
+    typename wt<T>::C* __restrict__ out, int nrhs, int ch, int nch, int ntiles, int nst, int ngrp, int sbytes, int soff,
+    T diag, int op, int dir, int disp, int apbc, int tvol, int Lt, const uint8_t* __restrict__ hskip,
+    double2* __restrict__ d1, double2* __restrict__ d2, int* __restrict__ err) {
+  typedef typename wt<T>::C C;
+  typedef PipeGeo<T> G;
+  constexpr int W = PipeCfg<T>::WARPS;
+  extern __shared__ __align__(128) unsigned char sm[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm);
+  uint64_t* empty = full + kPipeMaxStages;
+  double* Ds = reinterpret_cast<double*>(sm + kPipeHead);
+  unsigned char* stages = sm + soff;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t items = (int64_t)ntiles * nch;
+  const int srec = G::srec(ch);
 
-  if (t == 0) ac::mbar_init(bar, 1);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < nst; ++k) {
+      ac::mbar_init(&full[k], 1);
+      ac::mbar_init(&empty[k], W);  // one group consumes each fill of a stage
+    }
+  }
   if (DOTS)
-    for (int k = t; k < 3 * nrhs; k += blockDim.x) Ds[k] = 0.0;
+    for (int k = threadIdx.x; k < 3 * nrhs; k += blockDim.x) Ds[k] = 0.0;
   __syncthreads();
 
-  uint32_t phase = 0;
-  for (int64_t item = blockIdx.x; item < items; item += gridDim.x, phase ^= 1) {
-    const int chunk = (int)(item / ntiles), tile = (int)(item % ntiles);
-    const int s0 = tile * TS, nss = min(TS, V - s0);
-    const int r0 = chunk * kChunk, rc = min(kChunk, nrhs - r0);
-    // ---- stage: one bulk copy per slot, per site's links and clover, and the slot table
-    if (warp == 0) {
-      const int ns = plan_ns[tile];
-      const uint32_t rbytes = (uint32_t)(rc * 12 * sizeof(C));
+  if (warp == W * ngrp) {
+    // ---- producer: one stage per item, in the order the consumers take them
+    uint32_t n = 0;
+    for (int64_t it = blockIdx.x; it < items; it += gridDim.x, ++n) {
+      const int st = (int)(n % (uint32_t)nst);
+      const uint32_t use = n / (uint32_t)nst;
+      if (use > 0 && !ac::mbar_wait(&empty[st], (use - 1) & 1)) {
+        if (lane == 0) atomicCAS(err, 0, 2);
+        break;
+      }
+      const int tile = (int)(it / nch), chunk = (int)(it - (int64_t)tile * nch);
+      const int r0 = chunk * ch, rc = min(ch, nrhs - r0);
+      const PipeTile* tp = tiles + tile;
+      const int ns = tp->ns, nss = tp->nss, s0 = tp->s0;
+      unsigned char* sb = stages + (size_t)st * sbytes;
+      const uint32_t rbytes = (uint32_t)rc * 12u * (uint32_t)sizeof(C);
       if (lane == 0)
-        ac::mbar_expect_tx(bar, ns * rbytes + 2u * nss * 72u * (uint32_t)sizeof(C) + TS * 8u);
-      for (int k = lane; k < ns; k += 32) {
-        const int site = plan_site[(int64_t)tile * G::SMAX + k];
-        ac::bulk_g2s(spin + k * G::SREC, in + ((int64_t)site * nrhs + r0) * 12, rbytes, bar);
+        ac::mbar_expect_tx(&full[st], 48u + 2u * (uint32_t)nss * 72u * (uint32_t)sizeof(C) + (uint32_t)ns * rbytes);
+      __syncwarp();
+      if (lane < ns)
+        ac::bulk_g2s(sb + G::OFF_SLOTS + lane * srec, in + ((int64_t)tsites[(int64_t)tile * kPipeSMax + lane] * nrhs + r0) * 12,
+                     rbytes, &full[st]);
+      if (lane < nss) {
+        ac::bulk_g2s(sb + G::OFF_LINKS + lane * G::LREC, hop + (int64_t)(s0 + lane) * 72, 72 * sizeof(C), &full[st]);
+        ac::bulk_g2s(sb + G::OFF_CLOV + lane * G::LREC, clover + (int64_t)(s0 + lane) * 72, 72 * sizeof(C),
+                     &full[st]);
       }
-      for (int k = lane; k < nss; k += 32) {
-        ac::bulk_g2s(links + k * G::LREC, hop + (int64_t)(s0 + k) * 72, 72 * sizeof(C), bar);
-        ac::bulk_g2s(clov + k * G::LREC, clover + (int64_t)(s0 + k) * 72, 72 * sizeof(C), bar);
-      }
-      if (lane == 0) ac::bulk_g2s(sm + G::OFF_SLOTTAB, plan_slot + (int64_t)tile * TS * 8, TS * 8, bar);
+      if (lane == 31) ac::bulk_g2s(sb, tp, 48, &full[st]);
     }
-    if (t == 0) *ok_flag = ac::mbar_wait(bar, phase) ? 1 : 0;
-    __syncthreads();
-    if (!*ok_flag) {
-      // the copies did not land in time: record it, give our own copies a
-      // second bounded wait, and leave (every thread takes this branch)
-      if (t == 0) {
-        atomicCAS(err, 0, 1);
-        ac::mbar_wait(bar, phase);
+    // every stage this warp filled has landed before it exits (normally the
+    // consumers have waited for all of them already)
+    if (lane == 0) {
+      const uint32_t last = n < (uint32_t)nst ? n : (uint32_t)nst;
+      for (uint32_t k = 1; k <= last; ++k) {
+        const uint32_t m = n - k;
+        if (!ac::mbar_wait(&full[m % (uint32_t)nst], (m / (uint32_t)nst) & 1)) atomicCAS(err, 0, 2);
       }
-      return;
     }
-    ac::mbar_try_wait(bar, phase);  // completed: acquire the copied bytes in every thread
+    return;
+  }
 
-    const bool valid = j < nss && rr < rc;
-    C acc[4][3];
+  // ---- consumers: group g takes the items n = g, g + ngrp, ... (stage n mod nst)
+  const int grp = warp / W, cw = warp - grp * W, h = lane >> 4, qtr = (lane >> 3) & 1, in8 = lane & 7;
+  const int j = sizeof(T) == 4 ? 2 * qtr + (in8 >> 2) : in8 >> 1;
+  const int rr = sizeof(T) == 4 ? 4 * cw + (in8 & 3) : 4 * cw + 2 * qtr + (in8 & 1);
+  const bool g5 = (op == GMG_OP_MDAG);
+  const T sgn = h ? (T)1 : (T)-1;
+  uint32_t n = (uint32_t)grp;
+  for (int64_t it = blockIdx.x + (int64_t)grp * gridDim.x; it < items;
+       it += (int64_t)ngrp * gridDim.x, n += (uint32_t)ngrp) {
+    const int st = (int)(n % (uint32_t)nst);
+    const uint32_t use = n / (uint32_t)nst;
+    if (!ac::mbar_wait(&full[st], use & 1)) {
+      if (lane == 0) atomicCAS(err, 0, 3);
+      break;
+    }
+    const unsigned char* sb = stages + (size_t)st * sbytes;
+    const int chunk = (int)(it % nch);
+    const int r0 = chunk * ch, rc = min(ch, nrhs - r0);
+    if (4 * cw < rc) {
+      const PipeTile* tp = reinterpret_cast<const PipeTile*>(sb);
+      const int nss = tp->nss, site = tp->s0 + j;
+      const bool valid = j < nss && rr < rc;
+      const unsigned char* slots = sb + G::OFF_SLOTS;
+      C acc[4][3];
 #pragma unroll
-    for (int s = 0; s < 4; ++s)
+      for (int s = 0; s < 4; ++s)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) acc[s][c] = C{0, 0};
-    C cin[6];
-    if (valid) {
-      const int site = s0 + j;
-      if (op != GMG_OP_MDIR) {
-        C psi[12];
-        load_spinor<T>(psi, spin + j * G::SREC + rr * 12 * sizeof(C));
+        for (int c = 0; c < 3; ++c) acc[s][c] = C{0, 0};
+      C c6[6], cin[6];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) cin[k] = h ? psi[6 + k] : psi[k];
-        if (g5) {
-#pragma unroll
-          for (int k = 6; k < 12; ++k) psi[k] = C{-psi[k].x, -psi[k].y};
-        }
-        // own chiral block: rows 6h .. 6h + 5 = spins 2h, 2h + 1
-        const C* cl = reinterpret_cast<const C*>(clov + j * G::LREC) + h * 36;
-#pragma unroll
-        for (int a = 0; a < 6; ++a) {
-          C v;
-          const C pa = h ? psi[6 + a] : psi[a];
-          v.x = diag * pa.x;
-          v.y = diag * pa.y;
-#pragma unroll
-          for (int b = 0; b < 6; ++b) v = cadd(v, cmul(cl[a * 6 + b], h ? psi[6 + b] : psi[b]));
-          if (h)
-            acc[2 + a / 3][a % 3] = v;
-          else
-            acc[a / 3][a % 3] = v;
-        }
-      }
-      if (op != GMG_OP_MDIAG) {
+      for (int k = 0; k < 6; ++k) c6[k] = cin[k] = C{0, 0};
+      if (valid) {
         const int tc = site / tvol;
-        const C* Ls = reinterpret_cast<const C*>(links + j * G::LREC);
-        if (h == 0) {
+        const bool tedge = h ? tc == 0 : tc == Lt - 1;
+        const int skipb = SKIP ? (int)hskip[site] : 0;
+        if (op != GMG_OP_MDIAG) {
+          const uint8_t* tab = tp->slot + j * 8 + 4 * h;
+          const C* Ls = reinterpret_cast<const C*>(sb + G::OFF_LINKS + j * G::LREC);
+          pipe_role_hop<T, 0, SKIP>(acc, slots, srec, tab, Ls, rr, h, sgn, g5, op, dir, disp, skipb, tedge, apbc);
+          pipe_role_hop<T, 1, SKIP>(acc, slots, srec, tab, Ls, rr, h, sgn, g5, op, dir, disp, skipb, tedge, apbc);
+          pipe_role_hop<T, 2, SKIP>(acc, slots, srec, tab, Ls, rr, h, sgn, g5, op, dir, disp, skipb, tedge, apbc);
+          pipe_role_hop<T, 3, SKIP>(acc, slots, srec, tab, Ls, rr, h, sgn, g5, op, dir, disp, skipb, tedge, apbc);
+        }
+        if (op != GMG_OP_MDIR || DOTS) {
+          // this role's chiral half of the site's own record (spins 2h, 2h + 1)
+          load_spinor<T>(cin, slots + j * srec + (rr * 12 + 6 * h) * (int)sizeof(C), 6);
+        }
+        if (op != GMG_OP_MDIR) {
+          C pin[6];
 #pragma unroll
-          for (int mu = 0; mu < 4; ++mu) {
-            if (op == GMG_OP_MDIR && (mu != dir || disp != 1)) continue;
-            C psi[12];
-            load_spinor<T>(psi, spin + slottab[j * 8 + mu] * G::SREC + rr * 12 * sizeof(C));
-            if (g5) {
+          for (int k = 0; k < 6; ++k) pin[k] = (g5 && h) ? C{-cin[k].x, -cin[k].y} : cin[k];
+          const C* cl = reinterpret_cast<const C*>(sb + G::OFF_CLOV + j * G::LREC) + h * 36;
 #pragma unroll
-              for (int k = 6; k < 12; ++k) psi[k] = C{-psi[k].x, -psi[k].y};
-            }
-            const T coef = (apbc && mu == 3 && tc == Lt - 1) ? (T)0.5 : (T)-0.5;
-            wilson_hop<T>(acc, Ls + mu * 9, false, psi, mu, 1, coef);
-          }
-        } else {
+          for (int a = 0; a < 6; ++a) {
+            C v = C{diag * pin[a].x, diag * pin[a].y};
 #pragma unroll
-          for (int mu = 0; mu < 4; ++mu) {
-            if (op == GMG_OP_MDIR && (mu != dir || disp != -1)) continue;
-            C psi[12];
-            load_spinor<T>(psi, spin + slottab[j * 8 + 4 + mu] * G::SREC + rr * 12 * sizeof(C));
-            if (g5) {
-#pragma unroll
-              for (int k = 6; k < 12; ++k) psi[k] = C{-psi[k].x, -psi[k].y};
-            }
-            const T coef = (apbc && mu == 3 && tc == 0) ? (T)0.5 : (T)-0.5;
-            wilson_hop<T>(acc, Ls + (4 + mu) * 9, true, psi, mu, -1, coef);
+            for (int b = 0; b < 6; ++b) v = cadd(v, cmul(cl[a * 6 + b], pin[b]));
+            c6[a] = v;
           }
         }
       }
-    }
-    // ---- exchange the halves: each thread hands its partner the two spins it does not own
-    __syncthreads();  // every thread is done with the staged slots
-    {
-      C* xo = reinterpret_cast<C*>(spin + (h * TS * kChunk + u) * G::XREC);
-#pragma unroll
-      for (int k = 0; k < 6; ++k) xo[k] = h ? acc[k / 3][k % 3] : acc[2 + k / 3][k % 3];
-    }
-    __syncthreads();
-    if (valid) {
-      const C* xi = reinterpret_cast<const C*>(spin + ((1 - h) * TS * kChunk + u) * G::XREC);
+      // exchange: each role keeps its own two spins and hands the other two to its partner
       C o[6];
 #pragma unroll
       for (int k = 0; k < 6; ++k) {
-        o[k] = cadd(h ? acc[2 + k / 3][k % 3] : acc[k / 3][k % 3], xi[k]);
+        const C keep = h ? acc[2 + k / 3][k % 3] : acc[k / 3][k % 3];
+        const C give = h ? acc[k / 3][k % 3] : acc[2 + k / 3][k % 3];
+        C got;
+        got.x = __shfl_xor_sync(0xffffffffu, give.x, 16);
+        got.y = __shfl_xor_sync(0xffffffffu, give.y, 16);
+        o[k] = cadd(cadd(keep, got), c6[k]);
         if (g5 && h) o[k] = C{-o[k].x, -o[k].y};
       }
-      C* dst = out + ((int64_t)(s0 + j) * nrhs + r0 + rr) * 12 + 6 * h;
+      if (valid) {
+        C* dst = out + ((int64_t)site * nrhs + r0 + rr) * 12 + 6 * h;
+        if (sizeof(T) == 4) {
+          float4* q = reinterpret_cast<float4*>(dst);
 #pragma unroll
-      for (int k = 0; k < 6; ++k) dst[k] = o[k];
+          for (int k = 0; k < 3; ++k)
+            q[k] = make_float4((float)o[2 * k].x, (float)o[2 * k].y, (float)o[2 * k + 1].x, (float)o[2 * k + 1].y);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) dst[k] = o[k];
+        }
+      }
       if (DOTS) {
         double pr = 0.0, pi = 0.0, pn = 0.0;
+        if (valid) {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          const double vx = o[k].x, vy = o[k].y, ix = cin[k].x, iy = cin[k].y;
-          pr += vx * ix + vy * iy;
-          pi += vx * iy - vy * ix;
-          pn += vx * vx + vy * vy;
+          for (int k = 0; k < 6; ++k) {
+            const double vx = o[k].x, vy = o[k].y, ix = cin[k].x, iy = cin[k].y;
+            pr += vx * ix + vy * iy;
+            pi += vx * iy - vy * ix;
+            pn += vx * vx + vy * vy;
+          }
         }
-        atomicAdd(&Ds[3 * (r0 + rr)], pr);
-        atomicAdd(&Ds[3 * (r0 + rr) + 1], pi);
-        atomicAdd(&Ds[3 * (r0 + rr) + 2], pn);
+        // fold the lanes of one RHS: the sites (and the quarter for FP32) and the roles
+        const int m1 = sizeof(T) == 4 ? 4 : 2, m2 = sizeof(T) == 4 ? 8 : 4;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const int m = q == 0 ? m1 : q == 1 ? m2 : 16;
+          pr += __shfl_xor_sync(0xffffffffu, pr, m);
+          pi += __shfl_xor_sync(0xffffffffu, pi, m);
+          pn += __shfl_xor_sync(0xffffffffu, pn, m);
+        }
+        if ((lane & (m1 | m2 | 16)) == 0 && rr < rc) {
+          atomicAdd(&Ds[3 * (r0 + rr)], pr);
+          atomicAdd(&Ds[3 * (r0 + rr) + 1], pi);
+          atomicAdd(&Ds[3 * (r0 + rr) + 2], pn);
+        }
       }
     }
-    // the next item's bulk copies overwrite what this item wrote and read
-    ac::fence_proxy_async_smem();
-    __syncthreads();
+    __syncwarp();
+    if (lane == 0) ac::mbar_arrive(&empty[st]);
   }
   if (DOTS) {
-    __syncthreads();
-    for (int k = t; k < nrhs; k += blockDim.x) {
+    asm volatile("bar.sync 1, %0;" ::"r"(W * ngrp * 32) : "memory");
+    for (int k = threadIdx.x; k < nrhs; k += W * ngrp * 32) {
       atomicAdd(&d1[k].x, Ds[3 * k]);
       atomicAdd(&d1[k].y, Ds[3 * k + 1]);
       atomicAdd(&d2[k].x, Ds[3 * k + 2]);
@@ -823,15 +1006,21 @@ __global__ void __launch_bounds__(StageGeo<T>::THREADS) wilson_stage_kernel(
   }
 }
 
-// hop links: hop[x][p] = p < 4 ? U_p(x) : U_{p-4}(x - p)
+// hop links: hop[x][p] = p < 4 ? U_p(x) : U_{p-4}(x - p)^dagger, so that
+// every hop multiplies by its link as stored
 template <class C>
 __global__ void hop_links_kernel(const C* __restrict__ gauge, const int32_t* __restrict__ nbr, C* __restrict__ hop,
                                  int V) {
   const int64_t n = (int64_t)V * 72;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     const int site = (int)(e / 72), k = (int)(e % 72), p = k / 9, m = k % 9;
-    const int src = p < 4 ? site : nbr[(int64_t)p * V + site];
-    hop[e] = gauge[((int64_t)src * 4 + (p & 3)) * 9 + m];
+    if (p < 4) {
+      hop[e] = gauge[((int64_t)site * 4 + p) * 9 + m];
+    } else {
+      const int src = nbr[(int64_t)p * V + site];
+      const C u = gauge[((int64_t)src * 4 + (p & 3)) * 9 + (m % 3) * 3 + m / 3];
+      hop[e] = C{u.x, -u.y};
+    }
   }
 }
 
@@ -964,127 +1153,160 @@ gmg_status wilson_build_clover(gmg_wilson* h, cudaStream_t s) {
   return GMG_OK;
 }
 
-// Tile plan for TS-site tiles: [ntiles] slot counts, [ntiles][7 TS + 4] slot
-// sites (the tile's own sites first), [ntiles][TS][8] slot of each hop.
-// Every out-of-tile neighbour gets its own slot; the count bound 7 TS + 4
-// holds for every lattice (see the staged kernel), and is checked here.
-struct PlanView {
-  const int32_t* ns;
-  const int32_t* site;
-  const uint8_t* slot;
-};
-
+// Plan of the pipelined staged kernel, tiles in processing order: per tile a
+// PipeTile entry (first site, slot count, site count, the slot of each hop's
+// record) and the sites of its slots (the tile's own sites first, then every
+// distinct out-of-tile neighbour).  Tiles are sorted by (z / bz, t, z mod bz,
+// y, x): the records that neighbouring tiles in t share stay within a window
+// of about 2 bz Lx Ly sites.  At most 7 TS + 4 slots per tile (TS own, 6 TS
+// across y, z, t, at most 4 x halos where a tile starts or ends inside an x
+// row); a lattice that needs more gets no plan.
 static size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-static PlanView plan_view(const DevBuf& b, int ntiles, int TS) {
-  const int smax = 7 * TS + 4;
-  const unsigned char* p = b.as<unsigned char>();
-  const size_t o1 = align16(sizeof(int32_t) * ntiles);
-  const size_t o2 = o1 + align16(sizeof(int32_t) * (size_t)ntiles * smax);
-  return PlanView{reinterpret_cast<const int32_t*>(p), reinterpret_cast<const int32_t*>(p + o1),
-                  reinterpret_cast<const uint8_t*>(p + o2)};
-}
-
-static gmg_status build_plan(gmg_wilson* h, int which, cudaStream_t s) {
-  if (h->plan_ok[which] >= 0) return GMG_OK;
-  const int TS = which ? 16 : 8, smax = 7 * TS + 4;
-  const int64_t V = h->dims.vol();
-  const int ntiles = (int)((V + TS - 1) / TS);
-  std::vector<int32_t> nbr(9 * V);
-  host_neighbors(h->dims, nbr.data());
-  const size_t o1 = align16(sizeof(int32_t) * ntiles);
-  const size_t o2 = o1 + align16(sizeof(int32_t) * (size_t)ntiles * smax);
-  const size_t bytes = o2 + (size_t)ntiles * TS * 8;
-  std::vector<unsigned char> host(bytes, 0);
-  int32_t* ns = reinterpret_cast<int32_t*>(host.data());
-  int32_t* site = reinterpret_cast<int32_t*>(host.data() + o1);
-  uint8_t* slot = host.data() + o2;
-  bool ok = true;
-  for (int tile = 0; tile < ntiles && ok; ++tile) {
-    const int64_t s0 = (int64_t)tile * TS;
-    const int nss = (int)std::min<int64_t>(TS, V - s0);
-    int32_t* st = site + (size_t)tile * smax;
-    uint8_t* sl = slot + (size_t)tile * TS * 8;
-    int n = nss;
-    for (int j = 0; j < nss; ++j) st[j] = (int32_t)(s0 + j);
-    for (int p = 0; p < 8 && ok; ++p)
-      for (int j = 0; j < nss; ++j) {
-        const int32_t nb = nbr[(size_t)p * V + s0 + j];
-        if (nb >= s0 && nb < s0 + nss) {
-          sl[j * 8 + p] = (uint8_t)(nb - s0);
-        } else if (n < smax) {
-          st[n] = nb;
-          sl[j * 8 + p] = (uint8_t)n;
-          ++n;
-        } else {
-          ok = false;
-          break;
-        }
-      }
-    ns[tile] = n;
-  }
-  if (!ok) {
-    h->plan_ok[which] = 0;
+static gmg_status build_pipe_plan(gmg_wilson* h, int bz, cudaStream_t s, const gmg_wilson::PipePlan** out) {
+  auto found = h->pplans.find(bz);
+  if (found != h->pplans.end()) {
+    *out = &found->second;
     return GMG_OK;
   }
-  GMG_TRY(h->plan[which].alloc(bytes));
-  GMG_CUDA(cudaMemcpyAsync(h->plan[which].p, host.data(), bytes, cudaMemcpyHostToDevice, s));
+  gmg_wilson::PipePlan& plan = h->pplans[bz];
+  *out = &plan;
+  const int64_t V = h->dims.vol();
+  const int L0 = h->dims.d[0], L1 = h->dims.d[1], L2 = h->dims.d[2], L3 = h->dims.d[3];
+  const int ntiles = (int)((V + kPipeTS - 1) / kPipeTS);
+  std::vector<int32_t> nbr(9 * V);
+  host_neighbors(h->dims, nbr.data());
+  std::vector<int64_t> key(ntiles);
+  std::vector<int32_t> order(ntiles);
+  for (int tile = 0; tile < ntiles; ++tile) {
+    const int64_t s0 = (int64_t)tile * kPipeTS;
+    const int64_t x = s0 % L0, y = (s0 / L0) % L1, z = (s0 / ((int64_t)L0 * L1)) % L2,
+                  t = s0 / ((int64_t)L0 * L1 * L2);
+    key[tile] = ((((z / bz) * L3 + t) * bz + z % bz) * L1 + y) * L0 + x;
+    order[tile] = tile;
+  }
+  std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+  const size_t tbytes = sizeof(PipeTile) * (size_t)ntiles;
+  std::vector<unsigned char> host(tbytes + sizeof(int32_t) * (size_t)ntiles * kPipeSMax, 0);
+  PipeTile* tiles = reinterpret_cast<PipeTile*>(host.data());
+  int32_t* sites = reinterpret_cast<int32_t*>(host.data() + tbytes);
+  int smax = 0;
+  for (int k = 0; k < ntiles; ++k) {
+    const int64_t s0 = (int64_t)order[k] * kPipeTS;
+    const int nss = (int)std::min<int64_t>(kPipeTS, V - s0);
+    PipeTile& tp = tiles[k];
+    int32_t* st = sites + (size_t)k * kPipeSMax;
+    tp.s0 = (int32_t)s0;
+    tp.nss = nss;
+    int n = nss;
+    for (int j = 0; j < nss; ++j) st[j] = (int32_t)(s0 + j);
+    for (int p = 0; p < 8; ++p)
+      for (int j = 0; j < nss; ++j) {
+        const int32_t nb = nbr[(size_t)p * V + s0 + j];
+        int slot = -1;
+        for (int q = 0; q < n; ++q)
+          if (st[q] == nb) {
+            slot = q;
+            break;
+          }
+        if (slot < 0) {
+          if (n == kPipeSMax) return GMG_OK;  // no plan (smax 0): the staged kernel does not apply
+          st[n] = nb;
+          slot = n++;
+        }
+        tp.slot[j * 8 + p] = (uint8_t)slot;
+      }
+    tp.ns = n;
+    smax = std::max(smax, n);
+  }
+  GMG_TRY(plan.buf.alloc(host.size()));
+  GMG_CUDA(cudaMemcpyAsync(plan.buf.p, host.data(), host.size(), cudaMemcpyHostToDevice, s));
   GMG_CUDA(cudaStreamSynchronize(s));  // host goes out of scope
-  h->plan_ok[which] = 1;
+  plan.smax = smax;
   return GMG_OK;
 }
 
-template <class T, bool DOTS>
-static size_t stage_smem(int nrhs) {
-  return (size_t)StageGeo<T>::OFF_DOTS + (DOTS ? sizeof(double) * 3 * (size_t)nrhs : 0);
+// z block of the tile order: the largest divisor of Lz whose window of
+// records, 2 bz Lx Ly sites of rec_bytes each, stays within budget (at least 1)
+static int pipe_bz(const gmg_wilson* h, int64_t rec_bytes, double budget) {
+  const int L2 = h->dims.d[2];
+  const double plane = (double)h->dims.d[0] * h->dims.d[1] * (double)rec_bytes;
+  int bz = 1;
+  for (int b = 1; b <= L2; ++b)
+    if (L2 % b == 0 && 2.0 * b * plane <= budget) bz = b;
+  return bz;
 }
 
-// staged kernel launch; *launched = false when the staged path does not apply
-// (no plan for this lattice, unaligned fields, or too little shared memory)
+// pipelined staged kernel launch; *launched = false when it does not apply
+// (unaligned fields, no plan for this lattice, or too little shared memory for
+// two stages).  hskip (per site, bit p: leave hop p out) is the coarsening's
+// self-term restriction, or null.
 template <bool DOTS>
-static gmg_status launch_stage(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs, const void* in,
-                               void* out, double2* d1, double2* d2, cudaStream_t s, bool* launched) {
+static gmg_status launch_pipe(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs, const void* in,
+                              void* out, double2* d1, double2* d2, cudaStream_t s, bool* launched,
+                              const uint8_t* hskip = nullptr, int bz_scale = 1) {
   *launched = false;
   if (((uintptr_t)in | (uintptr_t)out) & 15) return GMG_OK;
   const bool f32 = vec_prec == GMG_F32;
   if (!f32 && vec_prec != GMG_F64) return GMG_OK;
-  const int which = f32 ? 1 : 0, TS = f32 ? StageGeo<float>::TS : StageGeo<double>::TS;
-  GMG_TRY(build_plan(h, which, s));
-  if (h->plan_ok[which] != 1) return GMG_OK;
-  const size_t smem = f32 ? stage_smem<float, DOTS>(nrhs) : stage_smem<double, DOTS>(nrhs);
-  if (smem > 200 * 1024) return GMG_OK;
+  const int cmax = f32 ? PipeCfg<float>::CMAX : PipeCfg<double>::CMAX;
+  const int nch = (nrhs + cmax - 1) / cmax, ch = (nrhs + nch - 1) / nch;
+  const int64_t rec = (int64_t)nrhs * 12 * (f32 ? sizeof(float2) : sizeof(double2));
+  int bz = pipe_bz(h, rec, 48.0 * 1024 * 1024);
+  for (int k = 1; k < bz_scale; k *= 2)
+    if (bz * 2 <= h->dims.d[2] && h->dims.d[2] % (bz * 2) == 0) bz *= 2;
+  const gmg_wilson::PipePlan* plan = nullptr;
+  GMG_TRY(build_pipe_plan(h, bz, s, &plan));
+  if (plan->smax == 0) return GMG_OK;
+  const int sbytes = f32 ? PipeGeo<float>::stage_bytes(ch, plan->smax) : PipeGeo<double>::stage_bytes(ch, plan->smax);
+  const int soff = kPipeHead + (DOTS ? (int)align16(sizeof(double) * 3 * (size_t)nrhs) : 0);
+  int dev = 0, nsm = 148, smem_optin = 0;
+  GMG_CUDA(cudaGetDevice(&dev));
+  GMG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  GMG_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const int nst = std::min(kPipeMaxStages, (smem_optin - soff) / sbytes);
+  if (nst < 2) return GMG_OK;
+  // consumer groups: all but one stage being computed, one being filled
+  const int gmax = f32 ? PipeCfg<float>::GMAX : PipeCfg<double>::GMAX;
+  const int ngrp = std::min(gmax, nst - 1);
+  const size_t smem = (size_t)soff + (size_t)nst * sbytes;
   if (!h->dev_err.p) {
     GMG_TRY(h->dev_err.alloc(256));
     GMG_CUDA(cudaMemsetAsync(h->dev_err.p, 0, 256, s));
   }
   const int V = (int)h->dims.vol();
   const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
-  const int ntiles = (V + TS - 1) / TS;
-  const int64_t items = (int64_t)ntiles * ((nrhs + kChunk - 1) / kChunk);
-  const PlanView pv = plan_view(h->plan[which], ntiles, TS);
-  int dev = 0, nsm = 148, occ = 1;
-  GMG_CUDA(cudaGetDevice(&dev));
-  GMG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int ntiles = (V + kPipeTS - 1) / kPipeTS;
+  const int64_t items = (int64_t)ntiles * nch;
+  const PipeTile* tiles = plan->buf.as<PipeTile>();
+  const int32_t* tsites =
+      reinterpret_cast<const int32_t*>(plan->buf.as<unsigned char>() + sizeof(PipeTile) * (size_t)ntiles);
+  const int g = (int)std::min<int64_t>(items, nsm);
+  auto go = [&](auto kern, int wpg, auto diag, const void* hp, const void* cp) -> gmg_status {
+    const int threads = (wpg * ngrp + 1) * 32;
+    typedef decltype(diag) T;
+    typedef typename wt<T>::C C;
+    GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<g, threads, smem, s>>>(reinterpret_cast<const C*>(hp), reinterpret_cast<const C*>(cp), tiles, tsites,
+                                  reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), nrhs, ch, nch, ntiles,
+                                  nst, ngrp, sbytes, soff, diag, op, dir, disp, h->apbc, tvol, h->dims.d[3], hskip, d1, d2,
+                                  h->dev_err.as<int>());
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  };
   if (f32) {
-    auto k = wilson_stage_kernel<float, DOTS>;
-    GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, StageGeo<float>::THREADS, smem));
-    const int g = (int)std::min<int64_t>(items, (int64_t)nsm * std::max(occ, 1));
-    k<<<g, StageGeo<float>::THREADS, smem, s>>>(h->hop_f.as<float2>(), h->clover_f.as<float2>(), pv.ns, pv.site,
-                                                 pv.slot, (const float2*)in, (float2*)out, V, nrhs,
-                                                 (float)(4.0 + h->mass), op, dir, disp, h->apbc, tvol, h->dims.d[3],
-                                                 d1, d2, h->dev_err.as<int>());
+    const float diag = (float)(4.0 + h->mass);
+    if (hskip)
+      GMG_TRY(go(wilson_pipe_kernel<float, DOTS, true>, PipeCfg<float>::WARPS, diag, h->hop_f.p, h->clover_f.p));
+    else
+      GMG_TRY(go(wilson_pipe_kernel<float, DOTS, false>, PipeCfg<float>::WARPS, diag, h->hop_f.p, h->clover_f.p));
   } else {
-    auto k = wilson_stage_kernel<double, DOTS>;
-    GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, StageGeo<double>::THREADS, smem));
-    const int g = (int)std::min<int64_t>(items, (int64_t)nsm * std::max(occ, 1));
-    k<<<g, StageGeo<double>::THREADS, smem, s>>>(h->hop.as<double2>(), h->clover.as<double2>(), pv.ns, pv.site,
-                                                  pv.slot, (const double2*)in, (double2*)out, V, nrhs, 4.0 + h->mass,
-                                                  op, dir, disp, h->apbc, tvol, h->dims.d[3], d1, d2,
-                                                  h->dev_err.as<int>());
+    const double diag = 4.0 + h->mass;
+    if (hskip)
+      GMG_TRY(go(wilson_pipe_kernel<double, DOTS, true>, PipeCfg<double>::WARPS, diag, h->hop.p, h->clover.p));
+    else
+      GMG_TRY(go(wilson_pipe_kernel<double, DOTS, false>, PipeCfg<double>::WARPS, diag, h->hop.p, h->clover.p));
   }
-  GMG_CUDA(cudaGetLastError());
   *launched = true;
   return GMG_OK;
 }
@@ -1174,22 +1396,35 @@ static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_
   const int tiles = (V + kTileSites - 1) / kTileSites;
   const int g = std::min(tiles, 148 * 16);
   const size_t dots = DOTS ? sizeof(double) * 3 * (size_t)nrhs : 0;
+  // 32-byte record accesses when both fields are 32-byte aligned
+  const bool v32 = ((((uintptr_t)in | (uintptr_t)out) & 31) == 0);
+  // tile order in z blocks (rows of whole tiles only)
+  const int64_t rec = (int64_t)nrhs * 12 * (vec_prec == GMG_F64 ? sizeof(double2) : sizeof(float2));
+  const int bz = (h->dims.d[0] % kTileSites == 0) ? pipe_bz(h, rec, 48.0 * 1024 * 1024) : 0;
+  auto go = [&](auto kern, auto diag, const void* hp, const void* cp, size_t csize) -> gmg_status {
+    typedef decltype(diag) T;
+    typedef typename wt<T>::C C;
+    const size_t smem = csize * 2 * kTileSites * 72 + dots;
+    if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<g, kTileSites * rt, smem, s>>>(reinterpret_cast<const C*>(hp), reinterpret_cast<const C*>(cp),
+                                          h->nbr.as<int32_t>(), reinterpret_cast<const C*>(in),
+                                          reinterpret_cast<C*>(out), V, nrhs, rt, diag, op, dir, disp, h->apbc, tvol,
+                                          h->dims.d[3], d1, d2, nullptr, 0, nullptr, h->dims.d[0], h->dims.d[1], bz);
+    return GMG_OK;
+  };
   if (vec_prec == GMG_F64) {
-    const size_t smem = sizeof(double2) * 2 * kTileSites * 72 + dots;
-    if (smem > 48 * 1024)
-      GMG_CUDA(cudaFuncSetAttribute(wilson_tile_kernel<double, DOTS, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
-    wilson_tile_kernel<double, DOTS, 2><<<g, kTileSites * rt, smem, s>>>(
-        h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(), (const double2*)in, (double2*)out, V,
-        nrhs, rt, 4.0 + h->mass, op, dir, disp, h->apbc, tvol, h->dims.d[3], d1, d2);
+    const double diag = 4.0 + h->mass;
+    if (v32)
+      GMG_TRY(go(wilson_tile_kernel<double, DOTS, 2, false, 2, true>, diag, h->hop.p, h->clover.p, sizeof(double2)));
+    else
+      GMG_TRY(go(wilson_tile_kernel<double, DOTS, 2, false, 1>, diag, h->hop.p, h->clover.p, sizeof(double2)));
   } else if (vec_prec == GMG_F32) {
-    const size_t smem = sizeof(float2) * 2 * kTileSites * 72 + dots;
-    if (smem > 48 * 1024)
-      GMG_CUDA(cudaFuncSetAttribute(wilson_tile_kernel<float, DOTS, MINB>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    wilson_tile_kernel<float, DOTS, MINB><<<g, kTileSites * rt, smem, s>>>(
-        h->hop_f.as<float2>(), h->clover_f.as<float2>(), h->nbr.as<int32_t>(), (const float2*)in, (float2*)out, V,
-        nrhs, rt, (float)(4.0 + h->mass), op, dir, disp, h->apbc, tvol, h->dims.d[3], d1, d2);
+    const float diag = (float)(4.0 + h->mass);
+    if (v32)
+      GMG_TRY(go(wilson_tile_kernel<float, DOTS, MINB, false, 2, MINB == 2>, diag, h->hop_f.p, h->clover_f.p,
+                 sizeof(float2)));
+    else
+      GMG_TRY(go(wilson_tile_kernel<float, DOTS, MINB, false, 1>, diag, h->hop_f.p, h->clover_f.p, sizeof(float2)));
   } else {
     return fail(GMG_ERR_UNSUPPORTED, "wilson apply: vectors must be F64 or F32");
   }
@@ -1221,8 +1456,8 @@ static gmg_status run_variant(gmg_wilson* h, int v, bool dots, int op, int dir, 
       return dots ? launch_quad<true>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s)
                   : launch_quad<false>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s);
     case GMG_WILSON_STAGED:
-      return dots ? launch_stage<true>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, launched)
-                  : launch_stage<false>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, launched);
+      return dots ? launch_pipe<true>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, launched)
+                  : launch_pipe<false>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s, launched);
     default:
       break;
   }
@@ -1317,7 +1552,7 @@ constexpr int kFacePad = 13;
 template <int MU>
 __device__ __forceinline__ void face_hop(double2 acc[4][3], const double2* __restrict__ U, const double2* psi,
                                          int disp, double coef) {
-  wilson_hop<double>(acc, U, disp < 0, psi, MU, disp, coef);
+  wilson_hop<double>(acc, U, false, psi, MU, disp, coef);  // backward links stored daggered
 }
 
 __global__ void __launch_bounds__(256, 3) wilson_face_hop_kernel(
@@ -1436,6 +1671,13 @@ gmg_status wilson_apply_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, 
   if (nrhs > 16 && rt < 8) rt = 16;
   const int nsites = sel ? nsel : V;
   if (nsites == 0) return GMG_OK;
+  if (!sel) {
+    // all sites: the pipelined staged kernel, hops restricted by hskip
+    bool launched = false;
+    KernelTimer kt("wilson", s);
+    GMG_TRY(launch_pipe<false>(h, op, dir, disp, GMG_F64, nrhs, in, out, nullptr, nullptr, s, &launched, hskip));
+    if (launched) return GMG_OK;
+  }
   const int tiles = (nsites + kTileSites - 1) / kTileSites;
   const int g = std::min(tiles, 148 * 16);
   const size_t smem = sizeof(double2) * 2 * kTileSites * 72;
@@ -1444,7 +1686,7 @@ gmg_status wilson_apply_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, 
   KernelTimer kt("wilson", s);
   k<<<g, kTileSites * rt, smem, s>>>(h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(),
                                      (const double2*)in, (double2*)out, V, nrhs, rt, 4.0 + h->mass, op, dir, disp,
-                                     h->apbc, tvol, h->dims.d[3], nullptr, nullptr, sel, nsel, hskip);
+                                     h->apbc, tvol, h->dims.d[3], nullptr, nullptr, sel, nsel, hskip, 0, 0, 0);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }

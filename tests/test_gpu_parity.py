@@ -391,11 +391,13 @@ VARIANTS = ["site", "tile", "quad", "staged"]
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
-@pytest.mark.parametrize("nrhs", [4, 7, 12, 13, 17, 20, 24])
+@pytest.mark.parametrize("nrhs", [4, 7, 12, 13, 17, 20, 24, 40])
 @pytest.mark.parametrize("op", ["M", "Mdag", "Mdiag"])
 def test_wilson_multi_rhs_variants(wil, forced, variant, nrhs, op):
     # tile: 16 sites x min(nrhs, 16) threads; quad: rt = largest divisor of nrhs
-    # up to 8 (13 -> 1, 7 -> 7, 20 -> 5); staged: chunks of 8 RHS (12 -> 8 + 4)
+    # up to 8 (13 -> 1, 7 -> 7, 20 -> 5); staged: RHS chunks of at most 24
+    # (FP32) or 16 (FP64) of equal size (FP64 17 -> 9 + 8, 40 -> 14 + 13 + 13;
+    # FP32 40 -> 20 + 20), partial warps in the last chunk
     dims, U, cl, w = wil
     forced(variant)
     x = inputs.gaussian_field((512, nrhs, 12), inputs.rng(stream=124 + nrhs))
@@ -475,10 +477,10 @@ def test_wilson_multi_rhs_mdir(wil, forced, variant):
 
 
 @pytest.mark.parametrize("variant", ["tile", "quad", "staged"])
-@pytest.mark.parametrize("nrhs", [1, 3, 12])
+@pytest.mark.parametrize("nrhs", [1, 3, 12, 24, 30])
 def test_wilson_apply_mr_products(wil, forced, variant, nrhs):
     # M with the minimal-residual inner products formed in the kernel's epilogue
-    # (staged needs nrhs >= 4 and falls back to the tuned choice below that)
+    # (FP32 30 RHS: two chunks of 15 in the staged kernel)
     dims, U, cl, w = wil
     forced(variant)
     x = inputs.gaussian_field((512, nrhs, 12), inputs.rng(stream=150 + nrhs))
