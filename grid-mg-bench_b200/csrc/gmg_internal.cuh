@@ -157,6 +157,7 @@ struct gmg_wilson {
   };
   std::map<int, PipePlan> pplans;
   gmg::DevBuf dev_err;    // device error word of the staged kernel
+  std::map<int, int> sel_pick;  // coarsening self term per nrhs: 0 pipelined staged kernel, 1 tile kernel
   int wforce = -1;                  // forced kernel variant (gmg_wilson_kernel), -1: autotuned
   std::map<uint64_t, int> wtune;    // autotuned variant per (precision, products, op class, nrhs class)
 };

@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
   double da[3] = {0.0, 0.0, 0.0}, db[3] = {0.0, 0.0, 0.0};
   for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
     int s0 = tile * kTileSites;
-    if (!SEL && bz > 0) {
+    if ((!SEL || !sel) && bz > 0) {
       int k = tile;
       const int nxt = L0 / kTileSites;
       const int xt = k % nxt;
@@ -1378,7 +1378,7 @@ static gmg_status launch_site(gmg_wilson* h, int op, int dir, int disp, int vec_
 
 // tile kernel: kTileSites sites x rt threads per CTA (rt <= 16); MINB: CTAs
 // per SM the register allocation must allow (FP32: 2 or 3)
-template <bool DOTS, int MINB = 2>
+template <bool DOTS, int MINB = 2, bool PF = (MINB == 2)>
 static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs, const void* in,
                               void* out, double2* d1, double2* d2, cudaStream_t s) {
   const int V = (int)h->dims.vol();
@@ -1421,7 +1421,7 @@ static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_
   } else if (vec_prec == GMG_F32) {
     const float diag = (float)(4.0 + h->mass);
     if (v32)
-      GMG_TRY(go(wilson_tile_kernel<float, DOTS, MINB, false, 2, MINB == 2>, diag, h->hop_f.p, h->clover_f.p,
+      GMG_TRY(go(wilson_tile_kernel<float, DOTS, MINB, false, 2, PF>, diag, h->hop_f.p, h->clover_f.p,
                  sizeof(float2)));
     else
       GMG_TRY(go(wilson_tile_kernel<float, DOTS, MINB, false, 1>, diag, h->hop_f.p, h->clover_f.p, sizeof(float2)));
@@ -1435,6 +1435,8 @@ static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_
 // internal variant id: a second register budget of the tile kernel, tuned
 // alongside the public variants and reported as GMG_WILSON_TILE
 constexpr int kTileOcc3 = 16;
+// and the same with the neighbour records prefetched (FP32)
+constexpr int kTileOcc3Pf = 17;
 
 // One launch of kernel variant v; *launched = false when v does not apply.
 static gmg_status run_variant(gmg_wilson* h, int v, bool dots, int op, int dir, int disp, int vec_prec, int nrhs,
@@ -1448,6 +1450,10 @@ static gmg_status run_variant(gmg_wilson* h, int v, bool dots, int op, int dir, 
       if (((uintptr_t)in | (uintptr_t)out) & 15) break;  // 16-byte spinor accesses
       return dots ? launch_tile<true>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s)
                   : launch_tile<false>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s);
+    case kTileOcc3Pf:
+      if ((((uintptr_t)in | (uintptr_t)out) & 31) || vec_prec != GMG_F32) break;
+      return dots ? launch_tile<true, 3, true>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s)
+                  : launch_tile<false, 3, true>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s);
     case kTileOcc3:  // the tile kernel with registers capped for 3 CTAs per SM (FP32)
       if ((((uintptr_t)in | (uintptr_t)out) & 15) || vec_prec != GMG_F32) break;
       return dots ? launch_tile<true, 3>(h, op, dir, disp, vec_prec, nrhs, in, out, d1, d2, s)
@@ -1499,7 +1505,10 @@ static gmg_status wilson_dispatch(gmg_wilson* h, bool dots, int op, int dir, int
   std::vector<int> cand;
   if (!dots && nrhs < 4) cand.push_back(GMG_WILSON_SITE);
   cand.push_back(GMG_WILSON_TILE);
-  if (vec_prec == GMG_F32) cand.push_back(kTileOcc3);
+  if (vec_prec == GMG_F32) {
+    cand.push_back(kTileOcc3);
+    cand.push_back(kTileOcc3Pf);
+  }
   cand.push_back(GMG_WILSON_QUAD);
   if (nrhs >= 4) cand.push_back(GMG_WILSON_STAGED);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -1654,12 +1663,12 @@ gmg_status wilson_apply_face(gmg_wilson* h, int p, int nrhs, const double* in, d
   return GMG_OK;
 }
 
-// The coarsening's forms of the FP64 operator (tile kernel, SEL instance):
-// op on the nsel sites of `sel` only (all sites when null; the other sites of
-// `out` are not written), and with hskip (per site, bit p set: leave hop p
-// out) the hops restricted to neighbours of the same block parity.
-gmg_status wilson_apply_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, const double* in, double* out,
-                            const int32_t* sel, int nsel, const uint8_t* hskip, cudaStream_t s) {
+// the tile kernel's SEL instance (FP64): op on the nsel sites of `sel` (all
+// sites when null), hops restricted by hskip; with all sites and 32-byte
+// aligned fields, 32-byte record accesses and the z-block tile order (the
+// prefetching form spills here)
+static gmg_status launch_tile_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, const double* in, double* out,
+                                  const int32_t* sel, int nsel, const uint8_t* hskip, cudaStream_t s) {
   const int V = (int)h->dims.vol();
   const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
   int rt = 1;
@@ -1670,24 +1679,81 @@ gmg_status wilson_apply_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, 
     }
   if (nrhs > 16 && rt < 8) rt = 16;
   const int nsites = sel ? nsel : V;
-  if (nsites == 0) return GMG_OK;
-  if (!sel) {
-    // all sites: the pipelined staged kernel, hops restricted by hskip
-    bool launched = false;
-    KernelTimer kt("wilson", s);
-    GMG_TRY(launch_pipe<false>(h, op, dir, disp, GMG_F64, nrhs, in, out, nullptr, nullptr, s, &launched, hskip));
-    if (launched) return GMG_OK;
-  }
   const int tiles = (nsites + kTileSites - 1) / kTileSites;
   const int g = std::min(tiles, 148 * 16);
   const size_t smem = sizeof(double2) * 2 * kTileSites * 72;
-  auto k = wilson_tile_kernel<double, false, 2, true>;
+  const bool fast = !sel && ((((uintptr_t)in | (uintptr_t)out) & 31) == 0);
+  const int bz = (fast && h->dims.d[0] % kTileSites == 0)
+                     ? pipe_bz(h, (int64_t)nrhs * 12 * sizeof(double2), 48.0 * 1024 * 1024)
+                     : 0;
+  auto k = fast ? wilson_tile_kernel<double, false, 2, true, 2> : wilson_tile_kernel<double, false, 2, true>;
   if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  KernelTimer kt("wilson", s);
   k<<<g, kTileSites * rt, smem, s>>>(h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(),
                                      (const double2*)in, (double2*)out, V, nrhs, rt, 4.0 + h->mass, op, dir, disp,
-                                     h->apbc, tvol, h->dims.d[3], nullptr, nullptr, sel, nsel, hskip, 0, 0, 0);
+                                     h->apbc, tvol, h->dims.d[3], nullptr, nullptr, sel, nsel, hskip, h->dims.d[0],
+                                     h->dims.d[1], bz);
   GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+// The coarsening's forms of the FP64 operator: op on the nsel sites of `sel`
+// only (all sites when null; the other sites of `out` are not written), and
+// with hskip (per site, bit p set: leave hop p out) the hops restricted to
+// neighbours of the same block parity.  With all sites, the pipelined staged
+// kernel and the tile kernel are timed once per nrhs (not while the stream is
+// being captured) and the faster one is kept.
+gmg_status wilson_apply_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, const double* in, double* out,
+                            const int32_t* sel, int nsel, const uint8_t* hskip, cudaStream_t s) {
+  const int nsites = sel ? nsel : (int)h->dims.vol();
+  if (nsites == 0) return GMG_OK;
+  if (sel) {
+    KernelTimer kt("wilson", s);
+    return launch_tile_sel(h, op, dir, disp, nrhs, in, out, sel, nsel, hskip, s);
+  }
+  auto run = [&](int which, bool* launched) -> gmg_status {
+    if (which == 0)
+      return launch_pipe<false>(h, op, dir, disp, GMG_F64, nrhs, in, out, nullptr, nullptr, s, launched, hskip);
+    *launched = true;
+    return launch_tile_sel(h, op, dir, disp, nrhs, in, out, nullptr, 0, hskip, s);
+  };
+  int pick = 1;
+  auto it = h->sel_pick.find(nrhs);
+  if (it != h->sel_pick.end()) {
+    pick = it->second;
+  } else {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    GMG_CUDA(cudaStreamIsCapturing(s, &cap));
+    if (cap == cudaStreamCaptureStatusNone) {
+      cudaEvent_t e0, e1;
+      GMG_CUDA(cudaEventCreate(&e0));
+      GMG_CUDA(cudaEventCreate(&e1));
+      float best = 1e30f;
+      gmg_status st = GMG_OK;
+      for (int which = 0; which < 2 && st == GMG_OK; ++which) {
+        bool launched = false;
+        st = run(which, &launched);  // warm-up
+        if (st != GMG_OK || !launched) continue;
+        if (cudaEventRecord(e0, s) != cudaSuccess) break;
+        for (int k = 0; k < 2 && st == GMG_OK; ++k) st = run(which, &launched);
+        float ms = 0.f;
+        if (st != GMG_OK || cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+          break;
+        if (ms < best) {
+          best = ms;
+          pick = which;
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      GMG_TRY(st);
+      if (best < 1e30f) h->sel_pick[nrhs] = pick;
+    }
+  }
+  KernelTimer kt("wilson", s);
+  bool launched = false;
+  GMG_TRY(run(pick, &launched));
+  if (!launched) GMG_TRY(run(1, &launched));
   return GMG_OK;
 }
 
