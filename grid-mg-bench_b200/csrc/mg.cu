@@ -68,7 +68,8 @@ struct gmg_mg {
   bool setup_done = false;
   // outer FGMRES workspace for max_rhs right-hand sides, allocated once
   gmg::VecBuf oV0, oZ0, ow, ot64, otz, obb, oxx;
-  gmg::DevBuf oidx;
+  gmg::VecBuf ozc, owc;   // compacted preconditioner output / operator output (in-cycle drop)
+  gmg::DevBuf oidx, oidx2;
   bool outer_ready = false;
   // captured K-cycle graphs per active-batch size (params.graph), their output
   // buffer and the capture streams of the nested conditional bodies
@@ -80,6 +81,7 @@ struct gmg_mg {
   // RHS left the active batch (its true residual below tol), and that residual
   std::vector<int> last_iters;
   std::vector<double> last_relres;
+  std::vector<int> last_batches;  // active batch size of every outer Arnoldi step of the last solve
   ~gmg_mg() {
     for (auto& g : kgraph) cudaGraphExecDestroy(g.second);
     for (auto& st : cap_st)
@@ -292,10 +294,30 @@ struct Krylov {
   Vec tz;       // Z-precision temporary for the preconditioner input (may equal V precision)
 };
 
+// In-cycle drop of converged right-hand sides (outer solve, flexible).  The
+// Arnoldi processes of the RHS are independent (one Hessenberg matrix each),
+// so an RHS whose residual estimate meets the tolerance at step j keeps its
+// j + 1 directions and takes no further part: the preconditioner and the
+// operator of the later steps run on the still-active columns only, gathered
+// into a compact batch (zc, wc; idx on the device) and scattered back into
+// the full-width Krylov vectors, whose other columns are zero.
+struct DropCtx {
+  Vec zc, wc;                  // compact scratch: preconditioner precision, FP64
+  int* idx = nullptr;          // device, active columns of the compact batch
+  bool enabled = false;        // drop (true) or only record the steps
+  std::vector<int> conv_step;  // out: per column, the step (1-based) its estimate met tol; 0: never
+  std::vector<int>* batches = nullptr;  // out: appended active-batch size of every step
+};
+
 template <class Prec>
 gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m, int maxit, double tol, Prec prec,
-                  bool flexible, int* iters_out, std::vector<double>* relres, cudaStream_t s) {
+                  bool flexible, int* iters_out, std::vector<double>* relres, cudaStream_t s,
+                  DropCtx* drop = nullptr) {
   const int R = b.R;
+  // per column: still iterating, and the Arnoldi steps it keeps
+  std::vector<char> live(R, 1);
+  std::vector<int> keep(R, 0), act;
+  if (drop) drop->conv_step.assign(R, 0);
   Vec V0 = K.V0.with_rhs(R), Z0 = K.Z0.with_rhs(R), w = K.w.with_rhs(R), t = K.t.with_rhs(R), tz = K.tz.with_rhs(R);
   const int64_t vstride = V0.elems(), zstride = Z0.elems();
   std::vector<zc> bn;
@@ -322,6 +344,10 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
       if (res[r] > tol) all = false;
     }
     if (all || iters >= maxit) break;
+    // a new cycle: every column takes part again (dropped ones have been folded into x)
+    std::fill(live.begin(), live.end(), 1);
+    act.resize(R);
+    for (int r = 0; r < R; ++r) act[r] = r;
     GMG_TRY(vec_scale_inv_norm(dn, w, v0, s));
     std::fill(H.begin(), H.end(), zc(0));
     std::fill(g.begin(), g.end(), zc(0));
@@ -330,12 +356,31 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
     for (int j = 0; j < m && iters < maxit; ++j) {
       Vec vj = nth(V0, j);
       Vec zj = flexible ? nth(Z0, j) : vj;
-      if (flexible) GMG_TRY(prec(vj, zj, tz));
-      if (zj.prec != w.prec) {
-        GMG_TRY(vec_convert(zj, t, s));
-        GMG_TRY(apply_op(h, l, t, w, s));
+      const int Ra = (int)act.size();
+      if (drop && drop->batches) drop->batches->push_back(Ra);
+      if (drop && drop->enabled && flexible && Ra < R) {
+        // compact: v_j's active columns -> preconditioner -> operator, scattered back
+        Vec vc = t.with_rhs(Ra), zc = drop->zc.with_rhs(Ra), wc = drop->wc.with_rhs(Ra);
+        GMG_TRY(vec_gather(vj, drop->idx, vc, s));
+        GMG_TRY(prec(vc, zc, tz));
+        GMG_CUDA(cudaMemsetAsync(zj.p, 0, zj.bytes(), s));
+        GMG_TRY(vec_scatter(zc, drop->idx, zj, s));
+        if (zc.prec != wc.prec) {
+          GMG_TRY(vec_convert(zc, vc, s));
+          GMG_TRY(apply_op(h, l, vc, wc, s));
+        } else {
+          GMG_TRY(apply_op(h, l, zc, wc, s));
+        }
+        GMG_CUDA(cudaMemsetAsync(w.p, 0, w.bytes(), s));
+        GMG_TRY(vec_scatter(wc, drop->idx, w, s));
       } else {
-        GMG_TRY(apply_op(h, l, zj, w, s));
+        if (flexible) GMG_TRY(prec(vj, zj, tz));
+        if (zj.prec != w.prec) {
+          GMG_TRY(vec_convert(zj, t, s));
+          GMG_TRY(apply_op(h, l, t, w, s));
+        } else {
+          GMG_TRY(apply_op(h, l, zj, w, s));
+        }
       }
       // classical Gram-Schmidt, twice, with the coefficients kept on the device;
       // the Hessenberg column comes back to the host in one transfer.  (With a
@@ -357,6 +402,7 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
       std::vector<zc> hc(nc);
       for (size_t k = 0; k < nc; ++k) hc[k] = col[k] + col[nc + k];
       for (int r = 0; r < R; ++r) {
+        if (!live[r]) continue;  // dropped: its Hessenberg matrix is complete
         const double hn = std::sqrt(std::max(col[2 * nc + r].real(), 0.0));
         // Hessenberg column j of RHS r, Givens rotations
         zc* Hr = &H[(size_t)r * (m + 1) * m];
@@ -388,10 +434,27 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
       }
       ++iters;
       jl = j;
-      bool conv = true;
-      for (int r = 0; r < R; ++r)
-        if (res[r] > tol) conv = false;
+      bool conv = true, dropped = false;
+      for (int r = 0; r < R; ++r) {
+        if (!live[r]) continue;
+        if (res[r] > tol) {
+          conv = false;
+        } else if (drop) {
+          if (!drop->conv_step[r]) drop->conv_step[r] = iters;
+          if (drop->enabled && flexible) {
+            live[r] = 0;
+            keep[r] = j + 1;
+            dropped = true;
+          }
+        }
+      }
       if (conv) break;
+      if (dropped) {
+        act.clear();
+        for (int r = 0; r < R; ++r)
+          if (live[r]) act.push_back(r);
+        GMG_CUDA(cudaMemcpyAsync(drop->idx, act.data(), sizeof(int) * act.size(), cudaMemcpyHostToDevice, s));
+      }
     }
     if (jl < 0) break;
     // y = H^{-1} g per RHS, x += sum_j y_j Z_j
@@ -400,9 +463,12 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
     for (int r = 0; r < R; ++r) {
       const zc* Hr = &H[(size_t)r * (m + 1) * m];
       const zc* gr = &g[(size_t)r * (m + 1)];
-      for (int i = n - 1; i >= 0; --i) {
+      // a dropped column uses the steps it kept; its later coefficients are zero
+      const int nr = live[r] ? n : keep[r];
+      for (int i = n - 1; i >= nr; --i) y[(size_t)i * R + r] = zc(0);
+      for (int i = nr - 1; i >= 0; --i) {
         zc acc = gr[i];
-        for (int k = i + 1; k < n; ++k) acc -= Hr[i * m + k] * y[(size_t)k * R + r];
+        for (int k = i + 1; k < nr; ++k) acc -= Hr[i * m + k] * y[(size_t)k * R + r];
         y[(size_t)i * R + r] = Hr[i * m + i] != zc(0) ? acc / Hr[i * m + i] : zc(0);
       }
     }
@@ -828,6 +894,11 @@ gmg_status outer_workspace(gmg_mg* h) {
   GMG_TRY(h->obb.alloc(V, R, 12, GMG_F64));
   GMG_TRY(h->oxx.alloc(V, R, 12, GMG_F64));
   GMG_TRY(h->oidx.alloc(sizeof(int) * R));
+  if (h->P.drop_in_cycle) {
+    GMG_TRY(h->ozc.alloc(V, R, 12, zp));
+    GMG_TRY(h->owc.alloc(V, R, 12, GMG_F64));
+    GMG_TRY(h->oidx2.alloc(sizeof(int) * R));
+  }
   if (h->P.graph && zp != GMG_F64) GMG_TRY(h->ogz.alloc(V, R, 12, zp));
   h->outer_ready = true;
   return GMG_OK;
@@ -938,6 +1009,7 @@ extern "C" gmg_status gmg_mg_params_default(gmg_mg_params* p) {
   p->graph = 1;
   p->refine_iters[0] = p->refine_iters[1] = 0;
   p->recursive_updates = 1;
+  p->drop_in_cycle = 1;
   return GMG_OK;
 }
 
@@ -1156,6 +1228,7 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
   for (int r = 0; r < nrhs; ++r) active[r] = r;
   std::vector<double> relres(nrhs, 1.0);
   std::vector<int> conv_it(nrhs, 0);
+  std::vector<int> batches;
   int total = 0;
   // per-RHS norms of b for the global convergence criterion
   std::vector<zc> bnz;
@@ -1172,21 +1245,22 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
     K.w = w.with_rhs(Ra);
     K.t = t64.with_rhs(Ra);
     K.tz = tz.with_rhs(Ra);
-    auto pc = [h, s, &tz, Ra, zp](const Vec& in, Vec& out, const Vec&) -> gmg_status {
+    auto pc = [h, s, &tz, zp](const Vec& in, Vec& out, const Vec&) -> gmg_status {
       // in: FP64 Krylov vector; out: Z direction in the preconditioner precision
-      Vec tin = tz.with_rhs(Ra);
+      const int Rb = in.R;  // the active columns (fewer than the batch after an in-cycle drop)
+      Vec tin = tz.with_rhs(Rb);
       if (zp == GMG_F64) return kcycle(h, 0, in, out, s);
       GMG_TRY(vec_convert(in, tin, s));
-      if (!h->P.graph || h->graph_broken || Ra > 1024) return kcycle(h, 0, tin, out, s);
-      auto it = h->kgraph.find(Ra);
+      if (!h->P.graph || h->graph_broken || Rb > 1024) return kcycle(h, 0, tin, out, s);
+      auto it = h->kgraph.find(Rb);
       if (it == h->kgraph.end()) {
         // first cycle of this batch size: host-driven (it also builds every
         // buffer and tuning key the cycle needs), then captured for the next ones
         GMG_TRY(kcycle(h, 0, tin, out, s));
         GMG_CUDA(cudaStreamSynchronize(s));
         cudaGraphExec_t ex = nullptr;
-        if (build_kcycle_graph(h, Ra, &ex) == GMG_OK)
-          h->kgraph[Ra] = ex;
+        if (build_kcycle_graph(h, Rb, &ex) == GMG_OK)
+          h->kgraph[Rb] = ex;
         else
           h->graph_broken = true;  // keep the host-driven cycle
         return GMG_OK;
@@ -1197,8 +1271,17 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
     };
     int it = 0;
     std::vector<double> rr;
-    GMG_TRY(fgmres(h, 0, bA, xA, K, m, std::min(m, maxiter - total), tol, pc, true, &it, &rr, s));
+    DropCtx dc;
+    dc.enabled = h->P.drop_in_cycle != 0;
+    if (dc.enabled) {
+      dc.zc = h->ozc.with_rhs(Ra);
+      dc.wc = h->owc.with_rhs(Ra);
+      dc.idx = h->oidx2.as<int>();
+    }
+    dc.batches = &batches;
+    GMG_TRY(fgmres(h, 0, bA, xA, K, m, std::min(m, maxiter - total), tol, pc, true, &it, &rr, s, &dc));
     GMG_TRY(vec_scatter(xA, idx.as<int>(), Xfull, s));
+    const int before = total;
     total += std::max(it, 1);
     // true residuals of the batch decide who stays active
     Vec rA = w.with_rhs(Ra);
@@ -1210,7 +1293,8 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
     for (int k = 0; k < Ra; ++k) {
       const int r = active[k];
       relres[r] = std::sqrt(std::max(rn[k].real(), 0.0) / std::max(bnz[r].real(), 1e-300));
-      conv_it[r] = total;
+      // the step at which its residual estimate met tol within this cycle, else the cycle's end
+      conv_it[r] = dc.conv_step[k] ? before + dc.conv_step[k] : total;
       if (relres[r] > tol) still.push_back(r);
     }
     if (it == 0 && still.size() == active.size()) break;  // no progress possible
@@ -1223,7 +1307,16 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
   if (max_relres) *max_relres = mx;
   h->last_iters = conv_it;
   h->last_relres = relres;
+  h->last_batches = batches;
   if (mx > tol) return fail(GMG_ERR_NOT_CONVERGED, "gmg_mg_solve: not converged within maxiter");
+  return GMG_OK;
+}
+
+extern "C" gmg_status gmg_mg_solve_batches(gmg_mg* h, int cap, int* sizes, int* n) {
+  GMG_CHECK(h && n, GMG_ERR_ARGUMENT, "gmg_mg_solve_batches: null argument");
+  *n = (int)h->last_batches.size();
+  GMG_CHECK(cap >= 0 && (cap == 0 || sizes), GMG_ERR_ARGUMENT, "gmg_mg_solve_batches: bad capacity");
+  for (int k = 0; k < std::min(cap, *n); ++k) sizes[k] = h->last_batches[k];
   return GMG_OK;
 }
 

@@ -425,7 +425,8 @@ class MGParams(ctypes.Structure):
                 ("coarsest_restart", ctypes.c_int), ("outer_restart", ctypes.c_int), ("prec", ctypes.c_int),
                 ("seed", ctypes.c_uint64), ("setup_solver", ctypes.c_int), ("setup_tol", ctypes.c_double),
                 ("setup_passes", ctypes.c_int), ("setup_null", ctypes.c_int), ("graph", ctypes.c_int),
-                ("refine_iters", ctypes.c_int * 2), ("recursive_updates", ctypes.c_int)]
+                ("refine_iters", ctypes.c_int * 2), ("recursive_updates", ctypes.c_int),
+                ("drop_in_cycle", ctypes.c_int)]
 
 
 class MultiGrid:
@@ -481,13 +482,21 @@ class MultiGrid:
         return it.value, rr.value
 
     def solve_stats(self, nrhs):
-        """Per-RHS (outer iterations until it left the active batch, final true relative residual)
-        of the last solve."""
+        """Per-RHS (outer iteration at which its residual estimate met the tolerance, final true
+        relative residual) of the last solve."""
         it = np.zeros(nrhs, dtype=np.int32)
         rr = np.zeros(nrhs, dtype=np.float64)
         _chk(lib().gmg_mg_solve_stats(self._h, int(nrhs), it.ctypes.data_as(ctypes.c_void_p),
                                       rr.ctypes.data_as(ctypes.c_void_p)))
         return it, rr
+
+    def solve_batches(self):
+        """Active-batch size of every outer Arnoldi step of the last solve."""
+        n = ctypes.c_int()
+        _chk(lib().gmg_mg_solve_batches(self._h, 0, None, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1), dtype=np.int32)
+        _chk(lib().gmg_mg_solve_batches(self._h, n.value, out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(n)))
+        return out[: n.value]
 
     def level(self, l):
         op, ag = ctypes.c_void_p(), ctypes.c_void_p()

@@ -356,6 +356,11 @@ typedef struct {
   int recursive_updates; /* 1: the refinement of a level also replaces the next level's test vectors
                             by its coarse solutions and rebuilds every coarser operator
                             (setupRecursiveUpdates, default 1) */
+  int drop_in_cycle;     /* 1 (default): an RHS whose outer FGMRES residual estimate meets the
+                            tolerance leaves the batch at that Arnoldi step: the later steps of the
+                            cycle apply the preconditioner and the operator to the still-active
+                            RHS only.  0: converged RHS leave at the next restart.  No counterpart
+                            (the reference solves one RHS at a time). */
 } gmg_mg_params;
 
 /* Defaults of MultiGridParams (MultigridParams.h:95-113) adapted to the MR smoother, with the
@@ -381,17 +386,23 @@ gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream s);
 gmg_status gmg_mg_refine(gmg_mg* h, gmg_stream s);
 /* Solve D x = b for nrhs right-hand sides with FP64 FGMRES + MG preconditioner to
    per-RHS relative residual |b - D x| / |b| <= tol.  b, x: device FP64
-   [V][nrhs][12]; x holds the initial guess.  Converged RHS drop out at every
-   outer restart.  Synchronises; GMG_ERR_NOT_CONVERGED if maxiter is reached. */
+   [V][nrhs][12]; x holds the initial guess.  Converged RHS drop out at the
+   Arnoldi step their residual estimate meets tol (params.drop_in_cycle), and
+   at every outer restart by their true residual.  Synchronises;
+   GMG_ERR_NOT_CONVERGED if maxiter is reached. */
 gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double* x, double tol, int maxiter, int* iters,
                         double* max_relres, gmg_stream s);
 /* Per-RHS outcome of the last gmg_mg_solve on this handle (nrhs must be that
-   solve's): iters[r], the outer iteration count after which RHS r left the
-   active batch (its true relative residual at or below tol; the last count
-   reached if it never did), and relres[r], that true relative residual.  No
+   solve's): iters[r], the outer iteration at which RHS r's residual estimate
+   met tol (the last count reached if it never did), and relres[r], its true
+   relative residual at the end.  No
    counterpart: the reference solves one RHS per solver call and times it
    (Test_wilsonclover_mg.cc:140-151). */
 gmg_status gmg_mg_solve_stats(gmg_mg* h, int nrhs, int* iters, double* relres);
+/* The active-batch size of every outer Arnoldi step of the last gmg_mg_solve
+   (the RHS the preconditioner and the operator were applied to): *n steps,
+   the first min(cap, *n) written to sizes.  No counterpart. */
+gmg_status gmg_mg_solve_batches(gmg_mg* h, int cap, int* sizes, int* n);
 /* Captured K-cycle graphs of this handle (params.graph): how many (one per
    active-batch size met so far) and whether a capture failed, in which case
    the solver kept the host-driven cycle.  No counterpart in the reference. */

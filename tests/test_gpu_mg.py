@@ -90,10 +90,11 @@ def test_mg_graph_captured_cycle(fine, prec, levels):
 def test_mg_graph_after_compaction(fine):
     # RHS that converge early drop out at the first outer restart; the smaller
     # batch gets its own captured cycle, and every RHS still reaches 1e-10
+    # (restart-time drops only: the in-cycle drop has its own test below)
     dims, w = fine
     nrhs = 4
     mg = gmg.MultiGrid(w, nrhs, nlevels=3, block=((2, 2, 2, 2), (2, 2, 2, 2)), nvec=(6, 6), setup_iters=30,
-                       prec="f32", coarsest_iters=30, wrapper_iters=6, outer_restart=4)
+                       prec="f32", coarsest_iters=30, wrapper_iters=6, outer_restart=4, drop_in_cycle=0)
     mg.setup()
     b = torch.from_numpy(inputs.gaussian_field((4096, nrhs, 12), inputs.rng(stream=305))).cuda()
     x = torch.zeros_like(b)
@@ -223,3 +224,47 @@ def test_mg_refinement_stops_at_a_level_without_iterations(fine):
     mg.refine()
     assert np.array_equal(_links(op1, 256, 12), l1)
     assert np.array_equal(_links(op2, 16, 12), l2)
+
+
+@pytest.mark.parametrize("prec,graph", [("f32", 1), ("bf16", 1), ("f64", 0)])
+def test_mg_converged_rhs_leave_within_a_cycle(fine, prec, graph):
+    # Right-hand sides whose initial guesses sit at different distances from
+    # the solution converge at different Arnoldi steps of one outer cycle.  With
+    # drop_in_cycle each leaves the batch at its step: the preconditioner and
+    # the operator of the later steps run on fewer RHS (the recorded batch sizes
+    # fall), every RHS keeps the iteration count it has without the drop (up to
+    # one step: the inner K-cycle solves stop on the slowest RHS of their
+    # batch), and every RHS meets the 1e-10 true residual.
+    dims, w = fine
+    nrhs = 4
+    kw = dict(nlevels=3, nvec=(6, 6), setup_iters=30, prec=prec, coarsest_iters=30, wrapper_iters=6, graph=graph,
+              block=((2, 2, 2, 2), (2, 2, 2, 2)), outer_restart=24)
+    b = torch.from_numpy(inputs.gaussian_field((4096, nrhs, 12), inputs.rng(stream=311))).cuda()
+    mg = gmg.MultiGrid(w, nrhs, drop_in_cycle=0, **kw)
+    mg.setup()
+    xs = torch.zeros_like(b)
+    mg.solve(b, xs, tol=1e-12, maxiter=400)
+    noise = torch.from_numpy(inputs.gaussian_field((4096, nrhs, 12), inputs.rng(stream=312))).cuda()
+    scale = torch.tensor([10.0 ** -(2 * r + 1) for r in range(nrhs)], dtype=torch.float64, device="cuda")
+    scale = scale * torch.linalg.vector_norm(xs, dim=(0, 2)) / torch.linalg.vector_norm(noise, dim=(0, 2))
+    x0 = xs + noise * scale.view(1, nrhs, 1)
+    res = {}
+    for drop in (0, 1):
+        m = gmg.MultiGrid(w, nrhs, drop_in_cycle=drop, **kw)
+        m.setup()
+        x = x0.clone()
+        it, rr = m.solve(b, x, tol=1e-10, maxiter=300)
+        assert rr <= 1e-10
+        assert true_relres(w, b, x) <= 2e-10, (drop, it, rr)
+        its, _ = m.solve_stats(nrhs)
+        res[drop] = (its, m.solve_batches())
+    its0, b0 = res[0]
+    its1, b1 = res[1]
+    assert len(set(its1.tolist())) >= 3, its1  # the RHS converge at different steps
+    assert np.abs(its1 - its0).max() <= 1, (its0, its1)
+    assert b0.min() == nrhs  # without the drop every step of the cycle runs the full batch
+    assert b1[0] == nrhs and b1.min() < nrhs and np.all(np.diff(b1) <= 0), b1
+    # each drop happened at the step its RHS met the tolerance: the batch of
+    # step k counts the RHS that had not converged before it
+    for k, sz in enumerate(b1):
+        assert sz == int((its1 > k).sum()), (k, b1, its1)
