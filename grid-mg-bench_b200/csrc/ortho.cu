@@ -141,17 +141,42 @@ template <int NT, int TW>
 __device__ __forceinline__ void gram_steps(double (&acc)[NT + 1][2], const double* fb, int stride_d, int grp, int nk4,
                                            int kgw) {
   constexpr int I1 = TW, I2 = NT - 1 - TW;
-  for (int k4 = grp; k4 < nk4; k4 += kgw) {
-    const double* f = fb + 4 * k4 * stride_d;
-    double fr[I2 + 1];
+  if (NT > 8) {
+    // (the register budget holds one set of fragments only)
+    for (int k4 = grp; k4 < nk4; k4 += kgw) {
+      const double* f = fb + 4 * k4 * stride_d;
+      double fr[I2 + 1];
 #pragma unroll
-    for (int X = 0; X <= I2; ++X) fr[X] = f[8 * X];
+      for (int X = 0; X <= I2; ++X) fr[X] = f[8 * X];
+#pragma unroll
+      for (int J = 0; J <= I1; ++J) dmma(acc[J], fr[I1], fr[J]);
+      if (I2 != I1) {
+#pragma unroll
+        for (int J = 0; J <= I2; ++J) dmma(acc[I1 + 1 + J], fr[I2], fr[J]);
+      }
+    }
+    return;
+  }
+  if (grp >= nk4) return;
+  // the fragments of the next step are loaded while this step's MMAs issue
+  double fr[I2 + 1], fn[I2 + 1];
+#pragma unroll
+  for (int X = 0; X <= I2; ++X) fr[X] = fb[4 * grp * stride_d + 8 * X];
+  for (int k4 = grp; k4 < nk4; k4 += kgw) {
+    const int kn = k4 + kgw;
+    if (kn < nk4) {
+      const double* f = fb + 4 * kn * stride_d;
+#pragma unroll
+      for (int X = 0; X <= I2; ++X) fn[X] = f[8 * X];
+    }
 #pragma unroll
     for (int J = 0; J <= I1; ++J) dmma(acc[J], fr[I1], fr[J]);
     if (I2 != I1) {
 #pragma unroll
       for (int J = 0; J <= I2; ++J) dmma(acc[I1 + 1 + J], fr[I2], fr[J]);
     }
+#pragma unroll
+    for (int X = 0; X <= I2; ++X) fr[X] = fn[X];
   }
 }
 
