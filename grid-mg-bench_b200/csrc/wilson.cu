@@ -353,18 +353,16 @@ constexpr int kTileSites = 16;
 // the nsel sites of the list `sel` (all V sites when null) and only those are
 // written; hskip (per site, bit p: leave hop p out) restricts the hops to
 // neighbours of the same block parity (see wilson_site).
-// bz > 0 (L0 a multiple of kTileSites, all sites): tile k of the loop is the
-// k-th in (z / bz, t, z mod bz, y, x) order, so that the records tiles share
-// with their t and z neighbours are still in L2 when those are processed.
-// PF: the neighbour records are software-pipelined (see wilson_site).
+// PF: the neighbour records are software-pipelined (see wilson_site).  (A
+// z-blocked tile order, as the staged kernel uses, measured no different here:
+// 2.73-2.79 ms at 32^4 x 24 RHS FP32 for z blocks of 1 to 32 planes.)
 template <class T, bool DOTS, int MINB, bool SEL = false, int VEC = 1, bool PF = false>
 __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
     const typename wt<T>::C* __restrict__ hop, const typename wt<T>::C* __restrict__ clover,
     const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
     typename wt<T>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
     int apbc, int tvol, int Lt, double2* __restrict__ d1, double2* __restrict__ d2,
-    const int32_t* __restrict__ sel = nullptr, int nsel = 0, const uint8_t* __restrict__ hskip = nullptr,
-    int L0 = 0, int L1 = 0, int bz = 0) {
+    const int32_t* __restrict__ sel = nullptr, int nsel = 0, const uint8_t* __restrict__ hskip = nullptr) {
   typedef typename wt<T>::C C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* Ls = reinterpret_cast<C*>(smem_raw);  // [kTileSites][8][9]: p < 4 U_mu(x), p >= 4 U_mu(x - mu)^dagger
@@ -378,19 +376,7 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
   const bool two = nrhs <= 2 * rt;
   double da[3] = {0.0, 0.0, 0.0}, db[3] = {0.0, 0.0, 0.0};
   for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
-    int s0 = tile * kTileSites;
-    if ((!SEL || !sel) && bz > 0) {
-      int k = tile;
-      const int nxt = L0 / kTileSites;
-      const int xt = k % nxt;
-      k /= nxt;
-      const int y = k % L1;
-      k /= L1;
-      const int zi = k % bz;
-      k /= bz;
-      const int t = k % Lt, z = (k / Lt) * bz + zi;
-      s0 = xt * kTileSites + L0 * (y + L1 * z) + tvol * t;
-    }
+    const int s0 = tile * kTileSites;
     const int ns = min(kTileSites, nsites - s0);
     __syncthreads();
     if (!SEL) {
@@ -1244,7 +1230,7 @@ static int pipe_bz(const gmg_wilson* h, int64_t rec_bytes, double budget) {
 template <bool DOTS>
 static gmg_status launch_pipe(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs, const void* in,
                               void* out, double2* d1, double2* d2, cudaStream_t s, bool* launched,
-                              const uint8_t* hskip = nullptr, int bz_scale = 1) {
+                              const uint8_t* hskip = nullptr) {
   *launched = false;
   if (((uintptr_t)in | (uintptr_t)out) & 15) return GMG_OK;
   const bool f32 = vec_prec == GMG_F32;
@@ -1252,9 +1238,7 @@ static gmg_status launch_pipe(gmg_wilson* h, int op, int dir, int disp, int vec_
   const int cmax = f32 ? PipeCfg<float>::CMAX : PipeCfg<double>::CMAX;
   const int nch = (nrhs + cmax - 1) / cmax, ch = (nrhs + nch - 1) / nch;
   const int64_t rec = (int64_t)nrhs * 12 * (f32 ? sizeof(float2) : sizeof(double2));
-  int bz = pipe_bz(h, rec, 48.0 * 1024 * 1024);
-  for (int k = 1; k < bz_scale; k *= 2)
-    if (bz * 2 <= h->dims.d[2] && h->dims.d[2] % (bz * 2) == 0) bz *= 2;
+  const int bz = pipe_bz(h, rec, 48.0 * 1024 * 1024);
   const gmg_wilson::PipePlan* plan = nullptr;
   GMG_TRY(build_pipe_plan(h, bz, s, &plan));
   if (plan->smax == 0) return GMG_OK;
@@ -1398,9 +1382,6 @@ static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_
   const size_t dots = DOTS ? sizeof(double) * 3 * (size_t)nrhs : 0;
   // 32-byte record accesses when both fields are 32-byte aligned
   const bool v32 = ((((uintptr_t)in | (uintptr_t)out) & 31) == 0);
-  // tile order in z blocks (rows of whole tiles only)
-  const int64_t rec = (int64_t)nrhs * 12 * (vec_prec == GMG_F64 ? sizeof(double2) : sizeof(float2));
-  const int bz = (h->dims.d[0] % kTileSites == 0) ? pipe_bz(h, rec, 48.0 * 1024 * 1024) : 0;
   auto go = [&](auto kern, auto diag, const void* hp, const void* cp, size_t csize) -> gmg_status {
     typedef decltype(diag) T;
     typedef typename wt<T>::C C;
@@ -1409,7 +1390,7 @@ static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_
     kern<<<g, kTileSites * rt, smem, s>>>(reinterpret_cast<const C*>(hp), reinterpret_cast<const C*>(cp),
                                           h->nbr.as<int32_t>(), reinterpret_cast<const C*>(in),
                                           reinterpret_cast<C*>(out), V, nrhs, rt, diag, op, dir, disp, h->apbc, tvol,
-                                          h->dims.d[3], d1, d2, nullptr, 0, nullptr, h->dims.d[0], h->dims.d[1], bz);
+                                          h->dims.d[3], d1, d2, nullptr, 0, nullptr);
     return GMG_OK;
   };
   if (vec_prec == GMG_F64) {
@@ -1665,8 +1646,7 @@ gmg_status wilson_apply_face(gmg_wilson* h, int p, int nrhs, const double* in, d
 
 // the tile kernel's SEL instance (FP64): op on the nsel sites of `sel` (all
 // sites when null), hops restricted by hskip; with all sites and 32-byte
-// aligned fields, 32-byte record accesses and the z-block tile order (the
-// prefetching form spills here)
+// aligned fields, 32-byte record accesses (the prefetching form spills here)
 static gmg_status launch_tile_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, const double* in, double* out,
                                   const int32_t* sel, int nsel, const uint8_t* hskip, cudaStream_t s) {
   const int V = (int)h->dims.vol();
@@ -1683,15 +1663,11 @@ static gmg_status launch_tile_sel(gmg_wilson* h, int op, int dir, int disp, int 
   const int g = std::min(tiles, 148 * 16);
   const size_t smem = sizeof(double2) * 2 * kTileSites * 72;
   const bool fast = !sel && ((((uintptr_t)in | (uintptr_t)out) & 31) == 0);
-  const int bz = (fast && h->dims.d[0] % kTileSites == 0)
-                     ? pipe_bz(h, (int64_t)nrhs * 12 * sizeof(double2), 48.0 * 1024 * 1024)
-                     : 0;
   auto k = fast ? wilson_tile_kernel<double, false, 2, true, 2> : wilson_tile_kernel<double, false, 2, true>;
   if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k<<<g, kTileSites * rt, smem, s>>>(h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(),
                                      (const double2*)in, (double2*)out, V, nrhs, rt, 4.0 + h->mass, op, dir, disp,
-                                     h->apbc, tvol, h->dims.d[3], nullptr, nullptr, sel, nsel, hskip, h->dims.d[0],
-                                     h->dims.d[1], bz);
+                                     h->apbc, tvol, h->dims.d[3], nullptr, nullptr, sel, nsel, hskip);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
