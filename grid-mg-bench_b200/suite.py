@@ -350,26 +350,42 @@ def profile_rows(rows):
         torch.cuda.synchronize()
         line("p_ortho orthonormalise 16^4, nbasis 32, 4^4 blocks", ok=True, max_err=ag.CheckOrthogonal())
     if "p_w" in rows:
-        # the two fine-operator forms of the C5 solve at 24 RHS: M with the fused
-        # MR products in FP32 (smoother) and M in FP64 (outer FGMRES); the first
-        # call of each tunes the kernel variant, the calls inside the NVTX range
-        # "p_w" run the tuned kernels once each
+        # the fine-operator forms of the C5 solve at 24 RHS: M in FP32, M with the
+        # fused MR products in FP32 (smoother) and M in FP64 (outer FGMRES).  The
+        # first call of each tunes the kernel variant; the calls inside the NVTX
+        # range "p_w" run the tuned kernels once each, those inside "p_w_staged"
+        # the pipelined staged kernel (forced) in FP32 and FP64
         U = inputs.torch_smooth_gauge(fd, 613, 0.3)
         w = gmg.WilsonClover(fd, -0.35, 1.0, antiperiodic=True)
         w.set_gauge(U)
+        del U
         x = inputs.torch_gaussian((Vf, 24, 12), 614)
         y = torch.zeros_like(x)
         x32, y32 = x.to(torch.complex64), y.to(torch.complex64)
-        w.M_mr(x32, y32)
-        w.M(x, y)
+        for _ in range(2):
+            w.M(x32, y32)
+            w.M_mr(x32, y32)
+            w.M(x, y)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("p_w")
+        w.M(x32, y32)
         w.M_mr(x32, y32)
         w.M(x, y)
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
-        line("p_w Wilson-clover 16^4, 24 RHS: FP32 M with MR products, FP64 M", ok=True,
-             tuned={"f32_mr": w.tuned_kernel("f32", 24, fused_mr=True), "f64": w.tuned_kernel("f64", 24)})
+        w.set_kernel("staged")
+        w.M(x32, y32)
+        w.M(x, y)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("p_w_staged")
+        w.M(x32, y32)
+        w.M(x, y)
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        w.set_kernel("auto")
+        line("p_w Wilson-clover 16^4, 24 RHS: FP32 M, FP32 M with MR products, FP64 M; staged FP32 / FP64 M",
+             ok=True, tuned={"f32": w.tuned_kernel("f32", 24), "f32_mr": w.tuned_kernel("f32", 24, fused_mr=True),
+                             "f64": w.tuned_kernel("f64", 24)})
     if "p_c4" in rows:
         # CoarsenOperator 16^4 -> 4^4, nbasis 40 (the C4 construction on a
         # sixteenth of its volume): two calls, each with 4 face hops, one
