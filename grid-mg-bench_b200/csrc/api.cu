@@ -405,6 +405,15 @@ gmg_status gmg_wilson_apply(gmg_wilson* h, gmg_op op, int dir, int disp, gmg_pre
   return wilson_apply(h, op, dir, disp, vec_prec, nrhs, in, out, S(s));
 }
 
+gmg_status gmg_wilson_apply_f32_in(gmg_wilson* h, gmg_op op, int nrhs, const float* in, double* out,
+                                   gmg_stream s) {
+  GMG_CHECK(h && in && out, GMG_ERR_ARGUMENT, "gmg_wilson_apply_f32_in: null argument");
+  GMG_CHECK(h->gauge_set, GMG_ERR_STATE, "gmg_wilson_apply_f32_in: gauge not set");
+  GMG_CHECK(nrhs >= 1 && nrhs <= 1024, GMG_ERR_ARGUMENT, "gmg_wilson_apply_f32_in: nrhs out of range");
+  GMG_CHECK(op == GMG_OP_M || op == GMG_OP_MDAG, GMG_ERR_ARGUMENT, "gmg_wilson_apply_f32_in: op must be M or Mdag");
+  return wilson_apply_f32_in(h, op, nrhs, in, out, S(s));
+}
+
 gmg_status gmg_wilson_set_kernel(gmg_wilson* h, gmg_wilson_kernel k) {
   GMG_CHECK(h != nullptr, GMG_ERR_ARGUMENT, "gmg_wilson_set_kernel: null handle");
   GMG_CHECK(k >= GMG_WILSON_AUTO && k <= GMG_WILSON_STAGED, GMG_ERR_ARGUMENT, "gmg_wilson_set_kernel: bad kernel");

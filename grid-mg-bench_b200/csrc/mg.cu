@@ -95,6 +95,19 @@ namespace gmg {
 namespace {
 
 // ------------------------------------------------------------- small helpers
+gmg_status apply_op(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s);
+
+// out = A in with in in the preconditioner precision and out in FP64: on the
+// fine level the FP64 operator reads the FP32 field directly; elsewhere `in`
+// is converted into t (FP64) first
+gmg_status apply_op_mixed(gmg_mg* h, int l, const Vec& in, Vec& t, Vec& out, cudaStream_t s) {
+  if (l == 0 && in.prec == GMG_F32 && out.prec == GMG_F64)
+    return gmg_wilson_apply_f32_in(h->L[0]->w, GMG_OP_M, in.R, static_cast<const float*>(in.p),
+                                   static_cast<double*>(out.p), (gmg_stream)s);
+  GMG_TRY(vec_convert(in, t, s));
+  return apply_op(h, l, t, out, s);
+}
+
 gmg_status apply_op(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s) {
   MGLevel& L = *h->L[l];
   if (l == 0) return gmg_wilson_apply(L.w, GMG_OP_M, 0, 0, (gmg_prec)in.prec, in.R, in.p, out.p, (gmg_stream)s);
@@ -366,8 +379,7 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
         GMG_CUDA(cudaMemsetAsync(zj.p, 0, zj.bytes(), s));
         GMG_TRY(vec_scatter(zc, drop->idx, zj, s));
         if (zc.prec != wc.prec) {
-          GMG_TRY(vec_convert(zc, vc, s));
-          GMG_TRY(apply_op(h, l, vc, wc, s));
+          GMG_TRY(apply_op_mixed(h, l, zc, vc, wc, s));
         } else {
           GMG_TRY(apply_op(h, l, zc, wc, s));
         }
@@ -376,8 +388,7 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
       } else {
         if (flexible) GMG_TRY(prec(vj, zj, tz));
         if (zj.prec != w.prec) {
-          GMG_TRY(vec_convert(zj, t, s));
-          GMG_TRY(apply_op(h, l, t, w, s));
+          GMG_TRY(apply_op_mixed(h, l, zj, t, w, s));
         } else {
           GMG_TRY(apply_op(h, l, zj, w, s));
         }

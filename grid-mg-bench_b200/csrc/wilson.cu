@@ -190,14 +190,28 @@ __device__ __forceinline__ void st12(typename wt<T>::C* __restrict__ p, const ty
   }
 }
 
+// a record of input type TI read as T: FP32 records promoted exactly to FP64
+// on load (the FP64 operator applied to FP32 vectors)
+template <class T, class TI, int VEC>
+__device__ __forceinline__ void ld12x(typename wt<T>::C v[12], const typename wt<TI>::C* __restrict__ p) {
+  if (sizeof(TI) == sizeof(T)) {
+    ld12<T, VEC>(v, reinterpret_cast<const typename wt<T>::C*>(p));
+  } else {
+    float2 f[12];
+    ld12<float, VEC>(f, reinterpret_cast<const float2*>(p));
+#pragma unroll
+    for (int k = 0; k < 12; ++k) v[k] = typename wt<T>::C{(T)f[k].x, (T)f[k].y};
+  }
+}
+
 // DOTS (op M or MDAG): also add <out, in> and <out, out> of this (site, r) to
 // dsum[0..1] and dsum[2].  VEC: 16-byte spinor accesses.  skip: hops p with
 // bit p set are left out (0 for the plain operator); with the bits of the
 // hops to blocks of the other parity this gives e D e + o D o of the
 // coarsening's self term in one pass.
-template <class T, class LinkFn, bool DOTS = false, int VEC = 0, bool LDAG = false, bool PF = false>
+template <class T, class LinkFn, bool DOTS = false, int VEC = 0, bool LDAG = false, bool PF = false, class TI = T>
 __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict__ cl, LinkFn links,
-                                            const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
+                                            const int32_t* __restrict__ nbr, const typename wt<TI>::C* __restrict__ in,
                                             typename wt<T>::C* __restrict__ out, int V, int nrhs, int site, int r,
                                             T diag, int op, int dir, int disp, int apbc, int tvol, int Lt,
                                             double* dsum = nullptr, int skip = 0) {
@@ -219,8 +233,8 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
 #pragma unroll
     for (int p = 0; p < 8; ++p) nbs[p] = nbr[(int64_t)p * V + site];
     C psi[12], nxt[12];
-    ld12<T, VEC>(psi, in + ((int64_t)site * nrhs + r) * 12);
-    ld12<T, VEC>(nxt, in + ((int64_t)nbs[0] * nrhs + r) * 12);
+    ld12x<T, TI, VEC>(psi, in + ((int64_t)site * nrhs + r) * 12);
+    ld12x<T, TI, VEC>(nxt, in + ((int64_t)nbs[0] * nrhs + r) * 12);
 #pragma unroll
     for (int k = 6; k < 12; ++k)
       if (g5) psi[k] = C{-psi[k].x, -psi[k].y};
@@ -242,7 +256,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
       C cur[12];
 #pragma unroll
       for (int k = 0; k < 12; ++k) cur[k] = nxt[k];
-      if (p < 7) ld12<T, VEC>(nxt, in + ((int64_t)nbs[p < 7 ? p + 1 : 7] * nrhs + r) * 12);
+      if (p < 7) ld12x<T, TI, VEC>(nxt, in + ((int64_t)nbs[p < 7 ? p + 1 : 7] * nrhs + r) * 12);
       if (skip & (1 << p)) continue;
       T coef = (T)-0.5;
       if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
@@ -256,7 +270,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
   if (op != GMG_OP_MDIR) {
     // diagonal: (4 + m) psi + Cl psi, two chiral 6x6 blocks
     C psi[12];
-    ld12<T, VEC>(psi, in + ((int64_t)site * nrhs + r) * 12);
+    ld12x<T, TI, VEC>(psi, in + ((int64_t)site * nrhs + r) * 12);
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
       if (g5 && k >= 6) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
@@ -284,7 +298,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
       T coef = (T)-0.5;
       if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
       C psi[12];
-      ld12<T, VEC>(psi, in + ((int64_t)nb * nrhs + r) * 12);
+      ld12x<T, TI, VEC>(psi, in + ((int64_t)nb * nrhs + r) * 12);
       if (g5) {
 #pragma unroll
         for (int k = 6; k < 12; ++k) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
@@ -298,7 +312,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
   C ov[12];
   // the input record again for the products (re-read rather than kept live
   // through the hops: registers decide the occupancy of this kernel)
-  if (DOTS) ld12<T, VEC>(cin, in + ((int64_t)site * nrhs + r) * 12);
+  if (DOTS) ld12x<T, TI, VEC>(cin, in + ((int64_t)site * nrhs + r) * 12);
 #pragma unroll
   for (int s = 0; s < 4; ++s)
 #pragma unroll
@@ -356,10 +370,12 @@ constexpr int kTileSites = 16;
 // PF: the neighbour records are software-pipelined (see wilson_site).  (A
 // z-blocked tile order, as the staged kernel uses, measured no different here:
 // 2.73-2.79 ms at 32^4 x 24 RHS FP32 for z blocks of 1 to 32 planes.)
-template <class T, bool DOTS, int MINB, bool SEL = false, int VEC = 1, bool PF = false>
+// TI: the input vectors' precision (float with T = double: the FP64 operator
+// on FP32 vectors, promoted on load).
+template <class T, bool DOTS, int MINB, bool SEL = false, int VEC = 1, bool PF = false, class TI = T>
 __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
     const typename wt<T>::C* __restrict__ hop, const typename wt<T>::C* __restrict__ clover,
-    const int32_t* __restrict__ nbr, const typename wt<T>::C* __restrict__ in,
+    const int32_t* __restrict__ nbr, const typename wt<TI>::C* __restrict__ in,
     typename wt<T>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
     int apbc, int tvol, int Lt, double2* __restrict__ d1, double2* __restrict__ d2,
     const int32_t* __restrict__ sel = nullptr, int nsel = 0, const uint8_t* __restrict__ hskip = nullptr) {
@@ -402,7 +418,7 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
       int k = 0;
       for (int r = rl; r < nrhs; r += rt, ++k) {
         double dt[3] = {0.0, 0.0, 0.0};
-        wilson_site<T, decltype(links), DOTS, VEC, true, PF>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op,
+        wilson_site<T, decltype(links), DOTS, VEC, true, PF, TI>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op,
                                                     dir, disp, apbc, tvol, Lt, dt, skip);
         if (DOTS) {
           if (two) {
@@ -1731,6 +1747,44 @@ gmg_status wilson_apply_sel(gmg_wilson* h, int op, int dir, int disp, int nrhs, 
   GMG_TRY(run(pick, &launched));
   if (!launched) GMG_TRY(run(1, &launched));
   return GMG_OK;
+}
+
+// out (FP64) = op in (FP32), op M or MDAG, in FP64 arithmetic on the FP32
+// records promoted exactly on load: the same result as converting `in` to FP64
+// and applying the FP64 operator, without the converted copy (the outer
+// Arnoldi step's apply to a preconditioned direction).  The tile kernel at 2
+// CTAs per SM with the records prefetched.
+gmg_status wilson_apply_f32_in(gmg_wilson* h, int op, int nrhs, const float* in, double* out, cudaStream_t s) {
+  GMG_CHECK(op == GMG_OP_M || op == GMG_OP_MDAG, GMG_ERR_UNSUPPORTED,
+            "wilson apply (FP32 in, FP64 out): op must be M or Mdag");
+  GMG_CHECK(nrhs >= 1, GMG_ERR_ARGUMENT, "wilson apply (FP32 in, FP64 out): nrhs must be positive");
+  const int V = (int)h->dims.vol();
+  const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
+  int rt = 1;
+  for (int c = std::min(nrhs, 16); c >= 1; --c)
+    if (nrhs % c == 0) {
+      rt = c;
+      break;
+    }
+  if (nrhs > 16 && rt < 8) rt = 16;
+  const int tiles = (V + kTileSites - 1) / kTileSites;
+  const int g = std::min(tiles, 148 * 16);
+  const size_t smem = sizeof(double2) * 2 * kTileSites * 72;
+  const uintptr_t al = (uintptr_t)in | (uintptr_t)out;
+  KernelTimer kt("wilson", s);
+  auto go = [&](auto kern) -> gmg_status {
+    if (smem > 48 * 1024)
+      GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<g, kTileSites * rt, smem, s>>>(h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(),
+                                          reinterpret_cast<const float2*>(in), reinterpret_cast<double2*>(out), V,
+                                          nrhs, rt, 4.0 + h->mass, op, 0, 0, h->apbc, tvol, h->dims.d[3], nullptr,
+                                          nullptr, nullptr, 0, nullptr);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  };
+  if ((al & 31) == 0) return go(wilson_tile_kernel<double, false, 2, false, 2, true, float>);
+  if ((al & 15) == 0) return go(wilson_tile_kernel<double, false, 2, false, 1, true, float>);
+  return go(wilson_tile_kernel<double, false, 2, false, 0, true, float>);
 }
 
 gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs,

@@ -408,6 +408,15 @@ class WilsonClover:
         st = lib().gmg_wilson_device_error(self._h, ctypes.byref(code))
         return st, code.value
 
+    def M_f32_in(self, inp, out, dag=False):
+        """out (complex128) = M in (or Mdag) with in complex64: FP64 arithmetic on the promoted input."""
+        assert inp.dtype == torch.complex64 and out.dtype == torch.complex128
+        _check_vec(inp, self.V, 12, "in")
+        _check_vec(out, self.V, 12, "out")
+        _chk(lib().gmg_wilson_apply_f32_in(self._h, OP_MDAG if dag else OP_M, inp.shape[1], _ptr(inp), _ptr(out),
+                                           _stream()))
+        return out
+
     def M_mr(self, inp, out):
         """out = M inp and the MR-step inner products <out, inp>, <out, out> per RHS."""
         _check_vec(inp, self.V, 12, "in")

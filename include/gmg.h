@@ -268,6 +268,13 @@ gmg_status gmg_wilson_get_clover(gmg_wilson* h, double* clover, int on_device, g
 /* op M / Mdag / Mdiag / Mdir(dir, disp); fields [V][nrhs][12] of vec_prec (F64/F32). */
 gmg_status gmg_wilson_apply(gmg_wilson* h, gmg_op op, int dir, int disp, gmg_prec vec_prec,
                             int nrhs, const void* in, void* out, gmg_stream s);
+/* op M / Mdag in FP64 arithmetic on an FP32 input field, FP64 output: the same
+   result as converting in to FP64 and calling gmg_wilson_apply, without the
+   converted copy (the FP32 records are promoted exactly on load).  The outer
+   FGMRES applies the operator to its FP32 preconditioned directions this way.
+   No counterpart (Grid converts between precisions with precisionChange). */
+gmg_status gmg_wilson_apply_f32_in(gmg_wilson* h, gmg_op op, int nrhs, const float* in, double* out,
+                                   gmg_stream s);
 /* out = M in together with the minimal-residual inner products of the MR
    smoother step (the smoother solve of include/MultigridPreconditioner.h:
    264-301): d1[r] = <out_r, in_r>,

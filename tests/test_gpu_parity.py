@@ -584,3 +584,23 @@ def test_coarsen_coarse_matches_oracle(coarsen_setup):
     got = cm.get_links()
     for p in range(9):
         assert orc.rel_dev_sq(ref[p], got[p]) < TOL64, p
+
+
+@pytest.mark.parametrize("nrhs", [1, 5, 24])
+@pytest.mark.parametrize("dag", [False, True])
+def test_wilson_f32_input_matches_converted_f64_apply(wil, forced, nrhs, dag):
+    # the FP64 operator on an FP32 field, promoted on load, is bit for bit the
+    # FP64 tile kernel on the field converted to FP64 (same kernel, same order
+    # of operations), and within the FP64 bound of the oracle on that field
+    dims, U, cl, w = wil
+    forced("tile")
+    x32 = dev(inputs.gaussian_field((512, nrhs, 12), inputs.rng(stream=190 + nrhs)), torch.complex64)
+    x64 = x32.to(torch.complex128)
+    want = torch.zeros_like(x64)
+    (w.Mdag if dag else w.M)(x64, want)
+    got = torch.zeros_like(x64)
+    w.M_f32_in(x32, got, dag=dag)
+    torch.cuda.synchronize()
+    assert torch.equal(want, got)
+    ref = orc.wilson_clover(dims, U, cl, -0.1, 1, host(x64), orc.OP_MDAG if dag else orc.OP_M)
+    assert orc.rel_dev_sq(ref, host(got)) < TOL64
