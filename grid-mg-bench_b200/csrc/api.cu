@@ -452,7 +452,10 @@ gmg_status gmg_wilson_apply_mr(gmg_wilson* h, gmg_prec vec_prec, int nrhs, const
   GMG_CHECK(in != out, GMG_ERR_ARGUMENT, "gmg_wilson_apply_mr: in and out must not alias");
   GMG_CHECK(h->gauge_set, GMG_ERR_STATE, "gmg_wilson_apply_mr: gauge not set");
   GMG_CHECK(nrhs >= 1 && nrhs <= 1024, GMG_ERR_ARGUMENT, "gmg_wilson_apply_mr: nrhs out of range");
-  GMG_CHECK(vec_prec_ok(vec_prec), GMG_ERR_ARGUMENT, "gmg_wilson_apply_mr: vectors must be F64 or F32");
+  if (vec_prec == GMG_BF16)
+    return wilson_apply_mr_bf16(h, nrhs, static_cast<const uint32_t*>(in), static_cast<uint32_t*>(out), (double2*)d1,
+                                (double2*)d2, S(s));
+  GMG_CHECK(vec_prec_ok(vec_prec), GMG_ERR_ARGUMENT, "gmg_wilson_apply_mr: vectors must be F64, F32 or BF16");
   return wilson_apply_mr(h, vec_prec, nrhs, in, out, (double2*)d1, (double2*)d2, S(s));
 }
 

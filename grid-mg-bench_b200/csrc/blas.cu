@@ -8,6 +8,8 @@
 #include <algorithm>
 #include <type_traits>
 
+#include <cuda_bf16.h>
+
 #include "mg_internal.cuh"
 
 namespace gmg {
@@ -427,6 +429,47 @@ __global__ void __launch_bounds__(1024) mr_update_row_kernel(const double2* __re
   }
 }
 
+__device__ __forceinline__ float2 bf16w_to_f2(uint32_t w) {
+  return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+}
+__device__ __forceinline__ uint32_t f2_to_bf16w(float re, float im) {
+  const __nv_bfloat162 b = __floats2bfloat162_rn(re, im);
+  return *reinterpret_cast<const uint32_t*>(&b);
+}
+
+// the MR step on BF16 residual fields: x (FP32) += a r; r = bf16(r - a Ar)
+__global__ void __launch_bounds__(1024) mr_update_bf16_row_kernel(const double2* __restrict__ d1,
+                                                                  const double2* __restrict__ d2,
+                                                                  float2* __restrict__ x, uint32_t* __restrict__ rr_,
+                                                                  const uint32_t* __restrict__ Ar, int64_t V, int R,
+                                                                  int dof, int spb, bool update_r) {
+  const int RD = R * dof, t = threadIdx.x;
+  if (t >= spb * RD) return;
+  const int so = t / RD, i = t % RD, k = i / dof;
+  const double den = d2[k].x;
+  const float ar = den > 0.0 ? (float)(d1[k].x / den) : 0.f, ai = den > 0.0 ? (float)(d1[k].y / den) : 0.f;
+  for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+    const int64_t e = s * RD + i;
+    const float2 r = bf16w_to_f2(rr_[e]);
+    float2 xv = x[e];
+    xv.x += ar * r.x - ai * r.y;
+    xv.y += ar * r.y + ai * r.x;
+    x[e] = xv;
+    if (update_r) {
+      const float2 q = bf16w_to_f2(Ar[e]);
+      rr_[e] = f2_to_bf16w(r.x - (ar * q.x - ai * q.y), r.y - (ar * q.y + ai * q.x));
+    }
+  }
+}
+
+__global__ void xmy_bf16_kernel(const float2* __restrict__ X, const float2* __restrict__ Y, uint32_t* __restrict__ Z,
+                                int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const float2 a = X[e], b = Y[e];
+    Z[e] = f2_to_bf16w(a.x - b.x, a.y - b.y);
+  }
+}
+
 // Y(r) = a[r] X(r) + b[r] Y(r)
 template <class T>
 __global__ void __launch_bounds__(1024) axpby_row_kernel(const double2* __restrict__ a,
@@ -719,6 +762,16 @@ gmg_status vec_multiaxpy_dot(const double2* a_dev, const Vec& X0, int nx, int64_
 
 gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s,
                          bool update_r) {
+  if (r.prec == GMG_BF16) {
+    GMG_CHECK(x.prec == GMG_F32 && Ar.prec == GMG_BF16 && x.R * x.dof <= 1024, GMG_ERR_UNSUPPORTED,
+              "mr update: BF16 residuals need an FP32 solution and at most 1024 values per site");
+    const blas::Row rg = blas::row_geom(x.V, x.R, x.dof);
+    blas::mr_update_bf16_row_kernel<<<rg.grid, rg.threads, 0, s>>>(d1, d2, (float2*)x.p, (uint32_t*)r.p,
+                                                                  (const uint32_t*)Ar.p, x.V, x.R, x.dof, rg.spb,
+                                                                  update_r);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  }
   if (x.R * x.dof <= 1024) {
     const blas::Row rg = blas::row_geom(x.V, x.R, x.dof);
     if (x.prec == GMG_F64)
@@ -746,6 +799,15 @@ gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s) {
   const int g = blas::grid1(n);
   if (Y.prec == GMG_F64) blas::xmy_kernel<double><<<g, 256, 0, s>>>((const double2*)X.p, (double2*)Y.p, n);
   else blas::xmy_kernel<float><<<g, 256, 0, s>>>((const float2*)X.p, (float2*)Y.p, n);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status vec_xmy_bf16(const Vec& X, const Vec& Y, Vec& Z, cudaStream_t s) {
+  GMG_CHECK(X.prec == GMG_F32 && Y.prec == GMG_F32 && Z.prec == GMG_BF16, GMG_ERR_UNSUPPORTED,
+            "xmy to BF16: FP32 operands and a BF16 result");
+  const int64_t n = Z.elems();
+  blas::xmy_bf16_kernel<<<blas::grid1(n), 256, 0, s>>>((const float2*)X.p, (const float2*)Y.p, (uint32_t*)Z.p, n);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }

@@ -36,12 +36,14 @@ struct MGLevel {
   int dof = 0;
   int vprec = GMG_F64;    // vector precision inside the preconditioner
   int compute = GMG_F64;  // coarse-operator compute form (F64, F32, BF16)
+  bool bf16_smoother = false;  // level 0: the MR smoother's residual fields in BF16
   gmg_wilson* w = nullptr;  // level 0 (not owned)
   gmg_coarse* c = nullptr;  // level > 0 (owned)
   gmg_agg* agg = nullptr;   // aggregation to level l+1 (owned)
   int m = 0;                // Krylov restart of the solver that runs on this level
   VecBuf V0, Z0, kw, kt;    // Krylov basis (m+1), flexible directions (m), temporaries
   VecBuf mr_r, mr_Ar, mr_t; // MR smoother
+  VecBuf mr_r16, mr_Ar16;    // the fine smoother's residual fields in BF16 (params.smoother_bf16)
   VecBuf bc, xc;            // right-hand side / solution of this level inside the cycle above
   VecBuf tv;                // test vectors (nvec[l]) the basis to level l+1 is built from
   // device state of this level's solver inside a captured K-cycle: Hessenberg
@@ -280,6 +282,18 @@ gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStre
   double2* d1 = h->dscr.as<double2>() + kScalars / 2;  // above the Krylov scalars
   double2* d2 = d1 + R;
   GMG_TRY(apply_op(h, l, x, r, s));
+  if (l == 0 && L.bf16_smoother && x.prec == GMG_F32) {
+    // the residual and the operator product kept in BF16 (FP32 arithmetic,
+    // FP32 solution): the smoother's sweeps move half the bytes
+    Vec r16 = L.mr_r16.with_rhs(R), Ar16 = L.mr_Ar16.with_rhs(R);
+    GMG_TRY(vec_xmy_bf16(b, r, r16, s));  // r = b - A x
+    for (int it = 0; it < iters; ++it) {
+      GMG_TRY(wilson_apply_mr_bf16(L.w, R, static_cast<const uint32_t*>(r16.p), static_cast<uint32_t*>(Ar16.p), d1,
+                                   d2, s));
+      GMG_TRY(vec_mr_update(d1, d2, x, r16, Ar16, s, it + 1 < iters));
+    }
+    return GMG_OK;
+  }
   GMG_TRY(vec_xmy(b, r, s));  // r = b - A x
   for (int it = 0; it < iters; ++it) {
     if (l == 0) {
@@ -880,6 +894,10 @@ gmg_status alloc_level_ws(MGLevel& L, int R, bool krylov, bool flexible) {
   GMG_TRY(L.mr_r.alloc(L.V, R, L.dof, p));
   GMG_TRY(L.mr_Ar.alloc(L.V, R, L.dof, p));
   GMG_TRY(L.mr_t.alloc(L.V, R, L.dof, p));
+  if (L.l == 0 && L.bf16_smoother) {
+    GMG_TRY(L.mr_r16.alloc(L.V, R, L.dof, GMG_BF16));
+    GMG_TRY(L.mr_Ar16.alloc(L.V, R, L.dof, GMG_BF16));
+  }
   if (L.l > 0) {
     GMG_TRY(L.bc.alloc(L.V, R, L.dof, p));
     GMG_TRY(L.xc.alloc(L.V, R, L.dof, p));
@@ -1021,6 +1039,7 @@ extern "C" gmg_status gmg_mg_params_default(gmg_mg_params* p) {
   p->refine_iters[0] = p->refine_iters[1] = 0;
   p->recursive_updates = 1;
   p->drop_in_cycle = 1;
+  p->smoother_bf16 = -1;
   return GMG_OK;
 }
 
@@ -1045,6 +1064,8 @@ extern "C" gmg_status gmg_mg_create(gmg_wilson* fine, const gmg_mg_params* p, in
     L->dof = dof;
     L->vprec = p->prec == GMG_F64 ? GMG_F64 : GMG_F32;
     L->compute = p->prec == GMG_BF16 && l > 0 ? GMG_BF16 : L->vprec;
+    L->bf16_smoother = l == 0 && L->vprec == GMG_F32 &&
+                       (p->smoother_bf16 > 0 || (p->smoother_bf16 < 0 && p->prec == GMG_BF16));
     L->w = l == 0 ? fine : nullptr;
     h->L.push_back(L);
     if (l + 1 < p->nlevels) {

@@ -5,7 +5,9 @@
 
 namespace gmg {
 
-// A device field [V][R][dof] complex of precision prec (GMG_F64 / GMG_F32).
+// A device field [V][R][dof] complex of precision prec (GMG_F64 / GMG_F32; GMG_BF16
+// for the fine smoother's residual fields: one 32-bit word per complex number,
+// real part in the low 16 bits).
 struct Vec {
   void* p = nullptr;
   int64_t V = 0;
@@ -13,7 +15,7 @@ struct Vec {
   int dof = 0;
   int prec = GMG_F64;
   int64_t elems() const { return V * (int64_t)R * dof; }
-  size_t esize() const { return prec == GMG_F64 ? 16 : 8; }
+  size_t esize() const { return prec == GMG_F64 ? 16 : prec == GMG_BF16 ? 4 : 8; }
   size_t bytes() const { return (size_t)elems() * esize(); }
   // the first R' right-hand sides of a buffer laid out for R' RHS (compacted batches)
   Vec with_rhs(int r) const {
@@ -63,10 +65,13 @@ gmg_status vec_gaussian(Vec& X, uint64_t seed, cudaStream_t s);
 gmg_status vec_scale_inv_norm(const double2* n_dev, const Vec& X, Vec& Y, cudaStream_t s);
 // MR step with alpha = d1 / d2 (device): x += alpha r, r -= alpha Ar
 // x += a r, and r -= a Ar unless update_r is false, a = <Ar, r> / <Ar, Ar> per RHS
+// (r, Ar BF16 with x FP32: the products in FP32, r rounded back to BF16)
 gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s,
                          bool update_r = true);
 // Y = X - Y
 gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s);
+// Z (BF16) = X - Y (FP32), rounded to nearest even
+gmg_status vec_xmy_bf16(const Vec& X, const Vec& Y, Vec& Z, cudaStream_t s);
 // G[a][b] = <X(a), X(b)> over the whole lattice (R <= 32 columns), FP64
 gmg_status vec_gram(const Vec& X, double2* G_dev, cudaStream_t s);
 // X(a) <- sum_{b <= a} T[a][b] X(b)   (lower-triangular recombination of the columns)

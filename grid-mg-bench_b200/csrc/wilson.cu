@@ -17,6 +17,9 @@
 // per (site, rhs); the (1 -+ gamma) projection halves the colour-matrix work
 // (rank-2 projector: lower spins are a phase times the upper ones).
 #include <algorithm>
+#include <type_traits>
+
+#include <cuda_bf16.h>
 #include <vector>
 
 #include "async_copy.cuh"
@@ -27,6 +30,10 @@ namespace gmg {
 template <class T> struct wt;
 template <> struct wt<double> { typedef double2 C; };
 template <> struct wt<float> { typedef float2 C; };
+// BF16 storage of a complex number: one 32-bit word, real part in the low
+// 16 bits (the fine smoother's residual fields; arithmetic in FP32)
+struct bf16s {};
+template <> struct wt<bf16s> { typedef uint32_t C; };
 
 template <class C> __device__ __forceinline__ C cmul(C a, C b) {
   C r;
@@ -191,10 +198,21 @@ __device__ __forceinline__ void st12(typename wt<T>::C* __restrict__ p, const ty
 }
 
 // a record of input type TI read as T: FP32 records promoted exactly to FP64
-// on load (the FP64 operator applied to FP32 vectors)
+// on load (the FP64 operator applied to FP32 vectors), BF16 records (48 bytes,
+// three 16-byte loads) widened to FP32
 template <class T, class TI, int VEC>
 __device__ __forceinline__ void ld12x(typename wt<T>::C v[12], const typename wt<TI>::C* __restrict__ p) {
-  if (sizeof(TI) == sizeof(T)) {
+  if (std::is_same<TI, bf16s>::value) {
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const uint4 u = __ldg(q + k);
+      const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        v[4 * k + i] = typename wt<T>::C{(T)__uint_as_float(w[i] << 16), (T)__uint_as_float(w[i] & 0xffff0000u)};
+    }
+  } else if (sizeof(TI) == sizeof(T)) {
     ld12<T, VEC>(v, reinterpret_cast<const typename wt<T>::C*>(p));
   } else {
     float2 f[12];
@@ -204,15 +222,36 @@ __device__ __forceinline__ void ld12x(typename wt<T>::C v[12], const typename wt
   }
 }
 
+// a record of T written as TO (BF16: rounded to nearest even, three 16-byte stores)
+template <class T, class TO, int VEC>
+__device__ __forceinline__ void st12x(typename wt<TO>::C* __restrict__ p, const typename wt<T>::C v[12]) {
+  if (std::is_same<TO, bf16s>::value) {
+    uint4* q = reinterpret_cast<uint4*>(p);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      uint32_t w[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const __nv_bfloat162 b = __floats2bfloat162_rn((float)v[4 * k + i].x, (float)v[4 * k + i].y);
+        w[i] = *reinterpret_cast<const uint32_t*>(&b);
+      }
+      q[k] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  } else {
+    st12<T, VEC>(reinterpret_cast<typename wt<T>::C*>(p), v);
+  }
+}
+
 // DOTS (op M or MDAG): also add <out, in> and <out, out> of this (site, r) to
 // dsum[0..1] and dsum[2].  VEC: 16-byte spinor accesses.  skip: hops p with
 // bit p set are left out (0 for the plain operator); with the bits of the
 // hops to blocks of the other parity this gives e D e + o D o of the
 // coarsening's self term in one pass.
-template <class T, class LinkFn, bool DOTS = false, int VEC = 0, bool LDAG = false, bool PF = false, class TI = T>
+template <class T, class LinkFn, bool DOTS = false, int VEC = 0, bool LDAG = false, bool PF = false, class TI = T,
+          class TO = T>
 __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict__ cl, LinkFn links,
                                             const int32_t* __restrict__ nbr, const typename wt<TI>::C* __restrict__ in,
-                                            typename wt<T>::C* __restrict__ out, int V, int nrhs, int site, int r,
+                                            typename wt<TO>::C* __restrict__ out, int V, int nrhs, int site, int r,
                                             T diag, int op, int dir, int disp, int apbc, int tvol, int Lt,
                                             double* dsum = nullptr, int skip = 0) {
   typedef typename wt<T>::C C;
@@ -327,7 +366,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
         pn += v.x * v.x + v.y * v.y;
       }
     }
-  st12<T, VEC>(out + ((int64_t)site * nrhs + r) * 12, ov);
+  st12x<T, TO, VEC>(out + ((int64_t)site * nrhs + r) * 12, ov);
   if (DOTS) {
     dsum[0] += pr;
     dsum[1] += pi;
@@ -372,11 +411,11 @@ constexpr int kTileSites = 16;
 // 2.73-2.79 ms at 32^4 x 24 RHS FP32 for z blocks of 1 to 32 planes.)
 // TI: the input vectors' precision (float with T = double: the FP64 operator
 // on FP32 vectors, promoted on load).
-template <class T, bool DOTS, int MINB, bool SEL = false, int VEC = 1, bool PF = false, class TI = T>
+template <class T, bool DOTS, int MINB, bool SEL = false, int VEC = 1, bool PF = false, class TI = T, class TO = T>
 __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
     const typename wt<T>::C* __restrict__ hop, const typename wt<T>::C* __restrict__ clover,
     const int32_t* __restrict__ nbr, const typename wt<TI>::C* __restrict__ in,
-    typename wt<T>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
+    typename wt<TO>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
     int apbc, int tvol, int Lt, double2* __restrict__ d1, double2* __restrict__ d2,
     const int32_t* __restrict__ sel = nullptr, int nsel = 0, const uint8_t* __restrict__ hskip = nullptr) {
   typedef typename wt<T>::C C;
@@ -418,7 +457,7 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
       int k = 0;
       for (int r = rl; r < nrhs; r += rt, ++k) {
         double dt[3] = {0.0, 0.0, 0.0};
-        wilson_site<T, decltype(links), DOTS, VEC, true, PF, TI>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op,
+        wilson_site<T, decltype(links), DOTS, VEC, true, PF, TI, TO>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op,
                                                     dir, disp, apbc, tvol, Lt, dt, skip);
         if (DOTS) {
           if (two) {
@@ -1785,6 +1824,39 @@ gmg_status wilson_apply_f32_in(gmg_wilson* h, int op, int nrhs, const float* in,
   if ((al & 31) == 0) return go(wilson_tile_kernel<double, false, 2, false, 2, true, float>);
   if ((al & 15) == 0) return go(wilson_tile_kernel<double, false, 2, false, 1, true, float>);
   return go(wilson_tile_kernel<double, false, 2, false, 0, true, float>);
+}
+
+// out = M in with the minimal-residual inner products d1[r] = <out, in>,
+// d2[r].x = <out, out> (zeroed here), on BF16 fields [V][nrhs][12] (one 32-bit
+// word per complex number): FP32 arithmetic on the widened records, the
+// products from the FP32 result, the result rounded to BF16.  The tile kernel
+// at 3 CTAs per SM with the records prefetched.
+gmg_status wilson_apply_mr_bf16(gmg_wilson* h, int nrhs, const uint32_t* in, uint32_t* out, double2* d1, double2* d2,
+                                cudaStream_t s) {
+  GMG_CHECK(((((uintptr_t)in | (uintptr_t)out) & 15) == 0), GMG_ERR_ARGUMENT,
+            "wilson apply (BF16): fields must be 16-byte aligned");
+  const int V = (int)h->dims.vol();
+  const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
+  int rt = 1;
+  for (int c = std::min(nrhs, 16); c >= 1; --c)
+    if (nrhs % c == 0) {
+      rt = c;
+      break;
+    }
+  if (nrhs > 16 && rt < 8) rt = 16;
+  const int tiles = (V + kTileSites - 1) / kTileSites;
+  const int g = std::min(tiles, 148 * 16);
+  const size_t smem = sizeof(float2) * 2 * kTileSites * 72 + sizeof(double) * 3 * (size_t)nrhs;
+  KernelTimer kt("wilson", s);
+  GMG_CUDA(cudaMemsetAsync(d1, 0, sizeof(double2) * nrhs, s));
+  GMG_CUDA(cudaMemsetAsync(d2, 0, sizeof(double2) * nrhs, s));
+  auto k = wilson_tile_kernel<float, true, 3, false, 1, true, bf16s, bf16s>;
+  if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k<<<g, kTileSites * rt, smem, s>>>(h->hop_f.as<float2>(), h->clover_f.as<float2>(), h->nbr.as<int32_t>(), in, out, V,
+                                     nrhs, rt, (float)(4.0 + h->mass), GMG_OP_M, 0, 0, h->apbc, tvol, h->dims.d[3], d1,
+                                     d2, nullptr, 0, nullptr);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
 }
 
 gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs,

@@ -418,12 +418,20 @@ class WilsonClover:
         return out
 
     def M_mr(self, inp, out):
-        """out = M inp and the MR-step inner products <out, inp>, <out, out> per RHS."""
-        _check_vec(inp, self.V, 12, "in")
-        _check_vec(out, self.V, 12, "out")
+        """out = M inp and the MR-step inner products <out, inp>, <out, out> per RHS.  BF16 fields
+        are torch.bfloat16 tensors of shape [V, nrhs, 12, 2] (real, imaginary)."""
+        if inp.dtype == torch.bfloat16:
+            if inp.dim() != 4 or inp.shape[0] != self.V or inp.shape[2:] != (12, 2) or not inp.is_contiguous():
+                raise ValueError("BF16 fields must be contiguous [V, nrhs, 12, 2]")
+            assert out.dtype == torch.bfloat16 and out.shape == inp.shape and out.is_contiguous()
+            prec = BF16
+        else:
+            _check_vec(inp, self.V, 12, "in")
+            _check_vec(out, self.V, 12, "out")
+            prec = _vec_prec(inp)
         d = torch.zeros((2, inp.shape[1]), dtype=torch.complex128, device=inp.device)
-        _chk(lib().gmg_wilson_apply_mr(self._h, _vec_prec(inp), inp.shape[1], _ptr(inp), _ptr(out), _ptr(d[0]),
-                                       _ptr(d[1]), _stream()))
+        _chk(lib().gmg_wilson_apply_mr(self._h, prec, inp.shape[1], _ptr(inp), _ptr(out), _ptr(d[0]), _ptr(d[1]),
+                                       _stream()))
         return d[0], d[1].real
 
 
@@ -435,7 +443,7 @@ class MGParams(ctypes.Structure):
                 ("seed", ctypes.c_uint64), ("setup_solver", ctypes.c_int), ("setup_tol", ctypes.c_double),
                 ("setup_passes", ctypes.c_int), ("setup_null", ctypes.c_int), ("graph", ctypes.c_int),
                 ("refine_iters", ctypes.c_int * 2), ("recursive_updates", ctypes.c_int),
-                ("drop_in_cycle", ctypes.c_int)]
+                ("drop_in_cycle", ctypes.c_int), ("smoother_bf16", ctypes.c_int)]
 
 
 class MultiGrid:

@@ -386,30 +386,35 @@ def profile_rows(rows):
         line("p_w Wilson-clover 16^4, 24 RHS: FP32 M, FP32 M with MR products, FP64 M; staged FP32 / FP64 M",
              ok=True, tuned={"f32": w.tuned_kernel("f32", 24), "f32_mr": w.tuned_kernel("f32", 24, fused_mr=True),
                              "f64": w.tuned_kernel("f64", 24)})
-    if "p_c5" in rows:
-        # the C5 mixed BF16 solve (32^4, 24 RHS, graph-captured K-cycle): setup and
-        # one solve (which captures), then the second solve inside the NVTX range "p_c5"
+    for row5, graph5 in (("p_c5", 1), ("p_c5h", 0)):
+        if row5 not in rows:
+            continue
+        # the C5 mixed BF16 solve (32^4, 24 RHS; p_c5: graph-captured K-cycle, p_c5h:
+        # host-driven, every kernel a plain launch): setup and one solve (which
+        # captures), then the second solve inside the NVTX range named after the row
         fd5 = (32, 32, 32, 32)
         U = inputs.torch_smooth_gauge(fd5, 801, 0.3)
         w5 = gmg.WilsonClover(fd5, -0.35, 1.0, antiperiodic=True)
         w5.set_gauge(U)
         del U
         b = inputs.torch_gaussian((32 ** 4, 24, 12), 802)
-        mg = gmg.MultiGrid(w5, 24, prec="bf16", graph=1, nlevels=3, block=((4, 4, 4, 4), (2, 2, 2, 2)),
+        mg = gmg.MultiGrid(w5, 24, prec="bf16", graph=graph5, nlevels=3, block=((4, 4, 4, 4), (2, 2, 2, 2)),
                            nvec=(12, 16), smoother_iters=8)
         mg.setup()
         x = torch.zeros_like(b)
         mg.solve(b, x, tol=1e-10, maxiter=400)
         x.zero_()
         torch.cuda.synchronize()
-        torch.cuda.nvtx.range_push("p_c5")
+        torch.cuda.nvtx.range_push(row5)
         t0 = time.perf_counter()
         it, rr = mg.solve(b, x, tol=1e-10, maxiter=400)
         torch.cuda.synchronize()
         t = time.perf_counter() - t0
         torch.cuda.nvtx.range_pop()
-        line("p_c5 MG solve 32^4, 24 RHS, mixed BF16, graph-captured K-cycle", ok=True, seconds=t, iters=it,
-             relres=rr)
+        line(f"{row5} MG solve 32^4, 24 RHS, mixed BF16, " + ("graph-captured" if graph5 else "host-driven") +
+             " K-cycle", ok=True, seconds=t, iters=it, relres=rr)
+        del mg, x, b, w5
+        torch.cuda.empty_cache()
     if "p_c4" in rows:
         # CoarsenOperator 16^4 -> 4^4, nbasis 40 (the C4 construction on a
         # sixteenth of its volume): two calls, each with 4 face hops, one

@@ -278,7 +278,10 @@ gmg_status gmg_wilson_apply_f32_in(gmg_wilson* h, gmg_op op, int nrhs, const flo
 /* out = M in together with the minimal-residual inner products of the MR
    smoother step (the smoother solve of include/MultigridPreconditioner.h:
    264-301): d1[r] = <out_r, in_r>,
-   d2[r] = <out_r, out_r> + 0i, device arrays of nrhs complex128. */
+   d2[r] = <out_r, out_r> + 0i, device arrays of nrhs complex128.  vec_prec
+   F64, F32, or BF16: fields of one 32-bit word per complex number (real part
+   in the low 16 bits), FP32 arithmetic, the products from the FP32 result,
+   the result rounded to nearest even (the fine smoother of params.smoother_bf16). */
 /* Kernel variants of the multi-RHS Wilson-clover apply.  By default the
    variant is autotuned: every applicable one is timed once per (vector
    precision, fused MR products or not, single-hop op or not, nrhs class) on
@@ -368,6 +371,11 @@ typedef struct {
                             cycle apply the preconditioner and the operator to the still-active
                             RHS only.  0: converged RHS leave at the next restart.  No counterpart
                             (the reference solves one RHS at a time). */
+  int smoother_bf16;     /* 1: with an FP32 or BF16 preconditioner, the fine level's MR smoother keeps
+                            its residual and operator product in BF16 (FP32 arithmetic, FP32
+                            solution, the MR inner products from the FP32 operator result), so its
+                            sweeps move half the bytes.  0: FP32.  -1 (default): on for the BF16
+                            preconditioner form (prec GMG_BF16), off otherwise. */
 } gmg_mg_params;
 
 /* Defaults of MultiGridParams (MultigridParams.h:95-113) adapted to the MR smoother, with the

@@ -268,3 +268,25 @@ def test_mg_converged_rhs_leave_within_a_cycle(fine, prec, graph):
     # step k counts the RHS that had not converged before it
     for k, sz in enumerate(b1):
         assert sz == int((its1 > k).sum()), (k, b1, its1)
+
+
+@pytest.mark.parametrize("prec", ["f32", "bf16"])
+def test_mg_bf16_smoother_reaches_1e10(fine, prec):
+    # the fine smoother with BF16 residual fields (FP32 arithmetic and solution):
+    # the outer FP64 FGMRES still reaches the 1e-10 true residual, within two
+    # outer iterations of the FP32 smoother
+    dims, w = fine
+    nrhs = 4
+    kw = dict(nlevels=3, nvec=(6, 6), setup_iters=30, prec=prec, coarsest_iters=30, wrapper_iters=6,
+              block=((2, 2, 2, 2), (2, 2, 2, 2)))
+    b = torch.from_numpy(inputs.gaussian_field((4096, nrhs, 12), inputs.rng(stream=321))).cuda()
+    its = {}
+    for bf in (0, 1):
+        mg = gmg.MultiGrid(w, nrhs, smoother_bf16=bf, **kw)
+        mg.setup()
+        x = torch.zeros_like(b)
+        it, rr = mg.solve(b, x, tol=1e-10, maxiter=300)
+        assert rr <= 1e-10
+        assert true_relres(w, b, x) <= 2e-10, (bf, it, rr)
+        its[bf] = it
+    assert its[1] <= its[0] + 2, its

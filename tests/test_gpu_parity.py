@@ -604,3 +604,25 @@ def test_wilson_f32_input_matches_converted_f64_apply(wil, forced, nrhs, dag):
     assert torch.equal(want, got)
     ref = orc.wilson_clover(dims, U, cl, -0.1, 1, host(x64), orc.OP_MDAG if dag else orc.OP_M)
     assert orc.rel_dev_sq(ref, host(got)) < TOL64
+
+
+@pytest.mark.parametrize("nrhs", [4, 24])
+def test_wilson_mr_products_bf16_fields(wil, nrhs):
+    # the fine smoother's BF16 form: BF16 input records widened to FP32, M in
+    # FP32, the result rounded to BF16, the MR products from the FP32 result.
+    # Against the FP64 oracle on the BF16-rounded input: the output within
+    # BF16 rounding (2^-8 relative per component, squared deviation < 4e-5),
+    # the products to FP32 accuracy of the unrounded result
+    dims, U, cl, w = wil
+    x = inputs.gaussian_field((512, nrhs, 12), inputs.rng(stream=200 + nrhs))
+    xb = torch.view_as_real(dev(x, torch.complex64)).to(torch.bfloat16).contiguous()
+    xr = torch.view_as_complex(xb.float()).to(torch.complex128)
+    ref = orc.wilson_clover(dims, U, cl, -0.1, 1, host(xr), orc.OP_M)
+    out = torch.zeros_like(xb)
+    d1, d2 = w.M_mr(xb, out)
+    got = torch.view_as_complex(out.float()).to(torch.complex128)
+    assert orc.rel_dev_sq(ref, host(got)) < 4e-5
+    d1_ref = np.einsum("srk,srk->r", ref.conj(), host(xr))
+    d2_ref = np.einsum("srk,srk->r", ref.conj(), ref).real
+    assert np.abs(d1.cpu().numpy() - d1_ref).max() / np.abs(d2_ref).max() < 1e-5
+    assert np.abs(d2.cpu().numpy() - d2_ref).max() / np.abs(d2_ref).max() < 1e-5
