@@ -385,6 +385,130 @@ __global__ void __launch_bounds__(MODE == 1 ? kAxDot1Threads : kAxDotThreads) mu
   }
 }
 
+// Delayed-reorthogonalisation Gram-Schmidt (DCGS2), FP64.  V_0 .. V_{NV-1}
+// are the finished basis vectors, A = V_NV the last one after one projection
+// (its second projection delayed to this step), B the new operator product.
+// Pass 1 (one sweep): out[k * R + r] for k < NV: <V_k, A>; NV <= k < 2 NV:
+// <V_{k-NV}, B>; 2 NV: <A, A>; 2 NV + 1: <A, B>; 2 NV + 2: <B, B>.
+constexpr int kDcgsThreads = 384;
+constexpr int kDcgsMaxNV = 9;
+
+template <int NV>
+__global__ void __launch_bounds__(kDcgsThreads) dcgs_dots_row_kernel(const double2* __restrict__ V0, int64_t vstride,
+                                                                     const double2* __restrict__ B, int64_t V, int R,
+                                                                     int dof, int spb, double2* __restrict__ out) {
+  extern __shared__ double part[];  // [8][NT]
+  constexpr int NP = 2 * NV + 3;
+  const int RD = R * dof, t = threadIdx.x, NT = blockDim.x;
+  const int so = t / RD, i = t % RD;
+  const bool act = t < spb * RD;
+  double pr[NP], pi[NP];
+#pragma unroll
+  for (int k = 0; k < NP; ++k) pr[k] = pi[k] = 0.0;
+  if (act) {
+    for (int64_t st = (int64_t)blockIdx.x * spb + so; st < V; st += (int64_t)gridDim.x * spb) {
+      const int64_t e = st * RD + i;
+      double2 xv[NV + 1];
+#pragma unroll
+      for (int k = 0; k <= NV; ++k) xv[k] = V0[k * vstride + e];
+      const double2 a = xv[NV], b = B[e];
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        pr[k] += xv[k].x * a.x + xv[k].y * a.y;
+        pi[k] += xv[k].x * a.y - xv[k].y * a.x;
+        pr[NV + k] += xv[k].x * b.x + xv[k].y * b.y;
+        pi[NV + k] += xv[k].x * b.y - xv[k].y * b.x;
+      }
+      pr[2 * NV] += a.x * a.x + a.y * a.y;
+      pr[2 * NV + 1] += a.x * b.x + a.y * b.y;
+      pi[2 * NV + 1] += a.x * b.y - a.y * b.x;
+      pr[2 * NV + 2] += b.x * b.x + b.y * b.y;
+    }
+  }
+  // block reduction, four products at a time: the spb site slots, then the
+  // dof components of each RHS, then one global atomic per (product, RHS)
+#pragma unroll
+  for (int k0 = 0; k0 < NP; k0 += 4) {
+    const int nk = min(4, NP - k0);
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double vr = 0.0, vi = 0.0;
+#pragma unroll
+      for (int k = 0; k < NP; ++k)
+        if (k == k0 + q) {
+          vr = pr[k];
+          vi = pi[k];
+        }
+      part[(2 * q) * NT + t] = act ? vr : 0.0;
+      part[(2 * q + 1) * NT + t] = act ? vi : 0.0;
+    }
+    __syncthreads();
+    if (spb > 1) {
+      for (int k = t; k < 2 * nk * RD; k += NT) {
+        const int jc = k / RD, ii = k % RD;
+        double v = part[jc * NT + ii];
+        for (int o = 1; o < spb; ++o) v += part[jc * NT + o * RD + ii];
+        part[jc * NT + ii] = v;
+      }
+      __syncthreads();
+    }
+    for (int k = t; k < nk * R; k += NT) {
+      const int q = k / R, rr = k % R;
+      double vr = 0.0, vi = 0.0;
+      for (int d = 0; d < dof; ++d) {
+        vr += part[(2 * q) * NT + rr * dof + d];
+        vi += part[(2 * q + 1) * NT + rr * dof + d];
+      }
+      atomicAdd(&out[(k0 + q) * R + rr].x, vr);
+      atomicAdd(&out[(k0 + q) * R + rr].y, vi);
+    }
+  }
+}
+
+// Pass 2 (one sweep): A <- (A - sum_k c_k V_k) / alpha (the finished basis
+// vector, in place), then V_{NV+1} <- (B - sum_k g_k V_k - d A) / beta (the
+// next one after one projection).  cf per RHS: c[NV], g[NV], (1/alpha, 0),
+// d, (1/beta, 0), at cf[k * R + r].
+template <int NV>
+__global__ void __launch_bounds__(kDcgsThreads) dcgs_update_row_kernel(const double2* __restrict__ cfg,
+                                                                       double2* __restrict__ V0, int64_t vstride,
+                                                                       const double2* __restrict__ B, int64_t V, int R,
+                                                                       int dof, int spb) {
+  extern __shared__ double2 cf[];  // [2 NV + 3][R]
+  constexpr int NC = 2 * NV + 3;
+  const int RD = R * dof, t = threadIdx.x;
+  for (int k = t; k < NC * R; k += blockDim.x) cf[k] = cfg[k];
+  __syncthreads();
+  if (t >= spb * RD) return;
+  const int so = t / RD, i = t % RD, r = i / dof;
+  for (int64_t st = (int64_t)blockIdx.x * spb + so; st < V; st += (int64_t)gridDim.x * spb) {
+    const int64_t e = st * RD + i;
+    double2 xv[NV + 1];
+#pragma unroll
+    for (int k = 0; k <= NV; ++k) xv[k] = V0[k * vstride + e];
+    const double2 b = B[e];
+    double ar = xv[NV].x, ai = xv[NV].y, br = b.x, bi = b.y;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      const double2 c = cf[k * R + r], g = cf[(NV + k) * R + r];
+      ar -= c.x * xv[k].x - c.y * xv[k].y;
+      ai -= c.x * xv[k].y + c.y * xv[k].x;
+      br -= g.x * xv[k].x - g.y * xv[k].y;
+      bi -= g.x * xv[k].y + g.y * xv[k].x;
+    }
+    const double ia = cf[(2 * NV) * R + r].x;
+    const double2 d = cf[(2 * NV + 1) * R + r];
+    const double ib = cf[(2 * NV + 2) * R + r].x;
+    ar *= ia;
+    ai *= ia;
+    br -= d.x * ar - d.y * ai;
+    bi -= d.x * ai + d.y * ar;
+    V0[NV * vstride + e] = make_double2(ar, ai);
+    V0[(NV + 1) * vstride + e] = make_double2(br * ib, bi * ib);
+  }
+}
+
 // Y(r) = X(r) / sqrt(n[r].x)
 template <class T>
 __global__ void __launch_bounds__(1024) scale_inv_norm_row_kernel(const double2* __restrict__ n,
@@ -801,6 +925,63 @@ gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s) {
   else blas::xmy_kernel<float><<<g, 256, 0, s>>>((const float2*)X.p, (float2*)Y.p, n);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
+}
+
+bool vec_dcgs_supported(const Vec& Y, int nv) {
+  return Y.prec == GMG_F64 && nv >= 0 && nv <= blas::kDcgsMaxNV && Y.R * Y.dof <= blas::kDcgsThreads;
+}
+
+gmg_status vec_dcgs_dots(const Vec& V0, int64_t vstride, int nv, const Vec& B, double2* out_dev, cudaStream_t s) {
+  GMG_CHECK(vec_dcgs_supported(B, nv), GMG_ERR_UNSUPPORTED, "dcgs: unsupported shape");
+  const int R = B.R;
+  GMG_CUDA(cudaMemsetAsync(out_dev, 0, sizeof(double2) * (2 * nv + 3) * R, s));
+  const blas::Row g = blas::row_geom(B.V, B.R, B.dof);
+  const size_t sm = sizeof(double) * 8 * g.threads;
+  const int grid = std::min(g.grid, 148 * std::max(1, 2048 / g.threads));
+  auto launch = [&](auto kern) -> gmg_status {
+    if (sm > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<grid, g.threads, sm, s>>>((const double2*)V0.p, vstride, (const double2*)B.p, B.V, B.R, B.dof, g.spb,
+                                     out_dev);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  };
+  switch (nv) {
+    case 0: return launch(blas::dcgs_dots_row_kernel<0>);
+    case 1: return launch(blas::dcgs_dots_row_kernel<1>);
+    case 2: return launch(blas::dcgs_dots_row_kernel<2>);
+    case 3: return launch(blas::dcgs_dots_row_kernel<3>);
+    case 4: return launch(blas::dcgs_dots_row_kernel<4>);
+    case 5: return launch(blas::dcgs_dots_row_kernel<5>);
+    case 6: return launch(blas::dcgs_dots_row_kernel<6>);
+    case 7: return launch(blas::dcgs_dots_row_kernel<7>);
+    case 8: return launch(blas::dcgs_dots_row_kernel<8>);
+    default: return launch(blas::dcgs_dots_row_kernel<9>);
+  }
+}
+
+gmg_status vec_dcgs_update(const double2* coef_dev, Vec& V0, int64_t vstride, int nv, const Vec& B, cudaStream_t s) {
+  GMG_CHECK(vec_dcgs_supported(B, nv), GMG_ERR_UNSUPPORTED, "dcgs: unsupported shape");
+  const blas::Row g = blas::row_geom(B.V, B.R, B.dof);
+  const size_t sm = sizeof(double2) * (2 * nv + 3) * B.R;
+  const int grid = std::min(g.grid, 148 * std::max(1, 2048 / g.threads));
+  auto launch = [&](auto kern) -> gmg_status {
+    if (sm > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<grid, g.threads, sm, s>>>(coef_dev, (double2*)V0.p, vstride, (const double2*)B.p, B.V, B.R, B.dof, g.spb);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  };
+  switch (nv) {
+    case 0: return launch(blas::dcgs_update_row_kernel<0>);
+    case 1: return launch(blas::dcgs_update_row_kernel<1>);
+    case 2: return launch(blas::dcgs_update_row_kernel<2>);
+    case 3: return launch(blas::dcgs_update_row_kernel<3>);
+    case 4: return launch(blas::dcgs_update_row_kernel<4>);
+    case 5: return launch(blas::dcgs_update_row_kernel<5>);
+    case 6: return launch(blas::dcgs_update_row_kernel<6>);
+    case 7: return launch(blas::dcgs_update_row_kernel<7>);
+    case 8: return launch(blas::dcgs_update_row_kernel<8>);
+    default: return launch(blas::dcgs_update_row_kernel<9>);
+  }
 }
 
 gmg_status vec_xmy_bf16(const Vec& X, const Vec& Y, Vec& Z, cudaStream_t s) {

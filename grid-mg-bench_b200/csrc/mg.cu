@@ -332,9 +332,45 @@ struct DropCtx {
   Vec zc, wc;                  // compact scratch: preconditioner precision, FP64
   int* idx = nullptr;          // device, active columns of the compact batch
   bool enabled = false;        // drop (true) or only record the steps
+  bool dcgs = false;           // Gram-Schmidt with delayed reorthogonalisation (params.outer_dcgs)
   std::vector<int> conv_step;  // out: per column, the step (1-based) its estimate met tol; 0: never
   std::vector<int>* batches = nullptr;  // out: appended active-batch size of every step
 };
+
+// min |beta0 e1 - H y| over y for the (n + 1) x n upper Hessenberg H (row
+// stride m), by Givens rotations on a copy; returns the residual norm and, when
+// y is given, the solution y[0 .. n-1] (entries at stride ys)
+double hess_lsq(const zc* H, int m, int n, double beta0, zc* y, int ys) {
+  std::vector<zc> A((size_t)(n + 1) * n), gg(n + 1, zc(0));
+  for (int i = 0; i <= n; ++i)
+    for (int k = 0; k < n; ++k) A[(size_t)i * n + k] = H[i * m + k];
+  gg[0] = beta0;
+  for (int k = 0; k < n; ++k) {
+    const zc a = A[(size_t)k * n + k], bq = A[(size_t)(k + 1) * n + k];
+    const double den = std::sqrt(std::norm(a) + std::norm(bq));
+    zc c = 1.0, sg = 0.0;
+    if (den > 0) {
+      c = a / den;
+      sg = bq / den;
+    }
+    for (int q = k; q < n; ++q) {
+      const zc u = A[(size_t)k * n + q], v = A[(size_t)(k + 1) * n + q];
+      A[(size_t)k * n + q] = std::conj(c) * u + std::conj(sg) * v;
+      A[(size_t)(k + 1) * n + q] = -sg * u + c * v;
+    }
+    const zc gk = gg[k];
+    gg[k] = std::conj(c) * gk;
+    gg[k + 1] = -sg * gk;
+  }
+  if (y) {
+    for (int i = n - 1; i >= 0; --i) {
+      zc acc = gg[i];
+      for (int k = i + 1; k < n; ++k) acc -= A[(size_t)i * n + k] * y[(size_t)k * ys];
+      y[(size_t)i * ys] = A[(size_t)i * n + i] != zc(0) ? acc / A[(size_t)i * n + i] : zc(0);
+    }
+  }
+  return std::abs(gg[n]);
+}
 
 template <class Prec>
 gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m, int maxit, double tol, Prec prec,
@@ -354,6 +390,10 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
   std::vector<double> res(R, 1.0);
   int iters = 0;
   std::vector<zc> H((size_t)(m + 1) * m * R), g((size_t)(m + 1) * R), cs((size_t)m * R), sn((size_t)m * R);
+  // DCGS2 (outer solve): H kept unrotated, with each column corrected one step
+  // later for the delayed second projection of its last basis vector
+  const bool dcgs = drop && drop->dcgs && flexible && vec_dcgs_supported(K.w.with_rhs(R), m - 1);
+  std::vector<double> beta0(R, 0.0), betaT(R, 0.0);
   while (true) {
     // r0 = b - A x -> V_0
     Vec v0 = nth(V0, 0);
@@ -379,6 +419,7 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
     std::fill(H.begin(), H.end(), zc(0));
     std::fill(g.begin(), g.end(), zc(0));
     for (int r = 0; r < R; ++r) g[(size_t)r * (m + 1)] = beta[r];  // per-RHS residual vector, [R][m+1]
+    beta0 = beta;
     int jl = -1;
     for (int j = 0; j < m && iters < maxit; ++j) {
       Vec vj = nth(V0, j);
@@ -407,6 +448,54 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
           GMG_TRY(apply_op(h, l, zj, w, s));
         }
       }
+      if (dcgs) {
+        // Gram-Schmidt with delayed reorthogonalisation: V_0 .. V_{j-1} are
+        // final, V_j has had one projection.  One sweep forms V_j's second
+        // projection coefficients c, w's projections g and three norms; the host
+        // forms alpha = |V_j - V c| and the new vector's coefficient d and norm
+        // beta by Pythagoras; a second sweep finishes V_j and writes V_{j+1}
+        // after one projection.  Two sweeps over the basis per step instead of
+        // three and a scaling sweep.
+        const int nv = j;
+        double2* dd = h->dscr.as<double2>();
+        GMG_TRY(vec_dcgs_dots(V0, vstride, nv, w, dd, s));
+        std::vector<zc> col;
+        GMG_TRY(download(h, dd, (2 * nv + 3) * R, col, s));
+        std::vector<zc> cf((size_t)(2 * nv + 3) * R, zc(0));
+        for (int r = 0; r < R; ++r) {
+          cf[(size_t)(2 * nv) * R + r] = 1.0;  // dropped columns: V_j unchanged, V_{j+1} = 0
+          if (!live[r]) continue;
+          const double t1 = col[(size_t)(2 * nv) * R + r].real(), t3 = col[(size_t)(2 * nv + 2) * R + r].real();
+          double a2 = t1;
+          zc d = col[(size_t)(2 * nv + 1) * R + r];
+          for (int k = 0; k < nv; ++k) a2 -= std::norm(col[(size_t)k * R + r]);
+          const double alpha = nv == 0 ? 1.0 : std::sqrt(std::max(a2, 1e-30 * std::max(t1, 1e-300)));
+          for (int k = 0; k < nv; ++k) d -= std::conj(col[(size_t)k * R + r]) * col[(size_t)(nv + k) * R + r];
+          d /= alpha;
+          double b2 = t3 - std::norm(d);
+          for (int k = 0; k < nv; ++k) b2 -= std::norm(col[(size_t)(nv + k) * R + r]);
+          const double bt = std::sqrt(std::max(b2, 0.0));
+          for (int k = 0; k < nv; ++k) {
+            cf[(size_t)k * R + r] = col[(size_t)k * R + r];
+            cf[(size_t)(nv + k) * R + r] = col[(size_t)(nv + k) * R + r];
+          }
+          cf[(size_t)(2 * nv) * R + r] = 1.0 / alpha;
+          cf[(size_t)(2 * nv + 1) * R + r] = d;
+          cf[(size_t)(2 * nv + 2) * R + r] = bt > 0 ? 1.0 / bt : 0.0;
+          zc* Hr = &H[(size_t)r * (m + 1) * m];
+          if (nv > 0) {  // column j - 1 with V_j's second projection
+            for (int k = 0; k < nv; ++k) Hr[k * m + (j - 1)] += betaT[r] * col[(size_t)k * R + r];
+            Hr[j * m + (j - 1)] = betaT[r] * alpha;
+          }
+          for (int k = 0; k < nv; ++k) Hr[k * m + j] = col[(size_t)(nv + k) * R + r];
+          Hr[j * m + j] = d;
+          Hr[(j + 1) * m + j] = bt;
+          betaT[r] = bt;
+          res[r] = hess_lsq(Hr, m, j + 1, beta0[r], nullptr, 0) / bnorm[r];
+        }
+        GMG_TRY(upload(h, cf, 0, s));
+        GMG_TRY(vec_dcgs_update(h->coef.as<double2>(), V0, vstride, nv, w, s));
+      } else {
       // classical Gram-Schmidt, twice, with the coefficients kept on the device;
       // the Hessenberg column comes back to the host in one transfer.  (With a
       // good preconditioner w = A z_j is close to v_j, the first pass cancels
@@ -457,6 +546,7 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
         gr[j + 1] = -sgn * gj;
         res[r] = std::abs(gr[j + 1]) / bnorm[r];
       }
+      }
       ++iters;
       jl = j;
       bool conv = true, dropped = false;
@@ -491,6 +581,10 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
       // a dropped column uses the steps it kept; its later coefficients are zero
       const int nr = live[r] ? n : keep[r];
       for (int i = n - 1; i >= nr; --i) y[(size_t)i * R + r] = zc(0);
+      if (dcgs) {
+        if (nr > 0) hess_lsq(Hr, m, nr, beta0[r], &y[r], R);
+        continue;
+      }
       for (int i = nr - 1; i >= 0; --i) {
         zc acc = gr[i];
         for (int k = i + 1; k < nr; ++k) acc -= Hr[i * m + k] * y[(size_t)k * R + r];
@@ -1040,6 +1134,7 @@ extern "C" gmg_status gmg_mg_params_default(gmg_mg_params* p) {
   p->recursive_updates = 1;
   p->drop_in_cycle = 1;
   p->smoother_bf16 = -1;
+  p->outer_dcgs = 1;
   return GMG_OK;
 }
 
@@ -1305,6 +1400,7 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
     std::vector<double> rr;
     DropCtx dc;
     dc.enabled = h->P.drop_in_cycle != 0;
+    dc.dcgs = h->P.outer_dcgs != 0;
     if (dc.enabled) {
       dc.zc = h->ozc.with_rhs(Ra);
       dc.wc = h->owc.with_rhs(Ra);

@@ -70,6 +70,14 @@ gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, c
                          bool update_r = true);
 // Y = X - Y
 gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s);
+// Delayed-reorthogonalisation Gram-Schmidt sweeps (FP64, V0 [nv + 2] vectors at
+// vstride elements): pass 1 forms <V_k, V_nv>, <V_k, B> (k < nv), <V_nv, V_nv>,
+// <V_nv, B>, <B, B> per RHS (2 nv + 3 values at out[k * R + r]); pass 2 sets
+// V_nv <- (V_nv - sum c_k V_k) / alpha and V_{nv+1} <- (B - sum g_k V_k - d V_nv) / beta
+// with coef[k * R + r] = c (nv), g (nv), 1/alpha, d, 1/beta
+bool vec_dcgs_supported(const Vec& B, int nv);
+gmg_status vec_dcgs_dots(const Vec& V0, int64_t vstride, int nv, const Vec& B, double2* out_dev, cudaStream_t s);
+gmg_status vec_dcgs_update(const double2* coef_dev, Vec& V0, int64_t vstride, int nv, const Vec& B, cudaStream_t s);
 // Z (BF16) = X - Y (FP32), rounded to nearest even
 gmg_status vec_xmy_bf16(const Vec& X, const Vec& Y, Vec& Z, cudaStream_t s);
 // G[a][b] = <X(a), X(b)> over the whole lattice (R <= 32 columns), FP64

@@ -376,6 +376,10 @@ typedef struct {
                             solution, the MR inner products from the FP32 operator result), so its
                             sweeps move half the bytes.  0: FP32.  -1 (default): on for the BF16
                             preconditioner form (prec GMG_BF16), off otherwise. */
+  int outer_dcgs;        /* 1 (default): the outer FGMRES orthogonalises with delayed
+                            reorthogonalisation (the second classical Gram-Schmidt pass of each
+                            basis vector merged into the next step): two sweeps over the FP64
+                            Krylov basis per step instead of three and a scaling sweep.  0: CGS2. */
 } gmg_mg_params;
 
 /* Defaults of MultiGridParams (MultigridParams.h:95-113) adapted to the MR smoother, with the
