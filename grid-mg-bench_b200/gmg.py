@@ -435,6 +435,55 @@ class WilsonClover:
         return d[0], d[1].real
 
 
+class GaugeInfo(ctypes.Structure):
+    _fields_ = [("dims", ctypes.c_int * 4), ("two_row", ctypes.c_int), ("precision", ctypes.c_int),
+                ("big_endian", ctypes.c_int), ("plaquette", ctypes.c_double), ("link_trace", ctypes.c_double),
+                ("checksum", ctypes.c_uint32), ("checksum_data", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {"dims": tuple(self.dims), "two_row": self.two_row, "precision": self.precision,
+                "big_endian": self.big_endian, "plaquette": self.plaquette, "link_trace": self.link_trace,
+                "checksum": self.checksum, "checksum_data": self.checksum_data}
+
+
+def read_nersc(path, verify=True):
+    """NerscIO::readConfiguration: (links [V, 4, 3, 3] complex128, header info)."""
+    info = GaugeInfo()
+    _chk(lib().gmg_gauge_read_nersc(str(path).encode(), ctypes.byref(info), None, 0))
+    U = np.zeros((vol(tuple(info.dims)), 4, 3, 3), dtype=np.complex128)
+    _chk(lib().gmg_gauge_read_nersc(str(path).encode(), ctypes.byref(info), U.ctypes.data_as(ctypes.c_void_p),
+                                    int(verify)))
+    return U, info.as_dict()
+
+
+def write_nersc(path, dims, U, two_row=False, precision=64, ensemble_id="synthetic", sequence_number=0):
+    """NerscIO::writeConfiguration of host links [V, 4, 3, 3] complex128."""
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    _chk(lib().gmg_gauge_write_nersc(str(path).encode(), _dims(dims), U.ctypes.data_as(ctypes.c_void_p),
+                                     int(two_row), int(precision), ensemble_id.encode(), int(sequence_number)))
+
+
+def read_ildg(path):
+    """IldgReader::readConfiguration: (links [V, 4, 3, 3] complex128, header info)."""
+    info = GaugeInfo()
+    _chk(lib().gmg_gauge_read_ildg(str(path).encode(), ctypes.byref(info), None))
+    U = np.zeros((vol(tuple(info.dims)), 4, 3, 3), dtype=np.complex128)
+    _chk(lib().gmg_gauge_read_ildg(str(path).encode(), ctypes.byref(info), U.ctypes.data_as(ctypes.c_void_p)))
+    return U, info.as_dict()
+
+
+def plaquette(dims, U):
+    """(average plaquette, average link trace) of links on the host or the device, on the GPU."""
+    p, t = ctypes.c_double(), ctypes.c_double()
+    if isinstance(U, torch.Tensor) and U.is_cuda:
+        _chk(lib().gmg_gauge_plaquette(_dims(dims), _ptr(U), 1, ctypes.byref(p), ctypes.byref(t), _stream()))
+    else:
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        _chk(lib().gmg_gauge_plaquette(_dims(dims), U.ctypes.data_as(ctypes.c_void_p), 0, ctypes.byref(p),
+                                       ctypes.byref(t), _stream()))
+    return p.value, t.value
+
+
 class MGParams(ctypes.Structure):
     _fields_ = [("nlevels", ctypes.c_int), ("block", (ctypes.c_int * 4) * 2), ("nvec", ctypes.c_int * 2),
                 ("setup_iters", ctypes.c_int), ("smoother_iters", ctypes.c_int), ("wrapper_iters", ctypes.c_int),

@@ -309,6 +309,44 @@ gmg_status gmg_wilson_apply_mr(gmg_wilson* h, gmg_prec vec_prec, int nrhs, const
                                double* d1, double* d2, gmg_stream s);
 
 /* ------------------------------------------------------------------------ */
+/* Gauge-field configuration files (Grid's NerscIO / IldgReader, used at      */
+/* src/Test_wilsonclover_mg_lime.cc:57-75, src/Test_wilsonclover_mg.cc:96-99, */
+/* NerscIO::writeConfiguration at src/Test_wilson_cg_unprec.cc:72).  Fields   */
+/* are host [V][mu][3][3] complex128, sites lexicographic with x fastest: the */
+/* layout gmg_wilson_set_gauge takes.                                         */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int dims[4];            /* lattice extents from the header */
+  int two_row;            /* NERSC 4D_SU3_GAUGE: two rows stored, the third reconstructed */
+  int precision;          /* 32 or 64 (bits per real) */
+  int big_endian;         /* 1: big-endian payload */
+  double plaquette;       /* NERSC header PLAQUETTE (0 if absent) */
+  double link_trace;      /* NERSC header LINK_TRACE (0 if absent) */
+  uint32_t checksum;      /* NERSC header CHECKSUM */
+  uint32_t checksum_data; /* the same sum formed over the payload read */
+} gmg_gauge_info;
+
+/* NerscIO::readConfiguration: the header into *info and, when U is not NULL,
+   the links into U (V * 36 complex128, from info->dims of a header-only call).
+   verify: the checksum, and the plaquette and link trace (formed on the host)
+   must match the header (Grid asserts the same three). */
+gmg_status gmg_gauge_read_nersc(const char* path, gmg_gauge_info* info, double* U, int verify);
+/* NerscIO::writeConfiguration: big-endian IEEE32 or IEEE64 (precision 32 / 64),
+   two_row selects 4D_SU3_GAUGE (the third row dropped; exact only for SU(3)
+   links) over 4D_SU3_GAUGE_3x3; the header carries the plaquette, link trace
+   and checksum. */
+gmg_status gmg_gauge_write_nersc(const char* path, const int dims[4], const double* U, int two_row, int precision,
+                                 const char* ensemble_id, int sequence_number);
+/* IldgReader::readConfiguration: the ildg-format and ildg-binary-data records
+   of a LIME file (precision and extents from the format record). */
+gmg_status gmg_gauge_read_ildg(const char* path, gmg_gauge_info* info, double* U);
+/* Average plaquette Re tr(U_mu U_nu U_mu^dag U_nu^dag) / 3 over sites and the
+   six planes, and average link trace Re tr U_mu / 3 (periodic lattice), on the
+   GPU; U on the host or the device. */
+gmg_status gmg_gauge_plaquette(const int dims[4], const double* U, int on_device, double* plaquette,
+                               double* link_trace, gmg_stream s);
+
+/* ------------------------------------------------------------------------ */
 /* Galerkin coarse-operator construction                                     */
 /* CoarsenOperator(FineGrid, linop, Aggregation) (CoarsenedMatrixUpstream.h: */
 /* 755-931, ...DirsaveLut.h:927-1097)                                        */
