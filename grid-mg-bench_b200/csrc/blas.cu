@@ -586,6 +586,65 @@ __global__ void __launch_bounds__(1024) mr_update_bf16_row_kernel(const double2*
   }
 }
 
+// rn = bf16(r - a Ar): one MR step on residuals that the sweep keeps
+__global__ void __launch_bounds__(1024) mr_resid_bf16_row_kernel(const double2* __restrict__ d1,
+                                                                 const double2* __restrict__ d2,
+                                                                 const uint32_t* __restrict__ r,
+                                                                 const uint32_t* __restrict__ Ar,
+                                                                 uint32_t* __restrict__ rn, int64_t V, int R, int dof,
+                                                                 int spb) {
+  const int RD = R * dof, t = threadIdx.x;
+  if (t >= spb * RD) return;
+  const int so = t / RD, i = t % RD, k = i / dof;
+  const double den = d2[k].x;
+  const float ar = den > 0.0 ? (float)(d1[k].x / den) : 0.f, ai = den > 0.0 ? (float)(d1[k].y / den) : 0.f;
+  for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+    const int64_t e = s * RD + i;
+    const float2 v = bf16w_to_f2(r[e]), q = bf16w_to_f2(Ar[e]);
+    rn[e] = f2_to_bf16w(v.x - (ar * q.x - ai * q.y), v.y - (ar * q.y + ai * q.x));
+  }
+}
+
+// x += sum_j a_j r_j over the K kept residuals of an MR sweep: the solution is
+// read and written once per sweep instead of once per step
+__global__ void __launch_bounds__(1024) mr_xsum_bf16_row_kernel(const double2* __restrict__ d, int dstride, int K,
+                                                                const uint32_t* __restrict__ r0, int64_t rstride,
+                                                                float2* __restrict__ x, int64_t V, int R, int dof,
+                                                                int spb) {
+  const int RD = R * dof, t = threadIdx.x;
+  if (t >= spb * RD) return;
+  const int so = t / RD, i = t % RD, k = i / dof;
+  float2 a[kMrMaxSteps];
+#pragma unroll
+  for (int j = 0; j < kMrMaxSteps; ++j) {
+    a[j] = make_float2(0.f, 0.f);
+    if (j < K) {
+      const double den = d[(int64_t)j * dstride + R + k].x;
+      const double2 num = d[(int64_t)j * dstride + k];
+      if (den > 0.0) a[j] = make_float2((float)(num.x / den), (float)(num.y / den));
+    }
+  }
+  for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+    const int64_t e = s * RD + i;
+    uint32_t w[kMrMaxSteps];
+#pragma unroll
+    for (int j = 0; j < kMrMaxSteps; ++j)
+      if (j < K) w[j] = __ldg(r0 + j * rstride + e);
+    float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < kMrMaxSteps; ++j)
+      if (j < K) {
+        const float2 v = bf16w_to_f2(w[j]);
+        acc.x += a[j].x * v.x - a[j].y * v.y;
+        acc.y += a[j].x * v.y + a[j].y * v.x;
+      }
+    float2 xv = x[e];
+    xv.x += acc.x;
+    xv.y += acc.y;
+    x[e] = xv;
+  }
+}
+
 __global__ void xmy_bf16_kernel(const float2* __restrict__ X, const float2* __restrict__ Y, uint32_t* __restrict__ Z,
                                 int64_t n) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
@@ -914,6 +973,28 @@ gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, c
   else
     blas::mr_update_kernel<float><<<g, 256, 0, s>>>(d1, d2, (float2*)x.p, (float2*)r.p, (const float2*)Ar.p, x.V, x.R,
                                                     x.dof, update_r);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status vec_mr_resid_bf16(const double2* d1, const double2* d2, const Vec& r, const Vec& Ar, Vec& rn,
+                             cudaStream_t s) {
+  GMG_CHECK(r.prec == GMG_BF16 && Ar.prec == GMG_BF16 && rn.prec == GMG_BF16 && r.R * r.dof <= 1024,
+            GMG_ERR_UNSUPPORTED, "mr residual: BF16 fields with at most 1024 values per site");
+  const blas::Row rg = blas::row_geom(r.V, r.R, r.dof);
+  blas::mr_resid_bf16_row_kernel<<<rg.grid, rg.threads, 0, s>>>(d1, d2, (const uint32_t*)r.p, (const uint32_t*)Ar.p,
+                                                               (uint32_t*)rn.p, r.V, r.R, r.dof, rg.spb);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+gmg_status vec_mr_xsum_bf16(const double2* d, int dstride, int K, const Vec& r0, int64_t rstride, Vec& x,
+                            cudaStream_t s) {
+  GMG_CHECK(r0.prec == GMG_BF16 && x.prec == GMG_F32 && K >= 1 && K <= kMrMaxSteps && x.R * x.dof <= 1024,
+            GMG_ERR_UNSUPPORTED, "mr sum: BF16 residuals, an FP32 solution, 1 to 16 steps");
+  const blas::Row rg = blas::row_geom(x.V, x.R, x.dof);
+  blas::mr_xsum_bf16_row_kernel<<<rg.grid, rg.threads, 0, s>>>(d, dstride, K, (const uint32_t*)r0.p, rstride,
+                                                              (float2*)x.p, x.V, x.R, x.dof, rg.spb);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }

@@ -44,6 +44,7 @@ struct MGLevel {
   VecBuf V0, Z0, kw, kt;    // Krylov basis (m+1), flexible directions (m), temporaries
   VecBuf mr_r, mr_Ar, mr_t; // MR smoother
   VecBuf mr_r16, mr_Ar16;    // the fine smoother's residual fields in BF16 (params.smoother_bf16)
+  int mr_keep = 1;           // residual fields in mr_r16: every step's (smoother_iters) or one
   VecBuf bc, xc;            // right-hand side / solution of this level inside the cycle above
   VecBuf tv;                // test vectors (nvec[l]) the basis to level l+1 is built from
   // device state of this level's solver inside a captured K-cycle: Hessenberg
@@ -287,6 +288,25 @@ gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStre
     // FP32 solution): the smoother's sweeps move half the bytes
     Vec r16 = L.mr_r16.with_rhs(R), Ar16 = L.mr_Ar16.with_rhs(R);
     GMG_TRY(vec_xmy_bf16(b, r, r16, s));  // r = b - A x
+    if (iters <= L.mr_keep) {
+      // every step's residual kept (r_j at j * fs words, its step length at
+      // d1 + 2 R j): x += sum_j a_j r_j in one sweep at the end, so a step
+      // moves r, Ar and the next r, and x is read and written once
+      const int64_t fs = r16.elems();
+      for (int it = 0; it < iters; ++it) {
+        Vec rj = r16;
+        rj.p = static_cast<uint32_t*>(r16.p) + it * fs;
+        double2* a1 = d1 + 2 * (size_t)R * it;
+        GMG_TRY(wilson_apply_mr_bf16(L.w, R, static_cast<const uint32_t*>(rj.p), static_cast<uint32_t*>(Ar16.p), a1,
+                                     a1 + R, s));
+        if (it + 1 < iters) {
+          Vec rn = rj;
+          rn.p = static_cast<uint32_t*>(rj.p) + fs;
+          GMG_TRY(vec_mr_resid_bf16(a1, a1 + R, rj, Ar16, rn, s));
+        }
+      }
+      return vec_mr_xsum_bf16(d1, 2 * R, iters, r16, fs, x, s);
+    }
     for (int it = 0; it < iters; ++it) {
       GMG_TRY(wilson_apply_mr_bf16(L.w, R, static_cast<const uint32_t*>(r16.p), static_cast<uint32_t*>(Ar16.p), d1,
                                    d2, s));
@@ -989,7 +1009,7 @@ gmg_status alloc_level_ws(MGLevel& L, int R, bool krylov, bool flexible) {
   GMG_TRY(L.mr_Ar.alloc(L.V, R, L.dof, p));
   GMG_TRY(L.mr_t.alloc(L.V, R, L.dof, p));
   if (L.l == 0 && L.bf16_smoother) {
-    GMG_TRY(L.mr_r16.alloc(L.V, R, L.dof, GMG_BF16));
+    GMG_TRY(alloc_fields(L.mr_r16, L.V, R, L.dof, GMG_BF16, L.mr_keep));
     GMG_TRY(L.mr_Ar16.alloc(L.V, R, L.dof, GMG_BF16));
   }
   if (L.l > 0) {
@@ -1161,6 +1181,9 @@ extern "C" gmg_status gmg_mg_create(gmg_wilson* fine, const gmg_mg_params* p, in
     L->compute = p->prec == GMG_BF16 && l > 0 ? GMG_BF16 : L->vprec;
     L->bf16_smoother = l == 0 && L->vprec == GMG_F32 &&
                        (p->smoother_bf16 > 0 || (p->smoother_bf16 < 0 && p->prec == GMG_BF16));
+    if (L->bf16_smoother && p->smoother_iters >= 1 && p->smoother_iters <= kMrMaxSteps &&
+        2 * (int64_t)max_rhs * p->smoother_iters <= kScalars / 2)
+      L->mr_keep = p->smoother_iters;
     L->w = l == 0 ? fine : nullptr;
     h->L.push_back(L);
     if (l + 1 < p->nlevels) {
