@@ -385,7 +385,9 @@ __global__ void __launch_bounds__(MODE == 1 ? kAxDot1Threads : kAxDotThreads) mu
   }
 }
 
-// Delayed-reorthogonalisation Gram-Schmidt (DCGS2), FP64.  V_0 .. V_{NV-1}
+// Delayed-reorthogonalisation Gram-Schmidt (DCGS2): vectors stored as T
+// (FP64, or FP32 for an FP32 Arnoldi cycle), products and updates formed in
+// FP64.  V_0 .. V_{NV-1}
 // are the finished basis vectors, A = V_NV the last one after one projection
 // (its second projection delayed to this step), B the new operator product.
 // Pass 1 (one sweep): out[k * R + r] for k < NV: <V_k, A>; NV <= k < 2 NV:
@@ -393,10 +395,12 @@ __global__ void __launch_bounds__(MODE == 1 ? kAxDot1Threads : kAxDotThreads) mu
 constexpr int kDcgsThreads = 384;
 constexpr int kDcgsMaxNV = 9;
 
-template <int NV>
-__global__ void __launch_bounds__(kDcgsThreads) dcgs_dots_row_kernel(const double2* __restrict__ V0, int64_t vstride,
-                                                                     const double2* __restrict__ B, int64_t V, int R,
-                                                                     int dof, int spb, double2* __restrict__ out) {
+template <int NV, class T = double>
+__global__ void __launch_bounds__(kDcgsThreads) dcgs_dots_row_kernel(const typename C2<T>::t* __restrict__ V0,
+                                                                     int64_t vstride,
+                                                                     const typename C2<T>::t* __restrict__ B, int64_t V,
+                                                                     int R, int dof, int spb,
+                                                                     double2* __restrict__ out) {
   extern __shared__ double part[];  // [8][NT]
   constexpr int NP = 2 * NV + 3;
   const int RD = R * dof, t = threadIdx.x, NT = blockDim.x;
@@ -410,8 +414,12 @@ __global__ void __launch_bounds__(kDcgsThreads) dcgs_dots_row_kernel(const doubl
       const int64_t e = st * RD + i;
       double2 xv[NV + 1];
 #pragma unroll
-      for (int k = 0; k <= NV; ++k) xv[k] = V0[k * vstride + e];
-      const double2 a = xv[NV], b = B[e];
+      for (int k = 0; k <= NV; ++k) {
+        const typename C2<T>::t q = V0[k * vstride + e];
+        xv[k] = make_double2(q.x, q.y);
+      }
+      const typename C2<T>::t bq = B[e];
+      const double2 a = xv[NV], b = make_double2(bq.x, bq.y);
 #pragma unroll
       for (int k = 0; k < NV; ++k) {
         pr[k] += xv[k].x * a.x + xv[k].y * a.y;
@@ -470,11 +478,13 @@ __global__ void __launch_bounds__(kDcgsThreads) dcgs_dots_row_kernel(const doubl
 // vector, in place), then V_{NV+1} <- (B - sum_k g_k V_k - d A) / beta (the
 // next one after one projection).  cf per RHS: c[NV], g[NV], (1/alpha, 0),
 // d, (1/beta, 0), at cf[k * R + r].
-template <int NV>
+template <int NV, class T = double>
 __global__ void __launch_bounds__(kDcgsThreads) dcgs_update_row_kernel(const double2* __restrict__ cfg,
-                                                                       double2* __restrict__ V0, int64_t vstride,
-                                                                       const double2* __restrict__ B, int64_t V, int R,
-                                                                       int dof, int spb) {
+                                                                       typename C2<T>::t* __restrict__ V0,
+                                                                       int64_t vstride,
+                                                                       const typename C2<T>::t* __restrict__ B,
+                                                                       int64_t V, int R, int dof, int spb) {
+  typedef typename C2<T>::t CT;
   extern __shared__ double2 cf[];  // [2 NV + 3][R]
   constexpr int NC = 2 * NV + 3;
   const int RD = R * dof, t = threadIdx.x;
@@ -486,8 +496,11 @@ __global__ void __launch_bounds__(kDcgsThreads) dcgs_update_row_kernel(const dou
     const int64_t e = st * RD + i;
     double2 xv[NV + 1];
 #pragma unroll
-    for (int k = 0; k <= NV; ++k) xv[k] = V0[k * vstride + e];
-    const double2 b = B[e];
+    for (int k = 0; k <= NV; ++k) {
+      const CT q = V0[k * vstride + e];
+      xv[k] = make_double2(q.x, q.y);
+    }
+    const CT b = B[e];
     double ar = xv[NV].x, ai = xv[NV].y, br = b.x, bi = b.y;
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
@@ -504,15 +517,16 @@ __global__ void __launch_bounds__(kDcgsThreads) dcgs_update_row_kernel(const dou
     ai *= ia;
     br -= d.x * ar - d.y * ai;
     bi -= d.x * ai + d.y * ar;
-    V0[NV * vstride + e] = make_double2(ar, ai);
-    V0[(NV + 1) * vstride + e] = make_double2(br * ib, bi * ib);
+    V0[NV * vstride + e] = CT{(T)ar, (T)ai};
+    V0[(NV + 1) * vstride + e] = CT{(T)(br * ib), (T)(bi * ib)};
   }
 }
 
-// Y(r) = X(r) / sqrt(n[r].x)
-template <class T>
+// Y(r) = X(r) / sqrt(n[r].x), X of type TX, Y of type T (FP64 -> FP32: the
+// first Krylov vector of an FP32 Arnoldi cycle from the FP64 residual)
+template <class T, class TX = T>
 __global__ void __launch_bounds__(1024) scale_inv_norm_row_kernel(const double2* __restrict__ n,
-                                                                  const typename C2<T>::t* __restrict__ X,
+                                                                  const typename C2<TX>::t* __restrict__ X,
                                                                   typename C2<T>::t* __restrict__ Y, int64_t V, int R,
                                                                   int dof, int spb) {
   const int RD = R * dof, t = threadIdx.x;
@@ -586,16 +600,22 @@ __global__ void __launch_bounds__(1024) mr_update_bf16_row_kernel(const double2*
   }
 }
 
-// rn = bf16(r - a Ar): one MR step on residuals that the sweep keeps
+// word i of a site's R x 12 block in the site-blocked BF16 layout [3][R][4]
+// <-> (RHS, component) of the [R][12] layout
+__device__ __forceinline__ int blocked_rhs(int i, int R) { return (i % (4 * R)) / 4; }
+__device__ __forceinline__ int blocked_word(int r, int c, int R) { return (c / 4) * 4 * R + r * 4 + c % 4; }
+
+// rn = bf16(r - a Ar): one MR step on residuals that the sweep keeps (fields
+// [V][R][dof], or site-blocked [V][3][R][4] words with `blocked`, dof 12)
 __global__ void __launch_bounds__(1024) mr_resid_bf16_row_kernel(const double2* __restrict__ d1,
                                                                  const double2* __restrict__ d2,
                                                                  const uint32_t* __restrict__ r,
                                                                  const uint32_t* __restrict__ Ar,
                                                                  uint32_t* __restrict__ rn, int64_t V, int R, int dof,
-                                                                 int spb) {
+                                                                 int spb, bool blocked) {
   const int RD = R * dof, t = threadIdx.x;
   if (t >= spb * RD) return;
-  const int so = t / RD, i = t % RD, k = i / dof;
+  const int so = t / RD, i = t % RD, k = blocked ? blocked_rhs(i, R) : i / dof;
   const double den = d2[k].x;
   const float ar = den > 0.0 ? (float)(d1[k].x / den) : 0.f, ai = den > 0.0 ? (float)(d1[k].y / den) : 0.f;
   for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
@@ -607,41 +627,56 @@ __global__ void __launch_bounds__(1024) mr_resid_bf16_row_kernel(const double2* 
 
 // x += sum_j a_j r_j over the K kept residuals of an MR sweep: the solution is
 // read and written once per sweep instead of once per step
-__global__ void __launch_bounds__(1024) mr_xsum_bf16_row_kernel(const double2* __restrict__ d, int dstride, int K,
+// (K a template argument: the step lengths and the K loaded words stay in
+// registers)
+template <int K>
+__global__ void __launch_bounds__(1024) mr_xsum_bf16_row_kernel(const double2* __restrict__ d, int dstride,
                                                                 const uint32_t* __restrict__ r0, int64_t rstride,
                                                                 float2* __restrict__ x, int64_t V, int R, int dof,
-                                                                int spb) {
+                                                                int spb, bool blocked) {
   const int RD = R * dof, t = threadIdx.x;
   if (t >= spb * RD) return;
   const int so = t / RD, i = t % RD, k = i / dof;
-  float2 a[kMrMaxSteps];
+  const int ri = blocked ? blocked_word(k, i % dof, R) : i;  // the same (RHS, component) in the residuals
+  float2 a[K];
 #pragma unroll
-  for (int j = 0; j < kMrMaxSteps; ++j) {
+  for (int j = 0; j < K; ++j) {
     a[j] = make_float2(0.f, 0.f);
-    if (j < K) {
-      const double den = d[(int64_t)j * dstride + R + k].x;
-      const double2 num = d[(int64_t)j * dstride + k];
-      if (den > 0.0) a[j] = make_float2((float)(num.x / den), (float)(num.y / den));
-    }
+    const double den = d[(int64_t)j * dstride + R + k].x;
+    const double2 num = d[(int64_t)j * dstride + k];
+    if (den > 0.0) a[j] = make_float2((float)(num.x / den), (float)(num.y / den));
   }
   for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
     const int64_t e = s * RD + i;
-    uint32_t w[kMrMaxSteps];
+    uint32_t w[K];
 #pragma unroll
-    for (int j = 0; j < kMrMaxSteps; ++j)
-      if (j < K) w[j] = __ldg(r0 + j * rstride + e);
+    for (int j = 0; j < K; ++j) w[j] = __ldg(r0 + j * rstride + s * RD + ri);
     float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int j = 0; j < kMrMaxSteps; ++j)
-      if (j < K) {
-        const float2 v = bf16w_to_f2(w[j]);
-        acc.x += a[j].x * v.x - a[j].y * v.y;
-        acc.y += a[j].x * v.y + a[j].y * v.x;
-      }
+    for (int j = 0; j < K; ++j) {
+      const float2 v = bf16w_to_f2(w[j]);
+      acc.x += a[j].x * v.x - a[j].y * v.y;
+      acc.y += a[j].x * v.y + a[j].y * v.x;
+    }
     float2 xv = x[e];
     xv.x += acc.x;
     xv.y += acc.y;
     x[e] = xv;
+  }
+}
+
+// Z (BF16, site-blocked [V][3][R][4] words) = X - Y (FP32, [V][R][12])
+__global__ void __launch_bounds__(1024) xmy_bf16_blocked_row_kernel(const float2* __restrict__ X,
+                                                                    const float2* __restrict__ Y,
+                                                                    uint32_t* __restrict__ Z, int64_t V, int R,
+                                                                    int spb) {
+  const int RD = R * 12, t = threadIdx.x;
+  if (t >= spb * RD) return;
+  const int so = t / RD, i = t % RD;
+  const int src = blocked_rhs(i, R) * 12 + (i / (4 * R)) * 4 + i % 4;
+  for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+    const float2 a = X[s * RD + src], b = Y[s * RD + src];
+    Z[s * RD + i] = f2_to_bf16w(a.x - b.x, a.y - b.y);
   }
 }
 
@@ -879,6 +914,15 @@ __global__ void xmy_kernel(const typename C2<T>::t* __restrict__ X, typename C2<
 }  // namespace blas
 
 gmg_status vec_scale_inv_norm(const double2* n_dev, const Vec& X, Vec& Y, cudaStream_t s) {
+  if (X.prec != Y.prec) {
+    GMG_CHECK(X.prec == GMG_F64 && Y.prec == GMG_F32 && Y.R * Y.dof <= 1024 && X.elems() == Y.elems(),
+              GMG_ERR_UNSUPPORTED, "scale: mixed precision only FP64 -> FP32 with at most 1024 values per site");
+    const blas::Row rg = blas::row_geom(Y.V, Y.R, Y.dof);
+    blas::scale_inv_norm_row_kernel<float, double><<<rg.grid, rg.threads, 0, s>>>(
+        n_dev, (const double2*)X.p, (float2*)Y.p, Y.V, Y.R, Y.dof, rg.spb);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  }
   if (Y.R * Y.dof <= 1024) {
     const blas::Row rg = blas::row_geom(Y.V, Y.R, Y.dof);
     if (Y.prec == GMG_F64)
@@ -978,23 +1022,45 @@ gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, c
 }
 
 gmg_status vec_mr_resid_bf16(const double2* d1, const double2* d2, const Vec& r, const Vec& Ar, Vec& rn,
-                             cudaStream_t s) {
-  GMG_CHECK(r.prec == GMG_BF16 && Ar.prec == GMG_BF16 && rn.prec == GMG_BF16 && r.R * r.dof <= 1024,
+                             cudaStream_t s, bool blocked) {
+  GMG_CHECK(r.prec == GMG_BF16 && Ar.prec == GMG_BF16 && rn.prec == GMG_BF16 && r.R * r.dof <= 1024 &&
+                (!blocked || r.dof == 12),
             GMG_ERR_UNSUPPORTED, "mr residual: BF16 fields with at most 1024 values per site");
   const blas::Row rg = blas::row_geom(r.V, r.R, r.dof);
   blas::mr_resid_bf16_row_kernel<<<rg.grid, rg.threads, 0, s>>>(d1, d2, (const uint32_t*)r.p, (const uint32_t*)Ar.p,
-                                                               (uint32_t*)rn.p, r.V, r.R, r.dof, rg.spb);
+                                                               (uint32_t*)rn.p, r.V, r.R, r.dof, rg.spb, blocked);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
 
 gmg_status vec_mr_xsum_bf16(const double2* d, int dstride, int K, const Vec& r0, int64_t rstride, Vec& x,
-                            cudaStream_t s) {
-  GMG_CHECK(r0.prec == GMG_BF16 && x.prec == GMG_F32 && K >= 1 && K <= kMrMaxSteps && x.R * x.dof <= 1024,
+                            cudaStream_t s, bool blocked) {
+  GMG_CHECK(r0.prec == GMG_BF16 && x.prec == GMG_F32 && K >= 1 && K <= kMrMaxSteps && x.R * x.dof <= 1024 &&
+                (!blocked || x.dof == 12),
             GMG_ERR_UNSUPPORTED, "mr sum: BF16 residuals, an FP32 solution, 1 to 16 steps");
   const blas::Row rg = blas::row_geom(x.V, x.R, x.dof);
-  blas::mr_xsum_bf16_row_kernel<<<rg.grid, rg.threads, 0, s>>>(d, dstride, K, (const uint32_t*)r0.p, rstride,
-                                                              (float2*)x.p, x.V, x.R, x.dof, rg.spb);
+  auto go = [&](auto kern) {
+    kern<<<rg.grid, rg.threads, 0, s>>>(d, dstride, (const uint32_t*)r0.p, rstride, (float2*)x.p, x.V, x.R, x.dof,
+                                        rg.spb, blocked);
+  };
+  switch (K) {
+    case 1: go(blas::mr_xsum_bf16_row_kernel<1>); break;
+    case 2: go(blas::mr_xsum_bf16_row_kernel<2>); break;
+    case 3: go(blas::mr_xsum_bf16_row_kernel<3>); break;
+    case 4: go(blas::mr_xsum_bf16_row_kernel<4>); break;
+    case 5: go(blas::mr_xsum_bf16_row_kernel<5>); break;
+    case 6: go(blas::mr_xsum_bf16_row_kernel<6>); break;
+    case 7: go(blas::mr_xsum_bf16_row_kernel<7>); break;
+    case 8: go(blas::mr_xsum_bf16_row_kernel<8>); break;
+    case 9: go(blas::mr_xsum_bf16_row_kernel<9>); break;
+    case 10: go(blas::mr_xsum_bf16_row_kernel<10>); break;
+    case 11: go(blas::mr_xsum_bf16_row_kernel<11>); break;
+    case 12: go(blas::mr_xsum_bf16_row_kernel<12>); break;
+    case 13: go(blas::mr_xsum_bf16_row_kernel<13>); break;
+    case 14: go(blas::mr_xsum_bf16_row_kernel<14>); break;
+    case 15: go(blas::mr_xsum_bf16_row_kernel<15>); break;
+    default: go(blas::mr_xsum_bf16_row_kernel<16>); break;
+  }
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
@@ -1009,7 +1075,8 @@ gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s) {
 }
 
 bool vec_dcgs_supported(const Vec& Y, int nv) {
-  return Y.prec == GMG_F64 && nv >= 0 && nv <= blas::kDcgsMaxNV && Y.R * Y.dof <= blas::kDcgsThreads;
+  return (Y.prec == GMG_F64 || Y.prec == GMG_F32) && nv >= 0 && nv <= blas::kDcgsMaxNV &&
+         Y.R * Y.dof <= blas::kDcgsThreads;
 }
 
 gmg_status vec_dcgs_dots(const Vec& V0, int64_t vstride, int nv, const Vec& B, double2* out_dev, cudaStream_t s) {
@@ -1019,25 +1086,31 @@ gmg_status vec_dcgs_dots(const Vec& V0, int64_t vstride, int nv, const Vec& B, d
   const blas::Row g = blas::row_geom(B.V, B.R, B.dof);
   const size_t sm = sizeof(double) * 8 * g.threads;
   const int grid = std::min(g.grid, 148 * std::max(1, 2048 / g.threads));
-  auto launch = [&](auto kern) -> gmg_status {
+  GMG_CHECK(V0.prec == B.prec, GMG_ERR_UNSUPPORTED, "dcgs: basis and new vector differ in precision");
+  auto launch = [&](auto kern, auto* p) -> gmg_status {
+    typedef std::remove_pointer_t<decltype(p)> CT;
     if (sm > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    kern<<<grid, g.threads, sm, s>>>((const double2*)V0.p, vstride, (const double2*)B.p, B.V, B.R, B.dof, g.spb,
-                                     out_dev);
+    kern<<<grid, g.threads, sm, s>>>((const CT*)V0.p, vstride, (const CT*)B.p, B.V, B.R, B.dof, g.spb, out_dev);
     GMG_CUDA(cudaGetLastError());
     return GMG_OK;
   };
-  switch (nv) {
-    case 0: return launch(blas::dcgs_dots_row_kernel<0>);
-    case 1: return launch(blas::dcgs_dots_row_kernel<1>);
-    case 2: return launch(blas::dcgs_dots_row_kernel<2>);
-    case 3: return launch(blas::dcgs_dots_row_kernel<3>);
-    case 4: return launch(blas::dcgs_dots_row_kernel<4>);
-    case 5: return launch(blas::dcgs_dots_row_kernel<5>);
-    case 6: return launch(blas::dcgs_dots_row_kernel<6>);
-    case 7: return launch(blas::dcgs_dots_row_kernel<7>);
-    case 8: return launch(blas::dcgs_dots_row_kernel<8>);
-    default: return launch(blas::dcgs_dots_row_kernel<9>);
-  }
+  auto run = [&](auto* p) -> gmg_status {
+    typedef std::conditional_t<std::is_same<std::remove_pointer_t<decltype(p)>, float2>::value, float, double> T;
+    switch (nv) {
+      case 0: return launch(blas::dcgs_dots_row_kernel<0, T>, p);
+      case 1: return launch(blas::dcgs_dots_row_kernel<1, T>, p);
+      case 2: return launch(blas::dcgs_dots_row_kernel<2, T>, p);
+      case 3: return launch(blas::dcgs_dots_row_kernel<3, T>, p);
+      case 4: return launch(blas::dcgs_dots_row_kernel<4, T>, p);
+      case 5: return launch(blas::dcgs_dots_row_kernel<5, T>, p);
+      case 6: return launch(blas::dcgs_dots_row_kernel<6, T>, p);
+      case 7: return launch(blas::dcgs_dots_row_kernel<7, T>, p);
+      case 8: return launch(blas::dcgs_dots_row_kernel<8, T>, p);
+      default: return launch(blas::dcgs_dots_row_kernel<9, T>, p);
+    }
+  };
+  if (B.prec == GMG_F32) return run((float2*)nullptr);
+  return run((double2*)nullptr);
 }
 
 gmg_status vec_dcgs_update(const double2* coef_dev, Vec& V0, int64_t vstride, int nv, const Vec& B, cudaStream_t s) {
@@ -1045,24 +1118,41 @@ gmg_status vec_dcgs_update(const double2* coef_dev, Vec& V0, int64_t vstride, in
   const blas::Row g = blas::row_geom(B.V, B.R, B.dof);
   const size_t sm = sizeof(double2) * (2 * nv + 3) * B.R;
   const int grid = std::min(g.grid, 148 * std::max(1, 2048 / g.threads));
-  auto launch = [&](auto kern) -> gmg_status {
+  GMG_CHECK(V0.prec == B.prec, GMG_ERR_UNSUPPORTED, "dcgs: basis and new vector differ in precision");
+  auto launch = [&](auto kern, auto* p) -> gmg_status {
+    typedef std::remove_pointer_t<decltype(p)> CT;
     if (sm > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    kern<<<grid, g.threads, sm, s>>>(coef_dev, (double2*)V0.p, vstride, (const double2*)B.p, B.V, B.R, B.dof, g.spb);
+    kern<<<grid, g.threads, sm, s>>>(coef_dev, (CT*)V0.p, vstride, (const CT*)B.p, B.V, B.R, B.dof, g.spb);
     GMG_CUDA(cudaGetLastError());
     return GMG_OK;
   };
-  switch (nv) {
-    case 0: return launch(blas::dcgs_update_row_kernel<0>);
-    case 1: return launch(blas::dcgs_update_row_kernel<1>);
-    case 2: return launch(blas::dcgs_update_row_kernel<2>);
-    case 3: return launch(blas::dcgs_update_row_kernel<3>);
-    case 4: return launch(blas::dcgs_update_row_kernel<4>);
-    case 5: return launch(blas::dcgs_update_row_kernel<5>);
-    case 6: return launch(blas::dcgs_update_row_kernel<6>);
-    case 7: return launch(blas::dcgs_update_row_kernel<7>);
-    case 8: return launch(blas::dcgs_update_row_kernel<8>);
-    default: return launch(blas::dcgs_update_row_kernel<9>);
-  }
+  auto run = [&](auto* p) -> gmg_status {
+    typedef std::conditional_t<std::is_same<std::remove_pointer_t<decltype(p)>, float2>::value, float, double> T;
+    switch (nv) {
+      case 0: return launch(blas::dcgs_update_row_kernel<0, T>, p);
+      case 1: return launch(blas::dcgs_update_row_kernel<1, T>, p);
+      case 2: return launch(blas::dcgs_update_row_kernel<2, T>, p);
+      case 3: return launch(blas::dcgs_update_row_kernel<3, T>, p);
+      case 4: return launch(blas::dcgs_update_row_kernel<4, T>, p);
+      case 5: return launch(blas::dcgs_update_row_kernel<5, T>, p);
+      case 6: return launch(blas::dcgs_update_row_kernel<6, T>, p);
+      case 7: return launch(blas::dcgs_update_row_kernel<7, T>, p);
+      case 8: return launch(blas::dcgs_update_row_kernel<8, T>, p);
+      default: return launch(blas::dcgs_update_row_kernel<9, T>, p);
+    }
+  };
+  if (B.prec == GMG_F32) return run((float2*)nullptr);
+  return run((double2*)nullptr);
+}
+
+gmg_status vec_xmy_bf16_blocked(const Vec& X, const Vec& Y, Vec& Z, cudaStream_t s) {
+  GMG_CHECK(X.prec == GMG_F32 && Y.prec == GMG_F32 && Z.prec == GMG_BF16 && X.dof == 12 && X.R * 12 <= 1024,
+            GMG_ERR_UNSUPPORTED, "xmy (site-blocked BF16): FP32 spin-colour inputs");
+  const blas::Row rg = blas::row_geom(X.V, X.R, 12);
+  blas::xmy_bf16_blocked_row_kernel<<<rg.grid, rg.threads, 0, s>>>((const float2*)X.p, (const float2*)Y.p,
+                                                                  (uint32_t*)Z.p, X.V, X.R, rg.spb);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
 }
 
 gmg_status vec_xmy_bf16(const Vec& X, const Vec& Y, Vec& Z, cudaStream_t s) {

@@ -219,8 +219,10 @@ gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, 
 gmg_status wilson_apply_mr(gmg_wilson* h, int vec_prec, int nrhs, const void* in, void* out, double2* d1,
                            double2* d2, cudaStream_t s);
 gmg_status wilson_apply_f32_in(gmg_wilson* h, int op, int nrhs, const float* in, double* out, cudaStream_t s);
+// BF16 fields [V][nrhs][12] words, or with `blocked` the site-blocked layout
+// [V][3][nrhs][4] (the 16-byte quarters of one site's records back to back)
 gmg_status wilson_apply_mr_bf16(gmg_wilson* h, int nrhs, const uint32_t* in, uint32_t* out, double2* d1, double2* d2,
-                                cudaStream_t s);
+                                cudaStream_t s, bool blocked = false);
 
 // coarse-operator construction (coarsen.cu)
 gmg_status coarsen_wilson(gmg_coarse* out, gmg_agg* agg, gmg_wilson* fine, cudaStream_t s);

@@ -69,8 +69,11 @@ struct gmg_mg {
   gmg::DevBuf dscr;        // device-only per-RHS scalars: dots, norms (double2)
   double2* hpin = nullptr; // pinned host staging for coefficient transfers
   bool setup_done = false;
-  // outer FGMRES workspace for max_rhs right-hand sides, allocated once
-  gmg::VecBuf oV0, oZ0, ow, ot64, otz, obb, oxx;
+  // outer FGMRES workspace for max_rhs right-hand sides, allocated once.  The
+  // Arnoldi fields (oV0, ow, otv, owc) are FP32 with params.arnoldi_f32, else
+  // FP64; the residuals (orr: all RHS, orA: the batch) and ot64 are FP64.
+  bool arn32 = false;
+  gmg::VecBuf oV0, oZ0, ow, ot64, otz, obb, oxx, otv, orr, orA;
   gmg::VecBuf ozc, owc;   // compacted preconditioner output / operator output (in-cycle drop)
   gmg::DevBuf oidx, oidx2;
   bool outer_ready = false;
@@ -287,26 +290,29 @@ gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStre
     // the residual and the operator product kept in BF16 (FP32 arithmetic,
     // FP32 solution): the smoother's sweeps move half the bytes
     Vec r16 = L.mr_r16.with_rhs(R), Ar16 = L.mr_Ar16.with_rhs(R);
-    GMG_TRY(vec_xmy_bf16(b, r, r16, s));  // r = b - A x
     if (iters <= L.mr_keep) {
       // every step's residual kept (r_j at j * fs words, its step length at
       // d1 + 2 R j): x += sum_j a_j r_j in one sweep at the end, so a step
-      // moves r, Ar and the next r, and x is read and written once
+      // moves r, Ar and the next r, and x is read and written once.  The
+      // residual fields are site-blocked (the quarters of one site's records
+      // back to back), so the operator's record gathers read contiguous runs.
+      GMG_TRY(vec_xmy_bf16_blocked(b, r, r16, s));  // r = b - A x
       const int64_t fs = r16.elems();
       for (int it = 0; it < iters; ++it) {
         Vec rj = r16;
         rj.p = static_cast<uint32_t*>(r16.p) + it * fs;
         double2* a1 = d1 + 2 * (size_t)R * it;
         GMG_TRY(wilson_apply_mr_bf16(L.w, R, static_cast<const uint32_t*>(rj.p), static_cast<uint32_t*>(Ar16.p), a1,
-                                     a1 + R, s));
+                                     a1 + R, s, true));
         if (it + 1 < iters) {
           Vec rn = rj;
           rn.p = static_cast<uint32_t*>(rj.p) + fs;
-          GMG_TRY(vec_mr_resid_bf16(a1, a1 + R, rj, Ar16, rn, s));
+          GMG_TRY(vec_mr_resid_bf16(a1, a1 + R, rj, Ar16, rn, s, true));
         }
       }
-      return vec_mr_xsum_bf16(d1, 2 * R, iters, r16, fs, x, s);
+      return vec_mr_xsum_bf16(d1, 2 * R, iters, r16, fs, x, s, true);
     }
+    GMG_TRY(vec_xmy_bf16(b, r, r16, s));  // r = b - A x
     for (int it = 0; it < iters; ++it) {
       GMG_TRY(wilson_apply_mr_bf16(L.w, R, static_cast<const uint32_t*>(r16.p), static_cast<uint32_t*>(Ar16.p), d1,
                                    d2, s));
@@ -355,6 +361,10 @@ struct DropCtx {
   bool dcgs = false;           // Gram-Schmidt with delayed reorthogonalisation (params.outer_dcgs)
   std::vector<int> conv_step;  // out: per column, the step (1-based) its estimate met tol; 0: never
   std::vector<int>* batches = nullptr;  // out: appended active-batch size of every step
+  // FP64 residual b - A x of the batch, formed by the caller: one restart
+  // cycle starts from it (the first Krylov vector in the basis precision)
+  // and the solve returns after that cycle, the caller forming the next one
+  const Vec* r0 = nullptr;
 };
 
 // min |beta0 e1 - H y| over y for the (n + 1) x n upper Hessenberg H (row
@@ -413,15 +423,20 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
   // DCGS2 (outer solve): H kept unrotated, with each column corrected one step
   // later for the delayed second projection of its last basis vector
   const bool dcgs = drop && drop->dcgs && flexible && vec_dcgs_supported(K.w.with_rhs(R), m - 1);
-  std::vector<double> beta0(R, 0.0), betaT(R, 0.0);
-  while (true) {
-    // r0 = b - A x -> V_0
+  std::vector<double> beta0(R, 0.0), betaT(R, 0.0), ctol(R, tol);
+  const Vec* r0 = drop ? drop->r0 : nullptr;
+  for (int cycle = 0;; ++cycle) {
+    // r0 = b - A x -> V_0 (given by the caller for one cycle, or formed here)
     Vec v0 = nth(V0, 0);
-    GMG_TRY(apply_op(h, l, x, w, s));
-    GMG_TRY(vec_xmy(b, w, s));  // w = b - A x
+    if (r0 && cycle > 0) break;
+    if (!r0) {
+      GMG_TRY(apply_op(h, l, x, w, s));
+      GMG_TRY(vec_xmy(b, w, s));  // w = b - A x
+    }
+    const Vec& rv = r0 ? *r0 : w;
     std::vector<zc> bb;
     double2* dn = h->dscr.as<double2>();
-    GMG_TRY(vec_multidot(w, 1, 0, w, dn, nullptr, s));
+    GMG_TRY(vec_multidot(rv, 1, 0, rv, dn, nullptr, s));
     GMG_TRY(download(h, dn, R, bb, s));
     bool all = true;
     std::vector<double> beta(R);
@@ -431,11 +446,17 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
       if (res[r] > tol) all = false;
     }
     if (all || iters >= maxit) break;
+    // a cycle in FP32 (the basis precision) cannot reduce a residual by much
+    // more than FP32 resolves: a column whose estimate falls to 1e-6 of the
+    // cycle's starting residual has done what the cycle can do, and is treated
+    // as converged for this cycle (the caller's FP64 residual decides)
+    const double floor = V0.prec == GMG_F32 ? 1e-6 : 0.0;
+    for (int r = 0; r < R; ++r) ctol[r] = std::max(tol, floor * res[r]);
     // a new cycle: every column takes part again (dropped ones have been folded into x)
     std::fill(live.begin(), live.end(), 1);
     act.resize(R);
     for (int r = 0; r < R; ++r) act[r] = r;
-    GMG_TRY(vec_scale_inv_norm(dn, w, v0, s));
+    GMG_TRY(vec_scale_inv_norm(dn, rv, v0, s));
     std::fill(H.begin(), H.end(), zc(0));
     std::fill(g.begin(), g.end(), zc(0));
     for (int r = 0; r < R; ++r) g[(size_t)r * (m + 1)] = beta[r];  // per-RHS residual vector, [R][m+1]
@@ -572,10 +593,10 @@ gmg_status fgmres(gmg_mg* h, int l, const Vec& b, Vec& x, const Krylov& K, int m
       bool conv = true, dropped = false;
       for (int r = 0; r < R; ++r) {
         if (!live[r]) continue;
-        if (res[r] > tol) {
+        if (res[r] > ctol[r]) {
           conv = false;
         } else if (drop) {
-          if (!drop->conv_step[r]) drop->conv_step[r] = iters;
+          if (!drop->conv_step[r] && res[r] <= tol) drop->conv_step[r] = iters;
           if (drop->enabled && flexible) {
             live[r] = 0;
             keep[r] = j + 1;
@@ -1019,27 +1040,30 @@ gmg_status alloc_level_ws(MGLevel& L, int R, bool krylov, bool flexible) {
   return GMG_OK;
 }
 
-// Outer FGMRES workspace for max_rhs right-hand sides (m + 1 FP64 Krylov
-// vectors, m flexible directions in the preconditioner precision, and the
-// residual / conversion / compacted-batch fields), allocated on first use and
-// kept: a solve then allocates nothing.
+// Outer FGMRES workspace for max_rhs right-hand sides (m + 1 Krylov vectors
+// in the Arnoldi precision, m flexible directions in the preconditioner
+// precision, the FP64 residuals, and the conversion / compacted-batch fields),
+// allocated on first use and kept: a solve then allocates nothing.
 gmg_status outer_workspace(gmg_mg* h) {
   if (h->outer_ready) return GMG_OK;
   MGLevel& F = *h->L[0];
   const int m = std::max(h->P.outer_restart, 2);
-  const int zp = F.vprec, R = h->Rmax;
+  const int zp = F.vprec, R = h->Rmax, vp = h->arn32 ? GMG_F32 : GMG_F64;
   const int64_t V = F.V;
-  GMG_TRY(alloc_fields(h->oV0, V, R, 12, GMG_F64, m + 1));
+  GMG_TRY(alloc_fields(h->oV0, V, R, 12, vp, m + 1));
   GMG_TRY(alloc_fields(h->oZ0, V, R, 12, zp, m));
-  GMG_TRY(h->ow.alloc(V, R, 12, GMG_F64));
+  GMG_TRY(h->ow.alloc(V, R, 12, vp));
   GMG_TRY(h->ot64.alloc(V, R, 12, GMG_F64));
+  if (vp != GMG_F64) GMG_TRY(h->otv.alloc(V, R, 12, vp));
+  GMG_TRY(h->orr.alloc(V, R, 12, GMG_F64));
+  GMG_TRY(h->orA.alloc(V, R, 12, GMG_F64));
   GMG_TRY(h->otz.alloc(V, R, 12, zp));
   GMG_TRY(h->obb.alloc(V, R, 12, GMG_F64));
   GMG_TRY(h->oxx.alloc(V, R, 12, GMG_F64));
   GMG_TRY(h->oidx.alloc(sizeof(int) * R));
   if (h->P.drop_in_cycle) {
     GMG_TRY(h->ozc.alloc(V, R, 12, zp));
-    GMG_TRY(h->owc.alloc(V, R, 12, GMG_F64));
+    GMG_TRY(h->owc.alloc(V, R, 12, vp));
     GMG_TRY(h->oidx2.alloc(sizeof(int) * R));
   }
   if (h->P.graph && zp != GMG_F64) GMG_TRY(h->ogz.alloc(V, R, 12, zp));
@@ -1054,9 +1078,9 @@ gmg_status outer_workspace(gmg_mg* h) {
 gmg_status pretune_fine(gmg_mg* h, cudaStream_t s) {
   MGLevel& F = *h->L[0];
   const int R = h->Rmax, zp = F.vprec;
-  GMG_CUDA(cudaMemsetAsync(h->ow.p, 0, h->ow.bytes(), s));
+  GMG_CUDA(cudaMemsetAsync(h->orr.p, 0, h->orr.bytes(), s));
   GMG_CUDA(cudaMemsetAsync(h->otz.p, 0, h->otz.bytes(), s));
-  GMG_TRY(gmg_wilson_apply(F.w, GMG_OP_M, 0, 0, GMG_F64, R, h->ow.p, h->ot64.p, (gmg_stream)s));
+  GMG_TRY(gmg_wilson_apply(F.w, GMG_OP_M, 0, 0, GMG_F64, R, h->orr.p, h->ot64.p, (gmg_stream)s));
   if (zp != GMG_F64) {
     Vec z0 = nth(h->oZ0, 0);
     GMG_TRY(gmg_wilson_apply(F.w, GMG_OP_M, 0, 0, (gmg_prec)zp, R, h->otz.p, z0.p, (gmg_stream)s));
@@ -1064,7 +1088,7 @@ gmg_status pretune_fine(gmg_mg* h, cudaStream_t s) {
   if (h->P.smoother_iters > 0) {
     Vec z0 = nth(h->oZ0, 0);
     double2* d1 = h->dscr.as<double2>() + kScalars / 2;
-    GMG_TRY(wilson_apply_mr(F.w, zp, R, zp == GMG_F64 ? h->ow.p : h->otz.p, zp == GMG_F64 ? h->ot64.p : z0.p, d1,
+    GMG_TRY(wilson_apply_mr(F.w, zp, R, zp == GMG_F64 ? h->orr.p : h->otz.p, zp == GMG_F64 ? h->ot64.p : z0.p, d1,
                             d1 + R, s));
   }
   GMG_CUDA(cudaStreamSynchronize(s));
@@ -1155,6 +1179,7 @@ extern "C" gmg_status gmg_mg_params_default(gmg_mg_params* p) {
   p->drop_in_cycle = 1;
   p->smoother_bf16 = -1;
   p->outer_dcgs = 1;
+  p->arnoldi_f32 = -1;
   return GMG_OK;
 }
 
@@ -1169,6 +1194,7 @@ extern "C" gmg_status gmg_mg_create(gmg_wilson* fine, const gmg_mg_params* p, in
   h->P = *p;
   h->fine = fine;
   h->Rmax = max_rhs;
+  h->arn32 = p->arnoldi_f32 > 0 || (p->arnoldi_f32 < 0 && p->prec != GMG_F64);
   Dims d = fine->dims;
   int dof = 12;
   for (int l = 0; l < p->nlevels; ++l) {
@@ -1181,8 +1207,10 @@ extern "C" gmg_status gmg_mg_create(gmg_wilson* fine, const gmg_mg_params* p, in
     L->compute = p->prec == GMG_BF16 && l > 0 ? GMG_BF16 : L->vprec;
     L->bf16_smoother = l == 0 && L->vprec == GMG_F32 &&
                        (p->smoother_bf16 > 0 || (p->smoother_bf16 < 0 && p->prec == GMG_BF16));
+    // the sweep that keeps every step's residual (site-blocked fields, whose
+    // operator indexes them with 32-bit offsets in 16-byte units)
     if (L->bf16_smoother && p->smoother_iters >= 1 && p->smoother_iters <= kMrMaxSteps &&
-        2 * (int64_t)max_rhs * p->smoother_iters <= kScalars / 2)
+        2 * (int64_t)max_rhs * p->smoother_iters <= kScalars / 2 && L->V * 3 * max_rhs < ((int64_t)1 << 31))
       L->mr_keep = p->smoother_iters;
     L->w = l == 0 ? fine : nullptr;
     h->L.push_back(L);
@@ -1349,10 +1377,14 @@ extern "C" gmg_status gmg_mg_refine(gmg_mg* h, gmg_stream stream) {
   return GMG_OK;
 }
 
-// Outer FGMRES in FP64 on the fine operator, preconditioned by the K-cycle in
-// the preconditioner precision.  b, x: device FP64 [V][nrhs][12]; x holds the
-// initial guess.  At every restart the still-unconverged RHS are compacted
-// into a contiguous batch, so converged ones drop out of all later work.
+// Outer FGMRES on the fine operator, preconditioned by the K-cycle in the
+// preconditioner precision.  b, x: device FP64 [V][nrhs][12]; x holds the
+// initial guess.  Every restart cycle starts from the FP64 residual b - A x
+// (formed once per cycle, after the solution update) and runs its Arnoldi
+// process in FP64 or, with params.arnoldi_f32, in FP32; the tolerance is
+// checked on that FP64 residual.  At every restart the still-unconverged RHS
+// are compacted into a contiguous batch, so converged ones drop out of all
+// later work.
 extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double* x, double tol, int maxiter,
                                    int* iters_out, double* max_relres, gmg_stream stream) {
   GMG_CHECK(h && b && x, GMG_ERR_ARGUMENT, "gmg_mg_solve: null argument");
@@ -1365,7 +1397,8 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
   const int zp = F.vprec;
   const int64_t V = F.V;
   GMG_TRY(outer_workspace(h));
-  VecBuf &V0 = h->oV0, &Z0 = h->oZ0, &w = h->ow, &t64 = h->ot64, &tz = h->otz, &bb = h->obb, &xx = h->oxx;
+  VecBuf &V0 = h->oV0, &Z0 = h->oZ0, &w = h->ow, &tz = h->otz, &bb = h->obb, &xx = h->oxx;
+  VecBuf& tv = h->arn32 ? h->otv : h->ot64;  // the batch's Krylov-precision scratch
   DevBuf& idx = h->oidx;
   Vec Bfull, Xfull;
   Bfull.p = const_cast<double*>(b);
@@ -1383,25 +1416,34 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
   // per-RHS norms of b for the global convergence criterion
   std::vector<zc> bnz;
   GMG_TRY(dots(h, Bfull, 1, 0, Bfull, bnz, s));
+  // FP64 residual of every RHS; each cycle starts from it and refreshes it
+  Vec Rfull = h->orr.with_rhs(nrhs);
+  GMG_TRY(apply_op(h, 0, Xfull, Rfull, s));
+  GMG_TRY(vec_xmy(Bfull, Rfull, s));
   while (!active.empty() && total < maxiter) {
     const int Ra = (int)active.size();
     GMG_CUDA(cudaMemcpyAsync(idx.p, active.data(), sizeof(int) * Ra, cudaMemcpyHostToDevice, s));
-    Vec bA = bb.with_rhs(Ra), xA = xx.with_rhs(Ra);
+    Vec bA = bb.with_rhs(Ra), xA = xx.with_rhs(Ra), rA = h->orA.with_rhs(Ra);
     GMG_TRY(vec_gather(Bfull, idx.as<int>(), bA, s));
     GMG_TRY(vec_gather(Xfull, idx.as<int>(), xA, s));
+    GMG_TRY(vec_gather(Rfull, idx.as<int>(), rA, s));
     Krylov K;
     K.V0 = V0.with_rhs(Ra);
     K.Z0 = Z0.with_rhs(Ra);
     K.w = w.with_rhs(Ra);
-    K.t = t64.with_rhs(Ra);
+    K.t = tv.with_rhs(Ra);
     K.tz = tz.with_rhs(Ra);
     auto pc = [h, s, &tz, zp](const Vec& in, Vec& out, const Vec&) -> gmg_status {
-      // in: FP64 Krylov vector; out: Z direction in the preconditioner precision
+      // in: Krylov vector (FP64, or FP32 in an FP32 Arnoldi cycle); out: Z
+      // direction in the preconditioner precision
       const int Rb = in.R;  // the active columns (fewer than the batch after an in-cycle drop)
       Vec tin = tz.with_rhs(Rb);
       if (zp == GMG_F64) return kcycle(h, 0, in, out, s);
+      const bool graph = h->P.graph && !h->graph_broken && Rb <= 1024;
+      if (!graph && in.prec == zp) return kcycle(h, 0, in, out, s);
+      // the captured cycle reads its input from tz
       GMG_TRY(vec_convert(in, tin, s));
-      if (!h->P.graph || h->graph_broken || Rb > 1024) return kcycle(h, 0, tin, out, s);
+      if (!graph) return kcycle(h, 0, tin, out, s);
       auto it = h->kgraph.find(Rb);
       if (it == h->kgraph.end()) {
         // first cycle of this batch size: host-driven (it also builds every
@@ -1430,15 +1472,16 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
       dc.idx = h->oidx2.as<int>();
     }
     dc.batches = &batches;
+    dc.r0 = &rA;
     GMG_TRY(fgmres(h, 0, bA, xA, K, m, std::min(m, maxiter - total), tol, pc, true, &it, &rr, s, &dc));
     GMG_TRY(vec_scatter(xA, idx.as<int>(), Xfull, s));
     const int before = total;
     total += std::max(it, 1);
-    // true residuals of the batch decide who stays active
-    Vec rA = w.with_rhs(Ra);
+    // true residuals of the batch decide who stays active, and start the next cycle
     GMG_TRY(apply_op(h, 0, xA, rA, s));
     std::vector<zc> rn;
     GMG_TRY(vec_xmy(bA, rA, s));
+    GMG_TRY(vec_scatter(rA, idx.as<int>(), Rfull, s));
     GMG_TRY(dots(h, rA, 1, 0, rA, rn, s));
     std::vector<int> still;
     for (int k = 0; k < Ra; ++k) {

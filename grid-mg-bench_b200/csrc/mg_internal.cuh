@@ -80,14 +80,19 @@ gmg_status vec_dcgs_dots(const Vec& V0, int64_t vstride, int nv, const Vec& B, d
 gmg_status vec_dcgs_update(const double2* coef_dev, Vec& V0, int64_t vstride, int nv, const Vec& B, cudaStream_t s);
 // Z (BF16) = X - Y (FP32), rounded to nearest even
 gmg_status vec_xmy_bf16(const Vec& X, const Vec& Y, Vec& Z, cudaStream_t s);
+// Z (BF16, site-blocked [V][3][R][4] words: the 16-byte quarters of one
+// site's records back to back) = X - Y (FP32 spin-colour fields)
+gmg_status vec_xmy_bf16_blocked(const Vec& X, const Vec& Y, Vec& Z, cudaStream_t s);
 // MR on stored BF16 residuals, for a sweep that keeps every step's residual:
-// rn = bf16(r - a Ar) with a = d1 / d2 (device) per RHS
-gmg_status vec_mr_resid_bf16(const double2* d1, const double2* d2, const Vec& r, const Vec& Ar, Vec& rn, cudaStream_t s);
+// rn = bf16(r - a Ar) with a = d1 / d2 (device) per RHS; `blocked`: the
+// fields are site-blocked
+gmg_status vec_mr_resid_bf16(const double2* d1, const double2* d2, const Vec& r, const Vec& Ar, Vec& rn, cudaStream_t s,
+                             bool blocked = false);
 // x (FP32) += sum_{j < K} a_j r_j with r_j = r0 + j * rstride words and
 // a_j = d[j * dstride + k] / d[j * dstride + R + k].x for RHS k (K <= kMrMaxSteps)
 constexpr int kMrMaxSteps = 16;
 gmg_status vec_mr_xsum_bf16(const double2* d, int dstride, int K, const Vec& r0, int64_t rstride, Vec& x,
-                            cudaStream_t s);
+                            cudaStream_t s, bool blocked = false);
 // G[a][b] = <X(a), X(b)> over the whole lattice (R <= 32 columns), FP64
 gmg_status vec_gram(const Vec& X, double2* G_dev, cudaStream_t s);
 // X(a) <- sum_{b <= a} T[a][b] X(b)   (lower-triangular recombination of the columns)

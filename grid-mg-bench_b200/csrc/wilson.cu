@@ -221,21 +221,70 @@ __device__ __forceinline__ void st12(typename wt<T>::C* __restrict__ p, const ty
   }
 }
 
+// Record (site, r) of a field: [V][nrhs][12] complex numbers, or for BF16
+// fields with VEC 3 the site-blocked layout [V][3][nrhs][4] words, in which
+// the 16-byte quarter g of the records of one site's right-hand sides lie
+// back to back, so that the lanes of a warp that hold consecutive RHS of a
+// site read one contiguous run (three 16-byte loads of a record at a stride
+// of 4 nrhs words).
+template <int VEC, class P>
+__device__ __forceinline__ P* recp(P* base, int64_t site, int r, int nrhs) {
+  return VEC == 3 ? base + site * 12 * nrhs + 4 * r : base + (site * nrhs + r) * 12;
+}
+
 // a record of input type TI read as T: FP32 records promoted exactly to FP64
 // on load (the FP64 operator applied to FP32 vectors), BF16 records (48 bytes,
 // three 16-byte loads) widened to FP32
+// A record as loaded, before widening: BF16 records stay packed (12 words), so
+// that a record prefetched one hop ahead holds 12 registers instead of 24.
+template <class T, class TI> struct RawRec { typedef typename wt<T>::C type; };
+template <class T> struct RawRec<T, bf16s> { typedef uint32_t type; };
+
 template <class T, class TI, int VEC>
-__device__ __forceinline__ void ld12x(typename wt<T>::C v[12], const typename wt<TI>::C* __restrict__ p) {
-  if (std::is_same<TI, bf16s>::value) {
-    const uint4* q = reinterpret_cast<const uint4*>(p);
+__device__ __forceinline__ void ld12x(typename wt<T>::C v[12], const typename wt<TI>::C* __restrict__ base,
+                                      int64_t site, int r, int nrhs);
+
+template <class T, class TI, int VEC>
+__device__ __forceinline__ void ld12raw(typename RawRec<T, TI>::type w[12],
+                                        const typename wt<TI>::C* __restrict__ base, int64_t site, int r, int nrhs) {
+  if constexpr (std::is_same<TI, bf16s>::value) {
+    // VEC 3: 32-bit index arithmetic in 16-byte units (the caller keeps the
+    // field below 2^31 of them)
+    const uint4* q = VEC == 3 ? reinterpret_cast<const uint4*>(base) + ((int)site * 3 * nrhs + r)
+                              : reinterpret_cast<const uint4*>(recp<VEC>(base, site, r, nrhs));
+    const int gs = VEC == 3 ? nrhs : 1;  // uint4 stride of the three quarters
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const uint4 u = __ldg(q + k);
-      const uint32_t w[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        v[4 * k + i] = typename wt<T>::C{(T)__uint_as_float(w[i] << 16), (T)__uint_as_float(w[i] & 0xffff0000u)};
+      const uint4 u = __ldg(q + k * gs);
+      w[4 * k] = u.x;
+      w[4 * k + 1] = u.y;
+      w[4 * k + 2] = u.z;
+      w[4 * k + 3] = u.w;
     }
+  } else {
+    ld12x<T, TI, VEC>(w, base, site, r, nrhs);
+  }
+}
+
+template <class T, class TI>
+__device__ __forceinline__ void unraw12(typename wt<T>::C v[12], const typename RawRec<T, TI>::type w[12]) {
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    if constexpr (std::is_same<TI, bf16s>::value)
+      v[i] = typename wt<T>::C{(T)__uint_as_float(w[i] << 16), (T)__uint_as_float(w[i] & 0xffff0000u)};
+    else
+      v[i] = w[i];
+  }
+}
+
+template <class T, class TI, int VEC>
+__device__ __forceinline__ void ld12x(typename wt<T>::C v[12], const typename wt<TI>::C* __restrict__ base,
+                                      int64_t site, int r, int nrhs) {
+  const typename wt<TI>::C* p = recp<VEC>(base, site, r, nrhs);
+  if constexpr (std::is_same<TI, bf16s>::value) {
+    uint32_t w[12];
+    ld12raw<T, TI, VEC>(w, base, site, r, nrhs);
+    unraw12<T, TI>(v, w);
   } else if (sizeof(TI) == sizeof(T)) {
     ld12<T, VEC>(v, reinterpret_cast<const typename wt<T>::C*>(p));
   } else {
@@ -248,9 +297,12 @@ __device__ __forceinline__ void ld12x(typename wt<T>::C v[12], const typename wt
 
 // a record of T written as TO (BF16: rounded to nearest even, three 16-byte stores)
 template <class T, class TO, int VEC>
-__device__ __forceinline__ void st12x(typename wt<TO>::C* __restrict__ p, const typename wt<T>::C v[12]) {
+__device__ __forceinline__ void st12x(typename wt<TO>::C* __restrict__ base, int64_t site, int r, int nrhs,
+                                      const typename wt<T>::C v[12]) {
+  typename wt<TO>::C* p = recp<VEC>(base, site, r, nrhs);
   if (std::is_same<TO, bf16s>::value) {
     uint4* q = reinterpret_cast<uint4*>(p);
+    const int gs = VEC == 3 ? nrhs : 1;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       uint32_t w[4];
@@ -259,7 +311,7 @@ __device__ __forceinline__ void st12x(typename wt<TO>::C* __restrict__ p, const 
         const __nv_bfloat162 b = __floats2bfloat162_rn((float)v[4 * k + i].x, (float)v[4 * k + i].y);
         w[i] = *reinterpret_cast<const uint32_t*>(&b);
       }
-      q[k] = make_uint4(w[0], w[1], w[2], w[3]);
+      q[k * gs] = make_uint4(w[0], w[1], w[2], w[3]);
     }
   } else {
     st12<T, VEC>(reinterpret_cast<typename wt<T>::C*>(p), v);
@@ -295,9 +347,10 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
     int nbs[8];
 #pragma unroll
     for (int p = 0; p < 8; ++p) nbs[p] = nbr[(int64_t)p * V + site];
-    C psi[12], nxt[12];
-    ld12x<T, TI, VEC>(psi, in + ((int64_t)site * nrhs + r) * 12);
-    ld12x<T, TI, VEC>(nxt, in + ((int64_t)nbs[0] * nrhs + r) * 12);
+    C psi[12];
+    typename RawRec<T, TI>::type nxt[12];
+    ld12x<T, TI, VEC>(psi, in, site, r, nrhs);
+    ld12raw<T, TI, VEC>(nxt, in, nbs[0], r, nrhs);
 #pragma unroll
     for (int k = 6; k < 12; ++k)
       if (g5) psi[k] = C{-psi[k].x, -psi[k].y};
@@ -317,9 +370,8 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
       const int mu = p & 3;
       const int dsp = p < 4 ? 1 : -1;
       C cur[12];
-#pragma unroll
-      for (int k = 0; k < 12; ++k) cur[k] = nxt[k];
-      if (p < 7) ld12x<T, TI, VEC>(nxt, in + ((int64_t)nbs[p < 7 ? p + 1 : 7] * nrhs + r) * 12);
+      unraw12<T, TI>(cur, nxt);
+      if (p < 7) ld12raw<T, TI, VEC>(nxt, in, nbs[p < 7 ? p + 1 : 7], r, nrhs);
       if (skip & (1 << p)) continue;
       T coef = (T)-0.5;
       if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
@@ -333,7 +385,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
   if (op != GMG_OP_MDIR) {
     // diagonal: (4 + m) psi + Cl psi, two chiral 6x6 blocks
     C psi[12];
-    ld12x<T, TI, VEC>(psi, in + ((int64_t)site * nrhs + r) * 12);
+    ld12x<T, TI, VEC>(psi, in, site, r, nrhs);
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
       if (g5 && k >= 6) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
@@ -361,7 +413,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
       T coef = (T)-0.5;
       if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
       C psi[12];
-      ld12x<T, TI, VEC>(psi, in + ((int64_t)nb * nrhs + r) * 12);
+      ld12x<T, TI, VEC>(psi, in, nb, r, nrhs);
       if (g5) {
 #pragma unroll
         for (int k = 6; k < 12; ++k) { psi[k].x = -psi[k].x; psi[k].y = -psi[k].y; }
@@ -375,7 +427,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
   C ov[12];
   // the input record again for the products (re-read rather than kept live
   // through the hops: registers decide the occupancy of this kernel)
-  if (DOTS) ld12x<T, TI, VEC>(cin, in + ((int64_t)site * nrhs + r) * 12);
+  if (DOTS) ld12x<T, TI, VEC>(cin, in, site, r, nrhs);
 #pragma unroll
   for (int s = 0; s < 4; ++s)
 #pragma unroll
@@ -390,7 +442,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
         pn += v.x * v.x + v.y * v.y;
       }
     }
-  st12x<T, TO, VEC>(out + ((int64_t)site * nrhs + r) * 12, ov);
+  st12x<T, TO, VEC>(out, site, r, nrhs, ov);
   if (DOTS) {
     dsum[0] += pr;
     dsum[1] += pi;
@@ -1851,14 +1903,17 @@ gmg_status wilson_apply_f32_in(gmg_wilson* h, int op, int nrhs, const float* in,
 }
 
 // out = M in with the minimal-residual inner products d1[r] = <out, in>,
-// d2[r].x = <out, out> (zeroed here), on BF16 fields [V][nrhs][12] (one 32-bit
-// word per complex number): FP32 arithmetic on the widened records, the
-// products from the FP32 result, the result rounded to BF16.  The tile kernel
-// at 3 CTAs per SM with the records prefetched.
+// d2[r].x = <out, out> (zeroed here), on BF16 fields (one 32-bit word per
+// complex number) [V][nrhs][12], or site-blocked [V][3][nrhs][4] with
+// `blocked`: FP32 arithmetic on the widened records, the products from the
+// FP32 result, the result rounded to BF16.  The tile kernel at 3 CTAs per SM
+// with the records prefetched.
 gmg_status wilson_apply_mr_bf16(gmg_wilson* h, int nrhs, const uint32_t* in, uint32_t* out, double2* d1, double2* d2,
-                                cudaStream_t s) {
+                                cudaStream_t s, bool blocked) {
   GMG_CHECK(((((uintptr_t)in | (uintptr_t)out) & 15) == 0), GMG_ERR_ARGUMENT,
             "wilson apply (BF16): fields must be 16-byte aligned");
+  GMG_CHECK(!blocked || h->dims.vol() * 3 * nrhs < ((int64_t)1 << 31), GMG_ERR_UNSUPPORTED,
+            "wilson apply (BF16, site-blocked): field above 2^31 16-byte units");
   const int V = (int)h->dims.vol();
   const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
   int rt = 1;
@@ -1874,7 +1929,8 @@ gmg_status wilson_apply_mr_bf16(gmg_wilson* h, int nrhs, const uint32_t* in, uin
   KernelTimer kt("wilson", s);
   GMG_CUDA(cudaMemsetAsync(d1, 0, sizeof(double2) * nrhs, s));
   GMG_CUDA(cudaMemsetAsync(d2, 0, sizeof(double2) * nrhs, s));
-  auto k = wilson_tile_kernel<float, true, 3, false, 1, true, bf16s, bf16s>;
+  auto k = blocked ? wilson_tile_kernel<float, true, 3, false, 3, true, bf16s, bf16s>
+                   : wilson_tile_kernel<float, true, 3, false, 1, true, bf16s, bf16s>;
   if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k<<<g, kTileSites * rt, smem, s>>>(h->hop_f.as<float2>(), h->clover_f.as<float2>(), h->nbr.as<int32_t>(), in, out, V,
                                      nrhs, rt, (float)(4.0 + h->mass), GMG_OP_M, 0, 0, h->apbc, tvol, h->dims.d[3], d1,

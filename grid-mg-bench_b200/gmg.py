@@ -492,7 +492,8 @@ class MGParams(ctypes.Structure):
                 ("seed", ctypes.c_uint64), ("setup_solver", ctypes.c_int), ("setup_tol", ctypes.c_double),
                 ("setup_passes", ctypes.c_int), ("setup_null", ctypes.c_int), ("graph", ctypes.c_int),
                 ("refine_iters", ctypes.c_int * 2), ("recursive_updates", ctypes.c_int),
-                ("drop_in_cycle", ctypes.c_int), ("smoother_bf16", ctypes.c_int), ("outer_dcgs", ctypes.c_int)]
+                ("drop_in_cycle", ctypes.c_int), ("smoother_bf16", ctypes.c_int), ("outer_dcgs", ctypes.c_int),
+                ("arnoldi_f32", ctypes.c_int)]
 
 
 class MultiGrid:

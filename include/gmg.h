@@ -418,6 +418,13 @@ typedef struct {
                             reorthogonalisation (the second classical Gram-Schmidt pass of each
                             basis vector merged into the next step): two sweeps over the FP64
                             Krylov basis per step instead of three and a scaling sweep.  0: CGS2. */
+  int arnoldi_f32;       /* 1: the outer FGMRES runs each restart cycle's Arnoldi process in FP32
+                            (basis, operator products, Gram-Schmidt sweeps; inner products and the
+                            Hessenberg least squares in FP64) on the FP64 residual that starts the
+                            cycle; the residual b - A x and the solution stay FP64, so every restart
+                            is an iterative-refinement step and the tolerance is checked on the FP64
+                            true residual.  0: FP64 Arnoldi.  -1 (default): on with an FP32 or BF16
+                            preconditioner (prec F32 / BF16), off with prec F64. */
 } gmg_mg_params;
 
 /* Defaults of MultiGridParams (MultigridParams.h:95-113) adapted to the MR smoother, with the

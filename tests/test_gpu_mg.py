@@ -237,8 +237,10 @@ def test_mg_converged_rhs_leave_within_a_cycle(fine, prec, graph):
     # batch), and every RHS meets the 1e-10 true residual.
     dims, w = fine
     nrhs = 4
+    # (FP64 Arnoldi: an FP32 cycle stops at 1e-6 of its starting residual, so
+    # the RHS started 1e-1 from the solution would need a second cycle)
     kw = dict(nlevels=3, nvec=(6, 6), setup_iters=30, prec=prec, coarsest_iters=30, wrapper_iters=6, graph=graph,
-              block=((2, 2, 2, 2), (2, 2, 2, 2)), outer_restart=24)
+              block=((2, 2, 2, 2), (2, 2, 2, 2)), outer_restart=24, arnoldi_f32=0)
     b = torch.from_numpy(inputs.gaussian_field((4096, nrhs, 12), inputs.rng(stream=311))).cuda()
     mg = gmg.MultiGrid(w, nrhs, drop_in_cycle=0, **kw)
     mg.setup()
@@ -290,3 +292,28 @@ def test_mg_bf16_smoother_reaches_1e10(fine, prec):
         assert true_relres(w, b, x) <= 2e-10, (bf, it, rr)
         its[bf] = it
     assert its[1] <= its[0] + 2, its
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f32", "bf16"])
+def test_mg_fp32_arnoldi_reaches_1e10(fine, prec):
+    # restart cycles whose Arnoldi process runs in FP32 on the FP64 residual
+    # (iterative refinement): the same 1e-10 FP64 true residual, within two
+    # outer iterations of the FP64 Arnoldi process, with and without the
+    # in-cycle drop
+    dims, w = fine
+    nrhs = 4
+    kw = dict(nlevels=3, nvec=(6, 6), setup_iters=30, prec=prec, coarsest_iters=30, wrapper_iters=6,
+              block=((2, 2, 2, 2), (2, 2, 2, 2)), outer_restart=8)
+    b = torch.from_numpy(inputs.gaussian_field((4096, nrhs, 12), inputs.rng(stream=331))).cuda()
+    for drop in (0, 1):
+        its = {}
+        for a in (0, 1):
+            mg = gmg.MultiGrid(w, nrhs, arnoldi_f32=a, drop_in_cycle=drop, **kw)
+            mg.setup()
+            x = torch.zeros_like(b)
+            it, rr = mg.solve(b, x, tol=1e-10, maxiter=300)
+            assert rr <= 1e-10
+            assert true_relres(w, b, x) <= 2e-10, (a, drop, it, rr)
+            its[a] = it
+        assert its[1] <= its[0] + 2, (drop, its)
