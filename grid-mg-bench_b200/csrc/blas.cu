@@ -395,6 +395,31 @@ __global__ void __launch_bounds__(MODE == 1 ? kAxDot1Threads : kAxDotThreads) mu
 constexpr int kDcgsThreads = 384;
 constexpr int kDcgsMaxNV = 9;
 
+// Two consecutive complex numbers of a field (one 16-byte load FP32, two
+// FP64), kept in the storage type until used; e is even and the field 16-byte
+// aligned.
+__device__ __forceinline__ void ld_pair(const float2* p, int64_t e, float2& u, float2& v) {
+  const float4 q = *reinterpret_cast<const float4*>(p + e);
+  u = make_float2(q.x, q.y);
+  v = make_float2(q.z, q.w);
+}
+__device__ __forceinline__ void ld_pair(const double2* p, int64_t e, double2& u, double2& v) {
+  u = p[e];
+  v = p[e + 1];
+}
+template <class C>
+__device__ __forceinline__ double2 wide(C a) { return make_double2(a.x, a.y); }
+__device__ __forceinline__ void st_pair(float2* p, int64_t e, double ur, double ui, double vr, double vi) {
+  *reinterpret_cast<float4*>(p + e) = make_float4((float)ur, (float)ui, (float)vr, (float)vi);
+}
+__device__ __forceinline__ void st_pair(double2* p, int64_t e, double ur, double ui, double vr, double vi) {
+  p[e] = make_double2(ur, ui);
+  p[e + 1] = make_double2(vr, vi);
+}
+
+// A thread takes two consecutive complex numbers of a site's R x dof row (dof
+// even, so both belong to one RHS): twice the bytes in flight per thread for
+// the same product accumulators, which bound the kernels' occupancy.
 template <int NV, class T = double>
 __global__ void __launch_bounds__(kDcgsThreads) dcgs_dots_row_kernel(const typename C2<T>::t* __restrict__ V0,
                                                                      int64_t vstride,
@@ -403,38 +428,39 @@ __global__ void __launch_bounds__(kDcgsThreads) dcgs_dots_row_kernel(const typen
                                                                      double2* __restrict__ out) {
   extern __shared__ double part[];  // [8][NT]
   constexpr int NP = 2 * NV + 3;
-  const int RD = R * dof, t = threadIdx.x, NT = blockDim.x;
-  const int so = t / RD, i = t % RD;
-  const bool act = t < spb * RD;
+  const int RD = R * dof, RH = RD / 2, dh = dof / 2, t = threadIdx.x, NT = blockDim.x;
+  const int so = t / RH, i = t % RH;
+  const bool act = t < spb * RH;
   double pr[NP], pi[NP];
 #pragma unroll
   for (int k = 0; k < NP; ++k) pr[k] = pi[k] = 0.0;
   if (act) {
     for (int64_t st = (int64_t)blockIdx.x * spb + so; st < V; st += (int64_t)gridDim.x * spb) {
-      const int64_t e = st * RD + i;
-      double2 xv[NV + 1];
+      const int64_t e = st * RD + 2 * i;
+      typename C2<T>::t xv[NV + 1][2], bv[2];
 #pragma unroll
-      for (int k = 0; k <= NV; ++k) {
-        const typename C2<T>::t q = V0[k * vstride + e];
-        xv[k] = make_double2(q.x, q.y);
-      }
-      const typename C2<T>::t bq = B[e];
-      const double2 a = xv[NV], b = make_double2(bq.x, bq.y);
+      for (int k = 0; k <= NV; ++k) ld_pair(V0 + k * vstride, e, xv[k][0], xv[k][1]);
+      ld_pair(B, e, bv[0], bv[1]);
 #pragma unroll
-      for (int k = 0; k < NV; ++k) {
-        pr[k] += xv[k].x * a.x + xv[k].y * a.y;
-        pi[k] += xv[k].x * a.y - xv[k].y * a.x;
-        pr[NV + k] += xv[k].x * b.x + xv[k].y * b.y;
-        pi[NV + k] += xv[k].x * b.y - xv[k].y * b.x;
+      for (int h = 0; h < 2; ++h) {
+        const double2 a = wide(xv[NV][h]), b = wide(bv[h]);
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+          const double2 x = wide(xv[k][h]);
+          pr[k] += x.x * a.x + x.y * a.y;
+          pi[k] += x.x * a.y - x.y * a.x;
+          pr[NV + k] += x.x * b.x + x.y * b.y;
+          pi[NV + k] += x.x * b.y - x.y * b.x;
+        }
+        pr[2 * NV] += a.x * a.x + a.y * a.y;
+        pr[2 * NV + 1] += a.x * b.x + a.y * b.y;
+        pi[2 * NV + 1] += a.x * b.y - a.y * b.x;
+        pr[2 * NV + 2] += b.x * b.x + b.y * b.y;
       }
-      pr[2 * NV] += a.x * a.x + a.y * a.y;
-      pr[2 * NV + 1] += a.x * b.x + a.y * b.y;
-      pi[2 * NV + 1] += a.x * b.y - a.y * b.x;
-      pr[2 * NV + 2] += b.x * b.x + b.y * b.y;
     }
   }
   // block reduction, four products at a time: the spb site slots, then the
-  // dof components of each RHS, then one global atomic per (product, RHS)
+  // dof / 2 pairs of each RHS, then one global atomic per (product, RHS)
 #pragma unroll
   for (int k0 = 0; k0 < NP; k0 += 4) {
     const int nk = min(4, NP - k0);
@@ -453,10 +479,10 @@ __global__ void __launch_bounds__(kDcgsThreads) dcgs_dots_row_kernel(const typen
     }
     __syncthreads();
     if (spb > 1) {
-      for (int k = t; k < 2 * nk * RD; k += NT) {
-        const int jc = k / RD, ii = k % RD;
+      for (int k = t; k < 2 * nk * RH; k += NT) {
+        const int jc = k / RH, ii = k % RH;
         double v = part[jc * NT + ii];
-        for (int o = 1; o < spb; ++o) v += part[jc * NT + o * RD + ii];
+        for (int o = 1; o < spb; ++o) v += part[jc * NT + o * RH + ii];
         part[jc * NT + ii] = v;
       }
       __syncthreads();
@@ -464,9 +490,9 @@ __global__ void __launch_bounds__(kDcgsThreads) dcgs_dots_row_kernel(const typen
     for (int k = t; k < nk * R; k += NT) {
       const int q = k / R, rr = k % R;
       double vr = 0.0, vi = 0.0;
-      for (int d = 0; d < dof; ++d) {
-        vr += part[(2 * q) * NT + rr * dof + d];
-        vi += part[(2 * q + 1) * NT + rr * dof + d];
+      for (int d = 0; d < dh; ++d) {
+        vr += part[(2 * q) * NT + rr * dh + d];
+        vi += part[(2 * q + 1) * NT + rr * dh + d];
       }
       atomicAdd(&out[(k0 + q) * R + rr].x, vr);
       atomicAdd(&out[(k0 + q) * R + rr].y, vi);
@@ -477,48 +503,52 @@ __global__ void __launch_bounds__(kDcgsThreads) dcgs_dots_row_kernel(const typen
 // Pass 2 (one sweep): A <- (A - sum_k c_k V_k) / alpha (the finished basis
 // vector, in place), then V_{NV+1} <- (B - sum_k g_k V_k - d A) / beta (the
 // next one after one projection).  cf per RHS: c[NV], g[NV], (1/alpha, 0),
-// d, (1/beta, 0), at cf[k * R + r].
+// d, (1/beta, 0), at cf[k * R + r].  Two complex numbers per thread.
 template <int NV, class T = double>
 __global__ void __launch_bounds__(kDcgsThreads) dcgs_update_row_kernel(const double2* __restrict__ cfg,
                                                                        typename C2<T>::t* __restrict__ V0,
                                                                        int64_t vstride,
                                                                        const typename C2<T>::t* __restrict__ B,
                                                                        int64_t V, int R, int dof, int spb) {
-  typedef typename C2<T>::t CT;
   extern __shared__ double2 cf[];  // [2 NV + 3][R]
   constexpr int NC = 2 * NV + 3;
-  const int RD = R * dof, t = threadIdx.x;
+  const int RD = R * dof, RH = RD / 2, t = threadIdx.x;
   for (int k = t; k < NC * R; k += blockDim.x) cf[k] = cfg[k];
   __syncthreads();
-  if (t >= spb * RD) return;
-  const int so = t / RD, i = t % RD, r = i / dof;
+  if (t >= spb * RH) return;
+  const int so = t / RH, i = t % RH, r = (2 * i) / dof;
+  const double ia = cf[(2 * NV) * R + r].x;
+  const double2 d = cf[(2 * NV + 1) * R + r];
+  const double ib = cf[(2 * NV + 2) * R + r].x;
   for (int64_t st = (int64_t)blockIdx.x * spb + so; st < V; st += (int64_t)gridDim.x * spb) {
-    const int64_t e = st * RD + i;
-    double2 xv[NV + 1];
+    const int64_t e = st * RD + 2 * i;
+    typename C2<T>::t xv[NV + 1][2], bv[2];
 #pragma unroll
-    for (int k = 0; k <= NV; ++k) {
-      const CT q = V0[k * vstride + e];
-      xv[k] = make_double2(q.x, q.y);
-    }
-    const CT b = B[e];
-    double ar = xv[NV].x, ai = xv[NV].y, br = b.x, bi = b.y;
+    for (int k = 0; k <= NV; ++k) ld_pair(V0 + k * vstride, e, xv[k][0], xv[k][1]);
+    ld_pair(B, e, bv[0], bv[1]);
+    double o[2][4];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      const double2 c = cf[k * R + r], g = cf[(NV + k) * R + r];
-      ar -= c.x * xv[k].x - c.y * xv[k].y;
-      ai -= c.x * xv[k].y + c.y * xv[k].x;
-      br -= g.x * xv[k].x - g.y * xv[k].y;
-      bi -= g.x * xv[k].y + g.y * xv[k].x;
+    for (int h = 0; h < 2; ++h) {
+      double ar = xv[NV][h].x, ai = xv[NV][h].y, br = bv[h].x, bi = bv[h].y;
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        const double2 c = cf[k * R + r], g = cf[(NV + k) * R + r], x = wide(xv[k][h]);
+        ar -= c.x * x.x - c.y * x.y;
+        ai -= c.x * x.y + c.y * x.x;
+        br -= g.x * x.x - g.y * x.y;
+        bi -= g.x * x.y + g.y * x.x;
+      }
+      ar *= ia;
+      ai *= ia;
+      br -= d.x * ar - d.y * ai;
+      bi -= d.x * ai + d.y * ar;
+      o[h][0] = ar;
+      o[h][1] = ai;
+      o[h][2] = br * ib;
+      o[h][3] = bi * ib;
     }
-    const double ia = cf[(2 * NV) * R + r].x;
-    const double2 d = cf[(2 * NV + 1) * R + r];
-    const double ib = cf[(2 * NV + 2) * R + r].x;
-    ar *= ia;
-    ai *= ia;
-    br -= d.x * ar - d.y * ai;
-    bi -= d.x * ai + d.y * ar;
-    V0[NV * vstride + e] = CT{(T)ar, (T)ai};
-    V0[(NV + 1) * vstride + e] = CT{(T)(br * ib), (T)(bi * ib)};
+    st_pair(V0 + NV * vstride, e, o[0][0], o[0][1], o[1][0], o[1][1]);
+    st_pair(V0 + (NV + 1) * vstride, e, o[0][2], o[0][3], o[1][2], o[1][3]);
   }
 }
 
@@ -1075,22 +1105,48 @@ gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s) {
 }
 
 bool vec_dcgs_supported(const Vec& Y, int nv) {
-  return (Y.prec == GMG_F64 || Y.prec == GMG_F32) && nv >= 0 && nv <= blas::kDcgsMaxNV &&
-         Y.R * Y.dof <= blas::kDcgsThreads;
+  return (Y.prec == GMG_F64 || Y.prec == GMG_F32) && nv >= 0 && nv <= blas::kDcgsMaxNV && Y.dof % 2 == 0 &&
+         Y.R * Y.dof / 2 <= blas::kDcgsThreads;
 }
+
+namespace {
+// DCGS launch shape: R dof / 2 threads per site and the number of sites per
+// CTA that keeps the most useful threads resident (the kernels hold many
+// registers: their product accumulators or projection coefficients), one
+// wave of CTAs.  smem_per_thread / smem_fixed: the kernel's dynamic shared memory.
+template <class K>
+blas::Row dcgs_geom(K kern, const Vec& B, size_t smem_per_thread, size_t smem_fixed, size_t* smem) {
+  blas::Row g;
+  g.RD = B.R * B.dof / 2;
+  int best = -1;
+  for (int spb = 1; spb * g.RD <= blas::kDcgsThreads; ++spb) {
+    const int threads = (spb * g.RD + 31) / 32 * 32;
+    const size_t sm = smem_per_thread * threads + smem_fixed;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, sm) != cudaSuccess) nb = 1;
+    nb = std::max(nb, 1);
+    if (nb * spb * g.RD > best) {
+      best = nb * spb * g.RD;
+      g.spb = spb;
+      g.threads = threads;
+      g.grid = (int)std::max<int64_t>(1, std::min<int64_t>((B.V + spb - 1) / spb, 148 * (int64_t)nb));
+      *smem = sm;
+    }
+  }
+  return g;
+}
+}  // namespace
 
 gmg_status vec_dcgs_dots(const Vec& V0, int64_t vstride, int nv, const Vec& B, double2* out_dev, cudaStream_t s) {
   GMG_CHECK(vec_dcgs_supported(B, nv), GMG_ERR_UNSUPPORTED, "dcgs: unsupported shape");
   const int R = B.R;
   GMG_CUDA(cudaMemsetAsync(out_dev, 0, sizeof(double2) * (2 * nv + 3) * R, s));
-  const blas::Row g = blas::row_geom(B.V, B.R, B.dof);
-  const size_t sm = sizeof(double) * 8 * g.threads;
-  const int grid = std::min(g.grid, 148 * std::max(1, 2048 / g.threads));
   GMG_CHECK(V0.prec == B.prec, GMG_ERR_UNSUPPORTED, "dcgs: basis and new vector differ in precision");
   auto launch = [&](auto kern, auto* p) -> gmg_status {
     typedef std::remove_pointer_t<decltype(p)> CT;
-    if (sm > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    kern<<<grid, g.threads, sm, s>>>((const CT*)V0.p, vstride, (const CT*)B.p, B.V, B.R, B.dof, g.spb, out_dev);
+    size_t sm = 0;
+    const blas::Row g = dcgs_geom(kern, B, sizeof(double) * 8, 0, &sm);
+    kern<<<g.grid, g.threads, sm, s>>>((const CT*)V0.p, vstride, (const CT*)B.p, B.V, B.R, B.dof, g.spb, out_dev);
     GMG_CUDA(cudaGetLastError());
     return GMG_OK;
   };
@@ -1115,14 +1171,12 @@ gmg_status vec_dcgs_dots(const Vec& V0, int64_t vstride, int nv, const Vec& B, d
 
 gmg_status vec_dcgs_update(const double2* coef_dev, Vec& V0, int64_t vstride, int nv, const Vec& B, cudaStream_t s) {
   GMG_CHECK(vec_dcgs_supported(B, nv), GMG_ERR_UNSUPPORTED, "dcgs: unsupported shape");
-  const blas::Row g = blas::row_geom(B.V, B.R, B.dof);
-  const size_t sm = sizeof(double2) * (2 * nv + 3) * B.R;
-  const int grid = std::min(g.grid, 148 * std::max(1, 2048 / g.threads));
   GMG_CHECK(V0.prec == B.prec, GMG_ERR_UNSUPPORTED, "dcgs: basis and new vector differ in precision");
   auto launch = [&](auto kern, auto* p) -> gmg_status {
     typedef std::remove_pointer_t<decltype(p)> CT;
-    if (sm > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    kern<<<grid, g.threads, sm, s>>>(coef_dev, (CT*)V0.p, vstride, (const CT*)B.p, B.V, B.R, B.dof, g.spb);
+    size_t sm = 0;
+    const blas::Row g = dcgs_geom(kern, B, 0, sizeof(double2) * (2 * nv + 3) * B.R, &sm);
+    kern<<<g.grid, g.threads, sm, s>>>(coef_dev, (CT*)V0.p, vstride, (const CT*)B.p, B.V, B.R, B.dof, g.spb);
     GMG_CUDA(cudaGetLastError());
     return GMG_OK;
   };

@@ -285,7 +285,6 @@ gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStre
   Vec r = L.mr_r.with_rhs(R), Ar = L.mr_Ar.with_rhs(R);
   double2* d1 = h->dscr.as<double2>() + kScalars / 2;  // above the Krylov scalars
   double2* d2 = d1 + R;
-  GMG_TRY(apply_op(h, l, x, r, s));
   if (l == 0 && L.bf16_smoother && x.prec == GMG_F32) {
     // the residual and the operator product kept in BF16 (FP32 arithmetic,
     // FP32 solution): the smoother's sweeps move half the bytes
@@ -296,7 +295,14 @@ gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStre
       // moves r, Ar and the next r, and x is read and written once.  The
       // residual fields are site-blocked (the quarters of one site's records
       // back to back), so the operator's record gathers read contiguous runs.
-      GMG_TRY(vec_xmy_bf16_blocked(b, r, r16, s));  // r = b - A x
+      if ((((uintptr_t)b.p | (uintptr_t)x.p) & 31) == 0) {
+        // r = b - A x, formed by the operator's epilogue
+        GMG_TRY(wilson_residual_bf16(L.w, R, static_cast<const float*>(b.p), static_cast<const float*>(x.p),
+                                     static_cast<uint32_t*>(r16.p), s));
+      } else {
+        GMG_TRY(apply_op(h, l, x, r, s));
+        GMG_TRY(vec_xmy_bf16_blocked(b, r, r16, s));  // r = b - A x
+      }
       const int64_t fs = r16.elems();
       for (int it = 0; it < iters; ++it) {
         Vec rj = r16;
@@ -312,6 +318,7 @@ gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStre
       }
       return vec_mr_xsum_bf16(d1, 2 * R, iters, r16, fs, x, s, true);
     }
+    GMG_TRY(apply_op(h, l, x, r, s));
     GMG_TRY(vec_xmy_bf16(b, r, r16, s));  // r = b - A x
     for (int it = 0; it < iters; ++it) {
       GMG_TRY(wilson_apply_mr_bf16(L.w, R, static_cast<const uint32_t*>(r16.p), static_cast<uint32_t*>(Ar16.p), d1,
@@ -320,6 +327,7 @@ gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStre
     }
     return GMG_OK;
   }
+  GMG_TRY(apply_op(h, l, x, r, s));
   GMG_TRY(vec_xmy(b, r, s));  // r = b - A x
   for (int it = 0; it < iters; ++it) {
     if (l == 0) {
@@ -1422,11 +1430,19 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
   GMG_TRY(vec_xmy(Bfull, Rfull, s));
   while (!active.empty() && total < maxiter) {
     const int Ra = (int)active.size();
-    GMG_CUDA(cudaMemcpyAsync(idx.p, active.data(), sizeof(int) * Ra, cudaMemcpyHostToDevice, s));
-    Vec bA = bb.with_rhs(Ra), xA = xx.with_rhs(Ra), rA = h->orA.with_rhs(Ra);
-    GMG_TRY(vec_gather(Bfull, idx.as<int>(), bA, s));
-    GMG_TRY(vec_gather(Xfull, idx.as<int>(), xA, s));
-    GMG_TRY(vec_gather(Rfull, idx.as<int>(), rA, s));
+    // every RHS still active (the active list is ascending): the batch is the
+    // caller's fields themselves, with no gather or scatter
+    const bool whole = Ra == nrhs;
+    Vec bA = Bfull, xA = Xfull, rA = Rfull;
+    if (!whole) {
+      GMG_CUDA(cudaMemcpyAsync(idx.p, active.data(), sizeof(int) * Ra, cudaMemcpyHostToDevice, s));
+      bA = bb.with_rhs(Ra);
+      xA = xx.with_rhs(Ra);
+      rA = h->orA.with_rhs(Ra);
+      GMG_TRY(vec_gather(Bfull, idx.as<int>(), bA, s));
+      GMG_TRY(vec_gather(Xfull, idx.as<int>(), xA, s));
+      GMG_TRY(vec_gather(Rfull, idx.as<int>(), rA, s));
+    }
     Krylov K;
     K.V0 = V0.with_rhs(Ra);
     K.Z0 = Z0.with_rhs(Ra);
@@ -1474,14 +1490,14 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
     dc.batches = &batches;
     dc.r0 = &rA;
     GMG_TRY(fgmres(h, 0, bA, xA, K, m, std::min(m, maxiter - total), tol, pc, true, &it, &rr, s, &dc));
-    GMG_TRY(vec_scatter(xA, idx.as<int>(), Xfull, s));
+    if (!whole) GMG_TRY(vec_scatter(xA, idx.as<int>(), Xfull, s));
     const int before = total;
     total += std::max(it, 1);
     // true residuals of the batch decide who stays active, and start the next cycle
     GMG_TRY(apply_op(h, 0, xA, rA, s));
     std::vector<zc> rn;
     GMG_TRY(vec_xmy(bA, rA, s));
-    GMG_TRY(vec_scatter(rA, idx.as<int>(), Rfull, s));
+    if (!whole) GMG_TRY(vec_scatter(rA, idx.as<int>(), Rfull, s));
     GMG_TRY(dots(h, rA, 1, 0, rA, rn, s));
     std::vector<int> still;
     for (int k = 0; k < Ra; ++k) {
@@ -1503,6 +1519,36 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
   h->last_relres = relres;
   h->last_batches = batches;
   if (mx > tol) return fail(GMG_ERR_NOT_CONVERGED, "gmg_mg_solve: not converged within maxiter");
+  return GMG_OK;
+}
+
+// MultiGridPreconditioner::operator() (include/MultigridPreconditioner.h:253):
+// one K-cycle on device FP64 fields [V][nrhs][12], run host-driven in the
+// preconditioner precision (in converted on entry, out on exit).
+extern "C" gmg_status gmg_mg_apply(gmg_mg* h, int nrhs, const double* in, double* out, gmg_stream stream) {
+  GMG_CHECK(h && in && out, GMG_ERR_ARGUMENT, "gmg_mg_apply: null argument");
+  GMG_CHECK(in != out, GMG_ERR_ARGUMENT, "gmg_mg_apply: in and out must not alias");
+  GMG_CHECK(h->setup_done, GMG_ERR_STATE, "gmg_mg_apply: call gmg_mg_setup first");
+  GMG_CHECK(nrhs >= 1 && nrhs <= h->Rmax, GMG_ERR_ARGUMENT, "gmg_mg_apply: nrhs exceeds max_rhs");
+  cudaStream_t s = S(stream);
+  MGLevel& F = *h->L[0];
+  GMG_TRY(outer_workspace(h));
+  Vec In, Out;
+  In.p = const_cast<double*>(in);
+  In.V = F.V;
+  In.R = nrhs;
+  In.dof = 12;
+  Out = In;
+  Out.p = out;
+  if (F.vprec == GMG_F64) {
+    GMG_TRY(kcycle(h, 0, In, Out, s));
+  } else {
+    Vec tin = h->otz.with_rhs(nrhs), z = nth(h->oZ0, 0).with_rhs(nrhs);
+    GMG_TRY(vec_convert(In, tin, s));
+    GMG_TRY(kcycle(h, 0, tin, z, s));
+    GMG_TRY(vec_convert(z, Out, s));
+  }
+  GMG_CUDA(cudaStreamSynchronize(s));
   return GMG_OK;
 }
 

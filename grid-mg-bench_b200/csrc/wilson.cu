@@ -323,13 +323,16 @@ __device__ __forceinline__ void st12x(typename wt<TO>::C* __restrict__ base, int
 // bit p set are left out (0 for the plain operator); with the bits of the
 // hops to blocks of the other parity this gives e D e + o D o of the
 // coarsening's self term in one pass.
+// VOUT: the output record layout (VEC by default); SUB: write bsub - M in
+// (bsub laid out and typed as the input) instead of M in.
 template <class T, class LinkFn, bool DOTS = false, int VEC = 0, bool LDAG = false, bool PF = false, class TI = T,
-          class TO = T>
+          class TO = T, int VOUT = VEC, bool SUB = false>
 __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict__ cl, LinkFn links,
                                             const int32_t* __restrict__ nbr, const typename wt<TI>::C* __restrict__ in,
                                             typename wt<TO>::C* __restrict__ out, int V, int nrhs, int site, int r,
                                             T diag, int op, int dir, int disp, int apbc, int tvol, int Lt,
-                                            double* dsum = nullptr, int skip = 0) {
+                                            double* dsum = nullptr, int skip = 0,
+                                            const typename wt<TI>::C* __restrict__ bsub = nullptr) {
   typedef typename wt<T>::C C;
   const bool g5 = (op == GMG_OP_MDAG);
   const int tc = site / tvol;
@@ -428,12 +431,17 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
   // the input record again for the products (re-read rather than kept live
   // through the hops: registers decide the occupancy of this kernel)
   if (DOTS) ld12x<T, TI, VEC>(cin, in, site, r, nrhs);
+  if (SUB) ld12x<T, TI, VEC>(ov, bsub, site, r, nrhs);
 #pragma unroll
   for (int s = 0; s < 4; ++s)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       C v = acc[s][c];
       if (g5 && s >= 2) { v.x = -v.x; v.y = -v.y; }
+      if (SUB) {
+        v.x = ov[s * 3 + c].x - v.x;
+        v.y = ov[s * 3 + c].y - v.y;
+      }
       ov[s * 3 + c] = v;
       if (DOTS) {
         const T ix = cin[s * 3 + c].x, iy = cin[s * 3 + c].y;
@@ -442,7 +450,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
         pn += v.x * v.x + v.y * v.y;
       }
     }
-  st12x<T, TO, VEC>(out, site, r, nrhs, ov);
+  st12x<T, TO, VOUT>(out, site, r, nrhs, ov);
   if (DOTS) {
     dsum[0] += pr;
     dsum[1] += pi;
@@ -487,13 +495,16 @@ constexpr int kTileSites = 16;
 // 2.73-2.79 ms at 32^4 x 24 RHS FP32 for z blocks of 1 to 32 planes.)
 // TI: the input vectors' precision (float with T = double: the FP64 operator
 // on FP32 vectors, promoted on load).
-template <class T, bool DOTS, int MINB, bool SEL = false, int VEC = 1, bool PF = false, class TI = T, class TO = T>
+// VOUT, SUB: the output layout and bsub - M in (see wilson_site).
+template <class T, bool DOTS, int MINB, bool SEL = false, int VEC = 1, bool PF = false, class TI = T, class TO = T,
+          int VOUT = VEC, bool SUB = false>
 __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
     const typename wt<T>::C* __restrict__ hop, const typename wt<T>::C* __restrict__ clover,
     const int32_t* __restrict__ nbr, const typename wt<TI>::C* __restrict__ in,
     typename wt<TO>::C* __restrict__ out, int V, int nrhs, int rt, T diag, int op, int dir, int disp,
     int apbc, int tvol, int Lt, double2* __restrict__ d1, double2* __restrict__ d2,
-    const int32_t* __restrict__ sel = nullptr, int nsel = 0, const uint8_t* __restrict__ hskip = nullptr) {
+    const int32_t* __restrict__ sel = nullptr, int nsel = 0, const uint8_t* __restrict__ hskip = nullptr,
+    const typename wt<TI>::C* __restrict__ bsub = nullptr) {
   typedef typename wt<T>::C C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* Ls = reinterpret_cast<C*>(smem_raw);  // [kTileSites][8][9]: p < 4 U_mu(x), p >= 4 U_mu(x - mu)^dagger
@@ -533,8 +544,8 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
       int k = 0;
       for (int r = rl; r < nrhs; r += rt, ++k) {
         double dt[3] = {0.0, 0.0, 0.0};
-        wilson_site<T, decltype(links), DOTS, VEC, true, PF, TI, TO>(Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op,
-                                                    dir, disp, apbc, tvol, Lt, dt, skip);
+        wilson_site<T, decltype(links), DOTS, VEC, true, PF, TI, TO, VOUT, SUB>(
+            Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op, dir, disp, apbc, tvol, Lt, dt, skip, bsub);
         if (DOTS) {
           if (two) {
 #pragma unroll
@@ -1521,7 +1532,7 @@ static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_
     kern<<<g, kTileSites * rt, smem, s>>>(reinterpret_cast<const C*>(hp), reinterpret_cast<const C*>(cp),
                                           h->nbr.as<int32_t>(), reinterpret_cast<const C*>(in),
                                           reinterpret_cast<C*>(out), V, nrhs, rt, diag, op, dir, disp, h->apbc, tvol,
-                                          h->dims.d[3], d1, d2, nullptr, 0, nullptr);
+                                          h->dims.d[3], d1, d2, nullptr, 0, nullptr, nullptr);
     return GMG_OK;
   };
   if (vec_prec == GMG_F64) {
@@ -1798,7 +1809,7 @@ static gmg_status launch_tile_sel(gmg_wilson* h, int op, int dir, int disp, int 
   if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k<<<g, kTileSites * rt, smem, s>>>(h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(),
                                      (const double2*)in, (double2*)out, V, nrhs, rt, 4.0 + h->mass, op, dir, disp,
-                                     h->apbc, tvol, h->dims.d[3], nullptr, nullptr, sel, nsel, hskip);
+                                     h->apbc, tvol, h->dims.d[3], nullptr, nullptr, sel, nsel, hskip, nullptr);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
@@ -1893,7 +1904,7 @@ gmg_status wilson_apply_f32_in(gmg_wilson* h, int op, int nrhs, const float* in,
     kern<<<g, kTileSites * rt, smem, s>>>(h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(),
                                           reinterpret_cast<const float2*>(in), reinterpret_cast<double2*>(out), V,
                                           nrhs, rt, 4.0 + h->mass, op, 0, 0, h->apbc, tvol, h->dims.d[3], nullptr,
-                                          nullptr, nullptr, 0, nullptr);
+                                          nullptr, nullptr, 0, nullptr, nullptr);
     GMG_CUDA(cudaGetLastError());
     return GMG_OK;
   };
@@ -1934,7 +1945,39 @@ gmg_status wilson_apply_mr_bf16(gmg_wilson* h, int nrhs, const uint32_t* in, uin
   if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k<<<g, kTileSites * rt, smem, s>>>(h->hop_f.as<float2>(), h->clover_f.as<float2>(), h->nbr.as<int32_t>(), in, out, V,
                                      nrhs, rt, (float)(4.0 + h->mass), GMG_OP_M, 0, 0, h->apbc, tvol, h->dims.d[3], d1,
-                                     d2, nullptr, 0, nullptr);
+                                     d2, nullptr, 0, nullptr, nullptr);
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
+// out = bf16(b - M x) in the site-blocked BF16 layout [V][3][nrhs][4] words,
+// x and b FP32 [V][nrhs][12] (32-byte aligned): the first residual of the
+// BF16 smoother in one pass.  The tile kernel at 3 CTAs per SM with the
+// records prefetched.
+gmg_status wilson_residual_bf16(gmg_wilson* h, int nrhs, const float* b, const float* x, uint32_t* out,
+                                cudaStream_t s) {
+  GMG_CHECK((((uintptr_t)b | (uintptr_t)x) & 31) == 0 && ((uintptr_t)out & 15) == 0, GMG_ERR_ARGUMENT,
+            "wilson residual (BF16): FP32 fields must be 32-byte aligned");
+  GMG_CHECK(h->dims.vol() * 3 * nrhs < ((int64_t)1 << 31), GMG_ERR_UNSUPPORTED,
+            "wilson residual (BF16): field above 2^31 16-byte units");
+  const int V = (int)h->dims.vol();
+  const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
+  int rt = 1;
+  for (int c = std::min(nrhs, 16); c >= 1; --c)
+    if (nrhs % c == 0) {
+      rt = c;
+      break;
+    }
+  if (nrhs > 16 && rt < 8) rt = 16;
+  const int tiles = (V + kTileSites - 1) / kTileSites;
+  const int g = std::min(tiles, 148 * 16);
+  const size_t smem = sizeof(float2) * 2 * kTileSites * 72;
+  KernelTimer kt("wilson", s);
+  auto k = wilson_tile_kernel<float, false, 3, false, 2, true, float, bf16s, 3, true>;
+  k<<<g, kTileSites * rt, smem, s>>>(h->hop_f.as<float2>(), h->clover_f.as<float2>(), h->nbr.as<int32_t>(),
+                                     reinterpret_cast<const float2*>(x), out, V, nrhs, rt, (float)(4.0 + h->mass),
+                                     GMG_OP_M, 0, 0, h->apbc, tvol, h->dims.d[3], nullptr, nullptr, nullptr, 0,
+                                     nullptr, reinterpret_cast<const float2*>(b));
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }

@@ -548,6 +548,13 @@ class MultiGrid:
                                 ctypes.byref(it), ctypes.byref(rr), _stream()))
         return it.value, rr.value
 
+    def apply(self, inp, out):
+        """One K-cycle, out = M^-1 inp (MultiGridPreconditioner::operator()); complex128 CUDA
+        tensors [V, nrhs, 12]."""
+        _check_vec(inp, self.fine.V, 12, "inp")
+        _check_vec(out, self.fine.V, 12, "out")
+        _chk(lib().gmg_mg_apply(self._h, inp.shape[1], _ptr(inp), _ptr(out), _stream()))
+
     def solve_stats(self, nrhs):
         """Per-RHS (outer iteration at which its residual estimate met the tolerance, final true
         relative residual) of the last solve."""

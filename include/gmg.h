@@ -448,6 +448,12 @@ gmg_status gmg_mg_setup(gmg_mg* h, gmg_stream s);
    of a batch go through the K-cycle together (up to max_rhs at a time).
    Synchronises; operator and aggregation handles keep their addresses. */
 gmg_status gmg_mg_refine(gmg_mg* h, gmg_stream s);
+/* The preconditioner itself (MultiGridPreconditioner::operator(),
+   MultigridPreconditioner.h:253): out = one K-cycle applied to in (restrict,
+   coarse K-cycle solve, prolong, MR post-smoothing), computed in the
+   preconditioner precision.  in, out: device FP64 [V][nrhs][12], not aliased.
+   Synchronises. */
+gmg_status gmg_mg_apply(gmg_mg* h, int nrhs, const double* in, double* out, gmg_stream s);
 /* Solve D x = b for nrhs right-hand sides with FP64 FGMRES + MG preconditioner to
    per-RHS relative residual |b - D x| / |b| <= tol.  b, x: device FP64
    [V][nrhs][12]; x holds the initial guess.  Converged RHS drop out at the

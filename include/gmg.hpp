@@ -276,6 +276,10 @@ class MultiGridPreconditioner {
 
   void initialSetup() { check(gmg_mg_setup(h_, stream_)); }
   void refinementSetup() { check(gmg_mg_refine(h_, stream_)); }
+  // one K-cycle: out = M^-1 in (F64 fields)
+  void operator()(const Field& in, Field& out) {
+    check(gmg_mg_apply(h_, in.nrhs, static_cast<const double*>(in.data), static_cast<double*>(out.data), stream_));
+  }
   int Solve(const Field& b, Field& x, double tol, int maxiter, double* max_relres = nullptr) {
     int it = 0;
     double rr = 0;

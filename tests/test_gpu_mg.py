@@ -295,6 +295,34 @@ def test_mg_bf16_smoother_reaches_1e10(fine, prec):
 
 
 @pytest.mark.gpu
+def test_mg_apply_bf16_smoother_matches_fp32_smoother(fine):
+    # one K-cycle (MultiGridPreconditioner::operator()) with the BF16 smoother
+    # (site-blocked BF16 residual fields, the operator's fused first residual,
+    # one solution update per sweep) against the same cycle with the FP32
+    # smoother: equal up to BF16 rounding of the smoother's residuals, and a
+    # real preconditioner (|D M^-1 b - b| well below |b|)
+    dims, w = fine
+    nrhs = 5  # not a multiple of the tile's threads per site
+    kw = dict(nlevels=3, nvec=(6, 6), setup_iters=30, prec="bf16", coarsest_iters=30, wrapper_iters=6,
+              block=((2, 2, 2, 2), (2, 2, 2, 2)), graph=0)
+    b = torch.from_numpy(inputs.gaussian_field((4096, nrhs, 12), inputs.rng(stream=341))).cuda()
+    outs = {}
+    for bf in (0, 1):
+        mg = gmg.MultiGrid(w, nrhs, smoother_bf16=bf, **kw)
+        mg.setup()
+        out = torch.zeros_like(b)
+        mg.apply(b, out)
+        outs[bf] = out
+    rel = (torch.linalg.vector_norm(outs[1] - outs[0], dim=(0, 2)) /
+           torch.linalg.vector_norm(outs[0], dim=(0, 2))).max().item()
+    assert rel < 2e-2, rel
+    Db = torch.zeros_like(b)
+    w.M(outs[1], Db)
+    red = (torch.linalg.vector_norm(Db - b, dim=(0, 2)) / torch.linalg.vector_norm(b, dim=(0, 2))).max().item()
+    assert red < 0.5, red
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("prec", ["f32", "bf16"])
 def test_mg_fp32_arnoldi_reaches_1e10(fine, prec):
     # restart cycles whose Arnoldi process runs in FP32 on the FP64 residual
