@@ -409,6 +409,11 @@ __device__ __forceinline__ void ld_pair(const double2* p, int64_t e, double2& u,
 }
 template <class C>
 __device__ __forceinline__ double2 wide(C a) { return make_double2(a.x, a.y); }
+// an empty statement that reads and (as far as the compiler knows) rewrites
+// v: applied to a batch of loaded values in turn, after the batch's loads, it
+// keeps every use of the batch after every load of the batch has been issued
+__device__ __forceinline__ void issued(float2& v) { asm volatile("" : "+f"(v.x), "+f"(v.y)); }
+__device__ __forceinline__ void issued(double2& v) { asm volatile("" : "+d"(v.x), "+d"(v.y)); }
 __device__ __forceinline__ void st_pair(float2* p, int64_t e, double ur, double ui, double vr, double vi) {
   *reinterpret_cast<float4*>(p + e) = make_float4((float)ur, (float)ui, (float)vr, (float)vi);
 }
@@ -435,12 +440,20 @@ __global__ void __launch_bounds__(kDcgsThreads) dcgs_dots_row_kernel(const typen
 #pragma unroll
   for (int k = 0; k < NP; ++k) pr[k] = pi[k] = 0.0;
   if (act) {
+#pragma unroll 1
     for (int64_t st = (int64_t)blockIdx.x * spb + so; st < V; st += (int64_t)gridDim.x * spb) {
       const int64_t e = st * RD + 2 * i;
       typename C2<T>::t xv[NV + 1][2], bv[2];
 #pragma unroll
       for (int k = 0; k <= NV; ++k) ld_pair(V0 + k * vstride, e, xv[k][0], xv[k][1]);
       ld_pair(B, e, bv[0], bv[1]);
+#pragma unroll
+      for (int k = 0; k <= NV; ++k) {
+        issued(xv[k][0]);
+        issued(xv[k][1]);
+      }
+      issued(bv[0]);
+      issued(bv[1]);
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const double2 a = wide(xv[NV][h]), b = wide(bv[h]);
@@ -526,6 +539,13 @@ __global__ void __launch_bounds__(kDcgsThreads) dcgs_update_row_kernel(const dou
 #pragma unroll
     for (int k = 0; k <= NV; ++k) ld_pair(V0 + k * vstride, e, xv[k][0], xv[k][1]);
     ld_pair(B, e, bv[0], bv[1]);
+#pragma unroll
+    for (int k = 0; k <= NV; ++k) {
+      issued(xv[k][0]);
+      issued(xv[k][1]);
+    }
+    issued(bv[0]);
+    issued(bv[1]);
     double o[2][4];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
