@@ -521,10 +521,12 @@ def main():
             "workload": "3-level K-cycle MG-preconditioned FGMRES, 32^4 Wilson-clover m=-0.35 csw 1, "
                         "nbasis 24 / 32 on 4^4 / 2^4 blocks, 8 MR smoother iterations per level, "
                         "24 RHS to 1e-10",
-            "forms": {"mixed_bf16_mrhs": "outer FGMRES in FP64 (residual, Arnoldi, Gram-Schmidt); K-cycle "
-                                         "with FP32 vectors, tensor-core BF16 coarse stencils and the fine MR "
-                                         "smoother's residual fields in BF16 (FP32 arithmetic); 24 RHS in one "
-                                         "batch, converged RHS leave at their Arnoldi step",
+            "forms": {"mixed_bf16_mrhs": "outer FGMRES(8): every restart cycle starts from the FP64 residual "
+                                         "b - A x and runs its Arnoldi process in FP32 (FP64 inner products, "
+                                         "Hessenberg least squares and solution; tolerance checked on the FP64 "
+                                         "residual); K-cycle with FP32 vectors, tensor-core BF16 coarse stencils "
+                                         "and the fine MR smoother's residual fields in BF16 (FP32 arithmetic); "
+                                         "24 RHS in one batch, converged RHS leave at their Arnoldi step",
                       "plain_f64_single_rhs": "the same algorithm with FP64 everywhere, one RHS per solve"},
             "unit": "s", "higher_is_better": False,
             "mixed_bf16_mrhs_graph_s": mg["mixed_bf16_mrhs_graph"]["solve_s_for_all_rhs"],
