@@ -598,12 +598,12 @@ __global__ void __launch_bounds__(1024) mr_update_row_kernel(const double2* __re
                                                              typename C2<T>::t* __restrict__ x,
                                                              typename C2<T>::t* __restrict__ rr_,
                                                              const typename C2<T>::t* __restrict__ Ar, int64_t V, int R,
-                                                             int dof, int spb, bool update_r) {
+                                                             int dof, int spb, bool update_r, double csg) {
   const int RD = R * dof, t = threadIdx.x;
   if (t >= spb * RD) return;
   const int so = t / RD, i = t % RD, k = i / dof;
   const double den = d2[k].x;
-  const double ar = den > 0.0 ? d1[k].x / den : 0.0, ai = den > 0.0 ? d1[k].y / den : 0.0;
+  const double ar = den > 0.0 ? d1[k].x / den : 0.0, ai = den > 0.0 ? csg * d1[k].y / den : 0.0;
   for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
     const int64_t e = s * RD + i;
     const double rr = rr_[e].x, ri = rr_[e].y;
@@ -928,19 +928,20 @@ __global__ void scale_inv_norm_kernel(const double2* __restrict__ n, const typen
   }
 }
 
-// minimal-residual step with per-RHS alpha = <Ar, r> / <Ar, Ar> read from the device:
-// x += alpha r, r -= alpha Ar
+// minimal-residual step with per-RHS alpha = <Ar, r> / <Ar, Ar> read from the device
+// (csg = -1: d1 holds the conjugate <r, Ar>): x += alpha r, r -= alpha Ar
 template <class T>
 __global__ void mr_update_kernel(const double2* __restrict__ d1, const double2* __restrict__ d2,
                                  typename C2<T>::t* __restrict__ x, typename C2<T>::t* __restrict__ r,
-                                 const typename C2<T>::t* __restrict__ Ar, int64_t V, int R, int dof, bool update_r) {
+                                 const typename C2<T>::t* __restrict__ Ar, int64_t V, int R, int dof, bool update_r,
+                                 double csg) {
   const int64_t tot = V * R * dof;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (RhsWalk w(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride, R, dof); w.e < tot; w.next(stride)) {
     const int64_t e = w.e;
     const int k = w.r();
     const double den = d2[k].x;
-    const double ar = den > 0.0 ? d1[k].x / den : 0.0, ai = den > 0.0 ? d1[k].y / den : 0.0;
+    const double ar = den > 0.0 ? d1[k].x / den : 0.0, ai = den > 0.0 ? csg * d1[k].y / den : 0.0;
     const double rr = r[e].x, ri = r[e].y;
     x[e].x = (T)(x[e].x + ar * rr - ai * ri);
     x[e].y = (T)(x[e].y + ar * ri + ai * rr);
@@ -1038,9 +1039,10 @@ gmg_status vec_multiaxpy_dot(const double2* a_dev, const Vec& X0, int nx, int64_
 }
 
 gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s,
-                         bool update_r) {
+                         bool update_r, bool conj_d1) {
+  const double csg = conj_d1 ? -1.0 : 1.0;
   if (r.prec == GMG_BF16) {
-    GMG_CHECK(x.prec == GMG_F32 && Ar.prec == GMG_BF16 && x.R * x.dof <= 1024, GMG_ERR_UNSUPPORTED,
+    GMG_CHECK(x.prec == GMG_F32 && Ar.prec == GMG_BF16 && x.R * x.dof <= 1024 && !conj_d1, GMG_ERR_UNSUPPORTED,
               "mr update: BF16 residuals need an FP32 solution and at most 1024 values per site");
     const blas::Row rg = blas::row_geom(x.V, x.R, x.dof);
     blas::mr_update_bf16_row_kernel<<<rg.grid, rg.threads, 0, s>>>(d1, d2, (float2*)x.p, (uint32_t*)r.p,
@@ -1053,20 +1055,20 @@ gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, c
     const blas::Row rg = blas::row_geom(x.V, x.R, x.dof);
     if (x.prec == GMG_F64)
       blas::mr_update_row_kernel<double><<<rg.grid, rg.threads, 0, s>>>(d1, d2, (double2*)x.p, (double2*)r.p,
-                                                                         (const double2*)Ar.p, x.V, x.R, x.dof, rg.spb, update_r);
+                                                                         (const double2*)Ar.p, x.V, x.R, x.dof, rg.spb, update_r, csg);
     else
       blas::mr_update_row_kernel<float><<<rg.grid, rg.threads, 0, s>>>(d1, d2, (float2*)x.p, (float2*)r.p,
-                                                                        (const float2*)Ar.p, x.V, x.R, x.dof, rg.spb, update_r);
+                                                                        (const float2*)Ar.p, x.V, x.R, x.dof, rg.spb, update_r, csg);
     GMG_CUDA(cudaGetLastError());
     return GMG_OK;
   }
   const int g = blas::grid1(x.elems());
   if (x.prec == GMG_F64)
     blas::mr_update_kernel<double><<<g, 256, 0, s>>>(d1, d2, (double2*)x.p, (double2*)r.p, (const double2*)Ar.p, x.V,
-                                                     x.R, x.dof, update_r);
+                                                     x.R, x.dof, update_r, csg);
   else
     blas::mr_update_kernel<float><<<g, 256, 0, s>>>(d1, d2, (float2*)x.p, (float2*)r.p, (const float2*)Ar.p, x.V, x.R,
-                                                    x.dof, update_r);
+                                                    x.dof, update_r, csg);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }

@@ -42,7 +42,7 @@ struct MGLevel {
   gmg_agg* agg = nullptr;   // aggregation to level l+1 (owned)
   int m = 0;                // Krylov restart of the solver that runs on this level
   VecBuf V0, Z0, kw, kt;    // Krylov basis (m+1), flexible directions (m), temporaries
-  VecBuf mr_r, mr_Ar, mr_t; // MR smoother
+  VecBuf mr_r;              // MR smoother: the residual r and A r, two fields of one buffer
   VecBuf mr_r16, mr_Ar16;    // the fine smoother's residual fields in BF16 (params.smoother_bf16)
   int mr_keep = 1;           // residual fields in mr_r16: every step's (smoother_iters) or one
   VecBuf bc, xc;            // right-hand side / solution of this level inside the cycle above
@@ -282,7 +282,8 @@ gmg_status bicgstab(gmg_mg* h, int l, const Vec& b, Vec& x, int maxit, double to
 gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStream_t s) {
   MGLevel& L = *h->L[l];
   const int R = b.R;
-  Vec r = L.mr_r.with_rhs(R), Ar = L.mr_Ar.with_rhs(R);
+  Vec r = L.mr_r.with_rhs(R), Ar = r;
+  Ar.p = static_cast<char*>(r.p) + r.bytes();
   double2* d1 = h->dscr.as<double2>() + kScalars / 2;  // above the Krylov scalars
   double2* d2 = d1 + R;
   if (l == 0 && L.bf16_smoother && x.prec == GMG_F32) {
@@ -333,13 +334,14 @@ gmg_status mr_smooth(gmg_mg* h, int l, const Vec& b, Vec& x, int iters, cudaStre
     if (l == 0) {
       // the fine operator forms both inner products in its epilogue
       GMG_TRY(wilson_apply_mr(L.w, r.prec, R, r.p, Ar.p, d1, d2, s));
+      // the residual of the last step is never read
+      GMG_TRY(vec_mr_update(d1, d2, x, r, Ar, s, it + 1 < iters));
     } else {
       GMG_TRY(apply_op(h, l, r, Ar, s));
-      GMG_TRY(vec_multidot(Ar, 1, 0, r, d1, nullptr, s));
-      GMG_TRY(vec_multidot(Ar, 1, 0, Ar, d2, nullptr, s));
+      // one sweep for both products: d1 = <r, Ar> (the conjugate of <Ar, r>), d2 = <Ar, Ar>
+      GMG_TRY(vec_multidot(r, 2, r.elems(), Ar, d1, nullptr, s));
+      GMG_TRY(vec_mr_update(d1, d2, x, r, Ar, s, it + 1 < iters, true));
     }
-    // the residual of the last step is never read
-    GMG_TRY(vec_mr_update(d1, d2, x, r, Ar, s, it + 1 < iters));
   }
   return GMG_OK;
 }
@@ -1034,9 +1036,7 @@ gmg_status alloc_level_ws(MGLevel& L, int R, bool krylov, bool flexible) {
     GMG_TRY(L.kw.alloc(L.V, R, L.dof, p));
     GMG_TRY(L.kt.alloc(L.V, R, L.dof, p));
   }
-  GMG_TRY(L.mr_r.alloc(L.V, R, L.dof, p));
-  GMG_TRY(L.mr_Ar.alloc(L.V, R, L.dof, p));
-  GMG_TRY(L.mr_t.alloc(L.V, R, L.dof, p));
+  GMG_TRY(alloc_fields(L.mr_r, L.V, R, L.dof, p, 2));
   if (L.l == 0 && L.bf16_smoother) {
     GMG_TRY(alloc_fields(L.mr_r16, L.V, R, L.dof, GMG_BF16, L.mr_keep));
     GMG_TRY(L.mr_Ar16.alloc(L.V, R, L.dof, GMG_BF16));

@@ -66,8 +66,9 @@ gmg_status vec_scale_inv_norm(const double2* n_dev, const Vec& X, Vec& Y, cudaSt
 // MR step with alpha = d1 / d2 (device): x += alpha r, r -= alpha Ar
 // x += a r, and r -= a Ar unless update_r is false, a = <Ar, r> / <Ar, Ar> per RHS
 // (r, Ar BF16 with x FP32: the products in FP32, r rounded back to BF16)
+// (conj_d1: d1 holds <r, Ar>, the conjugate)
 gmg_status vec_mr_update(const double2* d1, const double2* d2, Vec& x, Vec& r, const Vec& Ar, cudaStream_t s,
-                         bool update_r = true);
+                         bool update_r = true, bool conj_d1 = false);
 // Y = X - Y
 gmg_status vec_xmy(const Vec& X, Vec& Y, cudaStream_t s);
 // Delayed-reorthogonalisation Gram-Schmidt sweeps (FP64, V0 [nv + 2] vectors at

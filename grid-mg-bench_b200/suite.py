@@ -321,9 +321,10 @@ def c5_small(nrhs=24):
 
 
 def profile_rows(rows):
-    """Small cases of the C3 transfers, the fine operator and the C4 construction
-    for ncu captures: 16^4 fine lattice (nbasis 32 on 4^4 blocks, 32 RHS;
-    Wilson-clover with 24 RHS; CoarsenOperator with nbasis 40)."""
+    """Small cases of the C3 transfers, the fine operator, the MG solve and the C4
+    construction for ncu captures: 16^4 fine lattice (nbasis 32 on 4^4 blocks,
+    32 RHS; Wilson-clover with 24 RHS; one restart cycle of the C5 solve's
+    kernels with 24 RHS; CoarsenOperator with nbasis 40)."""
     fd, cd, N, R = (16, 16, 16, 16), (4, 4, 4, 4), 32, 32
     Vf, Vc = 16 ** 4, 4 ** 4
     if "p_c3" in rows:
@@ -415,6 +416,29 @@ def profile_rows(rows):
              " K-cycle", ok=True, seconds=t, iters=it, relres=rr)
         del mg, x, b, w5
         torch.cuda.empty_cache()
+    if "p_mg16" in rows:
+        # the C5 solve's kernels on a 16^4 lattice (24 RHS, mixed BF16, host-driven
+        # K-cycle): setup, then 8 outer iterations (one restart cycle, every
+        # Gram-Schmidt sweep of it) inside the NVTX range "p_mg16"; the solve stops
+        # at its iteration limit, well above the tolerance
+        U = inputs.torch_smooth_gauge(fd, 801, 0.3)
+        w = gmg.WilsonClover(fd, -0.35, 1.0, antiperiodic=True)
+        w.set_gauge(U)
+        del U
+        b = inputs.torch_gaussian((Vf, 24, 12), 802)
+        mg = gmg.MultiGrid(w, 24, prec="bf16", graph=0, nlevels=3, block=((4, 4, 4, 4), (2, 2, 2, 2)),
+                           nvec=(12, 16), smoother_iters=8, setup_iters=30)
+        mg.setup()
+        x = torch.zeros_like(b)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("p_mg16")
+        try:
+            mg.solve(b, x, tol=1e-10, maxiter=8)
+        except gmg.GmgError:
+            pass
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        line("p_mg16 MG solve kernels 16^4, 24 RHS, mixed BF16, 8 outer iterations", ok=True)
     if "p_c4" in rows:
         # CoarsenOperator 16^4 -> 4^4, nbasis 40 (the C4 construction on a
         # sixteenth of its volume): two calls, each with 4 face hops, one
