@@ -730,6 +730,91 @@ __global__ void __launch_bounds__(1024) xmy_bf16_blocked_row_kernel(const float2
   }
 }
 
+// The same two steps on site-blocked fields, one 16-byte quarter (four
+// complex numbers of one RHS) per thread: a quarter of the threads and of the
+// index arithmetic per element of the word-wise kernels.
+// rn = bf16(r - a Ar), a = d1 / d2 per RHS
+__global__ void __launch_bounds__(256) mr_resid_bf16_q_kernel(const double2* __restrict__ d1,
+                                                              const double2* __restrict__ d2,
+                                                              const uint4* __restrict__ r, const uint4* __restrict__ Ar,
+                                                              uint4* __restrict__ rn, int64_t V, int R, int spb) {
+  const int RQ = 3 * R, t = threadIdx.x;
+  if (t >= spb * RQ) return;
+  const int so = t / RQ, q = t % RQ, k = q % R;  // quarter q = g R + k of a site's block
+  const double den = d2[k].x;
+  const float ar = den > 0.0 ? (float)(d1[k].x / den) : 0.f, ai = den > 0.0 ? (float)(d1[k].y / den) : 0.f;
+  for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+    const int64_t e = s * RQ + q;
+    const uint4 u = r[e], v = Ar[e];
+    const uint32_t uw[4] = {u.x, u.y, u.z, u.w}, vw[4] = {v.x, v.y, v.z, v.w};
+    uint32_t o[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float2 x = bf16w_to_f2(uw[j]), y = bf16w_to_f2(vw[j]);
+      o[j] = f2_to_bf16w(x.x - (ar * y.x - ai * y.y), x.y - (ar * y.y + ai * y.x));
+    }
+    rn[e] = make_uint4(o[0], o[1], o[2], o[3]);
+  }
+}
+
+// x (FP32 [V][R][12]) += sum_j a_j r_j, the r_j site-blocked; a thread takes
+// components 4g .. 4g + 3 of RHS k (one quarter of every r_j, 32 bytes of x)
+template <int K>
+__global__ void __launch_bounds__(256) mr_xsum_bf16_q_kernel(const double2* __restrict__ d, int dstride,
+                                                             const uint4* __restrict__ r0, int64_t rstride,
+                                                             float4* __restrict__ x, int64_t V, int R, int spb) {
+  const int RQ = 3 * R, t = threadIdx.x;
+  if (t >= spb * RQ) return;
+  const int so = t / RQ, q = t % RQ, k = q / 3, g = q % 3;
+  float2 a[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    a[j] = make_float2(0.f, 0.f);
+    const double den = d[(int64_t)j * dstride + R + k].x;
+    const double2 num = d[(int64_t)j * dstride + k];
+    if (den > 0.0) a[j] = make_float2((float)(num.x / den), (float)(num.y / den));
+  }
+  const int rq = g * R + k;           // the quarter in the blocked layout
+  const int xq = (k * 12 + 4 * g) / 2;  // the first float4 of x (two complex numbers each)
+  for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
+    uint4 w[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) w[j] = __ldg(r0 + j * rstride + s * RQ + rq);
+    float2 acc[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      const uint32_t ww[4] = {w[j].x, w[j].y, w[j].z, w[j].w};
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float2 v = bf16w_to_f2(ww[c]);
+        acc[c].x += a[j].x * v.x - a[j].y * v.y;
+        acc[c].y += a[j].x * v.y + a[j].y * v.x;
+      }
+    }
+    float4* xp = x + s * 6 * R + xq;
+    float4 x0 = xp[0], x1 = xp[1];
+    x0.x += acc[0].x;
+    x0.y += acc[0].y;
+    x0.z += acc[1].x;
+    x0.w += acc[1].y;
+    x1.x += acc[2].x;
+    x1.y += acc[2].y;
+    x1.z += acc[3].x;
+    x1.w += acc[3].y;
+    xp[0] = x0;
+    xp[1] = x1;
+  }
+}
+
+static Row quarter_geom(int64_t V, int R) {
+  Row g;
+  g.RD = 3 * R;
+  g.spb = g.RD <= 256 ? std::max(1, 256 / g.RD) : 1;
+  g.threads = (g.spb * g.RD + 31) / 32 * 32;
+  g.grid = (int)std::max<int64_t>(1, std::min<int64_t>((V + g.spb - 1) / g.spb, 148 * 16));
+  return g;
+}
+
 __global__ void xmy_bf16_kernel(const float2* __restrict__ X, const float2* __restrict__ Y, uint32_t* __restrict__ Z,
                                 int64_t n) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
@@ -1078,6 +1163,13 @@ gmg_status vec_mr_resid_bf16(const double2* d1, const double2* d2, const Vec& r,
   GMG_CHECK(r.prec == GMG_BF16 && Ar.prec == GMG_BF16 && rn.prec == GMG_BF16 && r.R * r.dof <= 1024 &&
                 (!blocked || r.dof == 12),
             GMG_ERR_UNSUPPORTED, "mr residual: BF16 fields with at most 1024 values per site");
+  if (blocked && 3 * r.R <= 256) {
+    const blas::Row qg = blas::quarter_geom(r.V, r.R);
+    blas::mr_resid_bf16_q_kernel<<<qg.grid, qg.threads, 0, s>>>(d1, d2, (const uint4*)r.p, (const uint4*)Ar.p,
+                                                               (uint4*)rn.p, r.V, r.R, qg.spb);
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  }
   const blas::Row rg = blas::row_geom(r.V, r.R, r.dof);
   blas::mr_resid_bf16_row_kernel<<<rg.grid, rg.threads, 0, s>>>(d1, d2, (const uint32_t*)r.p, (const uint32_t*)Ar.p,
                                                                (uint32_t*)rn.p, r.V, r.R, r.dof, rg.spb, blocked);
@@ -1090,6 +1182,32 @@ gmg_status vec_mr_xsum_bf16(const double2* d, int dstride, int K, const Vec& r0,
   GMG_CHECK(r0.prec == GMG_BF16 && x.prec == GMG_F32 && K >= 1 && K <= kMrMaxSteps && x.R * x.dof <= 1024 &&
                 (!blocked || x.dof == 12),
             GMG_ERR_UNSUPPORTED, "mr sum: BF16 residuals, an FP32 solution, 1 to 16 steps");
+  if (blocked && 3 * x.R <= 256 && (((uintptr_t)x.p | (uintptr_t)r0.p) & 15) == 0 && rstride % 4 == 0) {
+    const blas::Row qg = blas::quarter_geom(x.V, x.R);
+    auto gq = [&](auto kern) {
+      kern<<<qg.grid, qg.threads, 0, s>>>(d, dstride, (const uint4*)r0.p, rstride / 4, (float4*)x.p, x.V, x.R, qg.spb);
+    };
+    switch (K) {
+      case 1: gq(blas::mr_xsum_bf16_q_kernel<1>); break;
+      case 2: gq(blas::mr_xsum_bf16_q_kernel<2>); break;
+      case 3: gq(blas::mr_xsum_bf16_q_kernel<3>); break;
+      case 4: gq(blas::mr_xsum_bf16_q_kernel<4>); break;
+      case 5: gq(blas::mr_xsum_bf16_q_kernel<5>); break;
+      case 6: gq(blas::mr_xsum_bf16_q_kernel<6>); break;
+      case 7: gq(blas::mr_xsum_bf16_q_kernel<7>); break;
+      case 8: gq(blas::mr_xsum_bf16_q_kernel<8>); break;
+      case 9: gq(blas::mr_xsum_bf16_q_kernel<9>); break;
+      case 10: gq(blas::mr_xsum_bf16_q_kernel<10>); break;
+      case 11: gq(blas::mr_xsum_bf16_q_kernel<11>); break;
+      case 12: gq(blas::mr_xsum_bf16_q_kernel<12>); break;
+      case 13: gq(blas::mr_xsum_bf16_q_kernel<13>); break;
+      case 14: gq(blas::mr_xsum_bf16_q_kernel<14>); break;
+      case 15: gq(blas::mr_xsum_bf16_q_kernel<15>); break;
+      default: gq(blas::mr_xsum_bf16_q_kernel<16>); break;
+    }
+    GMG_CUDA(cudaGetLastError());
+    return GMG_OK;
+  }
   const blas::Row rg = blas::row_geom(x.V, x.R, x.dof);
   auto go = [&](auto kern) {
     kern<<<rg.grid, rg.threads, 0, s>>>(d, dstride, (const uint32_t*)r0.p, rstride, (float2*)x.p, x.V, x.R, x.dof,

@@ -31,10 +31,13 @@
 // and returns.
 //
 // Global layouts (prepared once per link set / per apply):
-//   links  [V][9][Kc][Mp][8]   halves, Kc = ceil16(N)/8 K-chunks, Mp = 64 or
-//          128 rows, interleaved as above, zero-padded beyond 2N
-//   packed [V][Kc][2Rp][8]     halves: rows n < Rp = Re in[r=n][.],
-//          Rp <= n < 2Rp = Im in[r=n-Rp][.]  (Rp = R rounded up to 16)
+//   links  [V][9][Ks][Mr][8]   halves, Ks = ceil(N/8) K-chunks of Mr = 2N
+//          rows (rounded up to 8), interleaved as above, zero-padded beyond 2N
+//          and N (the MMA's M = 64 / 128 rows and whole K-steps are read
+//          across the tile boundaries, see link_geometry)
+//   packed [V][Kc][2Rp][8]     halves, Kc = ceil16(N)/8: rows n < Rp = Re
+//          in[r=n][.], Rp <= n < 2Rp = Im in[r=n-Rp][.]  (Rp = R rounded up
+//          to 16), zero beyond N and R
 // Both are the canonical no-swizzle K-major core-matrix layout
 // (8 rows x 16 B per core matrix): SBO = 128 B, LBO = rows * 16 B.
 #include <algorithm>
@@ -207,7 +210,7 @@ __device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, float* va,
 }
 
 struct Params {
-  const uint16_t* links;   // [V][9][Kc][Mp][8]
+  const uint16_t* links;   // [V][9][Ks][Mr][8]
   const uint16_t* packed;  // [V][Kc][2Rp][8]
   const int32_t* nbr;      // [9][V]: input index of point p's neighbour of output index o
   const int32_t* site_map; // [V] link site of output index o (null: o itself)
@@ -215,6 +218,7 @@ struct Params {
   float2* out;             // [V][nrhs][N]
   int* err;                // device error word
   int V, N, nrhs, R, Rp, Kc, Mp, p0, p1, g5, stages, kind, pps;
+  int Ks, Mr;              // stored link tile: Ks K-chunks of Mr rows (see link_geometry)
 };
 
 // The MMAs of one stage as straight-line code: PPS points x KH K-steps.  Issuing
@@ -249,7 +253,7 @@ template <int CTAS>  // CTAs per SM the register budget allows (1 or 2)
 __global__ void __launch_bounds__(kThreads, CTAS) coarse_mrhs_tc_kernel(const Params P) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t link_bytes = (uint32_t)P.Kc * P.Mp * 16;     // one stencil point of one site
+  const uint32_t link_bytes = (uint32_t)P.Ks * P.Mr * 16;     // one stencil point of one site
   const uint32_t vec_bytes = (uint32_t)P.Kc * 2 * P.Rp * 16;  // one neighbour tile
   const int pps = P.pps;                                      // stencil points per stage
   const uint32_t stage_bytes = (uint32_t)pps * (link_bytes + vec_bytes);
@@ -392,10 +396,10 @@ __global__ void __launch_bounds__(kThreads, CTAS) coarse_mrhs_tc_kernel(const Pa
                              | ((uint32_t)(2 * P.Rp) >> 3) << 17  // N
                              | ((uint32_t)P.Mp >> 4) << 24;       // M
       // Descriptors advance by adding 16-byte units to their start-address field.
-      const uint64_t adesc0 = make_desc(stage_base, (uint32_t)P.Mp * 16, 128);
+      const uint64_t adesc0 = make_desc(stage_base, (uint32_t)P.Mr * 16, 128);
       const uint64_t bdesc0 = make_desc(stage_base + (size_t)pps * link_bytes, (uint32_t)(2 * P.Rp) * 16, 128);
       const uint32_t st_units = stage_bytes >> 4, a_pt = link_bytes >> 4, b_pt = vec_bytes >> 4;
-      const uint32_t a_ks = 2 * P.Mp, b_ks = 4 * P.Rp;  // two 16-byte K-chunks per MMA
+      const uint32_t a_ks = 2 * P.Mr, b_ks = 4 * P.Rp;  // two 16-byte K-chunks per MMA
       const int kh = P.Kc / 2;
       int stage = 0;
       uint32_t phase = 0, st_off = 0;
@@ -514,7 +518,7 @@ __device__ __forceinline__ uint32_t to_half_pair(float a, float b, int kind) {
   return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// links (exchange layout, FP64) -> [V][9][Kc][Mp][8] halves
+// links (exchange layout, FP64) -> [V][9][Ks][Mr][8] halves (Kc, Mp: the chunk and row counts stored)
 __global__ void pack_links_kernel(const double2* __restrict__ A, uint4* __restrict__ dst, int V, int N, int Kc,
                                   int Mp, int kind) {
   const int64_t total = (int64_t)V * 9 * Kc * Mp;  // one 16-byte row each
@@ -759,19 +763,33 @@ inline gmg_status launch_pack(const float* in, uint4* packed, const int32_t* act
   return GMG_OK;
 }
 
+// The stored link tile of one stencil point: Ks = ceil(N / 8) K-chunks of
+// Mr = 2N rows rounded up to a core-matrix group of 8, i.e. without the MMA's
+// padding to a whole K-step (16) and to M = 64 / 128 rows.  The MMA still reads
+// whole K-steps and M rows at the chunk stride Mr * 16: its extra rows land on
+// the next chunk (only accumulator rows >= 2N, never read, see them) and its
+// extra K-chunk on the next point's tile or the stage's vector tiles (finite
+// values, multiplied by the zero K-padding of the packed vectors).  At
+// nbasis 24 a point's tile is 2304 bytes instead of 4096, at nbasis 40 6400
+// instead of 12288; at nbasis 32 nothing changes.
+inline void link_geometry(int N, int* Ks, int* Mr) {
+  *Ks = (N + 7) / 8;
+  *Mr = round_up(2 * N, 8);
+}
+
 }  // namespace tc
 
 gmg_status coarse_prepare_tc(gmg_coarse* h, int kind, cudaStream_t s) {
   const int N = h->N;
   GMG_CHECK(2 * N <= 128, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil needs nbasis <= 64");
-  const int Kc = tc::round_up(N, 16) / 8;
-  const int Mp = 2 * N <= 64 ? 64 : 128;
+  int Ks, Mr;
+  tc::link_geometry(N, &Ks, &Mr);
   const int V = (int)h->dims.vol();
-  const size_t bytes = (size_t)V * 9 * Kc * Mp * 16;
+  const size_t bytes = (size_t)V * 9 * Ks * Mr * 16;
   GMG_TRY(h->links_h.buf.alloc(bytes));
-  const int64_t rows = (int64_t)V * 9 * Kc * Mp;
+  const int64_t rows = (int64_t)V * 9 * Ks * Mr;
   tc::pack_links_kernel<<<(int)std::min<int64_t>((rows + 255) / 256, 148 * 64), 256, 0, s>>>(
-      h->links_ref.as<double2>(), h->links_h.buf.as<uint4>(), V, N, Kc, Mp, kind);
+      h->links_ref.as<double2>(), h->links_h.buf.as<uint4>(), V, N, Ks, Mr, kind);
   GMG_CUDA(cudaGetLastError());
   h->links_h.kind = kind;
   return GMG_OK;
@@ -826,7 +844,13 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, cons
   const int Rp = round_up(R, 16);
   const int Kc = round_up(N, 16) / 8;
   const int Mp = 2 * N <= 64 ? 64 : 128;
-  const uint32_t per_point = (uint32_t)Kc * Mp * 16 + (uint32_t)Kc * 2 * Rp * 16;
+  int Ks, Mr;
+  link_geometry(N, &Ks, &Mr);
+  // the MMA's reads beyond a point's stored tile stay inside the stage: the
+  // last K-step of the last point reaches at most this far past the link tiles
+  const uint32_t over = (uint32_t)(Kc - 1) * Mr * 16 + (uint32_t)Mp * 16 - (uint32_t)Ks * Mr * 16;
+  GMG_CHECK(over <= (uint32_t)Kc * 2 * Rp * 16, GMG_ERR_UNSUPPORTED, "tensor-core coarse stencil: link tile geometry");
+  const uint32_t per_point = (uint32_t)Ks * Mr * 16 + (uint32_t)Kc * 2 * Rp * 16;
   const int npts = p1 - p0;
   const uint32_t acc_cols = 2 * (uint32_t)Rp;
   const uint32_t nacc = std::min<uint32_t>(kAccBufs, 512u / acc_cols);
@@ -861,6 +885,8 @@ static gmg_status launch_stencil(gmg_coarse* h, const uint4* packed, int V, cons
   P.Rp = Rp;
   P.Kc = Kc;
   P.Mp = Mp;
+  P.Ks = Ks;
+  P.Mr = Mr;
   P.p0 = p0;
   P.p1 = p1;
   P.g5 = g5 ? 1 : 0;
