@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(1024) multidot_row_kernel(const typename C2<T>
   double ar[JB], ai[JB];
 #pragma unroll
   for (int j = 0; j < JB; ++j) ar[j] = ai[j] = 0.0;
-  if (act) {
+  if (act && sizeof(T) == 8) {
     for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += (int64_t)gridDim.x * spb) {
       const int64_t e = s * RD + i;
       const double yr = Y[e].x, yi = Y[e].y;
@@ -216,6 +216,33 @@ __global__ void __launch_bounds__(1024) multidot_row_kernel(const typename C2<T>
           const typename C2<T>::t x = X[(int64_t)(j0 + j) * xstride + e];
           ar[j] += (double)x.x * yr + (double)x.y * yi;
           ai[j] += (double)x.x * yi - (double)x.y * yr;
+        }
+      }
+    }
+  } else if (act) {
+    // FP32: two sites per round, their loads issued together (short vectors on
+    // the coarse levels give a thread a few dozen sites, each an L2 round trip)
+    const int64_t step = (int64_t)gridDim.x * spb;
+    for (int64_t s = (int64_t)blockIdx.x * spb + so; s < V; s += 2 * step) {
+      const bool two = s + step < V;
+      const int64_t e0 = s * RD + i, e1 = two ? (s + step) * RD + i : e0;
+      const typename C2<T>::t y0 = Y[e0], y1 = Y[e1];
+      typename C2<T>::t x0[JB], x1[JB];
+#pragma unroll
+      for (int j = 0; j < JB; ++j)
+        if (j < nj) {
+          x0[j] = X[(int64_t)(j0 + j) * xstride + e0];
+          x1[j] = X[(int64_t)(j0 + j) * xstride + e1];
+        }
+#pragma unroll
+      for (int j = 0; j < JB; ++j) {
+        if (j < nj) {
+          ar[j] += (double)x0[j].x * y0.x + (double)x0[j].y * y0.y;
+          ai[j] += (double)x0[j].x * y0.y - (double)x0[j].y * y0.x;
+          if (two) {
+            ar[j] += (double)x1[j].x * y1.x + (double)x1[j].y * y1.y;
+            ai[j] += (double)x1[j].x * y1.y - (double)x1[j].y * y1.x;
+          }
         }
       }
     }
@@ -858,8 +885,11 @@ gmg_status vec_multidot(const Vec& X0, int nx, int64_t xstride_elems, const Vec&
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     }
     // one resident wave of blocks: every block ends in nj * R global atomics on
-    // the same nj * R addresses, so more blocks than fit at once only add contention
-    const int grid = std::min(g.grid, 148 * std::max(1, 2048 / g.threads));
+    // the same nj * R addresses, so more blocks than fit at once only add
+    // contention; and on short vectors (the coarse levels) no more blocks than
+    // give each thread 32 sites, down to one per SM
+    const int64_t by_len = std::max<int64_t>(148, Y.V / (32 * (int64_t)g.spb));
+    const int grid = (int)std::min<int64_t>(std::min(g.grid, 148 * std::max(1, 2048 / g.threads)), by_len);
     for (int j0 = 0; j0 < nx; j0 += JB) {
       if (Y.prec == GMG_F64)
         blas::multidot_row_kernel<double, JB><<<grid, g.threads, sm, s>>>(

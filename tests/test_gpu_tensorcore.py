@@ -29,7 +29,7 @@ def run(cm, x, op, kind, point=8, active=None):
 
 
 @pytest.mark.parametrize("kind", ["bf16", "f16"])
-@pytest.mark.parametrize("N,R", [(32, 32), (32, 5), (24, 16), (40, 8), (16, 48)])
+@pytest.mark.parametrize("N,R", [(32, 32), (32, 5), (24, 16), (40, 8), (16, 48), (12, 24), (20, 8)])
 def test_tc_m_and_mdag(kind, N, R):
     dims = (4, 4, 4, 4)
     r = inputs.rng(stream=200 + N + R)
