@@ -187,6 +187,163 @@ __global__ void __launch_bounds__(256) coarse_simt_kernel(
   }
 }
 
+// ---------------------------------------------------------------------------
+// The multi-RHS stencil on the CUDA cores, pipelined: a CTA walks the (site,
+// point) items of its sites; while it multiplies item k, the link matrix and
+// the neighbour's R vectors of item k + 1 are copied into the other half of
+// its shared memory with cp.async.  A thread owns a TR x TB tile of the R x N
+// output, its rows and columns interleaved (r = rt + (R / TR) j, b = bt + (N /
+// TB) i), so that the lanes of a warp read consecutive rows of the padded
+// shared-memory tiles (row stride N + 1 complex numbers: no bank conflicts).
+// Needs TB | N and TR | R.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async_c(void* dst, const double2* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_c(void* dst, const float2* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <class T, int TR, int TB, int NC>  // NC: N as a compile-time constant (0: runtime)
+__global__ void __launch_bounds__(256) coarse_simt_pipe_kernel(
+    const typename cplx_t<T>::type* __restrict__ links, int link_pts, int pbase, const int32_t* __restrict__ site_map,
+    const int32_t* __restrict__ nbr, int dag, const typename cplx_t<T>::type* __restrict__ in,
+    typename cplx_t<T>::type* __restrict__ out, int V, int N_, int nrhs, const int32_t* __restrict__ active, int R,
+    int p0, int p1, int g5) {
+  typedef typename cplx_t<T>::type C;
+  const int N = NC ? NC : N_;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NP = N + 1;                     // padded row stride
+  const int stage = (N + R) * NP;           // complex numbers per stage: A [N][NP], X [R][NP]
+  C* S = reinterpret_cast<C*>(smem_raw);
+  const int t = threadIdx.x, nthr = blockDim.x;
+  const int NBT = N / TB, NRT = R / TR;
+  const int bt = t % NBT, rt = t / NBT;
+  const bool comp = t < NBT * NRT;
+  const int half = N / 2;
+  const int npts = p1 - p0;
+  const int nsites = (V - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int nitems = nsites * npts;
+
+  // copies of item k (site blockIdx.x + (k / npts) gridDim.x, point p0 + k % npts) into stage k & 1
+  auto issue = [&](int k) {
+    const int site = blockIdx.x + (k / npts) * gridDim.x;
+    const int p = p0 + k % npts;
+    const int64_t lsite = site_map ? site_map[site] : site;
+    const C* Ap = links + (lsite * link_pts + (p - pbase)) * (int64_t)N * N;
+    const int nb = nbr ? nbr[(int64_t)p * V + site] : site;
+    C* A = S + (k & 1) * stage;
+    C* X = A + N * NP;
+    for (int e = t; e < N * N; e += nthr) cp_async_c(A + (e / N) * NP + e % N, Ap + e);
+    const C* xs = in + (int64_t)nb * nrhs * N;
+    for (int e = t; e < R * N; e += nthr) {
+      const int r = e / N, bb = e - r * N;
+      const int slot = active ? active[r] : r;
+      cp_async_c(X + r * NP + bb, xs + slot * N + bb);
+    }
+    cp_async_commit();
+  };
+
+  C acc[TR][TB];
+  if (nitems > 0) issue(0);
+  for (int k = 0; k < nitems; ++k) {
+    if (k + 1 < nitems) {
+      issue(k + 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int kp = k % npts;
+    if (kp == 0) {
+#pragma unroll
+      for (int j = 0; j < TR; ++j)
+#pragma unroll
+        for (int i = 0; i < TB; ++i) acc[j][i] = C{0, 0};
+    }
+    if (comp) {
+      const C* A = S + (k & 1) * stage;
+      const C* X = A + N * NP;
+      for (int bb = 0; bb < N; ++bb) {
+        C a[TB], x[TR];
+#pragma unroll
+        for (int i = 0; i < TB; ++i) {
+          const int b = bt + NBT * i;
+          a[i] = dag ? cconj(A[bb * NP + b]) : A[b * NP + bb];  // (A^dag)[b][bb] = conj(A[bb][b])
+        }
+        const T sg = (g5 && bb >= half) ? (T)-1 : (T)1;
+#pragma unroll
+        for (int j = 0; j < TR; ++j) {
+          x[j] = X[(rt + NRT * j) * NP + bb];
+          x[j].x *= sg;
+          x[j].y *= sg;
+        }
+#pragma unroll
+        for (int j = 0; j < TR; ++j)
+#pragma unroll
+          for (int i = 0; i < TB; ++i) acc[j][i] = cmul_add(acc[j][i], a[i], x[j]);
+      }
+      if (kp == npts - 1) {
+        const int site = blockIdx.x + (k / npts) * gridDim.x;
+#pragma unroll
+        for (int j = 0; j < TR; ++j) {
+          const int r = rt + NRT * j;
+          const int slot = active ? active[r] : r;
+          C* o = out + ((int64_t)site * nrhs + slot) * N;
+#pragma unroll
+          for (int i = 0; i < TB; ++i) {
+            const int b = bt + NBT * i;
+            C v = acc[j][i];
+            if (g5 && b >= half) {
+              v.x = -v.x;
+              v.y = -v.y;
+            }
+            o[b] = v;
+          }
+        }
+      }
+    }
+    __syncthreads();  // stage k & 1 is refilled by the issue of item k + 2
+  }
+}
+
+template <class T, int TR, int TB>
+static bool launch_simt_pipe(const LinkSel& L, const void* in, void* out, int V, int N, int nrhs,
+                             const int32_t* active, int R, int p0, int p1, int g5, cudaStream_t s,
+                             gmg_status* st) {
+  typedef typename cplx_t<T>::type C;
+  if (N % TB || R % TR || (N / TB) * (R / TR) > 256 || p1 <= p0) return false;
+  const size_t smem = sizeof(C) * 2 * (size_t)(N + R) * (N + 1);
+  if (smem > 200 * 1024) return false;
+  const int threads = std::max(32, ((N / TB) * (R / TR) + 31) / 32 * 32);
+  auto kern = N == 32 ? coarse_simt_pipe_kernel<T, TR, TB, 32>
+             : N == 24 ? coarse_simt_pipe_kernel<T, TR, TB, 24>
+             : N == 40 ? coarse_simt_pipe_kernel<T, TR, TB, 40>
+                       : coarse_simt_pipe_kernel<T, TR, TB, 0>;
+  *st = GMG_OK;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    *st = fail(GMG_ERR_CUDA, "coarse apply: shared-memory attribute");
+    return true;
+  }
+  int dev = 0, nsm = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  const int grid = std::min(V, nsm * std::max(per_sm, 1));
+  KernelTimer kt("coarse_simt", s);
+  kern<<<grid, threads, smem, s>>>(reinterpret_cast<const C*>(L.links), L.link_pts, L.pbase, L.site_map, L.nbr, L.dag,
+                                   reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), V, N, nrhs, active, R,
+                                   p0, p1, g5);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) *st = fail(GMG_ERR_CUDA, std::string("coarse apply: ") + cudaGetErrorString(e));
+  return true;
+}
+
 template <class T, int TR, int TB>
 static gmg_status launch_simt(const LinkSel& L, const void* in, void* out,
                               int V, int N, int nrhs, const int32_t* active, int R, int p0, int p1,
@@ -396,10 +553,13 @@ gmg_status coarse_apply_simt_ex(gmg_coarse* h, int src, int V, const int32_t* si
     if (compute == GMG_F64) return launch_1rhs<double>(L, in, out, V, N, nrhs, 0, p0, p1, g5, s);
     return launch_1rhs<float>(L, in, out, V, N, nrhs, 0, p0, p1, g5, s);
   }
+  gmg_status st = GMG_OK;
   if (compute == GMG_F64) {
+    if (R >= 4 && launch_simt_pipe<double, 4, 2>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s, &st)) return st;
     if (R >= 4) return launch_simt<double, 4, 4>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
     return launch_simt<double, 1, 2>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
   }
+  if (R >= 4 && launch_simt_pipe<float, 4, 2>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s, &st)) return st;
   if (R >= 4) return launch_simt<float, 4, 4>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
   return launch_simt<float, 1, 2>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
 }
