@@ -455,7 +455,7 @@ def main():
     f64_leg = {
         "value": world * FLOPS * n64 / (t64 * 1e-3) / 1e12, "unit": UNIT, "steps": n64,
         "ms_per_step": t64 / n64, "dtype": "f64",
-        "form": "FP64 links and vectors on the CUDA cores (coarse_simt_kernel), the arithmetic of the reference "
+        "form": "FP64 links and vectors on the CUDA cores (coarse_simt_pipe_kernel), the arithmetic of the reference "
                 "and of its CPU arm",
         "e2e": {"value": e2e64, "unit": UNIT, "h2d_bytes_per_step": e2e64_bytes, "d2h_bytes_per_step": e2e64_bytes,
                 "how": "public gmg_coarse_apply (compute F64) with pinned complex128 host input/output every step, "
