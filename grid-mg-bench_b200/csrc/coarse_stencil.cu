@@ -209,6 +209,32 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// acc[j][i] += (or -= with NEG) a_i x_j over bb in [bb0, bb1), a_i = A[b_i][bb]
+// (DAG: conj(A[bb][b_i])), x_j = X[r_j][bb]; the signs are folded into the FMAs
+template <bool DAG, bool NEG, int TR, int TB, class C>
+__device__ __forceinline__ void pipe_mac(C (&acc)[TR][TB], const C* __restrict__ A, const C* __restrict__ X, int bb0,
+                                         int bb1, int NP, int bt, int NBT, int rt, int NRT) {
+  for (int bb = bb0; bb < bb1; ++bb) {
+    C a[TB], x[TR];
+#pragma unroll
+    for (int i = 0; i < TB; ++i) a[i] = DAG ? A[bb * NP + bt + NBT * i] : A[(bt + NBT * i) * NP + bb];
+#pragma unroll
+    for (int j = 0; j < TR; ++j) x[j] = X[(rt + NRT * j) * NP + bb];
+#pragma unroll
+    for (int j = 0; j < TR; ++j)
+#pragma unroll
+      for (int i = 0; i < TB; ++i) {
+        // (ar + i s ai)(xr + i xi) with s = -1 for the conjugate, the product negated with NEG
+        const auto ar = NEG ? -a[i].x : a[i].x;
+        const auto ai = (NEG != DAG) ? -a[i].y : a[i].y;
+        acc[j][i].x = fma(ar, x[j].x, acc[j][i].x);
+        acc[j][i].x = fma(-ai, x[j].y, acc[j][i].x);
+        acc[j][i].y = fma(ar, x[j].y, acc[j][i].y);
+        acc[j][i].y = fma(ai, x[j].x, acc[j][i].y);
+      }
+  }
+}
+
 template <class T, int TR, int TB, int NC>  // NC: N as a compile-time constant (0: runtime)
 __global__ void __launch_bounds__(256) coarse_simt_pipe_kernel(
     const typename cplx_t<T>::type* __restrict__ links, int link_pts, int pbase, const int32_t* __restrict__ site_map,
@@ -269,24 +295,17 @@ __global__ void __launch_bounds__(256) coarse_simt_pipe_kernel(
     if (comp) {
       const C* A = S + (k & 1) * stage;
       const C* X = A + N * NP;
-      for (int bb = 0; bb < N; ++bb) {
-        C a[TB], x[TR];
-#pragma unroll
-        for (int i = 0; i < TB; ++i) {
-          const int b = bt + NBT * i;
-          a[i] = dag ? cconj(A[bb * NP + b]) : A[b * NP + bb];  // (A^dag)[b][bb] = conj(A[bb][b])
-        }
-        const T sg = (g5 && bb >= half) ? (T)-1 : (T)1;
-#pragma unroll
-        for (int j = 0; j < TR; ++j) {
-          x[j] = X[(rt + NRT * j) * NP + bb];
-          x[j].x *= sg;
-          x[j].y *= sg;
-        }
-#pragma unroll
-        for (int j = 0; j < TR; ++j)
-#pragma unroll
-          for (int i = 0; i < TB; ++i) acc[j][i] = cmul_add(acc[j][i], a[i], x[j]);
+      // the dagger and the input G5C (the sign of components bb >= N / 2) are
+      // uniform per launch and per half of bb: four loop forms, no per-element
+      // selects or sign multiplies
+      if (!dag) {
+        pipe_mac<false, false, TR, TB>(acc, A, X, 0, half, NP, bt, NBT, rt, NRT);
+        if (g5) pipe_mac<false, true, TR, TB>(acc, A, X, half, N, NP, bt, NBT, rt, NRT);
+        else pipe_mac<false, false, TR, TB>(acc, A, X, half, N, NP, bt, NBT, rt, NRT);
+      } else {
+        pipe_mac<true, false, TR, TB>(acc, A, X, 0, half, NP, bt, NBT, rt, NRT);
+        if (g5) pipe_mac<true, true, TR, TB>(acc, A, X, half, N, NP, bt, NBT, rt, NRT);
+        else pipe_mac<true, false, TR, TB>(acc, A, X, half, N, NP, bt, NBT, rt, NRT);
       }
       if (kp == npts - 1) {
         const int site = blockIdx.x + (k / npts) * gridDim.x;
