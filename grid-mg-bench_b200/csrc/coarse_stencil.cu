@@ -578,7 +578,7 @@ gmg_status coarse_apply_simt_ex(gmg_coarse* h, int src, int V, const int32_t* si
     if (R >= 4) return launch_simt<double, 4, 4>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
     return launch_simt<double, 1, 2>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
   }
-  if (R >= 4 && launch_simt_pipe<float, 4, 2>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s, &st)) return st;
+  if (R >= 4 && launch_simt_pipe<float, 4, 4>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s, &st)) return st;
   if (R >= 4) return launch_simt<float, 4, 4>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
   return launch_simt<float, 1, 2>(L, in, out, V, N, nrhs, active, R, p0, p1, g5, s);
 }
