@@ -338,7 +338,9 @@ static bool launch_simt_pipe(const LinkSel& L, const void* in, void* out, int V,
   typedef typename cplx_t<T>::type C;
   if (N % TB || R % TR || (N / TB) * (R / TR) > 256 || p1 <= p0) return false;
   const size_t smem = sizeof(C) * 2 * (size_t)(N + R) * (N + 1);
-  if (smem > 200 * 1024) return false;
+  // at least 3 CTAs per SM: with two (FP64 nbasis 40 x 40 RHS, the coarse-of-
+  // coarse construction) the kernel without the pipeline, at 4, was faster
+  if (smem > 72 * 1024) return false;
   const int threads = std::max(32, ((N / TB) * (R / TR) + 31) / 32 * 32);
   auto kern = N == 32 ? coarse_simt_pipe_kernel<T, TR, TB, 32>
              : N == 24 ? coarse_simt_pipe_kernel<T, TR, TB, 24>
