@@ -128,6 +128,45 @@ def test_coarse_mrhs_config_sizes(dims, N):
     assert orc.rel_dev_sq(ref, host(out)) < TOL64
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("N,R", [(24, 4), (32, 12), (40, 8), (16, 32)])
+def test_coarse_pipelined_simt_ops(prec, N, R):
+    # the pipelined CUDA-core stencil (RHS counts the register tiles divide):
+    # M, Mdag (dagger and G5C loop forms), Mdiag, one Mdir point, and an active
+    # subset whose size the tiles divide, against the oracle
+    dims = (4, 4, 4, 2)
+    r = inputs.rng(stream=140 + N + R)
+    A = inputs.random_links(dims, N, r)
+    x = inputs.gaussian_field((int(np.prod(dims)), R + 2, N), r)
+    cm = gmg.CoarsenedMatrix(dims, N)
+    cm.set_links(A)
+    dt, tol = (torch.complex128, TOL64) if prec == "f64" else (torch.complex64, TOL32)
+    if prec == "f32":
+        cm.prepare("f32")
+    inp = dev(x[:, :R], dt)
+    for code, name in ((orc.OP_M, "M"), (orc.OP_MDAG, "Mdag"), (orc.OP_MDIAG, "Mdiag")):
+        ref = orc.coarse_apply(dims, A, x[:, :R], code)
+        out = torch.zeros_like(inp)
+        getattr(cm, name)(inp, out)
+        assert orc.rel_dev_sq(ref, host(out)) < tol, (name, orc.rel_dev_sq(ref, host(out)))
+    ref = orc.coarse_apply(dims, A, x[:, :R], orc.OP_MDIR, point=5)
+    out = torch.zeros_like(inp)
+    cm.Mdir(inp, out, 1, -1)
+    assert orc.rel_dev_sq(ref, host(out)) < tol
+    # active subset of R of the R + 2 columns
+    full = dev(x, dt)
+    outf = torch.full_like(full, 7.0)
+    active = list(range(R + 1, 1, -1))[:R]  # R columns in reverse order, skipping columns 0 and 1
+    cm.Mdag(full, outf, active=active)
+    reff = orc.coarse_apply(dims, A, x, orc.OP_MDAG)
+    got = host(outf)
+    for c in range(R + 2):
+        if c in active:
+            assert orc.rel_dev_sq(reff[:, c], got[:, c]) < tol
+        else:
+            assert np.all(got[:, c] == 7.0)
+
+
 def test_construct_remaining_links_matches_oracle():
     dims, N = (4, 2, 4, 2), 8
     A = inputs.gaussian_field((9, 64, N, N), inputs.rng(stream=105))
