@@ -223,6 +223,9 @@ gmg_status wilson_apply_f32_in(gmg_wilson* h, int op, int nrhs, const float* in,
 // [V][3][nrhs][4] (the 16-byte quarters of one site's records back to back)
 gmg_status wilson_apply_mr_bf16(gmg_wilson* h, int nrhs, const uint32_t* in, uint32_t* out, double2* d1, double2* d2,
                                 cudaStream_t s, bool blocked = false);
+// r = b - M x, FP64 fields (32-byte aligned)
+gmg_status wilson_residual_f64(gmg_wilson* h, int nrhs, const double* b, const double* x, double* r,
+                               cudaStream_t s);
 // out = bf16(b - M x), site-blocked BF16 out, FP32 b and x (32-byte aligned)
 gmg_status wilson_residual_bf16(gmg_wilson* h, int nrhs, const float* b, const float* x, uint32_t* out,
                                 cudaStream_t s);

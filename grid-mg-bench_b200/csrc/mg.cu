@@ -122,6 +122,17 @@ gmg_status apply_op(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s) {
                           (gmg_stream)s);
 }
 
+// r = b - A x on the fine level in FP64: one fused operator pass where the
+// tile kernel applies (4+ RHS, 32-byte aligned fields), else the operator and
+// a subtraction sweep
+gmg_status fine_residual(gmg_mg* h, const Vec& b, const Vec& x, Vec& r, cudaStream_t s) {
+  if (x.R >= 4 && x.prec == GMG_F64 && (((uintptr_t)b.p | (uintptr_t)x.p | (uintptr_t)r.p) & 31) == 0)
+    return wilson_residual_f64(h->L[0]->w, x.R, static_cast<const double*>(b.p), static_cast<const double*>(x.p),
+                               static_cast<double*>(r.p), s);
+  GMG_TRY(apply_op(h, 0, x, r, s));
+  return vec_xmy(b, r, s);
+}
+
 constexpr int kScalars = 8192;  // double2 slots of h->coef, h->dscr and h->hpin
 
 // host <- n device scalars (one stream synchronisation)
@@ -1426,8 +1437,7 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
   GMG_TRY(dots(h, Bfull, 1, 0, Bfull, bnz, s));
   // FP64 residual of every RHS; each cycle starts from it and refreshes it
   Vec Rfull = h->orr.with_rhs(nrhs);
-  GMG_TRY(apply_op(h, 0, Xfull, Rfull, s));
-  GMG_TRY(vec_xmy(Bfull, Rfull, s));
+  GMG_TRY(fine_residual(h, Bfull, Xfull, Rfull, s));
   while (!active.empty() && total < maxiter) {
     const int Ra = (int)active.size();
     // every RHS still active (the active list is ascending): the batch is the
@@ -1494,9 +1504,8 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
     const int before = total;
     total += std::max(it, 1);
     // true residuals of the batch decide who stays active, and start the next cycle
-    GMG_TRY(apply_op(h, 0, xA, rA, s));
+    GMG_TRY(fine_residual(h, bA, xA, rA, s));
     std::vector<zc> rn;
-    GMG_TRY(vec_xmy(bA, rA, s));
     if (!whole) GMG_TRY(vec_scatter(rA, idx.as<int>(), Rfull, s));
     GMG_TRY(dots(h, rA, 1, 0, rA, rn, s));
     std::vector<int> still;

@@ -1997,6 +1997,35 @@ gmg_status wilson_residual_bf16(gmg_wilson* h, int nrhs, const float* b, const f
   return GMG_OK;
 }
 
+// r = b - M x in FP64 ([V][nrhs][12], 32-byte aligned), one tile-kernel pass:
+// the outer solver's residual without a separate subtraction sweep
+gmg_status wilson_residual_f64(gmg_wilson* h, int nrhs, const double* b, const double* x, double* r,
+                               cudaStream_t s) {
+  GMG_CHECK((((uintptr_t)b | (uintptr_t)x | (uintptr_t)r) & 31) == 0, GMG_ERR_ARGUMENT,
+            "wilson residual (FP64): fields must be 32-byte aligned");
+  const int V = (int)h->dims.vol();
+  const int tvol = h->dims.d[0] * h->dims.d[1] * h->dims.d[2];
+  int rt = 1;
+  for (int c = std::min(nrhs, 16); c >= 1; --c)
+    if (nrhs % c == 0) {
+      rt = c;
+      break;
+    }
+  if (nrhs > 16 && rt < 8) rt = 16;
+  const int tiles = (V + kTileSites - 1) / kTileSites;
+  const size_t smem = sizeof(double2) * 2 * kTileSites * 72;
+  KernelTimer kt("wilson", s);
+  auto k = wilson_tile_kernel<double, false, 2, false, 2, true, double, double, 2, true>;
+  if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int g = wave_grid(k, kTileSites * rt, smem, tiles);
+  k<<<g, kTileSites * rt, smem, s>>>(h->hop.as<double2>(), h->clover.as<double2>(), h->nbr.as<int32_t>(),
+                                     reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(r), V, nrhs, rt,
+                                     4.0 + h->mass, GMG_OP_M, 0, 0, h->apbc, tvol, h->dims.d[3], nullptr, nullptr,
+                                     nullptr, 0, nullptr, reinterpret_cast<const double2*>(b));
+  GMG_CUDA(cudaGetLastError());
+  return GMG_OK;
+}
+
 gmg_status wilson_apply(gmg_wilson* h, int op, int dir, int disp, int vec_prec, int nrhs,
                         const void* in, void* out, cudaStream_t s) {
   if (vec_prec != GMG_F64 && vec_prec != GMG_F32)
