@@ -77,10 +77,9 @@ struct gmg_mg {
   gmg::VecBuf ozc, owc;   // compacted preconditioner output / operator output (in-cycle drop)
   gmg::DevBuf oidx, oidx2;
   bool outer_ready = false;
-  // captured K-cycle graphs per active-batch size (params.graph), their output
-  // buffer and the capture streams of the nested conditional bodies
+  // captured coarse-level solves of the K-cycle per active-batch size
+  // (params.graph) and the capture streams of the nested conditional bodies
   std::map<int, cudaGraphExec_t> kgraph;
-  gmg::VecBuf ogz;
   cudaStream_t cap_st[8] = {};
   bool graph_broken = false;
   // per-RHS outcome of the last solve: the outer iteration count at which the
@@ -671,7 +670,7 @@ Krylov level_krylov(MGLevel& L) {
 }
 
 // ------------------------------------------------------------- K-cycle
-gmg_status kcycle(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s);
+gmg_status kcycle(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s, cudaGraphExec_t graph = nullptr);
 
 gmg_status coarse_solve(gmg_mg* h, int lc, const Vec& b, Vec& x, cudaStream_t s) {
   MGLevel& C = *h->L[lc];
@@ -687,7 +686,9 @@ gmg_status coarse_solve(gmg_mg* h, int lc, const Vec& b, Vec& x, cudaStream_t s)
   return fgmres(h, lc, b, x, K, C.m, P.wrapper_iters, P.wrapper_tol, pc, true, nullptr, nullptr, s);
 }
 
-gmg_status kcycle(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s) {
+// graph: the captured coarse-level solve of level l + 1 for in.R RHS (l = 0
+// only), launched in place of the host-driven one
+gmg_status kcycle(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s, cudaGraphExec_t graph) {
   MGLevel& L = *h->L[l];
   MGLevel& C = *h->L[l + 1];
   const int R = in.R;
@@ -698,7 +699,10 @@ gmg_status kcycle(gmg_mg* h, int l, const Vec& in, Vec& out, cudaStream_t s) {
                           ? GMG_BF16
                           : (gmg_prec)in.prec;
   GMG_TRY(gmg_agg_project(L.agg, tc, (gmg_prec)in.prec, R, in.p, bc.p, (gmg_stream)s));
-  GMG_TRY(coarse_solve(h, l + 1, bc, xc, s));
+  if (graph)
+    GMG_CUDA(cudaGraphLaunch(graph, s));
+  else
+    GMG_TRY(coarse_solve(h, l + 1, bc, xc, s));
   GMG_TRY(gmg_agg_promote(L.agg, tc, (gmg_prec)in.prec, R, xc.p, out.p, (gmg_stream)s));
   return mr_smooth(h, l, in, out, h->P.smoother_iters, s);
 }
@@ -986,14 +990,19 @@ gmg_status graph_state(gmg_mg* h) {
   return GMG_OK;
 }
 
-// capture kcycle(0) on fixed buffers (input h->otz, output h->ogz) for R RHS
+// capture the coarse-level solve of kcycle(0) for R RHS: level 1's K-cycle
+// FGMRES and everything below it, on level 1's fixed right-hand-side and
+// solution buffers.  The fine-level steps (restriction, prolongation, MR
+// smoothing: a few large kernels) stay plain launches on the caller's vectors,
+// so the Krylov vectors need no copies in and out of fixed buffers.
 gmg_status build_kcycle_graph(gmg_mg* h, int R, cudaGraphExec_t* exec) {
   *exec = nullptr;
   GMG_TRY(graph_state(h));
   cudaStream_t s0 = h->cap_st[0];
-  Vec in = h->otz.with_rhs(R), out = h->ogz.with_rhs(R);
+  MGLevel& C = *h->L[1];
+  Vec bc = C.bc.with_rhs(R), xc = C.xc.with_rhs(R);
   GMG_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
-  gmg_status st = kcycle_cap(h, 0, in, out, 0);
+  gmg_status st = coarse_solve_cap(h, 1, bc, xc, 0);
   cudaGraph_t g = nullptr;
   // end every capture still open (an error inside a body leaves it open)
   for (int d = 7; d >= 1; --d) {
@@ -1085,7 +1094,6 @@ gmg_status outer_workspace(gmg_mg* h) {
     GMG_TRY(h->owc.alloc(V, R, 12, vp));
     GMG_TRY(h->oidx2.alloc(sizeof(int) * R));
   }
-  if (h->P.graph && zp != GMG_F64) GMG_TRY(h->ogz.alloc(V, R, 12, zp));
   h->outer_ready = true;
   return GMG_OK;
 }
@@ -1463,18 +1471,20 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
       // in: Krylov vector (FP64, or FP32 in an FP32 Arnoldi cycle); out: Z
       // direction in the preconditioner precision
       const int Rb = in.R;  // the active columns (fewer than the batch after an in-cycle drop)
-      Vec tin = tz.with_rhs(Rb);
       if (zp == GMG_F64) return kcycle(h, 0, in, out, s);
+      Vec src = in;
+      if (in.prec != zp) {  // an FP64 Arnoldi vector, converted for the FP32 cycle
+        src = tz.with_rhs(Rb);
+        GMG_TRY(vec_convert(in, src, s));
+      }
       const bool graph = h->P.graph && !h->graph_broken && Rb <= 1024;
-      if (!graph && in.prec == zp) return kcycle(h, 0, in, out, s);
-      // the captured cycle reads its input from tz
-      GMG_TRY(vec_convert(in, tin, s));
-      if (!graph) return kcycle(h, 0, tin, out, s);
+      if (!graph) return kcycle(h, 0, src, out, s);
       auto it = h->kgraph.find(Rb);
       if (it == h->kgraph.end()) {
         // first cycle of this batch size: host-driven (it also builds every
-        // buffer and tuning key the cycle needs), then captured for the next ones
-        GMG_TRY(kcycle(h, 0, tin, out, s));
+        // buffer and tuning key the cycle needs), then the coarse-level solve
+        // is captured for the next ones
+        GMG_TRY(kcycle(h, 0, src, out, s));
         GMG_CUDA(cudaStreamSynchronize(s));
         cudaGraphExec_t ex = nullptr;
         if (build_kcycle_graph(h, Rb, &ex) == GMG_OK)
@@ -1483,9 +1493,7 @@ extern "C" gmg_status gmg_mg_solve(gmg_mg* h, int nrhs, const double* b, double*
           h->graph_broken = true;  // keep the host-driven cycle
         return GMG_OK;
       }
-      GMG_CUDA(cudaGraphLaunch(it->second, s));
-      GMG_CUDA(cudaMemcpyAsync(out.p, h->ogz.p, out.bytes(), cudaMemcpyDeviceToDevice, s));
-      return GMG_OK;
+      return kcycle(h, 0, src, out, s, it->second);
     };
     int it = 0;
     std::vector<double> rr;

@@ -391,7 +391,9 @@ typedef struct {
                             previous pass's vectors (inverse iteration) */
   int setup_null;        /* 1: null-vector setup (setupBasisVectorsType nullVectors: solve A psi = 0 from
                             psi = v); 0: test-vector setup (solve A psi = v from psi = 0) */
-  int graph;             /* 1: replay the K-cycle preconditioner as a CUDA graph.  The coarse-level
+  int graph;             /* 1: replay the K-cycle's coarse-level solve (level 1's K-cycle FGMRES and
+                            everything below it) as a CUDA graph; the fine level's restriction,
+                            prolongation and smoother are plain launches on the Krylov vectors.  The coarse-level
                             solvers keep their Hessenberg / Givens state on the device; each restart
                             cycle and each Arnoldi step is a conditional (IF) node that a device kernel
                             switches on while the level's tolerance and iteration limit are not met,
