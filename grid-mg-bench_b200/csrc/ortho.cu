@@ -443,24 +443,52 @@ __global__ void __launch_bounds__(kSolveThreads) tri_solve_kernel(Params P) {
     for (int i = 0; i < NMAX; ++i) w[i] = (i < N && k < K) ? pre[i * NTS + t] : make_double2(0.0, 0.0);
     prefetch(nc, nch);  // the slots are free again: copy the next item's columns meanwhile
     if (k < K) {
+      // rows in groups of four: the products with the already solved entries
+      // (j below the group) are independent across the group's rows, two
+      // partial sums each, so eight chains run side by side; then the group's
+      // own 4 x 4 triangle in order
 #pragma unroll
-      for (int i = 0; i < NMAX; ++i) {
-        if (i < N) {
-          // four partial sums (j mod 4) shorten the dependent chains
-          const double2* Li = L + i * (i + 1) / 2;
-          double2 sp[4] = {w[i], make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+      for (int i0 = 0; i0 < NMAX; i0 += 4) {
+        if (i0 < N) {
+          double2 sp[4][2];
 #pragma unroll
-          for (int j = 0; j < i; ++j) {  // s -= conj(L[i][j]) w[j]
-            const double2 a = Li[j];
-            double2& s = sp[j & 3];
-            s.x = fma(-a.x, w[j].x, s.x);
-            s.x = fma(a.y, w[j].y, s.x);
-            s.y = fma(-a.x, w[j].y, s.y);
-            s.y = fma(-a.y, w[j].x, s.y);
+          for (int q = 0; q < 4; ++q) {
+            sp[q][0] = (i0 + q < N) ? w[i0 + q] : make_double2(0.0, 0.0);
+            sp[q][1] = make_double2(0.0, 0.0);
           }
-          const double inv = Li[i].x;
-          w[i] = make_double2(((sp[0].x + sp[1].x) + (sp[2].x + sp[3].x)) * inv,
-                              ((sp[0].y + sp[1].y) + (sp[2].y + sp[3].y)) * inv);
+#pragma unroll
+          for (int j = 0; j < i0; ++j) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {  // s -= conj(L[i][j]) w[j]
+              const int i = i0 + q;
+              if (i < NMAX && i < N) {  // L holds the N (N + 1) / 2 entries of rows i < N only
+                const double2 a = L[i * (i + 1) / 2 + j];
+                double2& sq = sp[q][j & 1];
+                sq.x = fma(-a.x, w[j].x, sq.x);
+                sq.x = fma(a.y, w[j].y, sq.x);
+                sq.y = fma(-a.x, w[j].y, sq.y);
+                sq.y = fma(-a.y, w[j].x, sq.y);
+              }
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int i = i0 + q;
+            if (i < NMAX && i < N) {
+              const double2* Li = L + i * (i + 1) / 2;
+              double2 sq = make_double2(sp[q][0].x + sp[q][1].x, sp[q][0].y + sp[q][1].y);
+#pragma unroll
+              for (int j = i0; j < i; ++j) {
+                const double2 a = Li[j];
+                sq.x = fma(-a.x, w[j].x, sq.x);
+                sq.x = fma(a.y, w[j].y, sq.x);
+                sq.y = fma(-a.x, w[j].y, sq.y);
+                sq.y = fma(-a.y, w[j].x, sq.y);
+              }
+              const double inv = Li[i].x;
+              w[i] = make_double2(sq.x * inv, sq.y * inv);
+            }
+          }
         }
       }
       double2* col = P.basis + (int64_t)c * N * K + k;
