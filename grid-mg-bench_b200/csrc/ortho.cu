@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(32 * kFactorWarps) factor_kernel(Params P) {
     }
 }
 
-constexpr int kSolveThreads = 128;  // columns per solve chunk (three CTAs per SM at 170 registers)
+constexpr int kSolveThreads = 128;  // columns per solve chunk (two CTAs per SM at 208 registers, N = 32)
 
 // W = conj(L)^{-1} V for every column of every block: thread per column, the
 // column in registers (NMAX entries, rows >= N unused), conj(L) in shared
