@@ -388,20 +388,26 @@ __global__ void __launch_bounds__(32 * kFactorWarps) factor_kernel(Params P) {
     }
 }
 
-constexpr int kSolveThreads = 128;  // columns per solve chunk (two CTAs per SM at 208 registers, N = 32)
+constexpr int kSolveThreads = 128;  // columns per solve chunk (three CTAs per SM at N = 32)
 
 // W = conj(L)^{-1} V for every column of every block: thread per column, the
 // column in registers (NMAX entries, rows >= N unused), conj(L) in shared
 // memory; the CTA walks the blocks of its grid stride and every 256-column
 // chunk of each, with the next chunk's columns copied into shared memory while
 // the current chunk is solved.
-template <int NMAX>
-__global__ void __launch_bounds__(kSolveThreads) tri_solve_kernel(Params P) {
+// EXACT: nbasis equals NMAX, so that every row bound is a compile-time
+// constant (no guards between the row groups' independent products; at
+// N = 32 that also frees registers: 176 instead of 214, and 168 without
+// spills at three CTAs per SM, tri_solve32_kernel).  C3 (32^4, 4^4 blocks,
+// N 32): 3.26 ms with the guards at two CTAs per SM, 2.98 ms without, 2.83 ms
+// without at three.
+template <int NMAX, bool EXACT>
+__device__ __forceinline__ void tri_solve_body(const Params& P) {
   constexpr int NTS = kSolveThreads;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* pre = reinterpret_cast<double2*>(smem_raw);  // [NMAX][NTS]: the prefetched columns
   double2* L = pre + NMAX * NTS;                        // packed conj(L) of the current block
-  const int N = P.N, K = P.K, t = threadIdx.x;
+  const int N = EXACT ? NMAX : P.N, K = P.K, t = threadIdx.x;
   const int nl = N * (N + 1) / 2;
   const int chunks = (K + NTS - 1) / NTS;
   // this CTA's work items (block, chunk) in order, skipping inactive blocks
@@ -502,6 +508,13 @@ __global__ void __launch_bounds__(kSolveThreads) tri_solve_kernel(Params P) {
   }
   cp_async_wait<0>();
 }
+
+template <int NMAX, bool EXACT>
+__global__ void __launch_bounds__(kSolveThreads) tri_solve_kernel(Params P) {
+  tri_solve_body<NMAX, EXACT>(P);
+}
+
+__global__ void __launch_bounds__(kSolveThreads, 3) tri_solve32_kernel(Params P) { tri_solve_body<32, true>(P); }
 
 // Cholesky G + shift I = L L^dag in place by the whole CTA (strict lower
 // triangle of G, row-major N x N; the diagonal goes to diag[]); false to every
@@ -767,11 +780,18 @@ static gmg_status launch_factor(const Params& P, cudaStream_t s) {
 template <int NMAX>
 static gmg_status launch_solve(const Params& P, cudaStream_t s) {
   const size_t smem = sizeof(double2) * ((size_t)NMAX * kSolveThreads + (size_t)P.N * (P.N + 1) / 2);
-  GMG_CUDA(cudaFuncSetAttribute(tri_solve_kernel<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  void (*kern)(Params) = tri_solve_kernel<NMAX, false>;
+  if (P.N == NMAX) {
+    if constexpr (NMAX == 32)
+      kern = tri_solve32_kernel;
+    else
+      kern = tri_solve_kernel<NMAX, true>;
+  }
+  GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 1;
-  GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tri_solve_kernel<NMAX>, kSolveThreads, smem));
+  GMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSolveThreads, smem));
   const int grid = std::min(P.Vc, num_sms() * std::max(per_sm, 1));
-  tri_solve_kernel<NMAX><<<grid, kSolveThreads, smem, s>>>(P);
+  kern<<<grid, kSolveThreads, smem, s>>>(P);
   GMG_CUDA(cudaGetLastError());
   return GMG_OK;
 }
