@@ -102,7 +102,7 @@ inline Geo geometry(int N) {
   g.kgw = std::max(1, 8 / g.ntw);
   g.ntiles = g.NT * (g.NT + 1) / 2;
   g.KC = 32;
-  for (int kc : {64, 48, 32}) {
+  for (int kc : {64, 32}) {  // both divide kThreads (the copy mapping relies on it)
     if ((kc / 4) % g.kgw) continue;
     if (sizeof(double2) * kStages * (size_t)kc * g.Np <= 72 * 1024) {
       g.KC = kc;
@@ -142,7 +142,7 @@ template <int NT, int TW>
 __device__ __forceinline__ void gram_steps(double (&acc)[NT + 1][2], const double* fb, int stride_d, int grp, int nk4,
                                            int kgw) {
   constexpr int I1 = TW, I2 = NT - 1 - TW;
-  if (NT > 5) {
+  if (NT > 4) {
     // (the register budget of three CTAs per SM holds one set of fragments only)
     for (int k4 = grp; k4 < nk4; k4 += kgw) {
       const double* f = fb + 4 * k4 * stride_d;
@@ -208,6 +208,10 @@ __global__ void __launch_bounds__(kThreads, 3) gram_kernel(Params P) {
   const int I1 = tw, I2 = NT - 1 - tw;  // this warp's tile rows (the same when NT is odd and tw is the middle)
   const int nch = (K + KC - 1) / KC;
   const int stage_elems = kStages * KC * Np;
+  // KC (32 or 64) divides the thread count: a thread copies one k offset of
+  // every chunk, for every (kThreads / KC)-th row, with no division per copy
+  const int kshift = KC == 64 ? 6 : 5;
+  const int ckk = t & (KC - 1), ci0 = t >> kshift, istep = kThreads >> kshift;
   // zero the staging buffers once: rows i >= N and k rows past the end of a
   // partial last chunk must read as zero
   for (int e = t; e < stage_elems; e += kThreads) stage[e] = make_double2(0.0, 0.0);
@@ -221,13 +225,17 @@ __global__ void __launch_bounds__(kThreads, 3) gram_kernel(Params P) {
         double2* buf = stage + (ch % kStages) * KC * Np;
         const int k0 = ch * KC;
         const int kc = min(KC, K - k0);
-        for (int e = t; e < N * KC; e += kThreads) {
-          const int i = e / KC, kk = e - i * KC;
-          if (kk < kc) cp_async16(buf + kk * Np + i, Vb + (int64_t)i * K + k0 + kk);
+        // this thread's copies: k offset ckk, rows ci0, ci0 + istep, ...
+        if (ckk < kc) {
+          const double2* src = Vb + (int64_t)ci0 * K + k0 + ckk;
+          for (int i = ci0; i < N; i += istep, src += (int64_t)istep * K) cp_async16(buf + ckk * Np + i, src);
         }
-        // a partial last chunk: the k rows up to the next multiple of 4 read as zero
-        const int kc4 = (kc + 3) & ~3;
-        for (int e = t; e < (kc4 - kc) * Np; e += kThreads) buf[(kc + e / Np) * Np + e % Np] = make_double2(0.0, 0.0);
+        if (kc < KC) {
+          // a partial last chunk: the k rows up to the next multiple of 4 read as zero
+          const int kc4 = (kc + 3) & ~3;
+          for (int e = t; e < (kc4 - kc) * Np; e += kThreads)
+            buf[(kc + e / Np) * Np + e % Np] = make_double2(0.0, 0.0);
+        }
       }
       cp_async_commit();  // an empty group past the last chunk keeps the group count uniform
     };
@@ -755,6 +763,7 @@ static gmg_status launch_gram(const Params& P, cudaStream_t s) {
   const Geo g = geometry(P.N);
   GMG_CHECK(g.NT <= kMaxNT, GMG_ERR_UNSUPPORTED, "orthonormalise: nbasis above the tensor-core Gram path");
   GMG_CHECK(g.smem <= 227 * 1024, GMG_ERR_UNSUPPORTED, "orthonormalise: tile does not fit shared memory");
+  GMG_CHECK((g.KC == 32 || g.KC == 64) && kThreads % g.KC == 0, GMG_ERR_UNSUPPORTED, "orthonormalise: chunk size");
   switch (g.NT) {
     case 1: return launch_gram_nt<1, CHECK>(P, g, s);
     case 2: return launch_gram_nt<2, CHECK>(P, g, s);
