@@ -325,15 +325,24 @@ __device__ __forceinline__ void st12x(typename wt<TO>::C* __restrict__ base, int
 // coarsening's self term in one pass.
 // VOUT: the output record layout (VEC by default); SUB: write bsub - M in
 // (bsub laid out and typed as the input) instead of M in.
+// NBS: nbr is a tile's staged neighbour table, entry p of this site at
+// nbr[p * nbs_stride + nbs_i] (instead of nbr[p * V + site]).
 template <class T, class LinkFn, bool DOTS = false, int VEC = 0, bool LDAG = false, bool PF = false, class TI = T,
-          class TO = T, int VOUT = VEC, bool SUB = false>
+          class TO = T, int VOUT = VEC, bool SUB = false, bool NBS = false>
 __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict__ cl, LinkFn links,
                                             const int32_t* __restrict__ nbr, const typename wt<TI>::C* __restrict__ in,
                                             typename wt<TO>::C* __restrict__ out, int V, int nrhs, int site, int r,
                                             T diag, int op, int dir, int disp, int apbc, int tvol, int Lt,
                                             double* dsum = nullptr, int skip = 0,
-                                            const typename wt<TI>::C* __restrict__ bsub = nullptr) {
+                                            const typename wt<TI>::C* __restrict__ bsub = nullptr, int nbs_stride = 0,
+                                            int nbs_i = 0) {
   typedef typename wt<T>::C C;
+  auto nbidx = [&](int p) -> int {
+    if constexpr (NBS)
+      return nbr[p * nbs_stride + nbs_i];
+    else
+      return nbr[(int64_t)p * V + site];
+  };
   const bool g5 = (op == GMG_OP_MDAG);
   const int tc = site / tvol;
   C acc[4][3];
@@ -349,7 +358,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
     // latency overlaps the previous hop's arithmetic
     int nbs[8];
 #pragma unroll
-    for (int p = 0; p < 8; ++p) nbs[p] = nbr[(int64_t)p * V + site];
+    for (int p = 0; p < 8; ++p) nbs[p] = nbidx(p);
     C psi[12];
     typename RawRec<T, TI>::type nxt[12];
     ld12x<T, TI, VEC>(psi, in, site, r, nrhs);
@@ -412,7 +421,7 @@ __device__ __forceinline__ void wilson_site(const typename wt<T>::C* __restrict_
       const int dsp = p < 4 ? 1 : -1;
       if (op == GMG_OP_MDIR && (mu != dir || dsp != disp)) continue;
       if (skip & (1 << p)) continue;
-      const int nb = nbr[(int64_t)p * V + site];
+      const int nb = nbidx(p);
       T coef = (T)-0.5;
       if (apbc && mu == 3 && ((dsp > 0 && tc == Lt - 1) || (dsp < 0 && tc == 0))) coef = (T)0.5;
       C psi[12];
@@ -481,6 +490,17 @@ __global__ void __launch_bounds__(256) wilson_kernel(
 
 constexpr int kTileSites = 16;
 
+// bytes of one staging buffer of the tile kernel for link / clover entries of
+// csize bytes: the tile's hop links and clover blocks and, without SEL, its
+// neighbour table
+__host__ __device__ constexpr int tile_stage_bytes(int csize, bool sel) {
+  return csize * 2 * kTileSites * 72 + (sel ? 0 : 4 * 8 * kTileSites);
+}
+// shared memory of a tile kernel launch (dots: the DOTS products' bytes)
+constexpr size_t tile_smem(int csize, bool sel, size_t dots) {
+  return (size_t)(sel ? 1 : 2) * tile_stage_bytes(csize, sel) + dots;
+}
+
 // Multi-RHS tile kernel: a CTA takes kTileSites consecutive sites and all
 // right-hand sides (rt threads per site, each looping over its RHS); the
 // sites' 8 hop links and clover blocks are staged in shared memory once and
@@ -507,9 +527,12 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
     const typename wt<TI>::C* __restrict__ bsub = nullptr) {
   typedef typename wt<T>::C C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* Ls = reinterpret_cast<C*>(smem_raw);  // [kTileSites][8][9]: p < 4 U_mu(x), p >= 4 U_mu(x - mu)^dagger
-  C* Cs = Ls + kTileSites * 72;            // [kTileSites][72]
-  double* Ds = reinterpret_cast<double*>(Cs + kTileSites * 72);  // DOTS: [nrhs][3]
+  // staging buffers (tile_stage_bytes each; two without SEL, the next tile's
+  // filled while this one is computed): [kTileSites][8][9] hop links (p < 4
+  // U_mu(x), p >= 4 U_mu(x - mu)^dagger), [kTileSites][72] clover and, without
+  // SEL, the [8][kTileSites] neighbour table; then DOTS: [nrhs][3] products
+  constexpr int kBuf = tile_stage_bytes(sizeof(C), SEL);
+  double* Ds = reinterpret_cast<double*>(smem_raw + (SEL ? 1 : 2) * kBuf);
   if (DOTS)
     for (int k = threadIdx.x; k < 3 * nrhs; k += blockDim.x) Ds[k] = 0.0;
   const int nsites = (SEL && sel) ? nsel : V;
@@ -517,23 +540,10 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
   const int sl = threadIdx.x / rt, rl = threadIdx.x % rt;
   const bool two = nrhs <= 2 * rt;
   double da[3] = {0.0, 0.0, 0.0}, db[3] = {0.0, 0.0, 0.0};
-  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+  // the tile's sites from buffer buf (links Ls, clover Cs, neighbour table Ns or nullptr)
+  auto compute = [&](int tile, const C* Ls, const C* Cs, const int32_t* Ns) {
     const int s0 = tile * kTileSites;
     const int ns = min(kTileSites, nsites - s0);
-    __syncthreads();
-    if (!SEL) {
-      for (int k = threadIdx.x; k < ns * 72; k += blockDim.x) {
-        Ls[k] = hop[(int64_t)s0 * 72 + k];
-        Cs[k] = clover[(int64_t)s0 * 72 + k];
-      }
-    } else {
-      for (int k = threadIdx.x; k < ns * 72; k += blockDim.x) {
-        const int64_t st = sel ? sel[s0 + k / 72] : s0 + k / 72;
-        Ls[k] = hop[st * 72 + k % 72];
-        Cs[k] = clover[st * 72 + k % 72];
-      }
-    }
-    __syncthreads();
     if (sl < ns) {
       const int site = (SEL && sel) ? sel[s0 + sl] : s0 + sl;
       const int skip = (SEL && hskip) ? hskip[site] : 0;
@@ -544,8 +554,9 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
       int k = 0;
       for (int r = rl; r < nrhs; r += rt, ++k) {
         double dt[3] = {0.0, 0.0, 0.0};
-        wilson_site<T, decltype(links), DOTS, VEC, true, PF, TI, TO, VOUT, SUB>(
-            Cs + sl * 72, links, nbr, in, out, V, nrhs, site, r, diag, op, dir, disp, apbc, tvol, Lt, dt, skip, bsub);
+        wilson_site<T, decltype(links), DOTS, VEC, true, PF, TI, TO, VOUT, SUB, !SEL>(
+            Cs + sl * 72, links, SEL ? nbr : Ns, in, out, V, nrhs, site, r, diag, op, dir, disp, apbc, tvol, Lt, dt,
+            skip, bsub, kTileSites, sl);
         if (DOTS) {
           if (two) {
 #pragma unroll
@@ -563,6 +574,60 @@ __global__ void __launch_bounds__(256, MINB) wilson_tile_kernel(
         }
       }
     }
+  };
+  if constexpr (SEL) {
+    C* Ls = reinterpret_cast<C*>(smem_raw);
+    C* Cs = Ls + kTileSites * 72;
+    for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+      const int s0 = tile * kTileSites;
+      const int ns = min(kTileSites, nsites - s0);
+      __syncthreads();
+      for (int k = threadIdx.x; k < ns * 72; k += blockDim.x) {
+        const int64_t st = sel ? sel[s0 + k / 72] : s0 + k / 72;
+        Ls[k] = hop[st * 72 + k % 72];
+        Cs[k] = clover[st * 72 + k % 72];
+      }
+      __syncthreads();
+      compute(tile, Ls, Cs, nullptr);
+    }
+  } else {
+    // cp.async copies of a tile's links, clover (16-byte pieces: a site's 72
+    // entries are a multiple of 16 bytes, the arrays 16-byte aligned) and
+    // neighbour indices (4-byte pieces) into buffer b; one copy group per call,
+    // empty past the last tile
+    auto stage = [&](int tile, int b) {
+      if (tile < nt) {
+        const int s0 = tile * kTileSites;
+        const int ns = min(kTileSites, nsites - s0);
+        unsigned char* base = smem_raw + b * kBuf;
+        const int n16 = ns * 72 * (int)sizeof(C) / 16;
+        const unsigned char* hs = reinterpret_cast<const unsigned char*>(hop + (int64_t)s0 * 72);
+        const unsigned char* cs = reinterpret_cast<const unsigned char*>(clover + (int64_t)s0 * 72);
+        unsigned char* cd = base + kTileSites * 72 * sizeof(C);
+        for (int k = threadIdx.x; k < n16; k += blockDim.x) {
+          ac::cpa16(base + 16 * k, hs + 16 * k);
+          ac::cpa16(cd + 16 * k, cs + 16 * k);
+        }
+        int32_t* nd = reinterpret_cast<int32_t*>(base + 2 * kTileSites * 72 * sizeof(C));
+        for (int k = threadIdx.x; k < 8 * ns; k += blockDim.x) {
+          const int p = k / ns, j = k - p * ns;
+          ac::cpa4(nd + p * kTileSites + j, nbr + (int64_t)p * V + s0 + j);
+        }
+      }
+      ac::cpa_commit();
+    };
+    int b = 0;
+    stage(blockIdx.x, 0);
+    for (int tile = blockIdx.x; tile < nt; tile += gridDim.x, b ^= 1) {
+      stage(tile + gridDim.x, b ^ 1);  // buffer b ^ 1 was last read before the previous iteration's final barrier
+      ac::cpa_wait<1>();               // this thread's copies of this tile have landed
+      __syncthreads();                 // everyone's have
+      const unsigned char* base = smem_raw + b * kBuf;
+      const C* Ls = reinterpret_cast<const C*>(base);
+      compute(tile, Ls, Ls + kTileSites * 72, reinterpret_cast<const int32_t*>(base + 2 * kTileSites * 72 * sizeof(C)));
+      __syncthreads();  // buffer b is read: the next iteration's staging may overwrite it
+    }
+    ac::cpa_wait<0>();
   }
   if (DOTS) {
     if (two) {
@@ -1540,7 +1605,7 @@ static gmg_status launch_tile(gmg_wilson* h, int op, int dir, int disp, int vec_
   auto go = [&](auto kern, auto diag, const void* hp, const void* cp, size_t csize) -> gmg_status {
     typedef decltype(diag) T;
     typedef typename wt<T>::C C;
-    const size_t smem = csize * 2 * kTileSites * 72 + dots;
+    const size_t smem = tile_smem((int)csize, false, dots);
     if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int g = wave_grid(kern, kTileSites * rt, smem, tiles);
     kern<<<g, kTileSites * rt, smem, s>>>(reinterpret_cast<const C*>(hp), reinterpret_cast<const C*>(cp),
@@ -1817,7 +1882,7 @@ static gmg_status launch_tile_sel(gmg_wilson* h, int op, int dir, int disp, int 
   const int nsites = sel ? nsel : V;
   const int tiles = (nsites + kTileSites - 1) / kTileSites;
   const int g = std::min(tiles, 148 * 16);
-  const size_t smem = sizeof(double2) * 2 * kTileSites * 72;
+  const size_t smem = tile_smem(sizeof(double2), true, 0);
   const bool fast = !sel && ((((uintptr_t)in | (uintptr_t)out) & 31) == 0);
   auto k = fast ? wilson_tile_kernel<double, false, 2, true, 2> : wilson_tile_kernel<double, false, 2, true>;
   if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1909,7 +1974,7 @@ gmg_status wilson_apply_f32_in(gmg_wilson* h, int op, int nrhs, const float* in,
   if (nrhs > 16 && rt < 8) rt = 16;
   const int tiles = (V + kTileSites - 1) / kTileSites;
   const int g = std::min(tiles, 148 * 16);
-  const size_t smem = sizeof(double2) * 2 * kTileSites * 72;
+  const size_t smem = tile_smem(sizeof(double2), false, 0);
   const uintptr_t al = (uintptr_t)in | (uintptr_t)out;
   KernelTimer kt("wilson", s);
   auto go = [&](auto kern) -> gmg_status {
@@ -1950,7 +2015,7 @@ gmg_status wilson_apply_mr_bf16(gmg_wilson* h, int nrhs, const uint32_t* in, uin
   if (nrhs > 16 && rt < 8) rt = 16;
   const int tiles = (V + kTileSites - 1) / kTileSites;
 
-  const size_t smem = sizeof(float2) * 2 * kTileSites * 72 + sizeof(double) * 3 * (size_t)nrhs;
+  const size_t smem = tile_smem(sizeof(float2), false, sizeof(double) * 3 * (size_t)nrhs);
   KernelTimer kt("wilson", s);
   GMG_CUDA(cudaMemsetAsync(d1, 0, sizeof(double2) * nrhs, s));
   GMG_CUDA(cudaMemsetAsync(d2, 0, sizeof(double2) * nrhs, s));
@@ -1985,9 +2050,10 @@ gmg_status wilson_residual_bf16(gmg_wilson* h, int nrhs, const float* b, const f
     }
   if (nrhs > 16 && rt < 8) rt = 16;
   const int tiles = (V + kTileSites - 1) / kTileSites;
-  const size_t smem = sizeof(float2) * 2 * kTileSites * 72;
+  const size_t smem = tile_smem(sizeof(float2), false, 0);
   KernelTimer kt("wilson", s);
   auto k = wilson_tile_kernel<float, false, 3, false, 2, true, float, bf16s, 3, true>;
+  if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int g = wave_grid(k, kTileSites * rt, smem, tiles);
   k<<<g, kTileSites * rt, smem, s>>>(h->hop_f.as<float2>(), h->clover_f.as<float2>(), h->nbr.as<int32_t>(),
                                      reinterpret_cast<const float2*>(x), out, V, nrhs, rt, (float)(4.0 + h->mass),
@@ -2013,7 +2079,7 @@ gmg_status wilson_residual_f64(gmg_wilson* h, int nrhs, const double* b, const d
     }
   if (nrhs > 16 && rt < 8) rt = 16;
   const int tiles = (V + kTileSites - 1) / kTileSites;
-  const size_t smem = sizeof(double2) * 2 * kTileSites * 72;
+  const size_t smem = tile_smem(sizeof(double2), false, 0);
   KernelTimer kt("wilson", s);
   auto k = wilson_tile_kernel<double, false, 2, false, 2, true, double, double, 2, true>;
   if (smem > 48 * 1024) GMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
