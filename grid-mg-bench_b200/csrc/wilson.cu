@@ -503,9 +503,10 @@ constexpr size_t tile_smem(int csize, bool sel, size_t dots) {
 
 // Multi-RHS tile kernel: a CTA takes kTileSites consecutive sites and all
 // right-hand sides (rt threads per site, each looping over its RHS); the
-// sites' 8 hop links and clover blocks are staged in shared memory once and
-// read by every RHS of the tile.  Thread per (site, RHS) otherwise, spinors
-// read from global memory.
+// sites' 8 hop links, clover blocks and neighbour indices are staged in
+// shared memory once and read by every RHS of the tile, the next tile's copied
+// (cp.async) into a second buffer while this one computes.  Thread per (site,
+// RHS) otherwise, spinors read from global memory.
 // SEL (the coarsening's self term, compiled separately): the tiles run over
 // the nsel sites of the list `sel` (all V sites when null) and only those are
 // written; hskip (per site, bit p: leave hop p out) restricts the hops to
