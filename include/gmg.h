@@ -101,7 +101,10 @@ gmg_status gmg_coarse_apply(gmg_coarse* h, gmg_op op, int point, gmg_prec comput
    right-hand sides over npoints stencil points (9 for M) in `compute`
    (GMG_BF16 / GMG_F16); 0, 0 before the first such apply.  The first apply
    of each (nbasis, padded nrhs, volume, point count, operand kind) times every
-   shape that fits and keeps the fastest.  No counterpart in the reference. */
+   shape that fits and keeps the fastest, each timed launch after a write of a
+   192 MB buffer that evicts L2 (as a solve's other work does); that buffer is
+   allocated on the first tuning call on a device and kept for the process.
+   No counterpart in the reference. */
 gmg_status gmg_coarse_tuned_shape(gmg_coarse* h, int nrhs, int npoints, gmg_prec compute, int* ctas,
                                   int* points_per_stage);
 /* Force the tensor-core stencil shape of this handle (CTAs per SM 1 or 2,
