@@ -498,6 +498,43 @@ def test_wilson_odd_lattices(dims, nrhs, variant):
     assert w.device_error() == (0, 0)
 
 
+def test_wilson_tile_kernel_several_tiles_per_cta():
+    # 644 tiles of 16 sites (the last one partial): more than one resident
+    # wave of CTAs holds (at most 4 x 148), so every CTA computes two or more
+    # tiles, alternating between its two staging buffers.  M and Mdag in FP64
+    # and FP32 at 16 and 24 RHS, and the BF16 smoother form with its products
+    dims = (13, 11, 8, 9)
+    V = int(np.prod(dims))
+    U = inputs.hot_gauge(dims, inputs.rng(stream=231))
+    w = gmg.WilsonClover(dims, -0.2, 1.0, antiperiodic=True)
+    w.set_gauge(U)
+    w.set_kernel("tile")
+    cl = orc.clover_build(dims, U, 1.0)
+    for nrhs in (16, 24):
+        x = inputs.gaussian_field((V, nrhs, 12), inputs.rng(stream=232 + nrhs))
+        for op, code in (("M", orc.OP_M), ("Mdag", orc.OP_MDAG)):
+            ref = orc.wilson_clover(dims, U, cl, -0.2, 1, x, code)
+            out = torch.zeros((V, nrhs, 12), dtype=torch.complex128, device=DEV)
+            getattr(w, op)(dev(x), out)
+            assert orc.rel_dev_sq(ref, host(out)) < TOL64, (op, nrhs)
+            out32 = torch.zeros((V, nrhs, 12), dtype=torch.complex64, device=DEV)
+            getattr(w, op)(dev(x, torch.complex64), out32)
+            assert orc.rel_dev_sq(ref, host(out32)) < TOL32, (op, nrhs)
+    # the BF16 smoother form (within BF16 rounding, as in the 512-site test)
+    xb = torch.view_as_real(dev(x, torch.complex64)).to(torch.bfloat16).contiguous()
+    xr = torch.view_as_complex(xb.float()).to(torch.complex128)
+    ref = orc.wilson_clover(dims, U, cl, -0.2, 1, host(xr), orc.OP_M)
+    outb = torch.zeros_like(xb)
+    d1, d2 = w.M_mr(xb, outb)
+    got = torch.view_as_complex(outb.float()).to(torch.complex128)
+    assert orc.rel_dev_sq(ref, host(got)) < 4e-5
+    d1_ref = np.einsum("srk,srk->r", ref.conj(), host(xr))
+    d2_ref = np.einsum("srk,srk->r", ref.conj(), ref).real
+    assert np.abs(d1.cpu().numpy() - d1_ref).max() / np.abs(d2_ref).max() < 1e-5
+    assert np.abs(d2.cpu().numpy() - d2_ref).max() / np.abs(d2_ref).max() < 1e-5
+    assert w.device_error() == (0, 0)
+
+
 @pytest.mark.parametrize("variant", VARIANTS)
 def test_wilson_multi_rhs_mdir(wil, forced, variant):
     # the single-hop form (CoarsenOperator's Mdir calls, nrhs >= 4) of every variant
